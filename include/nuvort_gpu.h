@@ -1,0 +1,192 @@
+/*
+ * nuvort_gpu.h -- C ABI of libnuvort_gpu.so, the B200 (sm_100a) filament-velocity
+ * path of the NuVort quantised-vortex code.
+ *
+ * The reference (a Fortran 90 program) has no plugin or FFI layer: its hot path is a
+ * set of argument-less module procedures called in order from the time loop in
+ * src/run.f90:24-65, communicating through the module globals f(:), pcount, t, dt and
+ * the run.in parameters (src/cdata.f90:19-127).  Each stage call below replaces one of
+ * those procedures and keeps its semantics; the filament state lives on the GPU between
+ * calls.  A Fortran caller binds these with ISO_C_BINDING (see fortran/nuvort_gpu.f90).
+ *
+ * Conventions
+ *   - Every function returns an int status: NV_OK (0) or a negative NV_ERR_* code.
+ *     nv_last_error() returns a message for the calling thread's last failure.
+ *     The reference prints and calls `stop` instead (fatal_error, src/cdata.f90:245-255).
+ *   - Slots are 1-based and system-local exactly as in the reference: infront==0 marks an
+ *     empty slot; pcount counts slots, empty ones included.
+ *   - Host arrays of 3-vectors are point-major, the memory layout of a Fortran
+ *     real(c_double) :: a(3,pcount) array: a[3*(k-1)+c] holds f(k)%x(c+1).
+ *   - A handle holds nsys independent filament systems (an ensemble).  A handle is used by
+ *     one host thread at a time and owns one CUDA stream; it is not reentrant.
+ *   - The library owns all device memory.  Host pointers are read or written only during
+ *     the call that receives them.
+ */
+#ifndef NUVORT_GPU_H
+#define NUVORT_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+enum {
+  NV_OK = 0,
+  NV_ERR_ARG = -1,         /* invalid argument */
+  NV_ERR_CUDA = -2,        /* CUDA runtime failure */
+  NV_ERR_CAPACITY = -3,    /* pinsert needed a slot beyond the system's capacity */
+  NV_ERR_SINGULAR = -4,    /* tree walk met dist<epsilon (src/tree.f90:289-295) */
+  NV_ERR_TREE_DEPTH = -5,  /* octree deeper than NV_TREE_MAX_DEPTH levels */
+  NV_ERR_NAN = -6,         /* NaN position (NAN_finder, src/general.f90:172-190) */
+  NV_ERR_EMPTY = -7,       /* no live points left (src/line.f90:25-27) */
+  NV_ERR_TIMESTEP = -8,    /* dt fails timestep_check (src/initial.f90:169-180) */
+  NV_ERR_UNSUPPORTED = -9, /* option outside this library (solid walls, grid normal fluid) */
+  NV_ERR_STATE = -10,      /* call out of order (e.g. tree search with no tree built) */
+  NV_ERR_QUEUE = -11,      /* serial topology resolver overflowed its work queue */
+  NV_ERR_IO = -12          /* run.in could not be opened */
+};
+
+/* ---- option values (the run.in strings of src/cdata.f90:131-241) -------------------- */
+enum { NV_VEL_LIA = 0, NV_VEL_BS = 1, NV_VEL_TREE = 2 };               /* velocity */
+enum { NV_BC_PERIODIC = 0, NV_BC_OPEN = 1, NV_BC_SOLID = 2 };          /* boundary_x/y/z */
+/* normal_velocity: 'zero' and 'xflow' as in src/normal_fluid.f90:94-97; 'uniform' is an
+ * extension (a constant vector norm_vel_vec) that the reference lacks. */
+enum { NV_NF_ZERO = 0, NV_NF_XFLOW = 1, NV_NF_UNIFORM = 2 };
+/* precision of the non-local sum: FP64 reproduces the reference's arithmetic; MIXED runs the
+ * far field in FP32 with compensated accumulation and keeps the near field in FP64. */
+enum { NV_PREC_FP64 = 0, NV_PREC_MIXED = 1 };
+/* non-local evaluation inside a handle: follow `velocity`, or (batched ensembles) pick the
+ * direct sum below a point-count crossover and the tree above it. */
+enum { NV_SCHED_AS_SET = 0, NV_SCHED_CROSSOVER = 1 };
+
+#define NV_TREE_MAX_DEPTH 42
+
+/* ---- parameters: one record per system; field names are the run.in keys ------------- */
+typedef struct nv_params {
+  int32_t nsteps;                 /* nsteps                                  cdata.f90:155 */
+  int32_t shots;                  /* shots                                   cdata.f90:158 */
+  int32_t recon_shots;            /* recon_shots (default 1)                 cdata.f90:161 */
+  int32_t velocity;               /* NV_VEL_*                                cdata.f90:181 */
+  int32_t boundary[3];            /* NV_BC_* for x,y,z (default periodic)    cdata.f90:184 */
+  int32_t normal_velocity;        /* NV_NF_*                                 cdata.f90:196 */
+  int32_t tree_extra_correction;  /* logical, default true                  cdata.f90:194 */
+  int32_t nan_test;               /* NAN_test, default true                 cdata.f90:218 */
+  int32_t overide_timestep_check; /* default false                           cdata.f90:222 */
+  int32_t precision;              /* NV_PREC_* (extension)                               */
+  double dt;                      /* dt                                      cdata.f90:167 */
+  double delta;                   /* delta                                   cdata.f90:170 */
+  double quant_circ;              /* default 9.97e-4                         cdata.f90:173 */
+  double corea;                   /* default 8.244023e-9                     cdata.f90:176 */
+  double box_size[3];             /* box_size                                cdata.f90:178 */
+  double tree_theta;              /* 0 = no tree, brute pclose               cdata.f90:190 */
+  double norm_vel_xflow;          /* default 0.5                             cdata.f90:202 */
+  double norm_vel_vec[3];         /* NV_NF_UNIFORM vector (extension)                    */
+  double alpha[2];                /* mutual friction alpha, alpha'           cdata.f90:204 */
+  double super_velocity[3];       /* imposed superflow                       cdata.f90:206 */
+  double normal_fluid_cutoff;     /* default 1e8                             cdata.f90:198 */
+  double t_zero_normal_fluid;     /* default 1e8                             cdata.f90:200 */
+} nv_params;
+
+/* Host view of one system's filament state (the fields of type(qvort), cdata.f90:19-29,
+ * that the hot path reads or writes).  Optional pointers may be NULL. */
+typedef struct nv_host_state {
+  int32_t pcount;     /* slots described by the arrays                           */
+  double *x;          /* [3*pcount] positions (required)                         */
+  double *u, *u1, *u2;/* [3*pcount] velocity and the two older velocities (opt.) */
+  double *ghosti;     /* [3*pcount] ghost of the point in front (optional)       */
+  double *ghostb;     /* [3*pcount] ghost of the point behind (optional)         */
+  int32_t *infront;   /* [pcount] 1-based, 0 = empty (required)                  */
+  int32_t *behind;    /* [pcount] (required)                                     */
+  int32_t *closest;   /* [pcount] reconnection candidate (optional)              */
+  double *closestd;   /* [pcount] its distance (optional)                        */
+} nv_host_state;
+
+/* Topology events, logged in the order the reference's serial sweeps make them. */
+enum { NV_EV_INSERT = 1, NV_EV_RECON = 2, NV_EV_REMOVE = 3, NV_EV_LOOPKILL = 4 };
+typedef struct nv_event {
+  int32_t itime; /* step number (the reference's itime)                                  */
+  int32_t kind;  /* NV_EV_*                                                              */
+  int32_t i;     /* INSERT: point i; RECON: point i; REMOVE: point i; LOOPKILL: start p   */
+  int32_t j;     /* INSERT: new slot; RECON: partner j; REMOVE: removed slot;
+                    LOOPKILL: points cleared                                            */
+} nv_event;
+
+typedef struct nv_counters {
+  int32_t pcount;        /* slots in use                                        */
+  int32_t live;          /* slots with infront>0                                */
+  int32_t recon_count;   /* reconnections so far         (recon_count)          */
+  int32_t remove_count;  /* premove removals so far      (remove_count)         */
+  int32_t insert_count;  /* pinsert insertions so far                           */
+  int32_t loop_kills;    /* loops cleared by loop_killer                        */
+  int64_t tree_eval;     /* accepted tree interactions in the last velocity pass */
+  int32_t itime;         /* last completed step                                 */
+  int32_t n_events;      /* events logged so far (ring buffer may have dropped) */
+  double t;              /* simulation time                                     */
+} nv_counters;
+
+typedef struct nv_handle nv_handle;
+
+/* ---- set-up ------------------------------------------------------------------------ */
+/* Fill *p with the reference defaults of src/cdata.f90:76-127. */
+int nv_params_default(nv_params *p);
+/* Read a run.in file into *p (fields not named in the file keep their values), with the
+ * semantics of read_run_file, src/cdata.f90:131-241: `key value` lines split at the first
+ * blank, unknown keys ignored, and a value that fails to parse ends the read silently. */
+int nv_read_run_file(const char *path, nv_params *p);
+/* Check one system's parameters as init_setup does (src/initial.f90:14-146). */
+int nv_check_params(const nv_params *p);
+
+/* Create a handle for nsys systems.  params[s] holds system s's parameters and
+ * capacity[s] its maximum slot count (pinsert appends beyond pcount up to it).
+ * All systems share params[0].precision.  device selects the CUDA device. */
+int nv_create(const nv_params *params, int32_t nsys, const int32_t *capacity,
+              int32_t device, nv_handle **out);
+int nv_destroy(nv_handle *h);
+
+/* Copy one system's state to the device (replaces f(:), pcount) and set its clock. */
+int nv_upload(nv_handle *h, int32_t sys, const nv_host_state *st);
+/* Copy one system's state back.  Arrays must hold at least `cap` slots; st->pcount
+ * receives the system's pcount (NV_ERR_ARG if it exceeds cap). */
+int nv_download(nv_handle *h, int32_t sys, nv_host_state *st, int32_t cap);
+int nv_set_clock(nv_handle *h, int32_t sys, double t, int32_t itime);
+int nv_counters_get(nv_handle *h, int32_t sys, nv_counters *c);
+/* Copy up to cap logged events of system sys; *n receives the number copied. */
+int nv_events_get(nv_handle *h, int32_t sys, nv_event *buf, int32_t cap, int32_t *n);
+
+/* ---- stages: one call per reference procedure, applied to every system -------------- */
+int nv_ghostp(nv_handle *h);            /* ghostp            src/boundary.f90:10-19      */
+int nv_construct_tree(nv_handle *h);    /* construct_tree    src/tree.f90:38-157         */
+int nv_pmotion(nv_handle *h);           /* pmotion           src/timestep.f90:16-45      */
+int nv_pinsert(nv_handle *h);           /* pinsert           src/line.f90:18-96          */
+int nv_pclose(nv_handle *h);            /* pclose_tree (tree_theta>0, src/tree.f90:190-244)
+                                           or pclose (src/line.f90:135-160)             */
+int nv_precon(nv_handle *h);            /* precon            src/reconnection.f90:11-61  */
+int nv_premove(nv_handle *h);           /* premove           src/line.f90:102-130        */
+int nv_enforce_boundary(nv_handle *h);  /* enforce_boundary  src/boundary.f90:91-138     */
+int nv_empty_tree(nv_handle *h);        /* empty_tree        src/tree.f90:160-186        */
+int nv_end_step(nv_handle *h);          /* t=t+dt, NAN_finder: src/run.f90:49,64         */
+
+/* Run nsteps whole time steps (the sequence of src/run.f90:26-64) on the device; the
+ * step is captured once in a CUDA graph and replayed. */
+int nv_step(nv_handle *h, int32_t nsteps);
+
+/* One calc_velocity pass for every slot of system sys at the current positions
+ * (ghostp, construct_tree when velocity is Tree, then src/timestep.f90:49-141).
+ * u3 receives [3*pcount] velocities (0 for empty slots).  Nothing is moved. */
+int nv_calc_velocity(nv_handle *h, int32_t sys, double *u3);
+
+/* Cumulative device time (ms) per stage since creation: ms[0] ghosts, [1] tree build,
+ * [2] velocity, [3] AB3 update, [4] topology, [5] whole steps.  n = entries wanted. */
+int nv_stage_times(nv_handle *h, double *ms, int32_t n);
+/* Block until the handle's stream is idle and report any device-side error. */
+int nv_sync(nv_handle *h);
+
+const char *nv_last_error(void);
+const char *nv_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NUVORT_GPU_H */

@@ -1,0 +1,268 @@
+"""ctypes mirror of include/nuvort_gpu.h (records and constants).
+
+The parameter record carries the reference's run.in keys (src/cdata.f90:131-241); the
+state record carries the fields of ``type(qvort)`` (src/cdata.f90:19-29) that the hot path
+touches.  Both the GPU library binding (:mod:`nuvort_b200.api`) and the test-only CPU
+oracle binding use these records, so both sides receive byte-identical inputs.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+# status codes
+NV_OK = 0
+NV_ERR_ARG = -1
+NV_ERR_CUDA = -2
+NV_ERR_CAPACITY = -3
+NV_ERR_SINGULAR = -4
+NV_ERR_TREE_DEPTH = -5
+NV_ERR_NAN = -6
+NV_ERR_EMPTY = -7
+NV_ERR_TIMESTEP = -8
+NV_ERR_UNSUPPORTED = -9
+NV_ERR_STATE = -10
+NV_ERR_QUEUE = -11
+NV_ERR_IO = -12
+
+ERR_NAMES = {v: k for k, v in globals().items() if k.startswith("NV_ERR_") or k == "NV_OK"}
+
+NV_VEL_LIA, NV_VEL_BS, NV_VEL_TREE = 0, 1, 2
+NV_BC_PERIODIC, NV_BC_OPEN, NV_BC_SOLID = 0, 1, 2
+NV_NF_ZERO, NV_NF_XFLOW, NV_NF_UNIFORM = 0, 1, 2
+NV_PREC_FP64, NV_PREC_MIXED = 0, 1
+NV_EV_INSERT, NV_EV_RECON, NV_EV_REMOVE, NV_EV_LOOPKILL = 1, 2, 3, 4
+NV_TREE_MAX_DEPTH = 42
+
+VELOCITY = {"LIA": NV_VEL_LIA, "BS": NV_VEL_BS, "Tree": NV_VEL_TREE}
+BOUNDARY = {"periodic": NV_BC_PERIODIC, "open": NV_BC_OPEN, "solid": NV_BC_SOLID}
+NORMAL = {"zero": NV_NF_ZERO, "xflow": NV_NF_XFLOW, "uniform": NV_NF_UNIFORM}
+
+
+class NvParams(C.Structure):
+    _fields_ = [
+        ("nsteps", C.c_int32),
+        ("shots", C.c_int32),
+        ("recon_shots", C.c_int32),
+        ("velocity", C.c_int32),
+        ("boundary", C.c_int32 * 3),
+        ("normal_velocity", C.c_int32),
+        ("tree_extra_correction", C.c_int32),
+        ("nan_test", C.c_int32),
+        ("overide_timestep_check", C.c_int32),
+        ("precision", C.c_int32),
+        ("dt", C.c_double),
+        ("delta", C.c_double),
+        ("quant_circ", C.c_double),
+        ("corea", C.c_double),
+        ("box_size", C.c_double * 3),
+        ("tree_theta", C.c_double),
+        ("norm_vel_xflow", C.c_double),
+        ("norm_vel_vec", C.c_double * 3),
+        ("alpha", C.c_double * 2),
+        ("super_velocity", C.c_double * 3),
+        ("normal_fluid_cutoff", C.c_double),
+        ("t_zero_normal_fluid", C.c_double),
+    ]
+
+
+class NvHostState(C.Structure):
+    _fields_ = [
+        ("pcount", C.c_int32),
+        ("x", C.POINTER(C.c_double)),
+        ("u", C.POINTER(C.c_double)),
+        ("u1", C.POINTER(C.c_double)),
+        ("u2", C.POINTER(C.c_double)),
+        ("ghosti", C.POINTER(C.c_double)),
+        ("ghostb", C.POINTER(C.c_double)),
+        ("infront", C.POINTER(C.c_int32)),
+        ("behind", C.POINTER(C.c_int32)),
+        ("closest", C.POINTER(C.c_int32)),
+        ("closestd", C.POINTER(C.c_double)),
+    ]
+
+
+class NvEvent(C.Structure):
+    _fields_ = [("itime", C.c_int32), ("kind", C.c_int32), ("i", C.c_int32), ("j", C.c_int32)]
+
+
+class NvCounters(C.Structure):
+    _fields_ = [
+        ("pcount", C.c_int32),
+        ("live", C.c_int32),
+        ("recon_count", C.c_int32),
+        ("remove_count", C.c_int32),
+        ("insert_count", C.c_int32),
+        ("loop_kills", C.c_int32),
+        ("tree_eval", C.c_int64),
+        ("itime", C.c_int32),
+        ("n_events", C.c_int32),
+        ("t", C.c_double),
+    ]
+
+
+class NvTreeNode(C.Structure):
+    """One octree node in preorder (the oracle's or_tree_node / the library's nv_tree_node)."""
+    _fields_ = [
+        ("pos", C.c_double * 3),
+        ("width", C.c_double),
+        ("cent", C.c_double * 3),
+        ("circ", C.c_double * 3),
+        ("pcount", C.c_int32),
+        ("depth", C.c_int32),
+        ("leaf", C.c_int32),
+        ("first_next", C.c_int32),
+    ]
+
+
+def default_params() -> NvParams:
+    """Reference defaults, src/cdata.f90:76-127 (same values as nv_params_default)."""
+    p = NvParams()
+    p.nsteps = 0
+    p.shots = 1
+    p.recon_shots = 1
+    p.velocity = NV_VEL_BS
+    for k in range(3):
+        p.boundary[k] = NV_BC_PERIODIC
+    p.normal_velocity = NV_NF_ZERO
+    p.tree_extra_correction = 1
+    p.nan_test = 1
+    p.overide_timestep_check = 0
+    p.precision = NV_PREC_FP64
+    p.dt = 0.0
+    p.delta = 0.0
+    p.quant_circ = 9.97e-4
+    p.corea = 8.244023e-9
+    p.tree_theta = 0.0
+    p.norm_vel_xflow = 0.5
+    p.normal_fluid_cutoff = 1e8
+    p.t_zero_normal_fluid = 1e8
+    return p
+
+
+def make_params(**kw) -> NvParams:
+    """Build an NvParams from run.in-style keyword values (strings or numbers)."""
+    p = default_params()
+    for key, val in kw.items():
+        if key == "velocity":
+            p.velocity = VELOCITY[val] if isinstance(val, str) else int(val)
+        elif key in ("boundary_x", "boundary_y", "boundary_z"):
+            p.boundary["xyz".index(key[-1])] = BOUNDARY[val] if isinstance(val, str) else int(val)
+        elif key == "boundary":
+            for k in range(3):
+                p.boundary[k] = BOUNDARY[val] if isinstance(val, str) else int(val)
+        elif key == "normal_velocity":
+            p.normal_velocity = NORMAL[val] if isinstance(val, str) else int(val)
+        elif key == "precision":
+            p.precision = {"fp64": NV_PREC_FP64, "mixed": NV_PREC_MIXED}[val] if isinstance(val, str) else int(val)
+        elif key in ("box_size", "norm_vel_vec", "super_velocity", "alpha"):
+            arr = getattr(p, key)
+            vals = [val] * len(arr) if np.isscalar(val) else list(val)
+            for k, v in enumerate(vals):
+                arr[k] = float(v)
+        elif key in ("tree_extra_correction", "nan_test", "overide_timestep_check"):
+            setattr(p, key, int(bool(val)))
+        elif key in ("nsteps", "shots", "recon_shots"):
+            setattr(p, key, int(val))
+        else:
+            if not hasattr(p, key):
+                raise KeyError(f"unknown parameter {key!r}")
+            setattr(p, key, float(val))
+    return p
+
+
+def _dptr(a: Optional[np.ndarray]):
+    if a is None:
+        return C.POINTER(C.c_double)()
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _iptr(a: Optional[np.ndarray]):
+    if a is None:
+        return C.POINTER(C.c_int32)()
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+@dataclass
+class State:
+    """Host copy of one system's filament state: 1-based slots stored at rows 0..pcount-1.
+
+    ``x``, ``u``, ``u1``, ``u2``, ``ghosti``, ``ghostb`` are (n, 3) float64; ``infront``,
+    ``behind``, ``closest`` are int32 (0 = empty / none); ``closestd`` float64.
+    """
+    x: np.ndarray
+    infront: np.ndarray
+    behind: np.ndarray
+    u: Optional[np.ndarray] = None
+    u1: Optional[np.ndarray] = None
+    u2: Optional[np.ndarray] = None
+    ghosti: Optional[np.ndarray] = None
+    ghostb: Optional[np.ndarray] = None
+    closest: Optional[np.ndarray] = None
+    closestd: Optional[np.ndarray] = None
+    _keep: list = field(default_factory=list, repr=False)
+
+    @property
+    def pcount(self) -> int:
+        return int(self.x.shape[0])
+
+    @staticmethod
+    def empty(cap: int) -> "State":
+        z3 = lambda: np.zeros((cap, 3), np.float64)
+        return State(x=z3(), infront=np.zeros(cap, np.int32), behind=np.zeros(cap, np.int32),
+                     u=z3(), u1=z3(), u2=z3(), ghosti=z3(), ghostb=z3(),
+                     closest=np.zeros(cap, np.int32), closestd=np.zeros(cap, np.float64))
+
+    def copy(self) -> "State":
+        cp = lambda a: None if a is None else np.array(a, copy=True)
+        return State(x=cp(self.x), infront=cp(self.infront), behind=cp(self.behind), u=cp(self.u),
+                     u1=cp(self.u1), u2=cp(self.u2), ghosti=cp(self.ghosti), ghostb=cp(self.ghostb),
+                     closest=cp(self.closest), closestd=cp(self.closestd))
+
+    def trimmed(self, n: int) -> "State":
+        cut = lambda a: None if a is None else np.ascontiguousarray(a[:n])
+        return State(x=cut(self.x), infront=cut(self.infront), behind=cut(self.behind), u=cut(self.u),
+                     u1=cut(self.u1), u2=cut(self.u2), ghosti=cut(self.ghosti), ghostb=cut(self.ghostb),
+                     closest=cut(self.closest), closestd=cut(self.closestd))
+
+    def to_c(self) -> NvHostState:
+        for name in ("x", "u", "u1", "u2", "ghosti", "ghostb", "closestd"):
+            a = getattr(self, name)
+            if a is not None:
+                setattr(self, name, np.ascontiguousarray(a, dtype=np.float64))
+        for name in ("infront", "behind", "closest"):
+            a = getattr(self, name)
+            if a is not None:
+                setattr(self, name, np.ascontiguousarray(a, dtype=np.int32))
+        s = NvHostState()
+        s.pcount = self.pcount
+        s.x = _dptr(self.x)
+        s.u = _dptr(self.u)
+        s.u1 = _dptr(self.u1)
+        s.u2 = _dptr(self.u2)
+        s.ghosti = _dptr(self.ghosti)
+        s.ghostb = _dptr(self.ghostb)
+        s.infront = _iptr(self.infront)
+        s.behind = _iptr(self.behind)
+        s.closest = _iptr(self.closest)
+        s.closestd = _dptr(self.closestd)
+        return s
+
+    @property
+    def live(self) -> np.ndarray:
+        return self.infront > 0
+
+
+TREE_NODE_DTYPE = np.dtype([("pos", "<f8", 3), ("width", "<f8"), ("cent", "<f8", 3), ("circ", "<f8", 3),
+                            ("pcount", "<i4"), ("depth", "<i4"), ("leaf", "<i4"), ("first_next", "<i4")])
+
+
+def tree_nodes_to_numpy(buf, n: int) -> np.ndarray:
+    """Copy n NvTreeNode records into a structured numpy array."""
+    assert TREE_NODE_DTYPE.itemsize == C.sizeof(NvTreeNode)
+    return np.frombuffer(bytes(memoryview(buf))[: n * TREE_NODE_DTYPE.itemsize], dtype=TREE_NODE_DTYPE).copy()

@@ -1,0 +1,187 @@
+"""Python binding of libnuvort_gpu.so (the C ABI in include/nuvort_gpu.h).
+
+The stage methods mirror the reference's module procedures called from its time loop
+(src/run.f90:26-64): ``ghostp``, ``construct_tree``, ``pmotion``, ``pinsert``, ``pclose``,
+``precon``, ``premove``, ``enforce_boundary``, ``empty_tree``; ``step`` runs whole steps.
+Errors the reference reports through ``fatal_error`` + ``stop`` (src/cdata.f90:245-255)
+raise :class:`NuvortError` with the library's status code.
+
+There is no CPU fallback: if the CUDA library is missing this module raises on load.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from .abi import (ERR_NAMES, NV_OK, NvCounters, NvEvent, NvHostState, NvParams, NvTreeNode, State,
+                  tree_nodes_to_numpy)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libnuvort_gpu.so")
+
+_lib = None
+
+STAGES = ("ghostp", "construct_tree", "pmotion", "pinsert", "pclose", "precon", "premove",
+          "enforce_boundary", "empty_tree", "end_step")
+STAGE_TIMES = ("ghost", "tree", "velocity", "ab3", "topology", "step")
+
+
+class NuvortError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Load the CUDA library (built in-tree by nuvort_b200.build); fail loudly if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libnuvort_gpu.so not found at {LIB_PATH}; run `python -m nuvort_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    P, vp, i32 = C.POINTER, C.c_void_p, C.c_int32
+    L.nv_params_default.argtypes = [P(NvParams)]
+    L.nv_read_run_file.argtypes = [C.c_char_p, P(NvParams)]
+    L.nv_check_params.argtypes = [P(NvParams)]
+    L.nv_create.argtypes = [P(NvParams), i32, P(i32), i32, P(vp)]
+    L.nv_destroy.argtypes = [vp]
+    L.nv_upload.argtypes = [vp, i32, P(NvHostState)]
+    L.nv_download.argtypes = [vp, i32, P(NvHostState), i32]
+    L.nv_set_clock.argtypes = [vp, i32, C.c_double, i32]
+    L.nv_counters_get.argtypes = [vp, i32, P(NvCounters)]
+    L.nv_events_get.argtypes = [vp, i32, P(NvEvent), i32, P(i32)]
+    for name in STAGES:
+        getattr(L, "nv_" + name).argtypes = [vp]
+    L.nv_step.argtypes = [vp, i32]
+    L.nv_calc_velocity.argtypes = [vp, i32, P(C.c_double)]
+    L.nv_stage_times.argtypes = [vp, P(C.c_double), i32]
+    L.nv_sync.argtypes = [vp]
+    L.nv_last_error.restype = C.c_char_p
+    L.nv_version.restype = C.c_char_p
+    if hasattr(L, "nv_tree_dump"):
+        L.nv_tree_dump.argtypes = [vp, i32, P(NvTreeNode), i32, P(i32)]
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != NV_OK:
+        raise NuvortError(rc, lib().nv_last_error().decode())
+
+
+def version() -> str:
+    return lib().nv_version().decode()
+
+
+def read_run_file(path: str, params: Optional[NvParams] = None) -> NvParams:
+    p = params if params is not None else NvParams()
+    if params is None:
+        _check(lib().nv_params_default(C.byref(p)))
+    _check(lib().nv_read_run_file(path.encode(), C.byref(p)))
+    return p
+
+
+def check_params(p: NvParams):
+    _check(lib().nv_check_params(C.byref(p)))
+
+
+class Handle:
+    """A device-resident ensemble of filament systems (one system is the common case)."""
+
+    def __init__(self, params, capacity: Sequence[int], device: int = 0,
+                 states: Optional[Sequence[State]] = None):
+        plist = list(params) if isinstance(params, (list, tuple)) else [params]
+        n = len(plist)
+        if len(capacity) != n:
+            raise ValueError("one capacity per system")
+        arr = (NvParams * n)(*plist)
+        caps = (C.c_int32 * n)(*[int(c) for c in capacity])
+        h = C.c_void_p()
+        _check(lib().nv_create(arr, n, caps, int(device), C.byref(h)))
+        self.h = h
+        self.nsys = n
+        self.capacity = [int(c) for c in capacity]
+        self.params = plist
+        if states is not None:
+            for s, st in enumerate(states):
+                self.upload(s, st)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().nv_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- state -------------------------------------------------------------------------
+    def upload(self, sys: int, st: State, t: Optional[float] = None, itime: Optional[int] = None):
+        cst = st.to_c()
+        _check(lib().nv_upload(self.h, int(sys), C.byref(cst)))
+        if t is not None or itime is not None:
+            c = self.counters(sys)
+            self.set_clock(sys, c.t if t is None else t, c.itime if itime is None else itime)
+
+    def download(self, sys: int = 0) -> State:
+        cap = self.capacity[sys]
+        st = State.empty(cap)
+        cst = st.to_c()
+        _check(lib().nv_download(self.h, int(sys), C.byref(cst), cap))
+        return st.trimmed(cst.pcount)
+
+    def set_clock(self, sys: int, t: float, itime: int):
+        _check(lib().nv_set_clock(self.h, int(sys), float(t), int(itime)))
+
+    def counters(self, sys: int = 0) -> NvCounters:
+        c = NvCounters()
+        _check(lib().nv_counters_get(self.h, int(sys), C.byref(c)))
+        return c
+
+    def events(self, sys: int = 0) -> List[tuple]:
+        n = C.c_int32()
+        _check(lib().nv_events_get(self.h, int(sys), None, 1 << 30, C.byref(n)))
+        buf = (NvEvent * max(n.value, 1))()
+        _check(lib().nv_events_get(self.h, int(sys), buf, n.value, C.byref(n)))
+        return [(e.itime, e.kind, e.i, e.j) for e in buf[: n.value]]
+
+    # ---- stages ------------------------------------------------------------------------
+    def stage(self, name: str):
+        if name not in STAGES:
+            raise ValueError(name)
+        _check(getattr(lib(), "nv_" + name)(self.h))
+
+    def step(self, n: int = 1):
+        _check(lib().nv_step(self.h, int(n)))
+
+    def calc_velocity(self, sys: int = 0) -> np.ndarray:
+        u = np.zeros((self.capacity[sys], 3), np.float64)
+        _check(lib().nv_calc_velocity(self.h, int(sys), u.ctypes.data_as(C.POINTER(C.c_double))))
+        return u[: self.counters(sys).pcount].copy()
+
+    def stage_times(self) -> dict:
+        ms = (C.c_double * len(STAGE_TIMES))()
+        _check(lib().nv_stage_times(self.h, ms, len(STAGE_TIMES)))
+        return dict(zip(STAGE_TIMES, list(ms)))
+
+    def sync(self):
+        _check(lib().nv_sync(self.h))
+
+    def tree_dump(self, sys: int = 0) -> np.ndarray:
+        n = C.c_int32()
+        _check(lib().nv_tree_dump(self.h, int(sys), None, 0, C.byref(n)))
+        buf = (NvTreeNode * max(n.value, 1))()
+        _check(lib().nv_tree_dump(self.h, int(sys), buf, n.value, C.byref(n)))
+        return tree_nodes_to_numpy(buf, n.value)

@@ -1,0 +1,639 @@
+// api.cu -- the extern "C" boundary of libnuvort_gpu (include/nuvort_gpu.h).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "handle.cuh"
+
+namespace {
+thread_local std::string g_err;
+}
+
+int set_error(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+int check_cuda(cudaError_t e, const char *what) {
+  return set_error(NV_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+
+const char *kVersion = "nuvort_b200 0.1.0 (sm_100a)";
+
+int err_code_from_bits(unsigned bits, std::string &msg) {
+  if (bits & DERR_SINGULAR) { msg = "tree_walk: singularity in BS (tree) velocity field (dist<epsilon)"; return NV_ERR_SINGULAR; }
+  if (bits & DERR_TREE_DEPTH) { msg = "octree deeper than NV_TREE_MAX_DEPTH levels (coincident points?)"; return NV_ERR_TREE_DEPTH; }
+  if (bits & DERR_TREE_NODES) { msg = "octree node buffer exhausted"; return NV_ERR_TREE_DEPTH; }
+  if (bits & DERR_NAN) { msg = "there is a NAN in the (filament) f%x array"; return NV_ERR_NAN; }
+  if (bits & DERR_EMPTY) { msg = "pinsert: vortex line length is 0, run over"; return NV_ERR_EMPTY; }
+  if (bits & DERR_CAPACITY) { msg = "pinsert: system capacity exhausted"; return NV_ERR_CAPACITY; }
+  if (bits & DERR_QUEUE) { msg = "topology resolver work queue overflow"; return NV_ERR_QUEUE; }
+  if (bits & DERR_TIMEOUT) { msg = "device wait gave up (bounded spin exceeded)"; return NV_ERR_CUDA; }
+  msg = "unknown device error";
+  return NV_ERR_CUDA;
+}
+
+// Synchronise the handle's stream and turn the device error word into a status.
+int finish(nv_handle *h) {
+  NV_CUDA(cudaStreamSynchronize(h->stream));
+  NV_CUDA(cudaGetLastError());
+  unsigned bits = 0;
+  NV_CUDA(cudaMemcpy(&bits, h->d_err, sizeof bits, cudaMemcpyDeviceToHost));
+  if (bits) {
+    std::string msg;
+    int code = err_code_from_bits(bits, msg);
+    return set_error(code, msg);
+  }
+  return NV_OK;
+}
+
+int set_device(nv_handle *h) {
+  NV_CUDA(cudaSetDevice(h->device));
+  return NV_OK;
+}
+
+SysConst make_sysconst(const nv_params &p, int base, int cap) {
+  SysConst s;
+  std::memset(&s, 0, sizeof s);
+  s.dt = p.dt;
+  s.delta = p.delta;
+  s.quant_circ = p.quant_circ;
+  s.corea = p.corea;
+  for (int c = 0; c < 3; ++c) s.box[c] = p.box_size[c];
+  s.tree_theta = p.tree_theta;
+  s.beta_pref = p.quant_circ / (4.0 * NV_PI);
+  s.log_pref = 1.1 / p.corea;
+  s.two_pi = 2 * NV_PI;
+  s.alpha[0] = p.alpha[0];
+  s.alpha[1] = p.alpha[1];
+  // get_normal_velocity (normal_fluid.f90:92-117): uniform fields, plus super_velocity.
+  double vn[3] = {0, 0, 0};
+  if (p.normal_velocity == NV_NF_XFLOW) vn[0] = p.norm_vel_xflow;
+  if (p.normal_velocity == NV_NF_UNIFORM)
+    for (int c = 0; c < 3; ++c) vn[c] = p.norm_vel_vec[c];
+  for (int c = 0; c < 3; ++c) s.vn[c] = vn[c] + p.super_velocity[c];
+  for (int c = 0; c < 3; ++c) s.super_velocity[c] = p.super_velocity[c];
+  s.normal_fluid_cutoff = p.normal_fluid_cutoff;
+  s.t_zero_normal_fluid = p.t_zero_normal_fluid;
+  s.bsize = std::max(p.box_size[0], std::max(p.box_size[1], p.box_size[2]));
+  // create_periodic_loop_array (boundary.f90:143-175): i,j,k in -1..1, k fastest.
+  int n = 0;
+  for (int i = -1; i <= 1; ++i)
+    for (int j = -1; j <= 1; ++j)
+      for (int k = -1; k <= 1; ++k) {
+        double ii, jj, kk;
+        if (p.boundary[0] == NV_BC_PERIODIC) ii = i * p.box_size[0];
+        else { if (i != 0) continue; ii = 0; }
+        if (p.boundary[1] == NV_BC_PERIODIC) jj = j * p.box_size[1];
+        else { if (j != 0) continue; jj = 0; }
+        if (p.boundary[2] == NV_BC_PERIODIC) kk = k * p.box_size[2];
+        else { if (k != 0) continue; kk = 0; }
+        if (ii == 0 && jj == 0 && kk == 0) continue;
+        s.shift[n][0] = ii;
+        s.shift[n][1] = jj;
+        s.shift[n][2] = kk;
+        ++n;
+      }
+  s.n_shift = n;
+  s.velocity = p.velocity;
+  for (int c = 0; c < 3; ++c) s.periodic[c] = p.boundary[c] == NV_BC_PERIODIC;
+  s.tree_extra_correction = p.tree_extra_correction != 0;
+  s.mf_on = (std::fabs(p.alpha[0]) > NV_EPS) || (std::fabs(p.alpha[1]) > NV_EPS);
+  s.recon_shots = p.recon_shots > 0 ? p.recon_shots : 1;
+  s.nan_test = p.nan_test != 0;
+  s.use_tree = p.tree_theta > 0;
+  s.sched_tree = p.velocity == NV_VEL_TREE;
+  s.base = base;
+  s.cap = cap;
+  return s;
+}
+
+template <class T>
+int dalloc(T **p, size_t n) {
+  NV_CUDA(cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T)));
+  NV_CUDA(cudaMemset(*p, 0, std::max<size_t>(n, 1) * sizeof(T)));
+  return NV_OK;
+}
+
+void build_worklist(nv_handle *h, int which, std::vector<int2> &w) {
+  w.clear();
+  const int tb = h->direct_tb;
+  for (int s = 0; s < h->nsys; ++s) {
+    const SysConst &sc = h->sc[s];
+    int kind = sc.velocity == NV_VEL_LIA ? 0 : (sc.sched_tree ? 2 : 1);
+    if (kind != which) continue;
+    for (int k = 1; k <= h->cap[s]; k += tb) w.push_back(make_int2(s, sc.base + k));
+  }
+}
+
+int upload_worklist(int2 **dptr, int *n, const std::vector<int2> &w) {
+  if (*dptr) cudaFree(*dptr);
+  *dptr = nullptr;
+  *n = (int)w.size();
+  if (w.empty()) return NV_OK;
+  NV_CUDA(cudaMalloc((void **)dptr, w.size() * sizeof(int2)));
+  NV_CUDA(cudaMemcpy(*dptr, w.data(), w.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  return NV_OK;
+}
+
+int rebuild_worklists(nv_handle *h) {
+  std::vector<int2> w;
+  int rc;
+  build_worklist(h, 0, w);
+  if ((rc = upload_worklist(&h->d_work_lia, &h->n_work_lia, w)) != NV_OK) return rc;
+  h->any_lia = !w.empty();
+  build_worklist(h, 1, w);
+  if ((rc = upload_worklist(&h->d_work_direct, &h->n_work_direct, w)) != NV_OK) return rc;
+  h->any_direct = !w.empty();
+  build_worklist(h, 2, w);
+  if ((rc = upload_worklist(&h->d_work_tree, &h->n_work_tree, w)) != NV_OK) return rc;
+  h->any_tree = !w.empty();
+  return NV_OK;
+}
+
+int pull_dyn(nv_handle *h) {
+  NV_CUDA(cudaMemcpyAsync(h->h_dyn.data(), h->d_dyn, h->nsys * sizeof(SysDyn), cudaMemcpyDeviceToHost, h->stream));
+  NV_CUDA(cudaStreamSynchronize(h->stream));
+  return NV_OK;
+}
+
+bool any_use_tree(nv_handle *h) {
+  for (auto &s : h->sc)
+    if (s.use_tree) return true;
+  return false;
+}
+bool any_needs_tree_walk(nv_handle *h) { return h->any_tree; }
+
+void time_begin(nv_handle *h, int st) {
+  if (h->timing) cudaEventRecord(h->ev[2 * st], h->stream);
+}
+void time_end(nv_handle *h, int st) {
+  if (h->timing) cudaEventRecord(h->ev[2 * st + 1], h->stream);
+}
+
+// The body of one time step, src/run.f90:26-64 (diagnostics and output excluded).
+void enqueue_step(nv_handle *h) {
+  launch_begin_step(h);
+  launch_ghost(h);
+  if (any_use_tree(h) || h->any_tree) launch_tree_build(h);
+  launch_velocity(h);
+  launch_ab3(h);
+  launch_pinsert(h);
+  launch_pclose(h, false);  // each system checks mod(itime, recon_shots) on the device
+  launch_precon(h);
+  launch_premove(h);
+  launch_wrap(h, 3);
+  launch_end_step(h);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *nv_last_error(void) { return g_err.c_str(); }
+const char *nv_version(void) { return kVersion; }
+
+int nv_params_default(nv_params *p) {
+  if (!p) return set_error(NV_ERR_ARG, "null params");
+  std::memset(p, 0, sizeof *p);
+  p->shots = 1;
+  p->recon_shots = 1;
+  p->velocity = NV_VEL_BS;
+  p->boundary[0] = p->boundary[1] = p->boundary[2] = NV_BC_PERIODIC;
+  p->normal_velocity = NV_NF_ZERO;
+  p->tree_extra_correction = 1;
+  p->nan_test = 1;
+  p->overide_timestep_check = 0;
+  p->precision = NV_PREC_FP64;
+  p->quant_circ = 9.97E-4;
+  p->corea = 8.244023E-9;
+  p->tree_theta = 0.0;
+  p->norm_vel_xflow = 0.5;
+  p->normal_fluid_cutoff = 1E8;
+  p->t_zero_normal_fluid = 1E8;
+  return NV_OK;
+}
+
+// init_setup checks (initial.f90:21-25,37-81,131-141) and timestep_check (:169-180).
+int nv_check_params(const nv_params *p) {
+  if (!p) return set_error(NV_ERR_ARG, "null params");
+  if (p->delta < NV_EPS) return set_error(NV_ERR_ARG, "delta must be set in run.in");
+  if (!(std::min(p->box_size[0], std::min(p->box_size[1], p->box_size[2])) > 0.))
+    return set_error(NV_ERR_ARG, "box size is less than or equal zero");
+  for (int c = 0; c < 3; ++c) {
+    if (p->boundary[c] == NV_BC_SOLID)
+      return set_error(NV_ERR_UNSUPPORTED, "solid boundaries (mirror images, pinning) are not supported");
+    if (p->boundary[c] != NV_BC_PERIODIC && p->boundary[c] != NV_BC_OPEN)
+      return set_error(NV_ERR_ARG, "incorrect boundary parameter");
+  }
+  if (p->velocity != NV_VEL_LIA && p->velocity != NV_VEL_BS && p->velocity != NV_VEL_TREE)
+    return set_error(NV_ERR_ARG, "correct value for \"velocity\" in run.in has not been set");
+  if (p->normal_velocity != NV_NF_ZERO && p->normal_velocity != NV_NF_XFLOW && p->normal_velocity != NV_NF_UNIFORM)
+    return set_error(NV_ERR_UNSUPPORTED, "only zero, xflow and uniform normal fluid fields are supported");
+  if (p->tree_theta > 0)
+    for (int c = 0; c < 3; ++c)
+      if (p->boundary[c] == NV_BC_OPEN)
+        return set_error(NV_ERR_ARG, "tree approximation cannot run with open boundaries in its current form");
+  if (p->precision != NV_PREC_FP64 && p->precision != NV_PREC_MIXED)
+    return set_error(NV_ERR_ARG, "unknown precision");
+  if (!p->overide_timestep_check) {
+    const double delta_min = p->delta / 2.;
+    const double dt_max = std::fabs(((delta_min) * (delta_min)) / (p->quant_circ * std::log(delta_min / (NV_PI * p->corea))));
+    if (!(p->dt < dt_max)) return set_error(NV_ERR_TIMESTEP, "dt is too large (timestep_check)");
+  }
+  return NV_OK;
+}
+
+int nv_create(const nv_params *params, int32_t nsys, const int32_t *capacity, int32_t device, nv_handle **out) {
+  if (!params || !capacity || !out || nsys < 1) return set_error(NV_ERR_ARG, "nv_create: bad arguments");
+  *out = nullptr;
+  for (int s = 0; s < nsys; ++s) {
+    int rc = nv_check_params(&params[s]);
+    if (rc != NV_OK) return rc;
+    if (capacity[s] < 1) return set_error(NV_ERR_ARG, "nv_create: capacity must be >= 1");
+    if (params[s].precision != params[0].precision)
+      return set_error(NV_ERR_ARG, "nv_create: all systems of a handle share one precision");
+  }
+  auto *h = new nv_handle();
+  h->device = device;
+  h->nsys = nsys;
+  h->precision = params[0].precision;
+  h->params.assign(params, params + nsys);
+  h->cap.assign(capacity, capacity + nsys);
+  long long off = 0;
+  for (int s = 0; s < nsys; ++s) {
+    h->base.push_back((int)off);
+    off += (long long)capacity[s] + 1;
+    h->max_cap = std::max(h->max_cap, (int)capacity[s]);
+  }
+  if (off >= (1LL << 31) - 1) {
+    delete h;
+    return set_error(NV_ERR_ARG, "nv_create: total capacity exceeds 2^31 slots");
+  }
+  h->T = off;
+  for (int s = 0; s < nsys; ++s) h->sc.push_back(make_sysconst(params[s], h->base[s], capacity[s]));
+  int rc = NV_OK;
+  auto bail = [&](int code) {
+    nv_destroy(h);
+    return code;
+  };
+  if ((rc = set_device(h)) != NV_OK) return bail(rc);
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(set_error(NV_ERR_CUDA, "stream creation failed"));
+  const long long T = h->T;
+  if ((rc = dalloc(&h->d_sc, nsys)) || (rc = dalloc(&h->d_dyn, nsys)) || (rc = dalloc(&h->x, 3 * T)) ||
+      (rc = dalloc(&h->u, 3 * T)) || (rc = dalloc(&h->u1, 3 * T)) || (rc = dalloc(&h->u2, 3 * T)) ||
+      (rc = dalloc(&h->gi, 3 * T)) || (rc = dalloc(&h->gb, 3 * T)) || (rc = dalloc(&h->closestd, T)) ||
+      (rc = dalloc(&h->nxt, T)) || (rc = dalloc(&h->prv, T)) || (rc = dalloc(&h->closest, T)) ||
+      (rc = dalloc(&h->sys_of, T)) || (rc = dalloc(&h->seg, 2 * T)) || (rc = dalloc(&h->d_err, 1)) ||
+      (rc = dalloc(&h->d_event_count, 1)))
+    return bail(rc);
+  if (h->precision == NV_PREC_MIXED && (rc = dalloc(&h->seg32, 2 * T))) return bail(rc);
+  h->event_cap = (int)std::min<long long>(std::max<long long>(1 << 16, T / 4), 1 << 22);
+  if ((rc = dalloc(&h->d_events, h->event_cap))) return bail(rc);
+  if (cudaMemcpy(h->d_sc, h->sc.data(), nsys * sizeof(SysConst), cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(set_error(NV_ERR_CUDA, "upload of system constants failed"));
+  std::vector<int> sys_of(T);
+  for (int s = 0; s < nsys; ++s)
+    for (int k = 0; k <= capacity[s]; ++k) sys_of[h->base[s] + k] = s;
+  if (cudaMemcpy(h->sys_of, sys_of.data(), T * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(set_error(NV_ERR_CUDA, "upload of slot map failed"));
+  h->h_dyn.assign(nsys, SysDyn{});
+  for (auto &d : h->h_dyn) std::memset(&d, 0, sizeof d);
+  if (cudaMemcpy(h->d_dyn, h->h_dyn.data(), nsys * sizeof(SysDyn), cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(set_error(NV_ERR_CUDA, "upload of system state failed"));
+  if ((rc = rebuild_worklists(h))) return bail(rc);
+  for (auto &e : h->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return bail(set_error(NV_ERR_CUDA, "event creation failed"));
+  tree_alloc(h);
+  topo_alloc(h);
+  if (cudaGetLastError() != cudaSuccess) return bail(set_error(NV_ERR_CUDA, "allocation failed"));
+  *out = h;
+  return NV_OK;
+}
+
+int nv_destroy(nv_handle *h) {
+  if (!h) return NV_OK;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  tree_free(h);
+  topo_free(h);
+  void *ptrs[] = {h->d_sc, h->d_dyn, h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv,
+                  h->closest, h->sys_of, h->seg, h->seg32, h->d_err, h->d_events, h->d_event_count,
+                  h->d_work_direct, h->d_work_tree, h->d_work_lia};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  for (auto &e : h->ev)
+    if (e) cudaEventDestroy(e);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return NV_OK;
+}
+
+int nv_upload(nv_handle *h, int32_t sys, const nv_host_state *st) {
+  if (!h || !st || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_upload: bad arguments");
+  if (!st->x || !st->infront || !st->behind) return set_error(NV_ERR_ARG, "nv_upload: x, infront, behind are required");
+  const int n = st->pcount, cap = h->cap[sys], base = h->base[sys];
+  if (n < 0 || n > cap) return set_error(NV_ERR_ARG, "nv_upload: pcount exceeds the system's capacity");
+  int rc = set_device(h);
+  if (rc) return rc;
+  const long long T = h->T;
+  const int rows = cap + 1;  // the system's dummy slot and all its slots
+  std::vector<double> buf(3 * (size_t)rows);
+  auto put3 = [&](double *dev, const double *src) -> int {
+    std::fill(buf.begin(), buf.end(), 0.0);
+    if (src)
+      for (int k = 1; k <= n; ++k)
+        for (int c = 0; c < 3; ++c) buf[(size_t)c * rows + k] = src[3 * (k - 1) + c];
+    for (int c = 0; c < 3; ++c)
+      NV_CUDA(cudaMemcpy(dev + c * T + base, buf.data() + (size_t)c * rows, rows * sizeof(double), cudaMemcpyHostToDevice));
+    return NV_OK;
+  };
+  std::vector<int> ib(rows);
+  auto put_link = [&](int *dev, const int *src) -> int {
+    std::fill(ib.begin(), ib.end(), 0);
+    if (src)
+      for (int k = 1; k <= n; ++k) {
+        const int v = src[k - 1];
+        if (v < 0 || v > n) return set_error(NV_ERR_ARG, "nv_upload: link out of range");
+        ib[k] = v ? base + v : 0;
+      }
+    NV_CUDA(cudaMemcpy(dev + base, ib.data(), rows * sizeof(int), cudaMemcpyHostToDevice));
+    return NV_OK;
+  };
+  if ((rc = put3(h->x, st->x)) || (rc = put3(h->u, st->u)) || (rc = put3(h->u1, st->u1)) ||
+      (rc = put3(h->u2, st->u2)) || (rc = put3(h->gi, st->ghosti)) || (rc = put3(h->gb, st->ghostb)) ||
+      (rc = put_link(h->nxt, st->infront)) || (rc = put_link(h->prv, st->behind)) ||
+      (rc = put_link(h->closest, st->closest)))
+    return rc;
+  std::vector<double> cd(rows, 0.0);
+  if (st->closestd)
+    for (int k = 1; k <= n; ++k) cd[k] = st->closestd[k - 1];
+  NV_CUDA(cudaMemcpy(h->closestd + base, cd.data(), rows * sizeof(double), cudaMemcpyHostToDevice));
+  // a slot that is empty must carry an empty link pair
+  for (int k = 1; k <= n; ++k)
+    if ((st->infront[k - 1] == 0) != (st->behind[k - 1] == 0))
+      return set_error(NV_ERR_ARG, "nv_upload: infront/behind disagree on an empty slot");
+  NV_CUDA(cudaStreamSynchronize(h->stream));
+  SysDyn &d = h->h_dyn[sys];
+  // keep the clock and counters; replace the slot count
+  rc = pull_dyn(h);
+  if (rc) return rc;
+  d.pcount = n;
+  d.live = 0;
+  for (int k = 0; k < n; ++k) d.live += st->infront[k] > 0;
+  NV_CUDA(cudaMemcpy(h->d_dyn + sys, &d, sizeof(SysDyn), cudaMemcpyHostToDevice));
+  unsigned zero = 0;
+  NV_CUDA(cudaMemcpy(h->d_err, &zero, sizeof zero, cudaMemcpyHostToDevice));
+  return NV_OK;
+}
+
+int nv_download(nv_handle *h, int32_t sys, nv_host_state *st, int32_t cap) {
+  if (!h || !st || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_download: bad arguments");
+  int rc = set_device(h);
+  if (rc) return rc;
+  if ((rc = pull_dyn(h))) return rc;
+  const int n = h->h_dyn[sys].pcount, base = h->base[sys];
+  st->pcount = n;
+  if (n > cap) return set_error(NV_ERR_ARG, "nv_download: arrays hold fewer slots than pcount");
+  const long long T = h->T;
+  std::vector<double> buf(3 * (size_t)(n + 1));
+  auto get3 = [&](const double *dev, double *dst) -> int {
+    if (!dst) return NV_OK;
+    for (int c = 0; c < 3; ++c)
+      NV_CUDA(cudaMemcpy(buf.data() + (size_t)c * (n + 1), dev + c * T + base, (n + 1) * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int k = 1; k <= n; ++k)
+      for (int c = 0; c < 3; ++c) dst[3 * (k - 1) + c] = buf[(size_t)c * (n + 1) + k];
+    return NV_OK;
+  };
+  std::vector<int> ib(n + 1);
+  auto get_link = [&](const int *dev, int *dst) -> int {
+    if (!dst) return NV_OK;
+    NV_CUDA(cudaMemcpy(ib.data(), dev + base, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int k = 1; k <= n; ++k) dst[k - 1] = ib[k] ? ib[k] - base : 0;
+    return NV_OK;
+  };
+  if ((rc = get3(h->x, st->x)) || (rc = get3(h->u, st->u)) || (rc = get3(h->u1, st->u1)) ||
+      (rc = get3(h->u2, st->u2)) || (rc = get3(h->gi, st->ghosti)) || (rc = get3(h->gb, st->ghostb)) ||
+      (rc = get_link(h->nxt, st->infront)) || (rc = get_link(h->prv, st->behind)) ||
+      (rc = get_link(h->closest, st->closest)))
+    return rc;
+  if (st->closestd) {
+    std::vector<double> cd(n + 1);
+    NV_CUDA(cudaMemcpy(cd.data(), h->closestd + base, (n + 1) * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int k = 1; k <= n; ++k) st->closestd[k - 1] = cd[k];
+  }
+  return NV_OK;
+}
+
+int nv_set_clock(nv_handle *h, int32_t sys, double t, int32_t itime) {
+  if (!h || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_set_clock: bad arguments");
+  int rc = set_device(h);
+  if (rc || (rc = pull_dyn(h))) return rc;
+  h->h_dyn[sys].t = t;
+  h->h_dyn[sys].itime = itime;
+  NV_CUDA(cudaMemcpy(h->d_dyn + sys, &h->h_dyn[sys], sizeof(SysDyn), cudaMemcpyHostToDevice));
+  return NV_OK;
+}
+
+int nv_counters_get(nv_handle *h, int32_t sys, nv_counters *c) {
+  if (!h || !c || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_counters_get: bad arguments");
+  int rc = set_device(h);
+  if (rc || (rc = pull_dyn(h))) return rc;
+  const SysDyn &d = h->h_dyn[sys];
+  c->pcount = d.pcount;
+  std::vector<int> nx(d.pcount + 1);
+  NV_CUDA(cudaMemcpy(nx.data(), h->nxt + h->base[sys], (d.pcount + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  int live = 0;
+  for (int k = 1; k <= d.pcount; ++k) live += nx[k] != 0;
+  c->live = live;
+  c->recon_count = d.recon_count;
+  c->remove_count = d.remove_count;
+  c->insert_count = d.insert_count;
+  c->loop_kills = d.loop_kills;
+  c->tree_eval = (int64_t)d.tree_eval;
+  c->itime = d.itime;
+  c->n_events = d.event_seq;
+  c->t = d.t;
+  return NV_OK;
+}
+
+int nv_events_get(nv_handle *h, int32_t sys, nv_event *buf, int32_t cap, int32_t *n) {
+  if (!h || !n || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_events_get: bad arguments");
+  int rc = set_device(h);
+  if (rc) return rc;
+  int total = 0;
+  NV_CUDA(cudaMemcpy(&total, h->d_event_count, sizeof(int), cudaMemcpyDeviceToHost));
+  total = std::min(total, h->event_cap);
+  std::vector<DevEvent> ev(total);
+  if (total) NV_CUDA(cudaMemcpy(ev.data(), h->d_events, total * sizeof(DevEvent), cudaMemcpyDeviceToHost));
+  std::vector<DevEvent> mine;
+  for (auto &e : ev)
+    if (e.sys == sys) mine.push_back(e);
+  std::sort(mine.begin(), mine.end(), [](const DevEvent &a, const DevEvent &b) { return a.seq < b.seq; });
+  const int base = h->base[sys];
+  int m = 0;
+  for (auto &e : mine) {
+    if (m >= cap) break;
+    if (buf) {
+      buf[m].itime = e.itime;
+      buf[m].kind = e.kind;
+      buf[m].i = e.i ? e.i - base : 0;
+      buf[m].j = (e.kind == NV_EV_LOOPKILL) ? e.j : (e.j ? e.j - base : 0);
+    }
+    ++m;
+  }
+  *n = m;
+  return NV_OK;
+}
+
+// ---- stages ---------------------------------------------------------------------------
+int nv_ghostp(nv_handle *h) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  int rc = set_device(h);
+  if (rc) return rc;
+  launch_ghost(h);
+  return finish(h);
+}
+int nv_construct_tree(nv_handle *h) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  int rc = set_device(h);
+  if (rc) return rc;
+  launch_tree_build(h);
+  return finish(h);
+}
+int nv_pmotion(nv_handle *h) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  int rc = set_device(h);
+  if (rc) return rc;
+  launch_velocity(h);
+  launch_ab3(h);
+  return finish(h);
+}
+int nv_pinsert(nv_handle *h) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  int rc = set_device(h);
+  if (rc) return rc;
+  launch_pinsert(h);
+  return finish(h);
+}
+int nv_pclose(nv_handle *h) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  int rc = set_device(h);
+  if (rc) return rc;
+  launch_pclose(h, false);
+  return finish(h);
+}
+int nv_precon(nv_handle *h) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  int rc = set_device(h);
+  if (rc) return rc;
+  launch_precon(h);
+  return finish(h);
+}
+int nv_premove(nv_handle *h) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  int rc = set_device(h);
+  if (rc) return rc;
+  launch_premove(h);
+  return finish(h);
+}
+int nv_enforce_boundary(nv_handle *h) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  int rc = set_device(h);
+  if (rc) return rc;
+  launch_wrap(h, 1);
+  return finish(h);
+}
+int nv_empty_tree(nv_handle *h) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  return NV_OK;  // the device tree is rebuilt in place by the next construct_tree
+}
+int nv_end_step(nv_handle *h) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  int rc = set_device(h);
+  if (rc) return rc;
+  launch_wrap(h, 2);
+  launch_end_step(h);
+  return finish(h);
+}
+
+int nv_step(nv_handle *h, int32_t nsteps) {
+  if (!h || nsteps < 0) return set_error(NV_ERR_ARG, "nv_step: bad arguments");
+  int rc = set_device(h);
+  if (rc) return rc;
+  if (!h->graph_valid) {
+    cudaGraph_t graph = nullptr;
+    NV_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(h);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    if (e != cudaSuccess) return check_cuda(e, "cudaStreamEndCapture");
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    e = cudaGraphInstantiate(&h->graph_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return check_cuda(e, "cudaGraphInstantiate");
+    h->graph_valid = true;
+  }
+  cudaEventRecord(h->ev[2 * ST_STEP], h->stream);
+  for (int k = 0; k < nsteps; ++k) NV_CUDA(cudaGraphLaunch(h->graph_exec, h->stream));
+  cudaEventRecord(h->ev[2 * ST_STEP + 1], h->stream);
+  rc = finish(h);
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, h->ev[2 * ST_STEP], h->ev[2 * ST_STEP + 1]) == cudaSuccess) h->stage_ms[ST_STEP] += ms;
+  return rc;
+}
+
+int nv_calc_velocity(nv_handle *h, int32_t sys, double *u3) {
+  if (!h || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_calc_velocity: bad arguments");
+  int rc = set_device(h);
+  if (rc) return rc;
+  time_begin(h, ST_GHOST);
+  launch_ghost(h);
+  time_end(h, ST_GHOST);
+  time_begin(h, ST_TREE);
+  if (h->any_tree) launch_tree_build(h);
+  time_end(h, ST_TREE);
+  time_begin(h, ST_VELOCITY);
+  launch_velocity(h);
+  time_end(h, ST_VELOCITY);
+  if ((rc = finish(h))) return rc;
+  if (h->timing) {
+    const int st[] = {ST_GHOST, ST_TREE, ST_VELOCITY};
+    for (int s : st) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, h->ev[2 * s], h->ev[2 * s + 1]) == cudaSuccess) h->stage_ms[s] += ms;
+    }
+  }
+  if (!u3) return NV_OK;
+  nv_host_state hs;
+  std::memset(&hs, 0, sizeof hs);
+  std::vector<int> inf(h->cap[sys]), beh(h->cap[sys]);
+  hs.u = u3;
+  hs.infront = inf.data();
+  hs.behind = beh.data();
+  if ((rc = nv_download(h, sys, &hs, h->cap[sys]))) return rc;
+  for (int k = 0; k < hs.pcount; ++k)
+    if (inf[k] == 0) u3[3 * k] = u3[3 * k + 1] = u3[3 * k + 2] = 0.0;
+  return NV_OK;
+}
+
+int nv_stage_times(nv_handle *h, double *ms, int32_t n) {
+  if (!h || !ms) return set_error(NV_ERR_ARG, "nv_stage_times: bad arguments");
+  for (int k = 0; k < n && k < ST_COUNT; ++k) ms[k] = h->stage_ms[k];
+  return NV_OK;
+}
+
+int nv_sync(nv_handle *h) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  int rc = set_device(h);
+  if (rc) return rc;
+  return finish(h);
+}
+
+}  // extern "C"

@@ -1,0 +1,200 @@
+// common.cuh -- shared device-side definitions of libnuvort_gpu.
+//
+// Device layout (one handle, nsys systems):
+//   * Global slot index g.  System s owns slots [base_s, base_s + cap_s]; slot base_s is
+//     an unused dummy (the reference's slot 0), slot base_s + k is the reference's f(k).
+//     System 0's dummy is global slot 0, so a link value 0 means "empty" in every system.
+//   * Links (infront/behind/closest) hold GLOBAL slot indices; the host converts to and
+//     from the reference's 1-based system-local numbering at upload/download.  The map is
+//     monotone inside a system, so "lowest j" tie-breaks are unchanged.
+//   * FP64 per-slot arrays are SoA: component c of slot g is a[c * T + g].
+//   * seg: the Biot-Savart segment of each slot, packed for staged tile loads.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/nuvort_gpu.h"
+
+#define NV_PI 3.14159265358979324
+#define NV_EPS 2.220446049250313e-16  // epsilon(0.) for real(8)
+
+// Device error word bits (OR-ed by kernels, read by the host after launches).
+enum : unsigned {
+  DERR_SINGULAR = 1u << 0,
+  DERR_TREE_DEPTH = 1u << 1,
+  DERR_NAN = 1u << 2,
+  DERR_EMPTY = 1u << 3,
+  DERR_CAPACITY = 1u << 4,
+  DERR_QUEUE = 1u << 5,
+  DERR_TIMEOUT = 1u << 6,
+  DERR_TREE_NODES = 1u << 7,
+};
+
+struct SysConst {
+  double dt, delta, quant_circ, corea;
+  double box[3];
+  double tree_theta;
+  double beta_pref;   // quant_circ/(4.*pi)       timestep.f90:79
+  double log_pref;    // 1.1/corea                timestep.f90:79
+  double two_pi;      // 2*pi                     timestep.f90:168
+  double alpha[2];
+  double vn[3];       // get_normal_velocity(x) for the uniform cases, +super_velocity
+  double super_velocity[3];
+  double normal_fluid_cutoff, t_zero_normal_fluid;
+  double bsize;       // maxval(box_size)         tree.f90:45
+  double shift[26][3];
+  int velocity;
+  int periodic[3];
+  int tree_extra_correction;
+  int mf_on;          // (|alpha(1)|>eps .or. |alpha(2)|>eps)   timestep.f90:126
+  int n_shift;
+  int recon_shots;
+  int nan_test;
+  int use_tree;       // tree_theta>0 (run.f90:29,37)
+  int base, cap;
+  int sched_tree;     // non-local sum by the tree walk (velocity==Tree)
+};
+
+struct SysDyn {
+  int pcount;
+  int itime;
+  double t;
+  int recon_count, remove_count, insert_count, loop_kills;
+  unsigned long long tree_eval;
+  int event_seq;
+  int live;
+  int old_pcount;
+  int pad;
+};
+
+// One logged topology event (system-local numbering is restored on the host).
+struct DevEvent {
+  int sys, seq, itime, kind, i, j;
+};
+
+// ---- exact IEEE FP64 operations (no FMA contraction), matching one rounding per op ----
+__device__ __forceinline__ double e_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double e_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double e_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double e_div(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double e_sqrt(double a) { return __dsqrt_rn(a); }
+__device__ __forceinline__ double e_sq(double a) { return __dmul_rn(a, a); }
+
+// dist_gen (derivatives.f90:40-47)
+__device__ __forceinline__ double dist_gen(const double a[3], const double b[3]) {
+  return e_sqrt(e_add(e_add(e_sq(e_sub(a[0], b[0])), e_sq(e_sub(a[1], b[1]))), e_sq(e_sub(a[2], b[2]))));
+}
+__device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
+  return e_add(e_add(e_mul(a[0], b[0]), e_mul(a[1], b[1])), e_mul(a[2], b[2]));
+}
+// cross_product (general.f90:152-159)
+__device__ __forceinline__ void cross3(const double a[3], const double b[3], double c[3]) {
+  c[0] = e_sub(e_mul(a[1], b[2]), e_mul(a[2], b[1]));
+  c[1] = e_sub(e_mul(a[2], b[0]), e_mul(a[0], b[2]));
+  c[2] = e_sub(e_mul(a[0], b[1]), e_mul(a[1], b[0]));
+}
+
+__device__ __forceinline__ void load3(const double *__restrict__ a, long long T, int g, double v[3]) {
+  v[0] = a[g];
+  v[1] = a[T + g];
+  v[2] = a[2 * T + g];
+}
+__device__ __forceinline__ void store3(double *__restrict__ a, long long T, int g, const double v[3]) {
+  a[g] = v[0];
+  a[T + g] = v[1];
+  a[2 * T + g] = v[2];
+}
+
+// get_ghost_p (boundary.f90:26-84, non-pinned branch): neighbour positions unwrapped
+// across periodic faces relative to x.
+__device__ __forceinline__ void ghost_adjust(const SysConst &sc, const double x[3], double g[3]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (!sc.periodic[c]) continue;
+    const double L = sc.box[c];
+    const double h = L / 2.0;
+    if (e_sub(x[c], g[c]) > h) g[c] = e_add(g[c], L);
+    else if (e_sub(x[c], g[c]) < -h) g[c] = e_sub(g[c], L);
+  }
+}
+
+// get_deriv_1 / get_deriv_2 (derivatives.f90:11-36)
+__device__ __forceinline__ void deriv1(const double x[3], const double gi[3], const double gb[3],
+                                       double s[3]) {
+  const double disti = dist_gen(x, gi), distb = dist_gen(x, gb);
+  const double den = e_mul(e_mul(2.0, distb), disti);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    double v = e_sub(e_add(e_mul(distb, gi[c]), e_mul(e_sub(disti, distb), x[c])), e_mul(disti, gb[c]));
+    s[c] = e_div(v, den);
+  }
+}
+__device__ __forceinline__ void deriv2(const double x[3], const double gi[3], const double gb[3],
+                                       double s[3]) {
+  const double disti = dist_gen(x, gi), distb = dist_gen(x, gb);
+  const double d1 = e_mul(disti, e_add(disti, distb));
+  const double d2 = e_mul(disti, distb);
+  const double d3 = e_mul(distb, e_add(disti, distb));
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    s[c] = e_mul(2.0, e_add(e_sub(e_div(gi[c], d1), e_div(x[c], d2)), e_div(gb[c], d3)));
+}
+
+// Local part of calc_velocity (timestep.f90:60-80,102-105): u = beta s' x s''.
+__device__ __forceinline__ void local_velocity(const SysConst &sc, const double x[3],
+                                               const double gi[3], const double gb[3], double u[3],
+                                               double fdot[3]) {
+  double fddot[3], cr[3];
+  deriv1(x, gi, gb, fdot);
+  deriv2(x, gi, gb, fddot);
+  double beta;
+  if (sc.velocity == NV_VEL_LIA) {
+    double curv = e_sqrt(dot3(fddot, fddot));
+    if (curv < NV_EPS) curv = NV_EPS;
+    else curv = e_div(1.0, curv);
+    beta = e_mul(sc.beta_pref, log(e_div(e_mul(4.6, curv), sc.corea)));
+  } else {
+    beta = e_mul(sc.beta_pref, log(e_mul(sc.log_pref, e_sqrt(e_mul(dist_gen(x, gi), dist_gen(x, gb))))));
+  }
+  cross3(fdot, fddot, cr);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) u[c] = e_mul(beta, cr[c]);
+}
+
+// Mutual friction and imposed flow (timestep.f90:126-140); u holds u_sup on entry.
+__device__ __forceinline__ void mf_epilogue(const SysConst &sc, double t, const double fdot[3],
+                                            double u[3]) {
+  if (sc.mf_on && t < sc.normal_fluid_cutoff) {
+    double un[3], w[3], c1[3], c2[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) un[c] = (t < sc.t_zero_normal_fluid) ? sc.vn[c] : 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) w[c] = e_sub(un[c], u[c]);
+    cross3(fdot, w, c1);
+    cross3(fdot, c1, c2);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], e_sub(e_mul(sc.alpha[0], c1[c]), e_mul(sc.alpha[1], c2[c])));
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], sc.super_velocity[c]);
+}
+
+// One desingularised segment term (timestep.f90:162-170 / 188-196), reference order:
+//   u_bs = (r x d) * quant_circ / ((2 pi)(4ac - b^2)) * ((2c+b)/sqrt(a+b+c) - b/sqrt(a)).
+// Returns false when the reference skips the term (4ac-b^2 == 0 exactly).
+__device__ __forceinline__ bool bs_term_exact(const double r[3], const double d[3], double a,
+                                              double c, double qc, double two_pi, double out[3]) {
+  const double b = e_mul(2.0, dot3(r, d));
+  const double D = e_sub(e_mul(e_mul(4.0, a), c), e_mul(b, b));
+  if (D == 0.0) return false;
+  double cr[3];
+  cross3(r, d, cr);
+  const double den = e_mul(two_pi, D);
+  const double fac = e_sub(e_div(e_add(e_mul(2.0, c), b), e_sqrt(e_add(e_add(a, b), c))), e_div(b, e_sqrt(a)));
+#pragma unroll
+  for (int k = 0; k < 3; ++k) out[k] = e_mul(e_div(e_mul(cr[k], qc), den), fac);
+  return true;
+}
+
+__device__ __forceinline__ void set_err(unsigned *err, unsigned bit) { atomicOr(err, bit); }

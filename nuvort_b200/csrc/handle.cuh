@@ -1,0 +1,97 @@
+// handle.cuh -- host-side definition of nv_handle and the kernel launchers.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+struct TreeBuffers;  // tree.cu
+struct TopoBuffers;  // topo.cu
+
+enum { ST_GHOST = 0, ST_TREE, ST_VELOCITY, ST_AB3, ST_TOPO, ST_STEP, ST_COUNT };
+
+struct nv_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int nsys = 0;
+  int precision = NV_PREC_FP64;
+  std::vector<nv_params> params;
+  std::vector<SysConst> sc;
+  std::vector<int> cap, base;
+  long long T = 0;  // slots including one dummy per system
+  int max_cap = 0;
+
+  // device state
+  SysConst *d_sc = nullptr;
+  SysDyn *d_dyn = nullptr;
+  double *x = nullptr, *u = nullptr, *u1 = nullptr, *u2 = nullptr;
+  double *gi = nullptr, *gb = nullptr, *closestd = nullptr;
+  int *nxt = nullptr, *prv = nullptr, *closest = nullptr, *sys_of = nullptr;
+  double4 *seg = nullptr;   // FP64 segment records, 2 per slot
+  float4 *seg32 = nullptr;  // FP32 segment records, 2 per slot (mixed precision)
+  unsigned *d_err = nullptr;
+  DevEvent *d_events = nullptr;
+  int *d_event_count = nullptr;
+  int event_cap = 0;
+
+  // work lists: blocks of target slots, (system, first global slot)
+  int2 *d_work_direct = nullptr;
+  int n_work_direct = 0;
+  int2 *d_work_tree = nullptr;
+  int n_work_tree = 0;
+  int2 *d_work_lia = nullptr;
+  int n_work_lia = 0;
+  int direct_tb = 64;  // targets per block of the direct sum
+  bool any_tree = false, any_direct = false, any_lia = false;
+
+  TreeBuffers *tree = nullptr;
+  TopoBuffers *topo = nullptr;
+
+  // CUDA graph of one whole step
+  cudaGraphExec_t graph_exec = nullptr;
+  bool graph_valid = false;
+
+  // stage timing
+  bool timing = true;
+  cudaEvent_t ev[2 * ST_COUNT] = {};
+  double stage_ms[ST_COUNT] = {};
+
+  // host mirrors
+  std::vector<SysDyn> h_dyn;
+};
+
+// launchers (each enqueues on h->stream)
+void launch_begin_step(nv_handle *h);
+void launch_ghost(nv_handle *h);
+void launch_velocity(nv_handle *h);
+void launch_ab3(nv_handle *h);
+void launch_wrap(nv_handle *h, int mode);  // bit 1 wrap, bit 2 NaN check
+void launch_end_step(nv_handle *h);
+
+// direct sum (direct.cu)
+void launch_direct(nv_handle *h);
+// tree (tree.cu)
+void tree_alloc(nv_handle *h);
+void tree_free(nv_handle *h);
+void launch_tree_build(nv_handle *h);
+void launch_tree_walk(nv_handle *h);
+void launch_closest_tree(nv_handle *h);
+int tree_dump(nv_handle *h, int sys, void *buf, int cap, int *n);
+// topology (topo.cu)
+void topo_alloc(nv_handle *h);
+void topo_free(nv_handle *h);
+void launch_pinsert(nv_handle *h);
+void launch_pclose(nv_handle *h, bool only_brute);
+void launch_precon(nv_handle *h);
+void launch_premove(nv_handle *h);
+
+int set_error(int code, const std::string &msg);
+int check_cuda(cudaError_t e, const char *what);
+#define NV_CUDA(call)                                   \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return check_cuda(_e, #call); \
+  } while (0)
+
+inline int grid_for(long long n, int tb) { return (int)((n + tb - 1) / tb); }
