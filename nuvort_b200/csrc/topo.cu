@@ -1,10 +1,524 @@
-// topo.cu -- topology stages (placeholder until the device resolvers land).
+// topo.cu -- topology stages: pinsert, pclose (brute), precon, premove, loop_killer.
+//
+// The reference runs pinsert, precon and premove as serial sweeps in ascending slot order
+// (src/line.f90:30, src/reconnection.f90:180, src/line.f90:107), where an event can change
+// what later slots see.  Here each stage is
+//   1. a parallel pass over all slots that marks the slots whose test can pass on the
+//      current state (or, for pinsert, whose stale-ghost test passes);
+//   2. a stable compaction of the marks into an ascending list per system (prefix sum);
+//   3. one thread per system that walks its list in ascending order, merged with a small
+//      min-heap of slots that an earlier event in the same sweep has touched (their test
+//      must be re-evaluated), and applies the reference's exact tests and updates.
+// A slot that is neither marked nor touched has a test that is false in the serial sweep
+// too, so the events are the reference's, event for event and in the same order.
+#include <cub/cub.cuh>
+
 #include "handle.cuh"
 
-struct TopoBuffers {};
-void topo_alloc(nv_handle *) {}
-void topo_free(nv_handle *) {}
-void launch_pinsert(nv_handle *) {}
-void launch_pclose(nv_handle *, bool) {}
-void launch_precon(nv_handle *) {}
-void launch_premove(nv_handle *) {}
+struct TopoBuffers {
+  int *flag_a = nullptr, *pos_a = nullptr, *list_a = nullptr;
+  int *flag_b = nullptr, *pos_b = nullptr, *list_b = nullptr;
+  void *cub_tmp = nullptr;
+  size_t cub_bytes = 0;
+};
+
+namespace {
+
+constexpr int TB = 256;
+constexpr int kHeap = 512;  // pending re-tests per system resolver
+
+struct Heap {  // min-heap of slot indices in thread-local memory
+  int v[kHeap];
+  int n = 0;
+  __device__ bool push(int x) {
+    if (n >= kHeap) return false;
+    int i = n++;
+    v[i] = x;
+    while (i > 0) {
+      int p = (i - 1) >> 1;
+      if (v[p] <= v[i]) break;
+      int t = v[p]; v[p] = v[i]; v[i] = t;
+      i = p;
+    }
+    return true;
+  }
+  __device__ int top() const { return v[0]; }
+  __device__ void pop() {
+    v[0] = v[--n];
+    int i = 0;
+    for (;;) {
+      int l = 2 * i + 1, r = l + 1, m = i;
+      if (l < n && v[l] < v[m]) m = l;
+      if (r < n && v[r] < v[m]) m = r;
+      if (m == i) break;
+      int t = v[m]; v[m] = v[i]; v[i] = t;
+      i = m;
+    }
+  }
+};
+
+// Next slot of the merged sweep (list[li..le) and the heap), strictly above `last`.
+__device__ __forceinline__ int sweep_next(const int *list, int &li, int le, Heap &hp, int last) {
+  for (;;) {
+    while (li < le && list[li] <= last) ++li;
+    while (hp.n > 0 && hp.top() <= last) hp.pop();
+    const int a = li < le ? list[li] : INT_MAX;
+    const int b = hp.n > 0 ? hp.top() : INT_MAX;
+    return a < b ? a : b;
+  }
+}
+
+__device__ __forceinline__ bool recon_step(const SysConst &sc, const SysDyn &d) {
+  return (d.itime % sc.recon_shots) == 0;
+}
+
+__device__ void log_event(SysDyn &d, int s, int kind, int i, int j, DevEvent *ev, int *ev_count, int ev_cap) {
+  const int seq = d.event_seq++;
+  const int slot = atomicAdd(ev_count, 1);
+  if (slot < ev_cap) ev[slot] = DevEvent{s, seq, d.itime, kind, i, j};
+}
+
+struct State {
+  double *X, *U, *U1, *U2, *GI, *GB, *CD;
+  int *nxt, *prv, *cl;
+  long long T;
+};
+
+__device__ void clear_particle(const State &S, int g) {  // general.f90:10-20
+  const long long T = S.T;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    S.X[c * T + g] = 0; S.U[c * T + g] = 0; S.U1[c * T + g] = 0; S.U2[c * T + g] = 0;
+    S.GI[c * T + g] = 0; S.GB[c * T + g] = 0;
+  }
+  S.nxt[g] = 0; S.prv[g] = 0; S.cl[g] = 0; S.CD[g] = 0;
+}
+
+// loop_killer (reconnection.f90:155-182).  Only "fewer than 4 points" matters, so the
+// count stops after three hops; the result equals the reference's full walk.
+__device__ void loop_killer(const State &S, SysDyn &d, int s, int particle, int pcount, DevEvent *ev,
+                            int *ev_count, int ev_cap) {
+  int counter = 1, nx = particle;
+  const int hops = pcount < 3 ? pcount : 3;
+  for (int it = 0; it < hops; ++it) {
+    nx = S.nxt[nx];
+    if (nx == particle) break;
+    counter++;
+  }
+  if (counter < 4) {
+    log_event(d, s, NV_EV_LOOPKILL, particle, counter, ev, ev_count, ev_cap);
+    d.loop_kills++;
+    nx = particle;
+    for (int it = 0; it < pcount; ++it) {
+      const int sn = S.nxt[nx];
+      clear_particle(S, nx);
+      nx = sn;
+      if (nx == particle) break;
+    }
+  }
+}
+
+__device__ __forceinline__ void get_ghost_p(const SysConst &sc, const State &S, int g, double gi[3], double gb[3]) {
+  double x[3];
+  load3(S.X, S.T, g, x);
+  load3(S.X, S.T, S.nxt[g], gi);
+  load3(S.X, S.T, S.prv[g], gb);
+  ghost_adjust(sc, x, gi);
+  ghost_adjust(sc, x, gb);
+}
+__device__ __forceinline__ void refresh_ghosts(const SysConst &sc, const State &S, int g) {
+  double gi[3], gb[3];
+  get_ghost_p(sc, S, g, gi, gb);
+  store3(S.GI, S.T, g, gi);
+  store3(S.GB, S.T, g, gb);
+}
+
+// ---- pass 1 kernels: marks ----------------------------------------------------------------
+// pinsert marks: A = live slot whose stale-ghost test |x - ghosti| > delta passes;
+//                B = empty slot (the free-slot list minloc() walks, line.f90:44-47).
+__global__ void k_mark_insert(const SysConst *__restrict__ scs, SysDyn *__restrict__ dyn, const int *__restrict__ sys_of,
+                              const double *__restrict__ X, const double *__restrict__ GI, const int *__restrict__ nxt,
+                              int *fa, int *fb, long long T, const unsigned *err) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g > T) return;
+  int a = 0, b = 0;
+  if (g < T && !*err) {
+    const int s = sys_of[g];
+    const SysConst &sc = scs[s];
+    const int k = (int)(g - sc.base);
+    if (k >= 1 && k <= dyn[s].pcount) {
+      if (nxt[g] == 0) {
+        b = 1;
+      } else {
+        double x[3], gi[3];
+        load3(X, T, (int)g, x);
+        load3(GI, T, (int)g, gi);
+        a = dist_gen(x, gi) > sc.delta;
+        dyn[s].live = 1;  // any live point (line.f90:25-27); idempotent store
+      }
+    }
+  }
+  fa[g] = a;
+  fb[g] = b;
+}
+
+// precon marks: live slot with delta/2 > closestd > epsilon(1.) (reconnection.f90:185).
+__global__ void k_mark_recon(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn, const int *__restrict__ sys_of,
+                             const double *__restrict__ CD, const int *__restrict__ nxt, int *fa, long long T,
+                             const unsigned *err) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g > T) return;
+  int a = 0;
+  if (g < T && !*err) {
+    const int s = sys_of[g];
+    const SysConst &sc = scs[s];
+    const int k = (int)(g - sc.base);
+    if (k >= 1 && k <= dyn[s].pcount && recon_step(sc, dyn[s]) && nxt[g] != 0) {
+      const double cd = CD[g];
+      a = (cd < sc.delta / 2.) && (cd > NV_EPS);
+    }
+  }
+  fa[g] = a;
+}
+
+// premove marks: live slot with |x_i - x_{i+2}| < .99 delta (line.f90:113-115).
+__global__ void k_mark_remove(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn, const int *__restrict__ sys_of,
+                              const double *__restrict__ X, const int *__restrict__ nxt, int *fa, long long T,
+                              const unsigned *err) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g > T) return;
+  int a = 0;
+  if (g < T && !*err) {
+    const int s = sys_of[g];
+    const SysConst &sc = scs[s];
+    const int k = (int)(g - sc.base);
+    if (k >= 1 && k <= dyn[s].pcount && recon_step(sc, dyn[s]) && nxt[g] != 0) {
+      double x[3], y[3];
+      load3(X, T, (int)g, x);
+      load3(X, T, nxt[nxt[g]], y);
+      a = dist_gen(x, y) < e_mul(.99, sc.delta);
+    }
+  }
+  fa[g] = a;
+}
+
+__global__ void k_scatter(const int *__restrict__ flag, const int *__restrict__ pos, int *__restrict__ list, long long T) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < T && flag[g]) list[pos[g]] = (int)g;
+}
+
+__global__ void k_zero_live(SysDyn *dyn, int nsys) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < nsys) dyn[s].live = 0;
+}
+
+// ---- pass 3: serial resolvers, one thread per system ---------------------------------------
+
+// pinsert (line.f90:18-96).
+__global__ void k_insert_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S,
+                                 const int *__restrict__ pos_a, const int *__restrict__ list_a,
+                                 const int *__restrict__ pos_b, const int *__restrict__ list_b, unsigned *err,
+                                 DevEvent *ev, int *ev_count, int ev_cap) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys || *err) return;
+  const SysConst &sc = scs[s];
+  SysDyn d = dyn[s];
+  if (d.live == 0) {
+    atomicOr(err, DERR_EMPTY);
+    return;
+  }
+  const int base = sc.base;
+  const int old_last = base + d.pcount;  // loop bound old_pcount (line.f90:28-30)
+  int pc = d.pcount;
+  int li = pos_a[base], le = pos_a[base + sc.cap + 1];
+  int ei = pos_b[base], ee = pos_b[base + sc.cap + 1];
+  Heap hp;
+  int last = base;
+  const long long T = S.T;
+  for (;;) {
+    const int i = sweep_next(list_a, li, le, hp, last);
+    if (i == INT_MAX || i > old_last) break;
+    last = i;
+    if (S.nxt[i] == 0) continue;
+    double x[3], gi[3], gb[3];
+    load3(S.X, T, i, x);
+    load3(S.GI, T, i, gi);
+    load3(S.GB, T, i, gb);
+    const double disti = dist_gen(x, gi);
+    if (!(disti > sc.delta)) continue;
+    int par_new;
+    if (ei < ee) {
+      par_new = list_b[ei++];
+    } else {
+      if (pc + 1 > sc.cap) {
+        atomicOr(err, DERR_CAPACITY);
+        break;
+      }
+      par_new = base + (++pc);
+    }
+    double fdd[3], xn[3];
+    deriv2(x, gi, gb, fdd);
+    double curv = e_sqrt(dot3(fdd, fdd));
+    double mid[3] = {e_mul(0.5, e_add(x[0], gi[0])), e_mul(0.5, e_add(x[1], gi[1])), e_mul(0.5, e_add(x[2], gi[2]))};
+    if (curv > 1E-5) {
+      curv = e_div(1.0, curv);
+      const double disc = e_sub(e_mul(curv, curv), e_mul(0.25, e_mul(disti, disti)));
+      if (disc > 0.) {
+        const double sfac = e_mul(e_sub(e_sqrt(disc), curv), curv);
+        for (int c = 0; c < 3; ++c) xn[c] = e_add(mid[c], e_mul(sfac, fdd[c]));
+      } else {
+        for (int c = 0; c < 3; ++c) xn[c] = mid[c];
+      }
+    } else {
+      for (int c = 0; c < 3; ++c) xn[c] = mid[c];
+    }
+    const int nx = S.nxt[i];
+    double ui[3], un[3], zero[3] = {0, 0, 0};
+    load3(S.U, T, i, ui);
+    load3(S.U, T, nx, un);
+    for (int c = 0; c < 3; ++c) un[c] = e_mul(0.5, e_add(ui[c], un[c]));
+    store3(S.X, T, par_new, xn);
+    store3(S.U, T, par_new, un);
+    store3(S.U1, T, par_new, zero);
+    store3(S.U2, T, par_new, zero);
+    S.prv[par_new] = i;
+    S.nxt[par_new] = nx;
+    refresh_ghosts(sc, S, par_new);
+    S.prv[nx] = par_new;
+    refresh_ghosts(sc, S, nx);
+    S.nxt[i] = par_new;
+    refresh_ghosts(sc, S, i);
+    log_event(d, s, NV_EV_INSERT, i, par_new, ev, ev_count, ev_cap);
+    d.insert_count++;
+    // slots whose test changed and that the sweep has not reached yet
+    bool ok = true;
+    if (nx > i && nx <= old_last) ok &= hp.push(nx);
+    if (par_new > i && par_new <= old_last) ok &= hp.push(par_new);
+    if (!ok) {
+      atomicOr(err, DERR_QUEUE);
+      break;
+    }
+  }
+  d.pcount = pc;
+  dyn[s] = d;
+}
+
+// precon (reconnection.f90:11-61).
+__device__ void norm_tanf(const State &S, int g, double t[3]) {  // general.f90:106-117
+  double x[3], gi[3], gb[3];
+  load3(S.X, S.T, g, x);
+  load3(S.GI, S.T, g, gi);
+  load3(S.GB, S.T, g, gb);
+  deriv1(x, gi, gb, t);
+  const double len = e_sqrt(e_add(e_add(e_sq(t[0]), e_sq(t[1])), e_sq(t[2])));
+  for (int c = 0; c < 3; ++c) t[c] = e_div(t[c], len);
+}
+
+__global__ void k_recon_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S,
+                                const int *__restrict__ pos_a, const int *__restrict__ list_a, unsigned *err,
+                                DevEvent *ev, int *ev_count, int ev_cap) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys || *err) return;
+  const SysConst &sc = scs[s];
+  SysDyn d = dyn[s];
+  if (!recon_step(sc, d)) return;
+  const int base = sc.base;
+  const int li = pos_a[base], le = pos_a[base + sc.cap + 1];
+  const long long T = S.T;
+  for (int idx = li; idx < le; ++idx) {
+    const int i = list_a[idx];
+    if (S.nxt[i] == 0) continue;
+    const int pari = S.nxt[i], parb = S.prv[i];
+    const int j = S.cl[i];
+    if (j == pari || j == parb || j == 0) continue;
+    if (S.nxt[j] == 0) continue;
+    const int parjb = S.prv[j];
+    double t1[3], t2[3];
+    norm_tanf(S, i, t1);
+    norm_tanf(S, j, t2);
+    const double dot_val = dot3(t1, t2);
+    if (dot_val > 0.9) continue;
+    double xi[3], gii[3], gbi[3], xj[3], gij[3], gbj[3], xpi[3], xpj[3];
+    load3(S.X, T, i, xi);
+    load3(S.GI, T, i, gii);
+    load3(S.GB, T, i, gbi);
+    load3(S.X, T, j, xj);
+    load3(S.GI, T, j, gij);
+    load3(S.GB, T, j, gbj);
+    load3(S.X, T, pari, xpi);
+    load3(S.X, T, parjb, xpj);
+    const double l_before = e_add(e_add(e_add(dist_gen(xi, gii), dist_gen(xi, gbi)), dist_gen(xj, gij)), dist_gen(xj, gbj));
+    const double l_after = e_add(e_add(e_add(dist_gen(xi, gbi), dist_gen(xi, xj)), dist_gen(xj, gij)), dist_gen(xpi, xpj));
+    if (l_after <= l_before) {
+      d.recon_count++;
+      log_event(d, s, NV_EV_RECON, i, j, ev, ev_count, ev_cap);
+      S.nxt[parjb] = pari;
+      S.prv[pari] = parjb;
+      S.nxt[i] = j;
+      S.prv[j] = i;
+      loop_killer(S, d, s, pari, d.pcount, ev, ev_count, ev_cap);
+      loop_killer(S, d, s, i, d.pcount, ev, ev_count, ev_cap);
+    }
+  }
+  dyn[s] = d;
+}
+
+// premove (line.f90:102-130).
+__global__ void k_remove_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S,
+                                 const int *__restrict__ pos_a, const int *__restrict__ list_a, unsigned *err,
+                                 DevEvent *ev, int *ev_count, int ev_cap) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys || *err) return;
+  const SysConst &sc = scs[s];
+  SysDyn d = dyn[s];
+  if (!recon_step(sc, d)) return;
+  const int base = sc.base;
+  int li = pos_a[base];
+  const int le = pos_a[base + sc.cap + 1];
+  const int lastslot = base + d.pcount;
+  const double thr = e_mul(.99, sc.delta);
+  Heap hp;
+  int last = base;
+  const long long T = S.T;
+  for (;;) {
+    const int i = sweep_next(list_a, li, le, hp, last);
+    if (i == INT_MAX || i > lastslot) break;
+    last = i;
+    if (S.nxt[i] == 0) continue;
+    const int infront = S.nxt[i];
+    const int tinfront = S.nxt[infront];
+    double xi[3], xt[3];
+    load3(S.X, T, i, xi);
+    load3(S.X, T, tinfront, xt);
+    if (!(dist_gen(xi, xt) < thr)) continue;
+    S.prv[tinfront] = i;
+    S.nxt[i] = tinfront;
+    clear_particle(S, infront);
+    log_event(d, s, NV_EV_REMOVE, i, infront, ev, ev_count, ev_cap);
+    loop_killer(S, d, s, i, d.pcount, ev, ev_count, ev_cap);
+    d.remove_count++;
+    const int p = S.prv[i];
+    if (p > i && p <= lastslot && !hp.push(p)) {
+      atomicOr(err, DERR_QUEUE);
+      break;
+    }
+  }
+  dyn[s] = d;
+}
+
+// pclose (line.f90:135-160): exact nearest non-neighbour, non-periodic distance, strict <
+// so ties keep the lowest j.  One thread per target slot.
+__global__ void k_pclose_brute(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn,
+                               const int *__restrict__ sys_of, const double *__restrict__ X,
+                               const int *__restrict__ nxt, const int *__restrict__ prv, int *__restrict__ cl,
+                               double *__restrict__ CD, long long T, const unsigned *err) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= T || *err) return;
+  const int s = sys_of[g];
+  const SysConst &sc = scs[s];
+  if (sc.use_tree || !recon_step(sc, dyn[s])) return;
+  const int pc = dyn[s].pcount;
+  const int k = (int)(g - sc.base);
+  if (k < 1 || k > pc || nxt[g] == 0) return;
+  const int ni = nxt[g], pi = prv[g];
+  double xi[3];
+  load3(X, T, (int)g, xi);
+  double best = 100.;
+  double best2 = 1e300;
+  int bj = cl[g];
+  for (int j = sc.base + 1; j <= sc.base + pc; ++j) {
+    if (nxt[j] == 0 || j == g || j == ni || j == pi) continue;
+    double xj[3];
+    load3(X, T, j, xj);
+    const double d2 = e_add(e_add(e_sq(e_sub(xi[0], xj[0])), e_sq(e_sub(xi[1], xj[1]))), e_sq(e_sub(xi[2], xj[2])));
+    if (d2 > best2) continue;  // sqrt is monotone: cannot be strictly closer
+    const double dist = e_sqrt(d2);
+    if (dist < best) {
+      best = dist;
+      best2 = d2;
+      bj = j;
+    }
+  }
+  cl[g] = bj;
+  CD[g] = best;
+}
+
+State make_state(nv_handle *h) {
+  return State{h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv, h->closest, h->T};
+}
+
+void compact(nv_handle *h, int *flag, int *pos, int *list) {
+  TopoBuffers *tb = h->topo;
+  size_t bytes = tb->cub_bytes;
+  cub::DeviceScan::ExclusiveSum(tb->cub_tmp, bytes, flag, pos, (int)(h->T + 1), h->stream);
+  k_scatter<<<grid_for(h->T, TB), TB, 0, h->stream>>>(flag, pos, list, h->T);
+}
+
+int resolver_grid(nv_handle *h) { return grid_for(h->nsys, 32); }
+
+}  // namespace
+
+void topo_alloc(nv_handle *h) {
+  auto *tb = new TopoBuffers();
+  const size_t n = (size_t)h->T + 1;
+  cudaMalloc(&tb->flag_a, n * sizeof(int));
+  cudaMalloc(&tb->pos_a, n * sizeof(int));
+  cudaMalloc(&tb->list_a, n * sizeof(int));
+  cudaMalloc(&tb->flag_b, n * sizeof(int));
+  cudaMalloc(&tb->pos_b, n * sizeof(int));
+  cudaMalloc(&tb->list_b, n * sizeof(int));
+  cub::DeviceScan::ExclusiveSum(nullptr, tb->cub_bytes, tb->flag_a, tb->pos_a, (int)n);
+  cudaMalloc(&tb->cub_tmp, std::max<size_t>(tb->cub_bytes, 16));
+  h->topo = tb;
+}
+
+void topo_free(nv_handle *h) {
+  TopoBuffers *tb = h->topo;
+  if (!tb) return;
+  cudaFree(tb->flag_a); cudaFree(tb->pos_a); cudaFree(tb->list_a);
+  cudaFree(tb->flag_b); cudaFree(tb->pos_b); cudaFree(tb->list_b);
+  cudaFree(tb->cub_tmp);
+  delete tb;
+  h->topo = nullptr;
+}
+
+void launch_pinsert(nv_handle *h) {
+  TopoBuffers *tb = h->topo;
+  k_zero_live<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_dyn, h->nsys);
+  k_mark_insert<<<grid_for(h->T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->gi, h->nxt,
+                                                               tb->flag_a, tb->flag_b, h->T, h->d_err);
+  compact(h, tb->flag_a, tb->pos_a, tb->list_a);
+  compact(h, tb->flag_b, tb->pos_b, tb->list_b);
+  k_insert_resolve<<<resolver_grid(h), 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a,
+                                                           tb->list_a, tb->pos_b, tb->list_b, h->d_err, h->d_events,
+                                                           h->d_event_count, h->event_cap);
+}
+
+void launch_pclose(nv_handle *h, bool only_brute) {
+  bool any_brute = false, any_tree = false;
+  for (auto &s : h->sc) (s.use_tree ? any_tree : any_brute) = true;
+  if (any_brute)
+    k_pclose_brute<<<grid_for(h->T, 128), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->nxt, h->prv,
+                                                               h->closest, h->closestd, h->T, h->d_err);
+  if (any_tree && !only_brute) launch_closest_tree(h);
+}
+
+void launch_precon(nv_handle *h) {
+  TopoBuffers *tb = h->topo;
+  k_mark_recon<<<grid_for(h->T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->closestd, h->nxt,
+                                                              tb->flag_a, h->T, h->d_err);
+  compact(h, tb->flag_a, tb->pos_a, tb->list_a);
+  k_recon_resolve<<<resolver_grid(h), 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a,
+                                                          tb->list_a, h->d_err, h->d_events, h->d_event_count,
+                                                          h->event_cap);
+}
+
+void launch_premove(nv_handle *h) {
+  TopoBuffers *tb = h->topo;
+  k_mark_remove<<<grid_for(h->T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->nxt,
+                                                               tb->flag_a, h->T, h->d_err);
+  compact(h, tb->flag_a, tb->pos_a, tb->list_a);
+  k_remove_resolve<<<resolver_grid(h), 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a,
+                                                           tb->list_a, h->d_err, h->d_events, h->d_event_count,
+                                                           h->event_cap);
+}

@@ -34,3 +34,22 @@ def rel_err(a: np.ndarray, b: np.ndarray) -> np.ndarray:
 
 def rms_rel(a: np.ndarray, b: np.ndarray) -> float:
     return float(np.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2)))
+
+
+def small_rings(seed: int, n: int, npts: int, R: float, spread: float = 0.04):
+    """n rings of npts points and radius R at random centres/orientations (no wrapping)."""
+    from nuvort_b200.abi import State
+    rng = np.random.default_rng(seed)
+    xs, nx, pv, b = [], [], [], 0
+    for _ in range(n):
+        s = single_ring(R, npts, centre=rng.uniform(-spread, spread, 3), normal=rng.standard_normal(3))
+        xs.append(s.x)
+        nx.append(s.infront + b)
+        pv.append(s.behind + b)
+        b += npts
+    x = np.ascontiguousarray(np.concatenate(xs))
+    N = len(x)
+    z = lambda: np.zeros((N, 3))
+    return State(x=x, infront=np.concatenate(nx).astype(np.int32), behind=np.concatenate(pv).astype(np.int32),
+                 u=z(), u1=z(), u2=z(), ghosti=z(), ghostb=z(), closest=np.zeros(N, np.int32),
+                 closestd=np.zeros(N))

@@ -1,0 +1,138 @@
+"""Topology stages on the GPU against the oracle.
+
+Identical-input tests upload one state to both sides and run a single stage: every slot,
+link, ghost and event must agree bit for bit (the stage's arithmetic is one rounding per
+operation on both sides).  The whole-step test runs the full time loop on both sides;
+positions then drift only by the ulp-level difference of the device log() in the local
+term, and the event logs must be identical."""
+import numpy as np
+import pytest
+
+from helpers import config0_params, small_rings, tangle
+from nuvort_b200.abi import NV_ERR_CAPACITY, State
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _moved_state(p, st, steps=1):
+    """Oracle state after ghostp+pmotion: positions moved, ghosts still the step-start ones."""
+    o = Oracle(p, st)
+    for _ in range(steps):
+        o.stage("ghostp")
+        o.stage("pmotion")
+    return o.download()
+
+
+def _assert_same(a: State, b: State):
+    assert a.pcount == b.pcount
+    for name in ("x", "u", "u1", "u2", "ghosti", "ghostb", "infront", "behind"):
+        assert np.array_equal(getattr(a, name), getattr(b, name)), name
+
+
+def _run_stage(p, st, stages, cap_extra=512):
+    from nuvort_b200.api import Handle
+    h = Handle(p, [st.pcount + cap_extra], states=[st])
+    h.set_clock(0, 0.0, 1)
+    o = Oracle(p, st, t=0.0, itime=1)
+    for s in stages:
+        h.stage(s)
+        o.stage(s)
+    a, b = h.download(), o.download()
+    ea, eb = h.events(), o.events()
+    ca, cb = h.counters(), o.counters()
+    h.close()
+    return a, b, ea, eb, ca, cb
+
+
+def test_pinsert_identical_inputs():
+    st = tangle(21, 0.002, n_rings=10)
+    p = config0_params()
+    mv = _moved_state(p, st)
+    p_ins = config0_params(delta=0.00185)  # many chords now exceed delta
+    a, b, ea, eb, ca, cb = _run_stage(p_ins, mv, ["pinsert"])
+    assert len(eb) > 20
+    assert ea == eb
+    _assert_same(a, b)
+    assert ca.insert_count == cb.insert_count and ca.pcount == cb.pcount
+
+
+def test_pinsert_fills_empty_slots_then_appends():
+    st = tangle(22, 0.002, n_rings=10)
+    # empty one ring so insertions reuse its slots first (minloc, line.f90:44-47)
+    n0 = 1
+    while st.infront[n0 - 1] != 1:
+        n0 += 1
+    first_ring = n0
+    st.x[:first_ring] = 0
+    st.infront[:first_ring] = 0
+    st.behind[:first_ring] = 0
+    p = config0_params()
+    mv = _moved_state(p, st)
+    a, b, ea, eb, ca, cb = _run_stage(config0_params(delta=0.0018), mv, ["pinsert"])
+    assert ea == eb
+    _assert_same(a, b)
+    assert any(j <= first_ring for (_, k, i, j) in eb if k == 1)
+
+
+def test_pinsert_capacity_error():
+    from nuvort_b200.api import Handle, NuvortError
+    st = tangle(23, 0.002, n_rings=6)
+    mv = _moved_state(config0_params(), st)
+    h = Handle(config0_params(delta=0.0018), [mv.pcount + 2], states=[mv])
+    with pytest.raises(NuvortError) as e:
+        h.stage("pinsert")
+    assert e.value.code == NV_ERR_CAPACITY
+    h.close()
+
+
+def test_premove_cascade_identical_inputs():
+    st = tangle(24, 0.002, n_rings=10)
+    p = config0_params()
+    mv = _moved_state(p, st)
+    p_rm = config0_params(delta=0.004, overide_timestep_check=True)
+    a, b, ea, eb, ca, cb = _run_stage(p_rm, mv, ["premove"])
+    assert ca.remove_count == cb.remove_count and cb.remove_count > 0
+    assert ea == eb
+    _assert_same(a, b)
+
+
+def test_premove_kills_small_loops():
+    st = small_rings(25, 8, 6, 0.0025)
+    p = config0_params()
+    mv = _moved_state(p, st)
+    p_rm = config0_params(delta=0.005, overide_timestep_check=True)  # loops fall below 4 points
+    a, b, ea, eb, ca, cb = _run_stage(p_rm, mv, ["premove"])
+    assert cb.loop_kills > 0
+    assert ea == eb
+    _assert_same(a, b)
+
+
+def test_pclose_precon_identical_inputs():
+    st = tangle(26, 0.002, n_rings=40)  # dense: rings cross at t=0
+    p = config0_params()
+    mv = _moved_state(p, st)
+    a, b, ea, eb, ca, cb = _run_stage(p, mv, ["pclose", "precon"])
+    assert np.array_equal(a.closest, b.closest)
+    assert np.array_equal(a.closestd, b.closestd)
+    assert cb.recon_count > 0
+    assert ea == eb
+    _assert_same(a, b)
+
+
+def test_whole_steps_config0_events_identical():
+    from nuvort_b200.api import Handle
+    st = tangle(0, 0.002, n_rings=8)
+    p = config0_params()
+    h = Handle(p, [st.pcount + 512], states=[st])
+    o = Oracle(p, st)
+    h.step(200)
+    o.step(200)
+    assert h.events() == o.events()
+    a, b = h.download(), o.download()
+    assert np.array_equal(a.infront, b.infront) and np.array_equal(a.behind, b.behind)
+    assert np.max(np.abs(a.x - b.x)) < 1e-12
+    ca, cb = h.counters(), o.counters()
+    assert (ca.recon_count, ca.remove_count, ca.insert_count) == (cb.recon_count, cb.remove_count, cb.insert_count)
+    assert ca.t == cb.t and ca.itime == cb.itime == 200
+    h.close()
