@@ -50,7 +50,7 @@ def test_pinsert_identical_inputs():
     p = config0_params()
     mv = _moved_state(p, st)
     p_ins = config0_params(delta=0.00185)  # many chords now exceed delta
-    a, b, ea, eb, ca, cb = _run_stage(p_ins, mv, ["pinsert"])
+    a, b, ea, eb, ca, cb = _run_stage(p_ins, mv, ["pinsert"], cap_extra=4096)
     assert len(eb) > 20
     assert ea == eb
     _assert_same(a, b)
@@ -69,7 +69,7 @@ def test_pinsert_fills_empty_slots_then_appends():
     st.behind[:first_ring] = 0
     p = config0_params()
     mv = _moved_state(p, st)
-    a, b, ea, eb, ca, cb = _run_stage(config0_params(delta=0.0018), mv, ["pinsert"])
+    a, b, ea, eb, ca, cb = _run_stage(config0_params(delta=0.0018), mv, ["pinsert"], cap_extra=4096)
     assert ea == eb
     _assert_same(a, b)
     assert any(j <= first_ring for (_, k, i, j) in eb if k == 1)
