@@ -126,6 +126,19 @@ typedef struct nv_counters {
   double t;              /* simulation time                                     */
 } nv_counters;
 
+/* One octree node (type node, src/tree.f90:20-32) as dumped in preorder by nv_tree_dump:
+ * children in the reference's fbl..btr order, empty (pcount==0) children omitted. */
+typedef struct nv_tree_node {
+  double pos[3];      /* corner posx, posy, posz                              */
+  double width;
+  double cent[3];     /* centx, centy, centz                                  */
+  double circ[3];
+  int32_t pcount;
+  int32_t depth;      /* root = 0                                             */
+  int32_t leaf;       /* the member slot when pcount==1, else 0               */
+  int32_t first_next; /* parray(1)%infront at construction (tree.f90:221,282) */
+} nv_tree_node;
+
 typedef struct nv_handle nv_handle;
 
 /* ---- set-up ------------------------------------------------------------------------ */
@@ -176,6 +189,10 @@ int nv_step(nv_handle *h, int32_t nsteps);
  * (ghostp, construct_tree when velocity is Tree, then src/timestep.f90:49-141).
  * u3 receives [3*pcount] velocities (0 for empty slots).  Nothing is moved. */
 int nv_calc_velocity(nv_handle *h, int32_t sys, double *u3);
+
+/* Dump system sys's current octree in preorder; *n receives the node count (records
+ * beyond cap are not written).  Replaces reading vtree (src/tree.f90:34). */
+int nv_tree_dump(nv_handle *h, int32_t sys, nv_tree_node *buf, int32_t cap, int32_t *n);
 
 /* Cumulative device time (ms) per stage since creation: ms[0] ghosts, [1] tree build,
  * [2] velocity, [3] AB3 update, [4] topology, [5] whole steps.  n = entries wanted. */

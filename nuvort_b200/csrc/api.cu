@@ -629,6 +629,13 @@ int nv_stage_times(nv_handle *h, double *ms, int32_t n) {
   return NV_OK;
 }
 
+int nv_tree_dump(nv_handle *h, int32_t sys, nv_tree_node *buf, int32_t cap, int32_t *n) {
+  if (!h || !n || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_tree_dump: bad arguments");
+  int rc = set_device(h);
+  if (rc) return rc;
+  return tree_dump(h, sys, buf, cap, n);
+}
+
 int nv_sync(nv_handle *h) {
   if (!h) return set_error(NV_ERR_ARG, "null handle");
   int rc = set_device(h);

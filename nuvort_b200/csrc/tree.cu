@@ -1,10 +1,651 @@
-// tree.cu -- octree build and walks (placeholder until the device tree lands).
+// tree.cu -- Barnes-Hut octree on the device: build, velocity walk, closest-point walk.
+//
+// Build (construct_tree/build_tree/new_tree, src/tree.f90:38-157), top-down, one level per
+// pass, all systems of the handle at once:
+//   * Node k's members are kept as a contiguous list of slots in ascending slot order.
+//     Splitting a node is a stable 8-way partition of that list by octant, so every child's
+//     list is again in ascending slot order -- the order in which the reference sums a
+//     node's centre and circulation (tree.f90:124-143), reproduced exactly.
+//   * The octant of a point is decided by the reference's own membership test against the
+//     child's corner, computed with the same FP64 additions (child corner = parent corner
+//     (+ width/2)); a point that fails its child's upper bound (rounding can make a child's
+//     far face differ by an ulp from the parent's) belongs to no child, as in the reference.
+//   * Octant digit = 4*[y upper] + 2*[z upper] + [x upper]: the child order fbl, fbr, ftl,
+//     ftr, bbl, bbr, btl, btr of tree.f90:71-93.  Only non-empty children are stored;
+//     siblings are contiguous, so a preorder walk follows first_child / skip links.
+//   * The root holds every slot (pcount includes empty slots, tree.f90:48), its centre is
+//     the mean over live slots and its circulation is zero (tree.f90:50-54).
+// Walks: one thread per target point, stackless preorder over first_child/skip, with the
+// reference's opening test and arithmetic (tree_walk tree.f90:250-316, closest_tree
+// :206-244) in the same order, so the accumulated velocity is the reference's bit for bit.
+#include <cub/cub.cuh>
+
 #include "handle.cuh"
 
-struct TreeBuffers {};
-void tree_alloc(nv_handle *) {}
-void tree_free(nv_handle *) {}
-void launch_tree_build(nv_handle *) {}
-void launch_tree_walk(nv_handle *) {}
-void launch_closest_tree(nv_handle *) {}
-int tree_dump(nv_handle *, int, void *, int, int *n) { *n = 0; return NV_ERR_UNSUPPORTED; }
+constexpr int kMaxLevels = NV_TREE_MAX_DEPTH;
+constexpr int kEnd = -1;
+constexpr int kBigNode = 2048;  // nodes with more members are split by a whole block
+
+struct TreeBuffers {
+  int max_nodes = 0;
+  long long max_members = 0;
+  double4 *nA = nullptr;  // cent.xyz, width
+  double4 *nB = nullptr;  // circ.xyz, geo_dist
+  double4 *nP = nullptr;  // corner posx,posy,posz
+  int4 *nI = nullptr;     // pcount, first_child, skip, first_next
+  int2 *nR = nullptr;     // member range start, member count
+  int *nDepth = nullptr;
+  int *nLeaf = nullptr;
+  int *members = nullptr;
+  int *ctr = nullptr;     // [0] n_nodes [1] n_members [2 + L] first node of level L
+  int *flag = nullptr, *pos = nullptr;
+  void *cub_tmp = nullptr;
+  size_t cub_bytes = 0;
+  bool built = false;
+};
+
+namespace {
+
+constexpr int TB = 256;
+
+__global__ void k_live_flags(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn,
+                             const int *__restrict__ sys_of, const int *__restrict__ nxt, int *flag, long long T) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g > T) return;
+  int f = 0;
+  if (g < T) {
+    const int s = sys_of[g];
+    const SysConst &sc = scs[s];
+    const int k = (int)(g - sc.base);
+    f = (sc.use_tree || sc.sched_tree) && k >= 1 && k <= dyn[s].pcount && nxt[g] != 0;
+  }
+  flag[g] = f;
+}
+
+__global__ void k_scatter_live(const int *__restrict__ flag, const int *__restrict__ pos, int *__restrict__ members,
+                               long long T) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < T && flag[g]) members[pos[g]] = (int)g;
+}
+
+// Root of every system (construct_tree, tree.f90:38-59).
+__global__ void k_roots(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, const int *__restrict__ nxt,
+                        const int *__restrict__ pos, TreeBuffers tb, long long T) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s == 0) {
+    tb.ctr[0] = nsys;
+    tb.ctr[2] = 0;
+    tb.ctr[3] = nsys;
+    tb.ctr[1] = pos[T];
+  }
+  if (s >= nsys) return;
+  const SysConst &sc = scs[s];
+  const int pc = (sc.use_tree || sc.sched_tree) ? dyn[s].pcount : 0;
+  const double h = -sc.bsize / 2.0;
+  tb.nP[s] = make_double4(h, h, h, 0);
+  tb.nA[s] = make_double4(0, 0, 0, sc.bsize);
+  tb.nB[s] = make_double4(0, 0, 0, 0);
+  tb.nI[s] = make_int4(pc, kEnd, kEnd, pc >= 1 ? nxt[sc.base + 1] : 0);
+  tb.nR[s] = make_int2(pos[sc.base], pos[sc.base + sc.cap + 1] - pos[sc.base]);
+  tb.nDepth[s] = 0;
+  tb.nLeaf[s] = pc == 1 ? sc.base + 1 : 0;
+  dyn[s].tree_eval = 0;
+}
+
+// Octant of x in node (corner P, half-width h), or 8 when x lies in no child.
+__device__ __forceinline__ int octant(const double x[3], const double4 P, double h) {
+  const double p[3] = {P.x, P.y, P.z};
+  int up[3];
+  bool in = true;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double mid = e_add(p[c], h);  // child corner posx+(width/2)      tree.f90:74
+    if (x[c] >= mid) {
+      up[c] = 1;
+      in = in && (x[c] < e_add(mid, h));  // x < posx+width of the upper child
+    } else {
+      up[c] = 0;
+      in = in && (x[c] >= p[c]);  // lower child: posx <= x < posx+width (= mid)
+    }
+  }
+  return in ? (4 * up[1] + 2 * up[2] + up[0]) : 8;
+}
+
+__device__ __forceinline__ double4 ldg4(const double4 *p) {
+  const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+  const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+__device__ __forceinline__ void load_x(const double *__restrict__ X, long long T, int g, double x[3]) {
+  x[0] = __ldg(X + g);
+  x[1] = __ldg(X + T + g);
+  x[2] = __ldg(X + 2 * T + g);
+}
+
+// Create the non-empty children of node p (counts cnt[0..7]); returns first child id via
+// *id0 and member base via *mb0 (or -1 on overflow).  Called by one thread.
+__device__ void make_children(TreeBuffers &tb, int p, const int cnt[8], int *id0_out, int *mb0_out, unsigned *err) {
+  int mask = 0, kept = 0;
+#pragma unroll
+  for (int d = 0; d < 8; ++d) {
+    if (cnt[d]) mask |= 1 << d;
+    kept += cnt[d];
+  }
+  const int nchild = __popc(mask);
+  int4 Ip = tb.nI[p];
+  if (nchild == 0) {
+    *id0_out = -1;
+    *mb0_out = -1;
+    return;
+  }
+  const int id0 = atomicAdd(&tb.ctr[0], nchild);
+  const int mb0 = atomicAdd(&tb.ctr[1], kept);
+  if (id0 + nchild > tb.max_nodes || (long long)mb0 + kept > tb.max_members) {
+    atomicOr(err, DERR_TREE_NODES);
+    *id0_out = -1;
+    *mb0_out = -1;
+    return;
+  }
+  const double4 P = tb.nP[p];
+  const double h = tb.nA[p].w / 2.0;
+  const int depth = tb.nDepth[p] + 1;
+  int off = 0, k = 0;
+#pragma unroll
+  for (int d = 0; d < 8; ++d) {
+    if (!cnt[d]) continue;
+    const int id = id0 + k;
+    const bool last = (k == nchild - 1);
+    const double cx = (d & 1) ? e_add(P.x, h) : P.x;
+    const double cz = (d & 2) ? e_add(P.z, h) : P.z;
+    const double cy = (d & 4) ? e_add(P.y, h) : P.y;
+    tb.nP[id] = make_double4(cx, cy, cz, 0);
+    tb.nA[id] = make_double4(0, 0, 0, h);
+    tb.nI[id] = make_int4(cnt[d], kEnd, last ? Ip.z : id + 1, 0);
+    tb.nR[id] = make_int2(mb0 + off, cnt[d]);
+    tb.nDepth[id] = depth;
+    off += cnt[d];
+    ++k;
+  }
+  tb.nI[p].y = id0;
+  *id0_out = id0;
+  *mb0_out = mb0;
+}
+
+// Split every node of `level` with at most kBigNode members: one warp per node.
+__global__ void __launch_bounds__(128) k_split_warp(const double *__restrict__ X, long long T, TreeBuffers tb, int level,
+                                                    unsigned *err) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int nb = tb.ctr[2 + level], ne = tb.ctr[3 + level];
+  const unsigned lt = (1u << lane) - 1u;
+  for (int p = nb + warp; p < ne; p += nwarps) {
+    const int4 Ip = tb.nI[p];
+    const int2 R = tb.nR[p];
+    if (Ip.x <= 1 || R.y > kBigNode) continue;
+    if (tb.nDepth[p] >= kMaxLevels) {
+      if (lane == 0) atomicOr(err, DERR_TREE_DEPTH);
+      continue;
+    }
+    const double4 P = tb.nP[p];
+    const double h = tb.nA[p].w / 2.0;
+    int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k0 = 0; k0 < R.y; k0 += 32) {
+      const int k = k0 + lane;
+      int d = 8;
+      if (k < R.y) {
+        double x[3];
+        load_x(X, T, tb.members[R.x + k], x);
+        d = octant(x, P, h);
+      }
+#pragma unroll
+      for (int dd = 0; dd < 8; ++dd) cnt[dd] += __popc(__ballot_sync(0xffffffffu, d == dd));
+    }
+    int id0 = -1, mb0 = -1;
+    if (lane == 0) make_children(tb, p, cnt, &id0, &mb0, err);
+    id0 = __shfl_sync(0xffffffffu, id0, 0);
+    mb0 = __shfl_sync(0xffffffffu, mb0, 0);
+    if (id0 < 0) continue;
+    int base_off[8], childid[8], run[8];
+    {
+      int off = 0, k = 0;
+#pragma unroll
+      for (int dd = 0; dd < 8; ++dd) {
+        base_off[dd] = off;
+        childid[dd] = cnt[dd] ? id0 + k : -1;
+        k += cnt[dd] ? 1 : 0;
+        off += cnt[dd];
+        run[dd] = 0;
+      }
+    }
+    for (int k0 = 0; k0 < R.y; k0 += 32) {
+      const int k = k0 + lane;
+      int d = 8, slot = 0;
+      if (k < R.y) {
+        double x[3];
+        slot = tb.members[R.x + k];
+        load_x(X, T, slot, x);
+        d = octant(x, P, h);
+      }
+      int mypos = -1;
+#pragma unroll
+      for (int dd = 0; dd < 8; ++dd) {
+        const unsigned b = __ballot_sync(0xffffffffu, d == dd);
+        if (d == dd) mypos = mb0 + base_off[dd] + run[dd] + __popc(b & lt);
+        run[dd] += __popc(b);
+      }
+      if (mypos >= 0) tb.members[mypos] = slot;
+    }
+    (void)childid;
+  }
+}
+
+// Split every node of `level` with more than kBigNode members: one block (32 warps) per
+// node, each warp taking a contiguous slice of the member list, so the partition stays
+// stable.
+__global__ void __launch_bounds__(1024) k_split_block(const double *__restrict__ X, long long T, TreeBuffers tb, int level,
+                                                      unsigned *err) {
+  __shared__ int wcnt[32][8];
+  __shared__ int s_id0, s_mb0, s_cnt[8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const int nb = tb.ctr[2 + level], ne = tb.ctr[3 + level];
+  for (int p = nb + blockIdx.x; p < ne; p += gridDim.x) {
+    const int4 Ip = tb.nI[p];
+    const int2 R = tb.nR[p];
+    if (Ip.x <= 1 || R.y <= kBigNode) continue;  // block-uniform
+    if (tb.nDepth[p] >= kMaxLevels) {
+      if (threadIdx.x == 0) atomicOr(err, DERR_TREE_DEPTH);
+      continue;
+    }
+    const double4 P = tb.nP[p];
+    const double h = tb.nA[p].w / 2.0;
+    const int per = (R.y + nw - 1) / nw;
+    const int s0 = w * per, s1 = min(R.y, s0 + per);
+    int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k0 = s0; k0 < s1; k0 += 32) {
+      const int k = k0 + lane;
+      int d = 8;
+      if (k < s1) {
+        double x[3];
+        load_x(X, T, tb.members[R.x + k], x);
+        d = octant(x, P, h);
+      }
+#pragma unroll
+      for (int dd = 0; dd < 8; ++dd) cnt[dd] += __popc(__ballot_sync(0xffffffffu, d == dd));
+    }
+    if (lane == 0)
+#pragma unroll
+      for (int dd = 0; dd < 8; ++dd) wcnt[w][dd] = cnt[dd];
+    __syncthreads();
+    if (threadIdx.x < 8) {
+      int tot = 0;
+      for (int ww = 0; ww < nw; ++ww) {
+        const int c = wcnt[ww][threadIdx.x];
+        wcnt[ww][threadIdx.x] = tot;  // exclusive prefix over warps
+        tot += c;
+      }
+      s_cnt[threadIdx.x] = tot;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int c[8];
+      for (int dd = 0; dd < 8; ++dd) c[dd] = s_cnt[dd];
+      int id0, mb0;
+      make_children(tb, p, c, &id0, &mb0, err);
+      s_id0 = id0;
+      s_mb0 = mb0;
+    }
+    __syncthreads();
+    const int mb0 = s_mb0;
+    if (s_id0 >= 0) {
+      int base_off[8], run[8];
+      int off = 0;
+#pragma unroll
+      for (int dd = 0; dd < 8; ++dd) {
+        base_off[dd] = off + wcnt[w][dd];
+        off += s_cnt[dd];
+        run[dd] = 0;
+      }
+      for (int k0 = s0; k0 < s1; k0 += 32) {
+        const int k = k0 + lane;
+        int d = 8, slot = 0;
+        if (k < s1) {
+          double x[3];
+          slot = tb.members[R.x + k];
+          load_x(X, T, slot, x);
+          d = octant(x, P, h);
+        }
+        int mypos = -1;
+#pragma unroll
+        for (int dd = 0; dd < 8; ++dd) {
+          const unsigned b = __ballot_sync(0xffffffffu, d == dd);
+          if (d == dd) mypos = mb0 + base_off[dd] + run[dd] + __popc(b & lt);
+          run[dd] += __popc(b);
+        }
+        if (mypos >= 0) tb.members[mypos] = slot;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_mark_level(TreeBuffers tb, int level) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) tb.ctr[4 + level] = tb.ctr[0];
+}
+
+// Centre and circulation of every node: sequential sums in ascending slot order
+// (new_tree, tree.f90:124-152; the root's masked mean, tree.f90:50-54), plus the
+// geometric distance of the opening test's correction (tree.f90:267-269).
+__global__ void k_node_sums(const SysConst *__restrict__ scs, const int *__restrict__ sys_of, const double *__restrict__ X,
+                            const double *__restrict__ GI, const int *__restrict__ nxt, long long T, TreeBuffers tb,
+                            int nsys, unsigned *err) {
+  const int n = tb.ctr[0];
+  for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
+    const int2 R = tb.nR[id];
+    int4 I = tb.nI[id];
+    const double4 P = tb.nP[id];
+    const double w = tb.nA[id].w;
+    double cx = 0, cy = 0, cz = 0, qx = 0, qy = 0, qz = 0;
+    const bool root = id < nsys;
+    for (int k = 0; k < R.y; ++k) {
+      const int g = tb.members[R.x + k];
+      const double x0 = __ldg(X + g), x1 = __ldg(X + T + g), x2 = __ldg(X + 2 * T + g);
+      cx = e_add(cx, x0);
+      cy = e_add(cy, x1);
+      cz = e_add(cz, x2);
+      if (!root) {
+        qx = e_sub(e_add(qx, __ldg(GI + g)), x0);
+        qy = e_sub(e_add(qy, __ldg(GI + T + g)), x1);
+        qz = e_sub(e_add(qz, __ldg(GI + 2 * T + g)), x2);
+      }
+    }
+    if (R.y != 0) {
+      cx = e_div(cx, (double)R.y);
+      cy = e_div(cy, (double)R.y);
+      cz = e_div(cz, (double)R.y);
+    }
+    const double hw = w / 2.;
+    const double geo = e_sqrt(e_add(e_add(e_sq(e_sub(cx, e_add(P.x, hw))), e_sq(e_sub(cy, e_add(P.y, hw)))),
+                                     e_sq(e_sub(cz, e_add(P.z, hw)))));
+    tb.nA[id] = make_double4(cx, cy, cz, w);
+    tb.nB[id] = make_double4(qx, qy, qz, geo);
+    if (!root) {
+      const int first = R.y > 0 ? tb.members[R.x] : 0;
+      I.w = first ? nxt[first] : 0;
+      tb.nI[id] = I;
+      tb.nLeaf[id] = I.x == 1 ? first : 0;
+      if (tb.nDepth[id] >= kMaxLevels && I.x > 1) atomicOr(err, DERR_TREE_DEPTH);
+    }
+  }
+}
+
+// tree_walk (tree.f90:250-316) for one image; accumulates into acc in preorder.
+__device__ __forceinline__ void walk_fp64(const TreeBuffers &tb, int root, const SysConst &sc, const double xi[3],
+                                          int gi_, int pi_, const int *__restrict__ prv, const double s[3], bool unshifted,
+                                          double acc[3], unsigned long long &evals, bool &singular) {
+  const double qc = sc.quant_circ, two_pi = sc.two_pi, theta0 = sc.tree_theta;
+  const bool corr = sc.tree_extra_correction;
+  int node = root;
+  while (node != kEnd) {
+    const double4 A = ldg4(&tb.nA[node]);
+    const int4 I = __ldg(&tb.nI[node]);
+    if (I.x == 0) {
+      node = I.z;
+      continue;
+    }
+    const double cs[3] = {e_add(A.x, s[0]), e_add(A.y, s[1]), e_add(A.z, s[2])};
+    const double dist = e_sqrt(e_add(e_add(e_sq(e_sub(xi[0], cs[0])), e_sq(e_sub(xi[1], cs[1]))), e_sq(e_sub(xi[2], cs[2]))));
+    const double4 B = ldg4(&tb.nB[node]);
+    double theta;
+    if (corr) {
+      const double dg = e_sub(dist, B.w);
+      theta = dg > 0. ? e_div(A.w, dg) : e_div(A.w, dist);
+    } else {
+      theta = e_div(A.w, dist);
+    }
+    if (I.x == 1 || theta < theta0) {
+      node = I.z;
+      if (I.x == 1) {
+        const int j = __ldg(prv + I.w);
+        if (unshifted && (j == gi_ || j == pi_)) continue;
+        if (dist < NV_EPS) {
+          singular = true;
+          continue;
+        }
+      }
+      const double vect[3] = {e_sub(cs[0], xi[0]), e_sub(cs[1], xi[1]), e_sub(cs[2], xi[2])};
+      const double circ[3] = {B.x, B.y, B.z};
+      const double a = e_mul(dist, dist);
+      const double b = e_mul(2.0, dot3(vect, circ));
+      const double c = dot3(circ, circ);
+      const double D = e_sub(e_mul(e_mul(4.0, a), c), e_mul(b, b));
+      if (D < NV_EPS) continue;
+      double cr[3];
+      cross3(vect, circ, cr);
+      const double den = e_mul(two_pi, D);
+      const double fac = e_sub(e_div(e_add(e_mul(2.0, c), b), e_sqrt(e_add(e_add(a, b), c))), e_div(b, e_sqrt(a)));
+#pragma unroll
+      for (int k = 0; k < 3; ++k) acc[k] = e_add(acc[k], e_mul(e_div(e_mul(cr[k], qc), den), fac));
+      ++evals;
+    } else {
+      node = I.y != kEnd ? I.y : I.z;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(64) k_tree_walk_fp64(const SysConst *__restrict__ scs, SysDyn *dyn,
+                                                       const int2 *__restrict__ work, const double *__restrict__ X,
+                                                       const double *__restrict__ GI, const double *__restrict__ GB,
+                                                       const int *__restrict__ nxt, const int *__restrict__ prv,
+                                                       double *__restrict__ U, long long T, TreeBuffers tb,
+                                                       unsigned *err) {
+  const int2 w = work[blockIdx.x];
+  const SysConst &sc = scs[w.x];
+  const int g = w.y + threadIdx.x;
+  const int k = g - sc.base;
+  unsigned long long evals = 0;
+  if (!*err && k <= dyn[w.x].pcount && k <= sc.cap && nxt[g] != 0) {
+    double xi[3];
+    load3(X, T, g, xi);
+    const int pi_ = prv[g];
+    bool singular = false;
+    double ub0[3] = {0, 0, 0}, ubs[3] = {0, 0, 0};
+    const double zero[3] = {0, 0, 0};
+    walk_fp64(tb, w.x, sc, xi, g, pi_, prv, zero, true, ub0, evals, singular);
+    for (int m = 0; m < sc.n_shift; ++m) walk_fp64(tb, w.x, sc, xi, g, pi_, prv, sc.shift[m], false, ubs, evals, singular);
+    if (singular) atomicOr(err, DERR_SINGULAR);
+    double gi[3], gb[3], u[3], fdot[3];
+    load3(GI, T, g, gi);
+    load3(GB, T, g, gb);
+    local_velocity(sc, xi, gi, gb, u, fdot);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], ub0[c]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], ubs[c]);
+    mf_epilogue(sc, dyn[w.x].t, fdot, u);
+    store3(U, T, g, u);
+  }
+  // tree_eval (tree.f90:308): one atomic per warp
+  unsigned long long tot = evals;
+  for (int o = 16; o > 0; o >>= 1) tot += __shfl_down_sync(0xffffffffu, tot, o);
+  if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&dyn[w.x].tree_eval, tot);
+}
+
+// pclose_tree + closest_tree (tree.f90:190-244): theta = width/dist < .5, no shift, no
+// correction; the candidate is prv(first member's infront at build time) with the links of
+// now (after pinsert).
+__global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn,
+                               const int *__restrict__ sys_of, const double *__restrict__ X,
+                               const int *__restrict__ nxt, const int *__restrict__ prv, int *__restrict__ cl,
+                               double *__restrict__ CD, long long T, TreeBuffers tb, const unsigned *err) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= T || *err) return;
+  const int s = sys_of[g];
+  const SysConst &sc = scs[s];
+  if (!sc.use_tree || (dyn[s].itime % sc.recon_shots) != 0) return;
+  const int k = (int)(g - sc.base);
+  if (k < 1 || k > dyn[s].pcount) return;
+  double cd = 100.;
+  const int ni = nxt[g];
+  if (ni == 0) {
+    CD[g] = cd;
+    return;
+  }
+  const int pi_ = prv[g];
+  int best = cl[g];
+  double xi[3];
+  load3(X, T, (int)g, xi);
+  int node = s;
+  while (node != kEnd) {
+    const double4 A = ldg4(&tb.nA[node]);
+    const int4 I = __ldg(&tb.nI[node]);
+    if (I.x == 0) {
+      node = I.z;
+      continue;
+    }
+    const double dist = e_sqrt(e_add(e_add(e_sq(e_sub(xi[0], A.x)), e_sq(e_sub(xi[1], A.y))), e_sq(e_sub(xi[2], A.z))));
+    const double theta = e_div(A.w, dist);
+    if (I.x == 1 || theta < .5) {
+      if (dist < cd) {
+        const int j = prv[I.w];
+        if (I.x > 1) {
+          best = 0;
+        } else if (j != (int)g && ni != j && pi_ != j) {
+          best = j;
+          cd = dist;
+        }
+      }
+      node = I.z;
+    } else {
+      node = I.y != kEnd ? I.y : I.z;
+    }
+  }
+  cl[g] = best;
+  CD[g] = cd;
+}
+
+int n_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+}  // namespace
+
+void tree_alloc(nv_handle *h) {
+  bool need = false;
+  for (auto &s : h->sc) need = need || s.use_tree || s.sched_tree;
+  if (!need) return;
+  auto *tb = new TreeBuffers();
+  const long long T = h->T;
+  tb->max_nodes = (int)std::min<long long>(3 * T + h->nsys + 1024, (1LL << 31) - 1);
+  tb->max_members = 24 * T + 1024;
+  cudaMalloc(&tb->nA, (size_t)tb->max_nodes * sizeof(double4));
+  cudaMalloc(&tb->nB, (size_t)tb->max_nodes * sizeof(double4));
+  cudaMalloc(&tb->nP, (size_t)tb->max_nodes * sizeof(double4));
+  cudaMalloc(&tb->nI, (size_t)tb->max_nodes * sizeof(int4));
+  cudaMalloc(&tb->nR, (size_t)tb->max_nodes * sizeof(int2));
+  cudaMalloc(&tb->nDepth, (size_t)tb->max_nodes * sizeof(int));
+  cudaMalloc(&tb->nLeaf, (size_t)tb->max_nodes * sizeof(int));
+  cudaMalloc(&tb->members, (size_t)tb->max_members * sizeof(int));
+  cudaMalloc(&tb->ctr, (kMaxLevels + 8) * sizeof(int));
+  cudaMemset(tb->ctr, 0, (kMaxLevels + 8) * sizeof(int));
+  cudaMalloc(&tb->flag, (T + 1) * sizeof(int));
+  cudaMalloc(&tb->pos, (T + 1) * sizeof(int));
+  cub::DeviceScan::ExclusiveSum(nullptr, tb->cub_bytes, tb->flag, tb->pos, (int)(T + 1));
+  cudaMalloc(&tb->cub_tmp, std::max<size_t>(tb->cub_bytes, 16));
+  h->tree = tb;
+}
+
+void tree_free(nv_handle *h) {
+  TreeBuffers *tb = h->tree;
+  if (!tb) return;
+  void *ptrs[] = {tb->nA, tb->nB, tb->nP, tb->nI, tb->nR, tb->nDepth, tb->nLeaf, tb->members, tb->ctr,
+                  tb->flag, tb->pos, tb->cub_tmp};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  delete tb;
+  h->tree = nullptr;
+}
+
+void launch_tree_build(nv_handle *h) {
+  TreeBuffers *tb = h->tree;
+  if (!tb) return;
+  const long long T = h->T;
+  k_live_flags<<<grid_for(T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->nxt, tb->flag, T);
+  size_t bytes = tb->cub_bytes;
+  cub::DeviceScan::ExclusiveSum(tb->cub_tmp, bytes, tb->flag, tb->pos, (int)(T + 1), h->stream);
+  k_scatter_live<<<grid_for(T, TB), TB, 0, h->stream>>>(tb->flag, tb->pos, tb->members, T);
+  k_roots<<<grid_for(h->nsys, 64), 64, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, h->nxt, tb->pos, *tb, T);
+  const int sms = n_sms();
+  for (int L = 0; L < kMaxLevels; ++L) {
+    k_split_block<<<sms, 1024, 0, h->stream>>>(h->x, T, *tb, L, h->d_err);
+    k_split_warp<<<sms * 8, 128, 0, h->stream>>>(h->x, T, *tb, L, h->d_err);
+    k_mark_level<<<1, 32, 0, h->stream>>>(*tb, L);
+  }
+  k_node_sums<<<sms * 4, 128, 0, h->stream>>>(h->d_sc, h->sys_of, h->x, h->gi, h->nxt, T, *tb, h->nsys, h->d_err);
+  tb->built = true;
+}
+
+void launch_tree_walk(nv_handle *h) {
+  TreeBuffers *tb = h->tree;
+  if (!tb || h->n_work_tree == 0) return;
+  k_tree_walk_fp64<<<h->n_work_tree, 64, 0, h->stream>>>(h->d_sc, h->d_dyn, h->d_work_tree, h->x, h->gi, h->gb,
+                                                         h->nxt, h->prv, h->u, h->T, *tb, h->d_err);
+}
+
+void launch_closest_tree(nv_handle *h) {
+  TreeBuffers *tb = h->tree;
+  if (!tb) return;
+  k_closest_tree<<<grid_for(h->T, 128), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->nxt, h->prv,
+                                                              h->closest, h->closestd, h->T, *tb, h->d_err);
+}
+
+// Preorder dump of system `sys`'s tree (host side: download nodes, follow first_child/skip).
+int tree_dump(nv_handle *h, int sys, void *buf, int cap, int *n) {
+  TreeBuffers *tb = h->tree;
+  if (!tb || !tb->built) return set_error(NV_ERR_STATE, "no tree has been built");
+  cudaStreamSynchronize(h->stream);
+  int nn = 0;
+  NV_CUDA(cudaMemcpy(&nn, tb->ctr, sizeof(int), cudaMemcpyDeviceToHost));
+  std::vector<double4> A(nn), B(nn), P(nn);
+  std::vector<int4> I(nn);
+  std::vector<int> D(nn), Lf(nn);
+  NV_CUDA(cudaMemcpy(A.data(), tb->nA, nn * sizeof(double4), cudaMemcpyDeviceToHost));
+  NV_CUDA(cudaMemcpy(B.data(), tb->nB, nn * sizeof(double4), cudaMemcpyDeviceToHost));
+  NV_CUDA(cudaMemcpy(P.data(), tb->nP, nn * sizeof(double4), cudaMemcpyDeviceToHost));
+  NV_CUDA(cudaMemcpy(I.data(), tb->nI, nn * sizeof(int4), cudaMemcpyDeviceToHost));
+  NV_CUDA(cudaMemcpy(D.data(), tb->nDepth, nn * sizeof(int), cudaMemcpyDeviceToHost));
+  NV_CUDA(cudaMemcpy(Lf.data(), tb->nLeaf, nn * sizeof(int), cudaMemcpyDeviceToHost));
+  struct Rec {
+    double pos[3], width, cent[3], circ[3];
+    int32_t pcount, depth, leaf, first_next;
+  };
+  Rec *out = static_cast<Rec *>(buf);
+  const int base = h->base[sys];
+  int m = 0;
+  for (int node = sys; node != kEnd;) {
+    if (out && m < cap) {
+      Rec &r = out[m];
+      r.pos[0] = P[node].x; r.pos[1] = P[node].y; r.pos[2] = P[node].z;
+      r.width = A[node].w;
+      r.cent[0] = A[node].x; r.cent[1] = A[node].y; r.cent[2] = A[node].z;
+      r.circ[0] = B[node].x; r.circ[1] = B[node].y; r.circ[2] = B[node].z;
+      r.pcount = I[node].x;
+      r.depth = D[node];
+      r.leaf = Lf[node] ? Lf[node] - base : 0;
+      r.first_next = I[node].w ? I[node].w - base : 0;
+    }
+    ++m;
+    node = (I[node].x > 1 && I[node].y != kEnd) ? I[node].y : I[node].z;
+  }
+  *n = m;
+  return NV_OK;
+}

@@ -1,0 +1,120 @@
+"""The device octree against the oracle: structure (every node's box, count, centre,
+circulation, leaf and first_next) bit for bit, the tree velocity (<=1e-12 relative, bit for
+bit apart from the local term's log), tree_eval, the closest-point walk, and whole steps."""
+import numpy as np
+import pytest
+
+from helpers import config1_params, rel_err, tangle
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _handle(p, st, extra=1024):
+    from nuvort_b200.api import Handle
+    return Handle(p, [st.pcount + extra], states=[st])
+
+
+@pytest.mark.parametrize("n,seed", [(2048, 1), (32768, 1)])
+def test_tree_structure_bit_exact(n, seed):
+    st = tangle(seed, 0.001, n_points=n)
+    p = config1_params("Tree")
+    h = _handle(p, st)
+    h.stage("ghostp")
+    h.stage("construct_tree")
+    tg = h.tree_dump()
+    o = Oracle(p, st)
+    o.stage("ghostp")
+    o.stage("construct_tree")
+    to = o.tree_dump()
+    assert len(tg) == len(to)
+    for f in ("pos", "width", "cent", "circ", "pcount", "depth", "leaf", "first_next"):
+        assert np.array_equal(tg[f], to[f]), f
+    h.close()
+
+
+def test_tree_with_empty_slots_and_point_on_box_face():
+    st = tangle(3, 0.001, n_points=4096)
+    st.infront[100:140] = 0
+    st.behind[100:140] = 0
+    st.x[100:140] = 0
+    # repair the ring(s) cut by the hole: make the neighbours of the hole close over it
+    for k in range(st.pcount):
+        if st.infront[k] and (100 < st.infront[k] <= 140):
+            st.infront[k] = k + 1
+        if st.behind[k] and (100 < st.behind[k] <= 140):
+            st.behind[k] = k + 1
+    st.x[7, 0] = -0.05  # exactly on the lower face
+    p = config1_params("Tree")
+    h = _handle(p, st)
+    h.stage("ghostp")
+    h.stage("construct_tree")
+    o = Oracle(p, st)
+    o.stage("ghostp")
+    o.stage("construct_tree")
+    tg, to = h.tree_dump(), o.tree_dump()
+    assert len(tg) == len(to)
+    for f in ("pos", "width", "cent", "circ", "pcount", "leaf", "first_next"):
+        assert np.array_equal(tg[f], to[f]), f
+    h.close()
+
+
+@pytest.mark.parametrize("theta,correction", [(0.4, True), (0.5, False), (0.2, True)])
+def test_tree_velocity(theta, correction):
+    st = tangle(1, 0.001, n_points=8192)
+    p = config1_params("Tree", tree_theta=theta, tree_extra_correction=correction)
+    h = _handle(p, st)
+    ug = h.calc_velocity()
+    evg = h.counters().tree_eval
+    o = Oracle(p, st)
+    uo = o.calc_velocity()
+    assert rel_err(ug, uo).max() <= 1e-12
+    assert evg == o.counters().tree_eval
+    h.close()
+
+
+def test_tree_velocity_matches_golden_fixture():
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "config1_tree_small.npz"))
+    st = tangle(1, 0.001, n_points=2048)
+    h = _handle(config1_params("Tree"), st)
+    assert rel_err(h.calc_velocity(), g["u"]).max() <= 1e-12
+    h.close()
+
+
+def test_closest_tree_identical_inputs():
+    st = tangle(31, 0.001, n_points=16384)
+    p = config1_params("Tree")
+    o = Oracle(p, st)
+    o.stage("ghostp")
+    o.stage("construct_tree")
+    o.stage("pmotion")
+    mv = o.download()
+    # the tree is built on the step-start state; pinsert then relinks before the search
+    from nuvort_b200.api import Handle
+    p_ins = config1_params("Tree", delta=0.00098, overide_timestep_check=True)
+    h = Handle(p_ins, [mv.pcount + 4096], states=[mv])
+    h.set_clock(0, 0.0, 1)
+    o2 = Oracle(p_ins, mv, itime=1)
+    for s in ("construct_tree", "pinsert", "pclose"):
+        h.stage(s)
+        o2.stage(s)
+    a, b = h.download(), o2.download()
+    assert np.array_equal(a.closest, b.closest)
+    assert np.array_equal(a.closestd, b.closestd)
+    assert h.events() == o2.events() and len(b.x) > len(mv.x)
+    h.close()
+
+
+def test_whole_steps_tree_config1_small():
+    st = tangle(1, 0.001, n_points=4096)
+    p = config1_params("Tree")
+    h = _handle(p, st)
+    o = Oracle(p, st)
+    h.step(20)
+    o.step(20)
+    assert h.events() == o.events()
+    a, b = h.download(), o.download()
+    assert np.array_equal(a.infront, b.infront)
+    assert np.max(np.abs(a.x - b.x)) < 1e-12
+    h.close()
