@@ -92,8 +92,8 @@ def test_closest_tree_identical_inputs():
     mv = o.download()
     # the tree is built on the step-start state; pinsert then relinks before the search
     from nuvort_b200.api import Handle
-    p_ins = config1_params("Tree", delta=0.00098, overide_timestep_check=True)
-    h = Handle(p_ins, [mv.pcount + 4096], states=[mv])
+    p_ins = config1_params("Tree", delta=0.000999, overide_timestep_check=True)  # ~3000 insertions
+    h = Handle(p_ins, [mv.pcount + 8192], states=[mv])
     h.set_clock(0, 0.0, 1)
     o2 = Oracle(p_ins, mv, itime=1)
     for s in ("construct_tree", "pinsert", "pclose"):
