@@ -121,6 +121,7 @@ typedef struct nv_counters {
   int32_t insert_count;  /* pinsert insertions so far                           */
   int32_t loop_kills;    /* loops cleared by loop_killer                        */
   int64_t tree_eval;     /* accepted tree interactions in the last velocity pass */
+  int64_t tree_tests;    /* opening tests (nodes visited) in the last velocity pass */
   int32_t itime;         /* last completed step                                 */
   int32_t n_events;      /* events logged so far (ring buffer may have dropped) */
   double t;              /* simulation time                                     */
@@ -197,6 +198,17 @@ int nv_tree_dump(nv_handle *h, int32_t sys, nv_tree_node *buf, int32_t cap, int3
 /* Cumulative device time (ms) per stage since creation: ms[0] ghosts, [1] tree build,
  * [2] velocity, [3] AB3 update, [4] topology, [5] whole steps.  n = entries wanted. */
 int nv_stage_times(nv_handle *h, double *ms, int32_t n);
+/* Turn per-step stage timing on (default) or off.  With timing on, nv_step waits for each
+ * step and adds its device time per stage to nv_stage_times; off, steps are queued back to
+ * back. */
+int nv_set_timing(nv_handle *h, int32_t on);
+/* Number of kernel launches one step replays (kernel nodes of the step's CUDA graph,
+ * library scan kernels included).  Captures the graph if needed. */
+int nv_step_launches(nv_handle *h, int32_t *n);
+/* Measure this device's FP64 fused-multiply-add rate (TFLOP/s, 2 flops per FMA) with a
+ * short throughput kernel: the denominator of the FP64 CUDA-core roofline. */
+int nv_measure_fp64_peak(int32_t device, double *tflops);
+
 /* Block until the handle's stream is idle and report any device-side error. */
 int nv_sync(nv_handle *h);
 

@@ -98,6 +98,7 @@ class NvCounters(C.Structure):
         ("insert_count", C.c_int32),
         ("loop_kills", C.c_int32),
         ("tree_eval", C.c_int64),
+        ("tree_tests", C.c_int64),
         ("itime", C.c_int32),
         ("n_events", C.c_int32),
         ("t", C.c_double),

@@ -62,8 +62,10 @@ def lib():
     L.nv_sync.argtypes = [vp]
     L.nv_last_error.restype = C.c_char_p
     L.nv_version.restype = C.c_char_p
-    if hasattr(L, "nv_tree_dump"):
-        L.nv_tree_dump.argtypes = [vp, i32, P(NvTreeNode), i32, P(i32)]
+    L.nv_tree_dump.argtypes = [vp, i32, P(NvTreeNode), i32, P(i32)]
+    L.nv_set_timing.argtypes = [vp, i32]
+    L.nv_step_launches.argtypes = [vp, P(i32)]
+    L.nv_measure_fp64_peak.argtypes = [i32, P(C.c_double)]
     _lib = L
     return L
 
@@ -83,6 +85,13 @@ def read_run_file(path: str, params: Optional[NvParams] = None) -> NvParams:
         _check(lib().nv_params_default(C.byref(p)))
     _check(lib().nv_read_run_file(path.encode(), C.byref(p)))
     return p
+
+
+def measure_fp64_peak(device: int = 0) -> float:
+    """FP64 FMA throughput of the device in TFLOP/s (the FP64 CUDA-core roofline peak)."""
+    v = C.c_double()
+    _check(lib().nv_measure_fp64_peak(int(device), C.byref(v)))
+    return v.value
 
 
 def check_params(p: NvParams):
@@ -175,6 +184,14 @@ class Handle:
         ms = (C.c_double * len(STAGE_TIMES))()
         _check(lib().nv_stage_times(self.h, ms, len(STAGE_TIMES)))
         return dict(zip(STAGE_TIMES, list(ms)))
+
+    def set_timing(self, on: bool):
+        _check(lib().nv_set_timing(self.h, int(bool(on))))
+
+    def step_launches(self) -> int:
+        n = C.c_int32()
+        _check(lib().nv_step_launches(self.h, C.byref(n)))
+        return n.value
 
     def sync(self):
         _check(lib().nv_sync(self.h))

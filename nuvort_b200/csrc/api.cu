@@ -176,19 +176,68 @@ void time_end(nv_handle *h, int st) {
   if (h->timing) cudaEventRecord(h->ev[2 * st + 1], h->stream);
 }
 
-// The body of one time step, src/run.f90:26-64 (diagnostics and output excluded).
+// The body of one time step, src/run.f90:26-64 (diagnostics and output excluded), with
+// stage timing events.
 void enqueue_step(nv_handle *h) {
   launch_begin_step(h);
+  time_begin(h, ST_GHOST);
   launch_ghost(h);
+  time_end(h, ST_GHOST);
+  time_begin(h, ST_TREE);
   if (any_use_tree(h) || h->any_tree) launch_tree_build(h);
+  time_end(h, ST_TREE);
+  time_begin(h, ST_VELOCITY);
   launch_velocity(h);
+  time_end(h, ST_VELOCITY);
+  time_begin(h, ST_AB3);
   launch_ab3(h);
+  time_end(h, ST_AB3);
+  time_begin(h, ST_TOPO);
   launch_pinsert(h);
   launch_pclose(h, false);  // each system checks mod(itime, recon_shots) on the device
   launch_precon(h);
   launch_premove(h);
   launch_wrap(h, 3);
   launch_end_step(h);
+  time_end(h, ST_TOPO);
+}
+
+int capture_step(nv_handle *h) {
+  if (h->graph_valid) return NV_OK;
+  cudaGraph_t graph = nullptr;
+  const bool timing = h->timing;
+  h->timing = true;  // the graph always records the stage events
+  NV_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  enqueue_step(h);
+  h->timing = timing;
+  cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+  if (e != cudaSuccess) return check_cuda(e, "cudaStreamEndCapture");
+  size_t n = 0;
+  cudaGraphGetNodes(graph, nullptr, &n);
+  std::vector<cudaGraphNode_t> nodes(n);
+  cudaGraphGetNodes(graph, nodes.data(), &n);
+  int kernels = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++kernels;
+  }
+  h->step_kernels = kernels;
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  e = cudaGraphInstantiate(&h->graph_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return check_cuda(e, "cudaGraphInstantiate");
+  h->graph_valid = true;
+  return NV_OK;
+}
+
+void accumulate_stage_times(nv_handle *h) {
+  const int st[] = {ST_GHOST, ST_TREE, ST_VELOCITY, ST_AB3, ST_TOPO};
+  for (int s : st) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, h->ev[2 * s], h->ev[2 * s + 1]) == cudaSuccess) h->stage_ms[s] += ms;
+  }
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, h->ev[2 * ST_GHOST], h->ev[2 * ST_TOPO + 1]) == cudaSuccess) h->stage_ms[ST_STEP] += ms;
 }
 
 }  // namespace
@@ -458,6 +507,7 @@ int nv_counters_get(nv_handle *h, int32_t sys, nv_counters *c) {
   c->insert_count = d.insert_count;
   c->loop_kills = d.loop_kills;
   c->tree_eval = (int64_t)d.tree_eval;
+  c->tree_tests = (int64_t)d.tree_tests;
   c->itime = d.itime;
   c->n_events = d.event_seq;
   c->t = d.t;
@@ -567,26 +617,29 @@ int nv_end_step(nv_handle *h) {
 int nv_step(nv_handle *h, int32_t nsteps) {
   if (!h || nsteps < 0) return set_error(NV_ERR_ARG, "nv_step: bad arguments");
   int rc = set_device(h);
-  if (rc) return rc;
-  if (!h->graph_valid) {
-    cudaGraph_t graph = nullptr;
-    NV_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_step(h);
-    cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
-    if (e != cudaSuccess) return check_cuda(e, "cudaStreamEndCapture");
-    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
-    e = cudaGraphInstantiate(&h->graph_exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) return check_cuda(e, "cudaGraphInstantiate");
-    h->graph_valid = true;
+  if (rc || (rc = capture_step(h))) return rc;
+  for (int k = 0; k < nsteps; ++k) {
+    NV_CUDA(cudaGraphLaunch(h->graph_exec, h->stream));
+    if (h->timing) {
+      if ((rc = finish(h))) return rc;
+      accumulate_stage_times(h);
+    }
   }
-  cudaEventRecord(h->ev[2 * ST_STEP], h->stream);
-  for (int k = 0; k < nsteps; ++k) NV_CUDA(cudaGraphLaunch(h->graph_exec, h->stream));
-  cudaEventRecord(h->ev[2 * ST_STEP + 1], h->stream);
-  rc = finish(h);
-  float ms = 0;
-  if (cudaEventElapsedTime(&ms, h->ev[2 * ST_STEP], h->ev[2 * ST_STEP + 1]) == cudaSuccess) h->stage_ms[ST_STEP] += ms;
-  return rc;
+  return finish(h);
+}
+
+int nv_set_timing(nv_handle *h, int32_t on) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  h->timing = on != 0;
+  return NV_OK;
+}
+
+int nv_step_launches(nv_handle *h, int32_t *n) {
+  if (!h || !n) return set_error(NV_ERR_ARG, "nv_step_launches: bad arguments");
+  int rc = set_device(h);
+  if (rc || (rc = capture_step(h))) return rc;
+  *n = h->step_kernels;
+  return NV_OK;
 }
 
 int nv_calc_velocity(nv_handle *h, int32_t sys, double *u3) {

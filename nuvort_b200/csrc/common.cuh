@@ -62,6 +62,7 @@ struct SysDyn {
   double t;
   int recon_count, remove_count, insert_count, loop_kills;
   unsigned long long tree_eval;
+  unsigned long long tree_tests;
   int event_seq;
   int live;
   int old_pcount;

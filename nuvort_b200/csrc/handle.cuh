@@ -51,6 +51,7 @@ struct nv_handle {
   // CUDA graph of one whole step
   cudaGraphExec_t graph_exec = nullptr;
   bool graph_valid = false;
+  int step_kernels = 0;
 
   // stage timing
   bool timing = true;

@@ -90,6 +90,7 @@ __global__ void k_roots(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys,
   tb.nDepth[s] = 0;
   tb.nLeaf[s] = pc == 1 ? sc.base + 1 : 0;
   dyn[s].tree_eval = 0;
+  dyn[s].tree_tests = 0;
 }
 
 // Octant of x in node (corner P, half-width h), or 8 when x lies in no child.
@@ -384,7 +385,8 @@ __global__ void k_node_sums(const SysConst *__restrict__ scs, const int *__restr
 // tree_walk (tree.f90:250-316) for one image; accumulates into acc in preorder.
 __device__ __forceinline__ void walk_fp64(const TreeBuffers &tb, int root, const SysConst &sc, const double xi[3],
                                           int gi_, int pi_, const int *__restrict__ prv, const double s[3], bool unshifted,
-                                          double acc[3], unsigned long long &evals, bool &singular) {
+                                          double acc[3], unsigned long long &evals, unsigned long long &tests,
+                                          bool &singular) {
   const double qc = sc.quant_circ, two_pi = sc.two_pi, theta0 = sc.tree_theta;
   const bool corr = sc.tree_extra_correction;
   int node = root;
@@ -395,6 +397,7 @@ __device__ __forceinline__ void walk_fp64(const TreeBuffers &tb, int root, const
       node = I.z;
       continue;
     }
+    ++tests;
     const double cs[3] = {e_add(A.x, s[0]), e_add(A.y, s[1]), e_add(A.z, s[2])};
     const double dist = e_sqrt(e_add(e_add(e_sq(e_sub(xi[0], cs[0])), e_sq(e_sub(xi[1], cs[1]))), e_sq(e_sub(xi[2], cs[2]))));
     const double4 B = ldg4(&tb.nB[node]);
@@ -445,7 +448,7 @@ __global__ void __launch_bounds__(64) k_tree_walk_fp64(const SysConst *__restric
   const SysConst &sc = scs[w.x];
   const int g = w.y + threadIdx.x;
   const int k = g - sc.base;
-  unsigned long long evals = 0;
+  unsigned long long evals = 0, tests = 0;
   if (!*err && k <= dyn[w.x].pcount && k <= sc.cap && nxt[g] != 0) {
     double xi[3];
     load3(X, T, g, xi);
@@ -453,8 +456,9 @@ __global__ void __launch_bounds__(64) k_tree_walk_fp64(const SysConst *__restric
     bool singular = false;
     double ub0[3] = {0, 0, 0}, ubs[3] = {0, 0, 0};
     const double zero[3] = {0, 0, 0};
-    walk_fp64(tb, w.x, sc, xi, g, pi_, prv, zero, true, ub0, evals, singular);
-    for (int m = 0; m < sc.n_shift; ++m) walk_fp64(tb, w.x, sc, xi, g, pi_, prv, sc.shift[m], false, ubs, evals, singular);
+    walk_fp64(tb, w.x, sc, xi, g, pi_, prv, zero, true, ub0, evals, tests, singular);
+    for (int m = 0; m < sc.n_shift; ++m)
+      walk_fp64(tb, w.x, sc, xi, g, pi_, prv, sc.shift[m], false, ubs, evals, tests, singular);
     if (singular) atomicOr(err, DERR_SINGULAR);
     double gi[3], gb[3], u[3], fdot[3];
     load3(GI, T, g, gi);
@@ -468,9 +472,13 @@ __global__ void __launch_bounds__(64) k_tree_walk_fp64(const SysConst *__restric
     store3(U, T, g, u);
   }
   // tree_eval (tree.f90:308): one atomic per warp
-  unsigned long long tot = evals;
-  for (int o = 16; o > 0; o >>= 1) tot += __shfl_down_sync(0xffffffffu, tot, o);
+  unsigned long long tot = evals, tt = tests;
+  for (int o = 16; o > 0; o >>= 1) {
+    tot += __shfl_down_sync(0xffffffffu, tot, o);
+    tt += __shfl_down_sync(0xffffffffu, tt, o);
+  }
   if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&dyn[w.x].tree_eval, tot);
+  if ((threadIdx.x & 31) == 0 && tt) atomicAdd(&dyn[w.x].tree_tests, tt);
 }
 
 // pclose_tree + closest_tree (tree.f90:190-244): theta = width/dist < .5, no shift, no

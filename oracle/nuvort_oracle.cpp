@@ -31,6 +31,7 @@ const double five_twelths = 5.0 / 12.0;
 const double eps = 2.220446049250313e-16;  // epsilon(0.) for real(8)
 
 thread_local std::string g_err;
+thread_local long long tests_tls = 0;  // opening tests of the calling thread
 
 struct Pt {  // type(qvort), src/cdata.f90:19-29 (pinning fields omitted: periodic/open only)
   double x[3], u[3], u1[3], u2[3], u_mf[3], u_sup[3];
@@ -75,6 +76,7 @@ struct Sys {
   int itime = 0;
   int recon_count = 0, remove_count = 0, insert_count = 0, loop_kills = 0;
   long long tree_eval = 0;
+  long long tree_tests = 0;
   double total_length = 0.0, avg_sep = 0.0;
   std::vector<std::array<double, 3>> shifts;  // periodic_loop_array
   Node *vtree = nullptr;
@@ -231,6 +233,7 @@ struct Sys {
   void tree_walk(int i, const Node *n, const double *shift, double *u, long long &evals,
                  int &singular) const {
     if (n->pcount == 0) return;
+    ++tests_tls;
     const Pt &qi = f[i];
     const double cs[3] = {n->centx + shift[0], n->centy + shift[1], n->centz + shift[2]};
     double dist = std::sqrt(sq(qi.x[0] - cs[0]) + sq(qi.x[1] - cs[1]) + sq(qi.x[2] - cs[2]));
@@ -338,17 +341,23 @@ struct Sys {
 
   // ---- timestep.f90:16-45 pmotion ----------------------------------------------------------
   int pmotion() {
-    long long evals = 0;
+    long long evals = 0, tests = 0;
     int singular = 0;
     const int velocity = p.velocity;
-#pragma omp parallel for schedule(dynamic, 16) reduction(+ : evals) reduction(| : singular)
-    for (int i = 1; i <= pcount; ++i) {
-      if (f[i].infront == 0) continue;
-      double u[3];
-      calc_velocity(u, i, velocity, evals, singular);
-      for (int c = 0; c < 3; ++c) f[i].u[c] = u[c];
+#pragma omp parallel reduction(+ : evals, tests) reduction(| : singular)
+    {
+      tests_tls = 0;
+#pragma omp for schedule(dynamic, 16)
+      for (int i = 1; i <= pcount; ++i) {
+        if (f[i].infront == 0) continue;
+        double u[3];
+        calc_velocity(u, i, velocity, evals, singular);
+        for (int c = 0; c < 3; ++c) f[i].u[c] = u[c];
+      }
+      tests += tests_tls;
     }
     tree_eval += evals;
+    tree_tests += tests;
     if (singular) { singular_error = 1; return NV_ERR_SINGULAR; }
     const double dt = p.dt;
 #pragma omp parallel for schedule(static)
@@ -775,6 +784,7 @@ int or_counters_get(or_handle *h, nv_counters *c) {
   c->insert_count = s.insert_count;
   c->loop_kills = s.loop_kills;
   c->tree_eval = s.tree_eval;
+  c->tree_tests = s.tree_tests;
   c->itime = s.itime;
   c->n_events = (int32_t)s.events.size();
   c->t = s.t;
@@ -797,6 +807,7 @@ int or_construct_tree(or_handle *h) {
 int or_pmotion(or_handle *h) {
   if (h->s.p.velocity == NV_VEL_TREE && !h->s.vtree) return fail(NV_ERR_STATE, "no tree");
   h->s.tree_eval = 0;
+  h->s.tree_tests = 0;
   int rc = h->s.pmotion();
   return rc == NV_OK ? rc : fail(rc, "singularity in BS (tree) velocity field");
 }
@@ -826,6 +837,7 @@ int or_end_step(or_handle *h) {
 int or_step(or_handle *h, int32_t nsteps) {
   for (int k = 0; k < nsteps; ++k) {
     h->s.tree_eval = 0;
+    h->s.tree_tests = 0;
     int rc = h->s.one_step();
     if (rc != NV_OK) return fail(rc, "step failed");
   }
@@ -840,16 +852,22 @@ int or_calc_velocity_targets(or_handle *h, int32_t velocity, const int32_t *targ
     int rc = s.construct_tree();
     if (rc != NV_OK) return fail(rc, "tree deeper than NV_TREE_MAX_DEPTH");
   }
-  long long evals = 0;
+  long long evals = 0, tests = 0;
   int singular = 0;
-#pragma omp parallel for schedule(dynamic, 4) reduction(+ : evals) reduction(| : singular)
-  for (int k = 0; k < n; ++k) {
-    const int i = targets[k];
-    double u[3] = {0.0, 0.0, 0.0};
-    if (i >= 1 && i <= s.pcount && s.f[i].infront != 0) s.calc_velocity(u, i, velocity, evals, singular);
-    for (int c = 0; c < 3; ++c) u3[3 * k + c] = u[c];
+#pragma omp parallel reduction(+ : evals, tests) reduction(| : singular)
+  {
+    tests_tls = 0;
+#pragma omp for schedule(dynamic, 4)
+    for (int k = 0; k < n; ++k) {
+      const int i = targets[k];
+      double u[3] = {0.0, 0.0, 0.0};
+      if (i >= 1 && i <= s.pcount && s.f[i].infront != 0) s.calc_velocity(u, i, velocity, evals, singular);
+      for (int c = 0; c < 3; ++c) u3[3 * k + c] = u[c];
+    }
+    tests += tests_tls;
   }
   s.tree_eval = evals;
+  s.tree_tests = tests;
   if (singular) return fail(NV_ERR_SINGULAR, "singularity in BS (tree) velocity field");
   return NV_OK;
 }

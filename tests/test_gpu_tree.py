@@ -118,3 +118,14 @@ def test_whole_steps_tree_config1_small():
     assert np.array_equal(a.infront, b.infront)
     assert np.max(np.abs(a.x - b.x)) < 1e-12
     h.close()
+
+
+def test_tree_opening_test_count_matches_oracle():
+    st = tangle(1, 0.001, n_points=4096)
+    p = config1_params("Tree")
+    h = _handle(p, st)
+    h.calc_velocity()
+    o = Oracle(p, st)
+    o.calc_velocity()
+    assert h.counters().tree_tests == o.counters().tree_tests
+    h.close()
