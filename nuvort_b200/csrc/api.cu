@@ -141,9 +141,43 @@ int upload_worklist(int2 **dptr, int *n, const std::vector<int2> &w) {
   return NV_OK;
 }
 
+int upload_worklist4(int4 **dptr, int *n, const std::vector<int4> &w) {
+  if (*dptr) cudaFree(*dptr);
+  *dptr = nullptr;
+  *n = (int)w.size();
+  if (w.empty()) return NV_OK;
+  NV_CUDA(cudaMalloc((void **)dptr, w.size() * sizeof(int4)));
+  NV_CUDA(cudaMemcpy(*dptr, w.data(), w.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  return NV_OK;
+}
+
+// (system, image, first slot) items over every image of every system of one kind
+void build_image_worklist(nv_handle *h, int which, int tb, std::vector<int4> &w) {
+  w.clear();
+  for (int s = 0; s < h->nsys; ++s) {
+    const SysConst &sc = h->sc[s];
+    int kind = sc.velocity == NV_VEL_LIA ? 0 : (sc.sched_tree ? 2 : 1);
+    if (kind != which) continue;
+    for (int m = 0; m <= sc.n_shift; ++m)
+      for (int k = 1; k <= h->cap[s]; k += tb) w.push_back(make_int4(s, m, sc.base + k, 0));
+  }
+}
+
 int rebuild_worklists(nv_handle *h) {
   std::vector<int2> w;
   int rc;
+  if (h->precision == NV_PREC_MIXED) {
+    std::vector<int4> w4;
+    build_image_worklist(h, 1, 128, w4);
+    if ((rc = upload_worklist4(&h->d_work_img, &h->n_work_img, w4)) != NV_OK) return rc;
+    build_image_worklist(h, 2, 128, w4);
+    if ((rc = upload_worklist4(&h->d_work_timg, &h->n_work_timg, w4)) != NV_OK) return rc;
+  }
+  for (int s = 0; s < h->nsys; ++s)
+    if (h->sc[s].sched_tree) {
+      h->tree_sys0 = s;
+      break;
+    }
   build_worklist(h, 0, w);
   if ((rc = upload_worklist(&h->d_work_lia, &h->n_work_lia, w)) != NV_OK) return rc;
   h->any_lia = !w.empty();
@@ -169,11 +203,19 @@ bool any_use_tree(nv_handle *h) {
 }
 bool any_needs_tree_walk(nv_handle *h) { return h->any_tree; }
 
+// During stream capture a plain cudaEventRecord only orders streams; the External flag
+// makes it an event-record node of the graph, whose timestamps cudaEventElapsedTime reads.
+void record(nv_handle *h, cudaEvent_t ev) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(h->stream, &cs);
+  if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(ev, h->stream, cudaEventRecordExternal);
+  else cudaEventRecord(ev, h->stream);
+}
 void time_begin(nv_handle *h, int st) {
-  if (h->timing) cudaEventRecord(h->ev[2 * st], h->stream);
+  if (h->timing) record(h, h->ev[2 * st]);
 }
 void time_end(nv_handle *h, int st) {
-  if (h->timing) cudaEventRecord(h->ev[2 * st + 1], h->stream);
+  if (h->timing) record(h, h->ev[2 * st + 1]);
 }
 
 // The body of one time step, src/run.f90:26-64 (diagnostics and output excluded), with
@@ -204,6 +246,7 @@ void enqueue_step(nv_handle *h) {
 
 int capture_step(nv_handle *h) {
   if (h->graph_valid) return NV_OK;
+  NV_CUDA(cudaGetLastError());
   cudaGraph_t graph = nullptr;
   const bool timing = h->timing;
   h->timing = true;  // the graph always records the stage events
@@ -212,32 +255,42 @@ int capture_step(nv_handle *h) {
   h->timing = timing;
   cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
   if (e != cudaSuccess) return check_cuda(e, "cudaStreamEndCapture");
+  NV_CUDA(cudaGetLastError());
   size_t n = 0;
-  cudaGraphGetNodes(graph, nullptr, &n);
+  NV_CUDA(cudaGraphGetNodes(graph, nullptr, &n));
   std::vector<cudaGraphNode_t> nodes(n);
-  cudaGraphGetNodes(graph, nodes.data(), &n);
+  if (n) NV_CUDA(cudaGraphGetNodes(graph, nodes.data(), &n));
   int kernels = 0;
   for (auto nd : nodes) {
     cudaGraphNodeType t;
-    if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++kernels;
+    NV_CUDA(cudaGraphNodeGetType(nd, &t));
+    if (t == cudaGraphNodeTypeKernel) ++kernels;
   }
   h->step_kernels = kernels;
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   e = cudaGraphInstantiate(&h->graph_exec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return check_cuda(e, "cudaGraphInstantiate");
+  NV_CUDA(cudaGetLastError());
   h->graph_valid = true;
   return NV_OK;
 }
 
+// Stage times of the step just replayed (the graph's event-record nodes).  A failed query
+// only drops the timing sample; it is cleared so that it cannot surface as a step error.
 void accumulate_stage_times(nv_handle *h) {
   const int st[] = {ST_GHOST, ST_TREE, ST_VELOCITY, ST_AB3, ST_TOPO};
   for (int s : st) {
     float ms = 0;
-    if (cudaEventElapsedTime(&ms, h->ev[2 * s], h->ev[2 * s + 1]) == cudaSuccess) h->stage_ms[s] += ms;
+    cudaError_t e = cudaEventElapsedTime(&ms, h->ev[2 * s], h->ev[2 * s + 1]);
+    if (e == cudaSuccess) h->stage_ms[s] += ms;
+    else h->timing_error = e;
   }
   float ms = 0;
-  if (cudaEventElapsedTime(&ms, h->ev[2 * ST_GHOST], h->ev[2 * ST_TOPO + 1]) == cudaSuccess) h->stage_ms[ST_STEP] += ms;
+  cudaError_t e = cudaEventElapsedTime(&ms, h->ev[2 * ST_GHOST], h->ev[2 * ST_TOPO + 1]);
+  if (e == cudaSuccess) h->stage_ms[ST_STEP] += ms;
+  else h->timing_error = e;
+  cudaGetLastError();
 }
 
 }  // namespace
@@ -307,6 +360,12 @@ int nv_create(const nv_params *params, int32_t nsys, const int32_t *capacity, in
     if (capacity[s] < 1) return set_error(NV_ERR_ARG, "nv_create: capacity must be >= 1");
     if (params[s].precision != params[0].precision)
       return set_error(NV_ERR_ARG, "nv_create: all systems of a handle share one precision");
+    if (params[0].precision == NV_PREC_MIXED && params[s].velocity == NV_VEL_TREE)
+      for (int q = 0; q < s; ++q)
+        if (params[q].velocity == NV_VEL_TREE &&
+            (params[q].tree_theta != params[s].tree_theta ||
+             params[q].tree_extra_correction != params[s].tree_extra_correction))
+          return set_error(NV_ERR_ARG, "nv_create: mixed-precision tree systems of a handle share tree_theta");
   }
   auto *h = new nv_handle();
   h->device = device;
@@ -342,7 +401,11 @@ int nv_create(const nv_params *params, int32_t nsys, const int32_t *capacity, in
       (rc = dalloc(&h->sys_of, T)) || (rc = dalloc(&h->seg, 2 * T)) || (rc = dalloc(&h->d_err, 1)) ||
       (rc = dalloc(&h->d_event_count, 1)))
     return bail(rc);
-  if (h->precision == NV_PREC_MIXED && (rc = dalloc(&h->seg32, 2 * T))) return bail(rc);
+  if (h->precision == NV_PREC_MIXED) {
+    if ((rc = dalloc(&h->seg32, 3 * T))) return bail(rc);
+    const int nimg = 27;
+    if ((rc = dalloc(&h->partial, (size_t)nimg * 3 * T))) return bail(rc);
+  }
   h->event_cap = (int)std::min<long long>(std::max<long long>(1 << 16, T / 4), 1 << 22);
   if ((rc = dalloc(&h->d_events, h->event_cap))) return bail(rc);
   if (cudaMemcpy(h->d_sc, h->sc.data(), nsys * sizeof(SysConst), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -373,9 +436,9 @@ int nv_destroy(nv_handle *h) {
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   tree_free(h);
   topo_free(h);
-  void *ptrs[] = {h->d_sc, h->d_dyn, h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv,
+  void *ptrs[] = {h->partial, h->d_sc, h->d_dyn, h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv,
                   h->closest, h->sys_of, h->seg, h->seg32, h->d_err, h->d_events, h->d_event_count,
-                  h->d_work_direct, h->d_work_tree, h->d_work_lia};
+                  h->d_work_direct, h->d_work_tree, h->d_work_lia, h->d_work_img, h->d_work_timg};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &e : h->ev)
@@ -678,6 +741,8 @@ int nv_calc_velocity(nv_handle *h, int32_t sys, double *u3) {
 
 int nv_stage_times(nv_handle *h, double *ms, int32_t n) {
   if (!h || !ms) return set_error(NV_ERR_ARG, "nv_stage_times: bad arguments");
+  if (h->timing_error != cudaSuccess)
+    return check_cuda(h->timing_error, "stage timing (cudaEventElapsedTime)");
   for (int k = 0; k < n && k < ST_COUNT; ++k) ms[k] = h->stage_ms[k];
   return NV_OK;
 }

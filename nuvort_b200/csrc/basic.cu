@@ -22,7 +22,8 @@ __global__ void k_begin_step(SysDyn *dyn, int nsys, const unsigned *err) {
 }
 
 // ghostp (boundary.f90:10-19) + get_ghost_p (:26-84); also packs the segment records
-// (x_j, gi_j - x_j, c_j) that the direct sum stages in shared memory.
+// (x_j, gi_j - x_j, c_j) that the direct sums stage in shared memory: FP64 (2 x 32 B)
+// and, for mixed precision, FP32 (3 x 16 B: position hi, position lo, segment).
 __global__ void k_ghost(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn,
                         const int *__restrict__ sys_of, const double *__restrict__ X,
                         const int *__restrict__ nxt, const int *__restrict__ prv,
@@ -37,8 +38,9 @@ __global__ void k_ghost(const SysConst *__restrict__ scs, const SysDyn *__restri
     seg[2 * g] = make_double4(0, 0, 0, 0);
     seg[2 * g + 1] = make_double4(0, 0, 0, 0);
     if (seg32) {
-      seg32[2 * g] = make_float4(0, 0, 0, 0);
-      seg32[2 * g + 1] = make_float4(0, 0, 0, 0);
+      seg32[3 * g] = make_float4(0, 0, 0, 0);
+      seg32[3 * g + 1] = make_float4(0, 0, 0, 0);
+      seg32[3 * g + 2] = make_float4(0, 0, 0, 0);
     }
     return;
   }
@@ -56,9 +58,11 @@ __global__ void k_ghost(const SysConst *__restrict__ scs, const SysDyn *__restri
   const double c = e_add(e_add(e_sq(d[0]), e_sq(d[1])), e_sq(d[2]));
   seg[2 * g] = make_double4(x[0], x[1], x[2], 1.0);
   seg[2 * g + 1] = make_double4(d[0], d[1], d[2], c);
-  if (seg32) {
-    seg32[2 * g] = make_float4((float)x[0], (float)x[1], (float)x[2], 1.0f);
-    seg32[2 * g + 1] = make_float4((float)d[0], (float)d[1], (float)d[2], (float)c);
+  if (seg32) {  // FP32 record: position split hi + lo (x = hi + lo to ~1e-16), segment vector
+    const float h0 = (float)x[0], h1 = (float)x[1], h2 = (float)x[2];
+    seg32[3 * g] = make_float4(h0, h1, h2, 1.0f);
+    seg32[3 * g + 1] = make_float4((float)(x[0] - (double)h0), (float)(x[1] - (double)h1), (float)(x[2] - (double)h2), 0.0f);
+    seg32[3 * g + 2] = make_float4((float)d[0], (float)d[1], (float)d[2], (float)c);
   }
 }
 
@@ -165,6 +169,17 @@ void launch_velocity(nv_handle *h) {
   if (h->any_lia)
     k_velocity_lia<<<h->n_work_lia, h->direct_tb, 0, h->stream>>>(h->d_sc, h->d_dyn, h->d_work_lia, h->x,
                                                                   h->gi, h->gb, h->nxt, h->u, h->T, h->d_err);
+  if (h->precision == NV_PREC_MIXED) {
+    if (h->any_direct) {
+      launch_direct_mixed(h);
+      launch_mixed_combine(h, 1);
+    }
+    if (h->any_tree) {
+      launch_tree_walk_mixed(h);
+      launch_mixed_combine(h, 2);
+    }
+    return;
+  }
   if (h->any_direct) launch_direct(h);
   if (h->any_tree) launch_tree_walk(h);
 }

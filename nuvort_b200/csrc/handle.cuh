@@ -29,7 +29,14 @@ struct nv_handle {
   double *gi = nullptr, *gb = nullptr, *closestd = nullptr;
   int *nxt = nullptr, *prv = nullptr, *closest = nullptr, *sys_of = nullptr;
   double4 *seg = nullptr;   // FP64 segment records, 2 per slot
-  float4 *seg32 = nullptr;  // FP32 segment records, 2 per slot (mixed precision)
+  float4 *seg32 = nullptr;  // FP32 segment records, 3 per slot (mixed precision)
+  double *partial = nullptr; // per-image partial sums [image][component][slot] (mixed precision)
+  int4 *d_work_img = nullptr;  // (system, image, first slot) items of the mixed direct sum
+  int n_work_img = 0;
+  int4 *d_work_timg = nullptr; // same for the mixed tree walk
+  int n_work_timg = 0;
+  double near_factor = 8.0;
+  int tree_sys0 = 0;           // first system that walks the tree (its theta0 builds the mixed nodes)    // near field: pairs closer than near_factor*delta run in FP64
   unsigned *d_err = nullptr;
   DevEvent *d_events = nullptr;
   int *d_event_count = nullptr;
@@ -57,6 +64,7 @@ struct nv_handle {
   bool timing = true;
   cudaEvent_t ev[2 * ST_COUNT] = {};
   double stage_ms[ST_COUNT] = {};
+  cudaError_t timing_error = cudaSuccess;
 
   // host mirrors
   std::vector<SysDyn> h_dyn;
@@ -72,6 +80,10 @@ void launch_end_step(nv_handle *h);
 
 // direct sum (direct.cu)
 void launch_direct(nv_handle *h);
+// mixed precision (mixed.cu)
+void launch_direct_mixed(nv_handle *h);
+void launch_mixed_combine(nv_handle *h, int which);
+void launch_tree_walk_mixed(nv_handle *h);
 // tree (tree.cu)
 void tree_alloc(nv_handle *h);
 void tree_free(nv_handle *h);

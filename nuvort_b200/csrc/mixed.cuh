@@ -1,0 +1,47 @@
+// mixed.cuh -- shared pieces of the mixed-precision non-local sum.
+//
+// Far field in FP32 with the cancellation-free form of the segment formula.  For a
+// segment from A to B = A + d seen from x, with r = A - x and e = r + d = B - x, the
+// reference's term (timestep.f90:162-169)
+//   Gamma/(2 pi) (r x d)/(4ac - b^2) ((2c+b)/sqrt(a+b+c) - b/sqrt(a))
+// (a = |r|^2, b = 2 r.d, c = |d|^2) equals
+//   Gamma/(4 pi) (r x d) (|r| + |e|) / (|r| |e| (|r| |e| + r.e)),
+// which subtracts nothing when the target is far from the segment (r.e ~ +|r||e|), so FP32
+// keeps ~1e-7 relative accuracy where the original form loses digits to 4ac - b^2 and to
+// the bracket.  The near field (leaves or segments closer than near_radius) is evaluated in
+// FP64 with the reference's own expression, so those terms equal the plain path's.
+#pragma once
+
+#include "common.cuh"
+
+struct MixedNodes {  // per tree node, built after the FP64 node sums
+  double4 *C = nullptr;  // cent.xyz, accept threshold t1^2 (dist^2 > t1^2 opens nothing)
+  float4 *Q = nullptr;   // circ.xyz in FP32, unused
+  double2 *G = nullptr;  // geo^2, t0^2 for the dist <= geo branch (theta0 > 2/sqrt(3) only)
+};
+
+__device__ __forceinline__ void seg_term_f32(float rx, float ry, float rz, float dx, float dy, float dz,
+                                             float gq, float &ux, float &uy, float &uz) {
+  const float ex = rx + dx, ey = ry + dy, ez = rz + dz;
+  const float a = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+  const float ee = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+  const float re = fmaf(rx, ex, fmaf(ry, ey, rz * ez));
+  const float r1 = a * rsqrtf(a);
+  const float r2 = ee * rsqrtf(ee);
+  const float p = r1 * r2;
+  const float f = gq * (r1 + r2) * __frcp_rn(p * (p + re));
+  const float cx = fmaf(ry, dz, -rz * dy);
+  const float cy = fmaf(rz, dx, -rx * dz);
+  const float cz = fmaf(rx, dy, -ry * dx);
+  ux = fmaf(f, cx, ux);
+  uy = fmaf(f, cy, uy);
+  uz = fmaf(f, cz, uz);
+}
+
+// Kahan-compensated FP32 accumulation of one tile's partial sum into (s, comp).
+__device__ __forceinline__ void kahan_add(float &s, float &comp, float v) {
+  const float y = v - comp;
+  const float t = s + y;
+  comp = (t - s) - y;
+  s = t;
+}

@@ -21,6 +21,7 @@
 #include <cub/cub.cuh>
 
 #include "handle.cuh"
+#include "mixed.cuh"
 
 constexpr int kMaxLevels = NV_TREE_MAX_DEPTH;
 constexpr int kEnd = -1;
@@ -42,6 +43,7 @@ struct TreeBuffers {
   void *cub_tmp = nullptr;
   size_t cub_bytes = 0;
   bool built = false;
+  MixedNodes mx;
 };
 
 namespace {
@@ -534,6 +536,127 @@ __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *_
   CD[g] = cd;
 }
 
+// Mixed-precision node records: FP64 centre with the squared acceptance distance, FP32
+// circulation.  The opening test of tree_walk (tree.f90:266-278) accepts a node when
+//   dist - geo > 0 and width/(dist - geo) < theta0   <=>  dist > geo + width/theta0, or
+//   dist - geo <= 0 and width/dist < theta0          <=>  geo >= dist > width/theta0,
+// (without the correction: dist > width/theta0); comparing squared distances in FP64 gives
+// the same decisions except at exact ties.  The second branch needs geo > width/theta0,
+// impossible for theta0 <= 2/sqrt(3) (geo <= sqrt(3)/2 width), so it is tested only above.
+__global__ void k_node_prep(TreeBuffers tb, double theta0, int corr) {
+  const int n = tb.ctr[0];
+  for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
+    const double4 A = tb.nA[id], B = tb.nB[id];
+    const double t0 = A.w / theta0;
+    const double t1 = corr ? B.w + t0 : t0;
+    tb.mx.C[id] = make_double4(A.x, A.y, A.z, t1 * t1);
+    tb.mx.Q[id] = make_float4((float)B.x, (float)B.y, (float)B.z, 0.f);
+    tb.mx.G[id] = make_double2(corr ? B.w * B.w : -1.0, t0 * t0);
+  }
+}
+
+// Mixed tree walk: one thread per (target, image).  Opening tests in FP64 (squared), far
+// interactions in FP32, accepted leaves within near_radius in FP64 with the reference
+// expression (so they equal the plain path's terms).  Writes the image's partial sum.
+__global__ void __launch_bounds__(128) k_tree_walk_mixed(const SysConst *__restrict__ scs, SysDyn *dyn,
+                                                         const int4 *__restrict__ work, const double *__restrict__ X,
+                                                         const int *__restrict__ nxt, const int *__restrict__ prv,
+                                                         double *__restrict__ partial, long long T, TreeBuffers tb,
+                                                         double near_factor, unsigned *err) {
+  const int4 w = work[blockIdx.x];
+  const SysConst &sc = scs[w.x];
+  const int m = w.y;
+  const int g = w.z + threadIdx.x;
+  const int k = g - sc.base;
+  unsigned long long evals = 0, tests = 0;
+  if (!*err && k <= dyn[w.x].pcount && k <= sc.cap && nxt[g] != 0) {
+    double xi[3], s[3] = {0, 0, 0};
+    load3(X, T, g, xi);
+    if (m > 0)
+      for (int c = 0; c < 3; ++c) s[c] = sc.shift[m - 1][c];
+    const int pi_ = prv[g];
+    const double nr = near_factor * sc.delta, near2 = nr * nr;
+    const float gq = (float)(sc.quant_circ / (4.0 * NV_PI));
+    const double qc = sc.quant_circ, two_pi = sc.two_pi;
+    const bool second = sc.tree_extra_correction && sc.tree_theta > 1.1547;
+    float fx = 0, fy = 0, fz = 0;
+    double nx = 0, ny = 0, nz = 0;
+    bool singular = false;
+    int node = w.x;
+    while (node != kEnd) {
+      const int cur = node;
+      const double4 C = ldg4(&tb.mx.C[cur]);
+      const int4 I = __ldg(&tb.nI[cur]);
+      if (I.x == 0) {
+        node = I.z;
+        continue;
+      }
+      ++tests;
+      const double cs[3] = {e_add(C.x, s[0]), e_add(C.y, s[1]), e_add(C.z, s[2])};
+      const double r[3] = {e_sub(cs[0], xi[0]), e_sub(cs[1], xi[1]), e_sub(cs[2], xi[2])};
+      const double d2 = e_add(e_add(e_sq(r[0]), e_sq(r[1])), e_sq(r[2]));
+      bool acc = I.x == 1 || d2 > C.w;
+      if (!acc && second) {
+        const double2 G = tb.mx.G[cur];
+        acc = d2 <= G.x && d2 > G.y;
+      }
+      if (!acc) {
+        node = I.y != kEnd ? I.y : I.z;
+        continue;
+      }
+      node = I.z;
+      if (I.x == 1) {
+        const int j = __ldg(prv + I.w);
+        if (m == 0 && (j == g || j == pi_)) continue;
+        if (d2 < near2) {
+          // near leaf: the reference arithmetic (tree.f90:289-307) in FP64
+          const double dist = e_sqrt(d2);
+          if (dist < NV_EPS) {
+            singular = true;
+            continue;
+          }
+          const double4 B = ldg4(&tb.nB[cur]);
+          const double circ[3] = {B.x, B.y, B.z};
+          const double a = e_mul(dist, dist);
+          const double b = e_mul(2.0, dot3(r, circ));
+          const double c = dot3(circ, circ);
+          const double D = e_sub(e_mul(e_mul(4.0, a), c), e_mul(b, b));
+          if (D < NV_EPS) continue;
+          double cr[3];
+          cross3(r, circ, cr);
+          const double den = e_mul(two_pi, D);
+          const double fac = e_sub(e_div(e_add(e_mul(2.0, c), b), e_sqrt(e_add(e_add(a, b), c))), e_div(b, e_sqrt(a)));
+          nx += e_mul(e_div(e_mul(cr[0], qc), den), fac);
+          ny += e_mul(e_div(e_mul(cr[1], qc), den), fac);
+          nz += e_mul(e_div(e_mul(cr[2], qc), den), fac);
+          ++evals;
+          continue;
+        }
+      }
+      const float4 Q = __ldg(&tb.mx.Q[cur]);
+      const float rx = (float)r[0], ry = (float)r[1], rz = (float)r[2];
+      // the reference skips 4ac-b^2 < epsilon (tree.f90:303); 4ac-b^2 = 4|r x circ|^2
+      const float cx = fmaf(ry, Q.z, -rz * Q.y), cy = fmaf(rz, Q.x, -rx * Q.z), cz = fmaf(rx, Q.y, -ry * Q.x);
+      const float D4 = 4.f * fmaf(cx, cx, fmaf(cy, cy, cz * cz));
+      if (D4 < (float)NV_EPS) continue;
+      seg_term_f32(rx, ry, rz, Q.x, Q.y, Q.z, gq, fx, fy, fz);
+      ++evals;
+    }
+    if (singular) atomicOr(err, DERR_SINGULAR);
+    const long long o = (long long)m * 3 * T + g;
+    partial[o] = (double)fx + nx;
+    partial[o + T] = (double)fy + ny;
+    partial[o + 2 * T] = (double)fz + nz;
+  }
+  unsigned long long tot = evals, tt = tests;
+  for (int o = 16; o > 0; o >>= 1) {
+    tot += __shfl_down_sync(0xffffffffu, tot, o);
+    tt += __shfl_down_sync(0xffffffffu, tt, o);
+  }
+  if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&dyn[w.x].tree_eval, tot);
+  if ((threadIdx.x & 31) == 0 && tt) atomicAdd(&dyn[w.x].tree_tests, tt);
+}
+
 int n_sms() {
   static int sms = 0;
   if (!sms) {
@@ -563,6 +686,11 @@ void tree_alloc(nv_handle *h) {
   cudaMalloc(&tb->nDepth, (size_t)tb->max_nodes * sizeof(int));
   cudaMalloc(&tb->nLeaf, (size_t)tb->max_nodes * sizeof(int));
   cudaMalloc(&tb->members, (size_t)tb->max_members * sizeof(int));
+  if (h->precision == NV_PREC_MIXED) {
+    cudaMalloc(&tb->mx.C, (size_t)tb->max_nodes * sizeof(double4));
+    cudaMalloc(&tb->mx.Q, (size_t)tb->max_nodes * sizeof(float4));
+    cudaMalloc(&tb->mx.G, (size_t)tb->max_nodes * sizeof(double2));
+  }
   cudaMalloc(&tb->ctr, (kMaxLevels + 8) * sizeof(int));
   cudaMemset(tb->ctr, 0, (kMaxLevels + 8) * sizeof(int));
   cudaMalloc(&tb->flag, (T + 1) * sizeof(int));
@@ -576,7 +704,7 @@ void tree_free(nv_handle *h) {
   TreeBuffers *tb = h->tree;
   if (!tb) return;
   void *ptrs[] = {tb->nA, tb->nB, tb->nP, tb->nI, tb->nR, tb->nDepth, tb->nLeaf, tb->members, tb->ctr,
-                  tb->flag, tb->pos, tb->cub_tmp};
+                  tb->flag, tb->pos, tb->cub_tmp, tb->mx.C, tb->mx.Q, tb->mx.G};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   delete tb;
@@ -599,6 +727,12 @@ void launch_tree_build(nv_handle *h) {
     k_mark_level<<<1, 32, 0, h->stream>>>(*tb, L);
   }
   k_node_sums<<<sms * 4, 128, 0, h->stream>>>(h->d_sc, h->sys_of, h->x, h->gi, h->nxt, T, *tb, h->nsys, h->d_err);
+  if (h->precision == NV_PREC_MIXED) {
+    // theta0 and the correction flag are per system; a handle's systems share them when
+    // any of them walks the tree (checked at creation)
+    k_node_prep<<<sms * 4, 256, 0, h->stream>>>(*tb, h->sc[h->tree_sys0].tree_theta,
+                                                h->sc[h->tree_sys0].tree_extra_correction);
+  }
   tb->built = true;
 }
 
@@ -607,6 +741,13 @@ void launch_tree_walk(nv_handle *h) {
   if (!tb || h->n_work_tree == 0) return;
   k_tree_walk_fp64<<<h->n_work_tree, 64, 0, h->stream>>>(h->d_sc, h->d_dyn, h->d_work_tree, h->x, h->gi, h->gb,
                                                          h->nxt, h->prv, h->u, h->T, *tb, h->d_err);
+}
+
+void launch_tree_walk_mixed(nv_handle *h) {
+  TreeBuffers *tb = h->tree;
+  if (!tb || h->n_work_timg == 0) return;
+  k_tree_walk_mixed<<<h->n_work_timg, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->d_work_timg, h->x, h->nxt, h->prv,
+                                                           h->partial, h->T, *tb, h->near_factor, h->d_err);
 }
 
 void launch_closest_tree(nv_handle *h) {

@@ -1,0 +1,66 @@
+"""Mixed-precision path (FP32 far field, FP64 near field and epilogue) against the plain
+FP64 path and the FP64 direct-sum oracle.
+
+Tolerance: relative RMS velocity error <= 1e-6 (sqrt(sum|u_mixed - u_ref|^2 / sum|u_ref|^2)),
+the bound the mixed path promises; events over 20 whole steps must equal the plain path's."""
+import numpy as np
+import pytest
+
+from helpers import config0_params, config1_params, rms_rel, tangle
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL_RMS = 1e-6
+
+
+def _vel(p, st, extra=512):
+    from nuvort_b200.api import Handle
+    with Handle(p, [st.pcount + extra], states=[st]) as h:
+        u = h.calc_velocity()
+        c = h.counters()
+    return u, c
+
+
+@pytest.mark.parametrize("n", [2048, 16384])
+def test_mixed_direct_vs_plain_and_oracle(n):
+    st = tangle(1, 0.001, n_points=n)
+    up, _ = _vel(config1_params("BS", precision="fp64"), st)
+    um, _ = _vel(config1_params("BS", precision="mixed"), st)
+    e = rms_rel(um, up)
+    print("mixed direct rms vs plain", e)
+    assert e <= TOL_RMS
+    if n <= 2048:
+        uo = Oracle(config1_params("BS"), st).calc_velocity()
+        assert rms_rel(um, uo) <= TOL_RMS
+
+
+def test_mixed_direct_config0_small_system():
+    st = tangle(0, 0.002, n_rings=8)
+    up, _ = _vel(config0_params(), st)
+    um, _ = _vel(config0_params(precision="mixed"), st)
+    assert rms_rel(um, up) <= TOL_RMS
+
+
+@pytest.mark.parametrize("theta", [0.4, 0.5])
+def test_mixed_tree_vs_plain(theta):
+    st = tangle(1, 0.001, n_points=32768)
+    up, cp = _vel(config1_params("Tree", tree_theta=theta, precision="fp64"), st)
+    um, cm = _vel(config1_params("Tree", tree_theta=theta, precision="mixed"), st)
+    e = rms_rel(um, up)
+    print("mixed tree rms vs plain", e, cp.tree_eval, cm.tree_eval)
+    assert e <= TOL_RMS
+    assert abs(cm.tree_tests - cp.tree_tests) <= 1e-6 * cp.tree_tests + 10
+    assert abs(cm.tree_eval - cp.tree_eval) <= 1e-5 * cp.tree_eval + 10
+
+
+def test_mixed_whole_steps_events_match_plain():
+    from nuvort_b200.api import Handle
+    st = tangle(1, 0.001, n_points=8192)
+    ev = []
+    for prec in ("fp64", "mixed"):
+        with Handle(config1_params("Tree", precision=prec), [st.pcount + 4096], states=[st]) as h:
+            h.step(20)
+            ev.append(h.events())
+    assert len(ev[0]) > 0
+    assert ev[0] == ev[1]
