@@ -198,6 +198,10 @@ int nv_tree_dump(nv_handle *h, int32_t sys, nv_tree_node *buf, int32_t cap, int3
 /* Cumulative device time (ms) per stage since creation: ms[0] ghosts, [1] tree build,
  * [2] velocity, [3] AB3 update, [4] topology, [5] whole steps.  n = entries wanted. */
 int nv_stage_times(nv_handle *h, double *ms, int32_t n);
+/* Mixed precision: interactions closer than factor*delta (leaves of the tree walk, segment
+ * pairs of the direct sum) are evaluated in FP64; the rest in FP32.  Default 8. */
+int nv_set_near_factor(nv_handle *h, double factor);
+
 /* Turn per-step stage timing on (default) or off.  With timing on, nv_step waits for each
  * step and adds its device time per stage to nv_stage_times; off, steps are queued back to
  * back. */

@@ -64,6 +64,7 @@ def lib():
     L.nv_version.restype = C.c_char_p
     L.nv_tree_dump.argtypes = [vp, i32, P(NvTreeNode), i32, P(i32)]
     L.nv_set_timing.argtypes = [vp, i32]
+    L.nv_set_near_factor.argtypes = [vp, C.c_double]
     L.nv_step_launches.argtypes = [vp, P(i32)]
     L.nv_measure_fp64_peak.argtypes = [i32, P(C.c_double)]
     _lib = L
@@ -184,6 +185,9 @@ class Handle:
         ms = (C.c_double * len(STAGE_TIMES))()
         _check(lib().nv_stage_times(self.h, ms, len(STAGE_TIMES)))
         return dict(zip(STAGE_TIMES, list(ms)))
+
+    def set_near_factor(self, factor: float):
+        _check(lib().nv_set_near_factor(self.h, float(factor)))
 
     def set_timing(self, on: bool):
         _check(lib().nv_set_timing(self.h, int(bool(on))))

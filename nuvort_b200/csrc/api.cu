@@ -691,6 +691,13 @@ int nv_step(nv_handle *h, int32_t nsteps) {
   return finish(h);
 }
 
+int nv_set_near_factor(nv_handle *h, double factor) {
+  if (!h || !(factor >= 0)) return set_error(NV_ERR_ARG, "nv_set_near_factor: bad arguments");
+  h->near_factor = factor;
+  h->graph_valid = false;  // the factor is a launch argument of the captured kernels
+  return NV_OK;
+}
+
 int nv_set_timing(nv_handle *h, int32_t on) {
   if (!h) return set_error(NV_ERR_ARG, "null handle");
   h->timing = on != 0;

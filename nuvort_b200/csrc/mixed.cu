@@ -92,42 +92,46 @@ __global__ void __launch_bounds__(kTB) k_direct_mixed(const SysConst *__restrict
     const int j0 = base + 1 + t * TJ;
     const float4 *tl4 = tiles + buf * 3 * TJ;
     if (active) {
-      float ux = 0, uy = 0, uz = 0;
+      // FP32 partial sums over sub-tiles of 32 segments, each added with Kahan compensation
+      for (int q0 = 0; q0 < n; q0 += 32) {
+        const int q1 = min(n, q0 + 32);
+        float ux = 0, uy = 0, uz = 0;
 #pragma unroll 4
-      for (int jj = 0; jj < n; ++jj) {
-        const float4 H = tl4[3 * jj], L = tl4[3 * jj + 1], D = tl4[3 * jj + 2];
-        const int gj = j0 + jj;
-        if (H.w == 0.f || gj == pi_ || (m == 0 && gj == g)) continue;
-        const float rx = (H.x - th[0]) + (L.x - tl[0]);
-        const float ry = (H.y - th[1]) + (L.y - tl[1]);
-        const float rz = (H.z - th[2]) + (L.z - tl[2]);
-        const float a = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-        if (a < near2) {
-          // near field: the reference expression in FP64 (timestep.f90:162-170, 188-196)
-          const double4 A = seg64[2 * (long long)gj], B = seg64[2 * (long long)gj + 1];
-          double r[3];
-          if (m == 0) {
-            r[0] = e_sub(A.x, xi[0]); r[1] = e_sub(A.y, xi[1]); r[2] = e_sub(A.z, xi[2]);
-          } else {
-            r[0] = e_sub(e_add(A.x, s[0]), xi[0]);
-            r[1] = e_sub(e_add(A.y, s[1]), xi[1]);
-            r[2] = e_sub(e_add(A.z, s[2]), xi[2]);
+        for (int jj = q0; jj < q1; ++jj) {
+          const float4 H = tl4[3 * jj], L = tl4[3 * jj + 1], D = tl4[3 * jj + 2];
+          const int gj = j0 + jj;
+          if (H.w == 0.f || gj == pi_ || (m == 0 && gj == g)) continue;
+          const float rx = (H.x - th[0]) + (L.x - tl[0]);
+          const float ry = (H.y - th[1]) + (L.y - tl[1]);
+          const float rz = (H.z - th[2]) + (L.z - tl[2]);
+          const float a = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+          if (a < near2) {
+            // near field: the reference expression in FP64 (timestep.f90:162-170, 188-196)
+            const double4 A = seg64[2 * (long long)gj], B = seg64[2 * (long long)gj + 1];
+            double r[3];
+            if (m == 0) {
+              r[0] = e_sub(A.x, xi[0]); r[1] = e_sub(A.y, xi[1]); r[2] = e_sub(A.z, xi[2]);
+            } else {
+              r[0] = e_sub(e_add(A.x, s[0]), xi[0]);
+              r[1] = e_sub(e_add(A.y, s[1]), xi[1]);
+              r[2] = e_sub(e_add(A.z, s[2]), xi[2]);
+            }
+            const double d[3] = {B.x, B.y, B.z};
+            const double aa = e_add(e_add(e_sq(r[0]), e_sq(r[1])), e_sq(r[2]));
+            double tm[3];
+            if (bs_term_exact(r, d, aa, B.w, qc, two_pi, tm)) {
+              nx += tm[0];
+              ny += tm[1];
+              nz += tm[2];
+            }
+            continue;
           }
-          const double d[3] = {B.x, B.y, B.z};
-          const double aa = e_add(e_add(e_sq(r[0]), e_sq(r[1])), e_sq(r[2]));
-          double tm[3];
-          if (bs_term_exact(r, d, aa, B.w, qc, two_pi, tm)) {
-            nx += tm[0];
-            ny += tm[1];
-            nz += tm[2];
-          }
-          continue;
+          seg_term_f32(rx, ry, rz, D.x, D.y, D.z, gq, ux, uy, uz);
         }
-        seg_term_f32(rx, ry, rz, D.x, D.y, D.z, gq, ux, uy, uz);
+        kahan_add(hx, cx, ux);
+        kahan_add(hy, cy, uy);
+        kahan_add(hz, cz, uz);
       }
-      kahan_add(hx, cx, ux);
-      kahan_add(hy, cy, uy);
-      kahan_add(hz, cz, uz);
     }
     __syncthreads();
     if (t + 2 < nt) {

@@ -16,7 +16,7 @@
 
 struct MixedNodes {  // per tree node, built after the FP64 node sums
   double4 *C = nullptr;  // cent.xyz, accept threshold t1^2 (dist^2 > t1^2 opens nothing)
-  float4 *Q = nullptr;   // circ.xyz in FP32, unused
+  float4 *Q = nullptr;   // circ.xyz in FP32, |circ|^2
   double2 *G = nullptr;  // geo^2, t0^2 for the dist <= geo branch (theta0 > 2/sqrt(3) only)
 };
 

@@ -26,6 +26,9 @@
 constexpr int kMaxLevels = NV_TREE_MAX_DEPTH;
 constexpr int kEnd = -1;
 constexpr int kBigNode = 2048;  // nodes with more members are split by a whole block
+constexpr int kFlush = 16;      // FP32 far-field terms summed before promotion to FP64
+constexpr float kLineGuard = 0.01f;  // (perpendicular distance / nearer end distance)^2 below
+                                     // which a far interaction is evaluated in FP64
 
 struct TreeBuffers {
   int max_nodes = 0;
@@ -550,7 +553,8 @@ __global__ void k_node_prep(TreeBuffers tb, double theta0, int corr) {
     const double t0 = A.w / theta0;
     const double t1 = corr ? B.w + t0 : t0;
     tb.mx.C[id] = make_double4(A.x, A.y, A.z, t1 * t1);
-    tb.mx.Q[id] = make_float4((float)B.x, (float)B.y, (float)B.z, 0.f);
+    const float qx = (float)B.x, qy = (float)B.y, qz = (float)B.z;
+    tb.mx.Q[id] = make_float4(qx, qy, qz, qx * qx + qy * qy + qz * qz);
     tb.mx.G[id] = make_double2(corr ? B.w * B.w : -1.0, t0 * t0);
   }
 }
@@ -579,8 +583,9 @@ __global__ void __launch_bounds__(128) k_tree_walk_mixed(const SysConst *__restr
     const float gq = (float)(sc.quant_circ / (4.0 * NV_PI));
     const double qc = sc.quant_circ, two_pi = sc.two_pi;
     const bool second = sc.tree_extra_correction && sc.tree_theta > 1.1547;
-    float fx = 0, fy = 0, fz = 0;
-    double nx = 0, ny = 0, nz = 0;
+    float fx = 0, fy = 0, fz = 0;  // FP32 partial over at most kFlush far interactions
+    int nfar = 0;
+    double nx = 0, ny = 0, nz = 0;  // FP64: near field plus the flushed FP32 partials
     bool singular = false;
     int node = w.x;
     while (node != kEnd) {
@@ -637,10 +642,48 @@ __global__ void __launch_bounds__(128) k_tree_walk_mixed(const SysConst *__restr
       const float rx = (float)r[0], ry = (float)r[1], rz = (float)r[2];
       // the reference skips 4ac-b^2 < epsilon (tree.f90:303); 4ac-b^2 = 4|r x circ|^2
       const float cx = fmaf(ry, Q.z, -rz * Q.y), cy = fmaf(rz, Q.x, -rx * Q.z), cz = fmaf(rx, Q.y, -ry * Q.x);
-      const float D4 = 4.f * fmaf(cx, cx, fmaf(cy, cy, cz * cz));
-      if (D4 < (float)NV_EPS) continue;
-      seg_term_f32(rx, ry, rz, Q.x, Q.y, Q.z, gq, fx, fy, fz);
+      const float cr2 = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
+      if (4.f * cr2 < (float)NV_EPS) continue;
+      const float ex = rx + Q.x, ey = ry + Q.y, ez = rz + Q.z;
+      const float a = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+      const float ee = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+      const float re = fmaf(rx, ex, fmaf(ry, ey, rz * ez));
+      const float r1 = a * rsqrtf(a), r2 = ee * rsqrtf(ee);
+      const float pp = r1 * r2;
+      if (pp + re < 0.5f * pp || cr2 < kLineGuard * Q.w * fminf(a, ee)) {
+        // the segment subtends more than 120 degrees at the target, or the target lies near its
+        // line (perpendicular distance under 0.1x the nearer end): |r||e| + r.e or r x circ
+        // cancels there and FP32 would lose digits, so use the reference arithmetic
+        const double dist = e_sqrt(d2);
+        const double4 B = ldg4(&tb.nB[cur]);
+        const double circ[3] = {B.x, B.y, B.z};
+        const double a64 = e_mul(dist, dist);
+        const double b = e_mul(2.0, dot3(r, circ));
+        const double c = dot3(circ, circ);
+        const double D = e_sub(e_mul(e_mul(4.0, a64), c), e_mul(b, b));
+        if (D < NV_EPS) continue;
+        double crd[3];
+        cross3(r, circ, crd);
+        const double den = e_mul(two_pi, D);
+        const double fac = e_sub(e_div(e_add(e_mul(2.0, c), b), e_sqrt(e_add(e_add(a64, b), c))), e_div(b, e_sqrt(a64)));
+        nx += e_mul(e_div(e_mul(crd[0], qc), den), fac);
+        ny += e_mul(e_div(e_mul(crd[1], qc), den), fac);
+        nz += e_mul(e_div(e_mul(crd[2], qc), den), fac);
+        ++evals;
+        continue;
+      }
+      const float f = gq * (r1 + r2) * __frcp_rn(pp * (pp + re));
+      fx = fmaf(f, cx, fx);
+      fy = fmaf(f, cy, fy);
+      fz = fmaf(f, cz, fz);
       ++evals;
+      if (++nfar == kFlush) {
+        nx += (double)fx;
+        ny += (double)fy;
+        nz += (double)fz;
+        fx = fy = fz = 0.f;
+        nfar = 0;
+      }
     }
     if (singular) atomicOr(err, DERR_SINGULAR);
     const long long o = (long long)m * 3 * T + g;
