@@ -650,10 +650,11 @@ __global__ void __launch_bounds__(128) k_tree_walk_mixed(const SysConst *__restr
       const float re = fmaf(rx, ex, fmaf(ry, ey, rz * ez));
       const float r1 = a * rsqrtf(a), r2 = ee * rsqrtf(ee);
       const float pp = r1 * r2;
-      if (pp + re < 0.5f * pp || cr2 < kLineGuard * Q.w * fminf(a, ee)) {
-        // the segment subtends more than 120 degrees at the target, or the target lies near its
-        // line (perpendicular distance under 0.1x the nearer end): |r||e| + r.e or r x circ
-        // cancels there and FP32 would lose digits, so use the reference arithmetic
+      if (pp + re < 0.5f * pp || cr2 < kLineGuard * Q.w * fminf(a, ee) || ee < kLineGuard * fmaxf(a, Q.w)) {
+        // the segment subtends more than 120 degrees at the target, the target lies near its
+        // line (perpendicular distance under 0.1x the nearer end) or near its far end
+        // (|e| < 0.1 max(|r|,|circ|)): |r||e| + r.e, r x circ or e = r + circ cancels there
+        // and FP32 would lose digits, so use the reference arithmetic
         const double dist = e_sqrt(d2);
         const double4 B = ldg4(&tb.nB[cur]);
         const double circ[3] = {B.x, B.y, B.z};
