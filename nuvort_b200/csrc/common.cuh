@@ -66,7 +66,7 @@ struct SysDyn {
   int event_seq;
   int live;
   int old_pcount;
-  int pad;
+  int ins_fallback;  // pinsert needs the serial resolver this step
 };
 
 // One logged topology event (system-local numbering is restored on the host).

@@ -18,6 +18,10 @@
 struct TopoBuffers {
   int *flag_a = nullptr, *pos_a = nullptr, *list_a = nullptr;
   int *flag_b = nullptr, *pos_b = nullptr, *list_b = nullptr;
+  int *flag_c = nullptr, *pos_c = nullptr, *list_c = nullptr;
+  int *dec = nullptr;       // per slot: bit0 stale test, bit1 fresh test, bit2 inserts, bit3 case A
+  int *newslot = nullptr;   // per slot: the slot its insertion fills
+  double *xnew = nullptr;   // per slot: new point position [3][T]
   void *cub_tmp = nullptr;
   size_t cub_bytes = 0;
 };
@@ -134,34 +138,6 @@ __device__ __forceinline__ void refresh_ghosts(const SysConst &sc, const State &
 }
 
 // ---- pass 1 kernels: marks ----------------------------------------------------------------
-// pinsert marks: A = live slot whose stale-ghost test |x - ghosti| > delta passes;
-//                B = empty slot (the free-slot list minloc() walks, line.f90:44-47).
-__global__ void k_mark_insert(const SysConst *__restrict__ scs, SysDyn *__restrict__ dyn, const int *__restrict__ sys_of,
-                              const double *__restrict__ X, const double *__restrict__ GI, const int *__restrict__ nxt,
-                              int *fa, int *fb, long long T, const unsigned *err) {
-  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g > T) return;
-  int a = 0, b = 0;
-  if (g < T && !*err) {
-    const int s = sys_of[g];
-    const SysConst &sc = scs[s];
-    const int k = (int)(g - sc.base);
-    if (k >= 1 && k <= dyn[s].pcount) {
-      if (nxt[g] == 0) {
-        b = 1;
-      } else {
-        double x[3], gi[3];
-        load3(X, T, (int)g, x);
-        load3(GI, T, (int)g, gi);
-        a = dist_gen(x, gi) > sc.delta;
-        dyn[s].live = 1;  // any live point (line.f90:25-27); idempotent store
-      }
-    }
-  }
-  fa[g] = a;
-  fb[g] = b;
-}
-
 // precon marks: live slot with delta/2 > closestd > epsilon(1.) (reconnection.f90:185).
 __global__ void k_mark_recon(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn, const int *__restrict__ sys_of,
                              const double *__restrict__ CD, const int *__restrict__ nxt, int *fa, long long T,
@@ -218,9 +194,10 @@ __global__ void k_zero_live(SysDyn *dyn, int nsys) {
 __global__ void k_insert_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S,
                                  const int *__restrict__ pos_a, const int *__restrict__ list_a,
                                  const int *__restrict__ pos_b, const int *__restrict__ list_b, unsigned *err,
-                                 DevEvent *ev, int *ev_count, int ev_cap) {
+                                 DevEvent *ev, int *ev_count, int ev_cap, int only_fallback) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys || *err) return;
+  if (only_fallback && !dyn[s].ins_fallback) return;
   const SysConst &sc = scs[s];
   SysDyn d = dyn[s];
   if (d.live == 0) {
@@ -443,6 +420,224 @@ __global__ void k_pclose_brute(const SysConst *__restrict__ scs, const SysDyn *_
   CD[g] = best;
 }
 
+
+// ---- parallel pinsert ---------------------------------------------------------------------
+// In the serial sweep (line.f90:30-93) slot k is tested against its step-start ghost unless
+// its predecessor p = behind(k) < k inserted earlier in the same sweep: that insertion
+// refreshed k's ghosts from the current positions (line.f90:88-89).  So each live slot has
+// two candidate outcomes, a stale test and a fresh test; when they agree the outcome is
+// known, and only slots where they differ depend on their predecessor's outcome.
+// New points that the sweep reaches later (placed in a free slot above their creator) are
+// tested again by the reference; when any such point would insert, the step falls back to
+// the serial resolver.
+
+// bit0 stale test, bit1 fresh test (ghost of the current infront position); list = either.
+__global__ void k_ins_mark(const SysConst *__restrict__ scs, SysDyn *__restrict__ dyn, const int *__restrict__ sys_of,
+                           const double *__restrict__ X, const double *__restrict__ GI, const int *__restrict__ nxt,
+                           int *fa, int *fb, int *dec, long long T, const unsigned *err) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g > T) return;
+  int a = 0, b = 0, dv = 0;
+  if (g < T && !*err) {
+    const int s = sys_of[g];
+    const SysConst &sc = scs[s];
+    const int k = (int)(g - sc.base);
+    if (k >= 1 && k <= dyn[s].pcount) {
+      if (nxt[g] == 0) {
+        b = 1;
+      } else {
+        double x[3], gi[3], gf[3];
+        load3(X, T, (int)g, x);
+        load3(GI, T, (int)g, gi);
+        load3(X, T, nxt[g], gf);
+        ghost_adjust(sc, x, gf);
+        const int st = dist_gen(x, gi) > sc.delta, fr = dist_gen(x, gf) > sc.delta;
+        dv = st | (fr << 1);
+        a = st | fr;
+        dyn[s].live = 1;
+      }
+    }
+  }
+  fa[g] = a;
+  fb[g] = b;
+  if (g < T) dec[g] = dv;
+}
+
+// Outcomes: known where the two tests agree; otherwise decided in ascending slot order from
+// the predecessor's outcome (one thread per system, touching only the differing slots).
+__global__ void k_ins_decide(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, const int *__restrict__ prv,
+                             const int *__restrict__ pos_a, const int *__restrict__ list_a, int *dec, int *fc,
+                             const unsigned *err) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys || *err) return;
+  const SysConst &sc = scs[s];
+  dyn[s].ins_fallback = 0;
+  const int li = pos_a[sc.base], le = pos_a[sc.base + sc.cap + 1];
+  for (int idx = li; idx < le; ++idx) {
+    const int k = list_a[idx];
+    int dv = dec[k];
+    const int st = dv & 1, fr = (dv >> 1) & 1;
+    const int p = prv[k];
+    const bool caseA = p < k && (dec[p] & 4);
+    const int d = (st == fr) ? st : (caseA ? fr : st);
+    dv |= (d << 2) | (caseA ? 8 : 0);
+    dec[k] = dv;
+    fc[k] = d;
+  }
+}
+
+__global__ void k_zero_flags(int *f, long long n) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g <= n) f[g] = 0;
+}
+
+// New points along chains of consecutive insertions: a chain starts at an inserting slot
+// whose ghosts were not refreshed (case B) and continues to infront(k) while that slot
+// inserts in case A (its ghosts then hold the current infront position and the new point
+// just placed behind it).  One thread per chain head.
+__global__ void k_ins_points(const SysConst *__restrict__ scs, SysDyn *dyn, const int *__restrict__ sys_of, State S,
+                             const int *__restrict__ pos_c, const int *__restrict__ list_c, const int *__restrict__ pos_b,
+                             const int *__restrict__ list_b, const int *__restrict__ dec, int *newslot, double *xnew,
+                             const int *__restrict__ nev_total, unsigned *err) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= *nev_total || *err) return;
+  int k = list_c[e];
+  if (dec[k] & 8) return;  // not a chain head
+  const int s = sys_of[k];
+  const SysConst &sc = scs[s];
+  const int base = sc.base;
+  const int ev0 = pos_c[base], fb0 = pos_b[base], nfree = pos_b[base + sc.cap + 1] - fb0;
+  const int pc = dyn[s].pcount;
+  const long long T = S.T;
+  const int old_last = base + pc;
+  double gbk[3];
+  bool fresh = false;
+  for (;;) {
+    const int rank = pos_c[k] - ev0;
+    const int slot = rank < nfree ? list_b[fb0 + rank] : base + pc + 1 + (rank - nfree);
+    if (slot > base + sc.cap) {
+      atomicOr(err, DERR_CAPACITY);
+      return;
+    }
+    newslot[k] = slot;
+    double x[3], gi[3], gb[3];
+    load3(S.X, T, k, x);
+    const int nx = S.nxt[k];
+    if (fresh) {  // ghosts refreshed by the predecessor's insertion (get_ghost_p, line.f90:89)
+      load3(S.X, T, nx, gi);
+      ghost_adjust(sc, x, gi);
+      for (int c = 0; c < 3; ++c) gb[c] = gbk[c];
+      ghost_adjust(sc, x, gb);
+    } else {
+      load3(S.GI, T, k, gi);
+      load3(S.GB, T, k, gb);
+    }
+    const double disti = dist_gen(x, gi);
+    double fdd[3], xn[3];
+    deriv2(x, gi, gb, fdd);
+    double curv = e_sqrt(dot3(fdd, fdd));
+    const double mid[3] = {e_mul(0.5, e_add(x[0], gi[0])), e_mul(0.5, e_add(x[1], gi[1])), e_mul(0.5, e_add(x[2], gi[2]))};
+    for (int c = 0; c < 3; ++c) xn[c] = mid[c];
+    if (curv > 1E-5) {
+      curv = e_div(1.0, curv);
+      const double disc = e_sub(e_mul(curv, curv), e_mul(0.25, e_mul(disti, disti)));
+      if (disc > 0.) {
+        const double sfac = e_mul(e_sub(e_sqrt(disc), curv), curv);
+        for (int c = 0; c < 3; ++c) xn[c] = e_add(mid[c], e_mul(sfac, fdd[c]));
+      }
+    }
+    for (int c = 0; c < 3; ++c) xnew[c * T + k] = xn[c];
+    // a new point the sweep reaches later is tested again (its ghost: infront of k)
+    if (slot > k && slot <= old_last) {
+      double gn[3];
+      load3(S.X, T, nx, gn);
+      ghost_adjust(sc, xn, gn);
+      if (dist_gen(xn, gn) > sc.delta) dyn[s].ins_fallback = 1;
+    }
+    // continue the chain: infront(k) inserts with ghosts refreshed by this insertion
+    if (nx > k && (dec[nx] & 8)) {
+      for (int c = 0; c < 3; ++c) gbk[c] = xn[c];
+      fresh = true;
+      k = nx;
+      continue;
+    }
+    break;
+  }
+}
+
+// Apply every insertion (links, new point state) and log the events in sweep order.
+__global__ void k_ins_apply(const SysConst *__restrict__ scs, SysDyn *dyn, const int *__restrict__ sys_of, State S,
+                            const int *__restrict__ pos_c, const int *__restrict__ list_c, const int *__restrict__ newslot,
+                            const double *__restrict__ xnew, const int *__restrict__ nev_total, DevEvent *ev,
+                            int *ev_count, int ev_cap, const unsigned *err) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= *nev_total || *err) return;
+  const int k = list_c[e];
+  const int s = sys_of[k];
+  if (dyn[s].ins_fallback) return;
+  const SysConst &sc = scs[s];
+  const long long T = S.T;
+  const int slot = newslot[k];
+  const int nx = S.nxt[k];
+  double ui[3], un[3], xn[3], zero[3] = {0, 0, 0};
+  load3(S.U, T, k, ui);
+  load3(S.U, T, nx, un);
+  for (int c = 0; c < 3; ++c) {
+    un[c] = e_mul(0.5, e_add(ui[c], un[c]));
+    xn[c] = xnew[c * T + k];
+  }
+  store3(S.X, T, slot, xn);
+  store3(S.U, T, slot, un);
+  store3(S.U1, T, slot, zero);
+  store3(S.U2, T, slot, zero);
+  S.cl[slot] = 0;
+  S.CD[slot] = 0;
+  S.prv[slot] = k;
+  S.nxt[slot] = nx;
+  S.prv[nx] = slot;
+  S.nxt[k] = slot;
+  const int rank = pos_c[k] - pos_c[sc.base];
+  const int seq = dyn[s].event_seq + rank;
+  const int at = atomicAdd(ev_count, 1);
+  if (at < ev_cap) ev[at] = DevEvent{s, seq, dyn[s].itime, NV_EV_INSERT, k, slot};
+}
+
+// Ghosts of every slot an insertion touched, from the final links and positions (each
+// touched slot's last refresh in the serial sweep sees exactly this state).
+__global__ void k_ins_ghosts(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn,
+                             const int *__restrict__ sys_of, State S, const int *__restrict__ list_c,
+                             const int *__restrict__ newslot, const int *__restrict__ nev_total, const unsigned *err) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= *nev_total || *err) return;
+  const int k = list_c[e];
+  const int s = sys_of[k];
+  if (dyn[s].ins_fallback) return;
+  const SysConst &sc = scs[s];
+  const int slot = newslot[k];
+  refresh_ghosts(sc, S, k);
+  refresh_ghosts(sc, S, slot);
+  refresh_ghosts(sc, S, S.nxt[slot]);
+}
+
+// Counters: pcount grows by the insertions beyond the free slots.
+__global__ void k_ins_finish(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, const int *__restrict__ pos_c,
+                             const int *__restrict__ pos_b, unsigned *err) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys || *err) return;
+  const SysConst &sc = scs[s];
+  SysDyn &d = dyn[s];
+  if (d.live == 0) {
+    atomicOr(err, DERR_EMPTY);
+    return;
+  }
+  if (d.ins_fallback) return;
+  const int nev = pos_c[sc.base + sc.cap + 1] - pos_c[sc.base];
+  const int nfree = pos_b[sc.base + sc.cap + 1] - pos_b[sc.base];
+  d.event_seq += nev;
+  d.insert_count += nev;
+  if (nev > nfree) d.pcount += nev - nfree;
+}
+
 State make_state(nv_handle *h) {
   return State{h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv, h->closest, h->T};
 }
@@ -467,6 +662,12 @@ void topo_alloc(nv_handle *h) {
   cudaMalloc(&tb->flag_b, n * sizeof(int));
   cudaMalloc(&tb->pos_b, n * sizeof(int));
   cudaMalloc(&tb->list_b, n * sizeof(int));
+  cudaMalloc(&tb->flag_c, n * sizeof(int));
+  cudaMalloc(&tb->pos_c, n * sizeof(int));
+  cudaMalloc(&tb->list_c, n * sizeof(int));
+  cudaMalloc(&tb->dec, n * sizeof(int));
+  cudaMalloc(&tb->newslot, n * sizeof(int));
+  cudaMalloc(&tb->xnew, 3 * n * sizeof(double));
   cub::DeviceScan::ExclusiveSum(nullptr, tb->cub_bytes, tb->flag_a, tb->pos_a, (int)n);
   cudaMalloc(&tb->cub_tmp, std::max<size_t>(tb->cub_bytes, 16));
   h->topo = tb;
@@ -477,6 +678,8 @@ void topo_free(nv_handle *h) {
   if (!tb) return;
   cudaFree(tb->flag_a); cudaFree(tb->pos_a); cudaFree(tb->list_a);
   cudaFree(tb->flag_b); cudaFree(tb->pos_b); cudaFree(tb->list_b);
+  cudaFree(tb->flag_c); cudaFree(tb->pos_c); cudaFree(tb->list_c);
+  cudaFree(tb->dec); cudaFree(tb->newslot); cudaFree(tb->xnew);
   cudaFree(tb->cub_tmp);
   delete tb;
   h->topo = nullptr;
@@ -484,14 +687,31 @@ void topo_free(nv_handle *h) {
 
 void launch_pinsert(nv_handle *h) {
   TopoBuffers *tb = h->topo;
+  const long long T = h->T;
   k_zero_live<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_dyn, h->nsys);
-  k_mark_insert<<<grid_for(h->T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->gi, h->nxt,
-                                                               tb->flag_a, tb->flag_b, h->T, h->d_err);
-  compact(h, tb->flag_a, tb->pos_a, tb->list_a);
-  compact(h, tb->flag_b, tb->pos_b, tb->list_b);
-  k_insert_resolve<<<resolver_grid(h), 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a,
-                                                           tb->list_a, tb->pos_b, tb->list_b, h->d_err, h->d_events,
-                                                           h->d_event_count, h->event_cap);
+  k_ins_mark<<<grid_for(T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->gi, h->nxt,
+                                                         tb->flag_a, tb->flag_b, tb->dec, T, h->d_err);
+  compact(h, tb->flag_a, tb->pos_a, tb->list_a);  // candidates (either test passes)
+  compact(h, tb->flag_b, tb->pos_b, tb->list_b);  // free slots
+  k_zero_flags<<<grid_for(T + 1, TB), TB, 0, h->stream>>>(tb->flag_c, T);
+  k_ins_decide<<<resolver_grid(h), 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, h->prv, tb->pos_a, tb->list_a,
+                                                       tb->dec, tb->flag_c, h->d_err);
+  compact(h, tb->flag_c, tb->pos_c, tb->list_c);  // insertions, in sweep order
+  const State S = make_state(h);
+  // the number of insertions (pos_c[T]) is known only on the device: launch over every
+  // slot, threads beyond the count return at once
+  const int grid = grid_for(T, 128);
+  const int *nev = tb->pos_c + T;
+  k_ins_points<<<grid, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, S, tb->pos_c, tb->list_c, tb->pos_b,
+                                            tb->list_b, tb->dec, tb->newslot, tb->xnew, nev, h->d_err);
+  k_ins_apply<<<grid, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, S, tb->pos_c, tb->list_c, tb->newslot,
+                                           tb->xnew, nev, h->d_events, h->d_event_count, h->event_cap, h->d_err);
+  k_ins_ghosts<<<grid, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, S, tb->list_c, tb->newslot, nev, h->d_err);
+  k_ins_finish<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, tb->pos_c, tb->pos_b,
+                                                              h->d_err);
+  k_insert_resolve<<<resolver_grid(h), 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, S, tb->pos_a, tb->list_a,
+                                                           tb->pos_b, tb->list_b, h->d_err, h->d_events,
+                                                           h->d_event_count, h->event_cap, 1);
 }
 
 void launch_pclose(nv_handle *h, bool only_brute) {

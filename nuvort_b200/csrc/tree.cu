@@ -344,17 +344,43 @@ __global__ void k_mark_level(TreeBuffers tb, int level) {
 // Centre and circulation of every node: sequential sums in ascending slot order
 // (new_tree, tree.f90:124-152; the root's masked mean, tree.f90:50-54), plus the
 // geometric distance of the opening test's correction (tree.f90:267-269).
-__global__ void k_node_sums(const SysConst *__restrict__ scs, const int *__restrict__ sys_of, const double *__restrict__ X,
-                            const double *__restrict__ GI, const int *__restrict__ nxt, long long T, TreeBuffers tb,
-                            int nsys, unsigned *err) {
+constexpr int kSmallNode = 16;  // nodes up to this many members are summed by one thread
+
+__device__ __forceinline__ void finish_node(TreeBuffers &tb, int id, bool root, double cx, double cy, double cz,
+                                            double qx, double qy, double qz, const int *__restrict__ nxt,
+                                            unsigned *err) {
+  const int2 R = tb.nR[id];
+  int4 I = tb.nI[id];
+  const double4 P = tb.nP[id];
+  const double w = tb.nA[id].w;
+  if (R.y != 0) {
+    cx = e_div(cx, (double)R.y);
+    cy = e_div(cy, (double)R.y);
+    cz = e_div(cz, (double)R.y);
+  }
+  const double hw = w / 2.;
+  const double geo = e_sqrt(e_add(e_add(e_sq(e_sub(cx, e_add(P.x, hw))), e_sq(e_sub(cy, e_add(P.y, hw)))),
+                                   e_sq(e_sub(cz, e_add(P.z, hw)))));
+  tb.nA[id] = make_double4(cx, cy, cz, w);
+  tb.nB[id] = make_double4(qx, qy, qz, geo);
+  if (!root) {
+    const int first = R.y > 0 ? tb.members[R.x] : 0;
+    I.w = first ? nxt[first] : 0;
+    tb.nI[id] = I;
+    tb.nLeaf[id] = I.x == 1 ? first : 0;
+    if (tb.nDepth[id] >= kMaxLevels && I.x > 1) atomicOr(err, DERR_TREE_DEPTH);
+  }
+}
+
+// Nodes with at most kSmallNode members (most of them leaves): one thread each.
+__global__ void k_node_sums_small(const double *__restrict__ X, const double *__restrict__ GI,
+                                  const int *__restrict__ nxt, long long T, TreeBuffers tb, int nsys, unsigned *err) {
   const int n = tb.ctr[0];
   for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
     const int2 R = tb.nR[id];
-    int4 I = tb.nI[id];
-    const double4 P = tb.nP[id];
-    const double w = tb.nA[id].w;
-    double cx = 0, cy = 0, cz = 0, qx = 0, qy = 0, qz = 0;
+    if (R.y > kSmallNode) continue;
     const bool root = id < nsys;
+    double cx = 0, cy = 0, cz = 0, qx = 0, qy = 0, qz = 0;
     for (int k = 0; k < R.y; ++k) {
       const int g = tb.members[R.x + k];
       const double x0 = __ldg(X + g), x1 = __ldg(X + T + g), x2 = __ldg(X + 2 * T + g);
@@ -367,23 +393,60 @@ __global__ void k_node_sums(const SysConst *__restrict__ scs, const int *__restr
         qz = e_sub(e_add(qz, __ldg(GI + 2 * T + g)), x2);
       }
     }
-    if (R.y != 0) {
-      cx = e_div(cx, (double)R.y);
-      cy = e_div(cy, (double)R.y);
-      cz = e_div(cz, (double)R.y);
+    finish_node(tb, id, root, cx, cy, cz, qx, qy, qz, nxt, err);
+  }
+}
+
+// Larger nodes: one warp each.  The warp gathers 32 members' coordinates and ghosts into
+// shared memory; lanes 0-2 then add the three centre components and lanes 3-5 the three
+// circulation components, each in ascending member order -- the same sequence of roundings
+// as the reference's loop.  The next chunk's loads are issued before the adds.
+__global__ void __launch_bounds__(128) k_node_sums_big(const double *__restrict__ X, const double *__restrict__ GI,
+                                                       const int *__restrict__ nxt, long long T, TreeBuffers tb,
+                                                       int nsys, unsigned *err) {
+  __shared__ double sm[4][6][32];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int n = tb.ctr[0];
+  double (*buf)[32] = sm[wl];
+  for (int id = warp; id < n; id += nwarps) {
+    const int2 R = tb.nR[id];
+    if (R.y <= kSmallNode) continue;
+    const bool root = id < nsys;
+    double acc = 0;  // lane c < 3: centre c; lane 3 + c: circulation c
+    double v[6];
+    auto gather = [&](int k0) {
+      const int k = k0 + lane;
+      if (k < R.y) {
+        const int g = tb.members[R.x + k];
+        v[0] = __ldg(X + g);
+        v[1] = __ldg(X + T + g);
+        v[2] = __ldg(X + 2 * T + g);
+        v[3] = __ldg(GI + g);
+        v[4] = __ldg(GI + T + g);
+        v[5] = __ldg(GI + 2 * T + g);
+      }
+    };
+    gather(0);
+    for (int k0 = 0; k0 < R.y; k0 += 32) {
+      __syncwarp();
+      if (k0 + lane < R.y)
+#pragma unroll
+        for (int c = 0; c < 6; ++c) buf[c][lane] = v[c];
+      __syncwarp();
+      if (k0 + 32 < R.y) gather(k0 + 32);
+      const int cnt = min(32, R.y - k0);
+      if (lane < 3) {
+        for (int l = 0; l < cnt; ++l) acc = e_add(acc, buf[lane][l]);
+      } else if (lane < 6 && !root) {
+        for (int l = 0; l < cnt; ++l) acc = e_sub(e_add(acc, buf[lane][l]), buf[lane - 3][l]);
+      }
     }
-    const double hw = w / 2.;
-    const double geo = e_sqrt(e_add(e_add(e_sq(e_sub(cx, e_add(P.x, hw))), e_sq(e_sub(cy, e_add(P.y, hw)))),
-                                     e_sq(e_sub(cz, e_add(P.z, hw)))));
-    tb.nA[id] = make_double4(cx, cy, cz, w);
-    tb.nB[id] = make_double4(qx, qy, qz, geo);
-    if (!root) {
-      const int first = R.y > 0 ? tb.members[R.x] : 0;
-      I.w = first ? nxt[first] : 0;
-      tb.nI[id] = I;
-      tb.nLeaf[id] = I.x == 1 ? first : 0;
-      if (tb.nDepth[id] >= kMaxLevels && I.x > 1) atomicOr(err, DERR_TREE_DEPTH);
-    }
+    const double cx = __shfl_sync(0xffffffffu, acc, 0), cy = __shfl_sync(0xffffffffu, acc, 1),
+                 cz = __shfl_sync(0xffffffffu, acc, 2), qx = __shfl_sync(0xffffffffu, acc, 3),
+                 qy = __shfl_sync(0xffffffffu, acc, 4), qz = __shfl_sync(0xffffffffu, acc, 5);
+    if (lane == 0) finish_node(tb, id, root, cx, cy, cz, root ? 0.0 : qx, root ? 0.0 : qy, root ? 0.0 : qz, nxt, err);
   }
 }
 
@@ -770,7 +833,8 @@ void launch_tree_build(nv_handle *h) {
     k_split_warp<<<sms * 8, 128, 0, h->stream>>>(h->x, T, *tb, L, h->d_err);
     k_mark_level<<<1, 32, 0, h->stream>>>(*tb, L);
   }
-  k_node_sums<<<sms * 4, 128, 0, h->stream>>>(h->d_sc, h->sys_of, h->x, h->gi, h->nxt, T, *tb, h->nsys, h->d_err);
+  k_node_sums_big<<<sms * 8, 128, 0, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->nsys, h->d_err);
+  k_node_sums_small<<<sms * 8, 128, 0, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->nsys, h->d_err);
   if (h->precision == NV_PREC_MIXED) {
     // theta0 and the correction flag are per system; a handle's systems share them when
     // any of them walks the tree (checked at creation)

@@ -136,3 +136,19 @@ def test_whole_steps_config0_events_identical():
     assert (ca.recon_count, ca.remove_count, ca.insert_count) == (cb.recon_count, cb.remove_count, cb.insert_count)
     assert ca.t == cb.t and ca.itime == cb.itime == 200
     h.close()
+
+
+def test_pinsert_new_points_revisited_fall_back_to_serial_order():
+    # chords near 0.002 with delta 0.0009: every segment inserts and each new midpoint is
+    # itself longer than delta from its infront.  Emptying the last ring puts free slots
+    # above the inserting points, so the sweep reaches those new points and inserts again.
+    st = tangle(27, 0.002, n_rings=6)
+    start = st.infront[st.pcount - 1]  # first slot of the last ring
+    st.x[start - 1:] = 0
+    st.infront[start - 1:] = 0
+    st.behind[start - 1:] = 0
+    mv = _moved_state(config0_params(), st)
+    p_ins = config0_params(delta=0.0009, overide_timestep_check=True)
+    a, b, ea, eb, ca, cb = _run_stage(p_ins, mv, ["pinsert"], cap_extra=8192)
+    assert ea == eb
+    _assert_same(a, b)
