@@ -213,6 +213,35 @@ int nv_step_launches(nv_handle *h, int32_t *n);
  * short throughput kernel: the denominator of the FP64 CUDA-core roofline. */
 int nv_measure_fp64_peak(int32_t device, double *tflops);
 
+/* ---- velocity pass without library allocations ------------------------------------------
+ * No counterpart in the reference: the Fortran program has no device memory at all.
+ *
+ * nv_calc_velocity_bs_static computes calc_velocity with velocity 'BS' in plain FP64 (the
+ * same kernels and the same results as nv_calc_velocity on a BS system) for ONE system
+ * whose filament state the caller already keeps in device memory, and it allocates
+ * nothing: no cudaMalloc, no cudaFree, no handle.  It is meant for callers that must own
+ * every device allocation themselves -- for example a CUDA Fortran or OpenACC host that
+ * keeps f(:) in its own device arrays or memory pool and budgets that memory, or a time
+ * loop that cannot afford the device-wide synchronisation that cudaMalloc/cudaFree imply.
+ * All scratch (ghosts, segment records, work list, constants, error word) lives in one
+ * static device array sized for NV_STATIC_MAX_SLOTS slots, about 5.6 MB, which every GPU
+ * that loads this library holds until the process exits.
+ *   p        parameters of the system (velocity must be NV_VEL_BS)
+ *   pcount   slots, 1..NV_STATIC_MAX_SLOTS (larger systems: NV_ERR_CAPACITY)
+ *   d_x3     device [3*pcount] positions, point-major as the host arrays above
+ *   d_infront, d_behind   device [pcount] 1-based links, 0 = empty slot
+ *   t        simulation time (mutual friction cut-offs)
+ *   d_u3     device [3*pcount] output velocities (0 for empty slots)
+ *   stream   a cudaStream_t (NULL = the default stream); the call waits for it to finish
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress);
+ * make that first call before any stream capture begins.  Every call uses the same array
+ * and leaves its contents behind; calls whose work overlaps on the GPU (two host threads,
+ * or two streams) race on it and must be serialised by the caller. */
+#define NV_STATIC_MAX_SLOTS 32768
+int nv_calc_velocity_bs_static(const nv_params *p, int32_t pcount, const double *d_x3,
+                               const int32_t *d_infront, const int32_t *d_behind, double t,
+                               double *d_u3, void *stream);
+
 /* Block until the handle's stream is idle and report any device-side error. */
 int nv_sync(nv_handle *h);
 

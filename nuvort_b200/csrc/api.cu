@@ -12,6 +12,8 @@ namespace {
 thread_local std::string g_err;
 }
 
+SysConst sysconst_for(const nv_params &p, int base, int cap);
+
 int set_error(int code, const std::string &msg) {
   g_err = msg;
   return code;
@@ -294,6 +296,9 @@ void accumulate_stage_times(nv_handle *h) {
 }
 
 }  // namespace
+
+// Per-system constants for callers outside this file (the static-scratch entry point).
+SysConst sysconst_for(const nv_params &p, int base, int cap) { return make_sysconst(p, base, cap); }
 
 extern "C" {
 

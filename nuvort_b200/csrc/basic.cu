@@ -198,3 +198,10 @@ void launch_wrap(nv_handle *h, int mode) {
 void launch_end_step(nv_handle *h) {
   k_end_step<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, h->d_err);
 }
+
+// Ghost/segment pass on explicitly given buffers (used by the static-scratch entry point).
+void launch_ghost_raw(cudaStream_t st, const SysConst *sc, const SysDyn *dyn, const int *sys_of, const double *x,
+                      const int *nxt, const int *prv, double *gi, double *gb, double4 *seg, long long T,
+                      unsigned *err) {
+  k_ghost<<<grid_for(T, TB), TB, 0, st>>>(sc, dyn, sys_of, x, nxt, prv, gi, gb, seg, nullptr, T, err);
+}

@@ -153,3 +153,12 @@ void launch_direct(nv_handle *h) {
   k_direct_fp64<kDirectTJ><<<h->n_work_direct, 64, smem, h->stream>>>(
       h->d_sc, h->d_dyn, h->d_work_direct, h->x, h->gi, h->gb, h->nxt, h->prv, h->seg, h->u, h->T, h->d_err);
 }
+
+// Direct sum on explicitly given buffers (used by the static-scratch entry point).
+void launch_direct_raw(cudaStream_t st, const SysConst *sc, const SysDyn *dyn, const int2 *work, int nwork,
+                       const double *x, const double *gi, const double *gb, const int *nxt, const int *prv,
+                       const double4 *seg, double *u, long long T, unsigned *err) {
+  if (nwork == 0) return;
+  const size_t smem = 2 * 2 * kDirectTJ * sizeof(double4);
+  k_direct_fp64<kDirectTJ><<<nwork, 64, smem, st>>>(sc, dyn, work, x, gi, gb, nxt, prv, seg, u, T, err);
+}

@@ -100,6 +100,13 @@ void launch_precon(nv_handle *h);
 void launch_premove(nv_handle *h);
 
 int set_error(int code, const std::string &msg);
+SysConst sysconst_for(const nv_params &p, int base, int cap);
+void launch_ghost_raw(cudaStream_t st, const SysConst *sc, const SysDyn *dyn, const int *sys_of, const double *x,
+                      const int *nxt, const int *prv, double *gi, double *gb, double4 *seg, long long T,
+                      unsigned *err);
+void launch_direct_raw(cudaStream_t st, const SysConst *sc, const SysDyn *dyn, const int2 *work, int nwork,
+                       const double *x, const double *gi, const double *gb, const int *nxt, const int *prv,
+                       const double4 *seg, double *u, long long T, unsigned *err);
 int check_cuda(cudaError_t e, const char *what);
 #define NV_CUDA(call)                                   \
   do {                                                  \
