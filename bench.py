@@ -1,25 +1,33 @@
 """Benchmark of the filament-velocity hot path: point-velocity evaluations per second.
 
-Workload (default): the tree-vs-direct tangle -- random vortex rings, seed 1, delta = 0.001
-cm, exactly 32,768 points in a periodic cube D = 0.1 cm; Barnes-Hut theta = 0.4 with the
-extra correction; mutual friction alpha = 0.1, alpha' = 0.01 against a uniform normal flow
-v_n = (0, 0, 0.5) cm/s; dt = 5e-6 s; insertion, removal and reconnection on.  Synthetic
-seeded input (no dataset).  One step = one whole time step (ghosts, tree build, velocity of
-every point with 27 periodic images, AB3 update, insertion, closest-point search,
-reconnection, removal, periodic wrap) on the device.
+Default workload (--workload tangle32k): random vortex rings, seed 1, delta = 0.001 cm,
+exactly 32,768 points in a periodic cube D = 0.1 cm; Barnes-Hut theta = 0.4 with the extra
+correction; mutual friction alpha = 0.1, alpha' = 0.01 against a uniform normal flow
+v_n = (0, 0, 0.5) cm/s; dt = 5e-6 s; insertion, removal and reconnection on.  Seeded
+synthetic input (no dataset).  Other workloads: rings8 (8 rings, direct sum, FP64 small
+case), ensemble512 (512 independent systems of 500-20,000 points), tangle1m (1,048,576
+points, theta = 0.5), ensemble32 (32 systems of 131k-262k points).
 
-value = sum over timed steps of live points / sum of per-step device time (CUDA events on
-the library's stream), max over ranks.  Between timed steps a 256 MiB buffer is written to
-flush L2 (the workload's state is smaller than L2).
+One step = one whole time step on the device (ghosts, tree build, velocity of every point
+with 27 periodic images, AB3 update, insertion, closest-point search, reconnection, removal,
+periodic wrap), replayed from a CUDA graph.  value = sum over timed steps of live points /
+sum of per-step device time (CUDA events recorded on the library's stream), max over ranks.
+Between timed steps a 256 MiB buffer is written to flush L2.
 
-Arms: --impl ours (default) runs libnuvort_gpu; --impl reference times the CPU oracle -- the
-line-by-line C++ restatement of the reference Fortran (the reference itself cannot be
-compiled here: no Fortran compiler) -- on all host threads, on the same workload.
+The product arm runs the mixed-precision path; the plain FP64 path (the drop-in that
+reproduces the reference arithmetic) is measured beside it on the same initial state, and
+the line reports both, their velocity difference, their error against the FP64 direct sum
+on a seeded subsample of points, and whether their topology event logs agree.
+
+--impl reference times the CPU oracle -- the line-by-line C++ restatement of the reference
+Fortran (the Fortran itself cannot be built here: no Fortran compiler) -- on all host
+threads, on the same workload.
 """
 from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -35,20 +43,86 @@ METRIC = "Biot-Savart point-evals/s on 1 B200: mixed+batched vs FP64 plain at â‰
 UNIT = "point-evals/s"
 
 
-def workload(rank: int, precision: str, velocity: str = "Tree"):
+# ---- workloads -----------------------------------------------------------------------------
+def _p(**kw):
     from nuvort_b200.abi import make_params
+    base = dict(box_size=0.1, corea=1.3e-8)
+    base.update(kw)
+    return make_params(**base)
+
+
+def workload(name: str, rank: int = 0, crossover: int = 3000):
+    """(params per system, states, config dict)."""
     from nuvort_b200.rings import random_rings
-    st = random_rings(1 + rank, 0.001, (0.1, 0.1, 0.1), n_points=32768)
-    p = make_params(dt=5e-6, delta=0.001, box_size=0.1, velocity=velocity, corea=1.3e-8, tree_theta=0.4,
-                    alpha=(0.1, 0.01), normal_velocity="uniform", norm_vel_vec=(0.0, 0.0, 0.5),
-                    precision=precision)
-    cfg = {"workload": "random-ring tangle, 32,768 points, delta=0.001 cm, D=0.1 cm periodic, seed 1+rank",
-           "velocity": velocity, "tree_theta": 0.4, "alpha": [0.1, 0.01], "v_n": [0.0, 0.0, 0.5], "dt": 5e-6,
-           "points": int(st.pcount), "images": 27, "precision": precision,
-           "l2": "256 MiB buffer written between timed steps (state < L2)"}
-    return p, st, cfg
+    L = (0.1, 0.1, 0.1)
+    if name == "rings8":
+        st = random_rings(0 + rank, 0.002, L, n_rings=8)
+        return [_p(dt=2e-5, delta=0.002, velocity="BS", tree_theta=0.0)], [st], {
+            "workload": "8 random rings, seed 0+rank, delta=0.002 cm, direct sum, no normal fluid",
+            "points": int(st.pcount), "dt": 2e-5}
+    if name == "tangle32k":
+        st = random_rings(1 + rank, 0.001, L, n_points=32768)
+        return [_p(dt=5e-6, delta=0.001, velocity="Tree", tree_theta=0.4, alpha=(0.1, 0.01),
+                   normal_velocity="uniform", norm_vel_vec=(0.0, 0.0, 0.5))], [st], {
+            "workload": "random-ring tangle, 32,768 points, delta=0.001 cm, D=0.1 cm periodic, seed 1+rank",
+            "velocity": "Tree", "tree_theta": 0.4, "alpha": [0.1, 0.01], "v_n": [0.0, 0.0, 0.5], "dt": 5e-6,
+            "points": 32768, "images": 27}
+    if name == "tangle1m":
+        st = random_rings(3 + rank, 0.0005, L, n_points=1048576)
+        return [_p(dt=1e-6, delta=0.0005, velocity="Tree", tree_theta=0.5, alpha=(0.1, 0.01),
+                   normal_velocity="xflow", norm_vel_xflow=1.0)], [st], {
+            "workload": "random-ring counterflow tangle, 1,048,576 points, delta=0.0005 cm, seed 3+rank",
+            "velocity": "Tree", "tree_theta": 0.5, "alpha": [0.1, 0.01], "v_n": [1.0, 0.0, 0.0], "dt": 1e-6,
+            "points": 1048576, "images": 27}
+    if name in ("ensemble512", "ensemble32"):
+        big = name == "ensemble32"
+        seed = (4 if big else 2) + 1000 * rank
+        rng = np.random.Generator(np.random.PCG64(seed))
+        nsys = 32 if big else 512
+        if big:
+            counts = rng.uniform(131072, 262144, size=nsys).astype(int)
+        else:
+            counts = np.round(np.exp(rng.uniform(math.log(500), math.log(20000), size=nsys))).astype(int)
+        delta = 0.0005 if big else 0.002
+        params, states = [], []
+        for s in range(nsys):
+            sub = int(rng.integers(0, 2**31 - 1))
+            if big:
+                a = float(rng.uniform(0.05, 0.15))
+                alpha = (a, 0.1 * a)
+                vmag = float(rng.uniform(0.2, 1.0))
+                vec = (vmag, 0.0, 0.0)
+            else:
+                alpha = (float(rng.uniform(0.03, 0.2)), float(rng.uniform(0.0, 0.02)))
+                vmag = float(rng.uniform(0.0, 1.0))
+                ax = rng.standard_normal(3)
+                ax /= np.linalg.norm(ax)
+                vec = tuple(float(v) for v in vmag * ax)
+            n = int(counts[s])
+            vel = "Tree" if (big or n >= crossover) else "BS"
+            theta = 0.5 if big else 0.4
+            params.append(_p(dt=1e-6 if big else 2e-5, delta=delta, velocity=vel, tree_theta=theta, alpha=alpha,
+                             normal_velocity="uniform", norm_vel_vec=vec))
+            states.append(random_rings(sub, delta, L, n_points=n))
+        cfg = {"workload": (f"ensemble of {nsys} independent random-ring systems, points "
+                            + ("U[131072,262144]" if big else "log-uniform [500,20000]") + f", seed {seed}"),
+               "systems": nsys, "points": int(sum(s.pcount for s in states)),
+               "direct_below": None if big else crossover, "tree_theta": 0.5 if big else 0.4,
+               "dt": 1e-6 if big else 2e-5}
+        return params, states, cfg
+    raise ValueError(name)
 
 
+def with_precision(params, precision: str):
+    out = []
+    for p in params:
+        q = type(p).from_buffer_copy(p)
+        q.precision = 1 if precision == "mixed" else 0
+        out.append(q)
+    return out
+
+
+# ---- helpers ---------------------------------------------------------------------------------
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms while active."""
 
@@ -105,16 +179,12 @@ class ClockSampler:
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    return int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
 
 
 def measured_peaks():
-    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
-        with open(path) as f:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             return json.load(f)
     except Exception:
         return {}
@@ -124,18 +194,43 @@ def profile_traffic(kernel: str):
     """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/traffic.json)."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            d = json.load(f)
-        return d.get(kernel)
+            return json.load(f).get(kernel)
     except Exception:
         return None
 
 
-def cpu_baseline_port(params, st, seconds: float = 15.0, max_steps: int = 40):
-    """Time the CPU oracle (whole steps) on all host threads on the same workload."""
+def rms_rel(a, b):
+    return float(np.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2)))
+
+
+def timed_steps(h, steps, flush, torch, sampler=None):
+    """Run `steps` single steps; per-step device time from the library's stage events."""
+    pts = 0
+    evals = tests = 0
+    per_step = []
+    vel = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        pts += sum(h.counters(s).live for s in range(h.nsys))
+        before = h.stage_times()
+        h.step(1)
+        after = h.stage_times()
+        per_step.append(after["step"] - before["step"])
+        vel += after["velocity"] - before["velocity"]
+        for s in range(h.nsys):
+            c = h.counters(s)
+            evals += c.tree_eval
+            tests += c.tree_tests
+    return pts, per_step, vel, evals, tests
+
+
+def cpu_baseline_port(params, states, seconds: float = 15.0, max_steps: int = 40):
+    """The CPU oracle (whole steps, all host threads) on the first system of the workload."""
     import oracle
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
-    o = oracle.Oracle(params, st)
+    o = oracle.Oracle(with_precision(params, "fp64")[0], states[0])
     o.step(1)  # warm-up (first tree build, page-in)
     pts, tot, n = 0, 0.0, 0
     while tot < seconds and n < max_steps:
@@ -146,36 +241,48 @@ def cpu_baseline_port(params, st, seconds: float = 15.0, max_steps: int = 40):
         pts += live
         n += 1
     return {"value": pts / tot, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{n} whole steps of the same 32,768-point workload on the C++ oracle "
-                      f"(OpenMP over points, serial tree build and topology as in the reference), {tot:.1f} s"}
+            "sample": f"{n} whole steps of system 0 of the workload ({states[0].pcount} points) on the C++ oracle "
+                      f"(OpenMP over points; tree build and topology serial as in the reference), {tot:.1f} s"}
 
 
+# ---- arms ------------------------------------------------------------------------------------
 def run_reference(args):
     world, rank, local = dist_setup()
     if rank != 0:
         return 0
-    params, st, cfg = workload(0, "fp64")
+    params, states, cfg = workload(args.workload, 0)
     import oracle
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
-    o = oracle.Oracle(params, st)
+    os_ = [oracle.Oracle(p, s) for p, s in zip(with_precision(params, "fp64"), states)]
+    # bounded sample: the first systems up to the point budget (all of a single tangle)
+    budget = max(states[0].pcount, 40000)
+    use, tot_pts = [], 0
+    for o, s in zip(os_, states):
+        if tot_pts and tot_pts + s.pcount > budget:
+            break
+        use.append(o)
+        tot_pts += s.pcount
     for _ in range(args.warmup):
-        o.step(1)
+        for o in use:
+            o.step(1)
     pts, tot = 0, 0.0
     for _ in range(args.steps):
-        live = o.counters().live
-        t0 = time.perf_counter()
-        o.step(1)
-        tot += time.perf_counter() - t0
-        pts += live
+        for o in use:
+            live = o.counters().live
+            t0 = time.perf_counter()
+            o.step(1)
+            tot += time.perf_counter() - t0
+            pts += live
     value = pts / tot
+    sample = (f"{args.steps} whole steps of {len(use)} of {len(states)} system(s) ({tot_pts} points) on the C++ "
+              "restatement of the reference (the Fortran is not buildable here: no Fortran compiler), "
+              f"{threads} threads")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
             "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{args.steps} whole steps on the C++ restatement of the reference "
-                                       "(reference Fortran not buildable here: no Fortran compiler)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -189,111 +296,139 @@ def run_ours(args):
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
     from nuvort_b200 import api
 
-    precision = args.precision
-    params, st, cfg = workload(rank, precision)
-    h = api.Handle(params, [st.pcount * 2], device=local, states=[st])
+    params, states, cfg = workload(args.workload, rank, crossover=args.crossover)
+    caps = [int(s.pcount * 1.6) + 256 for s in states]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
+    # velocity differences on the initial state (same state for both paths)
+    hm = api.Handle(with_precision(params, args.precision), caps, device=local, states=states)
+    hp = api.Handle(with_precision(params, "fp64"), caps, device=local, states=states) if args.compare else None
+    err = {}
+    if hp is not None:
+        um = [hm.calc_velocity(s) for s in range(len(states))]
+        up = [hp.calc_velocity(s) for s in range(len(states))]
+        err["rms_rel_vs_plain_fp64"] = rms_rel(np.concatenate(um), np.concatenate(up))
+        # FP64 direct-sum yardstick on a seeded subsample of system 0's points
+        rng = np.random.Generator(np.random.PCG64(12345))
+        n0 = states[0].pcount
+        sub = np.sort(rng.choice(np.arange(1, n0 + 1), size=min(args.subsample, n0), replace=False))
+        ud = hp.calc_velocity_direct_at(0, sub)
+        err["rms_rel_vs_direct_fp64"] = {"mixed": rms_rel(um[0][sub - 1], ud), "plain": rms_rel(up[0][sub - 1], ud),
+                                         "subsample": int(len(sub)), "system": 0}
+        for h in (hm, hp):  # fresh state for the timed run
+            for s, st in enumerate(states):
+                h.upload(s, st, t=0.0, itime=0)
+
     for _ in range(args.warmup):
-        h.step(1)
-    launches = h.step_launches()
+        hm.step(1)
+        if hp is not None:
+            hp.step(1)
+    launches = hm.step_launches()
 
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    t_before = h.stage_times()
-    pts = 0
-    evals = tests = 0
-    per_step_ms = []
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            c = h.counters()
-            pts += c.live
-            before = h.stage_times()["step"]
-            h.step(1)
-            per_step_ms.append(h.stage_times()["step"] - before)
-            c2 = h.counters()
-            evals += c2.tree_eval
-            tests += c2.tree_tests
+        pts, per_step, vel_ms, evals, tests = timed_steps(hm, args.steps, flush, torch)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    t_after = h.stage_times()
-    step_ms = t_after["step"] - t_before["step"]
-    vel_ms = t_after["velocity"] - t_before["velocity"]
-    tot_ms = torch.tensor([step_ms, vel_ms], dtype=torch.float64, device="cuda")
-    tot_pts = torch.tensor([float(pts)], dtype=torch.float64, device="cuda")
+    plain = None
+    if hp is not None:
+        ppts, pper, pvel, _, _ = timed_steps(hp, args.steps, flush, torch)
+        ev_m = [hm.events(s) for s in range(len(states))]
+        ev_p = [hp.events(s) for s in range(len(states))]
+        plain = {"value": ppts / (sum(pper) * 1e-3), "ms_per_step": sum(pper) / args.steps,
+                 "velocity_ms_per_step": pvel / args.steps}
+        err["events_match_plain"] = ev_m == ev_p
+        err["events_compared"] = int(sum(len(e) for e in ev_p))
+        err["steps_compared"] = args.warmup + args.steps
+
+    step_ms = sum(per_step)
+    t = torch.tensor([step_ms, vel_ms], dtype=torch.float64, device="cuda")
+    tp = torch.tensor([float(pts)], dtype=torch.float64, device="cuda")
     if dist:
-        dist.all_reduce(tot_ms, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tot_pts, op=dist.ReduceOp.SUM)
-    step_ms, vel_ms = float(tot_ms[0]), float(tot_ms[1])
-    all_pts = float(tot_pts[0])
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tp, op=dist.ReduceOp.SUM)
+    step_ms, vel_ms, all_pts = float(t[0]), float(t[1]), float(tp[0])
     value = all_pts / (step_ms * 1e-3)
 
     # end to end through the C ABI with host buffers: upload f(:), one step, download f(:)
     e2e = None
     if not args.no_e2e:
-        host = h.download()
-        nbytes_state = lambda s: sum(a.nbytes for a in (s.x, s.u, s.u1, s.u2, s.infront, s.behind) if a is not None)
-        h2d = d2h = 0
-        e_pts = 0
+        hosts = [hm.download(s) for s in range(len(states))]
+        nb = lambda s: sum(a.nbytes for a in (s.x, s.u, s.u1, s.u2, s.infront, s.behind) if a is not None)
+        h2d = d2h = e_pts = 0
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            hs = api.State(x=host.x, infront=host.infront, behind=host.behind, u=host.u, u1=host.u1, u2=host.u2)
-            h.upload(0, hs)
-            h2d += nbytes_state(hs)
-            e_pts += int(np.count_nonzero(host.infront))
-            h.step(1)
-            host = h.download()
-            d2h += nbytes_state(host)
+            for s, host in enumerate(hosts):
+                hs = api.State(x=host.x, infront=host.infront, behind=host.behind, u=host.u, u1=host.u1, u2=host.u2)
+                hm.upload(s, hs)
+                h2d += nb(hs)
+                e_pts += int(np.count_nonzero(host.infront))
+            hm.step(1)
+            hosts = [hm.download(s) for s in range(len(states))]
+            d2h += sum(nb(x) for x in hosts)
         e2e_s = time.perf_counter() - t0
-        e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        e2e_p = torch.tensor([float(e_pts)], dtype=torch.float64, device="cuda")
+        te = torch.tensor([e2e_s, float(e_pts)], dtype=torch.float64, device="cuda")
         if dist:
-            dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-            dist.all_reduce(e2e_p, op=dist.ReduceOp.SUM)
-        e2e = {"value": float(e2e_p[0]) / float(e2e_t[0]), "unit": UNIT,
+            m = te[:1].clone()
+            dist.all_reduce(m, op=dist.ReduceOp.MAX)
+            p_ = te[1:].clone()
+            dist.all_reduce(p_, op=dist.ReduceOp.SUM)
+            te = torch.cat([m, p_])
+        e2e = {"value": float(te[1]) / float(te[0]), "unit": UNIT,
                "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
                "path": "nv_upload (host f(:) -> device) + nv_step(1) + nv_download (device -> host) per step"}
 
     out = None
     if rank == 0:
-        fp64_peak = api.measure_fp64_peak(local)
-        # dominant kernel: the tree walk; algorithmic flops = 43 per accepted interaction + 12 per
-        # opening test (counted on the device), per launch (one launch per step)
-        flops = (43.0 * evals + 12.0 * tests) / args.steps
-        vel_launch_s = vel_ms / args.steps * 1e-3
-        achieved = flops / vel_launch_s / 1e12
-        roof = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                "frac": achieved / fp64_peak if fp64_peak else None,
-                "traffic": profile_traffic("k_tree_walk_fp64"),
-                "kernel": "k_tree_walk_fp64",
-                "peak_source": "FP64 FMA rate measured on this GPU by nv_measure_fp64_peak (MEASURED_PEAKS.json "
-                               "covers HBM and bf16 tensor only)",
-                "per_launch": {"interactions": evals / args.steps, "opening_tests": tests / args.steps,
-                               "ms": vel_ms / args.steps}}
+        mixed = args.precision == "mixed"
+        from nuvort_b200.abi import NV_VEL_BS
+        # direct-sum systems: 27 N^2 pair-images each (N = live points at the start)
+        pairs = sum(27.0 * float(st.pcount) ** 2 for p, st in zip(params, states) if p.velocity == NV_VEL_BS)
+        tree = evals / args.steps >= pairs
+        kernel = ("k_tree_walk_mixed" if mixed else "k_tree_walk_fp64") if tree else (
+            "k_direct_mixed" if mixed else "k_direct_fp64")
+        peak = api.measure_fp32_peak(local) if mixed else api.measure_fp64_peak(local)
+        flops = (43.0 * evals + 12.0 * tests) / args.steps + 43.0 * pairs
+        per_launch = {"interactions": evals / args.steps, "opening_tests": tests / args.steps,
+                      "direct_pair_images": pairs}
+        achieved = flops / (vel_ms / args.steps * 1e-3) / 1e12
+        per_launch["ms"] = vel_ms / args.steps
+        roof = {"bound": "fp32" if mixed else "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak if peak else None, "traffic": profile_traffic(kernel), "kernel": kernel,
+                "peak_source": ("FP32" if mixed else "FP64") + " FMA rate measured on this GPU by nv_measure_fp"
+                               + ("32" if mixed else "64") + "_peak (MEASURED_PEAKS.json covers HBM and bf16 tensor "
+                               "only); algorithmic flops = 43 per interaction + 12 per opening test",
+                "per_launch": per_launch}
         peaks = measured_peaks()
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": step_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == "fp64" else "f32+f64",
-                "data": "synthetic", "config": cfg, "impl": "ours",
-                "velocity_stage": {"ms_per_step": vel_ms / args.steps,
-                                   "point_evals_per_s": all_pts / (vel_ms * 1e-3)},
-                "roofline": roof, "hbm_peak_gbs": peaks.get("hbm_gbs"),
-                "clocks": clk.summary(), "gpu_launches": launches * args.steps,
-                "per_step_ms": [round(x, 4) for x in per_step_ms]}
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
+                "config": dict(cfg, precision=args.precision,
+                               l2="256 MiB buffer written between timed steps"),
+                "impl": "ours",
+                "velocity_stage": {"ms_per_step": vel_ms / args.steps, "point_evals_per_s": all_pts / (vel_ms * 1e-3)},
+                "roofline": roof, "hbm_peak_gbs": peaks.get("hbm_gbs"), "clocks": clk.summary(),
+                "gpu_launches": launches * args.steps, "per_step_ms": [round(x, 4) for x in per_step]}
+        if plain:
+            line["plain_fp64"] = plain
+            line["speedup_vs_plain"] = value / plain["value"]
+        if err:
+            line["error"] = err
         if e2e:
             line["e2e"] = e2e
         if world == 1 and not args.no_cpu:
-            line["cpu_baseline"] = cpu_baseline_port(params, st, seconds=args.cpu_seconds)
+            line["cpu_baseline"] = cpu_baseline_port(params, states, seconds=args.cpu_seconds)
         out = line
-    h.close()
+    hm.close()
+    if hp is not None:
+        hp.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -308,13 +443,17 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--workload", choices=["rings8", "tangle32k", "ensemble512", "tangle1m", "ensemble32"],
+                    default="tangle32k")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--crossover", type=int, default=3000, help="ensembles: direct sum below this many points")
+    ap.add_argument("--subsample", type=int, default=4096)
+    ap.add_argument("--no-compare", dest="compare", action="store_false", help="skip the plain FP64 arm")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     args = ap.parse_args()
-    if args.warmup < 3:
-        args.warmup = 3
+    args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

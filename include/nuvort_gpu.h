@@ -195,6 +195,13 @@ int nv_calc_velocity(nv_handle *h, int32_t sys, double *u3);
  * beyond cap are not written).  Replaces reading vtree (src/tree.f90:34). */
 int nv_tree_dump(nv_handle *h, int32_t sys, nv_tree_node *buf, int32_t cap, int32_t *n);
 
+/* The reference's direct Biot-Savart velocity (calc_velocity with velocity 'BS',
+ * src/timestep.f90:74-98 and :123-140, plain FP64) at n listed slots of system sys,
+ * whatever scheme the system itself uses: the FP64 direct-sum yardstick for tree and
+ * mixed-precision errors on large systems.  u3 receives [3*n] velocities in list order. */
+int nv_calc_velocity_direct_at(nv_handle *h, int32_t sys, const int32_t *targets, int32_t n,
+                               double *u3);
+
 /* Cumulative device time (ms) per stage since creation: ms[0] ghosts, [1] tree build,
  * [2] velocity, [3] AB3 update, [4] topology, [5] whole steps.  n = entries wanted. */
 int nv_stage_times(nv_handle *h, double *ms, int32_t n);
@@ -212,6 +219,8 @@ int nv_step_launches(nv_handle *h, int32_t *n);
 /* Measure this device's FP64 fused-multiply-add rate (TFLOP/s, 2 flops per FMA) with a
  * short throughput kernel: the denominator of the FP64 CUDA-core roofline. */
 int nv_measure_fp64_peak(int32_t device, double *tflops);
+/* The same for FP32 FMAs (the far-field arithmetic of the mixed-precision path). */
+int nv_measure_fp32_peak(int32_t device, double *tflops);
 
 /* ---- velocity pass without library allocations ------------------------------------------
  * No counterpart in the reference: the Fortran program has no device memory at all.

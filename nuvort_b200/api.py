@@ -67,6 +67,8 @@ def lib():
     L.nv_set_near_factor.argtypes = [vp, C.c_double]
     L.nv_step_launches.argtypes = [vp, P(i32)]
     L.nv_measure_fp64_peak.argtypes = [i32, P(C.c_double)]
+    L.nv_measure_fp32_peak.argtypes = [i32, P(C.c_double)]
+    L.nv_calc_velocity_direct_at.argtypes = [vp, i32, P(i32), i32, P(C.c_double)]
     _lib = L
     return L
 
@@ -92,6 +94,13 @@ def measure_fp64_peak(device: int = 0) -> float:
     """FP64 FMA throughput of the device in TFLOP/s (the FP64 CUDA-core roofline peak)."""
     v = C.c_double()
     _check(lib().nv_measure_fp64_peak(int(device), C.byref(v)))
+    return v.value
+
+
+def measure_fp32_peak(device: int = 0) -> float:
+    """FP32 FMA throughput of the device in TFLOP/s."""
+    v = C.c_double()
+    _check(lib().nv_measure_fp32_peak(int(device), C.byref(v)))
     return v.value
 
 
@@ -180,6 +189,14 @@ class Handle:
         u = np.zeros((self.capacity[sys], 3), np.float64)
         _check(lib().nv_calc_velocity(self.h, int(sys), u.ctypes.data_as(C.POINTER(C.c_double))))
         return u[: self.counters(sys).pcount].copy()
+
+    def calc_velocity_direct_at(self, sys: int, targets) -> np.ndarray:
+        """FP64 direct-sum (BS) velocity at the listed 1-based slots of system sys."""
+        tg = np.ascontiguousarray(np.asarray(targets, dtype=np.int32))
+        u = np.zeros((tg.shape[0], 3), np.float64)
+        _check(lib().nv_calc_velocity_direct_at(self.h, int(sys), tg.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                tg.shape[0], u.ctypes.data_as(C.POINTER(C.c_double))))
+        return u
 
     def stage_times(self) -> dict:
         ms = (C.c_double * len(STAGE_TIMES))()

@@ -751,6 +751,35 @@ int nv_calc_velocity(nv_handle *h, int32_t sys, double *u3) {
   return NV_OK;
 }
 
+int nv_calc_velocity_direct_at(nv_handle *h, int32_t sys, const int32_t *targets, int32_t n, double *u3) {
+  if (!h || !targets || !u3 || sys < 0 || sys >= h->nsys || n < 0)
+    return set_error(NV_ERR_ARG, "nv_calc_velocity_direct_at: bad arguments");
+  int rc = set_device(h);
+  if (rc || (rc = pull_dyn(h))) return rc;
+  std::vector<int> g(n);
+  for (int k = 0; k < n; ++k) {
+    if (targets[k] < 1 || targets[k] > h->h_dyn[sys].pcount)
+      return set_error(NV_ERR_ARG, "nv_calc_velocity_direct_at: target slot out of range");
+    g[k] = h->base[sys] + targets[k];
+  }
+  int *dt = nullptr;
+  double *du = nullptr;
+  NV_CUDA(cudaMalloc(&dt, std::max(n, 1) * sizeof(int)));
+  NV_CUDA(cudaMalloc(&du, std::max(n, 1) * 3 * sizeof(double)));
+  cudaMemcpy(dt, g.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemset(du, 0, std::max(n, 1) * 3 * sizeof(double));
+  launch_ghost(h);
+  launch_direct_targets(h, sys, dt, n, du);
+  rc = finish(h);
+  if (rc == NV_OK) {
+    cudaError_t e = cudaMemcpy(u3, du, n * 3 * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = check_cuda(e, "nv_calc_velocity_direct_at copy");
+  }
+  cudaFree(dt);
+  cudaFree(du);
+  return rc;
+}
+
 int nv_stage_times(nv_handle *h, double *ms, int32_t n) {
   if (!h || !ms) return set_error(NV_ERR_ARG, "nv_stage_times: bad arguments");
   if (h->timing_error != cudaSuccess)

@@ -9,6 +9,8 @@
 // reference arithmetic except for the ulp-level difference of the device log() in the
 // local term.  The image loop is outside the tile loop for that reason: each image
 // re-streams the tiles (from L2; the kernel is FP64-pipe bound, not memory bound).
+#include <vector>
+
 #include "handle.cuh"
 #include "tma.cuh"
 
@@ -21,7 +23,8 @@ __global__ void __launch_bounds__(64) k_direct_fp64(
     const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn, const int2 *__restrict__ work,
     const double *__restrict__ X, const double *__restrict__ GI, const double *__restrict__ GB,
     const int *__restrict__ nxt, const int *__restrict__ prv, const double4 *__restrict__ seg,
-    double *__restrict__ U, long long T, unsigned *err) {
+    double *__restrict__ U, long long T, unsigned *err, const int *__restrict__ targets = nullptr, int ntargets = 0,
+    double *__restrict__ Uout = nullptr) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double4 *tiles = reinterpret_cast<double4 *>(smem_raw);  // [2][2*TJ]
   __shared__ __align__(8) uint64_t bar[2];
@@ -31,11 +34,18 @@ __global__ void __launch_bounds__(64) k_direct_fp64(
   const SysConst &sc = scs[w.x];
   const int base = sc.base;
   const int pc = dyn[w.x].pcount;
-  if (w.y - base > pc) return;  // block-uniform: every target beyond pcount
-
   const int tid = threadIdx.x;
-  const int g = w.y + tid;
-  const bool active = (g - base <= pc) && (g - base <= sc.cap) && nxt[g] != 0;
+  int g;
+  bool active;
+  if (targets) {  // listed targets (k-th thread of block b takes targets[64 b + k])
+    const int idx = w.y + tid;
+    g = idx < ntargets ? targets[idx] : base;
+    active = idx < ntargets && g > base && g - base <= pc && nxt[g] != 0;
+  } else {
+    if (w.y - base > pc) return;  // block-uniform: every target beyond pcount
+    g = w.y + tid;
+    active = (g - base <= pc) && (g - base <= sc.cap) && nxt[g] != 0;
+  }
 
   // One thread reads the sticky error word so that the whole block agrees on it.
   if (tid == 0) {
@@ -142,6 +152,11 @@ __global__ void __launch_bounds__(64) k_direct_fp64(
 #pragma unroll
   for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], ubs[c]);
   mf_epilogue(sc, dyn[w.x].t, fdot, u);
+  if (targets) {
+    const int idx = w.y + tid;
+    for (int c = 0; c < 3; ++c) Uout[3 * (long long)idx + c] = u[c];
+    return;
+  }
   store3(U, T, g, u);
 }
 
@@ -161,4 +176,20 @@ void launch_direct_raw(cudaStream_t st, const SysConst *sc, const SysDyn *dyn, c
   if (nwork == 0) return;
   const size_t smem = 2 * 2 * kDirectTJ * sizeof(double4);
   k_direct_fp64<kDirectTJ><<<nwork, 64, smem, st>>>(sc, dyn, work, x, gi, gb, nxt, prv, seg, u, T, err);
+}
+
+// FP64 direct-sum velocity (the reference's BS scheme, whatever the system's own scheme) at
+// listed target slots; u3 is a device buffer of 3*n doubles (point-major, listed order).
+void launch_direct_targets(nv_handle *h, int sys, const int *d_targets, int n, double *d_u3) {
+  if (n <= 0) return;
+  std::vector<int2> w;
+  for (int b = 0; b < (n + 63) / 64; ++b) w.push_back(make_int2(sys, 64 * b));
+  int2 *dw = nullptr;
+  cudaMallocAsync((void **)&dw, w.size() * sizeof(int2), h->stream);
+  cudaMemcpyAsync(dw, w.data(), w.size() * sizeof(int2), cudaMemcpyHostToDevice, h->stream);
+  const size_t smem = 2 * 2 * kDirectTJ * sizeof(double4);
+  k_direct_fp64<kDirectTJ><<<(int)w.size(), 64, smem, h->stream>>>(h->d_sc, h->d_dyn, dw, h->x, h->gi, h->gb, h->nxt,
+                                                                   h->prv, h->seg, h->u, h->T, h->d_err, d_targets, n,
+                                                                   d_u3);
+  cudaFreeAsync(dw, h->stream);
 }

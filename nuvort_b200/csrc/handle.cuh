@@ -80,6 +80,7 @@ void launch_end_step(nv_handle *h);
 
 // direct sum (direct.cu)
 void launch_direct(nv_handle *h);
+void launch_direct_targets(nv_handle *h, int sys, const int *d_targets, int n, double *d_u3);
 // mixed precision (mixed.cu)
 void launch_direct_mixed(nv_handle *h);
 void launch_mixed_combine(nv_handle *h, int which);
