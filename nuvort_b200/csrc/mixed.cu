@@ -105,8 +105,28 @@ __global__ void __launch_bounds__(kTB) k_direct_mixed(const SysConst *__restrict
           const float ry = (H.y - th[1]) + (L.y - tl[1]);
           const float rz = (H.z - th[2]) + (L.z - tl[2]);
           const float a = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-          if (a < near2) {
-            // near field: the reference expression in FP64 (timestep.f90:162-170, 188-196)
+          if (a >= near2) {
+            // FP32 unless the pair is ill-conditioned in FP32: the segment subtends more than
+            // 120 degrees, the target lies near its line (typically the next-but-one segment
+            // along the target's own filament), or near its far end
+            const float ex = rx + D.x, ey = ry + D.y, ez = rz + D.z;
+            const float ee = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+            const float crx = fmaf(ry, D.z, -rz * D.y), cry = fmaf(rz, D.x, -rx * D.z), crz = fmaf(rx, D.y, -ry * D.x);
+            const float cr2 = fmaf(crx, crx, fmaf(cry, cry, crz * crz));
+            const float re = fmaf(rx, ex, fmaf(ry, ey, rz * ez));
+            const float r1 = a * rsqrtf(a), r2 = ee * rsqrtf(ee);
+            const float pp = r1 * r2;
+            if (!(pp + re < 0.5f * pp || cr2 < 0.01f * D.w * fminf(a, ee) || ee < 0.01f * fmaxf(a, D.w))) {
+              const float f = gq * (r1 + r2) * __frcp_rn(pp * (pp + re));
+              ux = fmaf(f, crx, ux);
+              uy = fmaf(f, cry, uy);
+              uz = fmaf(f, crz, uz);
+              continue;
+            }
+          }
+          {
+            // near field and ill-conditioned pairs: the reference expression in FP64
+            // (timestep.f90:162-170, 188-196) from the FP64 segment records
             const double4 A = seg64[2 * (long long)gj], B = seg64[2 * (long long)gj + 1];
             double r[3];
             if (m == 0) {
@@ -124,9 +144,7 @@ __global__ void __launch_bounds__(kTB) k_direct_mixed(const SysConst *__restrict
               ny += tm[1];
               nz += tm[2];
             }
-            continue;
           }
-          seg_term_f32(rx, ry, rz, D.x, D.y, D.z, gq, ux, uy, uz);
         }
         kahan_add(hx, cx, ux);
         kahan_add(hy, cy, uy);

@@ -6,9 +6,10 @@
 //   1. a parallel pass over all slots that marks the slots whose test can pass on the
 //      current state (or, for pinsert, whose stale-ghost test passes);
 //   2. a stable compaction of the marks into an ascending list per system (prefix sum);
-//   3. one thread per system that walks its list in ascending order, merged with a small
-//      min-heap of slots that an earlier event in the same sweep has touched (their test
-//      must be re-evaluated), and applies the reference's exact tests and updates.
+//   3. one thread per system that walks the marked slots in ascending order (a two-level
+//      bitmap; slots an earlier event in the same sweep has touched are marked on the way,
+//      since their test must be re-evaluated) and applies the reference's exact tests and
+//      updates.  pinsert has a parallel form for the common case (see below).
 // A slot that is neither marked nor touched has a test that is false in the serial sweep
 // too, so the events are the reference's, event for event and in the same order.
 #include <cub/cub.cuh>
@@ -22,6 +23,7 @@ struct TopoBuffers {
   int *dec = nullptr;       // per slot: bit0 stale test, bit1 fresh test, bit2 inserts, bit3 case A
   int *newslot = nullptr;   // per slot: the slot its insertion fills
   double *xnew = nullptr;   // per slot: new point position [3][T]
+  unsigned *l0 = nullptr, *l1 = nullptr;  // sweep bitmaps
   void *cub_tmp = nullptr;
   size_t cub_bytes = 0;
 };
@@ -29,47 +31,69 @@ struct TopoBuffers {
 namespace {
 
 constexpr int TB = 256;
-constexpr int kHeap = 512;  // pending re-tests per system resolver
 
-struct Heap {  // min-heap of slot indices in thread-local memory
-  int v[kHeap];
-  int n = 0;
-  __device__ bool push(int x) {
-    if (n >= kHeap) return false;
-    int i = n++;
-    v[i] = x;
-    while (i > 0) {
-      int p = (i - 1) >> 1;
-      if (v[p] <= v[i]) break;
-      int t = v[p]; v[p] = v[i]; v[i] = t;
-      i = p;
-    }
-    return true;
+// Two-level bitmap of the slots a serial sweep must still visit: bit g of l0 marks slot g,
+// bit w of l1 marks l0 word w as possibly non-empty.  The sweep takes the lowest marked
+// slot above the last one visited; events mark slots further ahead (there is no capacity
+// limit, unlike a fixed-size queue).
+struct Sweep {
+  unsigned *l0, *l1;
+  long long T;
+  __device__ void mark(int g) const {
+    atomicOr(&l0[g >> 5], 1u << (g & 31));
+    atomicOr(&l1[g >> 10], 1u << ((g >> 5) & 31));
   }
-  __device__ int top() const { return v[0]; }
-  __device__ void pop() {
-    v[0] = v[--n];
-    int i = 0;
+  __device__ void unmark(int g) const { atomicAnd(&l0[g >> 5], ~(1u << (g & 31))); }
+  // lowest marked slot >= from and <= last, or INT_MAX
+  __device__ int next(int from, int last) const {
+    if (from > last) return INT_MAX;
+    int w = from >> 5;
+    unsigned bits = l0[w] & (~0u << (from & 31));
     for (;;) {
-      int l = 2 * i + 1, r = l + 1, m = i;
-      if (l < n && v[l] < v[m]) m = l;
-      if (r < n && v[r] < v[m]) m = r;
-      if (m == i) break;
-      int t = v[m]; v[m] = v[i]; v[i] = t;
-      i = m;
+      if (bits) {
+        const int g = (w << 5) + __ffs(bits) - 1;
+        return g <= last ? g : INT_MAX;
+      }
+      // next non-empty l0 word after w, located through l1
+      int w1 = (w + 1) >> 5;
+      unsigned b1 = ((w + 1) & 31) ? (l1[w1] & (~0u << ((w + 1) & 31))) : l1[w1];
+      const int wlast = last >> 5;
+      for (;;) {
+        if (b1) break;
+        ++w1;
+        if ((w1 << 5) > wlast) return INT_MAX;
+        b1 = l1[w1];
+      }
+      w = (w1 << 5) + __ffs(b1) - 1;
+      if (w > wlast) return INT_MAX;
+      bits = l0[w];
+      if (!bits) {  // stale summary bit: clear it and keep looking
+        atomicAnd(&l1[w >> 5], ~(1u << (w & 31)));
+      }
     }
   }
 };
 
-// Next slot of the merged sweep (list[li..le) and the heap), strictly above `last`.
-__device__ __forceinline__ int sweep_next(const int *list, int &li, int le, Heap &hp, int last) {
-  for (;;) {
-    while (li < le && list[li] <= last) ++li;
-    while (hp.n > 0 && hp.top() <= last) hp.pop();
-    const int a = li < le ? list[li] : INT_MAX;
-    const int b = hp.n > 0 ? hp.top() : INT_MAX;
-    return a < b ? a : b;
+// l0/l1 from a 0/1 flag per slot (one thread per l0 word, then one per l1 word).
+__global__ void k_bits_l0(const int *__restrict__ flag, unsigned *l0, long long T) {
+  const long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (w * 32 >= T + 32) return;
+  unsigned b = 0;
+  for (int k = 0; k < 32; ++k) {
+    const long long g = w * 32 + k;
+    if (g < T && flag[g]) b |= 1u << k;
   }
+  l0[w] = b;
+}
+__global__ void k_bits_l1(const unsigned *__restrict__ l0, unsigned *l1, long long nw0) {
+  const long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (w * 32 >= nw0 + 32) return;
+  unsigned b = 0;
+  for (int k = 0; k < 32; ++k) {
+    const long long q = w * 32 + k;
+    if (q < nw0 && l0[q]) b |= 1u << k;
+  }
+  l1[w] = b;
 }
 
 __device__ __forceinline__ bool recon_step(const SysConst &sc, const SysDyn &d) {
@@ -191,8 +215,7 @@ __global__ void k_zero_live(SysDyn *dyn, int nsys) {
 // ---- pass 3: serial resolvers, one thread per system ---------------------------------------
 
 // pinsert (line.f90:18-96).
-__global__ void k_insert_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S,
-                                 const int *__restrict__ pos_a, const int *__restrict__ list_a,
+__global__ void k_insert_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S, Sweep sw,
                                  const int *__restrict__ pos_b, const int *__restrict__ list_b, unsigned *err,
                                  DevEvent *ev, int *ev_count, int ev_cap, int only_fallback) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -207,15 +230,14 @@ __global__ void k_insert_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, 
   const int base = sc.base;
   const int old_last = base + d.pcount;  // loop bound old_pcount (line.f90:28-30)
   int pc = d.pcount;
-  int li = pos_a[base], le = pos_a[base + sc.cap + 1];
   int ei = pos_b[base], ee = pos_b[base + sc.cap + 1];
-  Heap hp;
   int last = base;
   const long long T = S.T;
   for (;;) {
-    const int i = sweep_next(list_a, li, le, hp, last);
-    if (i == INT_MAX || i > old_last) break;
+    const int i = sw.next(last + 1, old_last);
+    if (i == INT_MAX) break;
     last = i;
+    sw.unmark(i);
     if (S.nxt[i] == 0) continue;
     double x[3], gi[3], gb[3];
     load3(S.X, T, i, x);
@@ -268,13 +290,8 @@ __global__ void k_insert_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, 
     log_event(d, s, NV_EV_INSERT, i, par_new, ev, ev_count, ev_cap);
     d.insert_count++;
     // slots whose test changed and that the sweep has not reached yet
-    bool ok = true;
-    if (nx > i && nx <= old_last) ok &= hp.push(nx);
-    if (par_new > i && par_new <= old_last) ok &= hp.push(par_new);
-    if (!ok) {
-      atomicOr(err, DERR_QUEUE);
-      break;
-    }
+    if (nx > i && nx <= old_last) sw.mark(nx);
+    if (par_new > i && par_new <= old_last) sw.mark(par_new);
   }
   d.pcount = pc;
   dyn[s] = d;
@@ -341,26 +358,23 @@ __global__ void k_recon_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, i
 }
 
 // premove (line.f90:102-130).
-__global__ void k_remove_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S,
-                                 const int *__restrict__ pos_a, const int *__restrict__ list_a, unsigned *err,
-                                 DevEvent *ev, int *ev_count, int ev_cap) {
+__global__ void k_remove_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S, Sweep sw,
+                                 unsigned *err, DevEvent *ev, int *ev_count, int ev_cap) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys || *err) return;
   const SysConst &sc = scs[s];
   SysDyn d = dyn[s];
   if (!recon_step(sc, d)) return;
   const int base = sc.base;
-  int li = pos_a[base];
-  const int le = pos_a[base + sc.cap + 1];
   const int lastslot = base + d.pcount;
   const double thr = e_mul(.99, sc.delta);
-  Heap hp;
   int last = base;
   const long long T = S.T;
   for (;;) {
-    const int i = sweep_next(list_a, li, le, hp, last);
-    if (i == INT_MAX || i > lastslot) break;
+    const int i = sw.next(last + 1, lastslot);
+    if (i == INT_MAX) break;
     last = i;
+    sw.unmark(i);
     if (S.nxt[i] == 0) continue;
     const int infront = S.nxt[i];
     const int tinfront = S.nxt[infront];
@@ -375,10 +389,7 @@ __global__ void k_remove_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, 
     loop_killer(S, d, s, i, d.pcount, ev, ev_count, ev_cap);
     d.remove_count++;
     const int p = S.prv[i];
-    if (p > i && p <= lastslot && !hp.push(p)) {
-      atomicOr(err, DERR_QUEUE);
-      break;
-    }
+    if (p > i && p <= lastslot) sw.mark(p);
   }
   dyn[s] = d;
 }
@@ -651,6 +662,16 @@ void compact(nv_handle *h, int *flag, int *pos, int *list) {
 
 int resolver_grid(nv_handle *h) { return grid_for(h->nsys, 32); }
 
+// Sweep bitmaps from a flag array.
+Sweep make_sweep(nv_handle *h, const int *flag) {
+  TopoBuffers *tb = h->topo;
+  const long long T = h->T;
+  const long long nw0 = T / 32 + 1;
+  k_bits_l0<<<grid_for(nw0, 256), 256, 0, h->stream>>>(flag, tb->l0, T);
+  k_bits_l1<<<grid_for(nw0 / 32 + 1, 256), 256, 0, h->stream>>>(tb->l0, tb->l1, nw0);
+  return Sweep{tb->l0, tb->l1, T};
+}
+
 }  // namespace
 
 void topo_alloc(nv_handle *h) {
@@ -668,6 +689,8 @@ void topo_alloc(nv_handle *h) {
   cudaMalloc(&tb->dec, n * sizeof(int));
   cudaMalloc(&tb->newslot, n * sizeof(int));
   cudaMalloc(&tb->xnew, 3 * n * sizeof(double));
+  cudaMalloc(&tb->l0, (n / 32 + 2) * sizeof(unsigned));
+  cudaMalloc(&tb->l1, (n / 1024 + 2) * sizeof(unsigned));
   cub::DeviceScan::ExclusiveSum(nullptr, tb->cub_bytes, tb->flag_a, tb->pos_a, (int)n);
   cudaMalloc(&tb->cub_tmp, std::max<size_t>(tb->cub_bytes, 16));
   h->topo = tb;
@@ -680,6 +703,7 @@ void topo_free(nv_handle *h) {
   cudaFree(tb->flag_b); cudaFree(tb->pos_b); cudaFree(tb->list_b);
   cudaFree(tb->flag_c); cudaFree(tb->pos_c); cudaFree(tb->list_c);
   cudaFree(tb->dec); cudaFree(tb->newslot); cudaFree(tb->xnew);
+  cudaFree(tb->l0); cudaFree(tb->l1);
   cudaFree(tb->cub_tmp);
   delete tb;
   h->topo = nullptr;
@@ -709,9 +733,9 @@ void launch_pinsert(nv_handle *h) {
   k_ins_ghosts<<<grid, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, S, tb->list_c, tb->newslot, nev, h->d_err);
   k_ins_finish<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, tb->pos_c, tb->pos_b,
                                                               h->d_err);
-  k_insert_resolve<<<resolver_grid(h), 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, S, tb->pos_a, tb->list_a,
-                                                           tb->pos_b, tb->list_b, h->d_err, h->d_events,
-                                                           h->d_event_count, h->event_cap, 1);
+  const Sweep sw = make_sweep(h, tb->flag_a);
+  k_insert_resolve<<<resolver_grid(h), 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, S, sw, tb->pos_b, tb->list_b,
+                                                           h->d_err, h->d_events, h->d_event_count, h->event_cap, 1);
 }
 
 void launch_pclose(nv_handle *h, bool only_brute) {
@@ -737,8 +761,7 @@ void launch_premove(nv_handle *h) {
   TopoBuffers *tb = h->topo;
   k_mark_remove<<<grid_for(h->T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->nxt,
                                                                tb->flag_a, h->T, h->d_err);
-  compact(h, tb->flag_a, tb->pos_a, tb->list_a);
-  k_remove_resolve<<<resolver_grid(h), 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a,
-                                                           tb->list_a, h->d_err, h->d_events, h->d_event_count,
-                                                           h->event_cap);
+  const Sweep sw = make_sweep(h, tb->flag_a);
+  k_remove_resolve<<<resolver_grid(h), 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), sw, h->d_err,
+                                                           h->d_events, h->d_event_count, h->event_cap);
 }
