@@ -209,6 +209,7 @@ def timed_steps(h, steps, flush, torch, sampler=None):
     evals = tests = 0
     per_step = []
     vel = 0.0
+    t_start = h.stage_times()
     for _ in range(steps):
         flush.zero_()
         torch.cuda.synchronize()
@@ -222,6 +223,8 @@ def timed_steps(h, steps, flush, torch, sampler=None):
             c = h.counters(s)
             evals += c.tree_eval
             tests += c.tree_tests
+    t_end = h.stage_times()
+    timed_steps.stages = {k: (t_end[k] - t_start[k]) / steps for k in t_end}
     return pts, per_step, vel, evals, tests
 
 
@@ -333,6 +336,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         pts, per_step, vel_ms, evals, tests = timed_steps(hm, args.steps, flush, torch)
+    stages = timed_steps.stages
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -414,6 +418,7 @@ def run_ours(args):
                                l2="256 MiB buffer written between timed steps"),
                 "impl": "ours",
                 "velocity_stage": {"ms_per_step": vel_ms / args.steps, "point_evals_per_s": all_pts / (vel_ms * 1e-3)},
+                "stage_ms_per_step": {k: round(v, 4) for k, v in stages.items()},
                 "roofline": roof, "hbm_peak_gbs": peaks.get("hbm_gbs"), "clocks": clk.summary(),
                 "gpu_launches": launches * args.steps, "per_step_ms": [round(x, 4) for x in per_step]}
         if plain:

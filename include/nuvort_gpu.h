@@ -206,7 +206,8 @@ int nv_calc_velocity_direct_at(nv_handle *h, int32_t sys, const int32_t *targets
  * [2] velocity, [3] AB3 update, [4] topology, [5] whole steps.  n = entries wanted. */
 int nv_stage_times(nv_handle *h, double *ms, int32_t n);
 /* Mixed precision: interactions closer than factor*delta (leaves of the tree walk, segment
- * pairs of the direct sum) are evaluated in FP64; the rest in FP32.  Default 8. */
+ * pairs of the direct sum) are evaluated in FP64; the rest in FP32, except interactions that
+ * are ill-conditioned in FP32 (checked per interaction), which also run in FP64.  Default 2. */
 int nv_set_near_factor(nv_handle *h, double factor);
 
 /* Turn per-step stage timing on (default) or off.  With timing on, nv_step waits for each
