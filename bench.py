@@ -351,13 +351,8 @@ def run_ours(args):
         err["events_compared"] = int(sum(len(e) for e in ev_p))
         err["steps_compared"] = args.warmup + args.steps
 
-    step_ms = sum(per_step)
-    t = torch.tensor([step_ms, vel_ms], dtype=torch.float64, device="cuda")
-    tp = torch.tensor([float(pts)], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tp, op=dist.ReduceOp.SUM)
-    step_ms, vel_ms, all_pts = float(t[0]), float(t[1]), float(tp[0])
+    from nuvort_b200.dist import reduce_max_sum
+    (step_ms, vel_ms), (all_pts,) = reduce_max_sum(dist, "cuda", [sum(per_step), vel_ms], [float(pts)])
     value = all_pts / (step_ms * 1e-3)
 
     # end to end through the C ABI with host buffers: upload f(:), one step, download f(:)
@@ -378,14 +373,8 @@ def run_ours(args):
             hosts = [hm.download(s) for s in range(len(states))]
             d2h += sum(nb(x) for x in hosts)
         e2e_s = time.perf_counter() - t0
-        te = torch.tensor([e2e_s, float(e_pts)], dtype=torch.float64, device="cuda")
-        if dist:
-            m = te[:1].clone()
-            dist.all_reduce(m, op=dist.ReduceOp.MAX)
-            p_ = te[1:].clone()
-            dist.all_reduce(p_, op=dist.ReduceOp.SUM)
-            te = torch.cat([m, p_])
-        e2e = {"value": float(te[1]) / float(te[0]), "unit": UNIT,
+        (e2e_s,), (e_pts,) = reduce_max_sum(dist, "cuda", [e2e_s], [float(e_pts)])
+        e2e = {"value": e_pts / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
                "path": "nv_upload (host f(:) -> device) + nv_step(1) + nv_download (device -> host) per step"}
 

@@ -1,0 +1,252 @@
+!> ISO_C_BINDING interface to libnuvort_gpu.so (include/nuvort_gpu.h) for the NuVort Fortran
+!> host.  type(qvort) (src/cdata.f90:19-29) is not interoperable, so the wrappers below pack
+!> f(:) into plain arrays for nv_upload and unpack them after nv_download; every status other
+!> than NV_OK ends the run through the host's fatal_error, as the replaced routines do.
+!>
+!> Not compiled in this repository's environment (there is no Fortran compiler here); the
+!> same C ABI is exercised by the Python binding and the tests.
+module nuvort_gpu
+  use iso_c_binding
+  implicit none
+
+  integer(c_int32_t), parameter :: NV_OK = 0
+  integer(c_int32_t), parameter :: NV_VEL_LIA = 0, NV_VEL_BS = 1, NV_VEL_TREE = 2
+  integer(c_int32_t), parameter :: NV_BC_PERIODIC = 0, NV_BC_OPEN = 1, NV_BC_SOLID = 2
+  integer(c_int32_t), parameter :: NV_NF_ZERO = 0, NV_NF_XFLOW = 1, NV_NF_UNIFORM = 2
+  integer(c_int32_t), parameter :: NV_PREC_FP64 = 0, NV_PREC_MIXED = 1
+
+  type, bind(c) :: nv_params
+    integer(c_int32_t) :: nsteps, shots, recon_shots, velocity
+    integer(c_int32_t) :: boundary(3)
+    integer(c_int32_t) :: normal_velocity, tree_extra_correction, nan_test
+    integer(c_int32_t) :: overide_timestep_check, precision
+    real(c_double) :: dt, delta, quant_circ, corea
+    real(c_double) :: box_size(3)
+    real(c_double) :: tree_theta, norm_vel_xflow
+    real(c_double) :: norm_vel_vec(3), alpha(2), super_velocity(3)
+    real(c_double) :: normal_fluid_cutoff, t_zero_normal_fluid
+  end type
+
+  type, bind(c) :: nv_host_state
+    integer(c_int32_t) :: pcount
+    type(c_ptr) :: x, u, u1, u2, ghosti, ghostb
+    type(c_ptr) :: infront, behind, closest, closestd
+  end type
+
+  type, bind(c) :: nv_counters
+    integer(c_int32_t) :: pcount, live, recon_count, remove_count, insert_count, loop_kills
+    integer(c_int64_t) :: tree_eval, tree_tests
+    integer(c_int32_t) :: itime, n_events
+    real(c_double) :: t
+  end type
+
+  interface
+    integer(c_int) function nv_params_default(p) bind(c, name='nv_params_default')
+      import :: c_int, nv_params
+      type(nv_params), intent(out) :: p
+    end function
+    integer(c_int) function nv_read_run_file(path, p) bind(c, name='nv_read_run_file')
+      import :: c_int, c_char, nv_params
+      character(kind=c_char), dimension(*), intent(in) :: path
+      type(nv_params), intent(inout) :: p
+    end function
+    integer(c_int) function nv_create(params, nsys, capacity, device, h) bind(c, name='nv_create')
+      import :: c_int, c_int32_t, c_ptr, nv_params
+      type(nv_params), dimension(*), intent(in) :: params
+      integer(c_int32_t), value :: nsys, device
+      integer(c_int32_t), dimension(*), intent(in) :: capacity
+      type(c_ptr), intent(out) :: h
+    end function
+    integer(c_int) function nv_destroy(h) bind(c, name='nv_destroy')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function nv_upload(h, sys, st) bind(c, name='nv_upload')
+      import :: c_int, c_int32_t, c_ptr, nv_host_state
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: sys
+      type(nv_host_state), intent(in) :: st
+    end function
+    integer(c_int) function nv_download(h, sys, st, cap) bind(c, name='nv_download')
+      import :: c_int, c_int32_t, c_ptr, nv_host_state
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: sys, cap
+      type(nv_host_state), intent(inout) :: st
+    end function
+    integer(c_int) function nv_set_clock(h, sys, t, itime) bind(c, name='nv_set_clock')
+      import :: c_int, c_int32_t, c_ptr, c_double
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: sys, itime
+      real(c_double), value :: t
+    end function
+    integer(c_int) function nv_counters_get(h, sys, c) bind(c, name='nv_counters_get')
+      import :: c_int, c_int32_t, c_ptr, nv_counters
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: sys
+      type(nv_counters), intent(out) :: c
+    end function
+    integer(c_int) function nv_step(h, nsteps) bind(c, name='nv_step')
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: nsteps
+    end function
+    ! one call per procedure of src/run.f90:26-64
+    integer(c_int) function nv_ghostp(h) bind(c, name='nv_ghostp')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function nv_construct_tree(h) bind(c, name='nv_construct_tree')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function nv_pmotion(h) bind(c, name='nv_pmotion')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function nv_pinsert(h) bind(c, name='nv_pinsert')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function nv_pclose(h) bind(c, name='nv_pclose')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function nv_precon(h) bind(c, name='nv_precon')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function nv_premove(h) bind(c, name='nv_premove')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function nv_enforce_boundary(h) bind(c, name='nv_enforce_boundary')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function nv_empty_tree(h) bind(c, name='nv_empty_tree')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function nv_end_step(h) bind(c, name='nv_end_step')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    type(c_ptr) function nv_last_error() bind(c, name='nv_last_error')
+      import :: c_ptr
+    end function
+  end interface
+
+  !> device handle of the run (one system)
+  type(c_ptr), save :: nv_h = c_null_ptr
+
+contains
+
+  !> run.in values of the host (module cdata) -> nv_params
+  subroutine nv_params_from_cdata(p)
+    use cdata
+    type(nv_params), intent(out) :: p
+    integer :: k, rc
+    rc = nv_params_default(p)
+    p%nsteps = nsteps ; p%shots = shots ; p%recon_shots = recon_shots
+    select case (velocity)
+      case ('LIA') ; p%velocity = NV_VEL_LIA
+      case ('BS') ; p%velocity = NV_VEL_BS
+      case ('Tree') ; p%velocity = NV_VEL_TREE
+    end select
+    do k = 1, 3
+      p%boundary(k) = NV_BC_PERIODIC
+    end do
+    if (boundary_x == 'open') p%boundary(1) = NV_BC_OPEN
+    if (boundary_y == 'open') p%boundary(2) = NV_BC_OPEN
+    if (boundary_z == 'open') p%boundary(3) = NV_BC_OPEN
+    if (boundary_x == 'solid') p%boundary(1) = NV_BC_SOLID
+    if (boundary_y == 'solid') p%boundary(2) = NV_BC_SOLID
+    if (boundary_z == 'solid') p%boundary(3) = NV_BC_SOLID
+    p%normal_velocity = NV_NF_ZERO
+    if (normal_velocity == 'xflow') p%normal_velocity = NV_NF_XFLOW
+    p%tree_extra_correction = merge(1, 0, tree_extra_correction)
+    p%nan_test = merge(1, 0, NAN_test)
+    p%overide_timestep_check = merge(1, 0, overide_timestep_check)
+    p%dt = dt ; p%delta = delta ; p%quant_circ = quant_circ ; p%corea = corea
+    p%box_size = box_size ; p%tree_theta = tree_theta ; p%norm_vel_xflow = norm_vel_xflow
+    p%alpha = alpha ; p%super_velocity = super_velocity
+    p%normal_fluid_cutoff = normal_fluid_cutoff ; p%t_zero_normal_fluid = t_zero_normal_fluid
+  end subroutine
+
+  subroutine nv_check(rc, where)
+    use cdata, only: fatal_error
+    integer(c_int), intent(in) :: rc
+    character(len=*), intent(in) :: where
+    character(kind=c_char), pointer :: msg(:)
+    character(len=256) :: text
+    integer :: k
+    if (rc == NV_OK) return
+    call c_f_pointer(nv_last_error(), msg, [256])
+    text = ' '
+    do k = 1, 256
+      if (msg(k) == c_null_char) exit
+      text(k:k) = msg(k)
+    end do
+    call fatal_error(where, trim(text))
+  end subroutine
+
+  !> f(:), pcount, t, itime -> device (replaces the host copy of the state)
+  subroutine nv_push_state(cap)
+    use cdata
+    integer, intent(in) :: cap
+    type(nv_params) :: p(1)
+    integer(c_int32_t) :: caps(1)
+    real(c_double), allocatable, target :: x(:,:), u(:,:), u1(:,:), u2(:,:)
+    integer(c_int32_t), allocatable, target :: inf(:), beh(:)
+    type(nv_host_state) :: st
+    integer :: i
+    if (.not. c_associated(nv_h)) then
+      call nv_params_from_cdata(p(1))
+      caps(1) = cap
+      call nv_check(nv_create(p, 1_c_int32_t, caps, 0_c_int32_t, nv_h), 'nuvort_gpu:nv_create')
+    end if
+    allocate(x(3,pcount), u(3,pcount), u1(3,pcount), u2(3,pcount), inf(pcount), beh(pcount))
+    do i = 1, pcount
+      x(:,i) = f(i)%x ; u(:,i) = f(i)%u ; u1(:,i) = f(i)%u1 ; u2(:,i) = f(i)%u2
+      inf(i) = f(i)%infront ; beh(i) = f(i)%behind
+    end do
+    st%pcount = pcount
+    st%x = c_loc(x) ; st%u = c_loc(u) ; st%u1 = c_loc(u1) ; st%u2 = c_loc(u2)
+    st%ghosti = c_null_ptr ; st%ghostb = c_null_ptr
+    st%infront = c_loc(inf) ; st%behind = c_loc(beh)
+    st%closest = c_null_ptr ; st%closestd = c_null_ptr
+    call nv_check(nv_upload(nv_h, 0_c_int32_t, st), 'nuvort_gpu:nv_upload')
+    call nv_check(nv_set_clock(nv_h, 0_c_int32_t, t, int(itime, c_int32_t)), 'nuvort_gpu:nv_set_clock')
+  end subroutine
+
+  !> device -> f(:), pcount (f is grown when pinsert appended slots on the device)
+  subroutine nv_pull_state(cap)
+    use cdata
+    integer, intent(in) :: cap
+    real(c_double), allocatable, target :: x(:,:), u(:,:), u1(:,:), u2(:,:)
+    integer(c_int32_t), allocatable, target :: inf(:), beh(:)
+    type(qvort), allocatable :: tmp(:)
+    type(nv_host_state) :: st
+    type(nv_counters) :: c
+    integer :: i
+    allocate(x(3,cap), u(3,cap), u1(3,cap), u2(3,cap), inf(cap), beh(cap))
+    st%x = c_loc(x) ; st%u = c_loc(u) ; st%u1 = c_loc(u1) ; st%u2 = c_loc(u2)
+    st%ghosti = c_null_ptr ; st%ghostb = c_null_ptr
+    st%infront = c_loc(inf) ; st%behind = c_loc(beh)
+    st%closest = c_null_ptr ; st%closestd = c_null_ptr
+    call nv_check(nv_download(nv_h, 0_c_int32_t, st, int(cap, c_int32_t)), 'nuvort_gpu:nv_download')
+    if (st%pcount > size(f)) then
+      allocate(tmp(st%pcount)) ; tmp(:)%infront = 0
+      tmp(1:size(f)) = f
+      call move_alloc(from=tmp, to=f)
+    end if
+    pcount = st%pcount
+    do i = 1, pcount
+      f(i)%x = x(:,i) ; f(i)%u = u(:,i) ; f(i)%u1 = u1(:,i) ; f(i)%u2 = u2(:,i)
+      f(i)%infront = inf(i) ; f(i)%behind = beh(i)
+    end do
+    call nv_check(nv_counters_get(nv_h, 0_c_int32_t, c), 'nuvort_gpu:nv_counters_get')
+    recon_count = c%recon_count ; remove_count = c%remove_count ; t = c%t
+  end subroutine
+
+end module

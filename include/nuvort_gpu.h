@@ -252,6 +252,12 @@ int nv_calc_velocity_bs_static(const nv_params *p, int32_t pcount, const double 
                                const int32_t *d_infront, const int32_t *d_behind, double t,
                                double *d_u3, void *stream);
 
+/* Diagnostic counters of system sys for the last step, for profiling the topology stages:
+ * [0] pinsert candidates, [1] insertions, [2] steps that needed the serial pinsert sweep
+ * (cumulative), [3] precon candidates, [4] premove candidates, [5]-[7] the first insertion
+ * that forced the serial sweep (slot, new slot, distance bits).  n = entries wanted (<= 8). */
+int nv_diagnostics(nv_handle *h, int32_t sys, int64_t *out, int32_t n);
+
 /* Block until the handle's stream is idle and report any device-side error. */
 int nv_sync(nv_handle *h);
 

@@ -68,6 +68,7 @@ def lib():
     L.nv_step_launches.argtypes = [vp, P(i32)]
     L.nv_measure_fp64_peak.argtypes = [i32, P(C.c_double)]
     L.nv_measure_fp32_peak.argtypes = [i32, P(C.c_double)]
+    L.nv_diagnostics.argtypes = [vp, i32, P(C.c_int64), i32]
     L.nv_calc_velocity_direct_at.argtypes = [vp, i32, P(i32), i32, P(C.c_double)]
     _lib = L
     return L
@@ -197,6 +198,11 @@ class Handle:
         _check(lib().nv_calc_velocity_direct_at(self.h, int(sys), tg.ctypes.data_as(C.POINTER(C.c_int32)),
                                                 tg.shape[0], u.ctypes.data_as(C.POINTER(C.c_double))))
         return u
+
+    def diagnostics(self, sys: int = 0) -> list:
+        out = (C.c_int64 * 8)()
+        _check(lib().nv_diagnostics(self.h, int(sys), out, 8))
+        return list(out)
 
     def stage_times(self) -> dict:
         ms = (C.c_double * len(STAGE_TIMES))()

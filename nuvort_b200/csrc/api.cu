@@ -795,6 +795,14 @@ int nv_tree_dump(nv_handle *h, int32_t sys, nv_tree_node *buf, int32_t cap, int3
   return tree_dump(h, sys, buf, cap, n);
 }
 
+int nv_diagnostics(nv_handle *h, int32_t sys, int64_t *out, int32_t n) {
+  if (!h || !out || sys < 0 || sys >= h->nsys || n < 0 || n > 8) return set_error(NV_ERR_ARG, "nv_diagnostics: bad arguments");
+  int rc = set_device(h);
+  if (rc || (rc = pull_dyn(h))) return rc;
+  for (int k = 0; k < n; ++k) out[k] = h->h_dyn[sys].diag[k];
+  return NV_OK;
+}
+
 int nv_sync(nv_handle *h) {
   if (!h) return set_error(NV_ERR_ARG, "null handle");
   int rc = set_device(h);

@@ -67,6 +67,7 @@ struct SysDyn {
   int live;
   int old_pcount;
   int ins_fallback;  // pinsert needs the serial resolver this step
+  long long diag[8];  // see nv_diagnostics
 };
 
 // One logged topology event (system-local numbering is restored on the host).

@@ -35,7 +35,7 @@ struct nv_handle {
   int n_work_img = 0;
   int4 *d_work_timg = nullptr; // same for the mixed tree walk
   int n_work_timg = 0;
-  double near_factor = 8.0;
+  double near_factor = 2.0;
   int tree_sys0 = 0;           // first system that walks the tree (its theta0 builds the mixed nodes)    // near field: pairs closer than near_factor*delta run in FP64
   unsigned *d_err = nullptr;
   DevEvent *d_events = nullptr;

@@ -318,6 +318,7 @@ __global__ void k_recon_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, i
   if (!recon_step(sc, d)) return;
   const int base = sc.base;
   const int li = pos_a[base], le = pos_a[base + sc.cap + 1];
+  d.diag[3] = le - li;
   const long long T = S.T;
   for (int idx = li; idx < le; ++idx) {
     const int i = list_a[idx];
@@ -484,6 +485,7 @@ __global__ void k_ins_decide(const SysConst *__restrict__ scs, SysDyn *dyn, int 
   const SysConst &sc = scs[s];
   dyn[s].ins_fallback = 0;
   const int li = pos_a[sc.base], le = pos_a[sc.base + sc.cap + 1];
+  dyn[s].diag[0] = le - li;
   for (int idx = li; idx < le; ++idx) {
     const int k = list_a[idx];
     int dv = dec[k];
@@ -563,7 +565,14 @@ __global__ void k_ins_points(const SysConst *__restrict__ scs, SysDyn *dyn, cons
       double gn[3];
       load3(S.X, T, nx, gn);
       ghost_adjust(sc, xn, gn);
-      if (dist_gen(xn, gn) > sc.delta) dyn[s].ins_fallback = 1;
+      const double dn = dist_gen(xn, gn);
+      if (dn > sc.delta) {
+        if (atomicExch(&dyn[s].ins_fallback, 1) == 0) {
+          dyn[s].diag[5] = k - base;
+          dyn[s].diag[6] = slot - base;
+          dyn[s].diag[7] = __double_as_longlong(dn);
+        }
+      }
     }
     // continue the chain: infront(k) inserts with ghosts refreshed by this insertion
     if (nx > k && (dec[nx] & 8)) {
@@ -641,8 +650,12 @@ __global__ void k_ins_finish(const SysConst *__restrict__ scs, SysDyn *dyn, int 
     atomicOr(err, DERR_EMPTY);
     return;
   }
-  if (d.ins_fallback) return;
   const int nev = pos_c[sc.base + sc.cap + 1] - pos_c[sc.base];
+  d.diag[1] = nev;
+  if (d.ins_fallback) {
+    d.diag[2] += 1;
+    return;
+  }
   const int nfree = pos_b[sc.base + sc.cap + 1] - pos_b[sc.base];
   d.event_seq += nev;
   d.insert_count += nev;

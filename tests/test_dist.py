@@ -1,0 +1,59 @@
+"""The multi-rank path on CPU: two gloo ranks shard an ensemble and reduce their timings."""
+import os
+import socket
+
+import pytest
+import torch.multiprocessing as mp
+
+from nuvort_b200.dist import reduce_max_sum, shard_systems
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _worker(rank, world, port, q):
+    import datetime
+
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    counts = [500, 20000, 1200, 7000, 300, 15000, 900]
+    mine = shard_systems(counts, world, rank)
+    work = float(sum(counts[s] for s in mine))
+    step_ms = 10.0 + 5.0 * rank
+    mx, sm = reduce_max_sum(dist, "cpu", [step_ms], [work, 1.0])
+    q.put((rank, mine, mx, sm))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_shard_and_reduce():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (r0, m0, mx0, sm0), (r1, m1, mx1, sm1) = res
+    assert sorted(m0 + m1) == list(range(7)) and not set(m0) & set(m1)
+    assert mx0 == mx1 == [15.0]
+    counts = [500, 20000, 1200, 7000, 300, 15000, 900]
+    assert sm0 == sm1 == [float(sum(counts)), 2.0]
+
+
+def test_shard_balances_quadratic_work():
+    counts = [20000, 15000, 12000, 9000, 3000, 1000]
+    loads = [sum(counts[s] ** 2 for s in shard_systems(counts, 3, r)) for r in range(3)]
+    # greedy longest-first: no rank exceeds the largest system or 4/3 of the mean load
+    assert max(loads) <= max(max(c ** 2 for c in counts), 4 / 3 * sum(loads) / 3)
+    assert shard_systems(counts, 1, 0) == list(range(6))
