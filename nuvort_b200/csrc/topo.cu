@@ -24,6 +24,9 @@ struct TopoBuffers {
   int *newslot = nullptr;   // per slot: the slot its insertion fills
   double *xnew = nullptr;   // per slot: new point position [3][T]
   unsigned *l0 = nullptr, *l1 = nullptr;  // sweep bitmaps
+  unsigned *touched = nullptr;             // per-system touched-slot bitmaps too big for smem
+  long long touched_words = 0;             // words per system
+  int smem_words = 0;                      // bitmap words the sweep keeps in shared memory
   void *cub_tmp = nullptr;
   size_t cub_bytes = 0;
 };
@@ -369,6 +372,7 @@ __global__ void k_remove_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, 
   const int base = sc.base;
   const int lastslot = base + d.pcount;
   const double thr = e_mul(.99, sc.delta);
+  d.diag[4] = 0;
   int last = base;
   const long long T = S.T;
   for (;;) {
@@ -376,6 +380,7 @@ __global__ void k_remove_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, 
     if (i == INT_MAX) break;
     last = i;
     sw.unmark(i);
+    d.diag[4]++;
     if (S.nxt[i] == 0) continue;
     const int infront = S.nxt[i];
     const int tinfront = S.nxt[infront];
@@ -475,28 +480,52 @@ __global__ void k_ins_mark(const SysConst *__restrict__ scs, SysDyn *__restrict_
   if (g < T) dec[g] = dv;
 }
 
-// Outcomes: known where the two tests agree; otherwise decided in ascending slot order from
-// the predecessor's outcome (one thread per system, touching only the differing slots).
-__global__ void k_ins_decide(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, const int *__restrict__ prv,
-                             const int *__restrict__ pos_a, const int *__restrict__ list_a, int *dec, int *fc,
-                             const unsigned *err) {
+// Outcomes: known where the two tests agree (decided here, in parallel); where they differ
+// the outcome is the fresh test if the predecessor p = behind(k) < k inserts, else the stale
+// one -- those "ambiguous" slots are marked for an ordered pass.
+__global__ void k_ins_decide_easy(const int *__restrict__ list_a, const int *__restrict__ n_ptr, int *dec, int *famb,
+                                  const unsigned *err) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= *n_ptr || *err) return;
+  const int k = list_a[e];
+  const int dv = dec[k];
+  const int st = dv & 1, fr = (dv >> 1) & 1;
+  if (st == fr) dec[k] = dv | (st << 2);
+  else famb[k] = 1;
+}
+
+// Ambiguous slots in ascending order, one thread per system (their predecessors' outcomes
+// are final: decided in parallel, or earlier in this pass).
+__global__ void k_ins_decide_amb(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, const int *__restrict__ prv,
+                                 const int *__restrict__ pos_m, const int *__restrict__ list_m,
+                                 const int *__restrict__ pos_a, int *dec, const unsigned *err) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys || *err) return;
   const SysConst &sc = scs[s];
   dyn[s].ins_fallback = 0;
-  const int li = pos_a[sc.base], le = pos_a[sc.base + sc.cap + 1];
-  dyn[s].diag[0] = le - li;
-  for (int idx = li; idx < le; ++idx) {
-    const int k = list_a[idx];
-    int dv = dec[k];
-    const int st = dv & 1, fr = (dv >> 1) & 1;
+  dyn[s].diag[0] = pos_a[sc.base + sc.cap + 1] - pos_a[sc.base];
+  const int mi = pos_m[sc.base], me = pos_m[sc.base + sc.cap + 1];
+  for (int idx = mi; idx < me; ++idx) {
+    const int k = list_m[idx];
+    const int dv = dec[k];
     const int p = prv[k];
     const bool caseA = p < k && (dec[p] & 4);
-    const int d = (st == fr) ? st : (caseA ? fr : st);
-    dv |= (d << 2) | (caseA ? 8 : 0);
-    dec[k] = dv;
-    fc[k] = d;
+    const int d = caseA ? (dv >> 1) & 1 : dv & 1;
+    dec[k] = dv | (d << 2);
   }
+}
+
+// Case A (ghosts refreshed by the predecessor's insertion) and the insertion flags.
+__global__ void k_ins_decide_case(const int *__restrict__ list_a, const int *__restrict__ n_ptr,
+                                  const int *__restrict__ prv, int *dec, int *fc, const unsigned *err) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= *n_ptr || *err) return;
+  const int k = list_a[e];
+  const int dv = dec[k];
+  const int p = prv[k];
+  const bool caseA = p < k && (dec[p] & 4);
+  if (caseA) dec[k] = dv | 8;
+  fc[k] = (dv >> 2) & 1;
 }
 
 __global__ void k_zero_flags(int *f, long long n) {
@@ -662,6 +691,191 @@ __global__ void k_ins_finish(const SysConst *__restrict__ scs, SysDyn *dyn, int 
   if (nev > nfree) d.pcount += nev - nfree;
 }
 
+
+// ---- precon sweep, warp-prefetched --------------------------------------------------------
+// The reference's sweep (reconnection.f90:180-221) is kept exactly: candidates in ascending
+// order, each decided on the state left by the events before it.  A warp loads 32
+// candidates at a time and decides each on the current state in parallel; lane 0 then walks
+// them in order.  A candidate's decision reads the links of i and of its partner j only
+// (nxt/prv of both; x and ghosts do not change in precon, and a cleared neighbour means a
+// cleared i or j), so the parallel decision stands unless an event earlier in the sweep
+// wrote the links of i or j -- tracked in a per-system bitmap of touched slots (shared
+// memory when it fits).  Touched candidates are decided again by lane 0 on the live state.
+
+struct ReconIn {
+  int i, pari, parb, j, nj, parjb;
+  int yes;  // 1: reconnect, 0: no, -1: skip (reconnection.f90:181-190)
+  double dot_val, l_before, l_after;
+};
+
+__device__ ReconIn recon_decide(const State &S, int i, double half_delta, int cl_i) {
+  ReconIn r;
+  r.i = i;
+  r.pari = S.nxt[i];
+  r.parb = S.prv[i];
+  r.j = cl_i;
+  r.nj = 0;
+  r.parjb = 0;
+  r.yes = -1;
+  r.dot_val = r.l_before = r.l_after = 0;
+  if (r.pari == 0) return r;
+  const int j = r.j;
+  if (j == r.pari || j == r.parb || j == 0) return r;
+  r.nj = S.nxt[j];
+  if (r.nj == 0) return r;
+  r.parjb = S.prv[j];
+  double t1[3], t2[3];
+  norm_tanf(S, i, t1);
+  norm_tanf(S, j, t2);
+  r.dot_val = dot3(t1, t2);
+  if (r.dot_val > 0.9) {
+    r.yes = 0;
+    return r;
+  }
+  const long long T = S.T;
+  double xi[3], gii[3], gbi[3], xj[3], gij[3], gbj[3], xpi[3], xpj[3];
+  load3(S.X, T, i, xi);
+  load3(S.GI, T, i, gii);
+  load3(S.GB, T, i, gbi);
+  load3(S.X, T, j, xj);
+  load3(S.GI, T, j, gij);
+  load3(S.GB, T, j, gbj);
+  load3(S.X, T, r.pari, xpi);
+  load3(S.X, T, r.parjb, xpj);
+  r.l_before = e_add(e_add(e_add(dist_gen(xi, gii), dist_gen(xi, gbi)), dist_gen(xj, gij)), dist_gen(xj, gbj));
+  r.l_after = e_add(e_add(e_add(dist_gen(xi, gbi), dist_gen(xi, xj)), dist_gen(xj, gij)), dist_gen(xpi, xpj));
+  r.yes = r.l_after <= r.l_before ? 1 : 0;
+  (void)half_delta;
+  return r;
+}
+
+__device__ __forceinline__ bool bit_get(const unsigned *b, int k) { return (b[k >> 5] >> (k & 31)) & 1u; }
+__device__ __forceinline__ void bit_set(unsigned *b, int k) { b[k >> 5] |= 1u << (k & 31); }
+
+// Slots whose links an event of the current chunk wrote: bit set in `bits` and recorded
+// in `list` so that the bits can be cleared when the chunk ends (the next chunk's parallel
+// decisions are taken on the state that already includes them).
+struct Touched {
+  unsigned *bits;
+  int *list;
+  int n;
+  int base;
+  __device__ void add(int g) {
+    if (g <= base) return;
+    const int k = g - base;
+    if (!bit_get(bits, k)) {
+      bit_set(bits, k);
+      list[n++] = k;
+    }
+  }
+  __device__ bool has(int g) const { return g > base && bit_get(bits, g - base); }
+};
+constexpr int kTouchedPerChunk = 32 * 10;  // 4 relinked + up to 6 cleared slots per event
+
+// loop_killer with the touched slots recorded (the cleared ones change their links)
+__device__ void loop_killer_mark(const State &S, SysDyn &d, int s, int particle, int pcount, DevEvent *ev,
+                                 int *ev_count, int ev_cap, Touched &tc) {
+  int counter = 1, nx = particle;
+  const int hops = pcount < 3 ? pcount : 3;
+  for (int it = 0; it < hops; ++it) {
+    nx = S.nxt[nx];
+    if (nx == particle) break;
+    counter++;
+  }
+  if (counter < 4) {
+    log_event(d, s, NV_EV_LOOPKILL, particle, counter, ev, ev_count, ev_cap);
+    d.loop_kills++;
+    nx = particle;
+    for (int it = 0; it < pcount; ++it) {
+      const int sn = S.nxt[nx];
+      tc.add(nx);
+      clear_particle(S, nx);
+      nx = sn;
+      if (nx == particle) break;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(32) k_recon_sweep(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S,
+                                                    const int *__restrict__ pos_a, const int *__restrict__ list_a,
+                                                    unsigned *gbits, long long gbits_words_per_sys, int smem_words,
+                                                    unsigned *err, DevEvent *ev, int *ev_count, int ev_cap) {
+  extern __shared__ unsigned sbits[];
+  __shared__ int tlist[kTouchedPerChunk];
+  const int s = blockIdx.x;
+  const int lane = threadIdx.x;
+  if (s >= nsys || *err) return;
+  const SysConst &sc = scs[s];
+  if (!recon_step(sc, dyn[s])) return;
+  const int base = sc.base;
+  const int nwords = (sc.cap + 1 + 31) / 32;
+  unsigned *bits = nwords <= smem_words ? sbits : gbits + (long long)s * gbits_words_per_sys;
+  for (int w = lane; w < nwords; w += 32) bits[w] = 0;
+  Touched tc{bits, tlist, 0, base};
+  const int li = pos_a[base], le = pos_a[base + sc.cap + 1];
+  SysDyn d = dyn[s];  // lane 0's copy is the live one
+  if (lane == 0) d.diag[3] = le - li;
+  __syncwarp();
+  const double half_delta = sc.delta / 2.;
+  for (int k0 = li; k0 < le; k0 += 32) {
+    const int k = k0 + lane;
+    ReconIn in;
+    in.yes = -1;
+    in.i = 0;
+    if (k < le) {
+      const int i = list_a[k];
+      in = recon_decide(S, i, half_delta, S.cl[i]);
+    }
+    __syncwarp();
+    const int n = min(32, le - k0);
+    for (int l = 0; l < n; ++l) {
+      int i = __shfl_sync(0xffffffffu, in.i, l);
+      int yes = __shfl_sync(0xffffffffu, in.yes, l);
+      int pari = __shfl_sync(0xffffffffu, in.pari, l);
+      int j = __shfl_sync(0xffffffffu, in.j, l);
+      int parjb = __shfl_sync(0xffffffffu, in.parjb, l);
+      if (lane == 0) {
+        if (tc.has(i) || tc.has(j)) {
+          // an earlier event wrote the links of i or j: decide again on the live state
+          if (S.nxt[i] == 0) {
+            yes = -1;
+          } else {
+            const ReconIn r = recon_decide(S, i, half_delta, S.cl[i]);
+            yes = r.yes;
+            pari = r.pari;
+            parjb = r.parjb;
+          }
+        }
+        if (yes == 1) {
+          d.recon_count++;
+          log_event(d, s, NV_EV_RECON, i, j, ev, ev_count, ev_cap);
+          S.nxt[parjb] = pari;
+          S.prv[pari] = parjb;
+          S.nxt[i] = j;
+          S.prv[j] = i;
+          tc.add(i);
+          tc.add(j);
+          tc.add(pari);
+          tc.add(parjb);
+          loop_killer_mark(S, d, s, pari, d.pcount, ev, ev_count, ev_cap, tc);
+          loop_killer_mark(S, d, s, i, d.pcount, ev, ev_count, ev_cap, tc);
+        }
+      }
+    }
+    // the chunk's writes are now visible to the next chunk's parallel decisions
+    __threadfence_block();
+    const int nt = __shfl_sync(0xffffffffu, tc.n, 0);
+    __syncwarp();
+    for (int q = lane; q < nt; q += 32) {
+      const int kk = tlist[q];
+      atomicAnd(&bits[kk >> 5], ~(1u << (kk & 31)));
+    }
+    if (lane == 0) tc.n = 0;
+    __syncwarp();
+  }
+  if (lane == 0) dyn[s] = d;
+}
+
 State make_state(nv_handle *h) {
   return State{h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv, h->closest, h->T};
 }
@@ -703,6 +917,18 @@ void topo_alloc(nv_handle *h) {
   cudaMalloc(&tb->newslot, n * sizeof(int));
   cudaMalloc(&tb->xnew, 3 * n * sizeof(double));
   cudaMalloc(&tb->l0, (n / 32 + 2) * sizeof(unsigned));
+  {
+    // touched-slot bitmaps: shared memory up to the device's opt-in limit, else global
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const int maxwords = (h->max_cap + 1 + 31) / 32;
+    tb->smem_words = std::min(maxwords, std::max(0, optin - 4096) / 4);
+    if (tb->smem_words < maxwords) {
+      tb->touched_words = maxwords;
+      cudaMalloc(&tb->touched, (size_t)h->nsys * maxwords * sizeof(unsigned));
+    }
+  }
   cudaMalloc(&tb->l1, (n / 1024 + 2) * sizeof(unsigned));
   cub::DeviceScan::ExclusiveSum(nullptr, tb->cub_bytes, tb->flag_a, tb->pos_a, (int)n);
   cudaMalloc(&tb->cub_tmp, std::max<size_t>(tb->cub_bytes, 16));
@@ -717,6 +943,7 @@ void topo_free(nv_handle *h) {
   cudaFree(tb->flag_c); cudaFree(tb->pos_c); cudaFree(tb->list_c);
   cudaFree(tb->dec); cudaFree(tb->newslot); cudaFree(tb->xnew);
   cudaFree(tb->l0); cudaFree(tb->l1);
+  if (tb->touched) cudaFree(tb->touched);
   cudaFree(tb->cub_tmp);
   delete tb;
   h->topo = nullptr;
@@ -731,8 +958,14 @@ void launch_pinsert(nv_handle *h) {
   compact(h, tb->flag_a, tb->pos_a, tb->list_a);  // candidates (either test passes)
   compact(h, tb->flag_b, tb->pos_b, tb->list_b);  // free slots
   k_zero_flags<<<grid_for(T + 1, TB), TB, 0, h->stream>>>(tb->flag_c, T);
-  k_ins_decide<<<resolver_grid(h), 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, h->prv, tb->pos_a, tb->list_a,
-                                                       tb->dec, tb->flag_c, h->d_err);
+  const int *ncand = tb->pos_a + T;
+  k_ins_decide_easy<<<grid_for(T, 128), 128, 0, h->stream>>>(tb->list_a, ncand, tb->dec, tb->flag_c, h->d_err);
+  compact(h, tb->flag_c, tb->pos_c, tb->list_c);  // ambiguous slots
+  k_ins_decide_amb<<<resolver_grid(h), 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, h->prv, tb->pos_c, tb->list_c,
+                                                           tb->pos_a, tb->dec, h->d_err);
+  k_zero_flags<<<grid_for(T + 1, TB), TB, 0, h->stream>>>(tb->flag_c, T);
+  k_ins_decide_case<<<grid_for(T, 128), 128, 0, h->stream>>>(tb->list_a, ncand, h->prv, tb->dec, tb->flag_c,
+                                                             h->d_err);
   compact(h, tb->flag_c, tb->pos_c, tb->list_c);  // insertions, in sweep order
   const State S = make_state(h);
   // the number of insertions (pos_c[T]) is known only on the device: launch over every
@@ -765,9 +998,15 @@ void launch_precon(nv_handle *h) {
   k_mark_recon<<<grid_for(h->T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->closestd, h->nxt,
                                                               tb->flag_a, h->T, h->d_err);
   compact(h, tb->flag_a, tb->pos_a, tb->list_a);
-  k_recon_resolve<<<resolver_grid(h), 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a,
-                                                          tb->list_a, h->d_err, h->d_events, h->d_event_count,
-                                                          h->event_cap);
+  const size_t smem = (size_t)tb->smem_words * sizeof(unsigned);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_recon_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr_set = true;
+  }
+  k_recon_sweep<<<h->nsys, 32, smem, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a, tb->list_a,
+                                                  tb->touched, tb->touched_words, tb->smem_words, h->d_err,
+                                                  h->d_events, h->d_event_count, h->event_cap);
 }
 
 void launch_premove(nv_handle *h) {
