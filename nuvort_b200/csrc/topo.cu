@@ -361,45 +361,6 @@ __global__ void k_recon_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, i
   dyn[s] = d;
 }
 
-// premove (line.f90:102-130).
-__global__ void k_remove_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S, Sweep sw,
-                                 unsigned *err, DevEvent *ev, int *ev_count, int ev_cap) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nsys || *err) return;
-  const SysConst &sc = scs[s];
-  SysDyn d = dyn[s];
-  if (!recon_step(sc, d)) return;
-  const int base = sc.base;
-  const int lastslot = base + d.pcount;
-  const double thr = e_mul(.99, sc.delta);
-  d.diag[4] = 0;
-  int last = base;
-  const long long T = S.T;
-  for (;;) {
-    const int i = sw.next(last + 1, lastslot);
-    if (i == INT_MAX) break;
-    last = i;
-    sw.unmark(i);
-    d.diag[4]++;
-    if (S.nxt[i] == 0) continue;
-    const int infront = S.nxt[i];
-    const int tinfront = S.nxt[infront];
-    double xi[3], xt[3];
-    load3(S.X, T, i, xi);
-    load3(S.X, T, tinfront, xt);
-    if (!(dist_gen(xi, xt) < thr)) continue;
-    S.prv[tinfront] = i;
-    S.nxt[i] = tinfront;
-    clear_particle(S, infront);
-    log_event(d, s, NV_EV_REMOVE, i, infront, ev, ev_count, ev_cap);
-    loop_killer(S, d, s, i, d.pcount, ev, ev_count, ev_cap);
-    d.remove_count++;
-    const int p = S.prv[i];
-    if (p > i && p <= lastslot) sw.mark(p);
-  }
-  dyn[s] = d;
-}
-
 // pclose (line.f90:135-160): exact nearest non-neighbour, non-periodic distance, strict <
 // so ties keep the lowest j.  One thread per target slot.
 __global__ void k_pclose_brute(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn,
@@ -772,9 +733,29 @@ struct Touched {
 };
 constexpr int kTouchedPerChunk = 32 * 10;  // 4 relinked + up to 6 cleared slots per event
 
-// loop_killer with the touched slots recorded (the cleared ones change their links)
-__device__ void loop_killer_mark(const State &S, SysDyn &d, int s, int particle, int pcount, DevEvent *ev,
-                                 int *ev_count, int ev_cap, Touched &tc) {
+// Events of one chunk, staged in shared memory by lane 0 and written with one atomic.
+struct EventStage {
+  DevEvent *buf;
+  int n;
+  __device__ void add(SysDyn &d, int s, int kind, int i, int j) {
+    buf[n++] = DevEvent{s, d.event_seq++, d.itime, kind, i, j};
+  }
+};
+__device__ void flush_events(EventStage &es, int lane, DevEvent *ev, int *ev_count, int ev_cap) {
+  int n = __shfl_sync(0xffffffffu, es.n, 0);
+  if (n == 0) return;
+  int at = 0;
+  if (lane == 0) at = atomicAdd(ev_count, n);
+  at = __shfl_sync(0xffffffffu, at, 0);
+  for (int q = lane; q < n; q += 32)
+    if (at + q < ev_cap) ev[at + q] = es.buf[q];
+  __syncwarp();
+  if (lane == 0) es.n = 0;
+  __syncwarp();
+}
+
+__device__ void loop_killer_stage(const State &S, SysDyn &d, int s, int particle, int pcount, EventStage &es,
+                                  Touched &tc) {
   int counter = 1, nx = particle;
   const int hops = pcount < 3 ? pcount : 3;
   for (int it = 0; it < hops; ++it) {
@@ -783,7 +764,7 @@ __device__ void loop_killer_mark(const State &S, SysDyn &d, int s, int particle,
     counter++;
   }
   if (counter < 4) {
-    log_event(d, s, NV_EV_LOOPKILL, particle, counter, ev, ev_count, ev_cap);
+    es.add(d, s, NV_EV_LOOPKILL, particle, counter);
     d.loop_kills++;
     nx = particle;
     for (int it = 0; it < pcount; ++it) {
@@ -802,6 +783,7 @@ __global__ void __launch_bounds__(32) k_recon_sweep(const SysConst *__restrict__
                                                     unsigned *err, DevEvent *ev, int *ev_count, int ev_cap) {
   extern __shared__ unsigned sbits[];
   __shared__ int tlist[kTouchedPerChunk];
+  __shared__ DevEvent ebuf[96];
   const int s = blockIdx.x;
   const int lane = threadIdx.x;
   if (s >= nsys || *err) return;
@@ -812,6 +794,7 @@ __global__ void __launch_bounds__(32) k_recon_sweep(const SysConst *__restrict__
   unsigned *bits = nwords <= smem_words ? sbits : gbits + (long long)s * gbits_words_per_sys;
   for (int w = lane; w < nwords; w += 32) bits[w] = 0;
   Touched tc{bits, tlist, 0, base};
+  EventStage es{ebuf, 0};
   const int li = pos_a[base], le = pos_a[base + sc.cap + 1];
   SysDyn d = dyn[s];  // lane 0's copy is the live one
   if (lane == 0) d.diag[3] = le - li;
@@ -848,7 +831,7 @@ __global__ void __launch_bounds__(32) k_recon_sweep(const SysConst *__restrict__
         }
         if (yes == 1) {
           d.recon_count++;
-          log_event(d, s, NV_EV_RECON, i, j, ev, ev_count, ev_cap);
+          es.add(d, s, NV_EV_RECON, i, j);
           S.nxt[parjb] = pari;
           S.prv[pari] = parjb;
           S.nxt[i] = j;
@@ -857,8 +840,8 @@ __global__ void __launch_bounds__(32) k_recon_sweep(const SysConst *__restrict__
           tc.add(j);
           tc.add(pari);
           tc.add(parjb);
-          loop_killer_mark(S, d, s, pari, d.pcount, ev, ev_count, ev_cap, tc);
-          loop_killer_mark(S, d, s, i, d.pcount, ev, ev_count, ev_cap, tc);
+          loop_killer_stage(S, d, s, pari, d.pcount, es, tc);
+          loop_killer_stage(S, d, s, i, d.pcount, es, tc);
         }
       }
     }
@@ -871,8 +854,117 @@ __global__ void __launch_bounds__(32) k_recon_sweep(const SysConst *__restrict__
       atomicAnd(&bits[kk >> 5], ~(1u << (kk & 31)));
     }
     if (lane == 0) tc.n = 0;
-    __syncwarp();
+    flush_events(es, lane, ev, ev_count, ev_cap);
   }
+  if (lane == 0) dyn[s] = d;
+}
+
+
+// ---- premove sweep, warp-prefetched --------------------------------------------------------
+// line.f90:107-129 in ascending slot order.  A candidate's test reads infront(i),
+// infront(infront(i)) and their positions; it is re-evaluated on the live state when an
+// event of the current chunk touched i or infront(i).  A removal at i changes the test of
+// p = behind(i); when p > i and p is not a candidate it is visited later as an extra slot
+// (the two-level bitmap).
+__global__ void __launch_bounds__(32) k_remove_sweep(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S,
+                                                     const int *__restrict__ pos_a, const int *__restrict__ list_a,
+                                                     const int *__restrict__ cand, Sweep sw, unsigned *gbits,
+                                                     long long gbits_words_per_sys, int smem_words, unsigned *err,
+                                                     DevEvent *ev, int *ev_count, int ev_cap) {
+  extern __shared__ unsigned sbits[];
+  __shared__ int tlist[kTouchedPerChunk];
+  __shared__ DevEvent ebuf[96];
+  const int s = blockIdx.x;
+  const int lane = threadIdx.x;
+  if (s >= nsys || *err) return;
+  const SysConst &sc = scs[s];
+  if (!recon_step(sc, dyn[s])) return;
+  const int base = sc.base;
+  const int nwords = (sc.cap + 1 + 31) / 32;
+  unsigned *bits = nwords <= smem_words ? sbits : gbits + (long long)s * gbits_words_per_sys;
+  for (int w = lane; w < nwords; w += 32) bits[w] = 0;
+  Touched tc{bits, tlist, 0, base};
+  EventStage es{ebuf, 0};
+  const int li = pos_a[base], le = pos_a[base + sc.cap + 1];
+  SysDyn d = dyn[s];
+  const int lastslot = base + d.pcount;
+  const double thr = e_mul(.99, sc.delta);
+  const long long T = S.T;
+  int extras = 0, last = base;  // lane 0: pending extra visits, last slot visited
+  if (lane == 0) d.diag[4] = le - li;
+  __syncwarp();
+  // one visit of slot i on the live state (lane 0)
+  auto visit = [&](int i) {
+    if (S.nxt[i] == 0) return;
+    const int infront = S.nxt[i];
+    const int tinfront = S.nxt[infront];
+    double xi[3], xt[3];
+    load3(S.X, T, i, xi);
+    load3(S.X, T, tinfront, xt);
+    if (!(dist_gen(xi, xt) < thr)) return;
+    S.prv[tinfront] = i;
+    S.nxt[i] = tinfront;
+    tc.add(i);
+    tc.add(infront);
+    tc.add(tinfront);
+    clear_particle(S, infront);
+    es.add(d, s, NV_EV_REMOVE, i, infront);
+    loop_killer_stage(S, d, s, i, d.pcount, es, tc);
+    d.remove_count++;
+    const int p = S.prv[i];
+    if (p > i && p <= lastslot && !cand[p]) {
+      sw.mark(p);
+      ++extras;
+    }
+  };
+  auto run_extras = [&](int upto) {  // extra slots in (last, upto]
+    while (extras > 0) {
+      const int e = sw.next(last + 1, upto);
+      if (e == INT_MAX) break;
+      sw.unmark(e);
+      --extras;
+      last = e;
+      visit(e);
+    }
+  };
+  for (int k0 = li; k0 < le; k0 += 32) {
+    const int k = k0 + lane;
+    int i = 0, inf = 0, yes = 0;
+    if (k < le) {
+      i = list_a[k];
+      inf = S.nxt[i];
+      if (inf) {
+        const int tinf = S.nxt[inf];
+        double xi[3], xt[3];
+        load3(S.X, T, i, xi);
+        load3(S.X, T, tinf, xt);
+        yes = dist_gen(xi, xt) < thr;
+      }
+    }
+    __syncwarp();
+    const int n = min(32, le - k0);
+    for (int l = 0; l < n; ++l) {
+      const int il = __shfl_sync(0xffffffffu, i, l);
+      const int infl = __shfl_sync(0xffffffffu, inf, l);
+      const int yl = __shfl_sync(0xffffffffu, yes, l);
+      if (lane == 0) {
+        run_extras(il - 1);
+        last = il;
+        if (tc.has(il) || tc.has(infl) || yl) visit(il);
+      }
+    }
+    __threadfence_block();
+    const int nt = __shfl_sync(0xffffffffu, tc.n, 0);
+    __syncwarp();
+    for (int q = lane; q < nt; q += 32) {
+      const int kk = tlist[q];
+      atomicAnd(&bits[kk >> 5], ~(1u << (kk & 31)));
+    }
+    if (lane == 0) tc.n = 0;
+    flush_events(es, lane, ev, ev_count, ev_cap);
+  }
+  if (lane == 0) run_extras(lastslot);
+  flush_events(es, lane, ev, ev_count, ev_cap);
   if (lane == 0) dyn[s] = d;
 }
 
@@ -928,6 +1020,9 @@ void topo_alloc(nv_handle *h) {
       tb->touched_words = maxwords;
       cudaMalloc(&tb->touched, (size_t)h->nsys * maxwords * sizeof(unsigned));
     }
+    const int smem = tb->smem_words * (int)sizeof(unsigned);
+    cudaFuncSetAttribute(k_recon_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_remove_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   }
   cudaMalloc(&tb->l1, (n / 1024 + 2) * sizeof(unsigned));
   cub::DeviceScan::ExclusiveSum(nullptr, tb->cub_bytes, tb->flag_a, tb->pos_a, (int)n);
@@ -999,11 +1094,6 @@ void launch_precon(nv_handle *h) {
                                                               tb->flag_a, h->T, h->d_err);
   compact(h, tb->flag_a, tb->pos_a, tb->list_a);
   const size_t smem = (size_t)tb->smem_words * sizeof(unsigned);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_recon_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr_set = true;
-  }
   k_recon_sweep<<<h->nsys, 32, smem, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a, tb->list_a,
                                                   tb->touched, tb->touched_words, tb->smem_words, h->d_err,
                                                   h->d_events, h->d_event_count, h->event_cap);
@@ -1013,7 +1103,12 @@ void launch_premove(nv_handle *h) {
   TopoBuffers *tb = h->topo;
   k_mark_remove<<<grid_for(h->T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->nxt,
                                                                tb->flag_a, h->T, h->d_err);
-  const Sweep sw = make_sweep(h, tb->flag_a);
-  k_remove_resolve<<<resolver_grid(h), 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), sw, h->d_err,
-                                                           h->d_events, h->d_event_count, h->event_cap);
+  compact(h, tb->flag_a, tb->pos_a, tb->list_a);
+  // extra visits start empty: bitmaps from an all-zero flag array
+  k_zero_flags<<<grid_for(h->T + 1, TB), TB, 0, h->stream>>>(tb->flag_b, h->T);
+  const Sweep sw = make_sweep(h, tb->flag_b);
+  const size_t smem = (size_t)tb->smem_words * sizeof(unsigned);
+  k_remove_sweep<<<h->nsys, 32, smem, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a, tb->list_a,
+                                                   tb->flag_a, sw, tb->touched, tb->touched_words, tb->smem_words,
+                                                   h->d_err, h->d_events, h->d_event_count, h->event_cap);
 }
