@@ -203,12 +203,17 @@ int nv_calc_velocity_direct_at(nv_handle *h, int32_t sys, const int32_t *targets
                                double *u3);
 
 /* Cumulative device time (ms) per stage since creation: ms[0] ghosts, [1] tree build,
- * [2] velocity, [3] AB3 update, [4] topology, [5] whole steps.  n = entries wanted. */
+ * [2] velocity, [3] AB3 update, [4] topology, [5] whole steps, and the parts of [4]:
+ * [6] pinsert, [7] pclose, [8] precon, [9] premove.  n = entries wanted (at most 10). */
 int nv_stage_times(nv_handle *h, double *ms, int32_t n);
 /* Mixed precision: interactions closer than factor*delta (leaves of the tree walk, segment
  * pairs of the direct sum) are evaluated in FP64; the rest in FP32, except interactions that
  * are ill-conditioned in FP32 (checked per interaction), which also run in FP64.  Default 2. */
 int nv_set_near_factor(nv_handle *h, double factor);
+/* pinsert places the insertions of new points that the sweep reaches again by a fixed-point
+ * iteration (default 6 rounds); a system that has not converged runs the serial sweep.
+ * Both give the reference's result.  n = 0 runs the serial sweep for every system (0..64). */
+int nv_set_insert_iterations(nv_handle *h, int32_t n);
 
 /* Turn per-step stage timing on (default) or off.  With timing on, nv_step waits for each
  * step and adds its device time per stage to nv_stage_times; off, steps are queued back to
@@ -254,8 +259,10 @@ int nv_calc_velocity_bs_static(const nv_params *p, int32_t pcount, const double 
 
 /* Diagnostic counters of system sys for the last step, for profiling the topology stages:
  * [0] pinsert candidates, [1] insertions, [2] steps that needed the serial pinsert sweep
- * (cumulative), [3] precon candidates, [4] premove candidates, [5]-[7] the first insertion
- * that forced the serial sweep (slot, new slot, distance bits).  n = entries wanted (<= 8). */
+ * (cumulative), [3] precon candidates, [4] premove candidates, [5] insertions made by new
+ * points that the sweep reached again, [6] fixed-point iterations the parallel pinsert took
+ * to place them (a system that has not converged after the last one runs the serial sweep),
+ * [7] unused.  n = entries wanted (<= 8). */
 int nv_diagnostics(nv_handle *h, int32_t sys, int64_t *out, int32_t n);
 
 /* Block until the handle's stream is idle and report any device-side error. */

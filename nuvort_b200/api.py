@@ -26,7 +26,7 @@ _lib = None
 
 STAGES = ("ghostp", "construct_tree", "pmotion", "pinsert", "pclose", "precon", "premove",
           "enforce_boundary", "empty_tree", "end_step")
-STAGE_TIMES = ("ghost", "tree", "velocity", "ab3", "topology", "step")
+STAGE_TIMES = ("ghost", "tree", "velocity", "ab3", "topology", "step", "insert", "close", "recon", "remove")
 
 
 class NuvortError(RuntimeError):
@@ -65,6 +65,7 @@ def lib():
     L.nv_tree_dump.argtypes = [vp, i32, P(NvTreeNode), i32, P(i32)]
     L.nv_set_timing.argtypes = [vp, i32]
     L.nv_set_near_factor.argtypes = [vp, C.c_double]
+    L.nv_set_insert_iterations.argtypes = [vp, C.c_int32]
     L.nv_step_launches.argtypes = [vp, P(i32)]
     L.nv_measure_fp64_peak.argtypes = [i32, P(C.c_double)]
     L.nv_measure_fp32_peak.argtypes = [i32, P(C.c_double)]
@@ -211,6 +212,10 @@ class Handle:
 
     def set_near_factor(self, factor: float):
         _check(lib().nv_set_near_factor(self.h, float(factor)))
+
+    def set_insert_iterations(self, n: int):
+        """Fixed-point rounds of the parallel pinsert (0: the serial sweep every step)."""
+        _check(lib().nv_set_insert_iterations(self.h, int(n)))
 
     def set_timing(self, on: bool):
         _check(lib().nv_set_timing(self.h, int(bool(on))))

@@ -237,10 +237,18 @@ void enqueue_step(nv_handle *h) {
   launch_ab3(h);
   time_end(h, ST_AB3);
   time_begin(h, ST_TOPO);
+  time_begin(h, ST_INSERT);
   launch_pinsert(h);
+  time_end(h, ST_INSERT);
+  time_begin(h, ST_CLOSE);
   launch_pclose(h, false);  // each system checks mod(itime, recon_shots) on the device
+  time_end(h, ST_CLOSE);
+  time_begin(h, ST_RECON);
   launch_precon(h);
+  time_end(h, ST_RECON);
+  time_begin(h, ST_REMOVE);
   launch_premove(h);
+  time_end(h, ST_REMOVE);
   launch_wrap(h, 3);
   launch_end_step(h);
   time_end(h, ST_TOPO);
@@ -281,7 +289,7 @@ int capture_step(nv_handle *h) {
 // Stage times of the step just replayed (the graph's event-record nodes).  A failed query
 // only drops the timing sample; it is cleared so that it cannot surface as a step error.
 void accumulate_stage_times(nv_handle *h) {
-  const int st[] = {ST_GHOST, ST_TREE, ST_VELOCITY, ST_AB3, ST_TOPO};
+  const int st[] = {ST_GHOST, ST_TREE, ST_VELOCITY, ST_AB3, ST_TOPO, ST_INSERT, ST_CLOSE, ST_RECON, ST_REMOVE};
   for (int s : st) {
     float ms = 0;
     cudaError_t e = cudaEventElapsedTime(&ms, h->ev[2 * s], h->ev[2 * s + 1]);
@@ -700,6 +708,13 @@ int nv_set_near_factor(nv_handle *h, double factor) {
   if (!h || !(factor >= 0)) return set_error(NV_ERR_ARG, "nv_set_near_factor: bad arguments");
   h->near_factor = factor;
   h->graph_valid = false;  // the factor is a launch argument of the captured kernels
+  return NV_OK;
+}
+
+int nv_set_insert_iterations(nv_handle *h, int32_t n) {
+  if (!h || n < 0 || n > 64) return set_error(NV_ERR_ARG, "nv_set_insert_iterations: n must be 0..64");
+  h->ins_iters = n;
+  h->graph_valid = false;  // the iteration count shapes the captured step
   return NV_OK;
 }
 

@@ -66,7 +66,9 @@ struct SysDyn {
   int event_seq;
   int live;
   int old_pcount;
-  int ins_fallback;  // pinsert needs the serial resolver this step
+  int ins_fallback;  // pinsert needs the serial sweep this step
+  int ins_conv;      // pinsert's fixed-point iteration has converged
+  int ins_mismatch;  // positions where the iteration's H and H' differ
   long long diag[8];  // see nv_diagnostics
 };
 

@@ -9,7 +9,7 @@
 struct TreeBuffers;  // tree.cu
 struct TopoBuffers;  // topo.cu
 
-enum { ST_GHOST = 0, ST_TREE, ST_VELOCITY, ST_AB3, ST_TOPO, ST_STEP, ST_COUNT };
+enum { ST_GHOST = 0, ST_TREE, ST_VELOCITY, ST_AB3, ST_TOPO, ST_STEP, ST_INSERT, ST_CLOSE, ST_RECON, ST_REMOVE, ST_COUNT };
 
 struct nv_handle {
   int device = 0;
@@ -36,6 +36,7 @@ struct nv_handle {
   int4 *d_work_timg = nullptr; // same for the mixed tree walk
   int n_work_timg = 0;
   double near_factor = 2.0;
+  int ins_iters = 6;  // fixed-point iterations of the parallel pinsert; 0: serial sweep only
   int tree_sys0 = 0;           // first system that walks the tree (its theta0 builds the mixed nodes)    // near field: pairs closer than near_factor*delta run in FP64
   unsigned *d_err = nullptr;
   DevEvent *d_events = nullptr;

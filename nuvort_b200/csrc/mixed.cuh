@@ -20,24 +20,6 @@ struct MixedNodes {  // per tree node, built after the FP64 node sums
   double2 *G = nullptr;  // geo^2, t0^2 for the dist <= geo branch (theta0 > 2/sqrt(3) only)
 };
 
-__device__ __forceinline__ void seg_term_f32(float rx, float ry, float rz, float dx, float dy, float dz,
-                                             float gq, float &ux, float &uy, float &uz) {
-  const float ex = rx + dx, ey = ry + dy, ez = rz + dz;
-  const float a = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-  const float ee = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-  const float re = fmaf(rx, ex, fmaf(ry, ey, rz * ez));
-  const float r1 = a * rsqrtf(a);
-  const float r2 = ee * rsqrtf(ee);
-  const float p = r1 * r2;
-  const float f = gq * (r1 + r2) * __frcp_rn(p * (p + re));
-  const float cx = fmaf(ry, dz, -rz * dy);
-  const float cy = fmaf(rz, dx, -rx * dz);
-  const float cz = fmaf(rx, dy, -ry * dx);
-  ux = fmaf(f, cx, ux);
-  uy = fmaf(f, cy, uy);
-  uz = fmaf(f, cz, uz);
-}
-
 // Kahan-compensated FP32 accumulation of one tile's partial sum into (s, comp).
 __device__ __forceinline__ void kahan_add(float &s, float &comp, float v) {
   const float y = v - comp;

@@ -6,10 +6,13 @@
 //   1. a parallel pass over all slots that marks the slots whose test can pass on the
 //      current state (or, for pinsert, whose stale-ghost test passes);
 //   2. a stable compaction of the marks into an ascending list per system (prefix sum);
-//   3. one thread per system that walks the marked slots in ascending order (a two-level
-//      bitmap; slots an earlier event in the same sweep has touched are marked on the way,
-//      since their test must be re-evaluated) and applies the reference's exact tests and
-//      updates.  pinsert has a parallel form for the common case (see below).
+//   3. one warp per system that walks the marked slots in ascending order, 32 at a time:
+//      the lanes decide their candidates on the state at the start of the chunk in
+//      parallel, lane 0 applies the events in order and decides again, on the live state,
+//      every candidate whose inputs an earlier event of the chunk wrote (a shared-memory set
+//      of touched slots).  Slots that an event makes testable and that the sweep reaches
+//      later are visited as extra slots (a two-level bitmap).  pinsert has a fully
+//      parallel form for the common case (see below) and sweeps only when that cannot apply.
 // A slot that is neither marked nor touched has a test that is false in the serial sweep
 // too, so the events are the reference's, event for event and in the same order.
 #include <cub/cub.cuh>
@@ -22,11 +25,12 @@ struct TopoBuffers {
   int *flag_c = nullptr, *pos_c = nullptr, *list_c = nullptr;
   int *dec = nullptr;       // per slot: bit0 stale test, bit1 fresh test, bit2 inserts, bit3 case A
   int *newslot = nullptr;   // per slot: the slot its insertion fills
-  double *xnew = nullptr;   // per slot: new point position [3][T]
+  double *xnew = nullptr;   // per insertion position: new point position [3][T]
+  double *unew = nullptr;   // per insertion position: new point velocity [3][T]
+  int *segnx = nullptr;     // per insertion position: infront of the original slot
+  int *fh[2] = {nullptr, nullptr};  // higher-order insertion positions, H and H'
+  int *pos_h = nullptr;     // exclusive prefix sum of H
   unsigned *l0 = nullptr, *l1 = nullptr;  // sweep bitmaps
-  unsigned *touched = nullptr;             // per-system touched-slot bitmaps too big for smem
-  long long touched_words = 0;             // words per system
-  int smem_words = 0;                      // bitmap words the sweep keeps in shared memory
   void *cub_tmp = nullptr;
   size_t cub_bytes = 0;
 };
@@ -103,12 +107,6 @@ __device__ __forceinline__ bool recon_step(const SysConst &sc, const SysDyn &d) 
   return (d.itime % sc.recon_shots) == 0;
 }
 
-__device__ void log_event(SysDyn &d, int s, int kind, int i, int j, DevEvent *ev, int *ev_count, int ev_cap) {
-  const int seq = d.event_seq++;
-  const int slot = atomicAdd(ev_count, 1);
-  if (slot < ev_cap) ev[slot] = DevEvent{s, seq, d.itime, kind, i, j};
-}
-
 struct State {
   double *X, *U, *U1, *U2, *GI, *GB, *CD;
   int *nxt, *prv, *cl;
@@ -125,29 +123,6 @@ __device__ void clear_particle(const State &S, int g) {  // general.f90:10-20
   S.nxt[g] = 0; S.prv[g] = 0; S.cl[g] = 0; S.CD[g] = 0;
 }
 
-// loop_killer (reconnection.f90:155-182).  Only "fewer than 4 points" matters, so the
-// count stops after three hops; the result equals the reference's full walk.
-__device__ void loop_killer(const State &S, SysDyn &d, int s, int particle, int pcount, DevEvent *ev,
-                            int *ev_count, int ev_cap) {
-  int counter = 1, nx = particle;
-  const int hops = pcount < 3 ? pcount : 3;
-  for (int it = 0; it < hops; ++it) {
-    nx = S.nxt[nx];
-    if (nx == particle) break;
-    counter++;
-  }
-  if (counter < 4) {
-    log_event(d, s, NV_EV_LOOPKILL, particle, counter, ev, ev_count, ev_cap);
-    d.loop_kills++;
-    nx = particle;
-    for (int it = 0; it < pcount; ++it) {
-      const int sn = S.nxt[nx];
-      clear_particle(S, nx);
-      nx = sn;
-      if (nx == particle) break;
-    }
-  }
-}
 
 __device__ __forceinline__ void get_ghost_p(const SysConst &sc, const State &S, int g, double gi[3], double gb[3]) {
   double x[3];
@@ -215,91 +190,6 @@ __global__ void k_zero_live(SysDyn *dyn, int nsys) {
   if (s < nsys) dyn[s].live = 0;
 }
 
-// ---- pass 3: serial resolvers, one thread per system ---------------------------------------
-
-// pinsert (line.f90:18-96).
-__global__ void k_insert_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S, Sweep sw,
-                                 const int *__restrict__ pos_b, const int *__restrict__ list_b, unsigned *err,
-                                 DevEvent *ev, int *ev_count, int ev_cap, int only_fallback) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nsys || *err) return;
-  if (only_fallback && !dyn[s].ins_fallback) return;
-  const SysConst &sc = scs[s];
-  SysDyn d = dyn[s];
-  if (d.live == 0) {
-    atomicOr(err, DERR_EMPTY);
-    return;
-  }
-  const int base = sc.base;
-  const int old_last = base + d.pcount;  // loop bound old_pcount (line.f90:28-30)
-  int pc = d.pcount;
-  int ei = pos_b[base], ee = pos_b[base + sc.cap + 1];
-  int last = base;
-  const long long T = S.T;
-  for (;;) {
-    const int i = sw.next(last + 1, old_last);
-    if (i == INT_MAX) break;
-    last = i;
-    sw.unmark(i);
-    if (S.nxt[i] == 0) continue;
-    double x[3], gi[3], gb[3];
-    load3(S.X, T, i, x);
-    load3(S.GI, T, i, gi);
-    load3(S.GB, T, i, gb);
-    const double disti = dist_gen(x, gi);
-    if (!(disti > sc.delta)) continue;
-    int par_new;
-    if (ei < ee) {
-      par_new = list_b[ei++];
-    } else {
-      if (pc + 1 > sc.cap) {
-        atomicOr(err, DERR_CAPACITY);
-        break;
-      }
-      par_new = base + (++pc);
-    }
-    double fdd[3], xn[3];
-    deriv2(x, gi, gb, fdd);
-    double curv = e_sqrt(dot3(fdd, fdd));
-    double mid[3] = {e_mul(0.5, e_add(x[0], gi[0])), e_mul(0.5, e_add(x[1], gi[1])), e_mul(0.5, e_add(x[2], gi[2]))};
-    if (curv > 1E-5) {
-      curv = e_div(1.0, curv);
-      const double disc = e_sub(e_mul(curv, curv), e_mul(0.25, e_mul(disti, disti)));
-      if (disc > 0.) {
-        const double sfac = e_mul(e_sub(e_sqrt(disc), curv), curv);
-        for (int c = 0; c < 3; ++c) xn[c] = e_add(mid[c], e_mul(sfac, fdd[c]));
-      } else {
-        for (int c = 0; c < 3; ++c) xn[c] = mid[c];
-      }
-    } else {
-      for (int c = 0; c < 3; ++c) xn[c] = mid[c];
-    }
-    const int nx = S.nxt[i];
-    double ui[3], un[3], zero[3] = {0, 0, 0};
-    load3(S.U, T, i, ui);
-    load3(S.U, T, nx, un);
-    for (int c = 0; c < 3; ++c) un[c] = e_mul(0.5, e_add(ui[c], un[c]));
-    store3(S.X, T, par_new, xn);
-    store3(S.U, T, par_new, un);
-    store3(S.U1, T, par_new, zero);
-    store3(S.U2, T, par_new, zero);
-    S.prv[par_new] = i;
-    S.nxt[par_new] = nx;
-    refresh_ghosts(sc, S, par_new);
-    S.prv[nx] = par_new;
-    refresh_ghosts(sc, S, nx);
-    S.nxt[i] = par_new;
-    refresh_ghosts(sc, S, i);
-    log_event(d, s, NV_EV_INSERT, i, par_new, ev, ev_count, ev_cap);
-    d.insert_count++;
-    // slots whose test changed and that the sweep has not reached yet
-    if (nx > i && nx <= old_last) sw.mark(nx);
-    if (par_new > i && par_new <= old_last) sw.mark(par_new);
-  }
-  d.pcount = pc;
-  dyn[s] = d;
-}
-
 // precon (reconnection.f90:11-61).
 __device__ void norm_tanf(const State &S, int g, double t[3]) {  // general.f90:106-117
   double x[3], gi[3], gb[3];
@@ -309,56 +199,6 @@ __device__ void norm_tanf(const State &S, int g, double t[3]) {  // general.f90:
   deriv1(x, gi, gb, t);
   const double len = e_sqrt(e_add(e_add(e_sq(t[0]), e_sq(t[1])), e_sq(t[2])));
   for (int c = 0; c < 3; ++c) t[c] = e_div(t[c], len);
-}
-
-__global__ void k_recon_resolve(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S,
-                                const int *__restrict__ pos_a, const int *__restrict__ list_a, unsigned *err,
-                                DevEvent *ev, int *ev_count, int ev_cap) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nsys || *err) return;
-  const SysConst &sc = scs[s];
-  SysDyn d = dyn[s];
-  if (!recon_step(sc, d)) return;
-  const int base = sc.base;
-  const int li = pos_a[base], le = pos_a[base + sc.cap + 1];
-  d.diag[3] = le - li;
-  const long long T = S.T;
-  for (int idx = li; idx < le; ++idx) {
-    const int i = list_a[idx];
-    if (S.nxt[i] == 0) continue;
-    const int pari = S.nxt[i], parb = S.prv[i];
-    const int j = S.cl[i];
-    if (j == pari || j == parb || j == 0) continue;
-    if (S.nxt[j] == 0) continue;
-    const int parjb = S.prv[j];
-    double t1[3], t2[3];
-    norm_tanf(S, i, t1);
-    norm_tanf(S, j, t2);
-    const double dot_val = dot3(t1, t2);
-    if (dot_val > 0.9) continue;
-    double xi[3], gii[3], gbi[3], xj[3], gij[3], gbj[3], xpi[3], xpj[3];
-    load3(S.X, T, i, xi);
-    load3(S.GI, T, i, gii);
-    load3(S.GB, T, i, gbi);
-    load3(S.X, T, j, xj);
-    load3(S.GI, T, j, gij);
-    load3(S.GB, T, j, gbj);
-    load3(S.X, T, pari, xpi);
-    load3(S.X, T, parjb, xpj);
-    const double l_before = e_add(e_add(e_add(dist_gen(xi, gii), dist_gen(xi, gbi)), dist_gen(xj, gij)), dist_gen(xj, gbj));
-    const double l_after = e_add(e_add(e_add(dist_gen(xi, gbi), dist_gen(xi, xj)), dist_gen(xj, gij)), dist_gen(xpi, xpj));
-    if (l_after <= l_before) {
-      d.recon_count++;
-      log_event(d, s, NV_EV_RECON, i, j, ev, ev_count, ev_cap);
-      S.nxt[parjb] = pari;
-      S.prv[pari] = parjb;
-      S.nxt[i] = j;
-      S.prv[j] = i;
-      loop_killer(S, d, s, pari, d.pcount, ev, ev_count, ev_cap);
-      loop_killer(S, d, s, i, d.pcount, ev, ev_count, ev_cap);
-    }
-  }
-  dyn[s] = d;
 }
 
 // pclose (line.f90:135-160): exact nearest non-neighbour, non-periodic distance, strict <
@@ -399,6 +239,29 @@ __global__ void k_pclose_brute(const SysConst *__restrict__ scs, const SysDyn *_
 }
 
 
+// new point of an insertion (line.f90:62-79)
+__device__ void new_point(const double x[3], const double gi[3], const double gb[3], double disti, double xn[3]) {
+  double fdd[3];
+  deriv2(x, gi, gb, fdd);
+  double curv = e_sqrt(dot3(fdd, fdd));
+  const double mid[3] = {e_mul(0.5, e_add(x[0], gi[0])), e_mul(0.5, e_add(x[1], gi[1])), e_mul(0.5, e_add(x[2], gi[2]))};
+  for (int c = 0; c < 3; ++c) xn[c] = mid[c];
+  if (curv > 1E-5) {
+    curv = e_div(1.0, curv);
+    const double disc = e_sub(e_mul(curv, curv), e_mul(0.25, e_mul(disti, disti)));
+    if (disc > 0.) {
+      const double sfac = e_mul(e_sub(e_sqrt(disc), curv), curv);
+      for (int c = 0; c < 3; ++c) xn[c] = e_add(mid[c], e_mul(sfac, fdd[c]));
+    }
+  }
+}
+
+// g as seen from x: the nearest periodic image (get_ghost_p's adjustment)
+__device__ __forceinline__ void ghost_of(const SysConst &sc, const double x[3], const double g[3], double out[3]) {
+  for (int c = 0; c < 3; ++c) out[c] = g[c];
+  ghost_adjust(sc, x, out);
+}
+
 // ---- parallel pinsert ---------------------------------------------------------------------
 // In the serial sweep (line.f90:30-93) slot k is tested against its step-start ghost unless
 // its predecessor p = behind(k) < k inserted earlier in the same sweep: that insertion
@@ -406,8 +269,8 @@ __global__ void k_pclose_brute(const SysConst *__restrict__ scs, const SysDyn *_
 // two candidate outcomes, a stale test and a fresh test; when they agree the outcome is
 // known, and only slots where they differ depend on their predecessor's outcome.
 // New points that the sweep reaches later (placed in a free slot above their creator) are
-// tested again by the reference; when any such point would insert, the step falls back to
-// the serial resolver.
+// tested again by the reference and may insert in turn; k_ins_chain resolves those
+// higher-order insertions by a fixed-point iteration over their positions.
 
 // bit0 stale test, bit1 fresh test (ghost of the current infront position); list = either.
 __global__ void k_ins_mark(const SysConst *__restrict__ scs, SysDyn *__restrict__ dyn, const int *__restrict__ sys_of,
@@ -464,6 +327,8 @@ __global__ void k_ins_decide_amb(const SysConst *__restrict__ scs, SysDyn *dyn, 
   if (s >= nsys || *err) return;
   const SysConst &sc = scs[s];
   dyn[s].ins_fallback = 0;
+  dyn[s].ins_conv = 0;
+  dyn[s].ins_mismatch = 0;
   dyn[s].diag[0] = pos_a[sc.base + sc.cap + 1] - pos_a[sc.base];
   const int mi = pos_m[sc.base], me = pos_m[sc.base + sc.cap + 1];
   for (int idx = mi; idx < me; ++idx) {
@@ -494,79 +359,114 @@ __global__ void k_zero_flags(int *f, long long n) {
   if (g <= n) f[g] = 0;
 }
 
-// New points along chains of consecutive insertions: a chain starts at an inserting slot
-// whose ghosts were not refreshed (case B) and continues to infront(k) while that slot
-// inserts in case A (its ghosts then hold the current infront position and the new point
-// just placed behind it).  One thread per chain head.
-__global__ void k_ins_points(const SysConst *__restrict__ scs, SysDyn *dyn, const int *__restrict__ sys_of, State S,
-                             const int *__restrict__ pos_c, const int *__restrict__ list_c, const int *__restrict__ pos_b,
-                             const int *__restrict__ list_b, const int *__restrict__ dec, int *newslot, double *xnew,
-                             const int *__restrict__ nev_total, unsigned *err) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= *nev_total || *err) return;
-  int k = list_c[e];
+// New points along chains of consecutive insertions, with the insertions of new points the
+// sweep reaches again.  A chain starts at an inserting slot whose ghosts were not refreshed
+// (case B) and continues to infront(k) while that slot inserts in case A (its ghosts then
+// hold the current infront position and the newest point placed behind it).
+//
+// The insertion at k puts e1 between k and nx = infront(k).  When e1's slot lies above k
+// (and within the step-start pcount) the sweep visits e1 at that position and tests it
+// against nx; if it inserts, e2 goes between e1 and nx, and so on: a sub-chain e1, e2, ...
+// whose points are fixed by positions alone (e_m's ghosts are nx and e_{m-1}, or k).  The
+// one quantity that couples different chains is the slot of each new point, the free slot
+// of the insertion's rank in sweep order, where the sweep order merges the original
+// insertions (at their slots) with these higher-order ones (at the new points' slots).
+// Given a set H of higher-order positions, pos_c + pos_h give every rank; the walk then
+// yields the higher-order positions H' it implies.  Each event depends only on events at
+// lower positions, so once H' = H every event is the serial sweep's (by induction over the
+// sweep position).  The walk is repeated from H = {} a fixed number of times; a system
+// that has not converged by then runs the serial sweep.
+__global__ void k_ins_chain(const SysConst *__restrict__ scs, SysDyn *dyn, const int *__restrict__ sys_of, State S,
+                            const int *__restrict__ pos_c, const int *__restrict__ list_c,
+                            const int *__restrict__ pos_b, const int *__restrict__ list_b, const int *__restrict__ dec,
+                            const int *__restrict__ pos_h, int *fout, int *newslot, int *segnx, double *xnew,
+                            double *unew, const int *__restrict__ nev_total, unsigned *err) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= *nev_total || *err) return;
+  int k = list_c[t];
   if (dec[k] & 8) return;  // not a chain head
   const int s = sys_of[k];
+  if (dyn[s].ins_conv || dyn[s].ins_fallback) return;
   const SysConst &sc = scs[s];
   const int base = sc.base;
-  const int ev0 = pos_c[base], fb0 = pos_b[base], nfree = pos_b[base + sc.cap + 1] - fb0;
+  const int ev0 = pos_c[base], h0 = pos_h[base];
+  const int fb0 = pos_b[base], nfree = pos_b[base + sc.cap + 1] - fb0;
   const int pc = dyn[s].pcount;
   const long long T = S.T;
   const int old_last = base + pc;
+  // slot of the insertion with sweep rank r: the free slots in ascending order, then pcount+1..
+  auto slot_of = [&](int g) -> int {
+    const int r = (pos_c[g] - ev0) + (pos_h[g] - h0);
+    const int slot = r < nfree ? list_b[fb0 + r] : base + pc + 1 + (r - nfree);
+    if (slot > base + sc.cap) {  // possibly an artefact of a not yet consistent H:
+      dyn[s].ins_fallback = 1;    // the serial sweep decides (and reports a real overflow)
+      return -1;
+    }
+    return slot;
+  };
+  auto put = [&](int g, int slot, int nx, const double xn[3], const double un[3]) {
+    newslot[g] = slot;
+    segnx[g] = nx;
+    for (int c = 0; c < 3; ++c) {
+      xnew[c * T + g] = xn[c];
+      unew[c * T + g] = un[c];
+    }
+  };
   double gbk[3];
   bool fresh = false;
   for (;;) {
-    const int rank = pos_c[k] - ev0;
-    const int slot = rank < nfree ? list_b[fb0 + rank] : base + pc + 1 + (rank - nfree);
-    if (slot > base + sc.cap) {
-      atomicOr(err, DERR_CAPACITY);
-      return;
-    }
-    newslot[k] = slot;
-    double x[3], gi[3], gb[3];
+    const int slot = slot_of(k);
+    if (slot < 0) return;
+    double x[3], gi[3], gb[3], xnx[3], uk[3], unx[3], xn[3], un[3];
     load3(S.X, T, k, x);
     const int nx = S.nxt[k];
+    load3(S.X, T, nx, xnx);
     if (fresh) {  // ghosts refreshed by the predecessor's insertion (get_ghost_p, line.f90:89)
-      load3(S.X, T, nx, gi);
-      ghost_adjust(sc, x, gi);
-      for (int c = 0; c < 3; ++c) gb[c] = gbk[c];
-      ghost_adjust(sc, x, gb);
+      ghost_of(sc, x, xnx, gi);
+      ghost_of(sc, x, gbk, gb);
     } else {
       load3(S.GI, T, k, gi);
       load3(S.GB, T, k, gb);
     }
-    const double disti = dist_gen(x, gi);
-    double fdd[3], xn[3];
-    deriv2(x, gi, gb, fdd);
-    double curv = e_sqrt(dot3(fdd, fdd));
-    const double mid[3] = {e_mul(0.5, e_add(x[0], gi[0])), e_mul(0.5, e_add(x[1], gi[1])), e_mul(0.5, e_add(x[2], gi[2]))};
-    for (int c = 0; c < 3; ++c) xn[c] = mid[c];
-    if (curv > 1E-5) {
-      curv = e_div(1.0, curv);
-      const double disc = e_sub(e_mul(curv, curv), e_mul(0.25, e_mul(disti, disti)));
-      if (disc > 0.) {
-        const double sfac = e_mul(e_sub(e_sqrt(disc), curv), curv);
-        for (int c = 0; c < 3; ++c) xn[c] = e_add(mid[c], e_mul(sfac, fdd[c]));
-      }
+    new_point(x, gi, gb, dist_gen(x, gi), xn);
+    load3(S.U, T, k, uk);
+    load3(S.U, T, nx, unx);
+    for (int c = 0; c < 3; ++c) un[c] = e_mul(0.5, e_add(uk[c], unx[c]));
+    put(k, slot, nx, xn, un);
+    // the sub-chain of new points the sweep reaches again
+    double last[3], xe[3], ue[3], xprev[3];
+    for (int c = 0; c < 3; ++c) {
+      last[c] = xn[c];
+      xe[c] = xn[c];
+      ue[c] = un[c];
+      xprev[c] = x[c];
     }
-    for (int c = 0; c < 3; ++c) xnew[c * T + k] = xn[c];
-    // a new point the sweep reaches later is tested again (its ghost: infront of k)
-    if (slot > k && slot <= old_last) {
-      double gn[3];
-      load3(S.X, T, nx, gn);
-      ghost_adjust(sc, xn, gn);
-      const double dn = dist_gen(xn, gn);
-      if (dn > sc.delta) {
-        if (atomicExch(&dyn[s].ins_fallback, 1) == 0) {
-          dyn[s].diag[5] = k - base;
-          dyn[s].diag[6] = slot - base;
-          dyn[s].diag[7] = __double_as_longlong(dn);
-        }
+    int at = k, e = slot;
+    while (e > at && e <= old_last) {
+      double gie[3], gbe[3], xq[3], uq[3];
+      ghost_of(sc, xe, xnx, gie);
+      const double dn = dist_gen(xe, gie);
+      if (!(dn > sc.delta)) break;
+      fout[e] = 1;
+      const int q = slot_of(e);
+      if (q < 0) return;
+      ghost_of(sc, xe, xprev, gbe);
+      new_point(xe, gie, gbe, dn, xq);
+      for (int c = 0; c < 3; ++c) uq[c] = e_mul(0.5, e_add(ue[c], unx[c]));
+      put(e, q, nx, xq, uq);
+      if (e < nx)  // inserted before the sweep reaches nx: nx's behind ghost
+        for (int c = 0; c < 3; ++c) last[c] = xq[c];
+      for (int c = 0; c < 3; ++c) {
+        xprev[c] = xe[c];
+        xe[c] = xq[c];
+        ue[c] = uq[c];
       }
+      at = e;
+      e = q;
     }
     // continue the chain: infront(k) inserts with ghosts refreshed by this insertion
     if (nx > k && (dec[nx] & 8)) {
-      for (int c = 0; c < 3; ++c) gbk[c] = xn[c];
+      for (int c = 0; c < 3; ++c) gbk[c] = last[c];
       fresh = true;
       k = nx;
       continue;
@@ -575,63 +475,126 @@ __global__ void k_ins_points(const SysConst *__restrict__ scs, SysDyn *dyn, cons
   }
 }
 
-// Apply every insertion (links, new point state) and log the events in sweep order.
+// Every system takes the serial sweep (no fixed-point rounds).
+__global__ void k_ins_all_serial(SysDyn *dyn, int nsys) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < nsys) dyn[s].ins_fallback = 1;
+}
+
+// Zero the output flags of the systems still iterating.
+__global__ void k_ins_zero_open(const SysDyn *__restrict__ dyn, const int *__restrict__ sys_of, int *f, long long T) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= T) return;
+  if (!dyn[sys_of[g]].ins_conv) f[g] = 0;
+}
+
+// Count, per system still iterating, the positions where H and H' differ.
+__global__ void k_ins_compare(SysDyn *dyn, const int *__restrict__ sys_of, const int *__restrict__ fin,
+                              const int *__restrict__ fout, long long T) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= T || fin[g] == fout[g]) return;
+  const int s = sys_of[g];
+  if (!dyn[s].ins_conv) atomicAdd(&dyn[s].ins_mismatch, 1);
+}
+
+// A system whose H' equals H has converged (iteration `it`, counted from 1).
+__global__ void k_ins_converge(SysDyn *dyn, int nsys, int it, int last) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys) return;
+  SysDyn &d = dyn[s];
+  if (d.ins_conv || d.ins_fallback) return;
+  if (d.ins_mismatch == 0) {
+    d.ins_conv = 1;
+    d.diag[6] = it;
+  } else if (last) {
+    d.ins_fallback = 1;
+    d.diag[6] = it;
+  }
+  d.ins_mismatch = 0;
+}
+
+// Apply every insertion (links, new point state) and log the events in sweep order: one
+// thread per original insertion, following its sub-chain.
 __global__ void k_ins_apply(const SysConst *__restrict__ scs, SysDyn *dyn, const int *__restrict__ sys_of, State S,
-                            const int *__restrict__ pos_c, const int *__restrict__ list_c, const int *__restrict__ newslot,
-                            const double *__restrict__ xnew, const int *__restrict__ nev_total, DevEvent *ev,
-                            int *ev_count, int ev_cap, const unsigned *err) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= *nev_total || *err) return;
-  const int k = list_c[e];
+                            const int *__restrict__ pos_c, const int *__restrict__ list_c,
+                            const int *__restrict__ pos_h, const int *__restrict__ fh,
+                            const int *__restrict__ newslot, const int *__restrict__ segnx,
+                            const double *__restrict__ xnew, const double *__restrict__ unew,
+                            const int *__restrict__ nev_total, DevEvent *ev, int *ev_count, int ev_cap,
+                            unsigned *err) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= *nev_total || *err) return;
+  const int k = list_c[t];
   const int s = sys_of[k];
   if (dyn[s].ins_fallback) return;
   const SysConst &sc = scs[s];
   const long long T = S.T;
-  const int slot = newslot[k];
-  const int nx = S.nxt[k];
-  double ui[3], un[3], xn[3], zero[3] = {0, 0, 0};
-  load3(S.U, T, k, ui);
-  load3(S.U, T, nx, un);
-  for (int c = 0; c < 3; ++c) {
-    un[c] = e_mul(0.5, e_add(ui[c], un[c]));
-    xn[c] = xnew[c * T + k];
+  const int ev0 = pos_c[sc.base], h0 = pos_h[sc.base];
+  const int seq0 = dyn[s].event_seq, itime = dyn[s].itime;
+  const int nx = segnx[k];
+  const double zero[3] = {0, 0, 0};
+  int g = k;
+  for (int hops = 0;; ++hops) {
+    if (hops > sc.cap) {  // a sub-chain is shorter than the free slots; guard only
+      atomicOr(err, DERR_QUEUE);
+      return;
+    }
+    const int q = newslot[g];
+    double xn[3], un[3];
+    for (int c = 0; c < 3; ++c) {
+      xn[c] = xnew[c * T + g];
+      un[c] = unew[c * T + g];
+    }
+    store3(S.X, T, q, xn);
+    store3(S.U, T, q, un);
+    store3(S.U1, T, q, zero);
+    store3(S.U2, T, q, zero);
+    S.cl[q] = 0;
+    S.CD[q] = 0;
+    S.prv[q] = g;
+    S.nxt[g] = q;
+    const int seq = seq0 + (pos_c[g] - ev0) + (pos_h[g] - h0);
+    const int a = atomicAdd(ev_count, 1);
+    if (a < ev_cap) ev[a] = DevEvent{s, seq, itime, NV_EV_INSERT, g, q};
+    if (fh[q]) {  // the sweep reaches q and it inserts
+      g = q;
+      continue;
+    }
+    S.nxt[q] = nx;
+    S.prv[nx] = q;
+    break;
   }
-  store3(S.X, T, slot, xn);
-  store3(S.U, T, slot, un);
-  store3(S.U1, T, slot, zero);
-  store3(S.U2, T, slot, zero);
-  S.cl[slot] = 0;
-  S.CD[slot] = 0;
-  S.prv[slot] = k;
-  S.nxt[slot] = nx;
-  S.prv[nx] = slot;
-  S.nxt[k] = slot;
-  const int rank = pos_c[k] - pos_c[sc.base];
-  const int seq = dyn[s].event_seq + rank;
-  const int at = atomicAdd(ev_count, 1);
-  if (at < ev_cap) ev[at] = DevEvent{s, seq, dyn[s].itime, NV_EV_INSERT, k, slot};
 }
 
 // Ghosts of every slot an insertion touched, from the final links and positions (each
 // touched slot's last refresh in the serial sweep sees exactly this state).
 __global__ void k_ins_ghosts(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn,
                              const int *__restrict__ sys_of, State S, const int *__restrict__ list_c,
-                             const int *__restrict__ newslot, const int *__restrict__ nev_total, const unsigned *err) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= *nev_total || *err) return;
-  const int k = list_c[e];
+                             const int *__restrict__ fh, const int *__restrict__ newslot,
+                             const int *__restrict__ nev_total, unsigned *err) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= *nev_total || *err) return;
+  const int k = list_c[t];
   const int s = sys_of[k];
   if (dyn[s].ins_fallback) return;
   const SysConst &sc = scs[s];
-  const int slot = newslot[k];
   refresh_ghosts(sc, S, k);
-  refresh_ghosts(sc, S, slot);
-  refresh_ghosts(sc, S, S.nxt[slot]);
+  int q = newslot[k];
+  for (int hops = 0;; ++hops) {
+    if (hops > sc.cap) {
+      atomicOr(err, DERR_QUEUE);
+      return;
+    }
+    refresh_ghosts(sc, S, q);
+    if (!fh[q]) break;
+    q = newslot[q];
+  }
+  refresh_ghosts(sc, S, S.nxt[q]);
 }
 
 // Counters: pcount grows by the insertions beyond the free slots.
 __global__ void k_ins_finish(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, const int *__restrict__ pos_c,
-                             const int *__restrict__ pos_b, unsigned *err) {
+                             const int *__restrict__ pos_h, const int *__restrict__ pos_b, unsigned *err) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys || *err) return;
   const SysConst &sc = scs[s];
@@ -640,13 +603,13 @@ __global__ void k_ins_finish(const SysConst *__restrict__ scs, SysDyn *dyn, int 
     atomicOr(err, DERR_EMPTY);
     return;
   }
-  const int nev = pos_c[sc.base + sc.cap + 1] - pos_c[sc.base];
+  const int end = sc.base + sc.cap + 1;
+  const int nhigh = pos_h[end] - pos_h[sc.base];
+  const int nev = pos_c[end] - pos_c[sc.base] + nhigh;
   d.diag[1] = nev;
-  if (d.ins_fallback) {
-    d.diag[2] += 1;
-    return;
-  }
-  const int nfree = pos_b[sc.base + sc.cap + 1] - pos_b[sc.base];
+  d.diag[5] = nhigh;
+  if (d.ins_fallback) return;
+  const int nfree = pos_b[end] - pos_b[sc.base];
   d.event_seq += nev;
   d.insert_count += nev;
   if (nev > nfree) d.pcount += nev - nfree;
@@ -660,8 +623,8 @@ __global__ void k_ins_finish(const SysConst *__restrict__ scs, SysDyn *dyn, int 
 // them in order.  A candidate's decision reads the links of i and of its partner j only
 // (nxt/prv of both; x and ghosts do not change in precon, and a cleared neighbour means a
 // cleared i or j), so the parallel decision stands unless an event earlier in the sweep
-// wrote the links of i or j -- tracked in a per-system bitmap of touched slots (shared
-// memory when it fits).  Touched candidates are decided again by lane 0 on the live state.
+// wrote the links of i or j -- tracked in a shared-memory set of touched slots.  Touched
+// candidates are decided again by lane 0 on the live state.
 
 struct ReconIn {
   int i, pari, parb, j, nj, parjb;
@@ -710,50 +673,95 @@ __device__ ReconIn recon_decide(const State &S, int i, double half_delta, int cl
   return r;
 }
 
-__device__ __forceinline__ bool bit_get(const unsigned *b, int k) { return (b[k >> 5] >> (k & 31)) & 1u; }
-__device__ __forceinline__ void bit_set(unsigned *b, int k) { b[k >> 5] |= 1u << (k & 31); }
-
-// Slots whose links an event of the current chunk wrote: bit set in `bits` and recorded
-// in `list` so that the bits can be cleared when the chunk ends (the next chunk's parallel
-// decisions are taken on the state that already includes them).
-struct Touched {
-  unsigned *bits;
-  int *list;
+// Slots written by the events of the current chunk, as an open-addressing hash set in
+// shared memory (keys are global slot indices, 0 = empty; the per-system dummy slot is
+// never recorded).  After kLimit slots the set is full and every slot counts as touched
+// until the chunk ends, so the remaining candidates are decided on the live state.
+template <int kBits, int kLimit>
+struct SlotSet {
+  static constexpr int kCap = 1 << kBits;
+  static_assert(2 * kLimit <= kCap, "load factor above one half");
+  int *keys;
   int n;
+  int full;
   int base;
-  __device__ void add(int g) {
-    if (g <= base) return;
-    const int k = g - base;
-    if (!bit_get(bits, k)) {
-      bit_set(bits, k);
-      list[n++] = k;
+  __device__ static int home(int g) { return (int)(((unsigned)g * 0x9E3779B1u) >> (32 - kBits)); }
+  // table index of g, or -1
+  __device__ int find(int g) const {
+    for (int h = home(g);; h = (h + 1) & (kCap - 1)) {
+      const int k = keys[h];
+      if (k == g) return h;
+      if (k == 0) return -1;
     }
   }
-  __device__ bool has(int g) const { return g > base && bit_get(bits, g - base); }
+  // table index of g after recording it, or -1 once the set is full
+  __device__ int add(int g) {
+    if (g <= base || full) return -1;
+    int h = home(g);
+    for (;; h = (h + 1) & (kCap - 1)) {
+      const int k = keys[h];
+      if (k == g) return h;
+      if (k == 0) break;
+    }
+    if (n == kLimit) {
+      full = 1;
+      return -1;
+    }
+    keys[h] = g;
+    ++n;
+    return h;
+  }
+  __device__ bool has(int g) const { return full || (g > base && find(g) >= 0); }
+  // warp-collective: empty the set for the next chunk (lane 0 holds n and full)
+  __device__ void reset(int lane) {
+    __syncwarp();
+    const int used = __shfl_sync(0xffffffffu, n | full, 0);
+    if (used) {
+      for (int q = lane; q < kCap; q += 32) keys[q] = 0;
+    }
+    n = 0;
+    full = 0;
+    __syncwarp();
+  }
 };
 constexpr int kTouchedPerChunk = 32 * 10;  // 4 relinked + up to 6 cleared slots per event
+using Touched = SlotSet<10, kTouchedPerChunk>;
 
-// Events of one chunk, staged in shared memory by lane 0 and written with one atomic.
+// Events of one chunk, staged in shared memory by lane 0 and written with one atomic.  A
+// chunk with more events than the stage holds spills the stage from lane 0.
+constexpr int kEventStage = 96;
 struct EventStage {
   DevEvent *buf;
   int n;
+  DevEvent *ev;
+  int *ev_count;
+  int ev_cap;
+  __device__ void spill() {
+    const int at = atomicAdd(ev_count, n);
+    for (int q = 0; q < n; ++q)
+      if (at + q < ev_cap) ev[at + q] = buf[q];
+    n = 0;
+  }
   __device__ void add(SysDyn &d, int s, int kind, int i, int j) {
+    if (n == kEventStage) spill();
     buf[n++] = DevEvent{s, d.event_seq++, d.itime, kind, i, j};
   }
 };
-__device__ void flush_events(EventStage &es, int lane, DevEvent *ev, int *ev_count, int ev_cap) {
-  int n = __shfl_sync(0xffffffffu, es.n, 0);
+__device__ void flush_events(EventStage &es, int lane) {
+  const int n = __shfl_sync(0xffffffffu, es.n, 0);
   if (n == 0) return;
   int at = 0;
-  if (lane == 0) at = atomicAdd(ev_count, n);
+  if (lane == 0) at = atomicAdd(es.ev_count, n);
   at = __shfl_sync(0xffffffffu, at, 0);
   for (int q = lane; q < n; q += 32)
-    if (at + q < ev_cap) ev[at + q] = es.buf[q];
+    if (at + q < es.ev_cap) es.ev[at + q] = es.buf[q];
   __syncwarp();
   if (lane == 0) es.n = 0;
   __syncwarp();
 }
 
+// loop_killer (reconnection.f90:155-182).  Only "fewer than 4 points" matters, so the
+// count stops after three hops; the result equals the reference's full walk.
 __device__ void loop_killer_stage(const State &S, SysDyn &d, int s, int particle, int pcount, EventStage &es,
                                   Touched &tc) {
   int counter = 1, nx = particle;
@@ -779,22 +787,18 @@ __device__ void loop_killer_stage(const State &S, SysDyn &d, int s, int particle
 
 __global__ void __launch_bounds__(32) k_recon_sweep(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S,
                                                     const int *__restrict__ pos_a, const int *__restrict__ list_a,
-                                                    unsigned *gbits, long long gbits_words_per_sys, int smem_words,
                                                     unsigned *err, DevEvent *ev, int *ev_count, int ev_cap) {
-  extern __shared__ unsigned sbits[];
-  __shared__ int tlist[kTouchedPerChunk];
-  __shared__ DevEvent ebuf[96];
+  __shared__ int tkeys[Touched::kCap];
+  __shared__ DevEvent ebuf[kEventStage];
   const int s = blockIdx.x;
   const int lane = threadIdx.x;
   if (s >= nsys || *err) return;
   const SysConst &sc = scs[s];
   if (!recon_step(sc, dyn[s])) return;
   const int base = sc.base;
-  const int nwords = (sc.cap + 1 + 31) / 32;
-  unsigned *bits = nwords <= smem_words ? sbits : gbits + (long long)s * gbits_words_per_sys;
-  for (int w = lane; w < nwords; w += 32) bits[w] = 0;
-  Touched tc{bits, tlist, 0, base};
-  EventStage es{ebuf, 0};
+  for (int q = lane; q < Touched::kCap; q += 32) tkeys[q] = 0;
+  Touched tc{tkeys, 0, 0, base};
+  EventStage es{ebuf, 0, ev, ev_count, ev_cap};
   const int li = pos_a[base], le = pos_a[base + sc.cap + 1];
   SysDyn d = dyn[s];  // lane 0's copy is the live one
   if (lane == 0) d.diag[3] = le - li;
@@ -847,14 +851,8 @@ __global__ void __launch_bounds__(32) k_recon_sweep(const SysConst *__restrict__
     }
     // the chunk's writes are now visible to the next chunk's parallel decisions
     __threadfence_block();
-    const int nt = __shfl_sync(0xffffffffu, tc.n, 0);
-    __syncwarp();
-    for (int q = lane; q < nt; q += 32) {
-      const int kk = tlist[q];
-      atomicAnd(&bits[kk >> 5], ~(1u << (kk & 31)));
-    }
-    if (lane == 0) tc.n = 0;
-    flush_events(es, lane, ev, ev_count, ev_cap);
+    tc.reset(lane);
+    flush_events(es, lane);
   }
   if (lane == 0) dyn[s] = d;
 }
@@ -868,23 +866,19 @@ __global__ void __launch_bounds__(32) k_recon_sweep(const SysConst *__restrict__
 // (the two-level bitmap).
 __global__ void __launch_bounds__(32) k_remove_sweep(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S,
                                                      const int *__restrict__ pos_a, const int *__restrict__ list_a,
-                                                     const int *__restrict__ cand, Sweep sw, unsigned *gbits,
-                                                     long long gbits_words_per_sys, int smem_words, unsigned *err,
+                                                     const int *__restrict__ cand, Sweep sw, unsigned *err,
                                                      DevEvent *ev, int *ev_count, int ev_cap) {
-  extern __shared__ unsigned sbits[];
-  __shared__ int tlist[kTouchedPerChunk];
-  __shared__ DevEvent ebuf[96];
+  __shared__ int tkeys[Touched::kCap];
+  __shared__ DevEvent ebuf[kEventStage];
   const int s = blockIdx.x;
   const int lane = threadIdx.x;
   if (s >= nsys || *err) return;
   const SysConst &sc = scs[s];
   if (!recon_step(sc, dyn[s])) return;
   const int base = sc.base;
-  const int nwords = (sc.cap + 1 + 31) / 32;
-  unsigned *bits = nwords <= smem_words ? sbits : gbits + (long long)s * gbits_words_per_sys;
-  for (int w = lane; w < nwords; w += 32) bits[w] = 0;
-  Touched tc{bits, tlist, 0, base};
-  EventStage es{ebuf, 0};
+  for (int q = lane; q < Touched::kCap; q += 32) tkeys[q] = 0;
+  Touched tc{tkeys, 0, 0, base};
+  EventStage es{ebuf, 0, ev, ev_count, ev_cap};
   const int li = pos_a[base], le = pos_a[base + sc.cap + 1];
   SysDyn d = dyn[s];
   const int lastslot = base + d.pcount;
@@ -954,18 +948,301 @@ __global__ void __launch_bounds__(32) k_remove_sweep(const SysConst *__restrict_
       }
     }
     __threadfence_block();
-    const int nt = __shfl_sync(0xffffffffu, tc.n, 0);
-    __syncwarp();
-    for (int q = lane; q < nt; q += 32) {
-      const int kk = tlist[q];
-      atomicAnd(&bits[kk >> 5], ~(1u << (kk & 31)));
-    }
-    if (lane == 0) tc.n = 0;
-    flush_events(es, lane, ev, ev_count, ev_cap);
+    tc.reset(lane);
+    flush_events(es, lane);
   }
   if (lane == 0) run_extras(lastslot);
-  flush_events(es, lane, ev, ev_count, ev_cap);
+  flush_events(es, lane);
   if (lane == 0) dyn[s] = d;
+}
+
+// ---- pinsert sweep, warp-prefetched --------------------------------------------------------
+// The reference's serial sweep (line.f90:30-93), used for a system whose step has an
+// insertion the parallel form cannot place: a new point put in a free slot that the sweep
+// reaches later and that inserts again.  Candidates (the slots whose stale or fresh test
+// passes) are taken 32 at a time; each lane decides its candidate on the state at the start
+// of the chunk and precomputes the new point, its velocity and the neighbour positions the
+// ghost refreshes need.  Lane 0 then applies the insertions in slot order.  What an
+// insertion writes -- the ghosts and links of i, infront(i) and the new point -- is mirrored
+// in a shared-memory table, so a later candidate of the same chunk whose slot or infront
+// slot was written reads its current ghosts and links from there instead of global memory.
+// New points that the sweep still reaches (free slots above their creator, up to the
+// step-start pcount) are visited as extra slots through the two-level bitmap, on the live
+// state; so are chunks whose table fills up.
+struct InsIn {
+  int k, nx, pk, nn, yes;
+  double x[3], gi[3], gb[3], xn[3], un[3], xnx[3], xpk[3], xnn[3];
+};
+
+__device__ InsIn ins_prefetch(const SysConst &sc, const State &S, int k) {
+  InsIn r;
+  r.k = k;
+  r.yes = 0;
+  r.nx = S.nxt[k];
+  if (r.nx == 0) return r;
+  const long long T = S.T;
+  load3(S.X, T, k, r.x);
+  load3(S.GI, T, k, r.gi);
+  load3(S.GB, T, k, r.gb);
+  r.pk = S.prv[k];
+  r.nn = S.nxt[r.nx];
+  load3(S.X, T, r.nx, r.xnx);
+  load3(S.X, T, r.pk, r.xpk);
+  load3(S.X, T, r.nn, r.xnn);
+  double uk[3], unx[3];
+  load3(S.U, T, k, uk);
+  load3(S.U, T, r.nx, unx);
+  for (int c = 0; c < 3; ++c) r.un[c] = e_mul(0.5, e_add(uk[c], unx[c]));
+  const double disti = dist_gen(r.x, r.gi);
+  if (disti > sc.delta) {
+    r.yes = 1;
+    new_point(r.x, r.gi, r.gb, disti, r.xn);
+  }
+  return r;
+}
+
+// the table of written slots: ghosts and links as they now stand in global memory
+struct InsTable {
+  static constexpr int kBits = 9;
+  static constexpr int kLimit = 240;
+  using Set = SlotSet<kBits, kLimit>;
+  double *gi, *gb;  // [kCap][3]
+  int *nxt, *prv;
+};
+
+__global__ void __launch_bounds__(32) k_insert_sweep(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S,
+                                                     const int *__restrict__ pos_a, const int *__restrict__ list_a,
+                                                     const int *__restrict__ pos_b, const int *__restrict__ list_b,
+                                                     Sweep sw, unsigned *err, DevEvent *ev, int *ev_count,
+                                                     int ev_cap) {
+  using Set = InsTable::Set;
+  __shared__ int tkeys[Set::kCap];
+  __shared__ double tgi[Set::kCap * 3], tgb[Set::kCap * 3];
+  __shared__ int tnxt[Set::kCap], tprv[Set::kCap];
+  __shared__ int fslot[32];
+  __shared__ DevEvent ebuf[kEventStage];
+  const int s = blockIdx.x;
+  const int lane = threadIdx.x;
+  if (s >= nsys || *err) return;
+  if (!dyn[s].ins_fallback) return;
+  const SysConst &sc = scs[s];
+  const int base = sc.base;
+  for (int q = lane; q < Set::kCap; q += 32) tkeys[q] = 0;
+  Set tc{tkeys, 0, 0, base};
+  EventStage es{ebuf, 0, ev, ev_count, ev_cap};
+  SysDyn d = dyn[s];  // lane 0's copy is the live one
+  const int old_last = base + d.pcount;  // loop bound old_pcount (line.f90:28-30)
+  const int li = pos_a[base], le = pos_a[base + sc.cap + 1];
+  const int ee = pos_b[base + sc.cap + 1];
+  const long long T = S.T;
+  int ei = pos_b[base], pc = d.pcount, extras = 0, last = base, fs0 = 0;
+  bool stop = false;
+  __syncwarp();
+
+  // mirror of slot g's ghosts and links (lane 0)
+  auto put = [&](int g, const double gi[3], const double gb[3], int nx, int pv) {
+    const int h = tc.add(g);
+    if (h < 0) return;
+    for (int c = 0; c < 3; ++c) {
+      tgi[3 * h + c] = gi[c];
+      tgb[3 * h + c] = gb[c];
+    }
+    tnxt[h] = nx;
+    tprv[h] = pv;
+  };
+  // the next free slot (line.f90:36-50): the step-start free slots in ascending order, then
+  // pcount + 1
+  auto take_slot = [&](int &slot) -> bool {
+    if (ei < ee) {
+      const int q = ei - fs0;
+      slot = (q >= 0 && q < 32) ? fslot[q] : list_b[ei];
+      ++ei;
+      return true;
+    }
+    if (pc + 1 > sc.cap) {
+      atomicOr(err, DERR_CAPACITY);
+      return false;
+    }
+    slot = base + (++pc);
+    return true;
+  };
+  auto after_insert = [&](int i, int p) {
+    es.add(d, s, NV_EV_INSERT, i, p);
+    d.insert_count++;
+    if (p > i && p <= old_last) {  // the sweep reaches the new point later
+      sw.mark(p);
+      ++extras;
+    }
+  };
+  // one visit of slot i on the live state: the reference's statements in order (lane 0)
+  auto visit_live = [&](int i) -> bool {
+    const int nx = S.nxt[i];
+    if (nx == 0) return true;
+    double x[3], gi[3], gb[3];
+    load3(S.X, T, i, x);
+    load3(S.GI, T, i, gi);
+    load3(S.GB, T, i, gb);
+    const double disti = dist_gen(x, gi);
+    if (!(disti > sc.delta)) return true;
+    int p;
+    if (!take_slot(p)) return false;
+    double xn[3], ui[3], un[3];
+    const double zero[3] = {0, 0, 0};
+    new_point(x, gi, gb, disti, xn);
+    load3(S.U, T, i, ui);
+    load3(S.U, T, nx, un);
+    for (int c = 0; c < 3; ++c) un[c] = e_mul(0.5, e_add(ui[c], un[c]));
+    store3(S.X, T, p, xn);
+    store3(S.U, T, p, un);
+    store3(S.U1, T, p, zero);
+    store3(S.U2, T, p, zero);
+    S.prv[p] = i;
+    S.nxt[p] = nx;
+    double a[3], b[3];
+    get_ghost_p(sc, S, p, a, b);
+    store3(S.GI, T, p, a);
+    store3(S.GB, T, p, b);
+    put(p, a, b, nx, i);
+    S.prv[nx] = p;
+    get_ghost_p(sc, S, nx, a, b);
+    store3(S.GI, T, nx, a);
+    store3(S.GB, T, nx, b);
+    put(nx, a, b, S.nxt[nx], p);
+    S.nxt[i] = p;
+    get_ghost_p(sc, S, i, a, b);
+    store3(S.GI, T, i, a);
+    store3(S.GB, T, i, b);
+    put(i, a, b, p, S.prv[i]);
+    after_insert(i, p);
+    return true;
+  };
+  auto run_extras = [&](int upto) -> bool {  // extra slots in (last, upto]
+    while (extras > 0) {
+      const int e = sw.next(last + 1, upto);
+      if (e == INT_MAX) break;
+      sw.unmark(e);
+      --extras;
+      last = e;
+      if (!visit_live(e)) return false;
+    }
+    return true;
+  };
+
+  for (int k0 = li; k0 < le; k0 += 32) {
+    const int k = k0 + lane;
+    InsIn in;
+    in.k = 0;
+    in.yes = 0;
+    in.nx = 0;
+    if (k < le) in = ins_prefetch(sc, S, list_a[k]);
+    fs0 = __shfl_sync(0xffffffffu, ei, 0);
+    if (fs0 + lane < ee) fslot[lane] = list_b[fs0 + lane];
+    __syncwarp();
+    const int n = min(32, le - k0);
+    for (int l = 0; l < n; ++l) {
+      // lane 0 takes candidate l from its lane (shuffles, all lanes take part)
+      const int kl = __shfl_sync(0xffffffffu, in.k, l);
+      const int nx = __shfl_sync(0xffffffffu, in.nx, l);
+      const int pk = __shfl_sync(0xffffffffu, in.pk, l);
+      const int nn = __shfl_sync(0xffffffffu, in.nn, l);
+      int yes = __shfl_sync(0xffffffffu, in.yes, l);
+      double x[3], gi[3], gb[3], xn[3], un[3], xnx[3], xpk[3], xnn[3];
+      for (int c = 0; c < 3; ++c) {
+        x[c] = __shfl_sync(0xffffffffu, in.x[c], l);
+        gi[c] = __shfl_sync(0xffffffffu, in.gi[c], l);
+        gb[c] = __shfl_sync(0xffffffffu, in.gb[c], l);
+        xn[c] = __shfl_sync(0xffffffffu, in.xn[c], l);
+        un[c] = __shfl_sync(0xffffffffu, in.un[c], l);
+        xnx[c] = __shfl_sync(0xffffffffu, in.xnx[c], l);
+        xpk[c] = __shfl_sync(0xffffffffu, in.xpk[c], l);
+        xnn[c] = __shfl_sync(0xffffffffu, in.xnn[c], l);
+      }
+      if (lane != 0 || stop) continue;
+      if (kl > old_last) {
+        stop = true;
+        continue;
+      }
+      if (!run_extras(kl - 1)) {
+        stop = true;
+        continue;
+      }
+      last = kl;
+      if (nx == 0) continue;  // free at the chunk start; pinsert frees nothing
+      const int hk = tc.full ? -1 : tc.find(kl);
+      const int hx = tc.full ? -1 : tc.find(nx);
+      if (tc.full || nx == kl || (hk >= 0 && tnxt[hk] != nx)) {
+        if (!visit_live(kl)) stop = true;
+        continue;
+      }
+      int pv = pk;
+      if (hk >= 0) {  // written earlier in this chunk: its ghosts and behind link from the table
+        for (int c = 0; c < 3; ++c) {
+          gi[c] = tgi[3 * hk + c];
+          gb[c] = tgb[3 * hk + c];
+        }
+        pv = tprv[hk];
+        const double disti = dist_gen(x, gi);
+        yes = disti > sc.delta;
+        if (yes) new_point(x, gi, gb, disti, xn);
+      }
+      if (!yes) continue;
+      int p;
+      if (!take_slot(p)) {
+        stop = true;
+        continue;
+      }
+      // the three ghost refreshes of line.f90:86-91 from known positions
+      double gip[3], gbp[3], gix[3], gbx[3], gik[3], gbk[3];
+      ghost_of(sc, xn, xnx, gip);
+      ghost_of(sc, xn, x, gbp);
+      int nnx = nn;
+      if (hx >= 0) {
+        for (int c = 0; c < 3; ++c) gix[c] = tgi[3 * hx + c];
+        nnx = tnxt[hx];
+      } else {
+        ghost_of(sc, xnx, xnn, gix);
+      }
+      ghost_of(sc, xnx, xn, gbx);
+      ghost_of(sc, x, xn, gik);
+      if (hk >= 0) {
+        for (int c = 0; c < 3; ++c) gbk[c] = gb[c];
+      } else {
+        ghost_of(sc, x, xpk, gbk);
+      }
+      const double zero[3] = {0, 0, 0};
+      store3(S.X, T, p, xn);
+      store3(S.U, T, p, un);
+      store3(S.U1, T, p, zero);
+      store3(S.U2, T, p, zero);
+      S.prv[p] = kl;
+      S.nxt[p] = nx;
+      store3(S.GI, T, p, gip);
+      store3(S.GB, T, p, gbp);
+      S.prv[nx] = p;
+      store3(S.GI, T, nx, gix);
+      store3(S.GB, T, nx, gbx);
+      S.nxt[kl] = p;
+      store3(S.GI, T, kl, gik);
+      store3(S.GB, T, kl, gbk);
+      put(p, gip, gbp, nx, kl);
+      put(nx, gix, gbx, nnx, p);
+      put(kl, gik, gbk, p, pv);
+      after_insert(kl, p);
+    }
+    stop = __shfl_sync(0xffffffffu, stop, 0);
+    // the chunk's writes are now visible to the next chunk's prefetch
+    __threadfence_block();
+    tc.reset(lane);
+    flush_events(es, lane);
+    if (stop) break;
+  }
+  if (lane == 0 && !stop) run_extras(old_last);
+  flush_events(es, lane);
+  if (lane == 0) {
+    d.pcount = pc;
+    d.diag[2] += 1;
+    dyn[s] = d;
+  }
 }
 
 State make_state(nv_handle *h) {
@@ -1008,22 +1285,12 @@ void topo_alloc(nv_handle *h) {
   cudaMalloc(&tb->dec, n * sizeof(int));
   cudaMalloc(&tb->newslot, n * sizeof(int));
   cudaMalloc(&tb->xnew, 3 * n * sizeof(double));
+  cudaMalloc(&tb->unew, 3 * n * sizeof(double));
+  cudaMalloc(&tb->segnx, n * sizeof(int));
+  cudaMalloc(&tb->fh[0], n * sizeof(int));
+  cudaMalloc(&tb->fh[1], n * sizeof(int));
+  cudaMalloc(&tb->pos_h, n * sizeof(int));
   cudaMalloc(&tb->l0, (n / 32 + 2) * sizeof(unsigned));
-  {
-    // touched-slot bitmaps: shared memory up to the device's opt-in limit, else global
-    int dev = 0, optin = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const int maxwords = (h->max_cap + 1 + 31) / 32;
-    tb->smem_words = std::min(maxwords, std::max(0, optin - 4096) / 4);
-    if (tb->smem_words < maxwords) {
-      tb->touched_words = maxwords;
-      cudaMalloc(&tb->touched, (size_t)h->nsys * maxwords * sizeof(unsigned));
-    }
-    const int smem = tb->smem_words * (int)sizeof(unsigned);
-    cudaFuncSetAttribute(k_recon_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_remove_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  }
   cudaMalloc(&tb->l1, (n / 1024 + 2) * sizeof(unsigned));
   cub::DeviceScan::ExclusiveSum(nullptr, tb->cub_bytes, tb->flag_a, tb->pos_a, (int)n);
   cudaMalloc(&tb->cub_tmp, std::max<size_t>(tb->cub_bytes, 16));
@@ -1037,8 +1304,8 @@ void topo_free(nv_handle *h) {
   cudaFree(tb->flag_b); cudaFree(tb->pos_b); cudaFree(tb->list_b);
   cudaFree(tb->flag_c); cudaFree(tb->pos_c); cudaFree(tb->list_c);
   cudaFree(tb->dec); cudaFree(tb->newslot); cudaFree(tb->xnew);
+  cudaFree(tb->unew); cudaFree(tb->segnx); cudaFree(tb->fh[0]); cudaFree(tb->fh[1]); cudaFree(tb->pos_h);
   cudaFree(tb->l0); cudaFree(tb->l1);
-  if (tb->touched) cudaFree(tb->touched);
   cudaFree(tb->cub_tmp);
   delete tb;
   h->topo = nullptr;
@@ -1067,16 +1334,39 @@ void launch_pinsert(nv_handle *h) {
   // slot, threads beyond the count return at once
   const int grid = grid_for(T, 128);
   const int *nev = tb->pos_c + T;
-  k_ins_points<<<grid, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, S, tb->pos_c, tb->list_c, tb->pos_b,
-                                            tb->list_b, tb->dec, tb->newslot, tb->xnew, nev, h->d_err);
-  k_ins_apply<<<grid, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, S, tb->pos_c, tb->list_c, tb->newslot,
-                                           tb->xnew, nev, h->d_events, h->d_event_count, h->event_cap, h->d_err);
-  k_ins_ghosts<<<grid, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, S, tb->list_c, tb->newslot, nev, h->d_err);
-  k_ins_finish<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, tb->pos_c, tb->pos_b,
-                                                              h->d_err);
-  const Sweep sw = make_sweep(h, tb->flag_a);
-  k_insert_resolve<<<resolver_grid(h), 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, S, sw, tb->pos_b, tb->list_b,
-                                                           h->d_err, h->d_events, h->d_event_count, h->event_cap, 1);
+  const int iters = h->ins_iters;
+  k_zero_flags<<<grid_for(T + 1, TB), TB, 0, h->stream>>>(tb->fh[0], T);
+  if (iters == 0) {
+    k_ins_all_serial<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_dyn, h->nsys);
+    size_t bytes = tb->cub_bytes;
+    cub::DeviceScan::ExclusiveSum(tb->cub_tmp, bytes, tb->fh[0], tb->pos_h, (int)(T + 1), h->stream);
+  }
+  for (int it = 0; it < iters; ++it) {
+    int *fin = tb->fh[it & 1], *fout = tb->fh[(it + 1) & 1];
+    k_ins_zero_open<<<grid_for(T, TB), TB, 0, h->stream>>>(h->d_dyn, h->sys_of, fout, T);
+    size_t bytes = tb->cub_bytes;
+    cub::DeviceScan::ExclusiveSum(tb->cub_tmp, bytes, fin, tb->pos_h, (int)(T + 1), h->stream);
+    k_ins_chain<<<grid, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, S, tb->pos_c, tb->list_c, tb->pos_b,
+                                             tb->list_b, tb->dec, tb->pos_h, fout, tb->newslot, tb->segnx, tb->xnew,
+                                             tb->unew, nev, h->d_err);
+    k_ins_compare<<<grid_for(T, TB), TB, 0, h->stream>>>(h->d_dyn, h->sys_of, fin, fout, T);
+    k_ins_converge<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_dyn, h->nsys, it + 1, it + 1 == iters);
+  }
+  const int *fh = tb->fh[iters > 0 ? (iters - 1) & 1 : 0];  // pos_h is its prefix sum
+  k_ins_apply<<<grid, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, S, tb->pos_c, tb->list_c, tb->pos_h, fh,
+                                           tb->newslot, tb->segnx, tb->xnew, tb->unew, nev, h->d_events,
+                                           h->d_event_count, h->event_cap, h->d_err);
+  k_ins_ghosts<<<grid, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, S, tb->list_c, fh, tb->newslot, nev,
+                                            h->d_err);
+  k_ins_finish<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, tb->pos_c, tb->pos_h,
+                                                              tb->pos_b, h->d_err);
+  // systems with an insertion the parallel form cannot place: the sweep (extra visits start
+  // empty: bitmaps from an all-zero flag array; flag_b is free once the free slots are listed)
+  k_zero_flags<<<grid_for(T + 1, TB), TB, 0, h->stream>>>(tb->flag_b, T);
+  const Sweep sw = make_sweep(h, tb->flag_b);
+  k_insert_sweep<<<h->nsys, 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, S, tb->pos_a, tb->list_a, tb->pos_b,
+                                                tb->list_b, sw, h->d_err, h->d_events, h->d_event_count,
+                                                h->event_cap);
 }
 
 void launch_pclose(nv_handle *h, bool only_brute) {
@@ -1093,10 +1383,8 @@ void launch_precon(nv_handle *h) {
   k_mark_recon<<<grid_for(h->T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->closestd, h->nxt,
                                                               tb->flag_a, h->T, h->d_err);
   compact(h, tb->flag_a, tb->pos_a, tb->list_a);
-  const size_t smem = (size_t)tb->smem_words * sizeof(unsigned);
-  k_recon_sweep<<<h->nsys, 32, smem, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a, tb->list_a,
-                                                  tb->touched, tb->touched_words, tb->smem_words, h->d_err,
-                                                  h->d_events, h->d_event_count, h->event_cap);
+  k_recon_sweep<<<h->nsys, 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a, tb->list_a,
+                                               h->d_err, h->d_events, h->d_event_count, h->event_cap);
 }
 
 void launch_premove(nv_handle *h) {
@@ -1107,8 +1395,7 @@ void launch_premove(nv_handle *h) {
   // extra visits start empty: bitmaps from an all-zero flag array
   k_zero_flags<<<grid_for(h->T + 1, TB), TB, 0, h->stream>>>(tb->flag_b, h->T);
   const Sweep sw = make_sweep(h, tb->flag_b);
-  const size_t smem = (size_t)tb->smem_words * sizeof(unsigned);
-  k_remove_sweep<<<h->nsys, 32, smem, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a, tb->list_a,
-                                                   tb->flag_a, sw, tb->touched, tb->touched_words, tb->smem_words,
-                                                   h->d_err, h->d_events, h->d_event_count, h->event_cap);
+  k_remove_sweep<<<h->nsys, 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a, tb->list_a,
+                                                tb->flag_a, sw, h->d_err, h->d_events, h->d_event_count,
+                                                h->event_cap);
 }

@@ -30,9 +30,11 @@ def _assert_same(a: State, b: State):
         assert np.array_equal(getattr(a, name), getattr(b, name)), name
 
 
-def _run_stage(p, st, stages, cap_extra=512):
+def _run_stage(p, st, stages, cap_extra=512, insert_iterations=None, diag=None):
     from nuvort_b200.api import Handle
     h = Handle(p, [st.pcount + cap_extra], states=[st])
+    if insert_iterations is not None:
+        h.set_insert_iterations(insert_iterations)
     h.set_clock(0, 0.0, 1)
     o = Oracle(p, st, t=0.0, itime=1)
     for s in stages:
@@ -41,6 +43,8 @@ def _run_stage(p, st, stages, cap_extra=512):
     a, b = h.download(), o.download()
     ea, eb = h.events(), o.events()
     ca, cb = h.counters(), o.counters()
+    if diag is not None:
+        diag.extend(h.diagnostics(0))
     h.close()
     return a, b, ea, eb, ca, cb
 
@@ -138,7 +142,8 @@ def test_whole_steps_config0_events_identical():
     h.close()
 
 
-def test_pinsert_new_points_revisited_fall_back_to_serial_order():
+@pytest.mark.parametrize("iters", [6, 0])
+def test_pinsert_new_points_revisited(iters):
     # chords near 0.002 with delta 0.0009: every segment inserts and each new midpoint is
     # itself longer than delta from its infront.  Emptying the last ring puts free slots
     # above the inserting points, so the sweep reaches those new points and inserts again.
@@ -149,6 +154,50 @@ def test_pinsert_new_points_revisited_fall_back_to_serial_order():
     st.behind[start - 1:] = 0
     mv = _moved_state(config0_params(), st)
     p_ins = config0_params(delta=0.0009, overide_timestep_check=True)
-    a, b, ea, eb, ca, cb = _run_stage(p_ins, mv, ["pinsert"], cap_extra=8192)
+    diag = []
+    a, b, ea, eb, ca, cb = _run_stage(p_ins, mv, ["pinsert"], cap_extra=8192, insert_iterations=iters, diag=diag)
     assert ea == eb
     _assert_same(a, b)
+    # the fixed-point rounds place the new points' own insertions; 0 rounds: serial sweep
+    assert diag[2] == (1 if iters == 0 else 0)
+    assert iters == 0 or diag[5] > 0
+
+
+def _ring_slots(st: State):
+    """Slots (1-based) of each loop, in order of their lowest slot."""
+    seen = np.zeros(st.pcount + 1, bool)
+    rings = []
+    for s in range(1, st.pcount + 1):
+        if seen[s] or st.infront[s - 1] == 0:
+            continue
+        ring, k = [], s
+        while not seen[k]:
+            seen[k] = True
+            ring.append(k)
+            k = int(st.infront[k - 1])
+        rings.append(sorted(ring))
+    return rings
+
+
+@pytest.mark.parametrize("iters", [6, 0])
+def test_pinsert_interleaved_free_slots_second_order(iters):
+    # every third loop emptied: the free slots lie between live loops, so new points are
+    # placed just above the loops that create them and the sweep reaches them (and their
+    # own new points) between ordinary candidates, many per chunk of 32 candidates
+    st = tangle(31, 0.002, n_rings=12)
+    for r in _ring_slots(st)[2::3]:
+        idx = np.asarray(r) - 1
+        for name in ("x", "u", "u1", "u2", "ghosti", "ghostb"):
+            getattr(st, name)[idx] = 0
+        st.infront[idx] = 0
+        st.behind[idx] = 0
+    mv = _moved_state(config0_params(), st)
+    p_ins = config0_params(delta=0.0009, overide_timestep_check=True)
+    diag = []
+    a, b, ea, eb, ca, cb = _run_stage(p_ins, mv, ["pinsert"], cap_extra=16384, insert_iterations=iters, diag=diag)
+    assert len(eb) > 200
+    assert diag[2] == (1 if iters == 0 else 0)
+    assert iters == 0 or diag[5] > 100
+    assert ea == eb
+    _assert_same(a, b)
+    assert ca.insert_count == cb.insert_count and ca.pcount == cb.pcount
