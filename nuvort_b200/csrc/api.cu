@@ -404,7 +404,10 @@ int nv_create(const nv_params *params, int32_t nsys, const int32_t *capacity, in
     return code;
   };
   if ((rc = set_device(h)) != NV_OK) return bail(rc);
-  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->join_ev, cudaEventDisableTiming) != cudaSuccess)
     return bail(set_error(NV_ERR_CUDA, "stream creation failed"));
   const long long T = h->T;
   if ((rc = dalloc(&h->d_sc, nsys)) || (rc = dalloc(&h->d_dyn, nsys)) || (rc = dalloc(&h->x, 3 * T)) ||
@@ -456,6 +459,9 @@ int nv_destroy(nv_handle *h) {
     if (p) cudaFree(p);
   for (auto &e : h->ev)
     if (e) cudaEventDestroy(e);
+  if (h->fork_ev) cudaEventDestroy(h->fork_ev);
+  if (h->join_ev) cudaEventDestroy(h->join_ev);
+  if (h->side) cudaStreamDestroy(h->side);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return NV_OK;

@@ -185,11 +185,6 @@ __global__ void k_scatter(const int *__restrict__ flag, const int *__restrict__ 
   if (g < T && flag[g]) list[pos[g]] = (int)g;
 }
 
-__global__ void k_zero_live(SysDyn *dyn, int nsys) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < nsys) dyn[s].live = 0;
-}
-
 // precon (reconnection.f90:11-61).
 __device__ void norm_tanf(const State &S, int g, double t[3]) {  // general.f90:106-117
   double x[3], gi[3], gb[3];
@@ -318,27 +313,39 @@ __global__ void k_ins_decide_easy(const int *__restrict__ list_a, const int *__r
   else famb[k] = 1;
 }
 
-// Ambiguous slots in ascending order, one thread per system (their predecessors' outcomes
-// are final: decided in parallel, or earlier in this pass).
-__global__ void k_ins_decide_amb(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, const int *__restrict__ prv,
-                                 const int *__restrict__ pos_m, const int *__restrict__ list_m,
-                                 const int *__restrict__ pos_a, int *dec, const unsigned *err) {
+// Ambiguous slots.  The outcome of ambiguous k is its fresh test when p = behind(k) < k
+// inserts, else its stale test; p's outcome is final unless p is ambiguous too.  So the
+// ambiguous slots form chains k -> infront(k) (while infront(k) > k is ambiguous), each
+// starting at a slot whose predecessor is decided or lies above it.  One thread per
+// ambiguous slot; the chain heads walk their chains.
+__global__ void k_ins_decide_amb(const int *__restrict__ list_m, const int *__restrict__ n_ptr,
+                                 const int *__restrict__ nxt, const int *__restrict__ prv,
+                                 const int *__restrict__ famb, int *dec, const unsigned *err) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= *n_ptr || *err) return;
+  int k = list_m[t];
+  const int p = prv[k];
+  if (p < k && famb[p]) return;  // inside a chain: its head decides it
+  int refreshed = p < k && (dec[p] & 4);
+  for (;;) {
+    const int dv = dec[k];
+    const int d = refreshed ? (dv >> 1) & 1 : dv & 1;
+    dec[k] = dv | (d << 2);
+    const int nx = nxt[k];
+    if (!(nx > k && famb[nx])) break;
+    refreshed = d;
+    k = nx;
+  }
+}
+
+// Per-system state of a pinsert: flags of the fixed-point iteration, live marker.
+__global__ void k_ins_begin(SysDyn *dyn, int nsys) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nsys || *err) return;
-  const SysConst &sc = scs[s];
+  if (s >= nsys) return;
+  dyn[s].live = 0;
   dyn[s].ins_fallback = 0;
   dyn[s].ins_conv = 0;
   dyn[s].ins_mismatch = 0;
-  dyn[s].diag[0] = pos_a[sc.base + sc.cap + 1] - pos_a[sc.base];
-  const int mi = pos_m[sc.base], me = pos_m[sc.base + sc.cap + 1];
-  for (int idx = mi; idx < me; ++idx) {
-    const int k = list_m[idx];
-    const int dv = dec[k];
-    const int p = prv[k];
-    const bool caseA = p < k && (dec[p] & 4);
-    const int d = caseA ? (dv >> 1) & 1 : dv & 1;
-    dec[k] = dv | (d << 2);
-  }
 }
 
 // Case A (ghosts refreshed by the predecessor's insertion) and the insertion flags.
@@ -593,8 +600,9 @@ __global__ void k_ins_ghosts(const SysConst *__restrict__ scs, const SysDyn *__r
 }
 
 // Counters: pcount grows by the insertions beyond the free slots.
-__global__ void k_ins_finish(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, const int *__restrict__ pos_c,
-                             const int *__restrict__ pos_h, const int *__restrict__ pos_b, unsigned *err) {
+__global__ void k_ins_finish(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, const int *__restrict__ pos_a,
+                             const int *__restrict__ pos_c, const int *__restrict__ pos_h,
+                             const int *__restrict__ pos_b, unsigned *err) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys || *err) return;
   const SysConst &sc = scs[s];
@@ -604,6 +612,7 @@ __global__ void k_ins_finish(const SysConst *__restrict__ scs, SysDyn *dyn, int 
     return;
   }
   const int end = sc.base + sc.cap + 1;
+  d.diag[0] = pos_a[end] - pos_a[sc.base];
   const int nhigh = pos_h[end] - pos_h[sc.base];
   const int nev = pos_c[end] - pos_c[sc.base] + nhigh;
   d.diag[1] = nev;
@@ -785,6 +794,24 @@ __device__ void loop_killer_stage(const State &S, SysDyn &d, int s, int particle
   }
 }
 
+// loop_killer's count (up to three hops) on links read from a small override table first
+// (the links an event just rewrote and links prefetched before it), global memory after.
+template <int N>
+__device__ int loop_count(const State &S, int particle, int pcount, const int (&key)[N], const int (&val)[N]) {
+  int counter = 1, nx = particle;
+  const int hops = pcount < 3 ? pcount : 3;
+  for (int it = 0; it < hops; ++it) {
+    int nn = -1;
+#pragma unroll
+    for (int q = 0; q < N; ++q)
+      if (nn < 0 && key[q] == nx) nn = val[q];
+    nx = nn >= 0 ? nn : S.nxt[nx];
+    if (nx == particle) break;
+    counter++;
+  }
+  return counter;
+}
+
 __global__ void __launch_bounds__(32) k_recon_sweep(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S,
                                                     const int *__restrict__ pos_a, const int *__restrict__ list_a,
                                                     unsigned *err, DevEvent *ev, int *ev_count, int ev_cap) {
@@ -809,9 +836,16 @@ __global__ void __launch_bounds__(32) k_recon_sweep(const SysConst *__restrict__
     ReconIn in;
     in.yes = -1;
     in.i = 0;
+    int a1 = 0, a2 = 0, a3 = 0, b2 = 0;  // links the two loop_killer walks follow
     if (k < le) {
       const int i = list_a[k];
       in = recon_decide(S, i, half_delta, S.cl[i]);
+      if (in.yes == 1) {
+        a1 = S.nxt[in.pari];
+        b2 = S.nxt[in.nj];
+        a2 = S.nxt[a1];
+        a3 = S.nxt[a2];
+      }
     }
     __syncwarp();
     const int n = min(32, le - k0);
@@ -821,8 +855,15 @@ __global__ void __launch_bounds__(32) k_recon_sweep(const SysConst *__restrict__
       int pari = __shfl_sync(0xffffffffu, in.pari, l);
       int j = __shfl_sync(0xffffffffu, in.j, l);
       int parjb = __shfl_sync(0xffffffffu, in.parjb, l);
+      const int nj = __shfl_sync(0xffffffffu, in.nj, l);
+      const int a1l = __shfl_sync(0xffffffffu, a1, l);
+      const int a2l = __shfl_sync(0xffffffffu, a2, l);
+      const int a3l = __shfl_sync(0xffffffffu, a3, l);
+      const int b2l = __shfl_sync(0xffffffffu, b2, l);
       if (lane == 0) {
+        bool live = false;
         if (tc.has(i) || tc.has(j)) {
+          live = true;
           // an earlier event wrote the links of i or j: decide again on the live state
           if (S.nxt[i] == 0) {
             yes = -1;
@@ -834,6 +875,8 @@ __global__ void __launch_bounds__(32) k_recon_sweep(const SysConst *__restrict__
           }
         }
         if (yes == 1) {
+          // the walks' links as prefetched, unless an earlier event of the chunk wrote them
+          live = live || tc.has(pari) || tc.has(a1l) || tc.has(a2l) || tc.has(nj);
           d.recon_count++;
           es.add(d, s, NV_EV_RECON, i, j);
           S.nxt[parjb] = pari;
@@ -844,8 +887,20 @@ __global__ void __launch_bounds__(32) k_recon_sweep(const SysConst *__restrict__
           tc.add(j);
           tc.add(pari);
           tc.add(parjb);
-          loop_killer_stage(S, d, s, pari, d.pcount, es, tc);
-          loop_killer_stage(S, d, s, i, d.pcount, es, tc);
+          bool killed = false;
+          if (live) {
+            loop_killer_stage(S, d, s, pari, d.pcount, es, tc);
+            loop_killer_stage(S, d, s, i, d.pcount, es, tc);
+          } else {
+            const int key[7] = {parjb, i, pari, a1l, a2l, j, nj};
+            const int val[7] = {pari, j, a1l, a2l, a3l, nj, b2l};
+            if (loop_count(S, pari, d.pcount, key, val) < 4) {
+              loop_killer_stage(S, d, s, pari, d.pcount, es, tc);
+              killed = true;
+            }
+            if (killed || loop_count(S, i, d.pcount, key, val) < 4)
+              loop_killer_stage(S, d, s, i, d.pcount, es, tc);
+          }
         }
       }
     }
@@ -921,18 +976,47 @@ __global__ void __launch_bounds__(32) k_remove_sweep(const SysConst *__restrict_
       visit(e);
     }
   };
+  // a removal decided on the prefetched links (i, infront and the walk's links untouched)
+  auto remove_fast = [&](int i, int infront, int tinfront, int c1, int c2, int pv, int pcand) {
+    S.prv[tinfront] = i;
+    S.nxt[i] = tinfront;
+    tc.add(i);
+    tc.add(infront);
+    tc.add(tinfront);
+    clear_particle(S, infront);
+    es.add(d, s, NV_EV_REMOVE, i, infront);
+    const int key[4] = {i, infront, tinfront, c1};  // infront is cleared: no infront link
+    const int val[4] = {tinfront, 0, c1, c2};
+    int p = pv, pc = pcand;
+    if (loop_count(S, i, d.pcount, key, val) < 4) {
+      loop_killer_stage(S, d, s, i, d.pcount, es, tc);
+      p = S.prv[i];
+      pc = p > i && p <= lastslot ? cand[p] : 1;
+    }
+    d.remove_count++;
+    if (p > i && p <= lastslot && !pc) {
+      sw.mark(p);
+      ++extras;
+    }
+  };
   for (int k0 = li; k0 < le; k0 += 32) {
     const int k = k0 + lane;
-    int i = 0, inf = 0, yes = 0;
+    int i = 0, inf = 0, yes = 0, tinf = 0, c1 = 0, c2 = 0, pv = 0, pcand = 1;
     if (k < le) {
       i = list_a[k];
       inf = S.nxt[i];
       if (inf) {
-        const int tinf = S.nxt[inf];
+        tinf = S.nxt[inf];
         double xi[3], xt[3];
         load3(S.X, T, i, xi);
         load3(S.X, T, tinf, xt);
         yes = dist_gen(xi, xt) < thr;
+        if (yes) {
+          pv = S.prv[i];
+          c1 = S.nxt[tinf];
+          if (pv > i && pv <= lastslot) pcand = cand[pv];
+          c2 = S.nxt[c1];
+        }
       }
     }
     __syncwarp();
@@ -941,10 +1025,20 @@ __global__ void __launch_bounds__(32) k_remove_sweep(const SysConst *__restrict_
       const int il = __shfl_sync(0xffffffffu, i, l);
       const int infl = __shfl_sync(0xffffffffu, inf, l);
       const int yl = __shfl_sync(0xffffffffu, yes, l);
+      const int tl = __shfl_sync(0xffffffffu, tinf, l);
+      const int c1l = __shfl_sync(0xffffffffu, c1, l);
+      const int c2l = __shfl_sync(0xffffffffu, c2, l);
+      const int pvl = __shfl_sync(0xffffffffu, pv, l);
+      const int pcl = __shfl_sync(0xffffffffu, pcand, l);
       if (lane == 0) {
         run_extras(il - 1);
         last = il;
-        if (tc.has(il) || tc.has(infl) || yl) visit(il);
+        if (tc.has(il) || tc.has(infl)) {
+          visit(il);  // an earlier event wrote i's or infront's links: the live state decides
+        } else if (yl) {
+          if (tc.has(tl) || tc.has(c1l)) visit(il);
+          else remove_fast(il, infl, tl, c1l, c2l, pvl, pcl);
+        }
       }
     }
     __threadfence_block();
@@ -1256,7 +1350,6 @@ void compact(nv_handle *h, int *flag, int *pos, int *list) {
   k_scatter<<<grid_for(h->T, TB), TB, 0, h->stream>>>(flag, pos, list, h->T);
 }
 
-int resolver_grid(nv_handle *h) { return grid_for(h->nsys, 32); }
 
 // Sweep bitmaps from a flag array.
 Sweep make_sweep(nv_handle *h, const int *flag) {
@@ -1314,7 +1407,7 @@ void topo_free(nv_handle *h) {
 void launch_pinsert(nv_handle *h) {
   TopoBuffers *tb = h->topo;
   const long long T = h->T;
-  k_zero_live<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_dyn, h->nsys);
+  k_ins_begin<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_dyn, h->nsys);
   k_ins_mark<<<grid_for(T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->gi, h->nxt,
                                                          tb->flag_a, tb->flag_b, tb->dec, T, h->d_err);
   compact(h, tb->flag_a, tb->pos_a, tb->list_a);  // candidates (either test passes)
@@ -1323,8 +1416,8 @@ void launch_pinsert(nv_handle *h) {
   const int *ncand = tb->pos_a + T;
   k_ins_decide_easy<<<grid_for(T, 128), 128, 0, h->stream>>>(tb->list_a, ncand, tb->dec, tb->flag_c, h->d_err);
   compact(h, tb->flag_c, tb->pos_c, tb->list_c);  // ambiguous slots
-  k_ins_decide_amb<<<resolver_grid(h), 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, h->prv, tb->pos_c, tb->list_c,
-                                                           tb->pos_a, tb->dec, h->d_err);
+  k_ins_decide_amb<<<grid_for(T, 128), 128, 0, h->stream>>>(tb->list_c, tb->pos_c + T, h->nxt, h->prv, tb->flag_c,
+                                                            tb->dec, h->d_err);
   k_zero_flags<<<grid_for(T + 1, TB), TB, 0, h->stream>>>(tb->flag_c, T);
   k_ins_decide_case<<<grid_for(T, 128), 128, 0, h->stream>>>(tb->list_a, ncand, h->prv, tb->dec, tb->flag_c,
                                                              h->d_err);
@@ -1358,8 +1451,8 @@ void launch_pinsert(nv_handle *h) {
                                            h->d_event_count, h->event_cap, h->d_err);
   k_ins_ghosts<<<grid, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, S, tb->list_c, fh, tb->newslot, nev,
                                             h->d_err);
-  k_ins_finish<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, tb->pos_c, tb->pos_h,
-                                                              tb->pos_b, h->d_err);
+  k_ins_finish<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, tb->pos_a, tb->pos_c,
+                                                              tb->pos_h, tb->pos_b, h->d_err);
   // systems with an insertion the parallel form cannot place: the sweep (extra visits start
   // empty: bitmaps from an all-zero flag array; flag_b is free once the free slots are listed)
   k_zero_flags<<<grid_for(T + 1, TB), TB, 0, h->stream>>>(tb->flag_b, T);

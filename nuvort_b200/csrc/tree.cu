@@ -26,6 +26,8 @@
 constexpr int kMaxLevels = NV_TREE_MAX_DEPTH;
 constexpr int kEnd = -1;
 constexpr int kBigNode = 2048;  // nodes with more members are split by a whole block
+constexpr int kBlockSumNode = 8192;  // nodes with more members are summed by a whole block
+constexpr int kCtrBig = kMaxLevels + 6;  // ctr[kCtrBig]: entries of the block-summed node list
 constexpr int kFlush = 16;      // FP32 far-field terms summed before promotion to FP64
 constexpr float kLineGuard = 0.01f;  // (perpendicular distance / nearer end distance)^2 below
                                      // which a far interaction is evaluated in FP64
@@ -41,6 +43,8 @@ struct TreeBuffers {
   int *nDepth = nullptr;
   int *nLeaf = nullptr;
   int *members = nullptr;
+  int *bigl = nullptr;    // non-root nodes with more than kBlockSumNode members
+  int max_big = 0;
   int *ctr = nullptr;     // [0] n_nodes [1] n_members [2 + L] first node of level L
   int *flag = nullptr, *pos = nullptr;
   void *cub_tmp = nullptr;
@@ -82,6 +86,7 @@ __global__ void k_roots(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys,
     tb.ctr[2] = 0;
     tb.ctr[3] = nsys;
     tb.ctr[1] = pos[T];
+    tb.ctr[kCtrBig] = 0;
   }
   if (s >= nsys) return;
   const SysConst &sc = scs[s];
@@ -170,6 +175,11 @@ __device__ void make_children(TreeBuffers &tb, int p, const int cnt[8], int *id0
     tb.nI[id] = make_int4(cnt[d], kEnd, last ? Ip.z : id + 1, 0);
     tb.nR[id] = make_int2(mb0 + off, cnt[d]);
     tb.nDepth[id] = depth;
+    if (cnt[d] > kBlockSumNode) {
+      const int b = atomicAdd(&tb.ctr[kCtrBig], 1);
+      if (b < tb.max_big) tb.bigl[b] = id;
+      else atomicOr(err, DERR_TREE_NODES);
+    }
     off += cnt[d];
     ++k;
   }
@@ -376,10 +386,10 @@ __device__ __forceinline__ void finish_node(TreeBuffers &tb, int id, bool root, 
 __global__ void k_node_sums_small(const double *__restrict__ X, const double *__restrict__ GI,
                                   const int *__restrict__ nxt, long long T, TreeBuffers tb, int nsys, unsigned *err) {
   const int n = tb.ctr[0];
-  for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
+  for (int id = nsys + blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
     const int2 R = tb.nR[id];
     if (R.y > kSmallNode) continue;
-    const bool root = id < nsys;
+    const bool root = false;
     double cx = 0, cy = 0, cz = 0, qx = 0, qy = 0, qz = 0;
     for (int k = 0; k < R.y; ++k) {
       const int g = tb.members[R.x + k];
@@ -397,57 +407,212 @@ __global__ void k_node_sums_small(const double *__restrict__ X, const double *__
   }
 }
 
-// Larger nodes: one warp each.  The warp gathers 32 members' coordinates and ghosts into
-// shared memory; lanes 0-2 then add the three centre components and lanes 3-5 the three
-// circulation components, each in ascending member order -- the same sequence of roundings
-// as the reference's loop.  The next chunk's loads are issued before the adds.
-__global__ void __launch_bounds__(128) k_node_sums_big(const double *__restrict__ X, const double *__restrict__ GI,
-                                                       const int *__restrict__ nxt, long long T, TreeBuffers tb,
-                                                       int nsys, unsigned *err) {
-  __shared__ double sm[4][6][32];
-  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  const int n = tb.ctr[0];
-  double (*buf)[32] = sm[wl];
-  for (int id = warp; id < n; id += nwarps) {
-    const int2 R = tb.nR[id];
-    if (R.y <= kSmallNode) continue;
-    const bool root = id < nsys;
-    double acc = 0;  // lane c < 3: centre c; lane 3 + c: circulation c
-    double v[6];
-    auto gather = [&](int k0) {
-      const int k = k0 + lane;
-      if (k < R.y) {
-        const int g = tb.members[R.x + k];
-        v[0] = __ldg(X + g);
-        v[1] = __ldg(X + T + g);
-        v[2] = __ldg(X + 2 * T + g);
+// Sequential sums of one node by one warp: the warp gathers 32 members' coordinates and
+// ghosts (coalesced member reads) into shared memory; lanes 0-2 then add the three centre
+// components and lanes 3-5 the three circulation components, each in ascending member order
+// -- the reference loop's sequence of roundings.  A lane first moves its 32 operands into
+// registers and then runs the dependent additions unrolled, so the chain proceeds at the
+// latency of the additions alone; the next tile's loads are issued before them.
+constexpr int kTilePad = 33;  // row stride: lanes 0-5 reading one column hit distinct banks
+
+__device__ __forceinline__ void warp_node_sums(const double *__restrict__ X, const double *__restrict__ GI,
+                                               long long T, const int *__restrict__ mem, int count, bool circ,
+                                               double (*buf)[kTilePad], int lane, double &acc) {
+  acc = 0;
+  double v[6];
+  auto gather = [&](int k0) {
+    const int k = k0 + lane;
+    if (k < count) {
+      const int g = mem[k];
+      v[0] = __ldg(X + g);
+      v[1] = __ldg(X + T + g);
+      v[2] = __ldg(X + 2 * T + g);
+      if (circ) {
         v[3] = __ldg(GI + g);
         v[4] = __ldg(GI + T + g);
         v[5] = __ldg(GI + 2 * T + g);
       }
-    };
-    gather(0);
-    for (int k0 = 0; k0 < R.y; k0 += 32) {
-      __syncwarp();
-      if (k0 + lane < R.y)
+    }
+  };
+  gather(0);
+  for (int k0 = 0; k0 < count; k0 += 32) {
+    __syncwarp();
+    if (k0 + lane < count) {
 #pragma unroll
-        for (int c = 0; c < 6; ++c) buf[c][lane] = v[c];
-      __syncwarp();
-      if (k0 + 32 < R.y) gather(k0 + 32);
-      const int cnt = min(32, R.y - k0);
+      for (int c = 0; c < 3; ++c) buf[c][lane] = v[c];
+      if (circ)
+#pragma unroll
+        for (int c = 3; c < 6; ++c) buf[c][lane] = v[c];
+    }
+    __syncwarp();
+    if (k0 + 32 < count) gather(k0 + 32);
+    const int cnt = min(32, count - k0);
+    if (cnt == 32) {
+      if (lane < 3) {
+        double r[32];
+#pragma unroll
+        for (int l = 0; l < 32; ++l) r[l] = buf[lane][l];
+#pragma unroll
+        for (int l = 0; l < 32; ++l) acc = e_add(acc, r[l]);
+      } else if (lane < 6 && circ) {
+        double r[32], q[32];
+#pragma unroll
+        for (int l = 0; l < 32; ++l) {
+          r[l] = buf[lane][l];
+          q[l] = buf[lane - 3][l];
+        }
+#pragma unroll
+        for (int l = 0; l < 32; ++l) acc = e_sub(e_add(acc, r[l]), q[l]);
+      }
+    } else {
       if (lane < 3) {
         for (int l = 0; l < cnt; ++l) acc = e_add(acc, buf[lane][l]);
-      } else if (lane < 6 && !root) {
+      } else if (lane < 6 && circ) {
         for (int l = 0; l < cnt; ++l) acc = e_sub(e_add(acc, buf[lane][l]), buf[lane - 3][l]);
       }
     }
+  }
+}
+
+// Nodes (roots excepted) with kSmallNode < members <= kBlockSumNode: one warp each.
+__global__ void __launch_bounds__(128) k_node_sums_big(const double *__restrict__ X, const double *__restrict__ GI,
+                                                       const int *__restrict__ nxt, long long T, TreeBuffers tb,
+                                                       int nsys, unsigned *err) {
+  __shared__ double sm[4][6][kTilePad];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int n = tb.ctr[0];
+  for (int id = nsys + warp; id < n; id += nwarps) {
+    const int2 R = tb.nR[id];
+    if (R.y <= kSmallNode || R.y > kBlockSumNode) continue;
+    double acc;
+    warp_node_sums(X, GI, T, tb.members + R.x, R.y, true, sm[wl], lane, acc);
     const double cx = __shfl_sync(0xffffffffu, acc, 0), cy = __shfl_sync(0xffffffffu, acc, 1),
                  cz = __shfl_sync(0xffffffffu, acc, 2), qx = __shfl_sync(0xffffffffu, acc, 3),
                  qy = __shfl_sync(0xffffffffu, acc, 4), qz = __shfl_sync(0xffffffffu, acc, 5);
-    if (lane == 0) finish_node(tb, id, root, cx, cy, cz, root ? 0.0 : qx, root ? 0.0 : qy, root ? 0.0 : qz, nxt, err);
+    if (lane == 0) finish_node(tb, id, false, cx, cy, cz, qx, qy, qz, nxt, err);
   }
+}
+
+// Sequential sums of one large node by a block: warps 1.. stream member tiles into a ring of
+// kSumDepth shared-memory tiles with 8-byte cp.async copies, kSumDepth - 1 tiles ahead of
+// warp 0, whose lanes 0-2 (centre) and 3-5 (circulation) add each tile in member order.
+constexpr int kSumTile = 512, kSumDepth = 4, kSumThreads = 256;
+constexpr int kSumRow = kSumTile + 1;  // padded: lanes 0-5 reading one column hit distinct banks
+constexpr size_t kSumSmem = (size_t)kSumDepth * 6 * kSumRow * sizeof(double);
+
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_depth() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(kSumDepth - 2) : "memory");
+}
+
+__device__ void block_node_sums(const double *__restrict__ X, const double *__restrict__ GI, long long T,
+                                const int *__restrict__ mem, int count, bool circ, double *sm, double &acc) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  const bool producer = tid >= 32;
+  const int ptid = tid - 32, np = kSumThreads - 32;
+  const int ntiles = (count + kSumTile - 1) / kSumTile;
+  const int ncomp = circ ? 6 : 3;
+  auto issue = [&](int t) {  // producers: copies of tile t into its ring slot
+    if (t < ntiles) {
+      double *slot = sm + (size_t)(t % kSumDepth) * 6 * kSumRow;
+      for (int e = ptid; e < kSumTile; e += np) {
+        const int k = t * kSumTile + e;
+        if (k >= count) break;
+        const int g = mem[k];
+        cp_async8(slot + e, X + g);
+        cp_async8(slot + kSumRow + e, X + T + g);
+        cp_async8(slot + 2 * kSumRow + e, X + 2 * T + g);
+        if (circ) {
+          cp_async8(slot + 3 * kSumRow + e, GI + g);
+          cp_async8(slot + 4 * kSumRow + e, GI + T + g);
+          cp_async8(slot + 5 * kSumRow + e, GI + 2 * T + g);
+        }
+      }
+    }
+    cp_async_commit();  // one group per tile, empty or not, so that the wait counts line up
+  };
+  acc = 0;
+  if (producer) {
+    for (int t = 0; t < kSumDepth - 1; ++t) issue(t);
+    cp_async_wait_depth();  // tile 0 has landed
+  }
+  __syncthreads();
+  for (int t = 0; t < ntiles; ++t) {
+    if (producer) {
+      issue(t + kSumDepth - 1);  // into the slot consumed in the previous round
+      cp_async_wait_depth();     // tile t + 1 has landed
+    } else if (lane < ncomp) {
+      const double *slot = sm + (size_t)(t % kSumDepth) * 6 * kSumRow;
+      const double *a = slot + lane * kSumRow;
+      const double *b = slot + (lane >= 3 ? lane - 3 : lane) * kSumRow;
+      const int cnt = min(kSumTile, count - t * kSumTile);
+      if (cnt == kSumTile) {
+        for (int e0 = 0; e0 < kSumTile; e0 += 32) {
+          double r[32], q[32];
+#pragma unroll
+          for (int l = 0; l < 32; ++l) r[l] = a[e0 + l];
+          if (lane < 3) {
+#pragma unroll
+            for (int l = 0; l < 32; ++l) acc = e_add(acc, r[l]);
+          } else {
+#pragma unroll
+            for (int l = 0; l < 32; ++l) q[l] = b[e0 + l];
+#pragma unroll
+            for (int l = 0; l < 32; ++l) acc = e_sub(e_add(acc, r[l]), q[l]);
+          }
+        }
+      } else if (lane < 3) {
+        for (int l = 0; l < cnt; ++l) acc = e_add(acc, a[l]);
+      } else {
+        for (int l = 0; l < cnt; ++l) acc = e_sub(e_add(acc, a[l]), b[l]);
+      }
+    }
+    __syncthreads();
+  }
+  if (producer) asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// Non-root nodes with more than kBlockSumNode members (listed by the splits): one block each.
+__global__ void __launch_bounds__(kSumThreads) k_node_sums_block(const double *__restrict__ X,
+                                                                  const double *__restrict__ GI,
+                                                                  const int *__restrict__ nxt, long long T,
+                                                                  TreeBuffers tb, unsigned *err) {
+  extern __shared__ double sm_dyn[];
+  const int nbig = min(tb.ctr[kCtrBig], tb.max_big);
+  for (int b = blockIdx.x; b < nbig; b += gridDim.x) {
+    const int id = tb.bigl[b];
+    const int2 R = tb.nR[id];
+    double acc;
+    block_node_sums(X, GI, T, tb.members + R.x, R.y, true, sm_dyn, acc);
+    const double cx = __shfl_sync(0xffffffffu, acc, 0), cy = __shfl_sync(0xffffffffu, acc, 1),
+                 cz = __shfl_sync(0xffffffffu, acc, 2), qx = __shfl_sync(0xffffffffu, acc, 3),
+                 qy = __shfl_sync(0xffffffffu, acc, 4), qz = __shfl_sync(0xffffffffu, acc, 5);
+    if (threadIdx.x == 0) finish_node(tb, id, false, cx, cy, cz, qx, qy, qz, nxt, err);
+    __syncthreads();
+  }
+}
+
+// Roots: the masked mean over live slots (tree.f90:50-54), circulation zero.  One block per
+// system; launched beside the level splits (it reads only the root's member list, which
+// the splits do not change).
+__global__ void __launch_bounds__(kSumThreads) k_root_sums(const double *__restrict__ X, long long T,
+                                                            TreeBuffers tb, int nsys, const int *__restrict__ nxt,
+                                                            unsigned *err) {
+  extern __shared__ double sm_dyn[];
+  const int id = blockIdx.x;
+  if (id >= nsys) return;
+  const int2 R = tb.nR[id];
+  double acc;
+  block_node_sums(X, nullptr, T, tb.members + R.x, R.y, false, sm_dyn, acc);
+  const double cx = __shfl_sync(0xffffffffu, acc, 0), cy = __shfl_sync(0xffffffffu, acc, 1),
+               cz = __shfl_sync(0xffffffffu, acc, 2);
+  if (threadIdx.x == 0) finish_node(tb, id, true, cx, cy, cz, 0.0, 0.0, 0.0, nxt, err);
 }
 
 // tree_walk (tree.f90:250-316) for one image; accumulates into acc in preorder.
@@ -793,6 +958,11 @@ void tree_alloc(nv_handle *h) {
   cudaMalloc(&tb->nDepth, (size_t)tb->max_nodes * sizeof(int));
   cudaMalloc(&tb->nLeaf, (size_t)tb->max_nodes * sizeof(int));
   cudaMalloc(&tb->members, (size_t)tb->max_members * sizeof(int));
+  // each level holds at most T / (kBlockSumNode + 1) nodes above the block threshold
+  tb->max_big = (int)std::min<long long>((long long)kMaxLevels * (T / (kBlockSumNode + 1) + 1) + 64, 1 << 30);
+  cudaMalloc(&tb->bigl, (size_t)tb->max_big * sizeof(int));
+  cudaFuncSetAttribute(k_root_sums, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSumSmem);
+  cudaFuncSetAttribute(k_node_sums_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSumSmem);
   if (h->precision == NV_PREC_MIXED) {
     cudaMalloc(&tb->mx.C, (size_t)tb->max_nodes * sizeof(double4));
     cudaMalloc(&tb->mx.Q, (size_t)tb->max_nodes * sizeof(float4));
@@ -810,7 +980,7 @@ void tree_alloc(nv_handle *h) {
 void tree_free(nv_handle *h) {
   TreeBuffers *tb = h->tree;
   if (!tb) return;
-  void *ptrs[] = {tb->nA, tb->nB, tb->nP, tb->nI, tb->nR, tb->nDepth, tb->nLeaf, tb->members, tb->ctr,
+  void *ptrs[] = {tb->nA, tb->nB, tb->nP, tb->nI, tb->nR, tb->nDepth, tb->nLeaf, tb->members, tb->bigl, tb->ctr,
                   tb->flag, tb->pos, tb->cub_tmp, tb->mx.C, tb->mx.Q, tb->mx.G};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -827,14 +997,21 @@ void launch_tree_build(nv_handle *h) {
   cub::DeviceScan::ExclusiveSum(tb->cub_tmp, bytes, tb->flag, tb->pos, (int)(T + 1), h->stream);
   k_scatter_live<<<grid_for(T, TB), TB, 0, h->stream>>>(tb->flag, tb->pos, tb->members, T);
   k_roots<<<grid_for(h->nsys, 64), 64, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, h->nxt, tb->pos, *tb, T);
+  // the roots' sums (one long sequential chain per system) run beside the splits
+  cudaEventRecord(h->fork_ev, h->stream);
+  cudaStreamWaitEvent(h->side, h->fork_ev, 0);
+  k_root_sums<<<h->nsys, kSumThreads, kSumSmem, h->side>>>(h->x, T, *tb, h->nsys, h->nxt, h->d_err);
+  cudaEventRecord(h->join_ev, h->side);
   const int sms = n_sms();
   for (int L = 0; L < kMaxLevels; ++L) {
     k_split_block<<<sms, 1024, 0, h->stream>>>(h->x, T, *tb, L, h->d_err);
     k_split_warp<<<sms * 8, 128, 0, h->stream>>>(h->x, T, *tb, L, h->d_err);
     k_mark_level<<<1, 32, 0, h->stream>>>(*tb, L);
   }
+  k_node_sums_block<<<sms, kSumThreads, kSumSmem, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->d_err);
   k_node_sums_big<<<sms * 8, 128, 0, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->nsys, h->d_err);
   k_node_sums_small<<<sms * 8, 128, 0, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->nsys, h->d_err);
+  cudaStreamWaitEvent(h->stream, h->join_ev, 0);
   if (h->precision == NV_PREC_MIXED) {
     // theta0 and the correction flag are per system; a handle's systems share them when
     // any of them walks the tree (checked at creation)
