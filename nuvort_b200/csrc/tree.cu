@@ -42,6 +42,7 @@ struct TreeBuffers {
   int2 *nR = nullptr;     // member range start, member count
   int *nDepth = nullptr;
   int *nLeaf = nullptr;
+  int *nSib = nullptr;    // next sibling, or kEnd for a last child (and roots)
   int *members = nullptr;
   int *bigl = nullptr;    // non-root nodes with more than kBlockSumNode members
   int max_big = 0;
@@ -49,6 +50,13 @@ struct TreeBuffers {
   int *flag = nullptr, *pos = nullptr;
   void *cub_tmp = nullptr;
   size_t cub_bytes = 0;
+  // walk order: each system's slots sorted by Morton code of the position (live slots first)
+  unsigned long long *okey[2] = {nullptr, nullptr};
+  int *oval[2] = {nullptr, nullptr};
+  int *perm = nullptr;  // = oval[1]: position base+q of system s -> slot
+  void *sort_tmp = nullptr;
+  size_t sort_bytes = 0;
+  int key_bits = 0;
   bool built = false;
   MixedNodes mx;
 };
@@ -98,9 +106,46 @@ __global__ void k_roots(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys,
   tb.nI[s] = make_int4(pc, kEnd, kEnd, pc >= 1 ? nxt[sc.base + 1] : 0);
   tb.nR[s] = make_int2(pos[sc.base], pos[sc.base + sc.cap + 1] - pos[sc.base]);
   tb.nDepth[s] = 0;
+  tb.nSib[s] = kEnd;
   tb.nLeaf[s] = pc == 1 ? sc.base + 1 : 0;
   dyn[s].tree_eval = 0;
   dyn[s].tree_tests = 0;
+}
+
+// Sort keys of the walk order: (system, class, Morton code of the position on a 1024^3 grid
+// of the box); class 0 is the dummy slot, 1 live slots, 2 the rest.  The order only decides
+// which lanes walk together; every target's result is independent of it.
+__device__ __forceinline__ unsigned spread3(unsigned v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+__global__ void k_order_keys(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn,
+                             const int *__restrict__ sys_of, const double *__restrict__ X,
+                             const int *__restrict__ nxt, unsigned long long *key, int *val, long long T) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= T) return;
+  const int s = sys_of[g];
+  const SysConst &sc = scs[s];
+  const int k = (int)(g - sc.base);
+  unsigned long long inner;
+  if (k == 0) {
+    inner = 0;
+  } else if (k <= dyn[s].pcount && nxt[g] != 0) {
+    unsigned q[3];
+    for (int c = 0; c < 3; ++c) {
+      const double f = (X[c * T + g] / sc.bsize + 0.5) * 1024.0;
+      q[c] = f <= 0. ? 0u : f >= 1023. ? 1023u : (unsigned)f;
+    }
+    inner = (1ull << 32) | (spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2));
+  } else {
+    inner = (2ull << 32) | (unsigned)k;
+  }
+  key[g] = ((unsigned long long)s << 34) | inner;
+  val[g] = (int)g;
 }
 
 // Octant of x in node (corner P, half-width h), or 8 when x lies in no child.
@@ -175,6 +220,7 @@ __device__ void make_children(TreeBuffers &tb, int p, const int cnt[8], int *id0
     tb.nI[id] = make_int4(cnt[d], kEnd, last ? Ip.z : id + 1, 0);
     tb.nR[id] = make_int2(mb0 + off, cnt[d]);
     tb.nDepth[id] = depth;
+    tb.nSib[id] = last ? kEnd : id + 1;
     if (cnt[d] > kBlockSumNode) {
       const int b = atomicAdd(&tb.ctr[kCtrBig], 1);
       if (b < tb.max_big) tb.bigl[b] = id;
@@ -679,10 +725,11 @@ __global__ void __launch_bounds__(64) k_tree_walk_fp64(const SysConst *__restric
                                                        unsigned *err) {
   const int2 w = work[blockIdx.x];
   const SysConst &sc = scs[w.x];
-  const int g = w.y + threadIdx.x;
+  const int q = w.y + threadIdx.x - sc.base;  // position in the system's walk order
+  const int g = q >= 1 && q <= sc.cap ? tb.perm[sc.base + q] : sc.base;
   const int k = g - sc.base;
   unsigned long long evals = 0, tests = 0;
-  if (!*err && k <= dyn[w.x].pcount && k <= sc.cap && nxt[g] != 0) {
+  if (!*err && k >= 1 && k <= dyn[w.x].pcount && nxt[g] != 0) {
     double xi[3];
     load3(X, T, g, xi);
     const int pi_ = prv[g];
@@ -787,43 +834,90 @@ __global__ void k_node_prep(TreeBuffers tb, double theta0, int corr) {
   }
 }
 
-// Mixed tree walk: one thread per (target, image).  Opening tests in FP64 (squared), far
-// interactions in FP32, accepted leaves within near_radius in FP64 with the reference
-// expression (so they equal the plain path's terms).  Writes the image's partial sum.
+// Mixed tree walk: one lane per (target, image), a warp walking together.  A warp holds 32
+// consecutive slots (neighbours along the filaments, so close in space) against one image
+// and traverses the union of their walks: a shared-memory stack of (node, lane mask)
+// entries, where an entry stands for a node and its following siblings and the mask holds
+// the lanes whose walk reaches them.  Each node's data is read once per warp (broadcast);
+// each lane takes the reference's opening decision for itself, so a lane accepts exactly
+// the nodes its own walk (tree.f90:250-316) accepts, in the same preorder.  Opening tests
+// in FP64 (squared distances), far interactions in FP32, accepted leaves within the near
+// radius and ill-conditioned far terms in FP64.  Writes the image's partial sum.
+constexpr int kWalkStack = kMaxLevels + 2;
+
 __global__ void __launch_bounds__(128) k_tree_walk_mixed(const SysConst *__restrict__ scs, SysDyn *dyn,
                                                          const int4 *__restrict__ work, const double *__restrict__ X,
                                                          const int *__restrict__ nxt, const int *__restrict__ prv,
                                                          double *__restrict__ partial, long long T, TreeBuffers tb,
                                                          double near_factor, unsigned *err) {
+  __shared__ int2 stk[4][kWalkStack];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  int2 *st = stk[wl];
   const int4 w = work[blockIdx.x];
   const SysConst &sc = scs[w.x];
   const int m = w.y;
-  const int g = w.z + threadIdx.x;
+  const int q = w.z + threadIdx.x - sc.base;  // position in the system's walk order
+  const int g = q >= 1 && q <= sc.cap ? tb.perm[sc.base + q] : sc.base;
   const int k = g - sc.base;
   unsigned long long evals = 0, tests = 0;
-  if (!*err && k <= dyn[w.x].pcount && k <= sc.cap && nxt[g] != 0) {
-    double xi[3], s[3] = {0, 0, 0};
+  const bool valid = !*err && k >= 1 && k <= dyn[w.x].pcount && nxt[g] != 0;
+  const unsigned live = __ballot_sync(0xffffffffu, valid);
+  double xi[3] = {0, 0, 0}, s[3] = {0, 0, 0};
+  int pi_ = 0;
+  if (valid) {
     load3(X, T, g, xi);
-    if (m > 0)
-      for (int c = 0; c < 3; ++c) s[c] = sc.shift[m - 1][c];
-    const int pi_ = prv[g];
-    const double nr = near_factor * sc.delta, near2 = nr * nr;
-    const float gq = (float)(sc.quant_circ / (4.0 * NV_PI));
-    const double qc = sc.quant_circ, two_pi = sc.two_pi;
-    const bool second = sc.tree_extra_correction && sc.tree_theta > 1.1547;
-    float fx = 0, fy = 0, fz = 0;  // FP32 partial over at most kFlush far interactions
-    int nfar = 0;
-    double nx = 0, ny = 0, nz = 0;  // FP64: near field plus the flushed FP32 partials
-    bool singular = false;
-    int node = w.x;
-    while (node != kEnd) {
-      const int cur = node;
+    pi_ = prv[g];
+  }
+  if (m > 0)
+    for (int c = 0; c < 3; ++c) s[c] = sc.shift[m - 1][c];
+  const double nr = near_factor * sc.delta, near2 = nr * nr;
+  const float gq = (float)(sc.quant_circ / (4.0 * NV_PI));
+  const double qc = sc.quant_circ, two_pi = sc.two_pi;
+  const bool second = sc.tree_extra_correction && sc.tree_theta > 1.1547;
+  float fx = 0, fy = 0, fz = 0;  // FP32 partial over at most kFlush far interactions
+  int nfar = 0;
+  double nx = 0, ny = 0, nz = 0;  // FP64: near field plus the flushed FP32 partials
+  bool singular = false;
+  // FP64 evaluation of an accepted node (tree.f90:289-307)
+  auto exact_term = [&](int cur, const double r[3], double d2) {
+    const double dist = e_sqrt(d2);
+    const double4 B = ldg4(&tb.nB[cur]);
+    const double circ[3] = {B.x, B.y, B.z};
+    const double a = e_mul(dist, dist);
+    const double b = e_mul(2.0, dot3(r, circ));
+    const double c = dot3(circ, circ);
+    const double D = e_sub(e_mul(e_mul(4.0, a), c), e_mul(b, b));
+    if (D < NV_EPS) return;
+    double cr[3];
+    cross3(r, circ, cr);
+    const double den = e_mul(two_pi, D);
+    const double fac = e_sub(e_div(e_add(e_mul(2.0, c), b), e_sqrt(e_add(e_add(a, b), c))), e_div(b, e_sqrt(a)));
+    nx += e_mul(e_div(e_mul(cr[0], qc), den), fac);
+    ny += e_mul(e_div(e_mul(cr[1], qc), den), fac);
+    nz += e_mul(e_div(e_mul(cr[2], qc), den), fac);
+    ++evals;
+  };
+  int top = -1;
+  if (live) {
+    if (lane == 0) st[0] = make_int2(w.x, (int)live);
+    top = 0;
+  }
+  __syncwarp();
+  while (top >= 0) {
+    const int2 e = st[top];
+    const int cur = e.x;
+    const unsigned mask = (unsigned)e.y;
+    const int4 I = __ldg(&tb.nI[cur]);
+    const int sib = __ldg(&tb.nSib[cur]);
+    __syncwarp();  // every lane has read the entry
+    if (lane == 0 && sib != kEnd) st[top].x = sib;  // the entry moves on to the next sibling
+    __syncwarp();
+    if (sib == kEnd) --top;
+    if (I.x == 0) continue;
+    const bool mine = (mask >> lane) & 1u;
+    bool open = false;
+    if (mine) {
       const double4 C = ldg4(&tb.mx.C[cur]);
-      const int4 I = __ldg(&tb.nI[cur]);
-      if (I.x == 0) {
-        node = I.z;
-        continue;
-      }
       ++tests;
       const double cs[3] = {e_add(C.x, s[0]), e_add(C.y, s[1]), e_add(C.z, s[2])};
       const double r[3] = {e_sub(cs[0], xi[0]), e_sub(cs[1], xi[1]), e_sub(cs[2], xi[2])};
@@ -834,87 +928,68 @@ __global__ void __launch_bounds__(128) k_tree_walk_mixed(const SysConst *__restr
         acc = d2 <= G.x && d2 > G.y;
       }
       if (!acc) {
-        node = I.y != kEnd ? I.y : I.z;
-        continue;
-      }
-      node = I.z;
-      if (I.x == 1) {
-        const int j = __ldg(prv + I.w);
-        if (m == 0 && (j == g || j == pi_)) continue;
-        if (d2 < near2) {
-          // near leaf: the reference arithmetic (tree.f90:289-307) in FP64
-          const double dist = e_sqrt(d2);
-          if (dist < NV_EPS) {
-            singular = true;
-            continue;
+        open = true;
+      } else {
+        bool skip = false;
+        if (I.x == 1) {
+          const int j = __ldg(prv + I.w);
+          if (m == 0 && (j == g || j == pi_)) {
+            skip = true;
+          } else if (d2 < near2) {
+            // near leaf: the reference arithmetic in FP64
+            if (e_sqrt(d2) < NV_EPS) singular = true;
+            else exact_term(cur, r, d2);
+            skip = true;
           }
-          const double4 B = ldg4(&tb.nB[cur]);
-          const double circ[3] = {B.x, B.y, B.z};
-          const double a = e_mul(dist, dist);
-          const double b = e_mul(2.0, dot3(r, circ));
-          const double c = dot3(circ, circ);
-          const double D = e_sub(e_mul(e_mul(4.0, a), c), e_mul(b, b));
-          if (D < NV_EPS) continue;
-          double cr[3];
-          cross3(r, circ, cr);
-          const double den = e_mul(two_pi, D);
-          const double fac = e_sub(e_div(e_add(e_mul(2.0, c), b), e_sqrt(e_add(e_add(a, b), c))), e_div(b, e_sqrt(a)));
-          nx += e_mul(e_div(e_mul(cr[0], qc), den), fac);
-          ny += e_mul(e_div(e_mul(cr[1], qc), den), fac);
-          nz += e_mul(e_div(e_mul(cr[2], qc), den), fac);
-          ++evals;
-          continue;
+        }
+        if (!skip) {
+          const float4 Q = __ldg(&tb.mx.Q[cur]);
+          const float rx = (float)r[0], ry = (float)r[1], rz = (float)r[2];
+          // the reference skips 4ac-b^2 < epsilon (tree.f90:303); 4ac-b^2 = 4|r x circ|^2
+          const float cx = fmaf(ry, Q.z, -rz * Q.y), cy = fmaf(rz, Q.x, -rx * Q.z), cz = fmaf(rx, Q.y, -ry * Q.x);
+          const float cr2 = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
+          if (!(4.f * cr2 < (float)NV_EPS)) {
+            const float ex = rx + Q.x, ey = ry + Q.y, ez = rz + Q.z;
+            const float a = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+            const float ee = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+            const float re = fmaf(rx, ex, fmaf(ry, ey, rz * ez));
+            const float r1 = a * rsqrtf(a), r2 = ee * rsqrtf(ee);
+            const float pp = r1 * r2;
+            if (pp + re < 0.5f * pp || cr2 < kLineGuard * Q.w * fminf(a, ee) || ee < kLineGuard * fmaxf(a, Q.w)) {
+              // the segment subtends more than 120 degrees at the target, the target lies
+              // near its line or near its far end: FP32 would cancel digits there
+              exact_term(cur, r, d2);
+            } else {
+              const float f = gq * (r1 + r2) * __frcp_rn(pp * (pp + re));
+              fx = fmaf(f, cx, fx);
+              fy = fmaf(f, cy, fy);
+              fz = fmaf(f, cz, fz);
+              ++evals;
+              if (++nfar == kFlush) {
+                nx += (double)fx;
+                ny += (double)fy;
+                nz += (double)fz;
+                fx = fy = fz = 0.f;
+                nfar = 0;
+              }
+            }
+          }
         }
       }
-      const float4 Q = __ldg(&tb.mx.Q[cur]);
-      const float rx = (float)r[0], ry = (float)r[1], rz = (float)r[2];
-      // the reference skips 4ac-b^2 < epsilon (tree.f90:303); 4ac-b^2 = 4|r x circ|^2
-      const float cx = fmaf(ry, Q.z, -rz * Q.y), cy = fmaf(rz, Q.x, -rx * Q.z), cz = fmaf(rx, Q.y, -ry * Q.x);
-      const float cr2 = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
-      if (4.f * cr2 < (float)NV_EPS) continue;
-      const float ex = rx + Q.x, ey = ry + Q.y, ez = rz + Q.z;
-      const float a = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-      const float ee = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-      const float re = fmaf(rx, ex, fmaf(ry, ey, rz * ez));
-      const float r1 = a * rsqrtf(a), r2 = ee * rsqrtf(ee);
-      const float pp = r1 * r2;
-      if (pp + re < 0.5f * pp || cr2 < kLineGuard * Q.w * fminf(a, ee) || ee < kLineGuard * fmaxf(a, Q.w)) {
-        // the segment subtends more than 120 degrees at the target, the target lies near its
-        // line (perpendicular distance under 0.1x the nearer end) or near its far end
-        // (|e| < 0.1 max(|r|,|circ|)): |r||e| + r.e, r x circ or e = r + circ cancels there
-        // and FP32 would lose digits, so use the reference arithmetic
-        const double dist = e_sqrt(d2);
-        const double4 B = ldg4(&tb.nB[cur]);
-        const double circ[3] = {B.x, B.y, B.z};
-        const double a64 = e_mul(dist, dist);
-        const double b = e_mul(2.0, dot3(r, circ));
-        const double c = dot3(circ, circ);
-        const double D = e_sub(e_mul(e_mul(4.0, a64), c), e_mul(b, b));
-        if (D < NV_EPS) continue;
-        double crd[3];
-        cross3(r, circ, crd);
-        const double den = e_mul(two_pi, D);
-        const double fac = e_sub(e_div(e_add(e_mul(2.0, c), b), e_sqrt(e_add(e_add(a64, b), c))), e_div(b, e_sqrt(a64)));
-        nx += e_mul(e_div(e_mul(crd[0], qc), den), fac);
-        ny += e_mul(e_div(e_mul(crd[1], qc), den), fac);
-        nz += e_mul(e_div(e_mul(crd[2], qc), den), fac);
-        ++evals;
-        continue;
-      }
-      const float f = gq * (r1 + r2) * __frcp_rn(pp * (pp + re));
-      fx = fmaf(f, cx, fx);
-      fy = fmaf(f, cy, fy);
-      fz = fmaf(f, cz, fz);
-      ++evals;
-      if (++nfar == kFlush) {
-        nx += (double)fx;
-        ny += (double)fy;
-        nz += (double)fz;
-        fx = fy = fz = 0.f;
-        nfar = 0;
-      }
     }
-    if (singular) atomicOr(err, DERR_SINGULAR);
+    const unsigned omask = __ballot_sync(0xffffffffu, open);
+    if (omask && I.y != kEnd) {  // the lanes that open cur walk its children first
+      ++top;
+      if (top >= kWalkStack) {  // deeper than any tree the build makes; guard only
+        if (lane == 0) atomicOr(err, DERR_TREE_DEPTH);
+        break;
+      }
+      if (lane == 0) st[top] = make_int2(I.y, (int)omask);
+    }
+    __syncwarp();
+  }
+  if (singular) atomicOr(err, DERR_SINGULAR);
+  if (valid) {
     const long long o = (long long)m * 3 * T + g;
     partial[o] = (double)fx + nx;
     partial[o + T] = (double)fy + ny;
@@ -925,8 +1000,8 @@ __global__ void __launch_bounds__(128) k_tree_walk_mixed(const SysConst *__restr
     tot += __shfl_down_sync(0xffffffffu, tot, o);
     tt += __shfl_down_sync(0xffffffffu, tt, o);
   }
-  if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&dyn[w.x].tree_eval, tot);
-  if ((threadIdx.x & 31) == 0 && tt) atomicAdd(&dyn[w.x].tree_tests, tt);
+  if (lane == 0 && tot) atomicAdd(&dyn[w.x].tree_eval, tot);
+  if (lane == 0 && tt) atomicAdd(&dyn[w.x].tree_tests, tt);
 }
 
 int n_sms() {
@@ -956,6 +1031,7 @@ void tree_alloc(nv_handle *h) {
   cudaMalloc(&tb->nI, (size_t)tb->max_nodes * sizeof(int4));
   cudaMalloc(&tb->nR, (size_t)tb->max_nodes * sizeof(int2));
   cudaMalloc(&tb->nDepth, (size_t)tb->max_nodes * sizeof(int));
+  cudaMalloc(&tb->nSib, (size_t)tb->max_nodes * sizeof(int));
   cudaMalloc(&tb->nLeaf, (size_t)tb->max_nodes * sizeof(int));
   cudaMalloc(&tb->members, (size_t)tb->max_members * sizeof(int));
   // each level holds at most T / (kBlockSumNode + 1) nodes above the block threshold
@@ -974,14 +1050,26 @@ void tree_alloc(nv_handle *h) {
   cudaMalloc(&tb->pos, (T + 1) * sizeof(int));
   cub::DeviceScan::ExclusiveSum(nullptr, tb->cub_bytes, tb->flag, tb->pos, (int)(T + 1));
   cudaMalloc(&tb->cub_tmp, std::max<size_t>(tb->cub_bytes, 16));
+  for (int b = 0; b < 2; ++b) {
+    cudaMalloc(&tb->okey[b], (size_t)T * sizeof(unsigned long long));
+    cudaMalloc(&tb->oval[b], (size_t)T * sizeof(int));
+  }
+  tb->perm = tb->oval[1];
+  int sb = 1;
+  while ((1LL << sb) < h->nsys) ++sb;
+  tb->key_bits = 34 + sb;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb->sort_bytes, tb->okey[0], tb->okey[1], tb->oval[0], tb->oval[1], (int)T,
+                                  0, tb->key_bits);
+  cudaMalloc(&tb->sort_tmp, std::max<size_t>(tb->sort_bytes, 16));
   h->tree = tb;
 }
 
 void tree_free(nv_handle *h) {
   TreeBuffers *tb = h->tree;
   if (!tb) return;
-  void *ptrs[] = {tb->nA, tb->nB, tb->nP, tb->nI, tb->nR, tb->nDepth, tb->nLeaf, tb->members, tb->bigl, tb->ctr,
-                  tb->flag, tb->pos, tb->cub_tmp, tb->mx.C, tb->mx.Q, tb->mx.G};
+  void *ptrs[] = {tb->nA, tb->nB, tb->nP, tb->nI, tb->nR, tb->nDepth, tb->nLeaf, tb->nSib, tb->members, tb->bigl, tb->ctr,
+                  tb->flag, tb->pos, tb->cub_tmp, tb->mx.C, tb->mx.Q, tb->mx.G, tb->okey[0], tb->okey[1],
+                  tb->oval[0], tb->oval[1], tb->sort_tmp};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   delete tb;
@@ -1000,6 +1088,13 @@ void launch_tree_build(nv_handle *h) {
   // the roots' sums (one long sequential chain per system) run beside the splits
   cudaEventRecord(h->fork_ev, h->stream);
   cudaStreamWaitEvent(h->side, h->fork_ev, 0);
+  k_order_keys<<<grid_for(T, TB), TB, 0, h->side>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->nxt, tb->okey[0],
+                                                    tb->oval[0], T);
+  {
+    size_t sb = tb->sort_bytes;
+    cub::DeviceRadixSort::SortPairs(tb->sort_tmp, sb, tb->okey[0], tb->okey[1], tb->oval[0], tb->oval[1], (int)T, 0,
+                                    tb->key_bits, h->side);
+  }
   k_root_sums<<<h->nsys, kSumThreads, kSumSmem, h->side>>>(h->x, T, *tb, h->nsys, h->nxt, h->d_err);
   cudaEventRecord(h->join_ev, h->side);
   const int sms = n_sms();
