@@ -14,10 +14,18 @@
 
 #include "common.cuh"
 
+// One node as the mixed walk reads it: 64 bytes, four 16-byte loads.
+struct __align__(16) WalkNode {
+  float4 a;  // centre (FP32 high part), accept threshold t1^2 rounded to FP32
+  float4 b;  // centre (FP32 low part: centre - high part), |circ|^2 in FP32
+  float4 c;  // circulation in FP32, unused
+  int4 d;    // pcount, first child, next sibling, first member's infront
+};
+
 struct MixedNodes {  // per tree node, built after the FP64 node sums
   double4 *C = nullptr;  // cent.xyz, accept threshold t1^2 (dist^2 > t1^2 opens nothing)
-  float4 *Q = nullptr;   // circ.xyz in FP32, |circ|^2
   double2 *G = nullptr;  // geo^2, t0^2 for the dist <= geo branch (theta0 > 2/sqrt(3) only)
+  WalkNode *W = nullptr;
 };
 
 // Kahan-compensated FP32 accumulation of one tile's partial sum into (s, comp).

@@ -829,27 +829,41 @@ __global__ void k_node_prep(TreeBuffers tb, double theta0, int corr) {
     const double t1 = corr ? B.w + t0 : t0;
     tb.mx.C[id] = make_double4(A.x, A.y, A.z, t1 * t1);
     const float qx = (float)B.x, qy = (float)B.y, qz = (float)B.z;
-    tb.mx.Q[id] = make_float4(qx, qy, qz, qx * qx + qy * qy + qz * qz);
     tb.mx.G[id] = make_double2(corr ? B.w * B.w : -1.0, t0 * t0);
+    const float hx = (float)A.x, hy = (float)A.y, hz = (float)A.z;
+    const int4 I = tb.nI[id];
+    WalkNode wn;
+    wn.a = make_float4(hx, hy, hz, (float)(t1 * t1));
+    wn.b = make_float4((float)(A.x - hx), (float)(A.y - hy), (float)(A.z - hz), qx * qx + qy * qy + qz * qz);
+    wn.c = make_float4(qx, qy, qz, 0.f);
+    wn.d = make_int4(I.x, I.y, tb.nSib[id], I.w);
+    tb.mx.W[id] = wn;
   }
 }
 
 // Mixed tree walk: one lane per (target, image), a warp walking together.  A warp holds 32
-// consecutive slots (neighbours along the filaments, so close in space) against one image
+// targets that are close in space (consecutive in the Morton walk order) against one image
 // and traverses the union of their walks: a shared-memory stack of (node, lane mask)
 // entries, where an entry stands for a node and its following siblings and the mask holds
-// the lanes whose walk reaches them.  Each node's data is read once per warp (broadcast);
-// each lane takes the reference's opening decision for itself, so a lane accepts exactly
-// the nodes its own walk (tree.f90:250-316) accepts, in the same preorder.  Opening tests
-// in FP64 (squared distances), far interactions in FP32, accepted leaves within the near
-// radius and ill-conditioned far terms in FP64.  Writes the image's partial sum.
+// the lanes whose walk reaches them.  Each node's 64-byte record is read once per warp
+// (broadcast); each lane takes the reference's opening decision for itself, so a lane
+// accepts exactly the nodes its own walk (tree.f90:250-316) accepts, in the same preorder.
+//
+// The opening test compares |r|^2 with t1^2.  r is formed in FP32 from the high and low
+// parts of the centre and of the image-shifted target (|r_FP32 - r| <~ 2^-23 |r|), so
+// |r|^2 in FP32 is within 1e-6 of its value; outside a 1e-5 band around t1^2 the FP32
+// comparison gives the FP64 answer, inside it the FP64 test runs.  Far interactions in FP32;
+// accepted leaves within the near radius and ill-conditioned far terms in FP64.  Writes
+// the image's partial sum.
 constexpr int kWalkStack = kMaxLevels + 2;
+constexpr float kTestBand = 1e-5f;
 
-__global__ void __launch_bounds__(128) k_tree_walk_mixed(const SysConst *__restrict__ scs, SysDyn *dyn,
-                                                         const int4 *__restrict__ work, const double *__restrict__ X,
-                                                         const int *__restrict__ nxt, const int *__restrict__ prv,
-                                                         double *__restrict__ partial, long long T, TreeBuffers tb,
-                                                         double near_factor, unsigned *err) {
+__global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__restrict__ scs, SysDyn *dyn,
+                                                            const int4 *__restrict__ work,
+                                                            const double *__restrict__ X,
+                                                            const int *__restrict__ nxt, const int *__restrict__ prv,
+                                                            double *__restrict__ partial, long long T, TreeBuffers tb,
+                                                            double near_factor, unsigned *err) {
   __shared__ int2 stk[4][kWalkStack];
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   int2 *st = stk[wl];
@@ -859,28 +873,50 @@ __global__ void __launch_bounds__(128) k_tree_walk_mixed(const SysConst *__restr
   const int q = w.z + threadIdx.x - sc.base;  // position in the system's walk order
   const int g = q >= 1 && q <= sc.cap ? tb.perm[sc.base + q] : sc.base;
   const int k = g - sc.base;
-  unsigned long long evals = 0, tests = 0;
+  unsigned evals = 0, tests = 0;
   const bool valid = !*err && k >= 1 && k <= dyn[w.x].pcount && nxt[g] != 0;
   const unsigned live = __ballot_sync(0xffffffffu, valid);
-  double xi[3] = {0, 0, 0}, s[3] = {0, 0, 0};
+  float xh[3] = {0, 0, 0}, xl[3] = {0, 0, 0};  // target - shift, FP32 high and low parts
   int pi_ = 0;
   if (valid) {
-    load3(X, T, g, xi);
+    double xs[3];
+    load3(X, T, g, xs);
+    if (m > 0)
+      for (int c = 0; c < 3; ++c) xs[c] -= sc.shift[m - 1][c];
+    for (int c = 0; c < 3; ++c) {
+      xh[c] = (float)xs[c];
+      xl[c] = (float)(xs[c] - (double)xh[c]);
+    }
     pi_ = prv[g];
   }
-  if (m > 0)
-    for (int c = 0; c < 3; ++c) s[c] = sc.shift[m - 1][c];
-  const double nr = near_factor * sc.delta, near2 = nr * nr;
+  const float near2 = (float)(near_factor * sc.delta * near_factor * sc.delta);
   const float gq = (float)(sc.quant_circ / (4.0 * NV_PI));
-  const double qc = sc.quant_circ, two_pi = sc.two_pi;
   const bool second = sc.tree_extra_correction && sc.tree_theta > 1.1547;
   float fx = 0, fy = 0, fz = 0;  // FP32 partial over at most kFlush far interactions
   int nfar = 0;
   double nx = 0, ny = 0, nz = 0;  // FP64: near field plus the flushed FP32 partials
   bool singular = false;
+  // r and |r|^2 in FP64 as the FP64 walk forms them: (centre + shift) - target
+  auto exact_r = [&](int cur, double r[3]) -> double {
+    const double4 C = ldg4(&tb.mx.C[cur]);
+    double xi[3];
+    load3(X, T, g, xi);
+    const double s0 = m > 0 ? sc.shift[m - 1][0] : 0., s1 = m > 0 ? sc.shift[m - 1][1] : 0.,
+                 s2 = m > 0 ? sc.shift[m - 1][2] : 0.;
+    r[0] = e_sub(e_add(C.x, s0), xi[0]);
+    r[1] = e_sub(e_add(C.y, s1), xi[1]);
+    r[2] = e_sub(e_add(C.z, s2), xi[2]);
+    return e_add(e_add(e_sq(r[0]), e_sq(r[1])), e_sq(r[2]));
+  };
   // FP64 evaluation of an accepted node (tree.f90:289-307)
-  auto exact_term = [&](int cur, const double r[3], double d2) {
+  auto exact_term = [&](int cur) {
+    double r[3];
+    const double d2 = exact_r(cur, r);
     const double dist = e_sqrt(d2);
+    if (dist < NV_EPS) {
+      singular = true;
+      return;
+    }
     const double4 B = ldg4(&tb.nB[cur]);
     const double circ[3] = {B.x, B.y, B.z};
     const double a = e_mul(dist, dist);
@@ -890,7 +926,8 @@ __global__ void __launch_bounds__(128) k_tree_walk_mixed(const SysConst *__restr
     if (D < NV_EPS) return;
     double cr[3];
     cross3(r, circ, cr);
-    const double den = e_mul(two_pi, D);
+    const double qc = sc.quant_circ;
+    const double den = e_mul(sc.two_pi, D);
     const double fac = e_sub(e_div(e_add(e_mul(2.0, c), b), e_sqrt(e_add(e_add(a, b), c))), e_div(b, e_sqrt(a)));
     nx += e_mul(e_div(e_mul(cr[0], qc), den), fac);
     ny += e_mul(e_div(e_mul(cr[1], qc), den), fac);
@@ -907,58 +944,65 @@ __global__ void __launch_bounds__(128) k_tree_walk_mixed(const SysConst *__restr
     const int2 e = st[top];
     const int cur = e.x;
     const unsigned mask = (unsigned)e.y;
-    const int4 I = __ldg(&tb.nI[cur]);
-    const int sib = __ldg(&tb.nSib[cur]);
+    const WalkNode *wn = tb.mx.W + cur;
+    const int4 D = __ldg(&wn->d);
     __syncwarp();  // every lane has read the entry
-    if (lane == 0 && sib != kEnd) st[top].x = sib;  // the entry moves on to the next sibling
+    if (lane == 0 && D.z != kEnd) st[top].x = D.z;  // the entry moves on to the next sibling
     __syncwarp();
-    if (sib == kEnd) --top;
-    if (I.x == 0) continue;
-    const bool mine = (mask >> lane) & 1u;
+    if (D.z == kEnd) --top;
+    if (D.x == 0) continue;
     bool open = false;
-    if (mine) {
-      const double4 C = ldg4(&tb.mx.C[cur]);
+    if ((mask >> lane) & 1u) {
+      const float4 A = __ldg(&wn->a), B = __ldg(&wn->b);
       ++tests;
-      const double cs[3] = {e_add(C.x, s[0]), e_add(C.y, s[1]), e_add(C.z, s[2])};
-      const double r[3] = {e_sub(cs[0], xi[0]), e_sub(cs[1], xi[1]), e_sub(cs[2], xi[2])};
-      const double d2 = e_add(e_add(e_sq(r[0]), e_sq(r[1])), e_sq(r[2]));
-      bool acc = I.x == 1 || d2 > C.w;
-      if (!acc && second) {
-        const double2 G = tb.mx.G[cur];
-        acc = d2 <= G.x && d2 > G.y;
+      const float rx = (A.x - xh[0]) + (B.x - xl[0]);
+      const float ry = (A.y - xh[1]) + (B.y - xl[1]);
+      const float rz = (A.z - xh[2]) + (B.z - xl[2]);
+      const float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+      bool acc;
+      if (D.x == 1) {
+        acc = true;
+      } else if (!second && d2 > A.w * (1.f + kTestBand)) {
+        acc = true;
+      } else if (!second && d2 < A.w * (1.f - kTestBand)) {
+        acc = false;
+      } else {  // near the threshold (or the second criterion): the FP64 test
+        double r[3];
+        const double d2e = exact_r(cur, r);
+        acc = d2e > tb.mx.C[cur].w;
+        if (!acc && second) {
+          const double2 G = tb.mx.G[cur];
+          acc = d2e <= G.x && d2e > G.y;
+        }
       }
       if (!acc) {
         open = true;
       } else {
-        bool skip = false;
-        if (I.x == 1) {
-          const int j = __ldg(prv + I.w);
+        bool done = false;
+        if (D.x == 1) {
+          const int j = __ldg(prv + D.w);
           if (m == 0 && (j == g || j == pi_)) {
-            skip = true;
+            done = true;
           } else if (d2 < near2) {
-            // near leaf: the reference arithmetic in FP64
-            if (e_sqrt(d2) < NV_EPS) singular = true;
-            else exact_term(cur, r, d2);
-            skip = true;
+            exact_term(cur);  // near leaf: the reference arithmetic in FP64
+            done = true;
           }
         }
-        if (!skip) {
-          const float4 Q = __ldg(&tb.mx.Q[cur]);
-          const float rx = (float)r[0], ry = (float)r[1], rz = (float)r[2];
+        if (!done) {
+          const float4 Q = __ldg(&wn->c);
           // the reference skips 4ac-b^2 < epsilon (tree.f90:303); 4ac-b^2 = 4|r x circ|^2
           const float cx = fmaf(ry, Q.z, -rz * Q.y), cy = fmaf(rz, Q.x, -rx * Q.z), cz = fmaf(rx, Q.y, -ry * Q.x);
           const float cr2 = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
           if (!(4.f * cr2 < (float)NV_EPS)) {
             const float ex = rx + Q.x, ey = ry + Q.y, ez = rz + Q.z;
-            const float a = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
             const float ee = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
             const float re = fmaf(rx, ex, fmaf(ry, ey, rz * ez));
-            const float r1 = a * rsqrtf(a), r2 = ee * rsqrtf(ee);
+            const float r1 = d2 * rsqrtf(d2), r2 = ee * rsqrtf(ee);
             const float pp = r1 * r2;
-            if (pp + re < 0.5f * pp || cr2 < kLineGuard * Q.w * fminf(a, ee) || ee < kLineGuard * fmaxf(a, Q.w)) {
+            if (pp + re < 0.5f * pp || cr2 < kLineGuard * B.w * fminf(d2, ee) || ee < kLineGuard * fmaxf(d2, B.w)) {
               // the segment subtends more than 120 degrees at the target, the target lies
               // near its line or near its far end: FP32 would cancel digits there
-              exact_term(cur, r, d2);
+              exact_term(cur);
             } else {
               const float f = gq * (r1 + r2) * __frcp_rn(pp * (pp + re));
               fx = fmaf(f, cx, fx);
@@ -978,13 +1022,13 @@ __global__ void __launch_bounds__(128) k_tree_walk_mixed(const SysConst *__restr
       }
     }
     const unsigned omask = __ballot_sync(0xffffffffu, open);
-    if (omask && I.y != kEnd) {  // the lanes that open cur walk its children first
+    if (omask && D.y != kEnd) {  // the lanes that open cur walk its children first
       ++top;
       if (top >= kWalkStack) {  // deeper than any tree the build makes; guard only
         if (lane == 0) atomicOr(err, DERR_TREE_DEPTH);
         break;
       }
-      if (lane == 0) st[top] = make_int2(I.y, (int)omask);
+      if (lane == 0) st[top] = make_int2(D.y, (int)omask);
     }
     __syncwarp();
   }
@@ -1041,7 +1085,7 @@ void tree_alloc(nv_handle *h) {
   cudaFuncSetAttribute(k_node_sums_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSumSmem);
   if (h->precision == NV_PREC_MIXED) {
     cudaMalloc(&tb->mx.C, (size_t)tb->max_nodes * sizeof(double4));
-    cudaMalloc(&tb->mx.Q, (size_t)tb->max_nodes * sizeof(float4));
+    cudaMalloc(&tb->mx.W, (size_t)tb->max_nodes * sizeof(WalkNode));
     cudaMalloc(&tb->mx.G, (size_t)tb->max_nodes * sizeof(double2));
   }
   cudaMalloc(&tb->ctr, (kMaxLevels + 8) * sizeof(int));
@@ -1068,7 +1112,7 @@ void tree_free(nv_handle *h) {
   TreeBuffers *tb = h->tree;
   if (!tb) return;
   void *ptrs[] = {tb->nA, tb->nB, tb->nP, tb->nI, tb->nR, tb->nDepth, tb->nLeaf, tb->nSib, tb->members, tb->bigl, tb->ctr,
-                  tb->flag, tb->pos, tb->cub_tmp, tb->mx.C, tb->mx.Q, tb->mx.G, tb->okey[0], tb->okey[1],
+                  tb->flag, tb->pos, tb->cub_tmp, tb->mx.C, tb->mx.W, tb->mx.G, tb->okey[0], tb->okey[1],
                   tb->oval[0], tb->oval[1], tb->sort_tmp};
   for (void *p : ptrs)
     if (p) cudaFree(p);
