@@ -262,7 +262,8 @@ int nv_calc_velocity_bs_static(const nv_params *p, int32_t pcount, const double 
  * (cumulative), [3] precon candidates, [4] premove candidates, [5] insertions made by new
  * points that the sweep reached again, [6] fixed-point iterations the parallel pinsert took
  * to place them (a system that has not converged after the last one runs the serial sweep),
- * [7] unused.  n = entries wanted (<= 8). */
+ * [7] premove visits on the live state: extra slots << 32 | candidates.  n = entries wanted
+ * (<= 8). */
 int nv_diagnostics(nv_handle *h, int32_t sys, int64_t *out, int32_t n);
 
 /* Block until the handle's stream is idle and report any device-side error. */

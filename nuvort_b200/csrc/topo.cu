@@ -694,6 +694,7 @@ struct SlotSet {
   int n;
   int full;
   int base;
+  unsigned char *fl = nullptr;  // optional per-entry flags (what was written)
   __device__ static int home(int g) { return (int)(((unsigned)g * 0x9E3779B1u) >> (32 - kBits)); }
   // table index of g, or -1
   __device__ int find(int g) const {
@@ -717,10 +718,23 @@ struct SlotSet {
       return -1;
     }
     keys[h] = g;
+    if (fl) fl[h] = 0;
     ++n;
     return h;
   }
+  // record g with flag bits f (the flags array must be set)
+  __device__ void add(int g, unsigned f) {
+    const int h = add(g);
+    if (h >= 0) fl[h] |= (unsigned char)f;
+  }
   __device__ bool has(int g) const { return full || (g > base && find(g) >= 0); }
+  // g recorded with any of the flag bits f
+  __device__ bool has(int g, unsigned f) const {
+    if (full) return true;
+    if (g <= base) return false;
+    const int h = find(g);
+    return h >= 0 && (fl[h] & f);
+  }
   // warp-collective: empty the set for the next chunk (lane 0 holds n and full)
   __device__ void reset(int lane) {
     __syncwarp();
@@ -735,6 +749,21 @@ struct SlotSet {
 };
 constexpr int kTouchedPerChunk = 32 * 10;  // 4 relinked + up to 6 cleared slots per event
 using Touched = SlotSet<10, kTouchedPerChunk>;
+
+// A sweep's running event number and counters, in registers of the thread that applies
+// the events; written back to the system's SysDyn when the sweep ends.
+struct Tally {
+  int seq, itime, pcount;
+  int recon, remove, insert, kills;
+  __device__ static Tally of(const SysDyn &d) { return Tally{d.event_seq, d.itime, d.pcount, 0, 0, 0, 0}; }
+  __device__ void store(SysDyn &d) const {
+    d.event_seq = seq;
+    d.recon_count += recon;
+    d.remove_count += remove;
+    d.insert_count += insert;
+    d.loop_kills += kills;
+  }
+};
 
 // Events of one chunk, staged in shared memory by lane 0 and written with one atomic.  A
 // chunk with more events than the stage holds spills the stage from lane 0.
@@ -751,9 +780,9 @@ struct EventStage {
       if (at + q < ev_cap) ev[at + q] = buf[q];
     n = 0;
   }
-  __device__ void add(SysDyn &d, int s, int kind, int i, int j) {
+  __device__ void add(Tally &t, int s, int kind, int i, int j) {
     if (n == kEventStage) spill();
-    buf[n++] = DevEvent{s, d.event_seq++, d.itime, kind, i, j};
+    buf[n++] = DevEvent{s, t.seq++, t.itime, kind, i, j};
   }
 };
 __device__ void flush_events(EventStage &es, int lane) {
@@ -771,8 +800,9 @@ __device__ void flush_events(EventStage &es, int lane) {
 
 // loop_killer (reconnection.f90:155-182).  Only "fewer than 4 points" matters, so the
 // count stops after three hops; the result equals the reference's full walk.
-__device__ void loop_killer_stage(const State &S, SysDyn &d, int s, int particle, int pcount, EventStage &es,
-                                  Touched &tc) {
+template <class Set, class OnClear>
+__device__ void loop_killer_stage(const State &S, Tally &d, int s, int particle, int pcount, EventStage &es,
+                                  Set &tc, OnClear on_clear) {
   int counter = 1, nx = particle;
   const int hops = pcount < 3 ? pcount : 3;
   for (int it = 0; it < hops; ++it) {
@@ -782,16 +812,23 @@ __device__ void loop_killer_stage(const State &S, SysDyn &d, int s, int particle
   }
   if (counter < 4) {
     es.add(d, s, NV_EV_LOOPKILL, particle, counter);
-    d.loop_kills++;
+    d.kills++;
     nx = particle;
     for (int it = 0; it < pcount; ++it) {
       const int sn = S.nxt[nx];
-      tc.add(nx);
+      if (tc.fl) tc.add(nx, 3u);
+      else tc.add(nx);
+      on_clear(nx);
       clear_particle(S, nx);
       nx = sn;
       if (nx == particle) break;
     }
   }
+}
+template <class Set>
+__device__ void loop_killer_stage(const State &S, Tally &d, int s, int particle, int pcount, EventStage &es,
+                                  Set &tc) {
+  loop_killer_stage(S, d, s, particle, pcount, es, tc, [](int) {});
 }
 
 // loop_killer's count (up to three hops) on links read from a small override table first
@@ -812,72 +849,145 @@ __device__ int loop_count(const State &S, int particle, int pcount, const int (&
   return counter;
 }
 
-__global__ void __launch_bounds__(32) k_recon_sweep(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S,
-                                                    const int *__restrict__ pos_a, const int *__restrict__ list_a,
-                                                    unsigned *err, DevEvent *ev, int *ev_count, int ev_cap) {
-  __shared__ int tkeys[Touched::kCap];
+// ---- sweeps by rounds of kRound candidates -------------------------------------------------
+// A block of kRound threads loads kRound candidates at once and decides each on the state at
+// the start of the round; warp 0 then walks them in ascending order, lane 0 applying the
+// events.  Lane 0 stops only at candidates whose prefetched test passes or whose inputs an
+// earlier event of the round wrote (the "need" bits, recomputed by the whole warp against
+// the shared-memory touched set after every event, for the candidates the sweep has not
+// reached yet); every other candidate's test fails in the serial sweep too.
+constexpr int kRound = 256;
+constexpr int kExtraHeap = 1024;  // pending extra slots of the premove sweep held in shared memory
+constexpr int kRoundWords = kRound / 32;
+using RoundTouched = SlotSet<11, 1024>;
+
+// first candidate above pos whose bit is set in a | b (words of 32), or n
+__device__ __forceinline__ int next_marked(const unsigned *a, const unsigned *b, int pos, int n) {
+  for (int l = pos + 1; l < n;) {
+    const int wd = l >> 5;
+    const unsigned bits = (a[wd] | b[wd]) & (~0u << (l & 31));
+    if (bits) {
+      const int r = (wd << 5) + __ffs(bits) - 1;
+      return r < n ? r : n;
+    }
+    l = (wd + 1) << 5;
+  }
+  return n;
+}
+
+// Slot -> index of a candidate of the current round that reads that slot's links (one
+// entry per slot a candidate reads; duplicates allowed), so that an event can mark exactly
+// the candidates it affects.  Built by the whole block at the start of a round.
+constexpr int kMapBits = 11;
+constexpr int kMapCap = 1 << kMapBits;  // up to 4 entries per candidate at half load
+struct CandMap {
+  int *key;
+  int *idx;
+  __device__ static int home(int g) { return (int)(((unsigned)g * 0x9E3779B1u) >> (32 - kMapBits)); }
+  __device__ void insert(int g, int q) const {
+    if (g <= 0) return;
+    for (int h = home(g);; h = (h + 1) & (kMapCap - 1)) {
+      if (atomicCAS(&key[h], 0, g) == 0) {
+        idx[h] = q;
+        return;
+      }
+    }
+  }
+  // set the need bit of every candidate q > bound recorded under slot g
+  __device__ void mark(int g, int bound, unsigned *need) const {
+    if (g <= 0) return;
+    for (int h = home(g);; h = (h + 1) & (kMapCap - 1)) {
+      const int k = key[h];
+      if (k == 0) return;
+      if (k == g) {
+        const int q = idx[h];
+        if (q > bound) need[q >> 5] |= 1u << (q & 31);
+      }
+    }
+  }
+};
+
+struct ReconRec {
+  int i, yes, pari, j, parjb, nj, a1, a2, a3, b2;
+};
+
+__global__ void __launch_bounds__(kRound) k_recon_sweep(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys,
+                                                        State S, const int *__restrict__ pos_a,
+                                                        const int *__restrict__ list_a, unsigned *err, DevEvent *ev,
+                                                        int *ev_count, int ev_cap) {
+  __shared__ int tkeys[RoundTouched::kCap];
+  __shared__ int mkey[kMapCap], midx[kMapCap];
   __shared__ DevEvent ebuf[kEventStage];
+  __shared__ ReconRec rec[kRound];
+  __shared__ unsigned ymask[kRoundWords], nmask[kRoundWords];
+  __shared__ int s_used;
   const int s = blockIdx.x;
-  const int lane = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   if (s >= nsys || *err) return;
   const SysConst &sc = scs[s];
   if (!recon_step(sc, dyn[s])) return;
   const int base = sc.base;
-  for (int q = lane; q < Touched::kCap; q += 32) tkeys[q] = 0;
-  Touched tc{tkeys, 0, 0, base};
+  for (int q = tid; q < RoundTouched::kCap; q += kRound) tkeys[q] = 0;
+  for (int q = tid; q < kMapCap; q += kRound) mkey[q] = 0;
+  RoundTouched tc{tkeys, 0, 0, base};
+  const CandMap map{mkey, midx};
   EventStage es{ebuf, 0, ev, ev_count, ev_cap};
   const int li = pos_a[base], le = pos_a[base + sc.cap + 1];
-  SysDyn d = dyn[s];  // lane 0's copy is the live one
-  if (lane == 0) d.diag[3] = le - li;
-  __syncwarp();
+  Tally d = Tally::of(dyn[s]);  // thread 0 applies the events
   const double half_delta = sc.delta / 2.;
-  for (int k0 = li; k0 < le; k0 += 32) {
-    const int k = k0 + lane;
-    ReconIn in;
-    in.yes = -1;
-    in.i = 0;
-    int a1 = 0, a2 = 0, a3 = 0, b2 = 0;  // links the two loop_killer walks follow
-    if (k < le) {
-      const int i = list_a[k];
-      in = recon_decide(S, i, half_delta, S.cl[i]);
-      if (in.yes == 1) {
-        a1 = S.nxt[in.pari];
-        b2 = S.nxt[in.nj];
-        a2 = S.nxt[a1];
-        a3 = S.nxt[a2];
+  __syncthreads();
+  for (int c0 = li; c0 < le; c0 += kRound) {
+    const int n = min(kRound, le - c0);
+    ReconRec r{0, -1, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (tid < n) {
+      const int i = list_a[c0 + tid];
+      const ReconIn in = recon_decide(S, i, half_delta, S.cl[i]);
+      r.i = i;
+      r.yes = in.yes;
+      r.pari = in.pari;
+      r.j = in.j;
+      r.parjb = in.parjb;
+      r.nj = in.nj;
+      if (in.yes == 1) {  // the links the two loop_killer walks follow
+        r.a1 = S.nxt[in.pari];
+        r.b2 = S.nxt[in.nj];
+        r.a2 = S.nxt[r.a1];
+        r.a3 = S.nxt[r.a2];
       }
+      // the decision reads the links of i and j
+      map.insert(i, tid);
+      if (in.j != i) map.insert(in.j, tid);
     }
-    __syncwarp();
-    const int n = min(32, le - k0);
-    for (int l = 0; l < n; ++l) {
-      int i = __shfl_sync(0xffffffffu, in.i, l);
-      int yes = __shfl_sync(0xffffffffu, in.yes, l);
-      int pari = __shfl_sync(0xffffffffu, in.pari, l);
-      int j = __shfl_sync(0xffffffffu, in.j, l);
-      int parjb = __shfl_sync(0xffffffffu, in.parjb, l);
-      const int nj = __shfl_sync(0xffffffffu, in.nj, l);
-      const int a1l = __shfl_sync(0xffffffffu, a1, l);
-      const int a2l = __shfl_sync(0xffffffffu, a2, l);
-      const int a3l = __shfl_sync(0xffffffffu, a3, l);
-      const int b2l = __shfl_sync(0xffffffffu, b2, l);
-      if (lane == 0) {
-        bool live = false;
-        if (tc.has(i) || tc.has(j)) {
-          live = true;
-          // an earlier event wrote the links of i or j: decide again on the live state
+    rec[tid] = r;
+    const unsigned yb = __ballot_sync(0xffffffffu, r.yes == 1);
+    if (lane == 0) {
+      ymask[wid] = yb;
+      nmask[wid] = 0;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int bound = -1;
+      auto on_clear = [&](int g) { map.mark(g, bound, nmask); };
+      for (int pos = -1;;) {
+        const int l = next_marked(ymask, nmask, pos, n);
+        if (l >= n) break;
+        bound = l;
+        const ReconRec &c = rec[l];
+        int i = c.i, j = c.j, yes = c.yes, pari = c.pari, parjb = c.parjb;
+        bool live = (nmask[l >> 5] >> (l & 31)) & 1u;
+        if (live) {  // an earlier event of the round wrote the links of i or j
           if (S.nxt[i] == 0) {
             yes = -1;
           } else {
-            const ReconIn r = recon_decide(S, i, half_delta, S.cl[i]);
-            yes = r.yes;
-            pari = r.pari;
-            parjb = r.parjb;
+            const ReconIn q = recon_decide(S, i, half_delta, S.cl[i]);
+            yes = q.yes;
+            pari = q.pari;
+            parjb = q.parjb;
           }
         }
         if (yes == 1) {
-          // the walks' links as prefetched, unless an earlier event of the chunk wrote them
-          live = live || tc.has(pari) || tc.has(a1l) || tc.has(a2l) || tc.has(nj);
-          d.recon_count++;
+          live = live || tc.has(pari) || tc.has(c.a1) || tc.has(c.a2) || tc.has(c.nj);
+          d.recon++;
           es.add(d, s, NV_EV_RECON, i, j);
           S.nxt[parjb] = pari;
           S.prv[pari] = parjb;
@@ -887,62 +997,146 @@ __global__ void __launch_bounds__(32) k_recon_sweep(const SysConst *__restrict__
           tc.add(j);
           tc.add(pari);
           tc.add(parjb);
-          bool killed = false;
+          map.mark(i, l, nmask);
+          map.mark(j, l, nmask);
+          map.mark(pari, l, nmask);
+          map.mark(parjb, l, nmask);
           if (live) {
-            loop_killer_stage(S, d, s, pari, d.pcount, es, tc);
-            loop_killer_stage(S, d, s, i, d.pcount, es, tc);
+            loop_killer_stage(S, d, s, pari, d.pcount, es, tc, on_clear);
+            loop_killer_stage(S, d, s, i, d.pcount, es, tc, on_clear);
           } else {
-            const int key[7] = {parjb, i, pari, a1l, a2l, j, nj};
-            const int val[7] = {pari, j, a1l, a2l, a3l, nj, b2l};
+            const int key[7] = {parjb, i, pari, c.a1, c.a2, j, c.nj};
+            const int val[7] = {pari, j, c.a1, c.a2, c.a3, c.nj, c.b2};
+            bool killed = false;
             if (loop_count(S, pari, d.pcount, key, val) < 4) {
-              loop_killer_stage(S, d, s, pari, d.pcount, es, tc);
+              loop_killer_stage(S, d, s, pari, d.pcount, es, tc, on_clear);
               killed = true;
             }
             if (killed || loop_count(S, i, d.pcount, key, val) < 4)
-              loop_killer_stage(S, d, s, i, d.pcount, es, tc);
+              loop_killer_stage(S, d, s, i, d.pcount, es, tc, on_clear);
           }
         }
+        pos = l;
       }
+      if (es.n) es.spill();
+      s_used = tc.n | tc.full;
+      tc.n = 0;
+      tc.full = 0;
+      __threadfence_block();  // the round's writes are visible to the next round's loads
     }
-    // the chunk's writes are now visible to the next chunk's parallel decisions
-    __threadfence_block();
-    tc.reset(lane);
-    flush_events(es, lane);
+    __syncthreads();
+    if (s_used)
+      for (int q = tid; q < RoundTouched::kCap; q += kRound) tkeys[q] = 0;
+    for (int q = tid; q < kMapCap; q += kRound) mkey[q] = 0;
+    __syncthreads();
   }
-  if (lane == 0) dyn[s] = d;
+  if (tid == 0) {
+    d.store(dyn[s]);
+    dyn[s].diag[3] = le - li;
+  }
 }
 
 
-// ---- premove sweep, warp-prefetched --------------------------------------------------------
-// line.f90:107-129 in ascending slot order.  A candidate's test reads infront(i),
-// infront(infront(i)) and their positions; it is re-evaluated on the live state when an
-// event of the current chunk touched i or infront(i).  A removal at i changes the test of
-// p = behind(i); when p > i and p is not a candidate it is visited later as an extra slot
-// (the two-level bitmap).
-__global__ void __launch_bounds__(32) k_remove_sweep(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, State S,
-                                                     const int *__restrict__ pos_a, const int *__restrict__ list_a,
-                                                     const int *__restrict__ cand, Sweep sw, unsigned *err,
-                                                     DevEvent *ev, int *ev_count, int ev_cap) {
-  __shared__ int tkeys[Touched::kCap];
+// ---- premove sweep ---------------------------------------------------------------------------
+// line.f90:107-129 in ascending slot order, by rounds.  A candidate's test reads infront(i),
+// infront(infront(i)) and their positions; it is taken again on the live state when an
+// event of the round wrote i's or infront's infront link (or cleared them).  A removal at i
+// changes the test of p = behind(i); when p > i and p is not a candidate it is visited
+// later as an extra slot, in slot order between the candidates (a min-heap in shared
+// memory, the two-level bitmap past it).
+struct RemoveRec {
+  int i, inf, yes, tinf, c1, c2, pv, pcand;
+};
+
+__global__ void __launch_bounds__(kRound) k_remove_sweep(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys,
+                                                         State S, const int *__restrict__ pos_a,
+                                                         const int *__restrict__ list_a, const int *__restrict__ cand,
+                                                         Sweep sw, unsigned *err, DevEvent *ev, int *ev_count,
+                                                         int ev_cap) {
+  __shared__ int tkeys[RoundTouched::kCap];
+  __shared__ unsigned char tflags[RoundTouched::kCap];
+  __shared__ int mkey[kMapCap], midx[kMapCap];
   __shared__ DevEvent ebuf[kEventStage];
+  __shared__ RemoveRec rec[kRound];
+  __shared__ unsigned ymask[kRoundWords], nmask[kRoundWords];
+  __shared__ int heap[kExtraHeap];  // pending extra slots (a min-heap); the bitmap past it
+  __shared__ int s_used;
   const int s = blockIdx.x;
-  const int lane = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   if (s >= nsys || *err) return;
   const SysConst &sc = scs[s];
   if (!recon_step(sc, dyn[s])) return;
   const int base = sc.base;
-  for (int q = lane; q < Touched::kCap; q += 32) tkeys[q] = 0;
-  Touched tc{tkeys, 0, 0, base};
+  for (int q = tid; q < RoundTouched::kCap; q += kRound) tkeys[q] = 0;
+  for (int q = tid; q < kMapCap; q += kRound) mkey[q] = 0;
+  // flag 1: the slot's infront link was written (or the slot cleared); flag 2: its behind link
+  RoundTouched tc{tkeys, 0, 0, base, tflags};
+  const CandMap map{mkey, midx};
   EventStage es{ebuf, 0, ev, ev_count, ev_cap};
   const int li = pos_a[base], le = pos_a[base + sc.cap + 1];
-  SysDyn d = dyn[s];
+  Tally d = Tally::of(dyn[s]);  // thread 0 applies the events
   const int lastslot = base + d.pcount;
   const double thr = e_mul(.99, sc.delta);
   const long long T = S.T;
-  int extras = 0, last = base;  // lane 0: pending extra visits, last slot visited
-  if (lane == 0) d.diag[4] = le - li;
-  __syncwarp();
-  // one visit of slot i on the live state (lane 0)
+  int last = base;               // thread 0: last slot visited
+  int bound = -1;                // thread 0: candidates above this index are not reached yet
+  long long n_live = 0, n_extra = 0;  // visits on the live state: candidates, extra slots
+  int hsize = 0, bm_extras = 0;  // pending extras in the heap / in the bitmap (heap full)
+  int popped = 0;                // last extra taken from the heap (a duplicate pops next to it)
+  auto push_extra = [&](int p) {
+    if (hsize < kExtraHeap) {
+      int c = hsize++;
+      while (c > 0) {
+        const int par = (c - 1) >> 1;
+        if (heap[par] <= p) break;
+        heap[c] = heap[par];
+        c = par;
+      }
+      heap[c] = p;
+    } else {
+      sw.mark(p);
+      ++bm_extras;
+    }
+  };
+  auto pop_heap = [&]() {
+    const int v = heap[--hsize];
+    int c = 0;
+    for (;;) {
+      int ch = 2 * c + 1;
+      if (ch >= hsize) break;
+      if (ch + 1 < hsize && heap[ch + 1] < heap[ch]) ++ch;
+      if (heap[ch] >= v) break;
+      heap[c] = heap[ch];
+      c = ch;
+    }
+    if (hsize > 0) heap[c] = v;
+  };
+  // lowest pending extra slot in (last, upto], taken off the pending set, or INT_MAX
+  auto take_extra = [&](int upto) -> int {
+    for (;;) {
+      int e = INT_MAX;
+      bool from_heap = false;
+      if (hsize > 0 && heap[0] <= upto) {
+        e = heap[0];
+        from_heap = true;
+      }
+      if (bm_extras > 0) {
+        const int b2 = sw.next(last + 1, min(upto, e == INT_MAX ? upto : e - 1));
+        if (b2 != INT_MAX) {
+          sw.unmark(b2);
+          --bm_extras;
+          return b2;
+        }
+      }
+      if (!from_heap) return INT_MAX;
+      pop_heap();
+      if (e == popped) continue;  // the same slot marked twice
+      popped = e;
+      return e;
+    }
+  };
+  auto on_clear = [&](int g) { map.mark(g, bound, nmask); };
+  // one visit of slot i on the live state (thread 0)
   auto visit = [&](int i) {
     if (S.nxt[i] == 0) return;
     const int infront = S.nxt[i];
@@ -953,101 +1147,128 @@ __global__ void __launch_bounds__(32) k_remove_sweep(const SysConst *__restrict_
     if (!(dist_gen(xi, xt) < thr)) return;
     S.prv[tinfront] = i;
     S.nxt[i] = tinfront;
-    tc.add(i);
-    tc.add(infront);
-    tc.add(tinfront);
+    tc.add(i, 1u);
+    tc.add(infront, 3u);
+    tc.add(tinfront, 2u);
+    map.mark(i, bound, nmask);
+    map.mark(infront, bound, nmask);
     clear_particle(S, infront);
     es.add(d, s, NV_EV_REMOVE, i, infront);
-    loop_killer_stage(S, d, s, i, d.pcount, es, tc);
-    d.remove_count++;
+    loop_killer_stage(S, d, s, i, d.pcount, es, tc, on_clear);
+    d.remove++;
     const int p = S.prv[i];
-    if (p > i && p <= lastslot && !cand[p]) {
-      sw.mark(p);
-      ++extras;
-    }
-  };
-  auto run_extras = [&](int upto) {  // extra slots in (last, upto]
-    while (extras > 0) {
-      const int e = sw.next(last + 1, upto);
-      if (e == INT_MAX) break;
-      sw.unmark(e);
-      --extras;
-      last = e;
-      visit(e);
-    }
+    if (p > i && p <= lastslot && !cand[p]) push_extra(p);
   };
   // a removal decided on the prefetched links (i, infront and the walk's links untouched)
-  auto remove_fast = [&](int i, int infront, int tinfront, int c1, int c2, int pv, int pcand) {
-    S.prv[tinfront] = i;
-    S.nxt[i] = tinfront;
-    tc.add(i);
-    tc.add(infront);
-    tc.add(tinfront);
-    clear_particle(S, infront);
-    es.add(d, s, NV_EV_REMOVE, i, infront);
-    const int key[4] = {i, infront, tinfront, c1};  // infront is cleared: no infront link
-    const int val[4] = {tinfront, 0, c1, c2};
-    int p = pv, pc = pcand;
-    if (loop_count(S, i, d.pcount, key, val) < 4) {
-      loop_killer_stage(S, d, s, i, d.pcount, es, tc);
+  auto remove_fast = [&](const RemoveRec &c) {
+    const int i = c.i, infront = c.inf, tinfront = c.tinf;
+    int p = c.pv, pc = c.pcand;
+    if (tc.has(i, 2u)) {  // an earlier event of the round wrote i's behind link
       p = S.prv[i];
       pc = p > i && p <= lastslot ? cand[p] : 1;
     }
-    d.remove_count++;
-    if (p > i && p <= lastslot && !pc) {
-      sw.mark(p);
-      ++extras;
+    S.prv[tinfront] = i;
+    S.nxt[i] = tinfront;
+    tc.add(i, 1u);
+    tc.add(infront, 3u);
+    tc.add(tinfront, 2u);
+    map.mark(i, bound, nmask);
+    map.mark(infront, bound, nmask);
+    clear_particle(S, infront);
+    es.add(d, s, NV_EV_REMOVE, i, infront);
+    const int key[4] = {i, infront, tinfront, c.c1};  // infront is cleared: no infront link
+    const int val[4] = {tinfront, 0, c.c1, c.c2};
+    if (loop_count(S, i, d.pcount, key, val) < 4) {
+      loop_killer_stage(S, d, s, i, d.pcount, es, tc, on_clear);
+      p = S.prv[i];
+      pc = p > i && p <= lastslot ? cand[p] : 1;
     }
+    d.remove++;
+    if (p > i && p <= lastslot && !pc) push_extra(p);
   };
-  for (int k0 = li; k0 < le; k0 += 32) {
-    const int k = k0 + lane;
-    int i = 0, inf = 0, yes = 0, tinf = 0, c1 = 0, c2 = 0, pv = 0, pcand = 1;
-    if (k < le) {
-      i = list_a[k];
-      inf = S.nxt[i];
-      if (inf) {
-        tinf = S.nxt[inf];
+  __syncthreads();
+  for (int c0 = li; c0 < le; c0 += kRound) {
+    const int n = min(kRound, le - c0);
+    RemoveRec r{0, 0, 0, 0, 0, 0, 0, 1};
+    if (tid < n) {
+      r.i = list_a[c0 + tid];
+      r.inf = S.nxt[r.i];
+      if (r.inf) {
+        r.tinf = S.nxt[r.inf];
         double xi[3], xt[3];
-        load3(S.X, T, i, xi);
-        load3(S.X, T, tinf, xt);
-        yes = dist_gen(xi, xt) < thr;
-        if (yes) {
-          pv = S.prv[i];
-          c1 = S.nxt[tinf];
-          if (pv > i && pv <= lastslot) pcand = cand[pv];
-          c2 = S.nxt[c1];
+        load3(S.X, T, r.i, xi);
+        load3(S.X, T, r.tinf, xt);
+        r.yes = dist_gen(xi, xt) < thr;
+        if (r.yes) {
+          r.pv = S.prv[r.i];
+          r.c1 = S.nxt[r.tinf];
+          if (r.pv > r.i && r.pv <= lastslot) r.pcand = cand[r.pv];
+          r.c2 = S.nxt[r.c1];
         }
       }
+      // the test reads the infront links of i and infront(i)
+      map.insert(r.i, tid);
+      if (r.inf != r.i) map.insert(r.inf, tid);
     }
-    __syncwarp();
-    const int n = min(32, le - k0);
-    for (int l = 0; l < n; ++l) {
-      const int il = __shfl_sync(0xffffffffu, i, l);
-      const int infl = __shfl_sync(0xffffffffu, inf, l);
-      const int yl = __shfl_sync(0xffffffffu, yes, l);
-      const int tl = __shfl_sync(0xffffffffu, tinf, l);
-      const int c1l = __shfl_sync(0xffffffffu, c1, l);
-      const int c2l = __shfl_sync(0xffffffffu, c2, l);
-      const int pvl = __shfl_sync(0xffffffffu, pv, l);
-      const int pcl = __shfl_sync(0xffffffffu, pcand, l);
-      if (lane == 0) {
-        run_extras(il - 1);
-        last = il;
-        if (tc.has(il) || tc.has(infl)) {
-          visit(il);  // an earlier event wrote i's or infront's links: the live state decides
-        } else if (yl) {
-          if (tc.has(tl) || tc.has(c1l)) visit(il);
-          else remove_fast(il, infl, tl, c1l, c2l, pvl, pcl);
+    rec[tid] = r;
+    const unsigned yb = __ballot_sync(0xffffffffu, r.yes != 0);
+    if (lane == 0) {
+      ymask[wid] = yb;
+      nmask[wid] = 0;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (int pos = -1;;) {
+        const int l = next_marked(ymask, nmask, pos, n);
+        // the sweep position of the next candidate; past the round: the next round's first
+        const int kl = l < n ? rec[l].i : c0 + n < le ? list_a[c0 + n] : lastslot + 1;
+        const int e = hsize > 0 || bm_extras > 0 ? take_extra(min(kl - 1, lastslot)) : INT_MAX;
+        if (e != INT_MAX) {  // an extra slot below the next candidate
+          last = e;
+          bound = pos;
+          ++n_extra;
+          visit(e);
+          continue;
         }
+        if (l >= n) break;
+        last = kl;
+        bound = l;
+        const RemoveRec &c = rec[l];
+        if (((nmask[l >> 5] >> (l & 31)) & 1u) || tc.has(c.tinf, 1u) || tc.has(c.c1, 1u)) {
+          ++n_live;  // an earlier event wrote links the test or the loop_killer walk reads
+          visit(kl);
+        } else {
+          remove_fast(c);
+        }
+        pos = l;
       }
+      if (es.n) es.spill();
+      s_used = tc.n | tc.full;
+      tc.n = 0;
+      tc.full = 0;
+      __threadfence_block();
     }
-    __threadfence_block();
-    tc.reset(lane);
-    flush_events(es, lane);
+    __syncthreads();
+    if (s_used)
+      for (int q = tid; q < RoundTouched::kCap; q += kRound) tkeys[q] = 0;
+    for (int q = tid; q < kMapCap; q += kRound) mkey[q] = 0;
+    __syncthreads();
   }
-  if (lane == 0) run_extras(lastslot);
-  flush_events(es, lane);
-  if (lane == 0) dyn[s] = d;
+  if (tid == 0) {
+    // extra slots above the last candidate
+    bound = kRound;
+    for (;;) {
+      const int e = take_extra(lastslot);
+      if (e == INT_MAX) break;
+      last = e;
+      ++n_extra;
+      visit(e);
+    }
+    if (es.n) es.spill();
+    d.store(dyn[s]);
+    dyn[s].diag[4] = le - li;
+    dyn[s].diag[7] = (n_extra << 32) | n_live;
+  }
 }
 
 // ---- pinsert sweep, warp-prefetched --------------------------------------------------------
@@ -1124,7 +1345,7 @@ __global__ void __launch_bounds__(32) k_insert_sweep(const SysConst *__restrict_
   for (int q = lane; q < Set::kCap; q += 32) tkeys[q] = 0;
   Set tc{tkeys, 0, 0, base};
   EventStage es{ebuf, 0, ev, ev_count, ev_cap};
-  SysDyn d = dyn[s];  // lane 0's copy is the live one
+  Tally d = Tally::of(dyn[s]);  // lane 0's copy is the live one
   const int old_last = base + d.pcount;  // loop bound old_pcount (line.f90:28-30)
   const int li = pos_a[base], le = pos_a[base + sc.cap + 1];
   const int ee = pos_b[base + sc.cap + 1];
@@ -1162,7 +1383,7 @@ __global__ void __launch_bounds__(32) k_insert_sweep(const SysConst *__restrict_
   };
   auto after_insert = [&](int i, int p) {
     es.add(d, s, NV_EV_INSERT, i, p);
-    d.insert_count++;
+    d.insert++;
     if (p > i && p <= old_last) {  // the sweep reaches the new point later
       sw.mark(p);
       ++extras;
@@ -1333,9 +1554,9 @@ __global__ void __launch_bounds__(32) k_insert_sweep(const SysConst *__restrict_
   if (lane == 0 && !stop) run_extras(old_last);
   flush_events(es, lane);
   if (lane == 0) {
-    d.pcount = pc;
-    d.diag[2] += 1;
-    dyn[s] = d;
+    d.store(dyn[s]);
+    dyn[s].pcount = pc;
+    dyn[s].diag[2] += 1;
   }
 }
 
@@ -1476,7 +1697,7 @@ void launch_precon(nv_handle *h) {
   k_mark_recon<<<grid_for(h->T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->closestd, h->nxt,
                                                               tb->flag_a, h->T, h->d_err);
   compact(h, tb->flag_a, tb->pos_a, tb->list_a);
-  k_recon_sweep<<<h->nsys, 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a, tb->list_a,
+  k_recon_sweep<<<h->nsys, kRound, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a, tb->list_a,
                                                h->d_err, h->d_events, h->d_event_count, h->event_cap);
 }
 
@@ -1488,7 +1709,7 @@ void launch_premove(nv_handle *h) {
   // extra visits start empty: bitmaps from an all-zero flag array
   k_zero_flags<<<grid_for(h->T + 1, TB), TB, 0, h->stream>>>(tb->flag_b, h->T);
   const Sweep sw = make_sweep(h, tb->flag_b);
-  k_remove_sweep<<<h->nsys, 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a, tb->list_a,
+  k_remove_sweep<<<h->nsys, kRound, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a, tb->list_a,
                                                 tb->flag_a, sw, h->d_err, h->d_events, h->d_event_count,
                                                 h->event_cap);
 }
