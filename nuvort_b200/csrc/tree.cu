@@ -28,6 +28,10 @@ constexpr int kEnd = -1;
 constexpr int kBigNode = 2048;  // nodes with more members are split by a whole block
 constexpr int kBlockSumNode = 8192;  // nodes with more members are summed by a whole block
 constexpr int kCtrBig = kMaxLevels + 6;  // ctr[kCtrBig]: entries of the block-summed node list
+// ctr[kCtrSplit + b]: entries of the level lists of nodes to split, by level parity b:
+// [+0, +1] nodes above kBigNode members (split by a block), [+2, +3] the others with >= 2
+constexpr int kCtrSplit = kMaxLevels + 8;
+constexpr int kCtrSize = kMaxLevels + 16;
 constexpr int kFlush = 16;      // FP32 far-field terms summed before promotion to FP64
 constexpr float kLineGuard = 0.01f;  // (perpendicular distance / nearer end distance)^2 below
                                      // which a far interaction is evaluated in FP64
@@ -46,6 +50,9 @@ struct TreeBuffers {
   int *members = nullptr;
   int *bigl = nullptr;    // non-root nodes with more than kBlockSumNode members
   int max_big = 0;
+  int *split_blk[2] = {nullptr, nullptr};  // nodes of a level split by a block, by level parity
+  int *split_wrp[2] = {nullptr, nullptr};  // nodes of a level split by a warp
+  int max_blk = 0, max_wrp = 0;
   int *ctr = nullptr;     // [0] n_nodes [1] n_members [2 + L] first node of level L
   int *flag = nullptr, *pos = nullptr;
   void *cub_tmp = nullptr;
@@ -66,7 +73,8 @@ namespace {
 constexpr int TB = 256;
 
 __global__ void k_live_flags(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn,
-                             const int *__restrict__ sys_of, const int *__restrict__ nxt, int *flag, long long T) {
+                             const int *__restrict__ sys_of, const int *__restrict__ nxt, int *flag, long long T,
+                             int *ctr) {
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (g > T) return;
   int f = 0;
@@ -77,12 +85,28 @@ __global__ void k_live_flags(const SysConst *__restrict__ scs, const SysDyn *__r
     f = (sc.use_tree || sc.sched_tree) && k >= 1 && k <= dyn[s].pcount && nxt[g] != 0;
   }
   flag[g] = f;
+  if (g == 0)
+    for (int b = 0; b < 4; ++b) ctr[kCtrSplit + b] = 0;
 }
 
 __global__ void k_scatter_live(const int *__restrict__ flag, const int *__restrict__ pos, int *__restrict__ members,
                                long long T) {
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (g < T && flag[g]) members[pos[g]] = (int)g;
+}
+
+// Record node id (count members, at `level`) on its level's list of nodes to split.
+__device__ __forceinline__ void push_split(TreeBuffers &tb, int id, int count, int level, unsigned *err) {
+  const int b = level & 1;
+  if (count > kBigNode) {
+    const int q = atomicAdd(&tb.ctr[kCtrSplit + b], 1);
+    if (q < tb.max_blk) tb.split_blk[b][q] = id;
+    else if (err) atomicOr(err, DERR_TREE_NODES);
+  } else {
+    const int q = atomicAdd(&tb.ctr[kCtrSplit + 2 + b], 1);
+    if (q < tb.max_wrp) tb.split_wrp[b][q] = id;
+    else if (err) atomicOr(err, DERR_TREE_NODES);
+  }
 }
 
 // Root of every system (construct_tree, tree.f90:38-59).
@@ -107,6 +131,7 @@ __global__ void k_roots(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys,
   tb.nR[s] = make_int2(pos[sc.base], pos[sc.base + sc.cap + 1] - pos[sc.base]);
   tb.nDepth[s] = 0;
   tb.nSib[s] = kEnd;
+  if (pc >= 2) push_split(tb, s, tb.nR[s].y, 0, nullptr);
   tb.nLeaf[s] = pc == 1 ? sc.base + 1 : 0;
   dyn[s].tree_eval = 0;
   dyn[s].tree_tests = 0;
@@ -146,6 +171,11 @@ __global__ void k_order_keys(const SysConst *__restrict__ scs, const SysDyn *__r
   }
   key[g] = ((unsigned long long)s << 34) | inner;
   val[g] = (int)g;
+}
+
+__global__ void k_iota(int *v, long long n) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < n) v[g] = (int)g;
 }
 
 // Octant of x in node (corner P, half-width h), or 8 when x lies in no child.
@@ -221,6 +251,7 @@ __device__ void make_children(TreeBuffers &tb, int p, const int cnt[8], int *id0
     tb.nR[id] = make_int2(mb0 + off, cnt[d]);
     tb.nDepth[id] = depth;
     tb.nSib[id] = last ? kEnd : id + 1;
+    if (cnt[d] >= 2) push_split(tb, id, cnt[d], depth, err);
     if (cnt[d] > kBlockSumNode) {
       const int b = atomicAdd(&tb.ctr[kCtrBig], 1);
       if (b < tb.max_big) tb.bigl[b] = id;
@@ -240,12 +271,12 @@ __global__ void __launch_bounds__(128) k_split_warp(const double *__restrict__ X
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  const int nb = tb.ctr[2 + level], ne = tb.ctr[3 + level];
+  const int nl = min(tb.ctr[kCtrSplit + 2 + (level & 1)], tb.max_wrp);
+  const int *list = tb.split_wrp[level & 1];
   const unsigned lt = (1u << lane) - 1u;
-  for (int p = nb + warp; p < ne; p += nwarps) {
-    const int4 Ip = tb.nI[p];
+  for (int wq = warp; wq < nl; wq += nwarps) {
+    const int p = list[wq];
     const int2 R = tb.nR[p];
-    if (Ip.x <= 1 || R.y > kBigNode) continue;
     if (tb.nDepth[p] >= kMaxLevels) {
       if (lane == 0) atomicOr(err, DERR_TREE_DEPTH);
       continue;
@@ -312,11 +343,11 @@ __global__ void __launch_bounds__(1024) k_split_block(const double *__restrict__
   __shared__ int s_id0, s_mb0, s_cnt[8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
-  const int nb = tb.ctr[2 + level], ne = tb.ctr[3 + level];
-  for (int p = nb + blockIdx.x; p < ne; p += gridDim.x) {
-    const int4 Ip = tb.nI[p];
+  const int nl = min(tb.ctr[kCtrSplit + (level & 1)], tb.max_blk);
+  const int *list = tb.split_blk[level & 1];
+  for (int bq = blockIdx.x; bq < nl; bq += gridDim.x) {
+    const int p = list[bq];
     const int2 R = tb.nR[p];
-    if (Ip.x <= 1 || R.y <= kBigNode) continue;  // block-uniform
     if (tb.nDepth[p] >= kMaxLevels) {
       if (threadIdx.x == 0) atomicOr(err, DERR_TREE_DEPTH);
       continue;
@@ -393,8 +424,13 @@ __global__ void __launch_bounds__(1024) k_split_block(const double *__restrict__
   }
 }
 
+// After level `level`: its lists have been consumed; they collect level + 2's nodes next.
 __global__ void k_mark_level(TreeBuffers tb, int level) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) tb.ctr[4 + level] = tb.ctr[0];
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    tb.ctr[4 + level] = tb.ctr[0];
+    tb.ctr[kCtrSplit + (level & 1)] = 0;
+    tb.ctr[kCtrSplit + 2 + (level & 1)] = 0;
+  }
 }
 
 // Centre and circulation of every node: sequential sums in ascending slot order
@@ -768,8 +804,9 @@ __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *_
                                const int *__restrict__ sys_of, const double *__restrict__ X,
                                const int *__restrict__ nxt, const int *__restrict__ prv, int *__restrict__ cl,
                                double *__restrict__ CD, long long T, TreeBuffers tb, const unsigned *err) {
-  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= T || *err) return;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= T || *err) return;
+  const long long g = tb.perm[t];  // the walk order: neighbouring threads, neighbouring targets
   const int s = sys_of[g];
   const SysConst &sc = scs[s];
   if (!sc.use_tree || (dyn[s].itime % sc.recon_shots) != 0) return;
@@ -1088,8 +1125,14 @@ void tree_alloc(nv_handle *h) {
     cudaMalloc(&tb->mx.W, (size_t)tb->max_nodes * sizeof(WalkNode));
     cudaMalloc(&tb->mx.G, (size_t)tb->max_nodes * sizeof(double2));
   }
-  cudaMalloc(&tb->ctr, (kMaxLevels + 8) * sizeof(int));
-  cudaMemset(tb->ctr, 0, (kMaxLevels + 8) * sizeof(int));
+  cudaMalloc(&tb->ctr, kCtrSize * sizeof(int));
+  cudaMemset(tb->ctr, 0, kCtrSize * sizeof(int));
+  tb->max_blk = (int)(T / (kBigNode + 1) + h->nsys + 64);
+  tb->max_wrp = (int)(T / 2 + h->nsys + 64);
+  for (int b = 0; b < 2; ++b) {
+    cudaMalloc(&tb->split_blk[b], (size_t)tb->max_blk * sizeof(int));
+    cudaMalloc(&tb->split_wrp[b], (size_t)tb->max_wrp * sizeof(int));
+  }
   cudaMalloc(&tb->flag, (T + 1) * sizeof(int));
   cudaMalloc(&tb->pos, (T + 1) * sizeof(int));
   cub::DeviceScan::ExclusiveSum(nullptr, tb->cub_bytes, tb->flag, tb->pos, (int)(T + 1));
@@ -1099,6 +1142,7 @@ void tree_alloc(nv_handle *h) {
     cudaMalloc(&tb->oval[b], (size_t)T * sizeof(int));
   }
   tb->perm = tb->oval[1];
+  k_iota<<<grid_for(T, TB), TB, 0, h->stream>>>(tb->perm, T);  // a permutation before the first build
   int sb = 1;
   while ((1LL << sb) < h->nsys) ++sb;
   tb->key_bits = 34 + sb;
@@ -1113,7 +1157,8 @@ void tree_free(nv_handle *h) {
   if (!tb) return;
   void *ptrs[] = {tb->nA, tb->nB, tb->nP, tb->nI, tb->nR, tb->nDepth, tb->nLeaf, tb->nSib, tb->members, tb->bigl, tb->ctr,
                   tb->flag, tb->pos, tb->cub_tmp, tb->mx.C, tb->mx.W, tb->mx.G, tb->okey[0], tb->okey[1],
-                  tb->oval[0], tb->oval[1], tb->sort_tmp};
+                  tb->oval[0], tb->oval[1], tb->sort_tmp, tb->split_blk[0], tb->split_blk[1],
+                  tb->split_wrp[0], tb->split_wrp[1]};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   delete tb;
@@ -1124,7 +1169,8 @@ void launch_tree_build(nv_handle *h) {
   TreeBuffers *tb = h->tree;
   if (!tb) return;
   const long long T = h->T;
-  k_live_flags<<<grid_for(T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->nxt, tb->flag, T);
+  k_live_flags<<<grid_for(T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->nxt, tb->flag, T,
+                                                         tb->ctr);
   size_t bytes = tb->cub_bytes;
   cub::DeviceScan::ExclusiveSum(tb->cub_tmp, bytes, tb->flag, tb->pos, (int)(T + 1), h->stream);
   k_scatter_live<<<grid_for(T, TB), TB, 0, h->stream>>>(tb->flag, tb->pos, tb->members, T);
