@@ -210,6 +210,12 @@ int nv_stage_times(nv_handle *h, double *ms, int32_t n);
  * pairs of the direct sum) are evaluated in FP64; the rest in FP32, except interactions that
  * are ill-conditioned in FP32 (checked per interaction), which also run in FP64.  Default 2. */
 int nv_set_near_factor(nv_handle *h, double factor);
+/* Mixed precision: a far term runs in FP64 instead of FP32 when FP32 would cancel digits:
+ * |r||e| + r.e < angle |r||e|, |r x circ|^2 < line |circ|^2 min(|r|^2,|e|^2) or
+ * |e|^2 < end max(|r|^2,|circ|^2) (r, e: target to the segment's ends).  Defaults 0.1,
+ * 1e-3, 1e-2 (mixed vs FP64 velocity within 1e-7 RMS on the benchmark tangles); smaller
+ * values trade accuracy for speed.  angle must be at least 1e-3. */
+int nv_set_fp32_guards(nv_handle *h, double angle, double line, double end);
 /* pinsert places the insertions of new points that the sweep reaches again by a fixed-point
  * iteration (default 6 rounds); a system that has not converged runs the serial sweep.
  * Both give the reference's result.  n = 0 runs the serial sweep for every system (0..64). */
@@ -262,8 +268,10 @@ int nv_calc_velocity_bs_static(const nv_params *p, int32_t pcount, const double 
  * (cumulative), [3] precon candidates, [4] premove candidates, [5] insertions made by new
  * points that the sweep reached again, [6] fixed-point iterations the parallel pinsert took
  * to place them (a system that has not converged after the last one runs the serial sweep),
- * [7] premove visits on the live state: extra slots << 32 | candidates.  n = entries wanted
- * (<= 8). */
+ * [7] premove visits on the live state: extra slots << 32 | candidates, and for the mixed
+ * tree walk of the last velocity evaluation: [8] terms evaluated in FP64 (near leaves and
+ * terms FP32 would evaluate badly), [9] opening tests decided in FP64 (FP32 too close to
+ * call), [10] terms evaluated in FP32, [11] unused.  n = entries wanted (<= 12). */
 int nv_diagnostics(nv_handle *h, int32_t sys, int64_t *out, int32_t n);
 
 /* Block until the handle's stream is idle and report any device-side error. */

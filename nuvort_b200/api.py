@@ -66,6 +66,7 @@ def lib():
     L.nv_set_timing.argtypes = [vp, i32]
     L.nv_set_near_factor.argtypes = [vp, C.c_double]
     L.nv_set_insert_iterations.argtypes = [vp, C.c_int32]
+    L.nv_set_fp32_guards.argtypes = [vp, C.c_double, C.c_double, C.c_double]
     L.nv_step_launches.argtypes = [vp, P(i32)]
     L.nv_measure_fp64_peak.argtypes = [i32, P(C.c_double)]
     L.nv_measure_fp32_peak.argtypes = [i32, P(C.c_double)]
@@ -201,8 +202,8 @@ class Handle:
         return u
 
     def diagnostics(self, sys: int = 0) -> list:
-        out = (C.c_int64 * 8)()
-        _check(lib().nv_diagnostics(self.h, int(sys), out, 8))
+        out = (C.c_int64 * 12)()
+        _check(lib().nv_diagnostics(self.h, int(sys), out, 12))
         return list(out)
 
     def stage_times(self) -> dict:
@@ -212,6 +213,10 @@ class Handle:
 
     def set_near_factor(self, factor: float):
         _check(lib().nv_set_near_factor(self.h, float(factor)))
+
+    def set_fp32_guards(self, angle: float, line: float, end: float):
+        """Thresholds below which a far mixed-precision term is evaluated in FP64."""
+        _check(lib().nv_set_fp32_guards(self.h, float(angle), float(line), float(end)))
 
     def set_insert_iterations(self, n: int):
         """Fixed-point rounds of the parallel pinsert (0: the serial sweep every step)."""

@@ -717,6 +717,17 @@ int nv_set_near_factor(nv_handle *h, double factor) {
   return NV_OK;
 }
 
+int nv_set_fp32_guards(nv_handle *h, double angle, double line, double end) {
+  if (!h || !(angle >= 1e-3 && angle <= 2) || !(line >= 0 && line <= 1) || !(end >= 0 && end <= 1))
+    return set_error(NV_ERR_ARG, "nv_set_fp32_guards: angle in [1e-3,2] (it also keeps the FP32 "
+                                 "term away from its singularity), line and end in [0,1]");
+  h->guards.angle = (float)angle;
+  h->guards.line = (float)line;
+  h->guards.end = (float)end;
+  h->graph_valid = false;  // launch arguments of the captured kernels
+  return NV_OK;
+}
+
 int nv_set_insert_iterations(nv_handle *h, int32_t n) {
   if (!h || n < 0 || n > 64) return set_error(NV_ERR_ARG, "nv_set_insert_iterations: n must be 0..64");
   h->ins_iters = n;
@@ -817,7 +828,7 @@ int nv_tree_dump(nv_handle *h, int32_t sys, nv_tree_node *buf, int32_t cap, int3
 }
 
 int nv_diagnostics(nv_handle *h, int32_t sys, int64_t *out, int32_t n) {
-  if (!h || !out || sys < 0 || sys >= h->nsys || n < 0 || n > 8) return set_error(NV_ERR_ARG, "nv_diagnostics: bad arguments");
+  if (!h || !out || sys < 0 || sys >= h->nsys || n < 0 || n > 12) return set_error(NV_ERR_ARG, "nv_diagnostics: bad arguments");
   int rc = set_device(h);
   if (rc || (rc = pull_dyn(h))) return rc;
   for (int k = 0; k < n; ++k) out[k] = h->h_dyn[sys].diag[k];

@@ -69,7 +69,7 @@ struct SysDyn {
   int ins_fallback;  // pinsert needs the serial sweep this step
   int ins_conv;      // pinsert's fixed-point iteration has converged
   int ins_mismatch;  // positions where the iteration's H and H' differ
-  long long diag[8];  // see nv_diagnostics
+  long long diag[12];  // see nv_diagnostics
 };
 
 // One logged topology event (system-local numbering is restored on the host).

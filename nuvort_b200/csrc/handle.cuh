@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "mixed.cuh"
 
 struct TreeBuffers;  // tree.cu
 struct TopoBuffers;  // topo.cu
@@ -38,6 +39,7 @@ struct nv_handle {
   int4 *d_work_timg = nullptr; // same for the mixed tree walk
   int n_work_timg = 0;
   double near_factor = 2.0;
+  Fp32Guards guards;
   int ins_iters = 6;  // fixed-point iterations of the parallel pinsert; 0: serial sweep only
   int tree_sys0 = 0;           // first system that walks the tree (its theta0 builds the mixed nodes)    // near field: pairs closer than near_factor*delta run in FP64
   unsigned *d_err = nullptr;

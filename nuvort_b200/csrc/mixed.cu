@@ -22,7 +22,7 @@ __global__ void __launch_bounds__(kTB) k_direct_mixed(const SysConst *__restrict
                                                       const int4 *__restrict__ work, const double *__restrict__ X,
                                                       const int *__restrict__ nxt, const int *__restrict__ prv,
                                                       const float4 *__restrict__ seg32, const double4 *__restrict__ seg64,
-                                                      double *__restrict__ partial, long long T, double near_factor,
+                                                      double *__restrict__ partial, long long T, double near_factor, Fp32Guards gd,
                                                       unsigned *err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float4 *tiles = reinterpret_cast<float4 *>(smem_raw);  // [2][3*TJ]
@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(kTB) k_direct_mixed(const SysConst *__restrict
             const float re = fmaf(rx, ex, fmaf(ry, ey, rz * ez));
             const float r1 = a * rsqrtf(a), r2 = ee * rsqrtf(ee);
             const float pp = r1 * r2;
-            if (!(pp + re < 0.5f * pp || cr2 < 0.01f * D.w * fminf(a, ee) || ee < 0.01f * fmaxf(a, D.w))) {
+            if (!(pp + re < gd.angle * pp || cr2 < gd.line * D.w * fminf(a, ee) || ee < gd.end * fmaxf(a, D.w))) {
               const float f = gq * (r1 + r2) * __frcp_rn(pp * (pp + re));
               ux = fmaf(f, crx, ux);
               uy = fmaf(f, cry, uy);
@@ -199,7 +199,7 @@ void launch_direct_mixed(nv_handle *h) {
   if (h->n_work_img == 0) return;
   const size_t smem = 2 * 3 * kTJ * sizeof(float4);
   k_direct_mixed<kTJ><<<h->n_work_img, kTB, smem, h->stream>>>(
-      h->d_sc, h->d_dyn, h->d_work_img, h->x, h->nxt, h->prv, h->seg32, h->seg, h->partial, h->T, h->near_factor,
+      h->d_sc, h->d_dyn, h->d_work_img, h->x, h->nxt, h->prv, h->seg32, h->seg, h->partial, h->T, h->near_factor, h->guards,
       h->d_err);
 }
 

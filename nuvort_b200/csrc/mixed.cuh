@@ -14,6 +14,15 @@
 
 #include "common.cuh"
 
+// Conditioning guards of the FP32 segment term: a far term is evaluated in FP64 when
+//   |r||e| + r.e < angle |r||e|         (the segment subtends nearly 180 degrees at the target),
+//   |r x circ|^2 < line |circ|^2 min(|r|^2, |e|^2)   (the target lies near the segment's line),
+//   |e|^2 < end max(|r|^2, |circ|^2)    (the target lies near the far end),
+// where FP32 cancellation would cost digits.
+struct Fp32Guards {
+  float angle = 0.1f, line = 1e-3f, end = 1e-2f;
+};
+
 // One node as the mixed walk reads it: 64 bytes, four 16-byte loads.
 struct __align__(16) WalkNode {
   float4 a;  // centre (FP32 high part), accept threshold t1^2 rounded to FP32

@@ -33,8 +33,6 @@ constexpr int kCtrBig = kMaxLevels + 6;  // ctr[kCtrBig]: entries of the block-s
 constexpr int kCtrSplit = kMaxLevels + 8;
 constexpr int kCtrSize = kMaxLevels + 16;
 constexpr int kFlush = 16;      // FP32 far-field terms summed before promotion to FP64
-constexpr float kLineGuard = 0.01f;  // (perpendicular distance / nearer end distance)^2 below
-                                     // which a far interaction is evaluated in FP64
 
 struct TreeBuffers {
   int max_nodes = 0;
@@ -135,6 +133,7 @@ __global__ void k_roots(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys,
   tb.nLeaf[s] = pc == 1 ? sc.base + 1 : 0;
   dyn[s].tree_eval = 0;
   dyn[s].tree_tests = 0;
+  dyn[s].diag[8] = dyn[s].diag[9] = dyn[s].diag[10] = 0;
 }
 
 // Sort keys of the walk order: (system, class, Morton code of the position on a 1024^3 grid
@@ -880,11 +879,12 @@ __global__ void k_node_prep(TreeBuffers tb, double theta0, int corr) {
 
 // Mixed tree walk: one lane per (target, image), a warp walking together.  A warp holds 32
 // targets that are close in space (consecutive in the Morton walk order) against one image
-// and traverses the union of their walks: a shared-memory stack of (node, lane mask)
-// entries, where an entry stands for a node and its following siblings and the mask holds
-// the lanes whose walk reaches them.  Each node's 64-byte record is read once per warp
-// (broadcast); each lane takes the reference's opening decision for itself, so a lane
-// accepts exactly the nodes its own walk (tree.f90:250-316) accepts, in the same preorder.
+// and traverses the union of their walks: a stack of (node, lane mask) entries, where an
+// entry stands for a node and its following siblings and the mask holds the lanes whose
+// walk reaches them.  The stack lives in registers, entry d in lane d % 32.  Each node's
+// 64-byte record is read once per warp (broadcast); each lane takes the reference's opening
+// decision for itself, so a lane accepts exactly the nodes its own walk (tree.f90:250-316)
+// accepts, in the same preorder.
 //
 // The opening test compares |r|^2 with t1^2.  r is formed in FP32 from the high and low
 // parts of the centre and of the image-shifted target (|r_FP32 - r| <~ 2^-23 |r|), so
@@ -892,7 +892,7 @@ __global__ void k_node_prep(TreeBuffers tb, double theta0, int corr) {
 // comparison gives the FP64 answer, inside it the FP64 test runs.  Far interactions in FP32;
 // accepted leaves within the near radius and ill-conditioned far terms in FP64.  Writes
 // the image's partial sum.
-constexpr int kWalkStack = kMaxLevels + 2;
+constexpr int kWalkStack = 64;  // two register entries per lane; the build stops at depth 42
 constexpr float kTestBand = 1e-5f;
 
 __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__restrict__ scs, SysDyn *dyn,
@@ -900,17 +900,15 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
                                                             const double *__restrict__ X,
                                                             const int *__restrict__ nxt, const int *__restrict__ prv,
                                                             double *__restrict__ partial, long long T, TreeBuffers tb,
-                                                            double near_factor, unsigned *err) {
-  __shared__ int2 stk[4][kWalkStack];
-  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-  int2 *st = stk[wl];
+                                                            double near_factor, Fp32Guards gd, unsigned *err) {
+  const int lane = threadIdx.x & 31;
   const int4 w = work[blockIdx.x];
   const SysConst &sc = scs[w.x];
   const int m = w.y;
   const int q = w.z + threadIdx.x - sc.base;  // position in the system's walk order
   const int g = q >= 1 && q <= sc.cap ? tb.perm[sc.base + q] : sc.base;
   const int k = g - sc.base;
-  unsigned evals = 0, tests = 0;
+  unsigned evals = 0, tests = 0, n64 = 0, nband = 0;
   const bool valid = !*err && k >= 1 && k <= dyn[w.x].pcount && nxt[g] != 0;
   const unsigned live = __ballot_sync(0xffffffffu, valid);
   float xh[3] = {0, 0, 0}, xl[3] = {0, 0, 0};  // target - shift, FP32 high and low parts
@@ -970,23 +968,27 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
     ny += e_mul(e_div(e_mul(cr[1], qc), den), fac);
     nz += e_mul(e_div(e_mul(cr[2], qc), den), fac);
     ++evals;
+    ++n64;
   };
-  int top = -1;
-  if (live) {
-    if (lane == 0) st[0] = make_int2(w.x, (int)live);
-    top = 0;
-  }
-  __syncwarp();
+  // stack entry d: (node, mask) in lane d % 32, register pair 0 for d < 32, 1 above
+  int sn0 = w.x, sn1 = 0;
+  unsigned sm0 = live, sm1 = 0;
+  int top = live ? 0 : -1;
   while (top >= 0) {
-    const int2 e = st[top];
-    const int cur = e.x;
-    const unsigned mask = (unsigned)e.y;
+    const int src = top & 31;
+    const bool hi = top >= 32;
+    const int cur = __shfl_sync(0xffffffffu, hi ? sn1 : sn0, src);
+    const unsigned mask = __shfl_sync(0xffffffffu, hi ? sm1 : sm0, src);
     const WalkNode *wn = tb.mx.W + cur;
     const int4 D = __ldg(&wn->d);
-    __syncwarp();  // every lane has read the entry
-    if (lane == 0 && D.z != kEnd) st[top].x = D.z;  // the entry moves on to the next sibling
-    __syncwarp();
-    if (D.z == kEnd) --top;
+    if (D.z != kEnd) {  // the entry moves on to the next sibling
+      if (lane == src) {
+        if (hi) sn1 = D.z;
+        else sn0 = D.z;
+      }
+    } else {
+      --top;
+    }
     if (D.x == 0) continue;
     bool open = false;
     if ((mask >> lane) & 1u) {
@@ -1004,6 +1006,7 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
       } else if (!second && d2 < A.w * (1.f - kTestBand)) {
         acc = false;
       } else {  // near the threshold (or the second criterion): the FP64 test
+        ++nband;
         double r[3];
         const double d2e = exact_r(cur, r);
         acc = d2e > tb.mx.C[cur].w;
@@ -1036,7 +1039,7 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
             const float re = fmaf(rx, ex, fmaf(ry, ey, rz * ez));
             const float r1 = d2 * rsqrtf(d2), r2 = ee * rsqrtf(ee);
             const float pp = r1 * r2;
-            if (pp + re < 0.5f * pp || cr2 < kLineGuard * B.w * fminf(d2, ee) || ee < kLineGuard * fmaxf(d2, B.w)) {
+            if (pp + re < gd.angle * pp || cr2 < gd.line * B.w * fminf(d2, ee) || ee < gd.end * fmaxf(d2, B.w)) {
               // the segment subtends more than 120 degrees at the target, the target lies
               // near its line or near its far end: FP32 would cancel digits there
               exact_term(cur);
@@ -1065,9 +1068,16 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
         if (lane == 0) atomicOr(err, DERR_TREE_DEPTH);
         break;
       }
-      if (lane == 0) st[top] = make_int2(D.y, (int)omask);
+      if (lane == (top & 31)) {
+        if (top >= 32) {
+          sn1 = D.y;
+          sm1 = omask;
+        } else {
+          sn0 = D.y;
+          sm0 = omask;
+        }
+      }
     }
-    __syncwarp();
   }
   if (singular) atomicOr(err, DERR_SINGULAR);
   if (valid) {
@@ -1076,13 +1086,18 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
     partial[o + T] = (double)fy + ny;
     partial[o + 2 * T] = (double)fz + nz;
   }
-  unsigned long long tot = evals, tt = tests;
+  unsigned long long tot = evals, tt = tests, t64 = n64, tb_ = nband;
   for (int o = 16; o > 0; o >>= 1) {
     tot += __shfl_down_sync(0xffffffffu, tot, o);
     tt += __shfl_down_sync(0xffffffffu, tt, o);
+    t64 += __shfl_down_sync(0xffffffffu, t64, o);
+    tb_ += __shfl_down_sync(0xffffffffu, tb_, o);
   }
   if (lane == 0 && tot) atomicAdd(&dyn[w.x].tree_eval, tot);
   if (lane == 0 && tt) atomicAdd(&dyn[w.x].tree_tests, tt);
+  if (lane == 0 && t64) atomicAdd((unsigned long long *)&dyn[w.x].diag[8], t64);
+  if (lane == 0 && tb_) atomicAdd((unsigned long long *)&dyn[w.x].diag[9], tb_);
+  if (lane == 0 && tot > t64) atomicAdd((unsigned long long *)&dyn[w.x].diag[10], tot - t64);
 }
 
 int n_sms() {
@@ -1217,7 +1232,8 @@ void launch_tree_walk_mixed(nv_handle *h) {
   TreeBuffers *tb = h->tree;
   if (!tb || h->n_work_timg == 0) return;
   k_tree_walk_mixed<<<h->n_work_timg, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->d_work_timg, h->x, h->nxt, h->prv,
-                                                           h->partial, h->T, *tb, h->near_factor, h->d_err);
+                                                           h->partial, h->T, *tb, h->near_factor, h->guards,
+                                                           h->d_err);
 }
 
 void launch_closest_tree(nv_handle *h) {
