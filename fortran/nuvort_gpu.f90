@@ -38,6 +38,7 @@ module nuvort_gpu
     integer(c_int64_t) :: tree_eval, tree_tests
     integer(c_int32_t) :: itime, n_events
     real(c_double) :: t
+    integer(c_int64_t) :: event_hash  ! unsigned on the C side; compare bit patterns only
   end type
 
   interface

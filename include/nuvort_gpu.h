@@ -123,8 +123,12 @@ typedef struct nv_counters {
   int64_t tree_eval;     /* accepted tree interactions in the last velocity pass */
   int64_t tree_tests;    /* opening tests (nodes visited) in the last velocity pass */
   int32_t itime;         /* last completed step                                 */
-  int32_t n_events;      /* events logged so far (ring buffer may have dropped) */
+  int32_t n_events;      /* events so far (the log keeps the first ones to fit)  */
   double t;              /* simulation time                                     */
+  uint64_t event_hash;   /* order-sensitive digest of every event so far: equal
+                            for two runs exactly when their event sequences agree
+                            (up to 64-bit collisions), whether or not the log kept
+                            them all                                            */
 } nv_counters;
 
 /* One octree node (type node, src/tree.f90:20-32) as dumped in preorder by nv_tree_dump:
@@ -166,7 +170,9 @@ int nv_upload(nv_handle *h, int32_t sys, const nv_host_state *st);
 int nv_download(nv_handle *h, int32_t sys, nv_host_state *st, int32_t cap);
 int nv_set_clock(nv_handle *h, int32_t sys, double t, int32_t itime);
 int nv_counters_get(nv_handle *h, int32_t sys, nv_counters *c);
-/* Copy up to cap logged events of system sys; *n receives the number copied. */
+/* Copy up to cap logged events of system sys; *n receives the number copied.  The log holds
+ * T events (all systems); when more have happened (n_events of the counters is larger),
+ * it is incomplete and event_hash is the record to compare. */
 int nv_events_get(nv_handle *h, int32_t sys, nv_event *buf, int32_t cap, int32_t *n);
 
 /* ---- stages: one call per reference procedure, applied to every system -------------- */

@@ -102,6 +102,7 @@ class NvCounters(C.Structure):
         ("itime", C.c_int32),
         ("n_events", C.c_int32),
         ("t", C.c_double),
+        ("event_hash", C.c_uint64),
     ]
 
 
@@ -267,3 +268,27 @@ def tree_nodes_to_numpy(buf, n: int) -> np.ndarray:
     """Copy n NvTreeNode records into a structured numpy array."""
     assert TREE_NODE_DTYPE.itemsize == C.sizeof(NvTreeNode)
     return np.frombuffer(bytes(memoryview(buf))[: n * TREE_NODE_DTYPE.itemsize], dtype=TREE_NODE_DTYPE).copy()
+
+
+_M64 = (1 << 64) - 1
+
+
+def _digest_mix(z: int) -> int:
+    z = (z + 0x9E3779B97F4A7C15) & _M64
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+    return z ^ (z >> 31)
+
+
+def event_digest(events, seq0: int = 0) -> int:
+    """Host mirror of the device event digest: the sum (mod 2^64) over events, in order,
+    of a hash of (sequence number, itime, kind, i, j); events as (itime, kind, i, j) with
+    system-local slots, the first one numbered seq0.  Equals nv_counters.event_hash for the
+    same event sequence."""
+    tot = 0
+    for q, (itime, kind, i, j) in enumerate(events):
+        h = _digest_mix((seq0 + q) & 0xFFFFFFFF)
+        h = _digest_mix(h ^ (((i & 0xFFFFFFFF) << 32) | (j & 0xFFFFFFFF)))
+        h = _digest_mix(h ^ (((itime & 0xFFFFFFFF) << 8) | (kind & 0xFFFFFFFF)))
+        tot = (tot + h) & _M64
+    return tot

@@ -422,7 +422,7 @@ int nv_create(const nv_params *params, int32_t nsys, const int32_t *capacity, in
     const int nimg = 27;
     if ((rc = dalloc(&h->partial, (size_t)nimg * 3 * T))) return bail(rc);
   }
-  h->event_cap = (int)std::min<long long>(std::max<long long>(1 << 16, T / 4), 1 << 22);
+  h->event_cap = (int)std::min<long long>(std::max<long long>(1 << 16, T), 1 << 24);
   if ((rc = dalloc(&h->d_events, h->event_cap))) return bail(rc);
   if (cudaMemcpy(h->d_sc, h->sc.data(), nsys * sizeof(SysConst), cudaMemcpyHostToDevice) != cudaSuccess)
     return bail(set_error(NV_ERR_CUDA, "upload of system constants failed"));
@@ -593,6 +593,7 @@ int nv_counters_get(nv_handle *h, int32_t sys, nv_counters *c) {
   c->itime = d.itime;
   c->n_events = d.event_seq;
   c->t = d.t;
+  c->event_hash = d.ev_hash;
   return NV_OK;
 }
 

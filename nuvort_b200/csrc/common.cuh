@@ -64,6 +64,7 @@ struct SysDyn {
   unsigned long long tree_eval;
   unsigned long long tree_tests;
   int event_seq;
+  unsigned long long ev_hash;  // sum of event_digest over this system's events
   int live;
   int old_pcount;
   int ins_fallback;  // pinsert needs the serial sweep this step
@@ -71,6 +72,21 @@ struct SysDyn {
   int ins_mismatch;  // positions where the iteration's H and H' differ
   long long diag[12];  // see nv_diagnostics
 };
+
+// Order-sensitive digest of one event (system-local slots; a loop kill's j is its count):
+// the per-system sum over all events is equal for two runs whose event sequences agree,
+// and differs otherwise except for 64-bit collisions.  splitmix64 finaliser as the mixer.
+__device__ __forceinline__ unsigned long long digest_mix(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+__device__ __forceinline__ unsigned long long event_digest(int seq, int itime, int kind, int i, int j) {
+  unsigned long long h = digest_mix((unsigned long long)(unsigned)seq);
+  h = digest_mix(h ^ (((unsigned long long)(unsigned)i << 32) | (unsigned)j));
+  return digest_mix(h ^ (((unsigned long long)(unsigned)itime << 8) | (unsigned)kind));
+}
 
 // One logged topology event (system-local numbering is restored on the host).
 struct DevEvent {

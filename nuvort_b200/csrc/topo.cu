@@ -563,6 +563,7 @@ __global__ void k_ins_apply(const SysConst *__restrict__ scs, SysDyn *dyn, const
     const int seq = seq0 + (pos_c[g] - ev0) + (pos_h[g] - h0);
     const int a = atomicAdd(ev_count, 1);
     if (a < ev_cap) ev[a] = DevEvent{s, seq, itime, NV_EV_INSERT, g, q};
+    atomicAdd(&dyn[s].ev_hash, event_digest(seq, itime, NV_EV_INSERT, g - sc.base, q - sc.base));
     if (fh[q]) {  // the sweep reaches q and it inserts
       g = q;
       continue;
@@ -753,11 +754,15 @@ using Touched = SlotSet<10, kTouchedPerChunk>;
 // A sweep's running event number and counters, in registers of the thread that applies
 // the events; written back to the system's SysDyn when the sweep ends.
 struct Tally {
-  int seq, itime, pcount;
+  int seq, itime, pcount, base;
   int recon, remove, insert, kills;
-  __device__ static Tally of(const SysDyn &d) { return Tally{d.event_seq, d.itime, d.pcount, 0, 0, 0, 0}; }
+  unsigned long long hash;
+  __device__ static Tally of(const SysDyn &d, int base) {
+    return Tally{d.event_seq, d.itime, d.pcount, base, 0, 0, 0, 0, 0ull};
+  }
   __device__ void store(SysDyn &d) const {
     d.event_seq = seq;
+    d.ev_hash += hash;
     d.recon_count += recon;
     d.remove_count += remove;
     d.insert_count += insert;
@@ -782,6 +787,7 @@ struct EventStage {
   }
   __device__ void add(Tally &t, int s, int kind, int i, int j) {
     if (n == kEventStage) spill();
+    t.hash += event_digest(t.seq, t.itime, kind, i - t.base, kind == NV_EV_LOOPKILL ? j : j - t.base);
     buf[n++] = DevEvent{s, t.seq++, t.itime, kind, i, j};
   }
 };
@@ -933,7 +939,7 @@ __global__ void __launch_bounds__(kRound) k_recon_sweep(const SysConst *__restri
   const CandMap map{mkey, midx};
   EventStage es{ebuf, 0, ev, ev_count, ev_cap};
   const int li = pos_a[base], le = pos_a[base + sc.cap + 1];
-  Tally d = Tally::of(dyn[s]);  // thread 0 applies the events
+  Tally d = Tally::of(dyn[s], base);  // thread 0 applies the events
   const double half_delta = sc.delta / 2.;
   __syncthreads();
   for (int c0 = li; c0 < le; c0 += kRound) {
@@ -1074,7 +1080,7 @@ __global__ void __launch_bounds__(kRound) k_remove_sweep(const SysConst *__restr
   const CandMap map{mkey, midx};
   EventStage es{ebuf, 0, ev, ev_count, ev_cap};
   const int li = pos_a[base], le = pos_a[base + sc.cap + 1];
-  Tally d = Tally::of(dyn[s]);  // thread 0 applies the events
+  Tally d = Tally::of(dyn[s], base);  // thread 0 applies the events
   const int lastslot = base + d.pcount;
   const double thr = e_mul(.99, sc.delta);
   const long long T = S.T;
@@ -1345,7 +1351,7 @@ __global__ void __launch_bounds__(32) k_insert_sweep(const SysConst *__restrict_
   for (int q = lane; q < Set::kCap; q += 32) tkeys[q] = 0;
   Set tc{tkeys, 0, 0, base};
   EventStage es{ebuf, 0, ev, ev_count, ev_cap};
-  Tally d = Tally::of(dyn[s]);  // lane 0's copy is the live one
+  Tally d = Tally::of(dyn[s], base);  // lane 0's copy is the live one
   const int old_last = base + d.pcount;  // loop bound old_pcount (line.f90:28-30)
   const int li = pos_a[base], le = pos_a[base + sc.cap + 1];
   const int ee = pos_b[base + sc.cap + 1];

@@ -132,7 +132,10 @@ def test_whole_steps_config0_events_identical():
     o = Oracle(p, st)
     h.step(200)
     o.step(200)
-    assert h.events() == o.events()
+    ev = o.events()
+    assert h.events() == ev
+    from nuvort_b200.abi import event_digest
+    assert h.counters().event_hash == event_digest(ev)  # the device digest of the same sequence
     a, b = h.download(), o.download()
     assert np.array_equal(a.infront, b.infront) and np.array_equal(a.behind, b.behind)
     assert np.max(np.abs(a.x - b.x)) < 1e-12
