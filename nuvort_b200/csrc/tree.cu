@@ -28,8 +28,8 @@ constexpr int kEnd = -1;
 constexpr int kBigNode = 2048;  // nodes with more members are split by a whole block
 constexpr int kBlockSumNode = 8192;  // nodes with more members are summed by a whole block
 constexpr int kCtrBig = kMaxLevels + 6;  // ctr[kCtrBig]: entries of the block-summed node list
-// ctr[kCtrSplit + b]: entries of the level lists of nodes to split, by level parity b:
-// [+0, +1] nodes above kBigNode members (split by a block), [+2, +3] the others with >= 2
+// ctr[kCtrSplit + b]: entries of the level lists of nodes to split, by level % 3 = b:
+// [+0..+2] nodes above kBigNode members (split by a block), [+3..+5] the others with >= 2
 constexpr int kCtrSplit = kMaxLevels + 8;
 constexpr int kCtrSize = kMaxLevels + 16;
 constexpr int kFlush = 16;      // FP32 far-field terms summed before promotion to FP64
@@ -48,8 +48,8 @@ struct TreeBuffers {
   int *members = nullptr;
   int *bigl = nullptr;    // non-root nodes with more than kBlockSumNode members
   int max_big = 0;
-  int *split_blk[2] = {nullptr, nullptr};  // nodes of a level split by a block, by level parity
-  int *split_wrp[2] = {nullptr, nullptr};  // nodes of a level split by a warp
+  int *split_blk[3] = {nullptr, nullptr, nullptr};  // nodes of a level split by a block, by level % 3
+  int *split_wrp[3] = {nullptr, nullptr, nullptr};  // nodes of a level split by a warp
   int max_blk = 0, max_wrp = 0;
   int *ctr = nullptr;     // [0] n_nodes [1] n_members [2 + L] first node of level L
   int *flag = nullptr, *pos = nullptr;
@@ -84,7 +84,7 @@ __global__ void k_live_flags(const SysConst *__restrict__ scs, const SysDyn *__r
   }
   flag[g] = f;
   if (g == 0)
-    for (int b = 0; b < 4; ++b) ctr[kCtrSplit + b] = 0;
+    for (int b = 0; b < 6; ++b) ctr[kCtrSplit + b] = 0;
 }
 
 __global__ void k_scatter_live(const int *__restrict__ flag, const int *__restrict__ pos, int *__restrict__ members,
@@ -95,13 +95,13 @@ __global__ void k_scatter_live(const int *__restrict__ flag, const int *__restri
 
 // Record node id (count members, at `level`) on its level's list of nodes to split.
 __device__ __forceinline__ void push_split(TreeBuffers &tb, int id, int count, int level, unsigned *err) {
-  const int b = level & 1;
+  const int b = level % 3;
   if (count > kBigNode) {
     const int q = atomicAdd(&tb.ctr[kCtrSplit + b], 1);
     if (q < tb.max_blk) tb.split_blk[b][q] = id;
     else if (err) atomicOr(err, DERR_TREE_NODES);
   } else {
-    const int q = atomicAdd(&tb.ctr[kCtrSplit + 2 + b], 1);
+    const int q = atomicAdd(&tb.ctr[kCtrSplit + 3 + b], 1);
     if (q < tb.max_wrp) tb.split_wrp[b][q] = id;
     else if (err) atomicOr(err, DERR_TREE_NODES);
   }
@@ -264,57 +264,124 @@ __device__ void make_children(TreeBuffers &tb, int p, const int cnt[8], int *id0
   *mb0_out = mb0;
 }
 
-// Split every node of `level` with at most kBigNode members: one warp per node.
-__global__ void __launch_bounds__(128) k_split_warp(const double *__restrict__ X, long long T, TreeBuffers tb, int level,
-                                                    unsigned *err) {
-  const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  const int nl = min(tb.ctr[kCtrSplit + 2 + (level & 1)], tb.max_wrp);
-  const int *list = tb.split_wrp[level & 1];
+// Split node p (at most kBigNode members) with one warp: count the members per octant, make
+// the children, then write each member to its child's list in member order (stable).
+__device__ void split_node_warp(const double *__restrict__ X, long long T, TreeBuffers &tb, int p, int lane,
+                                unsigned *err) {
   const unsigned lt = (1u << lane) - 1u;
-  for (int wq = warp; wq < nl; wq += nwarps) {
-    const int p = list[wq];
-    const int2 R = tb.nR[p];
-    if (tb.nDepth[p] >= kMaxLevels) {
-      if (lane == 0) atomicOr(err, DERR_TREE_DEPTH);
-      continue;
+  const int2 R = tb.nR[p];
+  const double4 P = tb.nP[p];
+  const double h = tb.nA[p].w / 2.0;
+  int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int k0 = 0; k0 < R.y; k0 += 32) {
+    const int k = k0 + lane;
+    int d = 8;
+    if (k < R.y) {
+      double x[3];
+      load_x(X, T, tb.members[R.x + k], x);
+      d = octant(x, P, h);
     }
-    const double4 P = tb.nP[p];
-    const double h = tb.nA[p].w / 2.0;
-    int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int k0 = 0; k0 < R.y; k0 += 32) {
-      const int k = k0 + lane;
-      int d = 8;
-      if (k < R.y) {
-        double x[3];
-        load_x(X, T, tb.members[R.x + k], x);
-        d = octant(x, P, h);
-      }
 #pragma unroll
-      for (int dd = 0; dd < 8; ++dd) cnt[dd] += __popc(__ballot_sync(0xffffffffu, d == dd));
-    }
-    int id0 = -1, mb0 = -1;
-    if (lane == 0) make_children(tb, p, cnt, &id0, &mb0, err);
-    id0 = __shfl_sync(0xffffffffu, id0, 0);
-    mb0 = __shfl_sync(0xffffffffu, mb0, 0);
-    if (id0 < 0) continue;
-    int base_off[8], childid[8], run[8];
-    {
-      int off = 0, k = 0;
+    for (int dd = 0; dd < 8; ++dd) cnt[dd] += __popc(__ballot_sync(0xffffffffu, d == dd));
+  }
+  int id0 = -1, mb0 = -1;
+  if (lane == 0) make_children(tb, p, cnt, &id0, &mb0, err);
+  id0 = __shfl_sync(0xffffffffu, id0, 0);
+  mb0 = __shfl_sync(0xffffffffu, mb0, 0);
+  if (id0 < 0) return;
+  int base_off[8], run[8];
+  {
+    int off = 0;
 #pragma unroll
-      for (int dd = 0; dd < 8; ++dd) {
-        base_off[dd] = off;
-        childid[dd] = cnt[dd] ? id0 + k : -1;
-        k += cnt[dd] ? 1 : 0;
-        off += cnt[dd];
-        run[dd] = 0;
-      }
+    for (int dd = 0; dd < 8; ++dd) {
+      base_off[dd] = off;
+      off += cnt[dd];
+      run[dd] = 0;
     }
-    for (int k0 = 0; k0 < R.y; k0 += 32) {
+  }
+  for (int k0 = 0; k0 < R.y; k0 += 32) {
+    const int k = k0 + lane;
+    int d = 8, slot = 0;
+    if (k < R.y) {
+      double x[3];
+      slot = tb.members[R.x + k];
+      load_x(X, T, slot, x);
+      d = octant(x, P, h);
+    }
+    int mypos = -1;
+#pragma unroll
+    for (int dd = 0; dd < 8; ++dd) {
+      const unsigned b = __ballot_sync(0xffffffffu, d == dd);
+      if (d == dd) mypos = mb0 + base_off[dd] + run[dd] + __popc(b & lt);
+      run[dd] += __popc(b);
+    }
+    if (mypos >= 0) tb.members[mypos] = slot;
+  }
+}
+
+// Split node p (more than kBigNode members) with a whole block: each warp takes a contiguous
+// slice of the member list and the slices' counts are prefix-summed, so the partition stays
+// stable.
+__device__ void split_node_block(const double *__restrict__ X, long long T, TreeBuffers &tb, int p,
+                                 unsigned *err) {
+  __shared__ int wcnt[32][8];
+  __shared__ int s_id0, s_mb0, s_cnt[8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const int2 R = tb.nR[p];
+  const double4 P = tb.nP[p];
+  const double h = tb.nA[p].w / 2.0;
+  const int per = (R.y + nw - 1) / nw;
+  const int s0 = w * per, s1 = min(R.y, s0 + per);
+  int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int k0 = s0; k0 < s1; k0 += 32) {
+    const int k = k0 + lane;
+    int d = 8;
+    if (k < s1) {
+      double x[3];
+      load_x(X, T, tb.members[R.x + k], x);
+      d = octant(x, P, h);
+    }
+#pragma unroll
+    for (int dd = 0; dd < 8; ++dd) cnt[dd] += __popc(__ballot_sync(0xffffffffu, d == dd));
+  }
+  if (lane == 0)
+#pragma unroll
+    for (int dd = 0; dd < 8; ++dd) wcnt[w][dd] = cnt[dd];
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    int tot = 0;
+    for (int ww = 0; ww < nw; ++ww) {
+      const int c = wcnt[ww][threadIdx.x];
+      wcnt[ww][threadIdx.x] = tot;  // exclusive prefix over warps
+      tot += c;
+    }
+    s_cnt[threadIdx.x] = tot;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int c[8];
+    for (int dd = 0; dd < 8; ++dd) c[dd] = s_cnt[dd];
+    int id0, mb0;
+    make_children(tb, p, c, &id0, &mb0, err);
+    s_id0 = id0;
+    s_mb0 = mb0;
+  }
+  __syncthreads();
+  const int mb0 = s_mb0;
+  if (s_id0 >= 0) {
+    int base_off[8], run[8];
+    int off = 0;
+#pragma unroll
+    for (int dd = 0; dd < 8; ++dd) {
+      base_off[dd] = off + wcnt[w][dd];
+      off += s_cnt[dd];
+      run[dd] = 0;
+    }
+    for (int k0 = s0; k0 < s1; k0 += 32) {
       const int k = k0 + lane;
       int d = 8, slot = 0;
-      if (k < R.y) {
+      if (k < s1) {
         double x[3];
         slot = tb.members[R.x + k];
         load_x(X, T, slot, x);
@@ -329,106 +396,40 @@ __global__ void __launch_bounds__(128) k_split_warp(const double *__restrict__ X
       }
       if (mypos >= 0) tb.members[mypos] = slot;
     }
-    (void)childid;
   }
 }
 
-// Split every node of `level` with more than kBigNode members: one block (32 warps) per
-// node, each warp taking a contiguous slice of the member list, so the partition stays
-// stable.
-__global__ void __launch_bounds__(1024) k_split_block(const double *__restrict__ X, long long T, TreeBuffers tb, int level,
-                                                      unsigned *err) {
-  __shared__ int wcnt[32][8];
-  __shared__ int s_id0, s_mb0, s_cnt[8];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const unsigned lt = (1u << lane) - 1u;
-  const int nl = min(tb.ctr[kCtrSplit + (level & 1)], tb.max_blk);
-  const int *list = tb.split_blk[level & 1];
-  for (int bq = blockIdx.x; bq < nl; bq += gridDim.x) {
-    const int p = list[bq];
-    const int2 R = tb.nR[p];
+// One level of the build: the listed big nodes by blocks, then the other listed nodes by
+// warps.  The children's lists (level + 1) fill as nodes split; the list of level + 2 is
+// idle during this level (read at level - 1, filled at level + 1) and is emptied here.
+__global__ void __launch_bounds__(1024) k_split_level(const double *__restrict__ X, long long T, TreeBuffers tb,
+                                                      int level, unsigned *err) {
+  const int b = level % 3, b2 = (level + 2) % 3;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    tb.ctr[kCtrSplit + b2] = 0;
+    tb.ctr[kCtrSplit + 3 + b2] = 0;
+  }
+  const int nbl = min(tb.ctr[kCtrSplit + b], tb.max_blk);
+  for (int bq = blockIdx.x; bq < nbl; bq += gridDim.x) {
+    const int p = tb.split_blk[b][bq];
     if (tb.nDepth[p] >= kMaxLevels) {
       if (threadIdx.x == 0) atomicOr(err, DERR_TREE_DEPTH);
       continue;
     }
-    const double4 P = tb.nP[p];
-    const double h = tb.nA[p].w / 2.0;
-    const int per = (R.y + nw - 1) / nw;
-    const int s0 = w * per, s1 = min(R.y, s0 + per);
-    int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int k0 = s0; k0 < s1; k0 += 32) {
-      const int k = k0 + lane;
-      int d = 8;
-      if (k < s1) {
-        double x[3];
-        load_x(X, T, tb.members[R.x + k], x);
-        d = octant(x, P, h);
-      }
-#pragma unroll
-      for (int dd = 0; dd < 8; ++dd) cnt[dd] += __popc(__ballot_sync(0xffffffffu, d == dd));
-    }
-    if (lane == 0)
-#pragma unroll
-      for (int dd = 0; dd < 8; ++dd) wcnt[w][dd] = cnt[dd];
-    __syncthreads();
-    if (threadIdx.x < 8) {
-      int tot = 0;
-      for (int ww = 0; ww < nw; ++ww) {
-        const int c = wcnt[ww][threadIdx.x];
-        wcnt[ww][threadIdx.x] = tot;  // exclusive prefix over warps
-        tot += c;
-      }
-      s_cnt[threadIdx.x] = tot;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      int c[8];
-      for (int dd = 0; dd < 8; ++dd) c[dd] = s_cnt[dd];
-      int id0, mb0;
-      make_children(tb, p, c, &id0, &mb0, err);
-      s_id0 = id0;
-      s_mb0 = mb0;
-    }
-    __syncthreads();
-    const int mb0 = s_mb0;
-    if (s_id0 >= 0) {
-      int base_off[8], run[8];
-      int off = 0;
-#pragma unroll
-      for (int dd = 0; dd < 8; ++dd) {
-        base_off[dd] = off + wcnt[w][dd];
-        off += s_cnt[dd];
-        run[dd] = 0;
-      }
-      for (int k0 = s0; k0 < s1; k0 += 32) {
-        const int k = k0 + lane;
-        int d = 8, slot = 0;
-        if (k < s1) {
-          double x[3];
-          slot = tb.members[R.x + k];
-          load_x(X, T, slot, x);
-          d = octant(x, P, h);
-        }
-        int mypos = -1;
-#pragma unroll
-        for (int dd = 0; dd < 8; ++dd) {
-          const unsigned b = __ballot_sync(0xffffffffu, d == dd);
-          if (d == dd) mypos = mb0 + base_off[dd] + run[dd] + __popc(b & lt);
-          run[dd] += __popc(b);
-        }
-        if (mypos >= 0) tb.members[mypos] = slot;
-      }
-    }
+    split_node_block(X, T, tb, p, err);
     __syncthreads();
   }
-}
-
-// After level `level`: its lists have been consumed; they collect level + 2's nodes next.
-__global__ void k_mark_level(TreeBuffers tb, int level) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    tb.ctr[4 + level] = tb.ctr[0];
-    tb.ctr[kCtrSplit + (level & 1)] = 0;
-    tb.ctr[kCtrSplit + 2 + (level & 1)] = 0;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int nwl = min(tb.ctr[kCtrSplit + 3 + b], tb.max_wrp);
+  for (int wq = warp; wq < nwl; wq += nwarps) {
+    const int p = tb.split_wrp[b][wq];
+    if (tb.nDepth[p] >= kMaxLevels) {
+      if (lane == 0) atomicOr(err, DERR_TREE_DEPTH);
+      continue;
+    }
+    split_node_warp(X, T, tb, p, lane, err);
   }
 }
 
@@ -821,6 +822,12 @@ __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *_
   int best = cl[g];
   double xi[3];
   load3(X, T, (int)g, xi);
+  // The reference forms dist = sqrt(d2) and theta = width/dist at every node.  Both are
+  // correctly rounded, so theta < .5 and dist < cd can differ from d2 > 4 width^2 and
+  // d2 < cd^2 only when d2 lies within a few ulps of the bound: outside a 1e-12 band the
+  // squared comparison decides, inside it the reference's own expressions do.
+  constexpr double kBand = 1e-12;
+  double cd2 = cd * cd;
   int node = s;
   while (node != kEnd) {
     const double4 A = ldg4(&tb.nA[node]);
@@ -829,16 +836,26 @@ __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *_
       node = I.z;
       continue;
     }
-    const double dist = e_sqrt(e_add(e_add(e_sq(e_sub(xi[0], A.x)), e_sq(e_sub(xi[1], A.y))), e_sq(e_sub(xi[2], A.z))));
-    const double theta = e_div(A.w, dist);
-    if (I.x == 1 || theta < .5) {
-      if (dist < cd) {
+    const double d2 = e_add(e_add(e_sq(e_sub(xi[0], A.x)), e_sq(e_sub(xi[1], A.y))), e_sq(e_sub(xi[2], A.z)));
+    bool acc = I.x == 1;
+    if (!acc) {
+      const double w4 = 4.0 * A.w * A.w;
+      if (d2 > w4 * (1 + kBand)) acc = true;
+      else if (d2 >= w4 * (1 - kBand)) acc = e_div(A.w, e_sqrt(d2)) < .5;
+    }
+    if (acc) {
+      bool closer;
+      if (d2 < cd2 * (1 - kBand)) closer = true;
+      else if (d2 > cd2 * (1 + kBand)) closer = false;
+      else closer = e_sqrt(d2) < cd;
+      if (closer) {
         const int j = prv[I.w];
         if (I.x > 1) {
           best = 0;
         } else if (j != (int)g && ni != j && pi_ != j) {
           best = j;
-          cd = dist;
+          cd = e_sqrt(d2);
+          cd2 = cd * cd;
         }
       }
       node = I.z;
@@ -1144,7 +1161,7 @@ void tree_alloc(nv_handle *h) {
   cudaMemset(tb->ctr, 0, kCtrSize * sizeof(int));
   tb->max_blk = (int)(T / (kBigNode + 1) + h->nsys + 64);
   tb->max_wrp = (int)(T / 2 + h->nsys + 64);
-  for (int b = 0; b < 2; ++b) {
+  for (int b = 0; b < 3; ++b) {
     cudaMalloc(&tb->split_blk[b], (size_t)tb->max_blk * sizeof(int));
     cudaMalloc(&tb->split_wrp[b], (size_t)tb->max_wrp * sizeof(int));
   }
@@ -1173,7 +1190,7 @@ void tree_free(nv_handle *h) {
   void *ptrs[] = {tb->nA, tb->nB, tb->nP, tb->nI, tb->nR, tb->nDepth, tb->nLeaf, tb->nSib, tb->members, tb->bigl, tb->ctr,
                   tb->flag, tb->pos, tb->cub_tmp, tb->mx.C, tb->mx.W, tb->mx.G, tb->okey[0], tb->okey[1],
                   tb->oval[0], tb->oval[1], tb->sort_tmp, tb->split_blk[0], tb->split_blk[1],
-                  tb->split_wrp[0], tb->split_wrp[1]};
+                  tb->split_blk[2], tb->split_wrp[0], tb->split_wrp[1], tb->split_wrp[2]};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   delete tb;
@@ -1203,11 +1220,8 @@ void launch_tree_build(nv_handle *h) {
   k_root_sums<<<h->nsys, kSumThreads, kSumSmem, h->side>>>(h->x, T, *tb, h->nsys, h->nxt, h->d_err);
   cudaEventRecord(h->join_ev, h->side);
   const int sms = n_sms();
-  for (int L = 0; L < kMaxLevels; ++L) {
-    k_split_block<<<sms, 1024, 0, h->stream>>>(h->x, T, *tb, L, h->d_err);
-    k_split_warp<<<sms * 8, 128, 0, h->stream>>>(h->x, T, *tb, L, h->d_err);
-    k_mark_level<<<1, 32, 0, h->stream>>>(*tb, L);
-  }
+  for (int L = 0; L < kMaxLevels; ++L)
+    k_split_level<<<sms, 1024, 0, h->stream>>>(h->x, T, *tb, L, h->d_err);
   k_node_sums_block<<<sms, kSumThreads, kSumSmem, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->d_err);
   k_node_sums_big<<<sms * 8, 128, 0, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->nsys, h->d_err);
   k_node_sums_small<<<sms * 8, 128, 0, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->nsys, h->d_err);
