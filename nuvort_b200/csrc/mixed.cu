@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(kTB) k_direct_mixed(const SysConst *__restrict
             const float r1 = a * rsqrtf(a), r2 = ee * rsqrtf(ee);
             const float pp = r1 * r2;
             if (!(pp + re < gd.angle * pp || cr2 < gd.line * D.w * fminf(a, ee) || ee < gd.end * fmaxf(a, D.w))) {
-              const float f = gq * (r1 + r2) * __frcp_rn(pp * (pp + re));
+              const float f = __fdividef(gq * (r1 + r2), pp * (pp + re));  // MUFU reciprocal
               ux = fmaf(f, crx, ux);
               uy = fmaf(f, cry, uy);
               uz = fmaf(f, crz, uz);

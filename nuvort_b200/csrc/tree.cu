@@ -1037,10 +1037,11 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
       } else {
         bool done = false;
         if (D.x == 1) {
-          const int j = __ldg(prv + D.w);
-          if (m == 0 && (j == g || j == pi_)) {
-            done = true;
-          } else if (d2 < near2) {
+          if (m == 0) {  // the target's own segments are skipped in the central image
+            const int j = __ldg(prv + D.w);
+            done = j == g || j == pi_;
+          }
+          if (!done && d2 < near2) {
             exact_term(cur);  // near leaf: the reference arithmetic in FP64
             done = true;
           }
@@ -1061,7 +1062,7 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
               // near its line or near its far end: FP32 would cancel digits there
               exact_term(cur);
             } else {
-              const float f = gq * (r1 + r2) * __frcp_rn(pp * (pp + re));
+              const float f = __fdividef(gq * (r1 + r2), pp * (pp + re));  // MUFU reciprocal
               fx = fmaf(f, cx, fx);
               fy = fmaf(f, cy, fy);
               fz = fmaf(f, cz, fz);
