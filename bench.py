@@ -302,7 +302,17 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
     from nuvort_b200 import api
 
-    params, states, cfg = workload(args.workload, rank, crossover=args.crossover)
+    crossover, tuned = args.crossover, None
+    if args.workload == "ensemble512" and crossover is None:
+        # the direct/tree crossover of the batched ensemble, measured on this GPU
+        from nuvort_b200.autotune import tune_crossover
+        tuned = tune_crossover(device=local, precision=args.precision, delta=0.002, theta=0.4)
+        crossover = tuned["crossover"]
+    params, states, cfg = workload(args.workload, rank, crossover=crossover or 3000)
+    if tuned is not None:
+        cfg["crossover_source"] = ("autotuned on this GPU (nuvort_b200/autotune.py): velocity + tree-build device "
+                                   "time per point of batched systems, direct vs tree"
+                                   + (", cached" if tuned.get("cached") else ""))
     caps = [int(s.pcount * 1.6) + 256 for s in states]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -443,7 +453,9 @@ def main():
     ap.add_argument("--workload", choices=["rings8", "tangle32k", "ensemble512", "tangle1m", "ensemble32"],
                     default="tangle32k")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
-    ap.add_argument("--crossover", type=int, default=3000, help="ensembles: direct sum below this many points")
+    ap.add_argument("--crossover", type=int, default=None,
+                    help="ensembles: direct sum below this many points (default: autotuned for ensemble512, 3000 "
+                         "otherwise)")
     ap.add_argument("--subsample", type=int, default=4096)
     ap.add_argument("--no-compare", dest="compare", action="store_false", help="skip the plain FP64 arm")
     ap.add_argument("--no-e2e", action="store_true")

@@ -55,3 +55,14 @@ def test_batched_velocity_mixed():
         assert rms_rel(um, up) <= 1e-6, k
     hp.close()
     hm.close()
+
+
+def test_autotuned_crossover_is_measured():
+    # two small trial sizes: the tuner runs both methods on batches of systems and returns a
+    # crossover inside the tried range, with the per-point costs it measured
+    from nuvort_b200.autotune import tune_crossover
+    r = tune_crossover(sizes=(400, 1600), batch_points=1 << 13, steps=1, use_cache=False)
+    assert 400 <= r["crossover"] <= 1600
+    assert len(r["trials"]) == 2
+    for t in r["trials"]:
+        assert t["direct_ms_per_point"] > 0 and t["tree_ms_per_point"] > 0
