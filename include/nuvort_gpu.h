@@ -226,6 +226,12 @@ int nv_set_fp32_guards(nv_handle *h, double angle, double line, double end);
  * iteration (default 6 rounds); a system that has not converged runs the serial sweep.
  * Both give the reference's result.  n = 0 runs the serial sweep for every system (0..64). */
 int nv_set_insert_iterations(nv_handle *h, int32_t n);
+/* The tree walks take each root's opening test from a parallel estimate of the root's centre
+ * (the exact centre is a sequential sum over all slots, computed meanwhile on a side stream);
+ * tests within the estimate's error bound are redone once the exact centre is known.
+ * scale (>= 1, default 1) multiplies that bound; a very large scale sends every root test
+ * through the exact path, for testing. */
+int nv_set_root_band(nv_handle *h, double scale);
 
 /* Turn per-step stage timing on (default) or off.  With timing on, nv_step waits for each
  * step and adds its device time per stage to nv_stage_times; off, steps are queued back to

@@ -67,6 +67,7 @@ def lib():
     L.nv_set_near_factor.argtypes = [vp, C.c_double]
     L.nv_set_insert_iterations.argtypes = [vp, C.c_int32]
     L.nv_set_fp32_guards.argtypes = [vp, C.c_double, C.c_double, C.c_double]
+    L.nv_set_root_band.argtypes = [vp, C.c_double]
     L.nv_step_launches.argtypes = [vp, P(i32)]
     L.nv_measure_fp64_peak.argtypes = [i32, P(C.c_double)]
     L.nv_measure_fp32_peak.argtypes = [i32, P(C.c_double)]
@@ -217,6 +218,10 @@ class Handle:
     def set_fp32_guards(self, angle: float, line: float, end: float):
         """Thresholds below which a far mixed-precision term is evaluated in FP64."""
         _check(lib().nv_set_fp32_guards(self.h, float(angle), float(line), float(end)))
+
+    def set_root_band(self, scale: float):
+        """Scale of the root-centre estimate's error bound (huge: every root test exact)."""
+        _check(lib().nv_set_root_band(self.h, float(scale)))
 
     def set_insert_iterations(self, n: int):
         """Fixed-point rounds of the parallel pinsert (0: the serial sweep every step)."""

@@ -407,7 +407,8 @@ int nv_create(const nv_params *params, int32_t nsys, const int32_t *capacity, in
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&h->join_ev, cudaEventDisableTiming) != cudaSuccess)
+      cudaEventCreateWithFlags(&h->join_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->sort_ev, cudaEventDisableTiming) != cudaSuccess)
     return bail(set_error(NV_ERR_CUDA, "stream creation failed"));
   const long long T = h->T;
   if ((rc = dalloc(&h->d_sc, nsys)) || (rc = dalloc(&h->d_dyn, nsys)) || (rc = dalloc(&h->x, 3 * T)) ||
@@ -461,6 +462,7 @@ int nv_destroy(nv_handle *h) {
     if (e) cudaEventDestroy(e);
   if (h->fork_ev) cudaEventDestroy(h->fork_ev);
   if (h->join_ev) cudaEventDestroy(h->join_ev);
+  if (h->sort_ev) cudaEventDestroy(h->sort_ev);
   if (h->side) cudaStreamDestroy(h->side);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -639,6 +641,7 @@ int nv_construct_tree(nv_handle *h) {
   int rc = set_device(h);
   if (rc) return rc;
   launch_tree_build(h);
+  join_root_sums(h);
   return finish(h);
 }
 int nv_pmotion(nv_handle *h) {
@@ -726,6 +729,13 @@ int nv_set_fp32_guards(nv_handle *h, double angle, double line, double end) {
   h->guards.line = (float)line;
   h->guards.end = (float)end;
   h->graph_valid = false;  // launch arguments of the captured kernels
+  return NV_OK;
+}
+
+int nv_set_root_band(nv_handle *h, double scale) {
+  if (!h || !(scale >= 1.0)) return set_error(NV_ERR_ARG, "nv_set_root_band: scale must be >= 1");
+  h->root_band_scale = scale;
+  h->graph_valid = false;  // a launch argument of the captured step
   return NV_OK;
 }
 

@@ -176,12 +176,18 @@ void launch_velocity(nv_handle *h) {
     }
     if (h->any_tree) {
       launch_tree_walk_mixed(h);
+      launch_walk_fixup(h);
       launch_mixed_combine(h, 2);
     }
+    join_root_sums(h);
     return;
   }
   if (h->any_direct) launch_direct(h);
-  if (h->any_tree) launch_tree_walk(h);
+  if (h->any_tree) {
+    launch_tree_walk(h);
+    launch_walk_fixup(h);
+  }
+  join_root_sums(h);
 }
 
 void launch_ab3(nv_handle *h) {

@@ -16,7 +16,7 @@ struct nv_handle {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t side = nullptr;  // concurrent branch of the tree build (root sums)
-  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr, sort_ev = nullptr;
   int nsys = 0;
   int precision = NV_PREC_FP64;
   std::vector<nv_params> params;
@@ -40,6 +40,7 @@ struct nv_handle {
   int n_work_timg = 0;
   double near_factor = 2.0;
   Fp32Guards guards;
+  double root_band_scale = 1.0;  // scale of the root centre estimate's error bound
   int ins_iters = 6;  // fixed-point iterations of the parallel pinsert; 0: serial sweep only
   int tree_sys0 = 0;           // first system that walks the tree (its theta0 builds the mixed nodes)    // near field: pairs closer than near_factor*delta run in FP64
   unsigned *d_err = nullptr;
@@ -96,6 +97,8 @@ void tree_free(nv_handle *h);
 void launch_tree_build(nv_handle *h);
 void launch_tree_walk(nv_handle *h);
 void launch_closest_tree(nv_handle *h);
+void join_root_sums(nv_handle *h);     // the main stream waits for the roots' exact sums
+void launch_walk_fixup(nv_handle *h);  // deferred root tests of the last tree walk
 int tree_dump(nv_handle *h, int sys, void *buf, int cap, int *n);
 // topology (topo.cu)
 void topo_alloc(nv_handle *h);

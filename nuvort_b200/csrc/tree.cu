@@ -32,6 +32,7 @@ constexpr int kCtrBig = kMaxLevels + 6;  // ctr[kCtrBig]: entries of the block-s
 // [+0..+2] nodes above kBigNode members (split by a block), [+3..+5] the others with >= 2
 constexpr int kCtrSplit = kMaxLevels + 8;
 constexpr int kCtrSize = kMaxLevels + 16;
+constexpr int kDeferCap = 1 << 20;  // deferred root tests listed per velocity pass
 constexpr int kFlush = 16;      // FP32 far-field terms summed before promotion to FP64
 
 struct TreeBuffers {
@@ -46,6 +47,14 @@ struct TreeBuffers {
   int *nLeaf = nullptr;
   int *nSib = nullptr;    // next sibling, or kEnd for a last child (and roots)
   int *members = nullptr;
+  // roots: a parallel estimate of the centre with a bound on its distance to the exact
+  // (sequential) one, so the walks need not wait for the exact sum; (target, image) pairs
+  // whose root test the bound cannot settle are listed and redone once the exact sum is in
+  double4 *root_apx = nullptr;  // per system: centre estimate, bound
+  double *root_part = nullptr;  // per system and part: partial sums of x, y, z, |x|, |y|, |z|
+  int root_parts = 1;
+  int2 *defer = nullptr;        // (slot, image) pairs, image -1: the whole target (FP64 walk)
+  int *defer_n = nullptr;
   int *bigl = nullptr;    // non-root nodes with more than kBlockSumNode members
   int max_big = 0;
   int *split_blk[3] = {nullptr, nullptr, nullptr};  // nodes of a level split by a block, by level % 3
@@ -697,14 +706,98 @@ __global__ void __launch_bounds__(kSumThreads) k_root_sums(const double *__restr
   if (threadIdx.x == 0) finish_node(tb, id, true, cx, cy, cz, 0.0, 0.0, 0.0, nxt, err);
 }
 
+// Estimate of each root's centre (the mean over live slots, tree.f90:50-52) by a blocked
+// sum over `parts` blocks per system (k_root_partial, then k_root_approx adding the parts in
+// order), and a bound on its distance to the reference's sequential sum: a sum of N
+// terms in FP64 is within (N-1) u sum|x| of the exact one in either order, so the two means
+// differ by at most 2 u (sum|x| + sum|y| + sum|z|) plus the roundings of the divisions.
+__global__ void __launch_bounds__(256) k_root_partial(const double *__restrict__ X, long long T, TreeBuffers tb,
+                                                      int nsys, int parts) {
+  __shared__ double red[6][8];
+  const int s = blockIdx.x / parts, part = blockIdx.x % parts;
+  if (s >= nsys) return;
+  const int2 R = tb.nR[s];
+  const int per = (R.y + parts - 1) / parts;
+  const int k0 = part * per, k1 = min(R.y, k0 + per);
+  const int *mem = tb.members + R.x;
+  double a[6] = {0, 0, 0, 0, 0, 0};
+  for (int k = k0 + (int)threadIdx.x; k < k1; k += blockDim.x) {
+    const int g = mem[k];
+    for (int c = 0; c < 3; ++c) {
+      const double v = __ldg(X + c * T + g);
+      a[c] += v;
+      a[3 + c] += fabs(v);
+    }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int c = 0; c < 6; ++c) {
+    double v = a[c];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) red[c][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[threadIdx.x][w];
+    tb.root_part[(long long)blockIdx.x * 6 + threadIdx.x] = t;
+  }
+}
+
+__global__ void k_root_approx(TreeBuffers tb, int nsys, int parts, double band_scale) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys) return;
+  double t[6] = {0, 0, 0, 0, 0, 0};
+  for (int q = 0; q < parts; ++q)
+    for (int c = 0; c < 6; ++c) t[c] += tb.root_part[((long long)s * parts + q) * 6 + c];
+  const int n = tb.nR[s].y;
+  const double dn = n > 0 ? (double)n : 1.0;
+  const double cx = t[0] / dn, cy = t[1] / dn, cz = t[2] / dn;
+  const double u = 1.2e-16;
+  const double bound =
+      band_scale * (2.0 * u * (t[3] + t[4] + t[5]) + 8.0 * u * (fabs(cx) + fabs(cy) + fabs(cz)) + 1e-300);
+  tb.root_apx[s] = n > 0 ? make_double4(cx, cy, cz, bound) : make_double4(0, 0, 0, 0);
+}
+
+// The opening test of root `root` (tree.f90:264-278) for target xi and image shift s from
+// the centre estimate: 0 the root is opened, 1 it is accepted (its circulation is zero, so
+// the image adds nothing), 2 the estimate cannot tell.  The root's box is centred on the
+// origin (corner -bsize/2, width bsize), so geo = |centre|.
+__device__ __forceinline__ int root_decision(const TreeBuffers &tb, const SysConst &sc, int root, const double xi[3],
+                                             const double s[3]) {
+  const int4 I = tb.nI[root];
+  if (I.x <= 1) return 2;  // empty or single-slot root: the exact path handles it
+  if (sc.tree_extra_correction && sc.tree_theta > 1.1547) return 2;  // dist <= geo branch
+  const double4 R = tb.root_apx[root];
+  const double d0 = xi[0] - (R.x + s[0]), d1 = xi[1] - (R.y + s[1]), d2 = xi[2] - (R.z + s[2]);
+  const double dist = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+  const double thr = sc.bsize / sc.tree_theta;
+  double margin = dist - thr, pert = R.w;
+  if (sc.tree_extra_correction) {
+    margin -= sqrt(R.x * R.x + R.y * R.y + R.z * R.z);
+    pert *= 2.0;
+  }
+  pert += 1e-12 * (dist + thr);
+  if (margin > pert) return 1;
+  if (margin < -pert) return 0;
+  return 2;
+}
+
+__device__ __forceinline__ void defer_push(const TreeBuffers &tb, int g, int m, unsigned *err) {
+  const int q = atomicAdd(tb.defer_n, 1);
+  if (q < kDeferCap) tb.defer[q] = make_int2(g, m);
+  else atomicOr(err, DERR_QUEUE);
+}
+
 // tree_walk (tree.f90:250-316) for one image; accumulates into acc in preorder.
-__device__ __forceinline__ void walk_fp64(const TreeBuffers &tb, int root, const SysConst &sc, const double xi[3],
+// `start` is the root, or the root's first child when the root is already known to be
+// opened (its test then counted by the caller).
+__device__ __forceinline__ void walk_fp64(const TreeBuffers &tb, int start, const SysConst &sc, const double xi[3],
                                           int gi_, int pi_, const int *__restrict__ prv, const double s[3], bool unshifted,
                                           double acc[3], unsigned long long &evals, unsigned long long &tests,
                                           bool &singular) {
   const double qc = sc.quant_circ, two_pi = sc.two_pi, theta0 = sc.tree_theta;
   const bool corr = sc.tree_extra_correction;
-  int node = root;
+  int node = start;
   while (node != kEnd) {
     const double4 A = ldg4(&tb.nA[node]);
     const int4 I = __ldg(&tb.nI[node]);
@@ -753,6 +846,51 @@ __device__ __forceinline__ void walk_fp64(const TreeBuffers &tb, int root, const
   }
 }
 
+// The velocity of target g (timestep.f90:49-141 with tree_walk): local term, the tree sum
+// over the unshifted image, then over the 26 shifts in order, mutual friction.  With
+// `decided` the root's tests come from the centre estimate: a target for which any of
+// them is too close to call is deferred whole (nothing counted), to be redone exactly.
+__device__ void fp64_target(const SysConst &sc, const SysDyn &dy, int sys, int g, const double *__restrict__ X,
+                            const double *__restrict__ GI, const double *__restrict__ GB,
+                            const int *__restrict__ prv, double *__restrict__ U, long long T, const TreeBuffers &tb,
+                            bool decided, unsigned long long &evals, unsigned long long &tests, unsigned *err) {
+  double xi[3];
+  load3(X, T, g, xi);
+  const double zero[3] = {0, 0, 0};
+  int start[27];
+  const int first = tb.nI[sys].y;
+  unsigned long long t0 = 0;
+  for (int m = 0; m <= sc.n_shift; ++m) {
+    start[m] = sys;
+    if (!decided) continue;
+    const int d = root_decision(tb, sc, sys, xi, m == 0 ? zero : sc.shift[m - 1]);
+    if (d == 2) {
+      defer_push(tb, g, -1, err);
+      return;
+    }
+    start[m] = d == 1 ? kEnd : first;  // accepted: adds nothing; opened: walk the children
+    ++t0;
+  }
+  tests += t0;
+  const int pi_ = prv[g];
+  bool singular = false;
+  double ub0[3] = {0, 0, 0}, ubs[3] = {0, 0, 0};
+  walk_fp64(tb, start[0], sc, xi, g, pi_, prv, zero, true, ub0, evals, tests, singular);
+  for (int m = 0; m < sc.n_shift; ++m)
+    walk_fp64(tb, start[m + 1], sc, xi, g, pi_, prv, sc.shift[m], false, ubs, evals, tests, singular);
+  if (singular) atomicOr(err, DERR_SINGULAR);
+  double gi[3], gb[3], u[3], fdot[3];
+  load3(GI, T, g, gi);
+  load3(GB, T, g, gb);
+  local_velocity(sc, xi, gi, gb, u, fdot);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], ub0[c]);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], ubs[c]);
+  mf_epilogue(sc, dy.t, fdot, u);
+  store3(U, T, g, u);
+}
+
 __global__ void __launch_bounds__(64) k_tree_walk_fp64(const SysConst *__restrict__ scs, SysDyn *dyn,
                                                        const int2 *__restrict__ work, const double *__restrict__ X,
                                                        const double *__restrict__ GI, const double *__restrict__ GB,
@@ -765,28 +903,8 @@ __global__ void __launch_bounds__(64) k_tree_walk_fp64(const SysConst *__restric
   const int g = q >= 1 && q <= sc.cap ? tb.perm[sc.base + q] : sc.base;
   const int k = g - sc.base;
   unsigned long long evals = 0, tests = 0;
-  if (!*err && k >= 1 && k <= dyn[w.x].pcount && nxt[g] != 0) {
-    double xi[3];
-    load3(X, T, g, xi);
-    const int pi_ = prv[g];
-    bool singular = false;
-    double ub0[3] = {0, 0, 0}, ubs[3] = {0, 0, 0};
-    const double zero[3] = {0, 0, 0};
-    walk_fp64(tb, w.x, sc, xi, g, pi_, prv, zero, true, ub0, evals, tests, singular);
-    for (int m = 0; m < sc.n_shift; ++m)
-      walk_fp64(tb, w.x, sc, xi, g, pi_, prv, sc.shift[m], false, ubs, evals, tests, singular);
-    if (singular) atomicOr(err, DERR_SINGULAR);
-    double gi[3], gb[3], u[3], fdot[3];
-    load3(GI, T, g, gi);
-    load3(GB, T, g, gb);
-    local_velocity(sc, xi, gi, gb, u, fdot);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], ub0[c]);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], ubs[c]);
-    mf_epilogue(sc, dyn[w.x].t, fdot, u);
-    store3(U, T, g, u);
-  }
+  if (!*err && k >= 1 && k <= dyn[w.x].pcount && nxt[g] != 0)
+    fp64_target(sc, dyn[w.x], w.x, g, X, GI, GB, prv, U, T, tb, true, evals, tests, err);
   // tree_eval (tree.f90:308): one atomic per warp
   unsigned long long tot = evals, tt = tests;
   for (int o = 16; o > 0; o >>= 1) {
@@ -795,6 +913,39 @@ __global__ void __launch_bounds__(64) k_tree_walk_fp64(const SysConst *__restric
   }
   if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&dyn[w.x].tree_eval, tot);
   if ((threadIdx.x & 31) == 0 && tt) atomicAdd(&dyn[w.x].tree_tests, tt);
+}
+
+// The deferred root tests, after the exact root sums: FP64 targets again whole (image -1),
+// mixed (target, image) pairs as that image's partial sum from the exact FP64 walk.
+__global__ void k_walk_fixup(const SysConst *__restrict__ scs, SysDyn *dyn, const int *__restrict__ sys_of,
+                             const double *__restrict__ X, const double *__restrict__ GI,
+                             const double *__restrict__ GB, const int *__restrict__ prv, double *__restrict__ U,
+                             double *__restrict__ partial, long long T, TreeBuffers tb, unsigned *err) {
+  const int n = min(*tb.defer_n, kDeferCap);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const int2 d = tb.defer[e];
+    const int g = d.x, s = sys_of[g];
+    const SysConst &sc = scs[s];
+    unsigned long long evals = 0, tests = 0;
+    if (d.y < 0) {
+      fp64_target(sc, dyn[s], s, g, X, GI, GB, prv, U, T, tb, false, evals, tests, err);
+    } else {
+      const int m = d.y;
+      double xi[3], acc[3] = {0, 0, 0};
+      const double zero[3] = {0, 0, 0};
+      load3(X, T, g, xi);
+      bool singular = false;
+      walk_fp64(tb, s, sc, xi, g, prv[g], prv, m == 0 ? zero : sc.shift[m - 1], m == 0, acc, evals, tests,
+                singular);
+      if (singular) atomicOr(err, DERR_SINGULAR);
+      const long long o = (long long)m * 3 * T + g;
+      partial[o] = acc[0];
+      partial[o + T] = acc[1];
+      partial[o + 2 * T] = acc[2];
+    }
+    if (evals) atomicAdd(&dyn[s].tree_eval, evals);
+    if (tests) atomicAdd(&dyn[s].tree_tests, tests);
+  }
 }
 
 // pclose_tree + closest_tree (tree.f90:190-244): theta = width/dist < .5, no shift, no
@@ -874,9 +1025,11 @@ __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *_
 // (without the correction: dist > width/theta0); comparing squared distances in FP64 gives
 // the same decisions except at exact ties.  The second branch needs geo > width/theta0,
 // impossible for theta0 <= 2/sqrt(3) (geo <= sqrt(3)/2 width), so it is tested only above.
-__global__ void k_node_prep(TreeBuffers tb, double theta0, int corr) {
+// Roots are skipped: their exact centre may still be summing (the walks take the roots'
+// tests from the centre estimate).
+__global__ void k_node_prep(TreeBuffers tb, int nsys, double theta0, int corr) {
   const int n = tb.ctr[0];
-  for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
+  for (int id = nsys + blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
     const double4 A = tb.nA[id], B = tb.nB[id];
     const double t0 = A.w / theta0;
     const double t1 = corr ? B.w + t0 : t0;
@@ -987,10 +1140,24 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
     ++evals;
     ++n64;
   };
+  // the root's test from the centre estimate: accepted (nothing to add), opened (the walk
+  // starts at its children) or deferred until the exact centre is known
+  int rd = 1;
+  if (valid) {
+    double xi[3];
+    const double zero[3] = {0, 0, 0};
+    load3(X, T, g, xi);
+    rd = root_decision(tb, sc, w.x, xi, m > 0 ? sc.shift[m - 1] : zero);
+    if (rd == 2) defer_push(tb, g, m, err);
+    else ++tests;
+  }
+  const unsigned open0 = __ballot_sync(0xffffffffu, valid && rd == 0);
+  const int first = tb.nI[w.x].y;
+  (void)live;
   // stack entry d: (node, mask) in lane d % 32, register pair 0 for d < 32, 1 above
-  int sn0 = w.x, sn1 = 0;
-  unsigned sm0 = live, sm1 = 0;
-  int top = live ? 0 : -1;
+  int sn0 = first, sn1 = 0;
+  unsigned sm0 = open0, sm1 = 0;
+  int top = open0 && first != kEnd ? 0 : -1;
   while (top >= 0) {
     const int src = top & 31;
     const bool hi = top >= 32;
@@ -1151,6 +1318,12 @@ void tree_alloc(nv_handle *h) {
   // each level holds at most T / (kBlockSumNode + 1) nodes above the block threshold
   tb->max_big = (int)std::min<long long>((long long)kMaxLevels * (T / (kBlockSumNode + 1) + 1) + 64, 1 << 30);
   cudaMalloc(&tb->bigl, (size_t)tb->max_big * sizeof(int));
+  cudaMalloc(&tb->root_apx, (size_t)h->nsys * sizeof(double4));
+  tb->root_parts = std::max(1, std::min(64, 4096 / h->nsys));
+  cudaMalloc(&tb->root_part, (size_t)h->nsys * tb->root_parts * 6 * sizeof(double));
+  cudaMalloc(&tb->defer, (size_t)kDeferCap * sizeof(int2));
+  cudaMalloc(&tb->defer_n, sizeof(int));
+  cudaMemset(tb->defer_n, 0, sizeof(int));
   cudaFuncSetAttribute(k_root_sums, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSumSmem);
   cudaFuncSetAttribute(k_node_sums_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSumSmem);
   if (h->precision == NV_PREC_MIXED) {
@@ -1188,7 +1361,7 @@ void tree_alloc(nv_handle *h) {
 void tree_free(nv_handle *h) {
   TreeBuffers *tb = h->tree;
   if (!tb) return;
-  void *ptrs[] = {tb->nA, tb->nB, tb->nP, tb->nI, tb->nR, tb->nDepth, tb->nLeaf, tb->nSib, tb->members, tb->bigl, tb->ctr,
+  void *ptrs[] = {tb->nA, tb->nB, tb->nP, tb->nI, tb->nR, tb->nDepth, tb->nLeaf, tb->nSib, tb->members, tb->bigl, tb->root_apx, tb->root_part, tb->defer, tb->defer_n, tb->ctr,
                   tb->flag, tb->pos, tb->cub_tmp, tb->mx.C, tb->mx.W, tb->mx.G, tb->okey[0], tb->okey[1],
                   tb->oval[0], tb->oval[1], tb->sort_tmp, tb->split_blk[0], tb->split_blk[1],
                   tb->split_blk[2], tb->split_wrp[0], tb->split_wrp[1], tb->split_wrp[2]};
@@ -1208,7 +1381,9 @@ void launch_tree_build(nv_handle *h) {
   cub::DeviceScan::ExclusiveSum(tb->cub_tmp, bytes, tb->flag, tb->pos, (int)(T + 1), h->stream);
   k_scatter_live<<<grid_for(T, TB), TB, 0, h->stream>>>(tb->flag, tb->pos, tb->members, T);
   k_roots<<<grid_for(h->nsys, 64), 64, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, h->nxt, tb->pos, *tb, T);
-  // the roots' sums (one long sequential chain per system) run beside the splits
+  // the walk order and the roots' exact sums (one long sequential chain per system) run
+  // on the side stream; the walks wait for the order, the fix-up of deferred root tests
+  // and the closest-point walk for the sums
   cudaEventRecord(h->fork_ev, h->stream);
   cudaStreamWaitEvent(h->side, h->fork_ev, 0);
   k_order_keys<<<grid_for(T, TB), TB, 0, h->side>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->nxt, tb->okey[0],
@@ -1218,6 +1393,7 @@ void launch_tree_build(nv_handle *h) {
     cub::DeviceRadixSort::SortPairs(tb->sort_tmp, sb, tb->okey[0], tb->okey[1], tb->oval[0], tb->oval[1], (int)T, 0,
                                     tb->key_bits, h->side);
   }
+  cudaEventRecord(h->sort_ev, h->side);
   k_root_sums<<<h->nsys, kSumThreads, kSumSmem, h->side>>>(h->x, T, *tb, h->nsys, h->nxt, h->d_err);
   cudaEventRecord(h->join_ev, h->side);
   const int sms = n_sms();
@@ -1226,19 +1402,34 @@ void launch_tree_build(nv_handle *h) {
   k_node_sums_block<<<sms, kSumThreads, kSumSmem, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->d_err);
   k_node_sums_big<<<sms * 8, 128, 0, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->nsys, h->d_err);
   k_node_sums_small<<<sms * 8, 128, 0, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->nsys, h->d_err);
-  cudaStreamWaitEvent(h->stream, h->join_ev, 0);
+  k_root_partial<<<h->nsys * tb->root_parts, 256, 0, h->stream>>>(h->x, T, *tb, h->nsys, tb->root_parts);
+  k_root_approx<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(*tb, h->nsys, tb->root_parts, h->root_band_scale);
+  cudaStreamWaitEvent(h->stream, h->sort_ev, 0);
   if (h->precision == NV_PREC_MIXED) {
     // theta0 and the correction flag are per system; a handle's systems share them when
     // any of them walks the tree (checked at creation)
-    k_node_prep<<<sms * 4, 256, 0, h->stream>>>(*tb, h->sc[h->tree_sys0].tree_theta,
+    k_node_prep<<<sms * 4, 256, 0, h->stream>>>(*tb, h->nsys, h->sc[h->tree_sys0].tree_theta,
                                                 h->sc[h->tree_sys0].tree_extra_correction);
   }
   tb->built = true;
 }
 
+void join_root_sums(nv_handle *h) {
+  if (h->tree) cudaStreamWaitEvent(h->stream, h->join_ev, 0);
+}
+
+void launch_walk_fixup(nv_handle *h) {
+  TreeBuffers *tb = h->tree;
+  if (!tb) return;
+  join_root_sums(h);
+  k_walk_fixup<<<n_sms(), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->gi, h->gb, h->prv, h->u,
+                                               h->partial, h->T, *tb, h->d_err);
+}
+
 void launch_tree_walk(nv_handle *h) {
   TreeBuffers *tb = h->tree;
   if (!tb || h->n_work_tree == 0) return;
+  cudaMemsetAsync(tb->defer_n, 0, sizeof(int), h->stream);
   k_tree_walk_fp64<<<h->n_work_tree, 64, 0, h->stream>>>(h->d_sc, h->d_dyn, h->d_work_tree, h->x, h->gi, h->gb,
                                                          h->nxt, h->prv, h->u, h->T, *tb, h->d_err);
 }
@@ -1246,6 +1437,7 @@ void launch_tree_walk(nv_handle *h) {
 void launch_tree_walk_mixed(nv_handle *h) {
   TreeBuffers *tb = h->tree;
   if (!tb || h->n_work_timg == 0) return;
+  cudaMemsetAsync(tb->defer_n, 0, sizeof(int), h->stream);
   k_tree_walk_mixed<<<h->n_work_timg, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->d_work_timg, h->x, h->nxt, h->prv,
                                                            h->partial, h->T, *tb, h->near_factor, h->guards,
                                                            h->d_err);
@@ -1254,6 +1446,7 @@ void launch_tree_walk_mixed(nv_handle *h) {
 void launch_closest_tree(nv_handle *h) {
   TreeBuffers *tb = h->tree;
   if (!tb) return;
+  join_root_sums(h);
   k_closest_tree<<<grid_for(h->T, 128), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->nxt, h->prv,
                                                               h->closest, h->closestd, h->T, *tb, h->d_err);
 }

@@ -64,3 +64,18 @@ def test_mixed_whole_steps_events_match_plain():
             ev.append(h.events())
     assert len(ev[0]) > 0
     assert ev[0] == ev[1]
+
+
+def test_mixed_tree_with_root_tests_deferred():
+    # every (target, image) root test deferred: those images' partials come from the exact
+    # FP64 walk after the root sums, still within the mixed tolerance of the plain path
+    from nuvort_b200.api import Handle
+    st = tangle(2, 0.001, n_points=4096)
+    hp = Handle(config1_params("Tree", tree_theta=0.4), [st.pcount + 512], states=[st])
+    up = hp.calc_velocity()
+    hm = Handle(config1_params("Tree", tree_theta=0.4, precision="mixed"), [st.pcount + 512], states=[st])
+    hm.set_root_band(1e30)
+    um = hm.calc_velocity()
+    assert rms_rel(um, up) <= TOL_RMS
+    hp.close()
+    hm.close()

@@ -129,3 +129,21 @@ def test_tree_opening_test_count_matches_oracle():
     o.calc_velocity()
     assert h.counters().tree_tests == o.counters().tree_tests
     h.close()
+
+
+def test_root_tests_all_deferred_give_the_same_velocity():
+    # the walks take the roots' tests from a parallel estimate of the root centre and redo
+    # the undecidable ones after the exact (sequential) sum: forcing every one through that
+    # path must give the same velocities, bit for bit, and the oracle's counts
+    st = tangle(1, 0.001, n_points=4096)
+    p = config1_params("Tree")
+    h = _handle(p, st)
+    u0 = h.calc_velocity()
+    h.set_root_band(1e30)
+    u1 = h.calc_velocity()
+    c1 = h.counters()
+    o = Oracle(p, st)
+    o.calc_velocity()
+    assert np.array_equal(u0, u1)
+    assert c1.tree_eval == o.counters().tree_eval and c1.tree_tests == o.counters().tree_tests
+    h.close()
