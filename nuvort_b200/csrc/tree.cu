@@ -50,6 +50,14 @@ struct TreeBuffers {
   // roots: a parallel estimate of the centre with a bound on its distance to the exact
   // (sequential) one, so the walks need not wait for the exact sum; (target, image) pairs
   // whose root test the bound cannot settle are listed and redone once the exact sum is in
+  // the roots' split as one stable radix sort of the live slots by (system, octant)
+  unsigned *rkey[2] = {nullptr, nullptr};
+  int *rval[2] = {nullptr, nullptr};
+  int *root_cnt = nullptr;  // per system: members per octant
+  int *root_mb = nullptr;   // per system: first member entry of the children
+  void *rsort_tmp = nullptr;
+  size_t rsort_bytes = 0;
+  int rkey_bits = 0;
   double4 *root_apx = nullptr;  // per system: centre estimate, bound
   double *root_part = nullptr;  // per system and part: partial sums of x, y, z, |x|, |y|, |z|
   int root_parts = 1;
@@ -138,7 +146,7 @@ __global__ void k_roots(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys,
   tb.nR[s] = make_int2(pos[sc.base], pos[sc.base + sc.cap + 1] - pos[sc.base]);
   tb.nDepth[s] = 0;
   tb.nSib[s] = kEnd;
-  if (pc >= 2) push_split(tb, s, tb.nR[s].y, 0, nullptr);
+  for (int d = 0; d < 8; ++d) tb.root_cnt[8 * s + d] = 0;
   tb.nLeaf[s] = pc == 1 ? sc.base + 1 : 0;
   dyn[s].tree_eval = 0;
   dyn[s].tree_tests = 0;
@@ -271,6 +279,54 @@ __device__ void make_children(TreeBuffers &tb, int p, const int cnt[8], int *id0
   tb.nI[p].y = id0;
   *id0_out = id0;
   *mb0_out = mb0;
+}
+
+// The roots' split (build_tree at the root, tree.f90:66-94) for every system at once: the
+// live slots, in slot order, are sorted stably by (system, octant digit; 8 for a point in
+// no child), which lists each child's members in slot order, as the warp and block splits
+// do node by node.
+__global__ void k_root_digits(const double *__restrict__ X, long long T, TreeBuffers tb,
+                              const int *__restrict__ sys_of, const int *__restrict__ pos) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= T) return;
+  const int n_live = pos[T];
+  if (q >= n_live) {
+    tb.rkey[0][q] = 0xFFFFFFFFu;
+    tb.rval[0][q] = 0;
+    return;
+  }
+  const int g = tb.members[q];
+  const int s = sys_of[g];
+  int d = 8;
+  if (tb.nI[s].x >= 2) {
+    double x[3];
+    load_x(X, T, g, x);
+    d = octant(x, tb.nP[s], tb.nA[s].w / 2.0);
+    if (d < 8) atomicAdd(&tb.root_cnt[8 * s + d], 1);
+  }
+  tb.rkey[0][q] = ((unsigned)s << 4) | (unsigned)d;
+  tb.rval[0][q] = g;
+}
+
+__global__ void k_root_children(TreeBuffers tb, int nsys, unsigned *err) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys) return;
+  tb.root_mb[s] = -1;
+  if (tb.nI[s].x < 2) return;
+  int cnt[8];
+  for (int d = 0; d < 8; ++d) cnt[d] = tb.root_cnt[8 * s + d];
+  int id0 = -1, mb0 = -1;
+  make_children(tb, s, cnt, &id0, &mb0, err);
+  tb.root_mb[s] = mb0;
+}
+
+__global__ void k_root_scatter(TreeBuffers tb, const int *__restrict__ pos, long long T) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= T || p >= pos[T]) return;
+  const unsigned key = tb.rkey[1][p];
+  const int s = (int)(key >> 4), d = (int)(key & 15u);
+  const int mb = tb.root_mb[s];
+  if (d < 8 && mb >= 0) tb.members[mb + (int)(p - tb.nR[s].x)] = tb.rval[1][p];
 }
 
 // Split node p (at most kBigNode members) with one warp: count the members per octant, make
@@ -1319,6 +1375,20 @@ void tree_alloc(nv_handle *h) {
   tb->max_big = (int)std::min<long long>((long long)kMaxLevels * (T / (kBlockSumNode + 1) + 1) + 64, 1 << 30);
   cudaMalloc(&tb->bigl, (size_t)tb->max_big * sizeof(int));
   cudaMalloc(&tb->root_apx, (size_t)h->nsys * sizeof(double4));
+  for (int b = 0; b < 2; ++b) {
+    cudaMalloc(&tb->rkey[b], (size_t)T * sizeof(unsigned));
+    cudaMalloc(&tb->rval[b], (size_t)T * sizeof(int));
+  }
+  cudaMalloc(&tb->root_cnt, (size_t)h->nsys * 8 * sizeof(int));
+  cudaMalloc(&tb->root_mb, (size_t)h->nsys * sizeof(int));
+  {
+    int sb = 1;
+    while ((1LL << sb) < h->nsys) ++sb;
+    tb->rkey_bits = std::min(32, 4 + sb);
+    cub::DeviceRadixSort::SortPairs(nullptr, tb->rsort_bytes, tb->rkey[0], tb->rkey[1], tb->rval[0], tb->rval[1],
+                                    (int)T, 0, tb->rkey_bits);
+    cudaMalloc(&tb->rsort_tmp, std::max<size_t>(tb->rsort_bytes, 16));
+  }
   tb->root_parts = std::max(1, std::min(64, 4096 / h->nsys));
   cudaMalloc(&tb->root_part, (size_t)h->nsys * tb->root_parts * 6 * sizeof(double));
   cudaMalloc(&tb->defer, (size_t)kDeferCap * sizeof(int2));
@@ -1361,7 +1431,8 @@ void tree_alloc(nv_handle *h) {
 void tree_free(nv_handle *h) {
   TreeBuffers *tb = h->tree;
   if (!tb) return;
-  void *ptrs[] = {tb->nA, tb->nB, tb->nP, tb->nI, tb->nR, tb->nDepth, tb->nLeaf, tb->nSib, tb->members, tb->bigl, tb->root_apx, tb->root_part, tb->defer, tb->defer_n, tb->ctr,
+  void *ptrs[] = {tb->nA, tb->nB, tb->nP, tb->nI, tb->nR, tb->nDepth, tb->nLeaf, tb->nSib, tb->members, tb->bigl, tb->root_apx, tb->root_part, tb->defer, tb->defer_n,
+                  tb->rkey[0], tb->rkey[1], tb->rval[0], tb->rval[1], tb->root_cnt, tb->root_mb, tb->rsort_tmp, tb->ctr,
                   tb->flag, tb->pos, tb->cub_tmp, tb->mx.C, tb->mx.W, tb->mx.G, tb->okey[0], tb->okey[1],
                   tb->oval[0], tb->oval[1], tb->sort_tmp, tb->split_blk[0], tb->split_blk[1],
                   tb->split_blk[2], tb->split_wrp[0], tb->split_wrp[1], tb->split_wrp[2]};
@@ -1397,7 +1468,15 @@ void launch_tree_build(nv_handle *h) {
   k_root_sums<<<h->nsys, kSumThreads, kSumSmem, h->side>>>(h->x, T, *tb, h->nsys, h->nxt, h->d_err);
   cudaEventRecord(h->join_ev, h->side);
   const int sms = n_sms();
-  for (int L = 0; L < kMaxLevels; ++L)
+  k_root_digits<<<grid_for(T, TB), TB, 0, h->stream>>>(h->x, T, *tb, h->sys_of, tb->pos);
+  {
+    size_t sb = tb->rsort_bytes;
+    cub::DeviceRadixSort::SortPairs(tb->rsort_tmp, sb, tb->rkey[0], tb->rkey[1], tb->rval[0], tb->rval[1], (int)T, 0,
+                                    tb->rkey_bits, h->stream);
+  }
+  k_root_children<<<grid_for(h->nsys, 64), 64, 0, h->stream>>>(*tb, h->nsys, h->d_err);
+  k_root_scatter<<<grid_for(T, TB), TB, 0, h->stream>>>(*tb, tb->pos, T);
+  for (int L = 1; L < kMaxLevels; ++L)
     k_split_level<<<sms, 1024, 0, h->stream>>>(h->x, T, *tb, L, h->d_err);
   k_node_sums_block<<<sms, kSumThreads, kSumSmem, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->d_err);
   k_node_sums_big<<<sms * 8, 128, 0, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->nsys, h->d_err);
