@@ -408,7 +408,10 @@ int nv_create(const nv_params *params, int32_t nsys, const int32_t *capacity, in
       cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->join_ev, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&h->sort_ev, cudaEventDisableTiming) != cudaSuccess)
+      cudaEventCreateWithFlags(&h->sort_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->side2, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->fork2_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->join2_ev, cudaEventDisableTiming) != cudaSuccess)
     return bail(set_error(NV_ERR_CUDA, "stream creation failed"));
   const long long T = h->T;
   if ((rc = dalloc(&h->d_sc, nsys)) || (rc = dalloc(&h->d_dyn, nsys)) || (rc = dalloc(&h->x, 3 * T)) ||
@@ -463,6 +466,9 @@ int nv_destroy(nv_handle *h) {
   if (h->fork_ev) cudaEventDestroy(h->fork_ev);
   if (h->join_ev) cudaEventDestroy(h->join_ev);
   if (h->sort_ev) cudaEventDestroy(h->sort_ev);
+  if (h->fork2_ev) cudaEventDestroy(h->fork2_ev);
+  if (h->join2_ev) cudaEventDestroy(h->join2_ev);
+  if (h->side2) cudaStreamDestroy(h->side2);
   if (h->side) cudaStreamDestroy(h->side);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;

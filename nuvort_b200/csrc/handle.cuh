@@ -15,7 +15,9 @@ enum { ST_GHOST = 0, ST_TREE, ST_VELOCITY, ST_AB3, ST_TOPO, ST_STEP, ST_INSERT, 
 struct nv_handle {
   int device = 0;
   cudaStream_t stream = nullptr;
-  cudaStream_t side = nullptr;  // concurrent branch of the tree build (root sums)
+  cudaStream_t side = nullptr;  // concurrent branch of the tree build (walk order, root sums)
+  cudaStream_t side2 = nullptr;  // second branch (sums of the large shallow nodes)
+  cudaEvent_t fork2_ev = nullptr, join2_ev = nullptr;
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr, sort_ev = nullptr;
   int nsys = 0;
   int precision = NV_PREC_FP64;

@@ -28,6 +28,8 @@ constexpr int kEnd = -1;
 constexpr int kBigNode = 2048;  // nodes with more members are split by a whole block
 constexpr int kBlockSumNode = 8192;  // nodes with more members are summed by a whole block
 constexpr int kCtrBig = kMaxLevels + 6;  // ctr[kCtrBig]: entries of the block-summed node list
+constexpr int kCtrBigSnap = kMaxLevels + 7;  // entries listed when the early block sums start
+constexpr int kSnapLevel = 4;  // after this level's split the early block sums start
 // ctr[kCtrSplit + b]: entries of the level lists of nodes to split, by level % 3 = b:
 // [+0..+2] nodes above kBigNode members (split by a block), [+3..+5] the others with >= 2
 constexpr int kCtrSplit = kMaxLevels + 8;
@@ -523,7 +525,7 @@ __device__ __forceinline__ void finish_node(TreeBuffers &tb, int id, bool root, 
   if (!root) {
     const int first = R.y > 0 ? tb.members[R.x] : 0;
     I.w = first ? nxt[first] : 0;
-    tb.nI[id] = I;
+    tb.nI[id].w = I.w;  // the node's other links belong to the splits
     tb.nLeaf[id] = I.x == 1 ? first : 0;
     if (tb.nDepth[id] >= kMaxLevels && I.x > 1) atomicOr(err, DERR_TREE_DEPTH);
   }
@@ -729,11 +731,17 @@ __device__ void block_node_sums(const double *__restrict__ X, const double *__re
 __global__ void __launch_bounds__(kSumThreads) k_node_sums_block(const double *__restrict__ X,
                                                                   const double *__restrict__ GI,
                                                                   const int *__restrict__ nxt, long long T,
-                                                                  TreeBuffers tb, unsigned *err) {
+                                                                  TreeBuffers tb, int part, unsigned *err) {
+  // part 0: the nodes listed by the snapshot (split by then, so their member lists are
+  // final), summed beside the deeper levels' splits; part 1: the ones listed after it
+  // (only nodes at depth <= kSnapLevel: already split, so nothing else writes them)
   extern __shared__ double sm_dyn[];
-  const int nbig = min(tb.ctr[kCtrBig], tb.max_big);
+  const int snap = tb.ctr[kCtrBigSnap];
+  const int nbig = part == 0 ? snap : min(tb.ctr[kCtrBig], tb.max_big);
   for (int b = blockIdx.x; b < nbig; b += gridDim.x) {
     const int id = tb.bigl[b];
+    const bool early = b < snap && tb.nDepth[id] <= kSnapLevel;
+    if (early != (part == 0)) continue;  // block-uniform
     const int2 R = tb.nR[id];
     double acc;
     block_node_sums(X, GI, T, tb.members + R.x, R.y, true, sm_dyn, acc);
@@ -743,6 +751,10 @@ __global__ void __launch_bounds__(kSumThreads) k_node_sums_block(const double *_
     if (threadIdx.x == 0) finish_node(tb, id, false, cx, cy, cz, qx, qy, qz, nxt, err);
     __syncthreads();
   }
+}
+
+__global__ void k_big_snapshot(TreeBuffers tb) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) tb.ctr[kCtrBigSnap] = min(tb.ctr[kCtrBig], tb.max_big);
 }
 
 // Roots: the masked mean over live slots (tree.f90:50-54), circulation zero.  One block per
@@ -1476,14 +1488,23 @@ void launch_tree_build(nv_handle *h) {
   }
   k_root_children<<<grid_for(h->nsys, 64), 64, 0, h->stream>>>(*tb, h->nsys, h->d_err);
   k_root_scatter<<<grid_for(T, TB), TB, 0, h->stream>>>(*tb, tb->pos, T);
-  for (int L = 1; L < kMaxLevels; ++L)
+  for (int L = 1; L < kMaxLevels; ++L) {
     k_split_level<<<sms, 1024, 0, h->stream>>>(h->x, T, *tb, L, h->d_err);
-  k_node_sums_block<<<sms, kSumThreads, kSumSmem, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->d_err);
+    if (L == kSnapLevel) {  // the large shallow nodes' sums overlap the deeper splits
+      k_big_snapshot<<<1, 32, 0, h->stream>>>(*tb);
+      cudaEventRecord(h->fork2_ev, h->stream);
+      cudaStreamWaitEvent(h->side2, h->fork2_ev, 0);
+      k_node_sums_block<<<sms, kSumThreads, kSumSmem, h->side2>>>(h->x, h->gi, h->nxt, T, *tb, 0, h->d_err);
+      cudaEventRecord(h->join2_ev, h->side2);
+    }
+  }
+  k_node_sums_block<<<sms, kSumThreads, kSumSmem, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, 1, h->d_err);
   k_node_sums_big<<<sms * 8, 128, 0, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->nsys, h->d_err);
   k_node_sums_small<<<sms * 8, 128, 0, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->nsys, h->d_err);
   k_root_partial<<<h->nsys * tb->root_parts, 256, 0, h->stream>>>(h->x, T, *tb, h->nsys, tb->root_parts);
   k_root_approx<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(*tb, h->nsys, tb->root_parts, h->root_band_scale);
   cudaStreamWaitEvent(h->stream, h->sort_ev, 0);
+  cudaStreamWaitEvent(h->stream, h->join2_ev, 0);
   if (h->precision == NV_PREC_MIXED) {
     // theta0 and the correction flag are per system; a handle's systems share them when
     // any of them walks the tree (checked at creation)
