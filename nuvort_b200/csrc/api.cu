@@ -478,6 +478,7 @@ int nv_destroy(nv_handle *h) {
 int nv_upload(nv_handle *h, int32_t sys, const nv_host_state *st) {
   if (!h || !st || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_upload: bad arguments");
   if (!st->x || !st->infront || !st->behind) return set_error(NV_ERR_ARG, "nv_upload: x, infront, behind are required");
+  ++h->links_epoch;
   const int n = st->pcount, cap = h->cap[sys], base = h->base[sys];
   if (n < 0 || n > cap) return set_error(NV_ERR_ARG, "nv_upload: pcount exceeds the system's capacity");
   int rc = set_device(h);

@@ -40,11 +40,12 @@ struct nv_handle {
   int n_work_img = 0;
   int4 *d_work_timg = nullptr; // same for the mixed tree walk
   int n_work_timg = 0;
-  double near_factor = 2.0;
+  double near_factor = 2.0;    // near field: pairs closer than near_factor*delta run in FP64
   Fp32Guards guards;
   double root_band_scale = 1.0;  // scale of the root centre estimate's error bound
   int ins_iters = 6;  // fixed-point iterations of the parallel pinsert; 0: serial sweep only
-  int tree_sys0 = 0;           // first system that walks the tree (its theta0 builds the mixed nodes)    // near field: pairs closer than near_factor*delta run in FP64
+  int tree_sys0 = 0;           // first system that walks the tree (its theta0 builds the mixed nodes)
+  unsigned links_epoch = 0;    // bumped by every stage that relinks points (pinsert, precon, premove, upload)
   unsigned *d_err = nullptr;
   DevEvent *d_events = nullptr;
   int *d_event_count = nullptr;

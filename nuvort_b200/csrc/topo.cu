@@ -1632,6 +1632,7 @@ void topo_free(nv_handle *h) {
 }
 
 void launch_pinsert(nv_handle *h) {
+  ++h->links_epoch;
   TopoBuffers *tb = h->topo;
   const long long T = h->T;
   k_ins_begin<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_dyn, h->nsys);
@@ -1699,6 +1700,7 @@ void launch_pclose(nv_handle *h, bool only_brute) {
 }
 
 void launch_precon(nv_handle *h) {
+  ++h->links_epoch;
   TopoBuffers *tb = h->topo;
   k_mark_recon<<<grid_for(h->T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->closestd, h->nxt,
                                                               tb->flag_a, h->T, h->d_err);
@@ -1708,6 +1710,7 @@ void launch_precon(nv_handle *h) {
 }
 
 void launch_premove(nv_handle *h) {
+  ++h->links_epoch;
   TopoBuffers *tb = h->topo;
   k_mark_remove<<<grid_for(h->T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->nxt,
                                                                tb->flag_a, h->T, h->d_err);

@@ -36,6 +36,7 @@ constexpr int kCtrSplit = kMaxLevels + 8;
 constexpr int kCtrSize = kMaxLevels + 16;
 constexpr int kDeferCap = 1 << 20;  // deferred root tests listed per velocity pass
 constexpr int kFlush = 16;      // FP32 far-field terms summed before promotion to FP64
+static_assert((kFlush & (kFlush - 1)) == 0, "the walk tests the flush by a mask");
 
 struct TreeBuffers {
   int max_nodes = 0;
@@ -83,6 +84,7 @@ struct TreeBuffers {
   int key_bits = 0;
   bool built = false;
   MixedNodes mx;
+  unsigned prep_epoch = ~0u;  // the handle's links epoch when the mixed records took prv
 };
 
 namespace {
@@ -1016,6 +1018,19 @@ __global__ void k_walk_fixup(const SysConst *__restrict__ scs, SysDyn *dyn, cons
   }
 }
 
+// Squared distance from x to the cell [P, P + w]^3 (0 inside).
+__device__ __forceinline__ double cube_dist2(const double x[3], const double4 P, double w) {
+  const double p[3] = {P.x, P.y, P.z};
+  double d2 = 0.;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double lo = p[c] - x[c], hi = x[c] - (p[c] + w);
+    const double d = fmax(fmax(lo, hi), 0.);
+    d2 += d * d;
+  }
+  return d2;
+}
+
 // pclose_tree + closest_tree (tree.f90:190-244): theta = width/dist < .5, no shift, no
 // correction; the candidate is prv(first member's infront at build time) with the links of
 // now (after pinsert).
@@ -1047,6 +1062,9 @@ __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *_
   // squared comparison decides, inside it the reference's own expressions do.
   constexpr double kBand = 1e-12;
   double cd2 = cd * cd;
+  // slack of the subtree skip below: covers the rounding of the centroids (sums of up to
+  // 2^24 positions) and of the distances
+  const double margin = 1e-8 * sc.bsize;
   int node = s;
   while (node != kEnd) {
     const double4 A = ldg4(&tb.nA[node]);
@@ -1078,6 +1096,11 @@ __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *_
         }
       }
       node = I.z;
+    } else if (I.y != kEnd && node != s && cube_dist2(xi, ldg4(&tb.nP[node]), A.w) > (cd + margin) * (cd + margin)) {
+      // Every member of this node lies in its cell (the splits drop points outside the
+      // children's cells), so every centroid in its subtree is farther than cd: none is
+      // closer, now or later (cd only shrinks), and none changes best or cd.  Skipped.
+      node = I.z;
     } else {
       node = I.y != kEnd ? I.y : I.z;
     }
@@ -1095,7 +1118,7 @@ __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *_
 // impossible for theta0 <= 2/sqrt(3) (geo <= sqrt(3)/2 width), so it is tested only above.
 // Roots are skipped: their exact centre may still be summing (the walks take the roots'
 // tests from the centre estimate).
-__global__ void k_node_prep(TreeBuffers tb, int nsys, double theta0, int corr) {
+__global__ void k_node_prep(TreeBuffers tb, int nsys, double theta0, int corr, const int *__restrict__ prv) {
   const int n = tb.ctr[0];
   for (int id = nsys + blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
     const double4 A = tb.nA[id], B = tb.nB[id];
@@ -1110,8 +1133,18 @@ __global__ void k_node_prep(TreeBuffers tb, int nsys, double theta0, int corr) {
     wn.a = make_float4(hx, hy, hz, (float)(t1 * t1));
     wn.b = make_float4((float)(A.x - hx), (float)(A.y - hy), (float)(A.z - hz), qx * qx + qy * qy + qz * qz);
     wn.c = make_float4(qx, qy, qz, 0.f);
-    wn.d = make_int4(I.x, I.y, tb.nSib[id], I.w);
+    wn.d = make_int4(I.x, I.y, tb.nSib[id], I.x == 1 ? prv[I.w] : I.w);
     tb.mx.W[id] = wn;
+  }
+}
+
+// A leaf's record holds prv of its member, the start of the leaf's segment, for the walk's
+// own-segment test; this refreshes it when points were relinked after the build.
+__global__ void k_leaf_links(TreeBuffers tb, int nsys, const int *__restrict__ prv) {
+  const int n = tb.ctr[0];
+  for (int id = nsys + blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
+    const int4 I = tb.nI[id];
+    if (I.x == 1) tb.mx.W[id].d.w = prv[I.w];
   }
 }
 
@@ -1166,7 +1199,6 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
   const float gq = (float)(sc.quant_circ / (4.0 * NV_PI));
   const bool second = sc.tree_extra_correction && sc.tree_theta > 1.1547;
   float fx = 0, fy = 0, fz = 0;  // FP32 partial over at most kFlush far interactions
-  int nfar = 0;
   double nx = 0, ny = 0, nz = 0;  // FP64: near field plus the flushed FP32 partials
   bool singular = false;
   // r and |r|^2 in FP64 as the FP64 walk forms them: (centre + shift) - target
@@ -1222,29 +1254,22 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
   const unsigned open0 = __ballot_sync(0xffffffffu, valid && rd == 0);
   const int first = tb.nI[w.x].y;
   (void)live;
-  // stack entry d: (node, mask) in lane d % 32, register pair 0 for d < 32, 1 above
-  int sn0 = first, sn1 = 0;
-  unsigned sm0 = open0, sm1 = 0;
-  int top = open0 && first != kEnd ? 0 : -1;
-  while (top >= 0) {
-    const int src = top & 31;
-    const bool hi = top >= 32;
-    const int cur = __shfl_sync(0xffffffffu, hi ? sn1 : sn0, src);
-    const unsigned mask = __shfl_sync(0xffffffffu, hi ? sm1 : sm0, src);
+  // (cur, mask): the node the warp is at and the lanes whose walk reaches it, warp-uniform.
+  // The stack holds the pending next siblings of the nodes opened on the way down: entry d
+  // (node, mask) in lane d % 32, register pair 0 for d < 32, 1 above.
+  int sn0 = 0, sn1 = 0;
+  unsigned sm0 = 0, sm1 = 0;
+  int top = -1;
+  int cur = first;
+  unsigned mask = open0;
+  bool more = open0 && first != kEnd;
+  while (more) {
     const WalkNode *wn = tb.mx.W + cur;
+    // the whole 64-byte record at once: one load latency per node instead of a chain
     const int4 D = __ldg(&wn->d);
-    if (D.z != kEnd) {  // the entry moves on to the next sibling
-      if (lane == src) {
-        if (hi) sn1 = D.z;
-        else sn0 = D.z;
-      }
-    } else {
-      --top;
-    }
-    if (D.x == 0) continue;
+    const float4 A = __ldg(&wn->a), B = __ldg(&wn->b), Q = __ldg(&wn->c);
     bool open = false;
-    if ((mask >> lane) & 1u) {
-      const float4 A = __ldg(&wn->a), B = __ldg(&wn->b);
+    if (D.x != 0 && ((mask >> lane) & 1u)) {
       ++tests;
       const float rx = (A.x - xh[0]) + (B.x - xl[0]);
       const float ry = (A.y - xh[1]) + (B.y - xl[1]);
@@ -1272,17 +1297,14 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
       } else {
         bool done = false;
         if (D.x == 1) {
-          if (m == 0) {  // the target's own segments are skipped in the central image
-            const int j = __ldg(prv + D.w);
-            done = j == g || j == pi_;
-          }
+          if (m == 0)  // the target's own segments are skipped in the central image
+            done = D.w == g || D.w == pi_;  // D.w: prv of the leaf's member
           if (!done && d2 < near2) {
             exact_term(cur);  // near leaf: the reference arithmetic in FP64
             done = true;
           }
         }
         if (!done) {
-          const float4 Q = __ldg(&wn->c);
           // the reference skips 4ac-b^2 < epsilon (tree.f90:303); 4ac-b^2 = 4|r x circ|^2
           const float cx = fmaf(ry, Q.z, -rz * Q.y), cy = fmaf(rz, Q.x, -rx * Q.z), cz = fmaf(rx, Q.y, -ry * Q.x);
           const float cr2 = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
@@ -1301,13 +1323,11 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
               fx = fmaf(f, cx, fx);
               fy = fmaf(f, cy, fy);
               fz = fmaf(f, cz, fz);
-              ++evals;
-              if (++nfar == kFlush) {
+              if ((++evals & (kFlush - 1)) == 0) {  // at most kFlush FP32 terms per partial
                 nx += (double)fx;
                 ny += (double)fy;
                 nz += (double)fz;
                 fx = fy = fz = 0.f;
-                nfar = 0;
               }
             }
           }
@@ -1316,20 +1336,34 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
     }
     const unsigned omask = __ballot_sync(0xffffffffu, open);
     if (omask && D.y != kEnd) {  // the lanes that open cur walk its children first
-      ++top;
-      if (top >= kWalkStack) {  // deeper than any tree the build makes; guard only
-        if (lane == 0) atomicOr(err, DERR_TREE_DEPTH);
-        break;
-      }
-      if (lane == (top & 31)) {
-        if (top >= 32) {
-          sn1 = D.y;
-          sm1 = omask;
-        } else {
-          sn0 = D.y;
-          sm0 = omask;
+      if (D.z != kEnd) {         // and come back to cur's next sibling afterwards
+        ++top;
+        if (top >= kWalkStack) {  // deeper than any tree the build makes; guard only
+          if (lane == 0) atomicOr(err, DERR_TREE_DEPTH);
+          break;
+        }
+        if (lane == (top & 31)) {
+          if (top >= 32) {
+            sn1 = D.z;
+            sm1 = mask;
+          } else {
+            sn0 = D.z;
+            sm0 = mask;
+          }
         }
       }
+      cur = D.y;
+      mask = omask;
+    } else if (D.z != kEnd) {
+      cur = D.z;
+    } else if (top >= 0) {
+      const int src = top & 31;
+      const bool hi = top >= 32;
+      cur = __shfl_sync(0xffffffffu, hi ? sn1 : sn0, src);
+      mask = __shfl_sync(0xffffffffu, hi ? sm1 : sm0, src);
+      --top;
+    } else {
+      more = false;
     }
   }
   if (singular) atomicOr(err, DERR_SINGULAR);
@@ -1509,7 +1543,8 @@ void launch_tree_build(nv_handle *h) {
     // theta0 and the correction flag are per system; a handle's systems share them when
     // any of them walks the tree (checked at creation)
     k_node_prep<<<sms * 4, 256, 0, h->stream>>>(*tb, h->nsys, h->sc[h->tree_sys0].tree_theta,
-                                                h->sc[h->tree_sys0].tree_extra_correction);
+                                                h->sc[h->tree_sys0].tree_extra_correction, h->prv);
+    tb->prep_epoch = h->links_epoch;
   }
   tb->built = true;
 }
@@ -1537,6 +1572,10 @@ void launch_tree_walk(nv_handle *h) {
 void launch_tree_walk_mixed(nv_handle *h) {
   TreeBuffers *tb = h->tree;
   if (!tb || h->n_work_timg == 0) return;
+  if (tb->prep_epoch != h->links_epoch) {  // relinked since the build
+    k_leaf_links<<<n_sms() * 4, 256, 0, h->stream>>>(*tb, h->nsys, h->prv);
+    tb->prep_epoch = h->links_epoch;
+  }
   cudaMemsetAsync(tb->defer_n, 0, sizeof(int), h->stream);
   k_tree_walk_mixed<<<h->n_work_timg, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->d_work_timg, h->x, h->nxt, h->prv,
                                                            h->partial, h->T, *tb, h->near_factor, h->guards,

@@ -79,3 +79,22 @@ def test_mixed_tree_with_root_tests_deferred():
     assert rms_rel(um, up) <= TOL_RMS
     hp.close()
     hm.close()
+
+
+def test_mixed_walk_after_a_relinking_stage_between_build_and_velocity():
+    # Stages one by one with pinsert between the tree build and the velocity: the mixed walk
+    # refreshes the links its leaf records took at the build (the own-segment test follows
+    # the links of the moment, as the FP64 walk does).  delta is above the state's spacing,
+    # so pinsert inserts nothing and the refreshed records equal the built ones: the velocity
+    # must equal the one computed right after the build, bit for bit.
+    from nuvort_b200.api import Handle
+    st = tangle(3, 0.001, n_points=4096)
+    p = config1_params("Tree", delta=0.0015, precision="mixed")
+    with Handle(p, [2 * st.pcount], states=[st]) as h:
+        u0 = h.calc_velocity()
+    with Handle(p, [2 * st.pcount], states=[st]) as h:
+        for s_ in ("ghostp", "construct_tree", "pinsert", "pmotion"):
+            h.stage(s_)
+        assert h.counters().insert_count == 0
+        u1 = h.download().u[: st.pcount]
+    assert np.array_equal(u0, u1)
