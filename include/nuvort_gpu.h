@@ -232,6 +232,11 @@ int nv_set_insert_iterations(nv_handle *h, int32_t n);
  * scale (>= 1, default 1) multiplies that bound; a very large scale sends every root test
  * through the exact path, for testing. */
 int nv_set_root_band(nv_handle *h, double scale);
+/* Mixed-precision tree walk: the central image's walks (the deepest) are split over `parts`
+ * groups of the root's children (1, 2, 4 or 8), each a work item of its own, so that a small
+ * system still fills the GPU; the groups' sums are added in group order.  0 (the default)
+ * picks the split from the number of central work items and the SM count. */
+int nv_set_walk_parts(nv_handle *h, int32_t parts);
 
 /* Turn per-step stage timing on (default) or off.  With timing on, nv_step waits for each
  * step and adds its device time per stage to nv_stage_times; off, steps are queued back to

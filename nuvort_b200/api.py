@@ -68,6 +68,7 @@ def lib():
     L.nv_set_insert_iterations.argtypes = [vp, C.c_int32]
     L.nv_set_fp32_guards.argtypes = [vp, C.c_double, C.c_double, C.c_double]
     L.nv_set_root_band.argtypes = [vp, C.c_double]
+    L.nv_set_walk_parts.argtypes = [vp, C.c_int32]
     L.nv_step_launches.argtypes = [vp, P(i32)]
     L.nv_measure_fp64_peak.argtypes = [i32, P(C.c_double)]
     L.nv_measure_fp32_peak.argtypes = [i32, P(C.c_double)]
@@ -222,6 +223,10 @@ class Handle:
     def set_root_band(self, scale: float):
         """Scale of the root-centre estimate's error bound (huge: every root test exact)."""
         _check(lib().nv_set_root_band(self.h, float(scale)))
+
+    def set_walk_parts(self, parts: int):
+        """Split of the mixed tree walk's central image over groups of root children (0: automatic)."""
+        _check(lib().nv_set_walk_parts(self.h, int(parts)))
 
     def set_insert_iterations(self, n: int):
         """Fixed-point rounds of the parallel pinsert (0: the serial sweep every step)."""

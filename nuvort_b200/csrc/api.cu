@@ -153,16 +153,34 @@ int upload_worklist4(int4 **dptr, int *n, const std::vector<int4> &w) {
   return NV_OK;
 }
 
-// (system, image, first slot) items over every image of every system of one kind
-void build_image_worklist(nv_handle *h, int which, int tb, std::vector<int4> &w) {
+// (system, image, first slot, part) items over every image of every system of one kind.
+// With parts > 1 the central image (the deepest walks) is listed once per part, each part
+// walking a group of the root's children; all central items come first.
+void build_image_worklist(nv_handle *h, int which, int tb, std::vector<int4> &w, int parts = 1) {
   w.clear();
-  for (int s = 0; s < h->nsys; ++s) {
-    const SysConst &sc = h->sc[s];
-    int kind = sc.velocity == NV_VEL_LIA ? 0 : (sc.sched_tree ? 2 : 1);
-    if (kind != which) continue;
-    for (int m = 0; m <= sc.n_shift; ++m)
-      for (int k = 1; k <= h->cap[s]; k += tb) w.push_back(make_int4(s, m, sc.base + k, 0));
-  }
+  for (int pass = 0; pass < 2; ++pass)
+    for (int s = 0; s < h->nsys; ++s) {
+      const SysConst &sc = h->sc[s];
+      int kind = sc.velocity == NV_VEL_LIA ? 0 : (sc.sched_tree ? 2 : 1);
+      if (kind != which) continue;
+      for (int m = pass == 0 ? 0 : 1; m <= (pass == 0 ? 0 : sc.n_shift); ++m)
+        for (int part = 0; part < (m == 0 ? parts : 1); ++part)
+          for (int k = 1; k <= h->cap[s]; k += tb) w.push_back(make_int4(s, m, sc.base + k, part));
+    }
+}
+
+// Central-image split of the mixed tree walk: enough central blocks to fill the GPU about
+// four times over (the central walks are the longest, and a few hundred of them leave most
+// SMs idle), at most one part per root child.
+int auto_walk_parts(const nv_handle *h) {
+  long long central = 0;
+  for (int s = 0; s < h->nsys; ++s)
+    if (h->sc[s].sched_tree && h->sc[s].velocity != NV_VEL_LIA) central += (h->cap[s] + 127) / 128;
+  if (central == 0) return 1;
+  const long long resident = 8LL * n_sms_host();
+  int p = 1;
+  while (p < kMaxWalkParts && central * p < 4 * resident) p *= 2;
+  return p;
 }
 
 int rebuild_worklists(nv_handle *h) {
@@ -172,7 +190,8 @@ int rebuild_worklists(nv_handle *h) {
     std::vector<int4> w4;
     build_image_worklist(h, 1, 128, w4);
     if ((rc = upload_worklist4(&h->d_work_img, &h->n_work_img, w4)) != NV_OK) return rc;
-    build_image_worklist(h, 2, 128, w4);
+    h->walk_parts_used = h->walk_parts > 0 ? h->walk_parts : auto_walk_parts(h);
+    build_image_worklist(h, 2, 128, w4, h->walk_parts_used);
     if ((rc = upload_worklist4(&h->d_work_timg, &h->n_work_timg, w4)) != NV_OK) return rc;
   }
   for (int s = 0; s < h->nsys; ++s)
@@ -423,7 +442,7 @@ int nv_create(const nv_params *params, int32_t nsys, const int32_t *capacity, in
     return bail(rc);
   if (h->precision == NV_PREC_MIXED) {
     if ((rc = dalloc(&h->seg32, 3 * T))) return bail(rc);
-    const int nimg = 27;
+    const int nimg = 27 + kMaxWalkParts - 1;  // the images, then the central image's extra parts
     if ((rc = dalloc(&h->partial, (size_t)nimg * 3 * T))) return bail(rc);
   }
   h->event_cap = (int)std::min<long long>(std::max<long long>(1 << 16, T), 1 << 24);
@@ -743,6 +762,17 @@ int nv_set_root_band(nv_handle *h, double scale) {
   if (!h || !(scale >= 1.0)) return set_error(NV_ERR_ARG, "nv_set_root_band: scale must be >= 1");
   h->root_band_scale = scale;
   h->graph_valid = false;  // a launch argument of the captured step
+  return NV_OK;
+}
+
+int nv_set_walk_parts(nv_handle *h, int32_t parts) {
+  if (!h || parts < 0 || parts > kMaxWalkParts || (parts & (parts - 1)))
+    return set_error(NV_ERR_ARG, "nv_set_walk_parts: parts must be 0 (automatic), 1, 2, 4 or 8");
+  int rc = set_device(h);
+  if (rc) return rc;
+  h->walk_parts = parts;
+  if ((rc = rebuild_worklists(h))) return rc;
+  h->graph_valid = false;  // the work list is a launch argument of the captured walk
   return NV_OK;
 }
 

@@ -45,6 +45,8 @@ struct nv_handle {
   double root_band_scale = 1.0;  // scale of the root centre estimate's error bound
   int ins_iters = 6;  // fixed-point iterations of the parallel pinsert; 0: serial sweep only
   int tree_sys0 = 0;           // first system that walks the tree (its theta0 builds the mixed nodes)
+  int walk_parts = 0;          // central image of the mixed tree walk split over this many root-child groups (0: automatic)
+  int walk_parts_used = 1;     // the split the work list was built with
   unsigned links_epoch = 0;    // bumped by every stage that relinks points (pinsert, precon, premove, upload)
   unsigned *d_err = nullptr;
   DevEvent *d_events = nullptr;
@@ -95,6 +97,8 @@ void launch_direct_mixed(nv_handle *h);
 void launch_mixed_combine(nv_handle *h, int which);
 void launch_tree_walk_mixed(nv_handle *h);
 // tree (tree.cu)
+constexpr int kMaxWalkParts = 8;  // the central image's walk splits over at most the root's 8 children
+int n_sms_host();                  // SMs of the current device
 void tree_alloc(nv_handle *h);
 void tree_free(nv_handle *h);
 void launch_tree_build(nv_handle *h);

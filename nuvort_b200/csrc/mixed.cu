@@ -172,7 +172,7 @@ __global__ void k_mixed_combine(const SysConst *__restrict__ scs, const SysDyn *
                                 const int2 *__restrict__ work, const double *__restrict__ X,
                                 const double *__restrict__ GI, const double *__restrict__ GB,
                                 const int *__restrict__ nxt, const double *__restrict__ partial,
-                                double *__restrict__ U, long long T, const unsigned *err) {
+                                double *__restrict__ U, long long T, int extra, const unsigned *err) {
   if (*err) return;
   const int2 w = work[blockIdx.x];
   const SysConst &sc = scs[w.x];
@@ -186,6 +186,8 @@ __global__ void k_mixed_combine(const SysConst *__restrict__ scs, const SysDyn *
   local_velocity(sc, xi, gi, gb, u, fdot);
   double b0[3], bs[3] = {0, 0, 0};
   for (int c = 0; c < 3; ++c) b0[c] = partial[(long long)c * T + g];
+  for (int e = 1; e <= extra; ++e)  // the central image's other parts, in part order
+    for (int c = 0; c < 3; ++c) b0[c] += partial[((long long)(26 + e) * 3 + c) * T + g];
   for (int m = 1; m <= sc.n_shift; ++m)
     for (int c = 0; c < 3; ++c) bs[c] += partial[((long long)m * 3 + c) * T + g];
   for (int c = 0; c < 3; ++c) u[c] = e_add(e_add(u[c], b0[c]), bs[c]);
@@ -208,8 +210,9 @@ void launch_mixed_combine(nv_handle *h, int which) {
   const int2 *wl = which == 1 ? h->d_work_direct : h->d_work_tree;
   const int n = which == 1 ? h->n_work_direct : h->n_work_tree;
   if (n == 0) return;
+  const int extra = which == 2 ? h->walk_parts_used - 1 : 0;
   k_mixed_combine<<<n, h->direct_tb, 0, h->stream>>>(h->d_sc, h->d_dyn, wl, h->x, h->gi, h->gb, h->nxt, h->partial,
-                                                     h->u, h->T, h->d_err);
+                                                     h->u, h->T, extra, h->d_err);
 }
 
 int mixed_tiles_per_block() { return kTB; }

@@ -1171,11 +1171,12 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
                                                             const double *__restrict__ X,
                                                             const int *__restrict__ nxt, const int *__restrict__ prv,
                                                             double *__restrict__ partial, long long T, TreeBuffers tb,
-                                                            double near_factor, Fp32Guards gd, unsigned *err) {
+                                                            double near_factor, Fp32Guards gd, int parts,
+                                                            unsigned *err) {
   const int lane = threadIdx.x & 31;
-  const int4 w = work[blockIdx.x];
+  const int4 w = work[blockIdx.x];  // system, image, first position, part of a split central image
   const SysConst &sc = scs[w.x];
-  const int m = w.y;
+  const int m = w.y, part = w.w;
   const int q = w.z + threadIdx.x - sc.base;  // position in the system's walk order
   const int g = q >= 1 && q <= sc.cap ? tb.perm[sc.base + q] : sc.base;
   const int k = g - sc.base;
@@ -1248,11 +1249,23 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
     const double zero[3] = {0, 0, 0};
     load3(X, T, g, xi);
     rd = root_decision(tb, sc, w.x, xi, m > 0 ? sc.shift[m - 1] : zero);
-    if (rd == 2) defer_push(tb, g, m, err);
-    else ++tests;
+    if (part == 0) {  // the parts of a split central image share one root test
+      if (rd == 2) defer_push(tb, g, m, err);
+      else ++tests;
+    }
   }
   const unsigned open0 = __ballot_sync(0xffffffffu, valid && rd == 0);
   const int first = tb.nI[w.x].y;
+  // The root's children are nodes first .. first+nc-1.  A part of a split central image
+  // walks children lo .. hi-1 of them (ids below lim); every other item walks them all.
+  int start = first, lim = INT_MAX;
+  if (m == 0 && parts > 1 && first != kEnd) {
+    int nc = 0;
+    for (int d = 0; d < 8; ++d) nc += tb.root_cnt[8 * w.x + d] != 0;
+    const int lo = part * 8 / parts, hi = min((part + 1) * 8 / parts, nc);
+    start = lo < nc ? first + lo : kEnd;
+    lim = first + hi;
+  }
   (void)live;
   // (cur, mask): the node the warp is at and the lanes whose walk reaches it, warp-uniform.
   // The stack holds the pending next siblings of the nodes opened on the way down: entry d
@@ -1260,14 +1273,17 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
   int sn0 = 0, sn1 = 0;
   unsigned sm0 = 0, sm1 = 0;
   int top = -1;
-  int cur = first;
+  int cur = start;
   unsigned mask = open0;
-  bool more = open0 && first != kEnd;
+  bool more = open0 && start != kEnd;
   while (more) {
     const WalkNode *wn = tb.mx.W + cur;
     // the whole 64-byte record at once: one load latency per node instead of a chain
     const int4 D = __ldg(&wn->d);
     const float4 A = __ldg(&wn->a), B = __ldg(&wn->b), Q = __ldg(&wn->c);
+    // the next sibling, none past the last root child of this item's group (the root's
+    // children are the only nodes with ids in [first, lim))
+    const int sib = D.z >= lim && cur >= first && cur < lim ? kEnd : D.z;
     bool open = false;
     if (D.x != 0 && ((mask >> lane) & 1u)) {
       ++tests;
@@ -1336,7 +1352,7 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
     }
     const unsigned omask = __ballot_sync(0xffffffffu, open);
     if (omask && D.y != kEnd) {  // the lanes that open cur walk its children first
-      if (D.z != kEnd) {         // and come back to cur's next sibling afterwards
+      if (sib != kEnd) {         // and come back to cur's next sibling afterwards
         ++top;
         if (top >= kWalkStack) {  // deeper than any tree the build makes; guard only
           if (lane == 0) atomicOr(err, DERR_TREE_DEPTH);
@@ -1344,18 +1360,18 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
         }
         if (lane == (top & 31)) {
           if (top >= 32) {
-            sn1 = D.z;
+            sn1 = sib;
             sm1 = mask;
           } else {
-            sn0 = D.z;
+            sn0 = sib;
             sm0 = mask;
           }
         }
       }
       cur = D.y;
       mask = omask;
-    } else if (D.z != kEnd) {
-      cur = D.z;
+    } else if (sib != kEnd) {
+      cur = sib;
     } else if (top >= 0) {
       const int src = top & 31;
       const bool hi = top >= 32;
@@ -1368,7 +1384,8 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
   }
   if (singular) atomicOr(err, DERR_SINGULAR);
   if (valid) {
-    const long long o = (long long)m * 3 * T + g;
+    const int slot = m == 0 && part > 0 ? 26 + part : m;  // extra parts after the 27 images
+    const long long o = (long long)slot * 3 * T + g;
     partial[o] = (double)fx + nx;
     partial[o + T] = (double)fy + ny;
     partial[o + 2 * T] = (double)fz + nz;
@@ -1399,6 +1416,8 @@ int n_sms() {
 }
 
 }  // namespace
+
+int n_sms_host() { return n_sms(); }
 
 void tree_alloc(nv_handle *h) {
   bool need = false;
@@ -1579,7 +1598,7 @@ void launch_tree_walk_mixed(nv_handle *h) {
   cudaMemsetAsync(tb->defer_n, 0, sizeof(int), h->stream);
   k_tree_walk_mixed<<<h->n_work_timg, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->d_work_timg, h->x, h->nxt, h->prv,
                                                            h->partial, h->T, *tb, h->near_factor, h->guards,
-                                                           h->d_err);
+                                                           h->walk_parts_used, h->d_err);
 }
 
 void launch_closest_tree(nv_handle *h) {

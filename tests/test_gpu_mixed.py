@@ -98,3 +98,39 @@ def test_mixed_walk_after_a_relinking_stage_between_build_and_velocity():
         assert h.counters().insert_count == 0
         u1 = h.download().u[: st.pcount]
     assert np.array_equal(u0, u1)
+
+
+@pytest.mark.parametrize("parts", [1, 2, 8])
+@pytest.mark.parametrize("band", [1.0, 1e30])
+def test_mixed_tree_central_image_split(parts, band):
+    # The central image's walks split over groups of the root's children: the union of the
+    # groups' walks is the whole walk, so the opening tests and accepted nodes are the
+    # unsplit walk's; only the grouping of the FP32 partial sums and of their FP64 additions
+    # changes (both results within the mixed tolerance of the plain path).
+    # band 1e30 defers every root test (the exact FP64 fix-up then writes the central image
+    # whole and the other groups must hold zeros).
+    from nuvort_b200.api import Handle
+    st = tangle(1, 0.001, n_points=16384)
+    p = config1_params("Tree", tree_theta=0.4, precision="mixed")
+    out = {}
+    for k in (1, parts):
+        with Handle(p, [st.pcount + 512], states=[st]) as h:
+            h.set_walk_parts(k)
+            h.set_root_band(band)
+            u = h.calc_velocity()
+            c = h.counters()
+            out[k] = (u, c.tree_tests, c.tree_eval)
+    (u1, t1, e1), (uk, tk, ek) = out[1], out[parts]
+    assert (tk, ek) == (t1, e1)
+    assert rms_rel(uk, u1) <= 2e-7
+    up, _ = _vel(config1_params("Tree", tree_theta=0.4, precision="fp64"), st)
+    assert rms_rel(uk, up) <= TOL_RMS
+
+
+def test_walk_parts_argument_checked():
+    from nuvort_b200.api import Handle, NuvortError
+    st = tangle(1, 0.001, n_points=1024)
+    with Handle(config1_params("Tree", precision="mixed"), [st.pcount + 64], states=[st]) as h:
+        for bad in (-1, 3, 16):
+            with pytest.raises(NuvortError):
+                h.set_walk_parts(bad)
