@@ -232,10 +232,13 @@ int nv_set_insert_iterations(nv_handle *h, int32_t n);
  * scale (>= 1, default 1) multiplies that bound; a very large scale sends every root test
  * through the exact path, for testing. */
 int nv_set_root_band(nv_handle *h, double scale);
-/* Mixed-precision tree walk: the central image's walks (the deepest) are split over `parts`
- * groups of the root's children (1, 2, 4 or 8), each a work item of its own, so that a small
- * system still fills the GPU; the groups' sums are added in group order.  0 (the default)
- * picks the split from the number of central work items and the SM count. */
+/* Split of the tree walks' work, so that a small system still fills the GPU.  Mixed
+ * precision: the central image's walks (the deepest) are split over `parts` groups of the
+ * root's children (1, 2, 4 or 8), each a work item of its own; the groups' sums are added in
+ * group order.  Plain FP64: parts > 1 gives each target two threads, one summing the
+ * unshifted image and one the 26 shifted ones, added in the reference's order (the result
+ * is the same bit for bit); 1 keeps one thread per target.  0 (the default) picks the split
+ * from the number of work items and the SM count. */
 int nv_set_walk_parts(nv_handle *h, int32_t parts);
 
 /* Turn per-step stage timing on (default) or off.  With timing on, nv_step waits for each

@@ -225,7 +225,8 @@ class Handle:
         _check(lib().nv_set_root_band(self.h, float(scale)))
 
     def set_walk_parts(self, parts: int):
-        """Split of the mixed tree walk's central image over groups of root children (0: automatic)."""
+        """Split of the tree walks' work (mixed: central image over groups of root children;
+        FP64: unshifted / shifted images on two threads per target); 0: automatic."""
         _check(lib().nv_set_walk_parts(self.h, int(parts)))
 
     def set_insert_iterations(self, n: int):

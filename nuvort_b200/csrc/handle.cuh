@@ -60,7 +60,7 @@ struct nv_handle {
   int n_work_tree = 0;
   int2 *d_work_lia = nullptr;
   int n_work_lia = 0;
-  int direct_tb = 64;  // targets per block of the direct sum
+  int direct_tb = 64;  // targets per block of the direct sum and of the FP64 tree walk (which assumes 64)
   bool any_tree = false, any_direct = false, any_lia = false;
 
   TreeBuffers *tree = nullptr;

@@ -916,40 +916,13 @@ __device__ __forceinline__ void walk_fp64(const TreeBuffers &tb, int start, cons
   }
 }
 
-// The velocity of target g (timestep.f90:49-141 with tree_walk): local term, the tree sum
-// over the unshifted image, then over the 26 shifts in order, mutual friction.  With
-// `decided` the root's tests come from the centre estimate: a target for which any of
-// them is too close to call is deferred whole (nothing counted), to be redone exactly.
-__device__ void fp64_target(const SysConst &sc, const SysDyn &dy, int sys, int g, const double *__restrict__ X,
-                            const double *__restrict__ GI, const double *__restrict__ GB,
-                            const int *__restrict__ prv, double *__restrict__ U, long long T, const TreeBuffers &tb,
-                            bool decided, unsigned long long &evals, unsigned long long &tests, unsigned *err) {
-  double xi[3];
+// Local term, the unshifted image's tree sum ub0, the shifted images' sum ubs, mutual
+// friction, in the reference's order of additions (timestep.f90:79-140).
+__device__ void fp64_epilogue(const SysConst &sc, const SysDyn &dy, int g, const double *__restrict__ X,
+                              const double *__restrict__ GI, const double *__restrict__ GB, double *__restrict__ U,
+                              long long T, const double ub0[3], const double ubs[3]) {
+  double xi[3], gi[3], gb[3], u[3], fdot[3];
   load3(X, T, g, xi);
-  const double zero[3] = {0, 0, 0};
-  int start[27];
-  const int first = tb.nI[sys].y;
-  unsigned long long t0 = 0;
-  for (int m = 0; m <= sc.n_shift; ++m) {
-    start[m] = sys;
-    if (!decided) continue;
-    const int d = root_decision(tb, sc, sys, xi, m == 0 ? zero : sc.shift[m - 1]);
-    if (d == 2) {
-      defer_push(tb, g, -1, err);
-      return;
-    }
-    start[m] = d == 1 ? kEnd : first;  // accepted: adds nothing; opened: walk the children
-    ++t0;
-  }
-  tests += t0;
-  const int pi_ = prv[g];
-  bool singular = false;
-  double ub0[3] = {0, 0, 0}, ubs[3] = {0, 0, 0};
-  walk_fp64(tb, start[0], sc, xi, g, pi_, prv, zero, true, ub0, evals, tests, singular);
-  for (int m = 0; m < sc.n_shift; ++m)
-    walk_fp64(tb, start[m + 1], sc, xi, g, pi_, prv, sc.shift[m], false, ubs, evals, tests, singular);
-  if (singular) atomicOr(err, DERR_SINGULAR);
-  double gi[3], gb[3], u[3], fdot[3];
   load3(GI, T, g, gi);
   load3(GB, T, g, gb);
   local_velocity(sc, xi, gi, gb, u, fdot);
@@ -961,20 +934,79 @@ __device__ void fp64_target(const SysConst &sc, const SysDyn &dy, int sys, int g
   store3(U, T, g, u);
 }
 
-__global__ void __launch_bounds__(64) k_tree_walk_fp64(const SysConst *__restrict__ scs, SysDyn *dyn,
-                                                       const int2 *__restrict__ work, const double *__restrict__ X,
-                                                       const double *__restrict__ GI, const double *__restrict__ GB,
-                                                       const int *__restrict__ nxt, const int *__restrict__ prv,
-                                                       double *__restrict__ U, long long T, TreeBuffers tb,
-                                                       unsigned *err) {
+// The tree sums of target g (timestep.f90:49-141 with tree_walk): over the unshifted image
+// into ub0, then over the 26 shifts in order into ubs.  part 0 does both and the epilogue;
+// part 1 only ub0, part 2 only ubs (the epilogue then runs where both are known) -- each
+// sum is the same chain of additions either way.  With `decided` the root's tests come from
+// the centre estimate: a target for which any of them is too close to call is deferred
+// whole (nothing counted; part 2 leaves the push to part 1), to be redone exactly.  Returns
+// false for a deferred target.
+__device__ bool fp64_target(const SysConst &sc, const SysDyn &dy, int sys, int g, const double *__restrict__ X,
+                            const double *__restrict__ GI, const double *__restrict__ GB,
+                            const int *__restrict__ prv, double *__restrict__ U, long long T, const TreeBuffers &tb,
+                            bool decided, int part, double ub0[3], double ubs[3], unsigned long long &evals,
+                            unsigned long long &tests, unsigned *err) {
+  double xi[3];
+  load3(X, T, g, xi);
+  const double zero[3] = {0, 0, 0};
+  int start[27];
+  const int first = tb.nI[sys].y;
+  unsigned long long t0 = 0;
+  for (int m = 0; m <= sc.n_shift; ++m) {
+    start[m] = sys;
+    if (!decided) continue;
+    const int d = root_decision(tb, sc, sys, xi, m == 0 ? zero : sc.shift[m - 1]);
+    if (d == 2) {
+      if (part != 2) defer_push(tb, g, -1, err);
+      return false;
+    }
+    start[m] = d == 1 ? kEnd : first;  // accepted: adds nothing; opened: walk the children
+    ++t0;
+  }
+  if (part != 2) tests += t0;  // the root tests are counted once
+  const int pi_ = prv[g];
+  bool singular = false;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) ub0[c] = ubs[c] = 0.;
+  if (part != 2) walk_fp64(tb, start[0], sc, xi, g, pi_, prv, zero, true, ub0, evals, tests, singular);
+  if (part != 1)
+    for (int m = 0; m < sc.n_shift; ++m)
+      walk_fp64(tb, start[m + 1], sc, xi, g, pi_, prv, sc.shift[m], false, ubs, evals, tests, singular);
+  if (singular) atomicOr(err, DERR_SINGULAR);
+  if (part == 0) fp64_epilogue(sc, dy, g, X, GI, GB, U, T, ub0, ubs);
+  return true;
+}
+
+// Plain FP64 tree walk, 64 targets per block.  With `split`, two threads per target (128
+// per block): warps 0-1 sum the unshifted image (the deepest walk), warps 2-3 the 26 shifted
+// ones, and the second thread adds the two sums in the reference's order once both are
+// done -- for small systems, whose few blocks would leave most SMs idle.  Without, one
+// thread per target does it all (64 per block).
+__global__ void __launch_bounds__(128) k_tree_walk_fp64(const SysConst *__restrict__ scs, SysDyn *dyn,
+                                                        const int2 *__restrict__ work, const double *__restrict__ X,
+                                                        const double *__restrict__ GI, const double *__restrict__ GB,
+                                                        const int *__restrict__ nxt, const int *__restrict__ prv,
+                                                        double *__restrict__ U, long long T, TreeBuffers tb,
+                                                        int split, unsigned *err) {
+  __shared__ double s_ub0[3][64];
   const int2 w = work[blockIdx.x];
   const SysConst &sc = scs[w.x];
-  const int q = w.y + threadIdx.x - sc.base;  // position in the system's walk order
+  const int t = threadIdx.x & 63, part = split ? 1 + (threadIdx.x >> 6) : 0;
+  const int q = w.y + t - sc.base;  // position in the system's walk order
   const int g = q >= 1 && q <= sc.cap ? tb.perm[sc.base + q] : sc.base;
   const int k = g - sc.base;
   unsigned long long evals = 0, tests = 0;
+  double ub0[3] = {0, 0, 0}, ubs[3] = {0, 0, 0};
+  bool done = false;
   if (!*err && k >= 1 && k <= dyn[w.x].pcount && nxt[g] != 0)
-    fp64_target(sc, dyn[w.x], w.x, g, X, GI, GB, prv, U, T, tb, true, evals, tests, err);
+    done = fp64_target(sc, dyn[w.x], w.x, g, X, GI, GB, prv, U, T, tb, true, part, ub0, ubs, evals, tests, err);
+  if (part == 1)
+    for (int c = 0; c < 3; ++c) s_ub0[c][t] = ub0[c];
+  __syncthreads();
+  if (part == 2 && done) {
+    for (int c = 0; c < 3; ++c) ub0[c] = s_ub0[c][t];
+    fp64_epilogue(sc, dyn[w.x], g, X, GI, GB, U, T, ub0, ubs);
+  }
   // tree_eval (tree.f90:308): one atomic per warp
   unsigned long long tot = evals, tt = tests;
   for (int o = 16; o > 0; o >>= 1) {
@@ -998,7 +1030,8 @@ __global__ void k_walk_fixup(const SysConst *__restrict__ scs, SysDyn *dyn, cons
     const SysConst &sc = scs[s];
     unsigned long long evals = 0, tests = 0;
     if (d.y < 0) {
-      fp64_target(sc, dyn[s], s, g, X, GI, GB, prv, U, T, tb, false, evals, tests, err);
+      double ub0[3], ubs[3];
+      fp64_target(sc, dyn[s], s, g, X, GI, GB, prv, U, T, tb, false, 0, ub0, ubs, evals, tests, err);
     } else {
       const int m = d.y;
       double xi[3], acc[3] = {0, 0, 0};
@@ -1584,8 +1617,11 @@ void launch_tree_walk(nv_handle *h) {
   TreeBuffers *tb = h->tree;
   if (!tb || h->n_work_tree == 0) return;
   cudaMemsetAsync(tb->defer_n, 0, sizeof(int), h->stream);
-  k_tree_walk_fp64<<<h->n_work_tree, 64, 0, h->stream>>>(h->d_sc, h->d_dyn, h->d_work_tree, h->x, h->gi, h->gb,
-                                                         h->nxt, h->prv, h->u, h->T, *tb, h->d_err);
+  // two threads per target while the one-thread blocks would fill the GPU less than ~4
+  // times (automatic), or as nv_set_walk_parts asks
+  const int split = h->walk_parts == 0 ? h->n_work_tree < 32 * n_sms() : h->walk_parts > 1;
+  k_tree_walk_fp64<<<h->n_work_tree, split ? 128 : 64, 0, h->stream>>>(
+      h->d_sc, h->d_dyn, h->d_work_tree, h->x, h->gi, h->gb, h->nxt, h->prv, h->u, h->T, *tb, split, h->d_err);
 }
 
 void launch_tree_walk_mixed(nv_handle *h) {

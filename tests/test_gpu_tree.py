@@ -147,3 +147,20 @@ def test_root_tests_all_deferred_give_the_same_velocity():
     assert np.array_equal(u0, u1)
     assert c1.tree_eval == o.counters().tree_eval and c1.tree_tests == o.counters().tree_tests
     h.close()
+
+
+@pytest.mark.parametrize("theta", [0.4, 0.8])
+def test_fp64_tree_walk_split_is_bit_identical(theta):
+    # Two threads per target (unshifted image / 26 shifted images, added afterwards in the
+    # reference's order) must give the one-thread walk's velocities bit for bit.
+    from nuvort_b200.api import Handle
+    st = tangle(1, 0.001, n_points=8192)
+    out = []
+    for parts in (1, 2):
+        with Handle(config1_params("Tree", tree_theta=theta), [st.pcount + 512], states=[st]) as h:
+            h.set_walk_parts(parts)
+            u = h.calc_velocity()
+            c = h.counters()
+            out.append((u, c.tree_eval, c.tree_tests))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1:] == out[1][1:]
