@@ -27,7 +27,7 @@ struct Fp32Guards {
 struct __align__(16) WalkNode {
   float4 a;  // centre (FP32 high part), accept threshold t1^2 rounded to FP32
   float4 b;  // centre (FP32 low part: centre - high part), |circ|^2 in FP32
-  float4 c;  // circulation in FP32, unused
+  float4 c;  // circulation in FP32, the line guard's threshold (Fp32Guards::line x |circ|^2)
   int4 d;    // pcount, first child, next sibling, first member's infront
 };
 

@@ -1151,7 +1151,8 @@ __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *_
 // impossible for theta0 <= 2/sqrt(3) (geo <= sqrt(3)/2 width), so it is tested only above.
 // Roots are skipped: their exact centre may still be summing (the walks take the roots'
 // tests from the centre estimate).
-__global__ void k_node_prep(TreeBuffers tb, int nsys, double theta0, int corr, const int *__restrict__ prv) {
+__global__ void k_node_prep(TreeBuffers tb, int nsys, double theta0, int corr, float line_guard,
+                            const int *__restrict__ prv) {
   const int n = tb.ctr[0];
   for (int id = nsys + blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
     const double4 A = tb.nA[id], B = tb.nB[id];
@@ -1164,8 +1165,9 @@ __global__ void k_node_prep(TreeBuffers tb, int nsys, double theta0, int corr, c
     const int4 I = tb.nI[id];
     WalkNode wn;
     wn.a = make_float4(hx, hy, hz, (float)(t1 * t1));
-    wn.b = make_float4((float)(A.x - hx), (float)(A.y - hy), (float)(A.z - hz), qx * qx + qy * qy + qz * qz);
-    wn.c = make_float4(qx, qy, qz, 0.f);
+    const float q2 = qx * qx + qy * qy + qz * qz;
+    wn.b = make_float4((float)(A.x - hx), (float)(A.y - hy), (float)(A.z - hz), q2);
+    wn.c = make_float4(qx, qy, qz, line_guard * q2);
     wn.d = make_int4(I.x, I.y, tb.nSib[id], I.x == 1 ? prv[I.w] : I.w);
     tb.mx.W[id] = wn;
   }
@@ -1199,6 +1201,7 @@ __global__ void k_leaf_links(TreeBuffers tb, int nsys, const int *__restrict__ p
 constexpr int kWalkStack = 64;  // two register entries per lane; the build stops at depth 42
 constexpr float kTestBand = 1e-5f;
 
+template <bool kSplit>
 __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__restrict__ scs, SysDyn *dyn,
                                                             const int4 *__restrict__ work,
                                                             const double *__restrict__ X,
@@ -1292,7 +1295,7 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
   // The root's children are nodes first .. first+nc-1.  A part of a split central image
   // walks children lo .. hi-1 of them (ids below lim); every other item walks them all.
   int start = first, lim = INT_MAX;
-  if (m == 0 && parts > 1 && first != kEnd) {
+  if (kSplit && m == 0 && first != kEnd) {
     int nc = 0;
     for (int d = 0; d < 8; ++d) nc += tb.root_cnt[8 * w.x + d] != 0;
     const int lo = part * 8 / parts, hi = min((part + 1) * 8 / parts, nc);
@@ -1316,7 +1319,7 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
     const float4 A = __ldg(&wn->a), B = __ldg(&wn->b), Q = __ldg(&wn->c);
     // the next sibling, none past the last root child of this item's group (the root's
     // children are the only nodes with ids in [first, lim))
-    const int sib = D.z >= lim && cur >= first && cur < lim ? kEnd : D.z;
+    const int sib = kSplit && D.z >= lim && cur >= first && cur < lim ? kEnd : D.z;
     bool open = false;
     if (D.x != 0 && ((mask >> lane) & 1u)) {
       ++tests;
@@ -1361,14 +1364,17 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
             const float ex = rx + Q.x, ey = ry + Q.y, ez = rz + Q.z;
             const float ee = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
             const float re = fmaf(rx, ex, fmaf(ry, ey, rz * ez));
-            const float r1 = d2 * rsqrtf(d2), r2 = ee * rsqrtf(ee);
-            const float pp = r1 * r2;
-            if (pp + re < gd.angle * pp || cr2 < gd.line * B.w * fminf(d2, ee) || ee < gd.end * fmaxf(d2, B.w)) {
+            // ia = 1/|r|, ib = 1/|r + circ|; pp = |r||r + circ|
+            const float ia = rsqrtf(d2), ib = rsqrtf(ee);
+            const float pp = (d2 * ia) * (ee * ib);
+            const float den = pp + re;
+            if (den < gd.angle * pp || cr2 < Q.w * fminf(d2, ee) || ee < gd.end * fmaxf(d2, B.w)) {
               // the segment subtends more than 120 degrees at the target, the target lies
               // near its line or near its far end: FP32 would cancel digits there
               exact_term(cur);
             } else {
-              const float f = __fdividef(gq * (r1 + r2), pp * (pp + re));  // MUFU reciprocal
+              // (|r| + |r+circ|) / (pp (pp + r.(r+circ))) = (ia + ib) / (pp + r.(r+circ))
+              const float f = __fdividef(gq * (ia + ib), den);  // MUFU reciprocal
               fx = fmaf(f, cx, fx);
               fy = fmaf(f, cy, fy);
               fz = fmaf(f, cz, fz);
@@ -1595,7 +1601,7 @@ void launch_tree_build(nv_handle *h) {
     // theta0 and the correction flag are per system; a handle's systems share them when
     // any of them walks the tree (checked at creation)
     k_node_prep<<<sms * 4, 256, 0, h->stream>>>(*tb, h->nsys, h->sc[h->tree_sys0].tree_theta,
-                                                h->sc[h->tree_sys0].tree_extra_correction, h->prv);
+                                                h->sc[h->tree_sys0].tree_extra_correction, h->guards.line, h->prv);
     tb->prep_epoch = h->links_epoch;
   }
   tb->built = true;
@@ -1632,9 +1638,9 @@ void launch_tree_walk_mixed(nv_handle *h) {
     tb->prep_epoch = h->links_epoch;
   }
   cudaMemsetAsync(tb->defer_n, 0, sizeof(int), h->stream);
-  k_tree_walk_mixed<<<h->n_work_timg, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->d_work_timg, h->x, h->nxt, h->prv,
-                                                           h->partial, h->T, *tb, h->near_factor, h->guards,
-                                                           h->walk_parts_used, h->d_err);
+  auto walk = h->walk_parts_used > 1 ? k_tree_walk_mixed<true> : k_tree_walk_mixed<false>;
+  walk<<<h->n_work_timg, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->d_work_timg, h->x, h->nxt, h->prv, h->partial,
+                                              h->T, *tb, h->near_factor, h->guards, h->walk_parts_used, h->d_err);
 }
 
 void launch_closest_tree(nv_handle *h) {
