@@ -371,7 +371,11 @@ def run_ours(args):
     # end to end through the C ABI with host buffers: upload f(:), one step, download f(:)
     e2e = None
     if not args.no_e2e:
-        hosts = [hm.download(s) for s in range(len(states))]
+        # the caller's persistent host arrays f(:) (x, u, u1, u2, infront, behind), as the
+        # reference keeps them between steps
+        fields = ("x", "u", "u1", "u2", "infront", "behind")
+        bufs = [api.State.empty(c) for c in caps]
+        hosts = [hm.download(s, out=bufs[s], fields=fields) for s in range(len(states))]
         nb = lambda s: sum(a.nbytes for a in (s.x, s.u, s.u1, s.u2, s.infront, s.behind) if a is not None)
         h2d = d2h = e_pts = 0
         torch.cuda.synchronize()
@@ -383,7 +387,7 @@ def run_ours(args):
                 h2d += nb(hs)
                 e_pts += int(np.count_nonzero(host.infront))
             hm.step(1)
-            hosts = [hm.download(s) for s in range(len(states))]
+            hosts = [hm.download(s, out=bufs[s], fields=fields) for s in range(len(states))]
             d2h += sum(nb(x) for x in hosts)
         e2e_s = time.perf_counter() - t0
         (e2e_s,), (e_pts,) = reduce_max_sum(dist, "cuda", [e2e_s], [float(e_pts)])

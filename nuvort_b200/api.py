@@ -26,6 +26,7 @@ _lib = None
 
 STAGES = ("ghostp", "construct_tree", "pmotion", "pinsert", "pclose", "precon", "premove",
           "enforce_boundary", "empty_tree", "end_step")
+STATE_FIELDS = ("x", "infront", "behind", "u", "u1", "u2", "ghosti", "ghostb", "closest", "closestd")
 STAGE_TIMES = ("ghost", "tree", "velocity", "ab3", "topology", "step", "insert", "close", "recon", "remove")
 
 
@@ -159,9 +160,18 @@ class Handle:
             c = self.counters(sys)
             self.set_clock(sys, c.t if t is None else t, c.itime if itime is None else itime)
 
-    def download(self, sys: int = 0) -> State:
+    def download(self, sys: int = 0, out: Optional[State] = None, fields: Optional[Sequence[str]] = None) -> State:
+        """The system's state.  out: a State whose arrays (capacity rows, C-contiguous float64 /
+        int32) are filled in place, as a caller's persistent host arrays would be; the result's
+        arrays are views of them.  fields: the names to fetch (default: all)."""
         cap = self.capacity[sys]
-        st = State.empty(cap)
+        st = out if out is not None else State.empty(cap)
+        if fields is not None:
+            st = State(**{f: (getattr(st, f) if f in fields else None) for f in STATE_FIELDS})
+        for f in STATE_FIELDS:
+            a = getattr(st, f)
+            if a is not None and (a.shape[0] < cap or not a.flags.c_contiguous):
+                raise ValueError(f"download: {f} must be C-contiguous with {cap} rows")
         cst = st.to_c()
         _check(lib().nv_download(self.h, int(sys), C.byref(cst), cap))
         return st.trimmed(cst.pcount)

@@ -27,6 +27,55 @@ namespace {
 
 const char *kVersion = "nuvort_b200 0.1.0 (sm_100a)";
 
+// ---- host state <-> device slots (nv_upload / nv_download) -----------------------------------
+// The host arrays (point k of 1..n at row k-1, components interleaved, links 1-based within
+// the system) are copied as they are into the staging buffer; these kernels move them to and
+// from the system's slots base+1..base+cap (structure of arrays, global links).
+__global__ void k_put_rows(double *__restrict__ dev, long long T, int base, int rows, int n, int comps,
+                           const double *__restrict__ host) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;  // slot within the system, 0 = dummy
+  if (k >= rows) return;
+  for (int c = 0; c < comps; ++c)
+    dev[c * T + base + k] = host && k >= 1 && k <= n ? host[(long long)comps * (k - 1) + c] : 0.0;
+}
+
+__global__ void k_put_links(int *__restrict__ dev, int base, int rows, int n, const int *__restrict__ host,
+                            int *__restrict__ check) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= rows) return;
+  int v = host && k >= 1 && k <= n ? host[k - 1] : 0;
+  if (v < 0 || v > n) {
+    atomicOr(&check[0], 1);
+    v = 0;
+  }
+  dev[base + k] = v ? base + v : 0;
+}
+
+// an empty slot carries an empty link pair; counts the live slots
+__global__ void k_upload_check(const int *__restrict__ nxt, const int *__restrict__ prv, int base, int n,
+                               int *__restrict__ check) {
+  const int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const bool in = k <= n;
+  const bool live = in && nxt[base + k] > 0;
+  if (in && (nxt[base + k] == 0) != (prv[base + k] == 0)) atomicOr(&check[0], 2);
+  const unsigned b = __ballot_sync(0xffffffffu, live);
+  if ((threadIdx.x & 31) == 0 && b) atomicAdd(&check[1], __popc(b));
+}
+
+__global__ void k_get_rows(const double *__restrict__ dev, long long T, int base, int n, int comps,
+                           double *__restrict__ host) {
+  const int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > n) return;
+  for (int c = 0; c < comps; ++c) host[(long long)comps * (k - 1) + c] = dev[c * T + base + k];
+}
+
+__global__ void k_get_links(const int *__restrict__ dev, int base, int n, int *__restrict__ host) {
+  const int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > n) return;
+  const int v = dev[base + k];
+  host[k - 1] = v ? v - base : 0;
+}
+
 int err_code_from_bits(unsigned bits, std::string &msg) {
   if (bits & DERR_SINGULAR) { msg = "tree_walk: singularity in BS (tree) velocity field (dist<epsilon)"; return NV_ERR_SINGULAR; }
   if (bits & DERR_TREE_DEPTH) { msg = "octree deeper than NV_TREE_MAX_DEPTH levels (coincident points?)"; return NV_ERR_TREE_DEPTH; }
@@ -222,7 +271,6 @@ bool any_use_tree(nv_handle *h) {
     if (s.use_tree) return true;
   return false;
 }
-bool any_needs_tree_walk(nv_handle *h) { return h->any_tree; }
 
 // During stream capture a plain cudaEventRecord only orders streams; the External flag
 // makes it an event-record node of the graph, whose timestamps cudaEventElapsedTime reads.
@@ -438,8 +486,13 @@ int nv_create(const nv_params *params, int32_t nsys, const int32_t *capacity, in
       (rc = dalloc(&h->gi, 3 * T)) || (rc = dalloc(&h->gb, 3 * T)) || (rc = dalloc(&h->closestd, T)) ||
       (rc = dalloc(&h->nxt, T)) || (rc = dalloc(&h->prv, T)) || (rc = dalloc(&h->closest, T)) ||
       (rc = dalloc(&h->sys_of, T)) || (rc = dalloc(&h->seg, 2 * T)) || (rc = dalloc(&h->d_err, 1)) ||
-      (rc = dalloc(&h->d_event_count, 1)))
+      (rc = dalloc(&h->d_event_count, 1)) || (rc = dalloc(&h->d_upck, 2)))
     return bail(rc);
+  {
+    int maxcap = 0;
+    for (int s = 0; s < nsys; ++s) maxcap = std::max(maxcap, h->cap[s]);
+    if ((rc = dalloc(&h->stage, 3 * ((size_t)maxcap + 1)))) return bail(rc);
+  }
   if (h->precision == NV_PREC_MIXED) {
     if ((rc = dalloc(&h->seg32, 3 * T))) return bail(rc);
     const int nimg = 27 + kMaxWalkParts - 1;  // the images, then the central image's extra parts
@@ -475,7 +528,7 @@ int nv_destroy(nv_handle *h) {
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   tree_free(h);
   topo_free(h);
-  void *ptrs[] = {h->partial, h->d_sc, h->d_dyn, h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv,
+  void *ptrs[] = {h->partial, h->stage, h->d_upck, h->d_sc, h->d_dyn, h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv,
                   h->closest, h->sys_of, h->seg, h->seg32, h->d_err, h->d_events, h->d_event_count,
                   h->d_work_direct, h->d_work_tree, h->d_work_lia, h->d_work_img, h->d_work_timg};
   for (void *p : ptrs)
@@ -504,49 +557,40 @@ int nv_upload(nv_handle *h, int32_t sys, const nv_host_state *st) {
   if (rc) return rc;
   const long long T = h->T;
   const int rows = cap + 1;  // the system's dummy slot and all its slots
-  std::vector<double> buf(3 * (size_t)rows);
-  auto put3 = [&](double *dev, const double *src) -> int {
-    std::fill(buf.begin(), buf.end(), 0.0);
-    if (src)
-      for (int k = 1; k <= n; ++k)
-        for (int c = 0; c < 3; ++c) buf[(size_t)c * rows + k] = src[3 * (k - 1) + c];
-    for (int c = 0; c < 3; ++c)
-      NV_CUDA(cudaMemcpy(dev + c * T + base, buf.data() + (size_t)c * rows, rows * sizeof(double), cudaMemcpyHostToDevice));
+  cudaStream_t sm = h->stream;
+  // each host array goes to the staging buffer in one copy and from there to the slots (in
+  // stream order, so the buffer is reused array after array)
+  auto put = [&](double *dev, const double *src, int comps) -> int {
+    if (src && n > 0)
+      NV_CUDA(cudaMemcpyAsync(h->stage, src, (size_t)comps * n * sizeof(double), cudaMemcpyHostToDevice, sm));
+    k_put_rows<<<grid_for(rows, 256), 256, 0, sm>>>(dev, T, base, rows, n, comps, src ? h->stage : nullptr);
     return NV_OK;
   };
-  std::vector<int> ib(rows);
+  int *stage_i = reinterpret_cast<int *>(h->stage);
   auto put_link = [&](int *dev, const int *src) -> int {
-    std::fill(ib.begin(), ib.end(), 0);
-    if (src)
-      for (int k = 1; k <= n; ++k) {
-        const int v = src[k - 1];
-        if (v < 0 || v > n) return set_error(NV_ERR_ARG, "nv_upload: link out of range");
-        ib[k] = v ? base + v : 0;
-      }
-    NV_CUDA(cudaMemcpy(dev + base, ib.data(), rows * sizeof(int), cudaMemcpyHostToDevice));
+    if (src && n > 0) NV_CUDA(cudaMemcpyAsync(stage_i, src, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, sm));
+    k_put_links<<<grid_for(rows, 256), 256, 0, sm>>>(dev, base, rows, n, src ? stage_i : nullptr, h->d_upck);
     return NV_OK;
   };
-  if ((rc = put3(h->x, st->x)) || (rc = put3(h->u, st->u)) || (rc = put3(h->u1, st->u1)) ||
-      (rc = put3(h->u2, st->u2)) || (rc = put3(h->gi, st->ghosti)) || (rc = put3(h->gb, st->ghostb)) ||
+  NV_CUDA(cudaMemsetAsync(h->d_upck, 0, 2 * sizeof(int), sm));
+  if ((rc = put(h->x, st->x, 3)) || (rc = put(h->u, st->u, 3)) || (rc = put(h->u1, st->u1, 3)) ||
+      (rc = put(h->u2, st->u2, 3)) || (rc = put(h->gi, st->ghosti, 3)) || (rc = put(h->gb, st->ghostb, 3)) ||
       (rc = put_link(h->nxt, st->infront)) || (rc = put_link(h->prv, st->behind)) ||
-      (rc = put_link(h->closest, st->closest)))
+      (rc = put_link(h->closest, st->closest)) || (rc = put(h->closestd, st->closestd, 1)))
     return rc;
-  std::vector<double> cd(rows, 0.0);
-  if (st->closestd)
-    for (int k = 1; k <= n; ++k) cd[k] = st->closestd[k - 1];
-  NV_CUDA(cudaMemcpy(h->closestd + base, cd.data(), rows * sizeof(double), cudaMemcpyHostToDevice));
-  // a slot that is empty must carry an empty link pair
-  for (int k = 1; k <= n; ++k)
-    if ((st->infront[k - 1] == 0) != (st->behind[k - 1] == 0))
-      return set_error(NV_ERR_ARG, "nv_upload: infront/behind disagree on an empty slot");
-  NV_CUDA(cudaStreamSynchronize(h->stream));
+  // closest links were checked with the others; only infront/behind count for the live slots
+  k_upload_check<<<grid_for(std::max(n, 1), 256), 256, 0, sm>>>(h->nxt, h->prv, base, n, h->d_upck);
+  int check[2] = {0, 0};
+  NV_CUDA(cudaMemcpyAsync(check, h->d_upck, sizeof check, cudaMemcpyDeviceToHost, sm));
+  NV_CUDA(cudaStreamSynchronize(sm));
+  if (check[0] & 1) return set_error(NV_ERR_ARG, "nv_upload: link out of range");
+  if (check[0] & 2) return set_error(NV_ERR_ARG, "nv_upload: infront/behind disagree on an empty slot");
   SysDyn &d = h->h_dyn[sys];
   // keep the clock and counters; replace the slot count
   rc = pull_dyn(h);
   if (rc) return rc;
   d.pcount = n;
-  d.live = 0;
-  for (int k = 0; k < n; ++k) d.live += st->infront[k] > 0;
+  d.live = check[1];
   NV_CUDA(cudaMemcpy(h->d_dyn + sys, &d, sizeof(SysDyn), cudaMemcpyHostToDevice));
   unsigned zero = 0;
   NV_CUDA(cudaMemcpy(h->d_err, &zero, sizeof zero, cudaMemcpyHostToDevice));
@@ -562,32 +606,28 @@ int nv_download(nv_handle *h, int32_t sys, nv_host_state *st, int32_t cap) {
   st->pcount = n;
   if (n > cap) return set_error(NV_ERR_ARG, "nv_download: arrays hold fewer slots than pcount");
   const long long T = h->T;
-  std::vector<double> buf(3 * (size_t)(n + 1));
-  auto get3 = [&](const double *dev, double *dst) -> int {
-    if (!dst) return NV_OK;
-    for (int c = 0; c < 3; ++c)
-      NV_CUDA(cudaMemcpy(buf.data() + (size_t)c * (n + 1), dev + c * T + base, (n + 1) * sizeof(double), cudaMemcpyDeviceToHost));
-    for (int k = 1; k <= n; ++k)
-      for (int c = 0; c < 3; ++c) dst[3 * (k - 1) + c] = buf[(size_t)c * (n + 1) + k];
+  cudaStream_t sm = h->stream;
+  // slots -> staging buffer in the host layout -> one copy (to pageable memory the copy
+  // returns once it is done, so the buffer is free for the next array)
+  auto get = [&](const double *dev, double *dst, int comps) -> int {
+    if (!dst || n == 0) return NV_OK;
+    k_get_rows<<<grid_for(n, 256), 256, 0, sm>>>(dev, T, base, n, comps, h->stage);
+    NV_CUDA(cudaMemcpyAsync(dst, h->stage, (size_t)comps * n * sizeof(double), cudaMemcpyDeviceToHost, sm));
     return NV_OK;
   };
-  std::vector<int> ib(n + 1);
+  int *stage_i = reinterpret_cast<int *>(h->stage);
   auto get_link = [&](const int *dev, int *dst) -> int {
-    if (!dst) return NV_OK;
-    NV_CUDA(cudaMemcpy(ib.data(), dev + base, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost));
-    for (int k = 1; k <= n; ++k) dst[k - 1] = ib[k] ? ib[k] - base : 0;
+    if (!dst || n == 0) return NV_OK;
+    k_get_links<<<grid_for(n, 256), 256, 0, sm>>>(dev, base, n, stage_i);
+    NV_CUDA(cudaMemcpyAsync(dst, stage_i, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, sm));
     return NV_OK;
   };
-  if ((rc = get3(h->x, st->x)) || (rc = get3(h->u, st->u)) || (rc = get3(h->u1, st->u1)) ||
-      (rc = get3(h->u2, st->u2)) || (rc = get3(h->gi, st->ghosti)) || (rc = get3(h->gb, st->ghostb)) ||
+  if ((rc = get(h->x, st->x, 3)) || (rc = get(h->u, st->u, 3)) || (rc = get(h->u1, st->u1, 3)) ||
+      (rc = get(h->u2, st->u2, 3)) || (rc = get(h->gi, st->ghosti, 3)) || (rc = get(h->gb, st->ghostb, 3)) ||
       (rc = get_link(h->nxt, st->infront)) || (rc = get_link(h->prv, st->behind)) ||
-      (rc = get_link(h->closest, st->closest)))
+      (rc = get_link(h->closest, st->closest)) || (rc = get(h->closestd, st->closestd, 1)))
     return rc;
-  if (st->closestd) {
-    std::vector<double> cd(n + 1);
-    NV_CUDA(cudaMemcpy(cd.data(), h->closestd + base, (n + 1) * sizeof(double), cudaMemcpyDeviceToHost));
-    for (int k = 1; k <= n; ++k) st->closestd[k - 1] = cd[k];
-  }
+  NV_CUDA(cudaStreamSynchronize(sm));
   return NV_OK;
 }
 

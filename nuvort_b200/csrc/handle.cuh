@@ -36,6 +36,8 @@ struct nv_handle {
   double4 *seg = nullptr;   // FP64 segment records, 2 per slot
   float4 *seg32 = nullptr;  // FP32 segment records, 3 per slot (mixed precision)
   double *partial = nullptr; // per-image partial sums [image][component][slot] (mixed precision)
+  double *stage = nullptr;   // nv_upload / nv_download staging: host arrays as they are, 3 x (largest capacity + 1) doubles
+  int *d_upck = nullptr;     // nv_upload checks: [0] link errors (1 out of range, 2 empty-slot mismatch), [1] live slots
   int4 *d_work_img = nullptr;  // (system, image, first slot) items of the mixed direct sum
   int n_work_img = 0;
   int4 *d_work_timg = nullptr; // same for the mixed tree walk

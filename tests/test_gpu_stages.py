@@ -49,3 +49,34 @@ def test_enforce_boundary_bit_exact():
     o.stage("enforce_boundary")
     assert np.array_equal(h.download().x, o.download().x)
     h.close()
+
+
+def test_upload_download_round_trip_and_checks():
+    # every array of the host state goes up and comes back unchanged (links 1-based within
+    # the system, the slots past pcount empty); bad links are refused
+    from nuvort_b200.api import Handle, NuvortError
+    from nuvort_b200.abi import State
+    st = tangle(2, 0.002, n_rings=5)
+    n = st.pcount
+    rng = np.random.default_rng(7)
+    full = State(x=st.x.copy(), infront=st.infront.copy(), behind=st.behind.copy(),
+                 u=rng.standard_normal((n, 3)), u1=rng.standard_normal((n, 3)), u2=rng.standard_normal((n, 3)),
+                 ghosti=rng.standard_normal((n, 3)), ghostb=rng.standard_normal((n, 3)),
+                 closest=rng.integers(0, n + 1, n).astype(np.int32), closestd=rng.standard_normal(n))
+    with Handle([config0_params()] * 2, [n + 100, n + 50], states=[st, st]) as h:
+        h.upload(1, full)
+        back = h.download(1)
+        for name in ("x", "u", "u1", "u2", "ghosti", "ghostb", "closestd", "infront", "behind", "closest"):
+            assert np.array_equal(getattr(back, name), getattr(full, name)), name
+        assert h.counters(1).live == int(np.count_nonzero(st.infront))
+        assert np.array_equal(h.download(0).x, st.x)  # the other system untouched
+        part = h.download(1, out=State.empty(n + 50), fields=("x", "infront"))
+        assert part.u is None and np.array_equal(part.x, full.x) and np.array_equal(part.infront, full.infront)
+        bad = State(x=st.x.copy(), infront=st.infront.copy(), behind=st.behind.copy())
+        bad.infront[3] = n + 1
+        with pytest.raises(NuvortError, match="out of range"):
+            h.upload(1, bad)
+        bad = State(x=st.x.copy(), infront=st.infront.copy(), behind=st.behind.copy())
+        bad.behind[5] = 0
+        with pytest.raises(NuvortError, match="disagree"):
+            h.upload(1, bad)
