@@ -1151,6 +1151,10 @@ __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *_
 // impossible for theta0 <= 2/sqrt(3) (geo <= sqrt(3)/2 width), so it is tested only above.
 // Roots are skipped: their exact centre may still be summing (the walks take the roots'
 // tests from the centre estimate).
+// Relative half-width of the band around the opening threshold inside which the mixed
+// walk's FP32 test defers to the FP64 one (the FP32 |r|^2 is within ~1e-6 of its value).
+constexpr float kTestBand = 1e-5f;
+
 __global__ void k_node_prep(TreeBuffers tb, int nsys, double theta0, int corr, float line_guard,
                             const int *__restrict__ prv) {
   const int n = tb.ctr[0];
@@ -1199,7 +1203,6 @@ __global__ void k_leaf_links(TreeBuffers tb, int nsys, const int *__restrict__ p
 // accepted leaves within the near radius and ill-conditioned far terms in FP64.  Writes
 // the image's partial sum.
 constexpr int kWalkStack = 64;  // two register entries per lane; the build stops at depth 42
-constexpr float kTestBand = 1e-5f;
 
 template <bool kSplit>
 __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__restrict__ scs, SysDyn *dyn,
@@ -1321,7 +1324,7 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
     // children are the only nodes with ids in [first, lim))
     const int sib = kSplit && D.z >= lim && cur >= first && cur < lim ? kEnd : D.z;
     bool open = false;
-    if (D.x != 0 && ((mask >> lane) & 1u)) {
+    if ((mask >> lane) & 1u) {  // (every node below a root has members)
       ++tests;
       const float rx = (A.x - xh[0]) + (B.x - xl[0]);
       const float ry = (A.y - xh[1]) + (B.y - xl[1]);
