@@ -1067,6 +1067,7 @@ __device__ __forceinline__ double cube_dist2(const double x[3], const double4 P,
 // pclose_tree + closest_tree (tree.f90:190-244): theta = width/dist < .5, no shift, no
 // correction; the candidate is prv(first member's infront at build time) with the links of
 // now (after pinsert).
+template <bool kPrefetch>
 __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn,
                                const int *__restrict__ sys_of, const double *__restrict__ X,
                                const int *__restrict__ nxt, const int *__restrict__ prv, int *__restrict__ cl,
@@ -1099,44 +1100,66 @@ __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *_
   // 2^24 positions) and of the distances
   const double margin = 1e-8 * sc.bsize;
   int node = s;
-  while (node != kEnd) {
-    const double4 A = ldg4(&tb.nA[node]);
-    const int4 I = __ldg(&tb.nI[node]);
-    if (I.x == 0) {
-      node = I.z;
-      continue;
+  double4 A = ldg4(&tb.nA[node]);
+  int4 I = __ldg(&tb.nI[node]);
+  for (;;) {
+    // kPrefetch (few targets, latency-bound): the records of both possible successors (next
+    // in preorder past the subtree, first child) are requested before this node is decided,
+    // so their loads overlap the test; with a full GPU the extra loads cost more than that
+    const int nz = I.z, ny = I.y;
+    double4 Az = make_double4(0, 0, 0, 0), Ay = Az;
+    int4 Iz = make_int4(0, kEnd, kEnd, 0), Iy = Iz;
+    if (kPrefetch && nz != kEnd) {
+      Az = ldg4(&tb.nA[nz]);
+      Iz = __ldg(&tb.nI[nz]);
     }
-    const double d2 = e_add(e_add(e_sq(e_sub(xi[0], A.x)), e_sq(e_sub(xi[1], A.y))), e_sq(e_sub(xi[2], A.z)));
-    bool acc = I.x == 1;
-    if (!acc) {
-      const double w4 = 4.0 * A.w * A.w;
-      if (d2 > w4 * (1 + kBand)) acc = true;
-      else if (d2 >= w4 * (1 - kBand)) acc = e_div(A.w, e_sqrt(d2)) < .5;
+    if (kPrefetch && ny != kEnd) {
+      Ay = ldg4(&tb.nA[ny]);
+      Iy = __ldg(&tb.nI[ny]);
     }
-    if (acc) {
-      bool closer;
-      if (d2 < cd2 * (1 - kBand)) closer = true;
-      else if (d2 > cd2 * (1 + kBand)) closer = false;
-      else closer = e_sqrt(d2) < cd;
-      if (closer) {
-        const int j = prv[I.w];
-        if (I.x > 1) {
-          best = 0;
-        } else if (j != (int)g && ni != j && pi_ != j) {
-          best = j;
-          cd = e_sqrt(d2);
-          cd2 = cd * cd;
-        }
+    bool down = false;  // to the first child; else past the subtree
+    if (I.x != 0) {
+      const double d2 = e_add(e_add(e_sq(e_sub(xi[0], A.x)), e_sq(e_sub(xi[1], A.y))), e_sq(e_sub(xi[2], A.z)));
+      bool acc = I.x == 1;
+      if (!acc) {
+        const double w4 = 4.0 * A.w * A.w;
+        if (d2 > w4 * (1 + kBand)) acc = true;
+        else if (d2 >= w4 * (1 - kBand)) acc = e_div(A.w, e_sqrt(d2)) < .5;
       }
-      node = I.z;
-    } else if (I.y != kEnd && node != s && cube_dist2(xi, ldg4(&tb.nP[node]), A.w) > (cd + margin) * (cd + margin)) {
-      // Every member of this node lies in its cell (the splits drop points outside the
-      // children's cells), so every centroid in its subtree is farther than cd: none is
-      // closer, now or later (cd only shrinks), and none changes best or cd.  Skipped.
-      node = I.z;
-    } else {
-      node = I.y != kEnd ? I.y : I.z;
+      if (acc) {
+        bool closer;
+        if (d2 < cd2 * (1 - kBand)) closer = true;
+        else if (d2 > cd2 * (1 + kBand)) closer = false;
+        else closer = e_sqrt(d2) < cd;
+        if (closer) {
+          const int j = prv[I.w];
+          if (I.x > 1) {
+            best = 0;
+          } else if (j != (int)g && ni != j && pi_ != j) {
+            best = j;
+            cd = e_sqrt(d2);
+            cd2 = cd * cd;
+          }
+        }
+      } else if (ny != kEnd &&
+                 !(node != s && cube_dist2(xi, ldg4(&tb.nP[node]), A.w) > (cd + margin) * (cd + margin))) {
+        down = true;
+      }
+      // (an opened node whose cell lies farther than cd: every member of this node lies in
+      // its cell -- the splits drop points outside the children's cells -- so every
+      // centroid in its subtree is farther than cd: none is closer, now or later (cd only
+      // shrinks), and none changes best or cd.  Its subtree is skipped.)
     }
+    const int next = down ? ny : nz;
+    if (next == kEnd) break;
+    if (kPrefetch) {
+      A = down ? Ay : Az;
+      I = down ? Iy : Iz;
+    } else {
+      A = ldg4(&tb.nA[next]);
+      I = __ldg(&tb.nI[next]);
+    }
+    node = next;
   }
   cl[g] = best;
   CD[g] = cd;
@@ -1650,8 +1673,10 @@ void launch_closest_tree(nv_handle *h) {
   TreeBuffers *tb = h->tree;
   if (!tb) return;
   join_root_sums(h);
-  k_closest_tree<<<grid_for(h->T, 128), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->nxt, h->prv,
-                                                              h->closest, h->closestd, h->T, *tb, h->d_err);
+  // successor prefetch while the targets fill the GPU less than ~8 blocks per SM
+  auto walk = h->T < 8LL * 128 * n_sms() ? k_closest_tree<true> : k_closest_tree<false>;
+  walk<<<grid_for(h->T, 128), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->nxt, h->prv, h->closest,
+                                                   h->closestd, h->T, *tb, h->d_err);
 }
 
 // Preorder dump of system `sys`'s tree (host side: download nodes, follow first_child/skip).
