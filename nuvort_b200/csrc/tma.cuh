@@ -3,7 +3,7 @@
 //
 // Rules kept here: every source and destination address and every size is a multiple of
 // 16 bytes (callers stage whole 32- or 64-byte records from cudaMalloc'd arrays); no
-// `.multicast::cluster` form is used; every wait gives up after a fixed number of
+// cluster-multicast form is used; every wait gives up after a fixed number of
 // polls and reports it, so a lost completion cannot hang the GPU.
 #pragma once
 
