@@ -1227,8 +1227,11 @@ __global__ void k_leaf_links(TreeBuffers tb, int nsys, const int *__restrict__ p
 // the image's partial sum.
 constexpr int kWalkStack = 64;  // two register entries per lane; the build stops at depth 42
 
+// Large systems (kSplit false, the GPU full of long walks): the FP64 accumulators live in
+// shared memory and 9 blocks fit on an SM; small ones (split central image, a short tail):
+// accumulators in registers, 8 blocks (both measured faster than the other choice).
 template <bool kSplit>
-__global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__restrict__ scs, SysDyn *dyn,
+__global__ void __launch_bounds__(128, kSplit ? 8 : 9) k_tree_walk_mixed(const SysConst *__restrict__ scs, SysDyn *dyn,
                                                             const int4 *__restrict__ work,
                                                             const double *__restrict__ X,
                                                             const int *__restrict__ nxt, const int *__restrict__ prv,
@@ -1262,7 +1265,13 @@ __global__ void __launch_bounds__(128, 8) k_tree_walk_mixed(const SysConst *__re
   const float gq = (float)(sc.quant_circ / (4.0 * NV_PI));
   const bool second = sc.tree_extra_correction && sc.tree_theta > 1.1547;
   float fx = 0, fy = 0, fz = 0;  // FP32 partial over at most kFlush far interactions
-  double nx = 0, ny = 0, nz = 0;  // FP64: near field plus the flushed FP32 partials
+  // FP64: near field plus the flushed FP32 partials (touched only at a flush or an FP64 term)
+  __shared__ double s_acc[kSplit ? 1 : 3][128];
+  double r_acc0 = 0., r_acc1 = 0., r_acc2 = 0.;
+  double &nx = kSplit ? r_acc0 : s_acc[0][threadIdx.x];
+  double &ny = kSplit ? r_acc1 : s_acc[kSplit ? 0 : 1][threadIdx.x];
+  double &nz = kSplit ? r_acc2 : s_acc[kSplit ? 0 : 2][threadIdx.x];
+  nx = ny = nz = 0.;
   bool singular = false;
   // r and |r|^2 in FP64 as the FP64 walk forms them: (centre + shift) - target
   auto exact_r = [&](int cur, double r[3]) -> double {
