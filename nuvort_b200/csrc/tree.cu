@@ -306,7 +306,11 @@ __global__ void k_root_digits(const double *__restrict__ X, long long T, TreeBuf
     double x[3];
     load_x(X, T, g, x);
     d = octant(x, tb.nP[s], tb.nA[s].w / 2.0);
-    if (d < 8) atomicAdd(&tb.root_cnt[8 * s + d], 1);
+    if (d < 8) {  // one atomic per (system, octant) per warp: 8 counters take all the slots
+      const int key = 8 * s + d;
+      const unsigned peers = __match_any_sync(__activemask(), key);
+      if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&tb.root_cnt[key], __popc(peers));
+    }
   }
   tb.rkey[0][q] = ((unsigned)s << 4) | (unsigned)d;
   tb.rval[0][q] = g;
