@@ -114,19 +114,6 @@ __global__ void k_scatter_live(const int *__restrict__ flag, const int *__restri
   if (g < T && flag[g]) members[pos[g]] = (int)g;
 }
 
-// Record node id (count members, at `level`) on its level's list of nodes to split.
-__device__ __forceinline__ void push_split(TreeBuffers &tb, int id, int count, int level, unsigned *err) {
-  const int b = level % 3;
-  if (count > kBigNode) {
-    const int q = atomicAdd(&tb.ctr[kCtrSplit + b], 1);
-    if (q < tb.max_blk) tb.split_blk[b][q] = id;
-    else if (err) atomicOr(err, DERR_TREE_NODES);
-  } else {
-    const int q = atomicAdd(&tb.ctr[kCtrSplit + 3 + b], 1);
-    if (q < tb.max_wrp) tb.split_wrp[b][q] = id;
-    else if (err) atomicOr(err, DERR_TREE_NODES);
-  }
-}
 
 // Root of every system (construct_tree, tree.f90:38-59).
 __global__ void k_roots(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, const int *__restrict__ nxt,
@@ -245,9 +232,26 @@ __device__ void make_children(TreeBuffers &tb, int p, const int cnt[8], int *id0
     *mb0_out = -1;
     return;
   }
+  // one reservation per counter for the whole node (node ids, member slots, split-list and
+  // big-node entries), the atomics issued together rather than one per child
+  const int depth = tb.nDepth[p] + 1;
+  const int lb = depth % 3;
+  int nblk = 0, nwrp = 0, nbig = 0;
+#pragma unroll
+  for (int d = 0; d < 8; ++d) {
+    if (cnt[d] >= 2) {
+      if (cnt[d] > kBigNode) ++nblk;
+      else ++nwrp;
+    }
+    if (cnt[d] > kBlockSumNode) ++nbig;
+  }
   const int id0 = atomicAdd(&tb.ctr[0], nchild);
   const int mb0 = atomicAdd(&tb.ctr[1], kept);
-  if (id0 + nchild > tb.max_nodes || (long long)mb0 + kept > tb.max_members) {
+  const int qb = nblk ? atomicAdd(&tb.ctr[kCtrSplit + lb], nblk) : 0;
+  const int qw = nwrp ? atomicAdd(&tb.ctr[kCtrSplit + 3 + lb], nwrp) : 0;
+  const int qg = nbig ? atomicAdd(&tb.ctr[kCtrBig], nbig) : 0;
+  if (id0 + nchild > tb.max_nodes || (long long)mb0 + kept > tb.max_members || qb + nblk > tb.max_blk ||
+      qw + nwrp > tb.max_wrp || qg + nbig > tb.max_big) {
     atomicOr(err, DERR_TREE_NODES);
     *id0_out = -1;
     *mb0_out = -1;
@@ -255,8 +259,7 @@ __device__ void make_children(TreeBuffers &tb, int p, const int cnt[8], int *id0
   }
   const double4 P = tb.nP[p];
   const double h = tb.nA[p].w / 2.0;
-  const int depth = tb.nDepth[p] + 1;
-  int off = 0, k = 0;
+  int off = 0, k = 0, kb = 0, kw = 0, kg = 0;
 #pragma unroll
   for (int d = 0; d < 8; ++d) {
     if (!cnt[d]) continue;
@@ -271,12 +274,11 @@ __device__ void make_children(TreeBuffers &tb, int p, const int cnt[8], int *id0
     tb.nR[id] = make_int2(mb0 + off, cnt[d]);
     tb.nDepth[id] = depth;
     tb.nSib[id] = last ? kEnd : id + 1;
-    if (cnt[d] >= 2) push_split(tb, id, cnt[d], depth, err);
-    if (cnt[d] > kBlockSumNode) {
-      const int b = atomicAdd(&tb.ctr[kCtrBig], 1);
-      if (b < tb.max_big) tb.bigl[b] = id;
-      else atomicOr(err, DERR_TREE_NODES);
+    if (cnt[d] >= 2) {  // the child's level list of nodes still to split
+      if (cnt[d] > kBigNode) tb.split_blk[lb][qb + kb++] = id;
+      else tb.split_wrp[lb][qw + kw++] = id;
     }
+    if (cnt[d] > kBlockSumNode) tb.bigl[qg + kg++] = id;
     off += cnt[d];
     ++k;
   }
