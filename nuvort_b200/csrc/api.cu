@@ -260,8 +260,9 @@ int rebuild_worklists(nv_handle *h) {
   return NV_OK;
 }
 
-int pull_dyn(nv_handle *h) {
-  NV_CUDA(cudaMemcpyAsync(h->h_dyn.data(), h->d_dyn, h->nsys * sizeof(SysDyn), cudaMemcpyDeviceToHost, h->stream));
+// the host copy of one system's dynamic state (after the stream's work so far)
+int pull_dyn_one(nv_handle *h, int sys) {
+  NV_CUDA(cudaMemcpyAsync(&h->h_dyn[sys], h->d_dyn + sys, sizeof(SysDyn), cudaMemcpyDeviceToHost, h->stream));
   NV_CUDA(cudaStreamSynchronize(h->stream));
   return NV_OK;
 }
@@ -587,7 +588,7 @@ int nv_upload(nv_handle *h, int32_t sys, const nv_host_state *st) {
   if (check[0] & 2) return set_error(NV_ERR_ARG, "nv_upload: infront/behind disagree on an empty slot");
   SysDyn &d = h->h_dyn[sys];
   // keep the clock and counters; replace the slot count
-  rc = pull_dyn(h);
+  rc = pull_dyn_one(h, sys);
   if (rc) return rc;
   d.pcount = n;
   d.live = check[1];
@@ -601,7 +602,7 @@ int nv_download(nv_handle *h, int32_t sys, nv_host_state *st, int32_t cap) {
   if (!h || !st || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_download: bad arguments");
   int rc = set_device(h);
   if (rc) return rc;
-  if ((rc = pull_dyn(h))) return rc;
+  if ((rc = pull_dyn_one(h, sys))) return rc;
   const int n = h->h_dyn[sys].pcount, base = h->base[sys];
   st->pcount = n;
   if (n > cap) return set_error(NV_ERR_ARG, "nv_download: arrays hold fewer slots than pcount");
@@ -634,7 +635,7 @@ int nv_download(nv_handle *h, int32_t sys, nv_host_state *st, int32_t cap) {
 int nv_set_clock(nv_handle *h, int32_t sys, double t, int32_t itime) {
   if (!h || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_set_clock: bad arguments");
   int rc = set_device(h);
-  if (rc || (rc = pull_dyn(h))) return rc;
+  if (rc || (rc = pull_dyn_one(h, sys))) return rc;
   h->h_dyn[sys].t = t;
   h->h_dyn[sys].itime = itime;
   NV_CUDA(cudaMemcpy(h->d_dyn + sys, &h->h_dyn[sys], sizeof(SysDyn), cudaMemcpyHostToDevice));
@@ -644,7 +645,7 @@ int nv_set_clock(nv_handle *h, int32_t sys, double t, int32_t itime) {
 int nv_counters_get(nv_handle *h, int32_t sys, nv_counters *c) {
   if (!h || !c || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_counters_get: bad arguments");
   int rc = set_device(h);
-  if (rc || (rc = pull_dyn(h))) return rc;
+  if (rc || (rc = pull_dyn_one(h, sys))) return rc;
   const SysDyn &d = h->h_dyn[sys];
   c->pcount = d.pcount;
   std::vector<int> nx(d.pcount + 1);
@@ -875,7 +876,7 @@ int nv_calc_velocity_direct_at(nv_handle *h, int32_t sys, const int32_t *targets
   if (!h || !targets || !u3 || sys < 0 || sys >= h->nsys || n < 0)
     return set_error(NV_ERR_ARG, "nv_calc_velocity_direct_at: bad arguments");
   int rc = set_device(h);
-  if (rc || (rc = pull_dyn(h))) return rc;
+  if (rc || (rc = pull_dyn_one(h, sys))) return rc;
   std::vector<int> g(n);
   for (int k = 0; k < n; ++k) {
     if (targets[k] < 1 || targets[k] > h->h_dyn[sys].pcount)
@@ -918,7 +919,7 @@ int nv_tree_dump(nv_handle *h, int32_t sys, nv_tree_node *buf, int32_t cap, int3
 int nv_diagnostics(nv_handle *h, int32_t sys, int64_t *out, int32_t n) {
   if (!h || !out || sys < 0 || sys >= h->nsys || n < 0 || n > 12) return set_error(NV_ERR_ARG, "nv_diagnostics: bad arguments");
   int rc = set_device(h);
-  if (rc || (rc = pull_dyn(h))) return rc;
+  if (rc || (rc = pull_dyn_one(h, sys))) return rc;
   for (int k = 0; k < n; ++k) out[k] = h->h_dyn[sys].diag[k];
   return NV_OK;
 }
