@@ -1,27 +1,38 @@
 """Benchmark of the filament-velocity hot path: point-velocity evaluations per second.
 
-Default workload (--workload tangle32k): random vortex rings, seed 1, delta = 0.001 cm,
-exactly 32,768 points in a periodic cube D = 0.1 cm; Barnes-Hut theta = 0.4 with the extra
-correction; mutual friction alpha = 0.1, alpha' = 0.01 against a uniform normal flow
-v_n = (0, 0, 0.5) cm/s; dt = 5e-6 s; insertion, removal and reconnection on.  Seeded
-synthetic input (no dataset).  Other workloads: rings8 (8 rings, direct sum, FP64 small
-case), ensemble512 (512 independent systems of 500-20,000 points), tangle1m (1,048,576
-points, theta = 0.5), ensemble32 (32 systems of 131k-262k points).
+Default workload (--workload ensemble512): an ensemble of 512 independent random-ring systems
+(seed 2), point counts log-uniform in [500, 20000] (about 2.7M points), delta = 0.002 cm,
+periodic cube D = 0.1 cm; per system alpha ~ U[0.03,0.2], alpha' ~ U[0,0.02] and a uniform
+normal flow of magnitude U[0,1] cm/s along a random axis; direct sum below the autotuned
+direct/tree crossover, Barnes-Hut theta = 0.4 above it; dt = 2e-5 s; insertion, removal and
+reconnection on; every system advanced by the same launches (one per stage).  The same line
+carries the 1,048,576-point counterflow tangle (seed 3, delta = 0.0005 cm, theta = 0.5,
+alpha = (0.1, 0.01), v_n = (1,0,0) cm/s, dt = 1e-6 s) as the sub-object "tangle1m", with its
+own mixed/plain timing, error and event comparison over at least 20 steps.  Seeded synthetic
+input (no dataset).  Other workloads (--workload): rings8 (8 rings, direct sum, FP64 small
+case), tangle32k (32,768 points, theta = 0.4), tangle1m, ensemble32 (32 systems of
+131k-262k points).
 
 One step = one whole time step on the device (ghosts, tree build, velocity of every point
 with 27 periodic images, AB3 update, insertion, closest-point search, reconnection, removal,
 periodic wrap), replayed from a CUDA graph.  value = sum over timed steps of live points /
-sum of per-step device time (CUDA events recorded on the library's stream), max over ranks.
-Between timed steps a 256 MiB buffer is written to flush L2.
+sum of per-step device time of whole steps (CUDA events recorded on the library's stream),
+max over ranks; "velocity_stage" gives the same per velocity-stage time.  Between timed steps
+a 256 MiB buffer is written to flush L2.
 
 The product arm runs the mixed-precision path; the plain FP64 path (the drop-in that
 reproduces the reference arithmetic) is measured beside it on the same initial state, and
 the line reports both, their velocity difference, their error against the FP64 direct sum
 on a seeded subsample of points, and whether their topology event logs agree.
 
+Multi-GPU (torchrun, one rank per GPU): an ensemble's systems are split across the ranks by
+a greedy balance of sum N^2 (nuvort_b200.dist.shard_systems), the same ensemble whatever the
+rank count (strong scaling, no collective on the data path); a single-tangle workload runs one
+replica per rank (seed + rank, weak scaling).
+
 --impl reference times the CPU oracle -- the line-by-line C++ restatement of the reference
 Fortran (the Fortran itself cannot be built here: no Fortran compiler) -- on all host
-threads, on the same workload.
+threads, on a bounded sample of the same workload.
 """
 from __future__ import annotations
 
@@ -51,8 +62,10 @@ def _p(**kw):
     return make_params(**base)
 
 
-def workload(name: str, rank: int = 0, crossover: int = 3000):
-    """(params per system, states, config dict)."""
+def workload(name: str, rank: int = 0, crossover: int = 3000, world: int = 1):
+    """(params per system, states, config dict) of this rank.  Single tangles: one replica per
+    rank (seed + rank).  Ensembles: the same ensemble on every rank, its systems split across
+    the ranks by shard_systems (sum of N^2 balanced)."""
     from nuvort_b200.rings import random_rings
     L = (0.1, 0.1, 0.1)
     if name == "rings8":
@@ -75,8 +88,9 @@ def workload(name: str, rank: int = 0, crossover: int = 3000):
             "velocity": "Tree", "tree_theta": 0.5, "alpha": [0.1, 0.01], "v_n": [1.0, 0.0, 0.0], "dt": 1e-6,
             "points": 1048576, "images": 27}
     if name in ("ensemble512", "ensemble32"):
+        from nuvort_b200.dist import shard_systems
         big = name == "ensemble32"
-        seed = (4 if big else 2) + 1000 * rank
+        seed = 4 if big else 2
         rng = np.random.Generator(np.random.PCG64(seed))
         nsys = 32 if big else 512
         if big:
@@ -84,6 +98,7 @@ def workload(name: str, rank: int = 0, crossover: int = 3000):
         else:
             counts = np.round(np.exp(rng.uniform(math.log(500), math.log(20000), size=nsys))).astype(int)
         delta = 0.0005 if big else 0.002
+        mine = set(shard_systems([int(c) for c in counts], world, rank))
         params, states = [], []
         for s in range(nsys):
             sub = int(rng.integers(0, 2**31 - 1))
@@ -101,14 +116,19 @@ def workload(name: str, rank: int = 0, crossover: int = 3000):
             n = int(counts[s])
             vel = "Tree" if (big or n >= crossover) else "BS"
             theta = 0.5 if big else 0.4
+            if s not in mine:
+                continue
             params.append(_p(dt=1e-6 if big else 2e-5, delta=delta, velocity=vel, tree_theta=theta, alpha=alpha,
                              normal_velocity="uniform", norm_vel_vec=vec))
             states.append(random_rings(sub, delta, L, n_points=n))
         cfg = {"workload": (f"ensemble of {nsys} independent random-ring systems, points "
                             + ("U[131072,262144]" if big else "log-uniform [500,20000]") + f", seed {seed}"),
-               "systems": nsys, "points": int(sum(s.pcount for s in states)),
+               "systems": nsys, "points": int(sum(int(c) for c in counts)),
                "direct_below": None if big else crossover, "tree_theta": 0.5 if big else 0.4,
                "dt": 1e-6 if big else 2e-5}
+        if world > 1:
+            cfg["sharding"] = (f"{world} ranks, systems split by a greedy balance of sum N^2; this line's "
+                               "value counts every rank's points")
         return params, states, cfg
     raise ValueError(name)
 
@@ -253,7 +273,10 @@ def run_reference(args):
     world, rank, local = dist_setup()
     if rank != 0:
         return 0
-    params, states, cfg = workload(args.workload, 0)
+    # the ensemble's direct/tree split: the crossover the product arm's autotuner measured on
+    # the B200 (500 points, i.e. every system of at least 500 points walks the tree); the CPU
+    # reference itself has no crossover, each system runs with the velocity scheme it is given
+    params, states, cfg = workload(args.workload, 0, crossover=args.crossover or 500)
     import oracle
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
@@ -291,6 +314,109 @@ def run_reference(args):
     return 0
 
 
+def compare_arms(params, states, args, local, flush, torch, dist, steps, warmup, e2e=False):
+    """Mixed (product) and plain FP64 handles on the same initial state: errors on that state,
+    then warm-up and timed steps of each, event comparison over every step run.  Returns
+    (measurements dict, mixed handle, plain handle); the caller closes the handles."""
+    from nuvort_b200 import api
+    caps = [int(s.pcount * 1.6) + 256 for s in states]
+    hm = api.Handle(with_precision(params, args.precision), caps, device=local, states=states)
+    hp = api.Handle(with_precision(params, "fp64"), caps, device=local, states=states) if args.compare else None
+    err = {}
+    if hp is not None:
+        um = [hm.calc_velocity(s) for s in range(len(states))]
+        up = [hp.calc_velocity(s) for s in range(len(states))]
+        err["rms_rel_vs_plain_fp64"] = rms_rel(np.concatenate(um), np.concatenate(up))
+        # FP64 direct-sum yardstick on a seeded subsample of the first system's points
+        rng = np.random.Generator(np.random.PCG64(12345))
+        n0 = states[0].pcount
+        sub = np.sort(rng.choice(np.arange(1, n0 + 1), size=min(args.subsample, n0), replace=False))
+        ud = hp.calc_velocity_direct_at(0, sub)
+        err["rms_rel_vs_direct_fp64"] = {
+            "mixed": rms_rel(um[0][sub - 1], ud), "plain": rms_rel(up[0][sub - 1], ud),
+            "subsample": int(len(sub)), "system": 0,
+            "note": "the tree approximation itself (theta); the same in both arms"}
+        for h in (hm, hp):  # fresh state for the timed run
+            for s, st in enumerate(states):
+                h.upload(s, st, t=0.0, itime=0)
+    for _ in range(warmup):
+        hm.step(1)
+        if hp is not None:
+            hp.step(1)
+    launches = hm.step_launches()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        pts, per_step, vel_ms, evals, tests = timed_steps(hm, steps, flush, torch)
+    stages = timed_steps.stages
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    out = {"pts": pts, "per_step": per_step, "vel_ms": vel_ms, "evals": evals, "tests": tests, "stages": stages,
+           "launches": launches, "clocks": clk.summary(), "err": err, "plain": None}
+    if hp is not None:
+        ppts, pper, pvel, _, _ = timed_steps(hp, steps, flush, torch)
+        # every event of every system, through the device digest (the event log may be full)
+        cm = [hm.counters(s) for s in range(len(states))]
+        cp = [hp.counters(s) for s in range(len(states))]
+        out["plain"] = {"pts": ppts, "step_ms": sum(pper), "vel_ms": pvel}
+        err["events_match_plain"] = all(a.event_hash == b.event_hash and a.n_events == b.n_events
+                                        for a, b in zip(cm, cp))
+        err["events_compared"] = int(sum(c.n_events for c in cp))
+        err["steps_compared"] = warmup + steps
+        err["events_compared_by"] = "per-system event count and order-sensitive 64-bit digest"
+    return out, hm, hp, caps
+
+
+def roofline_of(params, states, m, steps, precision, local):
+    from nuvort_b200 import api
+    from nuvort_b200.abi import NV_VEL_BS
+    mixed = precision == "mixed"
+    # direct-sum systems: 27 N^2 pair-images each (N = live points at the start)
+    pairs = sum(27.0 * float(st.pcount) ** 2 for p, st in zip(params, states) if p.velocity == NV_VEL_BS)
+    tree = m["evals"] / steps >= pairs
+    kernel = ("k_tree_walk_mixed" if mixed else "k_tree_walk_fp64") if tree else (
+        "k_direct_mixed" if mixed else "k_direct_fp64")
+    peak = api.measure_fp32_peak(local) if mixed else api.measure_fp64_peak(local)
+    flops = (43.0 * m["evals"] + 12.0 * m["tests"]) / steps + 43.0 * pairs
+    per_launch = {"interactions": m["evals"] / steps, "opening_tests": m["tests"] / steps,
+                  "direct_pair_images": pairs, "ms": m["vel_ms"] / steps}
+    achieved = flops / (m["vel_ms"] / steps * 1e-3) / 1e12
+    return {"bound": "fp32" if mixed else "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak if peak else None, "traffic": profile_traffic(kernel), "kernel": kernel,
+            "peak_source": ("FP32" if mixed else "FP64") + " FMA rate measured on this GPU by nv_measure_fp"
+                           + ("32" if mixed else "64") + "_peak (MEASURED_PEAKS.json covers HBM and bf16 tensor "
+                           "only); algorithmic flops = 43 per interaction or pair-image + 12 per opening test; "
+                           "time = the velocity stage (all velocity kernels of the step)",
+            "per_launch": per_launch}
+
+
+def tangle1m_summary(args, local, flush, torch):
+    """The 1M-point counterflow tangle, mixed against plain, for the ensemble's line."""
+    params, states, cfg = workload("tangle1m", 0)
+    steps = args.steps
+    warmup = max(args.warmup, 20 - steps)  # events compared over at least 20 steps
+    m, hm, hp, _ = compare_arms(params, states, args, local, flush, torch, None, steps, warmup)
+    hm.close()
+    if hp is not None:
+        hp.close()
+    step_ms = sum(m["per_step"])
+    out = {"config": cfg, "steps": steps, "warmup": warmup,
+           "value": m["pts"] / (step_ms * 1e-3), "ms_per_step": step_ms / steps,
+           "velocity_stage": {"ms_per_step": m["vel_ms"] / steps, "point_evals_per_s": m["pts"] / (m["vel_ms"] * 1e-3)},
+           "stage_ms_per_step": {k: round(v, 4) for k, v in m["stages"].items()},
+           "roofline": roofline_of(params, states, m, steps, args.precision, local), "clocks": m["clocks"]}
+    if m["plain"]:
+        p = m["plain"]
+        out["plain_fp64"] = {"value": p["pts"] / (p["step_ms"] * 1e-3), "ms_per_step": p["step_ms"] / steps,
+                             "velocity_ms_per_step": p["vel_ms"] / steps}
+        out["speedup_vs_plain"] = out["value"] / out["plain_fp64"]["value"]
+        out["velocity_speedup_vs_plain"] = p["vel_ms"] / m["vel_ms"]
+    out["error"] = m["err"]
+    return out
+
+
 def run_ours(args):
     import torch
     world, rank, local = dist_setup()
@@ -308,65 +434,24 @@ def run_ours(args):
         from nuvort_b200.autotune import tune_crossover
         tuned = tune_crossover(device=local, precision=args.precision, delta=0.002, theta=0.4)
         crossover = tuned["crossover"]
-    params, states, cfg = workload(args.workload, rank, crossover=crossover or 3000)
+    params, states, cfg = workload(args.workload, rank, crossover=crossover or 3000, world=world)
+    ensemble = args.workload.startswith("ensemble")
     if tuned is not None:
         cfg["crossover_source"] = ("autotuned on this GPU (nuvort_b200/autotune.py): velocity + tree-build device "
                                    "time per point of batched systems, direct vs tree"
                                    + (", cached" if tuned.get("cached") else ""))
-    caps = [int(s.pcount * 1.6) + 256 for s in states]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    # velocity differences on the initial state (same state for both paths)
-    hm = api.Handle(with_precision(params, args.precision), caps, device=local, states=states)
-    hp = api.Handle(with_precision(params, "fp64"), caps, device=local, states=states) if args.compare else None
-    err = {}
-    if hp is not None:
-        um = [hm.calc_velocity(s) for s in range(len(states))]
-        up = [hp.calc_velocity(s) for s in range(len(states))]
-        err["rms_rel_vs_plain_fp64"] = rms_rel(np.concatenate(um), np.concatenate(up))
-        # FP64 direct-sum yardstick on a seeded subsample of system 0's points
-        rng = np.random.Generator(np.random.PCG64(12345))
-        n0 = states[0].pcount
-        sub = np.sort(rng.choice(np.arange(1, n0 + 1), size=min(args.subsample, n0), replace=False))
-        ud = hp.calc_velocity_direct_at(0, sub)
-        err["rms_rel_vs_direct_fp64"] = {"mixed": rms_rel(um[0][sub - 1], ud), "plain": rms_rel(up[0][sub - 1], ud),
-                                         "subsample": int(len(sub)), "system": 0}
-        for h in (hm, hp):  # fresh state for the timed run
-            for s, st in enumerate(states):
-                h.upload(s, st, t=0.0, itime=0)
-
-    for _ in range(args.warmup):
-        hm.step(1)
-        if hp is not None:
-            hp.step(1)
-    launches = hm.step_launches()
-
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        pts, per_step, vel_ms, evals, tests = timed_steps(hm, args.steps, flush, torch)
-    stages = timed_steps.stages
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    plain = None
-    if hp is not None:
-        ppts, pper, pvel, _, _ = timed_steps(hp, args.steps, flush, torch)
-        # every event of every system, through the device digest (the event log may be full)
-        cm = [hm.counters(s) for s in range(len(states))]
-        cp = [hp.counters(s) for s in range(len(states))]
-        plain = {"value": ppts / (sum(pper) * 1e-3), "ms_per_step": sum(pper) / args.steps,
-                 "velocity_ms_per_step": pvel / args.steps}
-        err["events_match_plain"] = all(a.event_hash == b.event_hash and a.n_events == b.n_events
-                                        for a, b in zip(cm, cp))
-        err["events_compared"] = int(sum(c.n_events for c in cp))
-        err["steps_compared"] = args.warmup + args.steps
-        err["events_compared_by"] = "per-system event count and order-sensitive 64-bit digest"
-
+    m, hm, hp, caps = compare_arms(params, states, args, local, flush, torch, dist, args.steps, args.warmup)
     from nuvort_b200.dist import reduce_max_sum
-    (step_ms, vel_ms), (all_pts,) = reduce_max_sum(dist, "cuda", [sum(per_step), vel_ms], [float(pts)])
+    (step_ms, vel_ms), (all_pts,) = reduce_max_sum(dist, "cuda", [sum(m["per_step"]), m["vel_ms"]], [float(m["pts"])])
     value = all_pts / (step_ms * 1e-3)
+    plain = None
+    if m["plain"]:
+        (pstep, pvel), (ppts,) = reduce_max_sum(dist, "cuda", [m["plain"]["step_ms"], m["plain"]["vel_ms"]],
+                                                [float(m["plain"]["pts"])])
+        plain = {"value": ppts / (pstep * 1e-3), "ms_per_step": pstep / args.steps,
+                 "velocity_ms_per_step": pvel / args.steps}
 
     # end to end through the C ABI with host buffers: upload f(:), one step, download f(:)
     e2e = None
@@ -394,52 +479,41 @@ def run_ours(args):
         e2e = {"value": e_pts / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
                "path": "nv_upload (host f(:) -> device) + nv_step(1) + nv_download (device -> host) per step"}
+    hm.close()
+    if hp is not None:
+        hp.close()
 
     out = None
     if rank == 0:
         mixed = args.precision == "mixed"
-        from nuvort_b200.abi import NV_VEL_BS
-        # direct-sum systems: 27 N^2 pair-images each (N = live points at the start)
-        pairs = sum(27.0 * float(st.pcount) ** 2 for p, st in zip(params, states) if p.velocity == NV_VEL_BS)
-        tree = evals / args.steps >= pairs
-        kernel = ("k_tree_walk_mixed" if mixed else "k_tree_walk_fp64") if tree else (
-            "k_direct_mixed" if mixed else "k_direct_fp64")
-        peak = api.measure_fp32_peak(local) if mixed else api.measure_fp64_peak(local)
-        flops = (43.0 * evals + 12.0 * tests) / args.steps + 43.0 * pairs
-        per_launch = {"interactions": evals / args.steps, "opening_tests": tests / args.steps,
-                      "direct_pair_images": pairs}
-        achieved = flops / (vel_ms / args.steps * 1e-3) / 1e12
-        per_launch["ms"] = vel_ms / args.steps
-        roof = {"bound": "fp32" if mixed else "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak if peak else None, "traffic": profile_traffic(kernel), "kernel": kernel,
-                "peak_source": ("FP32" if mixed else "FP64") + " FMA rate measured on this GPU by nv_measure_fp"
-                               + ("32" if mixed else "64") + "_peak (MEASURED_PEAKS.json covers HBM and bf16 tensor "
-                               "only); algorithmic flops = 43 per interaction + 12 per opening test",
-                "per_launch": per_launch}
         peaks = measured_peaks()
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": step_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
-                "config": dict(cfg, precision=args.precision,
-                               l2="256 MiB buffer written between timed steps"),
+                "scaling": "strong" if ensemble else "weak", "vs_baseline": None,
+                "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
+                "config": dict(cfg, precision=args.precision, l2="256 MiB buffer written between timed steps"),
                 "impl": "ours",
+                "value_basis": "whole steps (ghosts, tree build, velocity, AB3 update, topology); the velocity "
+                               "stage alone is in velocity_stage",
                 "velocity_stage": {"ms_per_step": vel_ms / args.steps, "point_evals_per_s": all_pts / (vel_ms * 1e-3)},
-                "stage_ms_per_step": {k: round(v, 4) for k, v in stages.items()},
-                "roofline": roof, "hbm_peak_gbs": peaks.get("hbm_gbs"), "clocks": clk.summary(),
-                "gpu_launches": launches * args.steps, "per_step_ms": [round(x, 4) for x in per_step]}
+                "stage_ms_per_step": {k: round(v, 4) for k, v in m["stages"].items()},
+                "roofline": roofline_of(params, states, m, args.steps, args.precision, local),
+                "hbm_peak_gbs": peaks.get("hbm_gbs"), "clocks": m["clocks"],
+                "gpu_launches": m["launches"] * args.steps, "per_step_ms": [round(x, 4) for x in m["per_step"]]}
         if plain:
             line["plain_fp64"] = plain
             line["speedup_vs_plain"] = value / plain["value"]
-        if err:
-            line["error"] = err
+            line["velocity_speedup_vs_plain"] = plain["velocity_ms_per_step"] / (vel_ms / args.steps)
+        if m["err"]:
+            line["error"] = dict(m["err"], scope="rank 0's systems" if world > 1 else "every system")
         if e2e:
             line["e2e"] = e2e
-        if world == 1 and not args.no_cpu:
-            line["cpu_baseline"] = cpu_baseline_port(params, states, seconds=args.cpu_seconds)
         out = line
-    hm.close()
-    if hp is not None:
-        hp.close()
+    # the 1M tangle beside the ensemble (rank 0's GPU; the other ranks wait at the barrier)
+    if rank == 0 and args.workload == "ensemble512" and args.with_1m:
+        out["tangle1m"] = tangle1m_summary(args, local, flush, torch)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline_port(params, states, seconds=args.cpu_seconds)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -451,11 +525,13 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["rings8", "tangle32k", "ensemble512", "tangle1m", "ensemble32"],
-                    default="tangle32k")
+                    default="ensemble512")
+    ap.add_argument("--no-1m", dest="with_1m", action="store_false",
+                    help="ensemble512: skip the 1M-tangle sub-object of the line")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--crossover", type=int, default=None,
                     help="ensembles: direct sum below this many points (default: autotuned for ensemble512, 3000 "

@@ -45,7 +45,8 @@ enum {
   NV_ERR_UNSUPPORTED = -9, /* option outside this library (solid walls, grid normal fluid) */
   NV_ERR_STATE = -10,      /* call out of order (e.g. tree search with no tree built) */
   NV_ERR_QUEUE = -11,      /* serial topology resolver overflowed its work queue */
-  NV_ERR_IO = -12          /* run.in could not be opened */
+  NV_ERR_IO = -12,         /* run.in (or a snapshot/restart file) could not be opened or read */
+  NV_ERR_TIMEOUT = -13     /* a bounded device-side wait gave up (the context stays usable) */
 };
 
 /* ---- option values (the run.in strings of src/cdata.f90:131-241) -------------------- */
@@ -115,7 +116,7 @@ typedef struct nv_event {
 
 typedef struct nv_counters {
   int32_t pcount;        /* slots in use                                        */
-  int32_t live;          /* slots with infront>0                                */
+  int32_t live;          /* slots with infront>0 (kept on the device)           */
   int32_t recon_count;   /* reconnections so far         (recon_count)          */
   int32_t remove_count;  /* premove removals so far      (remove_count)         */
   int32_t insert_count;  /* pinsert insertions so far                           */
@@ -163,7 +164,10 @@ int nv_create(const nv_params *params, int32_t nsys, const int32_t *capacity,
               int32_t device, nv_handle **out);
 int nv_destroy(nv_handle *h);
 
-/* Copy one system's state to the device (replaces f(:), pcount) and set its clock. */
+/* Copy one system's state to the device (replaces f(:), pcount); the clock and counters
+ * are kept.  The links are checked before anything is written: a link outside 0..pcount, or
+ * infront/behind disagreeing on an empty slot, returns NV_ERR_ARG and leaves the system's
+ * device state exactly as it was. */
 int nv_upload(nv_handle *h, int32_t sys, const nv_host_state *st);
 /* Copy one system's state back.  Arrays must hold at least `cap` slots; st->pcount
  * receives the system's pcount (NV_ERR_ARG if it exceeds cap). */
@@ -274,10 +278,14 @@ int nv_measure_fp32_peak(int32_t device, double *tflops);
  *   t        simulation time (mutual friction cut-offs)
  *   d_u3     device [3*pcount] output velocities (0 for empty slots)
  *   stream   a cudaStream_t (NULL = the default stream); the call waits for it to finish
- * The first call on a device looks up the array's device address (cudaGetSymbolAddress);
- * make that first call before any stream capture begins.  Every call uses the same array
- * and leaves its contents behind; calls whose work overlaps on the GPU (two host threads,
- * or two streams) race on it and must be serialised by the caller. */
+ * The first call on a device (and the first after a device reset, which creates a new
+ * context) looks up the array's device address with cudaGetSymbolAddress; make that first
+ * call before any stream capture begins.  Each call waits for `stream` to finish its work and
+ * then reads the device error word back to the host before it returns.  A call that fails
+ * (NV_ERR_ARG for links outside 0..pcount or infront/behind disagreeing on an empty slot,
+ * NV_ERR_TIMEOUT for a device wait that gave up) leaves d_u3 unwritten.  Every call uses the
+ * same array and leaves its contents behind; calls whose work overlaps on the GPU (two host
+ * threads, or two streams) race on it and must be serialised by the caller. */
 #define NV_STATIC_MAX_SLOTS 32768
 int nv_calc_velocity_bs_static(const nv_params *p, int32_t pcount, const double *d_x3,
                                const int32_t *d_infront, const int32_t *d_behind, double t,

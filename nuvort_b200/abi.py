@@ -27,6 +27,7 @@ NV_ERR_UNSUPPORTED = -9
 NV_ERR_STATE = -10
 NV_ERR_QUEUE = -11
 NV_ERR_IO = -12
+NV_ERR_TIMEOUT = -13
 
 ERR_NAMES = {v: k for k, v in globals().items() if k.startswith("NV_ERR_") or k == "NV_OK"}
 

@@ -39,27 +39,30 @@ __global__ void k_put_rows(double *__restrict__ dev, long long T, int base, int 
     dev[c * T + base + k] = host && k >= 1 && k <= n ? host[(long long)comps * (k - 1) + c] : 0.0;
 }
 
-__global__ void k_put_links(int *__restrict__ dev, int base, int rows, int n, const int *__restrict__ host,
-                            int *__restrict__ check) {
+// links already checked by k_upload_check
+__global__ void k_put_links(int *__restrict__ dev, int base, int rows, int n, const int *__restrict__ host) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= rows) return;
-  int v = host && k >= 1 && k <= n ? host[k - 1] : 0;
-  if (v < 0 || v > n) {
-    atomicOr(&check[0], 1);
-    v = 0;
-  }
+  const int v = host && k >= 1 && k <= n ? host[k - 1] : 0;
   dev[base + k] = v ? base + v : 0;
 }
 
-// an empty slot carries an empty link pair; counts the live slots
-__global__ void k_upload_check(const int *__restrict__ nxt, const int *__restrict__ prv, int base, int n,
-                               int *__restrict__ check) {
-  const int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  const bool in = k <= n;
-  const bool live = in && nxt[base + k] > 0;
-  if (in && (nxt[base + k] == 0) != (prv[base + k] == 0)) atomicOr(&check[0], 2);
-  const unsigned b = __ballot_sync(0xffffffffu, live);
-  if ((threadIdx.x & 31) == 0 && b) atomicAdd(&check[1], __popc(b));
+// The staged host links (infront, behind and, if given, closest: n each), before any of them
+// reaches the system's slots: every link in 0..n, and an empty slot carries an empty link
+// pair.  Counts the live slots.
+__global__ void k_upload_check(const int *__restrict__ inf, const int *__restrict__ beh,
+                               const int *__restrict__ clo, int n, int *__restrict__ check) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool in = k < n;
+  bool live = false;
+  if (in) {
+    const int a = inf[k], b = beh[k], c = clo ? clo[k] : 0;
+    if (a < 0 || a > n || b < 0 || b > n || c < 0 || c > n) atomicOr(&check[0], 1);
+    if ((a == 0) != (b == 0)) atomicOr(&check[0], 2);
+    live = a > 0;
+  }
+  const unsigned bl = __ballot_sync(0xffffffffu, live);
+  if ((threadIdx.x & 31) == 0 && bl) atomicAdd(&check[1], __popc(bl));
 }
 
 __global__ void k_get_rows(const double *__restrict__ dev, long long T, int base, int n, int comps,
@@ -84,10 +87,16 @@ int err_code_from_bits(unsigned bits, std::string &msg) {
   if (bits & DERR_EMPTY) { msg = "pinsert: vortex line length is 0, run over"; return NV_ERR_EMPTY; }
   if (bits & DERR_CAPACITY) { msg = "pinsert: system capacity exhausted"; return NV_ERR_CAPACITY; }
   if (bits & DERR_QUEUE) { msg = "topology resolver work queue overflow"; return NV_ERR_QUEUE; }
-  if (bits & DERR_TIMEOUT) { msg = "device wait gave up (bounded spin exceeded)"; return NV_ERR_CUDA; }
+  if (bits & DERR_TIMEOUT) { msg = "device wait gave up (bounded spin exceeded)"; return NV_ERR_TIMEOUT; }
   msg = "unknown device error";
   return NV_ERR_CUDA;
 }
+
+}  // namespace
+
+int status_from_device_bits(unsigned bits, std::string &msg) { return err_code_from_bits(bits, msg); }
+
+namespace {
 
 // Synchronise the handle's stream and turn the device error word into a status.
 int finish(nv_handle *h) {
@@ -551,7 +560,6 @@ int nv_destroy(nv_handle *h) {
 int nv_upload(nv_handle *h, int32_t sys, const nv_host_state *st) {
   if (!h || !st || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_upload: bad arguments");
   if (!st->x || !st->infront || !st->behind) return set_error(NV_ERR_ARG, "nv_upload: x, infront, behind are required");
-  ++h->links_epoch;
   const int n = st->pcount, cap = h->cap[sys], base = h->base[sys];
   if (n < 0 || n > cap) return set_error(NV_ERR_ARG, "nv_upload: pcount exceeds the system's capacity");
   int rc = set_device(h);
@@ -559,39 +567,46 @@ int nv_upload(nv_handle *h, int32_t sys, const nv_host_state *st) {
   const long long T = h->T;
   const int rows = cap + 1;  // the system's dummy slot and all its slots
   cudaStream_t sm = h->stream;
-  // each host array goes to the staging buffer in one copy and from there to the slots (in
-  // stream order, so the buffer is reused array after array)
+  // The links are staged and checked first, so that a rejected upload leaves the system as
+  // it was: infront, behind and closest side by side in the staging buffer (3n ints fit in
+  // its 3(cap+1) doubles).
+  int *stage_i = reinterpret_cast<int *>(h->stage);
+  int *s_inf = stage_i, *s_beh = stage_i + n, *s_clo = st->closest ? stage_i + 2 * (size_t)n : nullptr;
+  NV_CUDA(cudaMemsetAsync(h->d_upck, 0, 2 * sizeof(int), sm));
+  if (n > 0) {
+    NV_CUDA(cudaMemcpyAsync(s_inf, st->infront, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, sm));
+    NV_CUDA(cudaMemcpyAsync(s_beh, st->behind, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, sm));
+    if (s_clo) NV_CUDA(cudaMemcpyAsync(s_clo, st->closest, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, sm));
+    k_upload_check<<<grid_for(n, 256), 256, 0, sm>>>(s_inf, s_beh, s_clo, n, h->d_upck);
+  }
+  int check[2] = {0, 0};
+  NV_CUDA(cudaMemcpyAsync(check, h->d_upck, sizeof check, cudaMemcpyDeviceToHost, sm));
+  NV_CUDA(cudaStreamSynchronize(sm));
+  if (check[0] & 1) return set_error(NV_ERR_ARG, "nv_upload: link out of range (system left unchanged)");
+  if (check[0] & 2)
+    return set_error(NV_ERR_ARG, "nv_upload: infront/behind disagree on an empty slot (system left unchanged)");
+  ++h->links_epoch;
+  k_put_links<<<grid_for(rows, 256), 256, 0, sm>>>(h->nxt, base, rows, n, n > 0 ? s_inf : nullptr);
+  k_put_links<<<grid_for(rows, 256), 256, 0, sm>>>(h->prv, base, rows, n, n > 0 ? s_beh : nullptr);
+  k_put_links<<<grid_for(rows, 256), 256, 0, sm>>>(h->closest, base, rows, n, n > 0 ? s_clo : nullptr);
+  // each double array goes to the staging buffer in one copy and from there to the slots (in
+  // stream order, so the buffer is reused array after array, after the links above)
   auto put = [&](double *dev, const double *src, int comps) -> int {
     if (src && n > 0)
       NV_CUDA(cudaMemcpyAsync(h->stage, src, (size_t)comps * n * sizeof(double), cudaMemcpyHostToDevice, sm));
     k_put_rows<<<grid_for(rows, 256), 256, 0, sm>>>(dev, T, base, rows, n, comps, src ? h->stage : nullptr);
     return NV_OK;
   };
-  int *stage_i = reinterpret_cast<int *>(h->stage);
-  auto put_link = [&](int *dev, const int *src) -> int {
-    if (src && n > 0) NV_CUDA(cudaMemcpyAsync(stage_i, src, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, sm));
-    k_put_links<<<grid_for(rows, 256), 256, 0, sm>>>(dev, base, rows, n, src ? stage_i : nullptr, h->d_upck);
-    return NV_OK;
-  };
-  NV_CUDA(cudaMemsetAsync(h->d_upck, 0, 2 * sizeof(int), sm));
   if ((rc = put(h->x, st->x, 3)) || (rc = put(h->u, st->u, 3)) || (rc = put(h->u1, st->u1, 3)) ||
       (rc = put(h->u2, st->u2, 3)) || (rc = put(h->gi, st->ghosti, 3)) || (rc = put(h->gb, st->ghostb, 3)) ||
-      (rc = put_link(h->nxt, st->infront)) || (rc = put_link(h->prv, st->behind)) ||
-      (rc = put_link(h->closest, st->closest)) || (rc = put(h->closestd, st->closestd, 1)))
+      (rc = put(h->closestd, st->closestd, 1)))
     return rc;
-  // closest links were checked with the others; only infront/behind count for the live slots
-  k_upload_check<<<grid_for(std::max(n, 1), 256), 256, 0, sm>>>(h->nxt, h->prv, base, n, h->d_upck);
-  int check[2] = {0, 0};
-  NV_CUDA(cudaMemcpyAsync(check, h->d_upck, sizeof check, cudaMemcpyDeviceToHost, sm));
-  NV_CUDA(cudaStreamSynchronize(sm));
-  if (check[0] & 1) return set_error(NV_ERR_ARG, "nv_upload: link out of range");
-  if (check[0] & 2) return set_error(NV_ERR_ARG, "nv_upload: infront/behind disagree on an empty slot");
   SysDyn &d = h->h_dyn[sys];
-  // keep the clock and counters; replace the slot count
+  // keep the clock and counters; replace the slot count (pull_dyn_one waits for the copies)
   rc = pull_dyn_one(h, sys);
   if (rc) return rc;
   d.pcount = n;
-  d.live = check[1];
+  d.nlive = check[1];
   NV_CUDA(cudaMemcpy(h->d_dyn + sys, &d, sizeof(SysDyn), cudaMemcpyHostToDevice));
   unsigned zero = 0;
   NV_CUDA(cudaMemcpy(h->d_err, &zero, sizeof zero, cudaMemcpyHostToDevice));
@@ -648,11 +663,7 @@ int nv_counters_get(nv_handle *h, int32_t sys, nv_counters *c) {
   if (rc || (rc = pull_dyn_one(h, sys))) return rc;
   const SysDyn &d = h->h_dyn[sys];
   c->pcount = d.pcount;
-  std::vector<int> nx(d.pcount + 1);
-  NV_CUDA(cudaMemcpy(nx.data(), h->nxt + h->base[sys], (d.pcount + 1) * sizeof(int), cudaMemcpyDeviceToHost));
-  int live = 0;
-  for (int k = 1; k <= d.pcount; ++k) live += nx[k] != 0;
-  c->live = live;
+  c->live = d.nlive;
   c->recon_count = d.recon_count;
   c->remove_count = d.remove_count;
   c->insert_count = d.insert_count;

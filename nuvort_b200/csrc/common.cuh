@@ -65,7 +65,8 @@ struct SysDyn {
   unsigned long long tree_tests;
   int event_seq;
   unsigned long long ev_hash;  // sum of event_digest over this system's events
-  int live;
+  int live;          // pinsert: the system has a live point (src/line.f90:25-27)
+  int nlive;         // live slots: set by nv_upload, kept by the topology stages' events
   int old_pcount;
   int ins_fallback;  // pinsert needs the serial sweep this step
   int ins_conv;      // pinsert's fixed-point iteration has converged

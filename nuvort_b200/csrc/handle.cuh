@@ -118,6 +118,8 @@ void launch_precon(nv_handle *h);
 void launch_premove(nv_handle *h);
 
 int set_error(int code, const std::string &msg);
+// status code and message for a non-zero device error word (DERR_* bits)
+int status_from_device_bits(unsigned bits, std::string &msg);
 SysConst sysconst_for(const nv_params &p, int base, int cap);
 void launch_ghost_raw(cudaStream_t st, const SysConst *sc, const SysDyn *dyn, const int *sys_of, const double *x,
                       const int *nxt, const int *prv, double *gi, double *gb, double4 *seg, long long T,

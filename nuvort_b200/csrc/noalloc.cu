@@ -5,8 +5,10 @@
 //
 // The array is a file-scope __device__ symbol, so it exists on every GPU that loads the
 // library, from module load until the process exits.  Host code cannot use the symbol's
-// name as a device address; the first call on each device looks the address up with
-// cudaGetSymbolAddress (with that device current) and later calls reuse it.
+// name as a device address; the first call on each device context looks the address up with
+// cudaGetSymbolAddress (with that device current) and later calls in the same context reuse
+// it.  A device reset creates a new context (and reloads the module), so the address is
+// looked up again there.
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -38,22 +40,61 @@ static __device__ __align__(256) unsigned char g_scratch[kBytes];
 
 constexpr unsigned kErrLink = 1u << 8;  // a link outside 0..pcount
 
-unsigned char *g_base[64] = {};
+// Per device: the context the address was looked up in (its process-unique id) and the
+// address.  A context id of 0 means "not set up".
+struct ScratchAddr {
+  unsigned long long ctx_id;
+  unsigned char *ptr;
+};
+ScratchAddr g_addr[64] = {};
 std::mutex g_setup;
 
-// Device address of g_scratch on the current device, looked up once per device.
+// The id of the calling thread's current context (cuCtxGetCurrent + cuCtxGetId, reached
+// through the runtime's driver entry points so that the library needs no -lcuda).
+typedef int (*CtxGetCurrentFn)(void **);
+typedef int (*CtxGetIdFn)(void *, unsigned long long *);
+int current_context_id(unsigned long long *id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  if (!get_current || !get_id) {
+    void *f1 = nullptr, *f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+    NV_CUDA(cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1));
+    NV_CUDA(cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2));
+    if (q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2)
+      return set_error(NV_ERR_CUDA, "nv_calc_velocity_bs_static: driver context queries unavailable");
+    get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+    get_id = reinterpret_cast<CtxGetIdFn>(f2);
+  }
+  void *ctx = nullptr;
+  if (get_current(&ctx) != 0) return set_error(NV_ERR_CUDA, "nv_calc_velocity_bs_static: cuCtxGetCurrent failed");
+  if (!ctx) {  // no context current on this thread yet: the runtime's primary one
+    int dev = 0;
+    NV_CUDA(cudaGetDevice(&dev));
+    NV_CUDA(cudaSetDevice(dev));  // initialises and binds the device's primary context
+    if (get_current(&ctx) != 0 || !ctx)
+      return set_error(NV_ERR_CUDA, "nv_calc_velocity_bs_static: no current CUDA context");
+  }
+  if (get_id(ctx, id) != 0 || *id == 0) return set_error(NV_ERR_CUDA, "nv_calc_velocity_bs_static: cuCtxGetId failed");
+  return NV_OK;
+}
+
+// Device address of g_scratch in the current device's context: looked up once per context.
 int scratch_base(unsigned char **out) {
   int dev = 0;
   NV_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return set_error(NV_ERR_ARG, "nv_calc_velocity_bs_static: device index above 63");
+  unsigned long long ctx = 0;
+  int rc = current_context_id(&ctx);
+  if (rc != NV_OK) return rc;
   std::lock_guard<std::mutex> lock(g_setup);
-  if (!g_base[dev]) {
+  if (g_addr[dev].ctx_id != ctx) {
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
     if (e != cudaSuccess) return check_cuda(e, "cudaGetSymbolAddress(static scratch)");
-    g_base[dev] = static_cast<unsigned char *>(p);
+    g_addr[dev] = ScratchAddr{ctx, static_cast<unsigned char *>(p)};
   }
-  *out = g_base[dev];
+  *out = g_addr[dev].ptr;
   return NV_OK;
 }
 
@@ -75,10 +116,13 @@ __global__ void k_static_pack(const double *__restrict__ x3, const int32_t *__re
   for (int c = 0; c < 3; ++c) X[c * kS + k] = x3[3 * (k - 1) + c];
 }
 
-// SoA velocities -> the caller's point-major output (0 for empty slots).
-__global__ void k_static_unpack(const double *__restrict__ U, const int *__restrict__ nxt, int n, double *__restrict__ u3) {
+// SoA velocities -> the caller's point-major output (0 for empty slots).  After any device
+// error (bad links, a wait that gave up) the output is left untouched: U would hold another
+// call's velocities.
+__global__ void k_static_unpack(const double *__restrict__ U, const int *__restrict__ nxt, int n, double *__restrict__ u3,
+                                const unsigned *__restrict__ err) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  if (k > n) return;
+  if (k > n || *err) return;
   const bool live = nxt[k] != 0;
   for (int c = 0; c < 3; ++c) u3[3 * (k - 1) + c] = live ? U[c * kS + k] : 0.0;
 }
@@ -131,12 +175,18 @@ extern "C" int nv_calc_velocity_bs_static(const nv_params *p, int32_t pcount, co
   k_static_pack<<<grid_for(pcount + 1, 256), 256, 0, st>>>(d_x3, d_infront, d_behind, pcount, X, nxt, prv, d_err);
   launch_ghost_raw(st, d_sc, d_dyn, sys_of, X, nxt, prv, GI, GB, seg, kS, d_err);
   launch_direct_raw(st, d_sc, d_dyn, work, nwork, X, GI, GB, nxt, prv, seg, U, kS, d_err);
-  k_static_unpack<<<grid_for(pcount, 256), 256, 0, st>>>(U, nxt, pcount, d_u3);
+  k_static_unpack<<<grid_for(pcount, 256), 256, 0, st>>>(U, nxt, pcount, d_u3, d_err);
   NV_CUDA(cudaGetLastError());
   NV_CUDA(cudaStreamSynchronize(st));
   unsigned bits = 0;
   NV_CUDA(cudaMemcpy(&bits, d_err, sizeof bits, cudaMemcpyDeviceToHost));
-  if (bits & kErrLink) return set_error(NV_ERR_ARG, "nv_calc_velocity_bs_static: infront/behind out of range");
-  if (bits) return set_error(NV_ERR_CUDA, "nv_calc_velocity_bs_static: device wait gave up");
+  if (bits & kErrLink)
+    return set_error(NV_ERR_ARG, "nv_calc_velocity_bs_static: infront/behind out of range or disagreeing on an "
+                                 "empty slot (output left unwritten)");
+  if (bits) {
+    std::string msg;
+    const int code = status_from_device_bits(bits, msg);
+    return set_error(code, "nv_calc_velocity_bs_static: " + msg + " (output left unwritten)");
+  }
   return NV_OK;
 }

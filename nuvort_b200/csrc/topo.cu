@@ -622,6 +622,7 @@ __global__ void k_ins_finish(const SysConst *__restrict__ scs, SysDyn *dyn, int 
   const int nfree = pos_b[end] - pos_b[sc.base];
   d.event_seq += nev;
   d.insert_count += nev;
+  d.nlive += nev;
   if (nev > nfree) d.pcount += nev - nfree;
 }
 
@@ -755,10 +756,10 @@ using Touched = SlotSet<10, kTouchedPerChunk>;
 // the events; written back to the system's SysDyn when the sweep ends.
 struct Tally {
   int seq, itime, pcount, base;
-  int recon, remove, insert, kills;
+  int recon, remove, insert, kills, cleared;  // cleared: points the loop kills cleared
   unsigned long long hash;
   __device__ static Tally of(const SysDyn &d, int base) {
-    return Tally{d.event_seq, d.itime, d.pcount, base, 0, 0, 0, 0, 0ull};
+    return Tally{d.event_seq, d.itime, d.pcount, base, 0, 0, 0, 0, 0, 0ull};
   }
   __device__ void store(SysDyn &d) const {
     d.event_seq = seq;
@@ -767,6 +768,7 @@ struct Tally {
     d.remove_count += remove;
     d.insert_count += insert;
     d.loop_kills += kills;
+    d.nlive += insert - remove - cleared;
   }
 };
 
@@ -819,6 +821,7 @@ __device__ void loop_killer_stage(const State &S, Tally &d, int s, int particle,
   if (counter < 4) {
     es.add(d, s, NV_EV_LOOPKILL, particle, counter);
     d.kills++;
+    d.cleared += counter;
     nx = particle;
     for (int it = 0; it < pcount; ++it) {
       const int sn = S.nxt[nx];

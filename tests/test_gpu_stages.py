@@ -72,11 +72,21 @@ def test_upload_download_round_trip_and_checks():
         assert np.array_equal(h.download(0).x, st.x)  # the other system untouched
         part = h.download(1, out=State.empty(n + 50), fields=("x", "infront"))
         assert part.u is None and np.array_equal(part.x, full.x) and np.array_equal(part.infront, full.infront)
-        bad = State(x=st.x.copy(), infront=st.infront.copy(), behind=st.behind.copy())
+        # a refused upload leaves the system exactly as it was
+        moved = State(x=st.x + 0.001, infront=st.infront.copy(), behind=st.behind.copy())
+        bad = State(x=moved.x, infront=st.infront.copy(), behind=st.behind.copy())
         bad.infront[3] = n + 1
         with pytest.raises(NuvortError, match="out of range"):
             h.upload(1, bad)
-        bad = State(x=st.x.copy(), infront=st.infront.copy(), behind=st.behind.copy())
+        bad = State(x=moved.x, infront=st.infront.copy(), behind=st.behind.copy())
         bad.behind[5] = 0
         with pytest.raises(NuvortError, match="disagree"):
             h.upload(1, bad)
+        bad = State(x=moved.x, infront=st.infront.copy(), behind=st.behind.copy(),
+                    closest=np.full(n, -1, np.int32))
+        with pytest.raises(NuvortError, match="out of range"):
+            h.upload(1, bad)
+        back = h.download(1)
+        for name in ("x", "u", "u1", "u2", "ghosti", "ghostb", "closestd", "infront", "behind", "closest"):
+            assert np.array_equal(getattr(back, name), getattr(full, name)), name
+        assert h.counters(1).live == int(np.count_nonzero(st.infront)) and h.counters(1).pcount == n

@@ -43,6 +43,8 @@ def _run_stage(p, st, stages, cap_extra=512, insert_iterations=None, diag=None):
     a, b = h.download(), o.download()
     ea, eb = h.events(), o.events()
     ca, cb = h.counters(), o.counters()
+    # the device keeps the live count through the stage's events (no download needed)
+    assert ca.live == int(np.count_nonzero(a.infront)) and cb.live == int(np.count_nonzero(b.infront))
     if diag is not None:
         diag.extend(h.diagnostics(0))
     h.close()
@@ -141,6 +143,7 @@ def test_whole_steps_config0_events_identical():
     assert np.max(np.abs(a.x - b.x)) < 1e-12
     ca, cb = h.counters(), o.counters()
     assert (ca.recon_count, ca.remove_count, ca.insert_count) == (cb.recon_count, cb.remove_count, cb.insert_count)
+    assert ca.live == cb.live == int(np.count_nonzero(a.infront))
     assert ca.t == cb.t and ca.itime == cb.itime == 200
     h.close()
 
