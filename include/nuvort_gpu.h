@@ -244,6 +244,13 @@ int nv_set_root_band(nv_handle *h, double scale);
  * is the same bit for bit); 1 keeps one thread per target.  0 (the default) picks the split
  * from the number of work items and the SM count. */
 int nv_set_walk_parts(nv_handle *h, int32_t parts);
+/* Split of the plain FP64 direct sum's work.  64: one thread per target, each summing its
+ * terms as it computes them.  1, 2, 4 or 8: a block of 128 threads per that many targets;
+ * three warps compute the terms tile by tile and one lane per (target, component) adds them
+ * in the reference's order, so a small system still fills the GPU (the result is the same
+ * bit for bit).  0 (the default) takes 64 when the direct-sum systems' slots give at least
+ * two blocks of 64 per SM, else the largest split with about four blocks per SM. */
+int nv_set_direct_split(nv_handle *h, int32_t targets_per_block);
 
 /* Turn per-step stage timing on (default) or off.  With timing on, nv_step waits for each
  * step and adds its device time per stage to nv_stage_times; off, steps are queued back to

@@ -263,6 +263,18 @@ int rebuild_worklists(nv_handle *h) {
   build_worklist(h, 1, w);
   if ((rc = upload_worklist(&h->d_work_direct, &h->n_work_direct, w)) != NV_OK) return rc;
   h->any_direct = !w.empty();
+  {  // the split direct sum for few targets: items of direct_g slots
+    long long slots = 0;
+    for (int s = 0; s < h->nsys; ++s)
+      if (h->sc[s].velocity == NV_VEL_BS) slots += h->cap[s];
+    h->direct_g = h->any_direct ? direct_targets_per_block(h, slots) : 64;
+    w.clear();
+    if (h->direct_g < 64)
+      for (int s = 0; s < h->nsys; ++s)
+        if (h->sc[s].velocity == NV_VEL_BS)
+          for (int k = 1; k <= h->cap[s]; k += h->direct_g) w.push_back(make_int2(s, h->sc[s].base + k));
+    if ((rc = upload_worklist(&h->d_work_split, &h->n_work_split, w)) != NV_OK) return rc;
+  }
   build_worklist(h, 2, w);
   if ((rc = upload_worklist(&h->d_work_tree, &h->n_work_tree, w)) != NV_OK) return rc;
   h->any_tree = !w.empty();
@@ -540,7 +552,7 @@ int nv_destroy(nv_handle *h) {
   topo_free(h);
   void *ptrs[] = {h->partial, h->stage, h->d_upck, h->d_sc, h->d_dyn, h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv,
                   h->closest, h->sys_of, h->seg, h->seg32, h->d_err, h->d_events, h->d_event_count,
-                  h->d_work_direct, h->d_work_tree, h->d_work_lia, h->d_work_img, h->d_work_timg};
+                  h->d_work_direct, h->d_work_tree, h->d_work_lia, h->d_work_img, h->d_work_timg, h->d_work_split};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &e : h->ev)
@@ -825,6 +837,18 @@ int nv_set_walk_parts(nv_handle *h, int32_t parts) {
   h->walk_parts = parts;
   if ((rc = rebuild_worklists(h))) return rc;
   h->graph_valid = false;  // the work list is a launch argument of the captured walk
+  return NV_OK;
+}
+
+int nv_set_direct_split(nv_handle *h, int32_t targets_per_block) {
+  const int g = targets_per_block;
+  if (!h || !(g == 0 || g == 1 || g == 2 || g == 4 || g == 8 || g == 64))
+    return set_error(NV_ERR_ARG, "nv_set_direct_split: targets_per_block must be 0 (automatic), 1, 2, 4, 8 or 64");
+  int rc = set_device(h);
+  if (rc) return rc;
+  h->direct_split = g;
+  if ((rc = rebuild_worklists(h))) return rc;
+  h->graph_valid = false;  // the work list is a launch argument of the captured direct sum
   return NV_OK;
 }
 

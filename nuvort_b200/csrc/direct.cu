@@ -160,10 +160,185 @@ __global__ void __launch_bounds__(64) k_direct_fp64(
   store3(U, T, g, u);
 }
 
+// Few targets (a small system, or a short list of targets): the same sums with the work of
+// each target spread over a block.  A block takes G targets; three warps compute the terms
+// of a step -- one tile of segments of one image, 192 terms -- into shared memory while warp
+// 0 adds the previous step's terms, one lane per (target, component), in slot order: the
+// additions are the reference's, in the reference's order, only the terms are computed
+// elsewhere.  A skipped term (empty slot, excluded neighbour, 4ac-b^2 == 0) is stored as
+// +0.0: the accumulators start at +0.0 and a round-to-nearest sum is never -0.0 unless both
+// operands are, so adding +0.0 leaves them bit for bit unchanged, exactly as skipping does.
+constexpr int kSplitTerms = 192;  // terms per step: two per computing thread
+
+template <int G>
+__global__ void __launch_bounds__(128) k_direct_fp64_split(
+    const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn, const int2 *__restrict__ work,
+    const double *__restrict__ X, const double *__restrict__ GI, const double *__restrict__ GB,
+    const int *__restrict__ nxt, const int *__restrict__ prv, const double4 *__restrict__ seg,
+    double *__restrict__ U, long long T, const unsigned *err, const int *__restrict__ targets, int ntargets,
+    double *__restrict__ Uout) {
+  constexpr int TJ = kSplitTerms / G;  // segments per step
+  constexpr int LD = TJ + 1;           // padded row: the adding lanes read different banks
+  __shared__ double s_terms[2][3 * G][LD];
+  __shared__ double s_x[G][3];
+  __shared__ double s_sum[G][3][2];
+  __shared__ int s_g[G], s_p[G], s_act[G];
+  __shared__ int s_abort;
+
+  const int2 w = work[blockIdx.x];
+  const SysConst &sc = scs[w.x];
+  const int base = sc.base;
+  const int pc = dyn[w.x].pcount;
+  const int tid = threadIdx.x;
+  if (!targets && w.y - base > pc) return;  // block-uniform: every target beyond pcount
+  if (tid == 0) s_abort = (*err != 0);
+  if (tid < G) {
+    int g;
+    bool act;
+    if (targets) {
+      const int idx = w.y + tid;
+      g = idx < ntargets ? targets[idx] : base;
+      act = idx < ntargets && g > base && g - base <= pc && nxt[g] != 0;
+    } else {
+      g = w.y + tid;
+      act = g - base <= pc && g - base <= sc.cap && nxt[g] != 0;
+    }
+    s_g[tid] = g;
+    s_act[tid] = act;
+    s_p[tid] = act ? prv[g] : -1;
+    double xi[3] = {0, 0, 0};
+    if (act) load3(X, T, g, xi);
+    for (int c = 0; c < 3; ++c) s_x[tid][c] = xi[c];
+  }
+  __syncthreads();
+  if (s_abort) return;
+
+  const int nt = (pc + TJ - 1) / TJ;
+  const int Q = (1 + sc.n_shift) * nt;
+  const double qc = sc.quant_circ, two_pi = sc.two_pi;
+  double acc0 = 0.0, accs = 0.0;  // adding lanes: unshifted and shifted sums of one component
+  for (int q = 0; q <= Q; ++q) {
+    if (tid >= 32) {
+      if (q < Q) {  // terms of step q
+        const int m = q / nt, t = q % nt;
+        const int n = min(TJ, pc - t * TJ);
+        double(*out)[LD] = s_terms[q & 1];
+        double s0 = 0, s1 = 0, s2 = 0;
+        if (m > 0) {
+          s0 = sc.shift[m - 1][0];
+          s1 = sc.shift[m - 1][1];
+          s2 = sc.shift[m - 1][2];
+        }
+#pragma unroll
+        for (int r = 0; r < kSplitTerms / 96; ++r) {
+          const int e = (tid - 32) + 96 * r;
+          const int tq = e / TJ, jj = e % TJ;
+          if (jj >= n) continue;
+          const int gj = base + 1 + t * TJ + jj;
+          double tm[3] = {0.0, 0.0, 0.0};
+          if (s_act[tq] && gj != s_p[tq] && (m > 0 || gj != s_g[tq])) {
+            const double4 A = seg[2 * (long long)gj], B = seg[2 * (long long)gj + 1];
+            if (A.w != 0.0) {
+              double rr[3];
+              if (m == 0) {
+                rr[0] = e_sub(A.x, s_x[tq][0]);
+                rr[1] = e_sub(A.y, s_x[tq][1]);
+                rr[2] = e_sub(A.z, s_x[tq][2]);
+              } else {
+                rr[0] = e_sub(e_add(A.x, s0), s_x[tq][0]);
+                rr[1] = e_sub(e_add(A.y, s1), s_x[tq][1]);
+                rr[2] = e_sub(e_add(A.z, s2), s_x[tq][2]);
+              }
+              const double d[3] = {B.x, B.y, B.z};
+              const double a = e_add(e_add(e_sq(rr[0]), e_sq(rr[1])), e_sq(rr[2]));
+              if (!bs_term_exact(rr, d, a, B.w, qc, two_pi, tm)) tm[0] = tm[1] = tm[2] = 0.0;
+            }
+          }
+          out[3 * tq + 0][jj] = tm[0];
+          out[3 * tq + 1][jj] = tm[1];
+          out[3 * tq + 2][jj] = tm[2];
+        }
+      }
+    } else if (q >= 1 && tid < 3 * G) {  // add the terms of step q-1, in slot order
+      const int m = (q - 1) / nt, t = (q - 1) % nt;
+      const int n = min(TJ, pc - t * TJ);
+      const double *row = s_terms[(q - 1) & 1][tid];
+      double acc = m == 0 ? acc0 : accs;
+#pragma unroll 8
+      for (int jj = 0; jj < n; ++jj) acc = e_add(acc, row[jj]);
+      if (m == 0) acc0 = acc;
+      else accs = acc;
+    }
+    __syncthreads();
+  }
+  if (tid < 3 * G) {
+    s_sum[tid / 3][tid % 3][0] = acc0;
+    s_sum[tid / 3][tid % 3][1] = accs;
+  }
+  __syncthreads();
+  if (tid >= G || !s_act[tid]) return;
+  const int g = s_g[tid];
+  double xi[3] = {s_x[tid][0], s_x[tid][1], s_x[tid][2]};
+  double gi[3], gb[3], u[3], fdot[3];
+  load3(GI, T, g, gi);
+  load3(GB, T, g, gb);
+  local_velocity(sc, xi, gi, gb, u, fdot);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], s_sum[tid][c][0]);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], s_sum[tid][c][1]);
+  mf_epilogue(sc, dyn[w.x].t, fdot, u);
+  if (targets) {
+    const int idx = w.y + tid;
+    for (int c = 0; c < 3; ++c) Uout[3 * (long long)idx + c] = u[c];
+    return;
+  }
+  store3(U, T, g, u);
+}
+
+template <int G>
+void launch_split(cudaStream_t st, const nv_handle *h, const int2 *work, int nwork, const int *targets, int ntargets,
+                  double *Uout) {
+  k_direct_fp64_split<G><<<nwork, 128, 0, st>>>(h->d_sc, h->d_dyn, work, h->x, h->gi, h->gb, h->nxt, h->prv,
+                                                   h->seg, h->u, h->T, h->d_err, targets, ntargets, Uout);
+}
+
+void launch_split_g(int G, cudaStream_t st, const nv_handle *h, const int2 *work, int nwork, const int *targets,
+                    int ntargets, double *Uout) {
+  switch (G) {
+    case 1: launch_split<1>(st, h, work, nwork, targets, ntargets, Uout); break;
+    case 2: launch_split<2>(st, h, work, nwork, targets, ntargets, Uout); break;
+    case 4: launch_split<4>(st, h, work, nwork, targets, ntargets, Uout); break;
+    default: launch_split<8>(st, h, work, nwork, targets, ntargets, Uout); break;
+  }
+}
+
 }  // namespace
+
+// Targets per block of the split direct sum for n target slots: the largest of 8, 4, 2, 1
+// that still gives about four blocks per SM (1 when even that is not reached).
+int direct_split_g(long long n) {
+  const long long want = 4LL * n_sms_host();
+  int G = 8;
+  while (G > 1 && n / G < want) G /= 2;
+  return G;
+}
+
+// Direct-sum targets per block in use: 64 (one thread per target, k_direct_fp64) when the
+// direct systems' slots fill the GPU with at least two blocks of 64 per SM, else the split
+// kernel's G.  direct_split (nv_set_direct_split) overrides the choice.
+int direct_targets_per_block(const nv_handle *h, long long slots) {
+  if (h->direct_split > 0) return h->direct_split;
+  if (slots >= 2LL * 64 * n_sms_host()) return 64;
+  return direct_split_g(slots);
+}
 
 void launch_direct(nv_handle *h) {
   if (h->n_work_direct == 0) return;
+  if (h->direct_g < 64) {
+    launch_split_g(h->direct_g, h->stream, h, h->d_work_split, h->n_work_split, nullptr, 0, nullptr);
+    return;
+  }
   const size_t smem = 2 * 2 * kDirectTJ * sizeof(double4);
   k_direct_fp64<kDirectTJ><<<h->n_work_direct, 64, smem, h->stream>>>(
       h->d_sc, h->d_dyn, h->d_work_direct, h->x, h->gi, h->gb, h->nxt, h->prv, h->seg, h->u, h->T, h->d_err);
@@ -182,14 +357,19 @@ void launch_direct_raw(cudaStream_t st, const SysConst *sc, const SysDyn *dyn, c
 // listed target slots; u3 is a device buffer of 3*n doubles (point-major, listed order).
 void launch_direct_targets(nv_handle *h, int sys, const int *d_targets, int n, double *d_u3) {
   if (n <= 0) return;
+  const int G = direct_targets_per_block(h, n);
   std::vector<int2> w;
-  for (int b = 0; b < (n + 63) / 64; ++b) w.push_back(make_int2(sys, 64 * b));
+  for (int b = 0; b < (n + G - 1) / G; ++b) w.push_back(make_int2(sys, G * b));
   int2 *dw = nullptr;
   cudaMallocAsync((void **)&dw, w.size() * sizeof(int2), h->stream);
   cudaMemcpyAsync(dw, w.data(), w.size() * sizeof(int2), cudaMemcpyHostToDevice, h->stream);
-  const size_t smem = 2 * 2 * kDirectTJ * sizeof(double4);
-  k_direct_fp64<kDirectTJ><<<(int)w.size(), 64, smem, h->stream>>>(h->d_sc, h->d_dyn, dw, h->x, h->gi, h->gb, h->nxt,
-                                                                   h->prv, h->seg, h->u, h->T, h->d_err, d_targets, n,
-                                                                   d_u3);
+  if (G < 64) {
+    launch_split_g(G, h->stream, h, dw, (int)w.size(), d_targets, n, d_u3);
+  } else {
+    const size_t smem = 2 * 2 * kDirectTJ * sizeof(double4);
+    k_direct_fp64<kDirectTJ><<<(int)w.size(), 64, smem, h->stream>>>(h->d_sc, h->d_dyn, dw, h->x, h->gi, h->gb,
+                                                                     h->nxt, h->prv, h->seg, h->u, h->T, h->d_err,
+                                                                     d_targets, n, d_u3);
+  }
   cudaFreeAsync(dw, h->stream);
 }

@@ -63,6 +63,10 @@ struct nv_handle {
   int2 *d_work_lia = nullptr;
   int n_work_lia = 0;
   int direct_tb = 64;  // targets per block of the direct sum and of the FP64 tree walk (which assumes 64)
+  int direct_split = 0;  // nv_set_direct_split: 0 automatic, 64 one thread per target, 1/2/4/8 split kernel
+  int direct_g = 64;     // targets per block of the direct sum in use
+  int2 *d_work_split = nullptr;  // (system, first slot) items of direct_g slots for the split kernel
+  int n_work_split = 0;
   bool any_tree = false, any_direct = false, any_lia = false;
 
   TreeBuffers *tree = nullptr;
@@ -92,6 +96,7 @@ void launch_wrap(nv_handle *h, int mode);  // bit 1 wrap, bit 2 NaN check
 void launch_end_step(nv_handle *h);
 
 // direct sum (direct.cu)
+int direct_targets_per_block(const nv_handle *h, long long slots);
 void launch_direct(nv_handle *h);
 void launch_direct_targets(nv_handle *h, int sys, const int *d_targets, int n, double *d_u3);
 // mixed precision (mixed.cu)

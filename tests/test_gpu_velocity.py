@@ -70,3 +70,44 @@ def test_velocity_bs_4096():
     ug = _gpu_velocity(p, st)
     uo = Oracle(p, st).calc_velocity()
     assert rel_err(ug, uo).max() <= TOL
+
+
+def test_direct_split_bit_identical_to_one_thread_per_target():
+    # the split kernel computes the terms of each target's sum on many threads and adds them
+    # in the reference's order on one lane per component: the same bits as one thread per
+    # target, for every split, with holes (empty slots) and mutual friction
+    from nuvort_b200.api import Handle
+    st = tangle(11, 0.002, n_rings=9)
+    # empty the third ring (its slots run from the slot after the second ring's last one)
+    ends = [k for k in range(1, st.pcount + 1) if st.infront[k - 1] < k]  # last slot of each ring
+    a, b = ends[1], ends[2]  # 0-based slice [a, b) = 1-based slots a+1..b
+    st.infront[a:b] = 0
+    st.behind[a:b] = 0
+    st.x[a:b] = 0
+    p = config0_params(alpha=(0.1, 0.01), normal_velocity="uniform", norm_vel_vec=(0.1, 0.0, 0.3))
+    uo = Oracle(p, st).calc_velocity()
+    live = st.infront > 0
+    res = {}
+    with Handle(p, [st.pcount + 77], states=[st]) as h:
+        for g in (64, 1, 2, 4, 8, 0):
+            h.set_direct_split(g)
+            res[g] = h.calc_velocity()
+    for g, u in res.items():
+        assert np.array_equal(u, res[64]), g
+    assert np.all(res[64][~live] == 0)
+    assert rel_err(res[64][live], uo[live]).max() <= TOL
+
+
+@pytest.mark.parametrize("split", [64, 4, 0])
+def test_direct_at_listed_targets_split(split):
+    # the FP64 direct-sum yardstick at listed slots, in list order (repeats and unsorted)
+    from nuvort_b200.abi import NV_VEL_BS
+    from nuvort_b200.api import Handle
+    st = tangle(1, 0.001, n_points=4096)
+    p = config1_params("Tree")
+    tg = np.array([4096, 1, 17, 17, 2048, 3000, 5, 999], np.int32)
+    uo = Oracle(p, st).calc_velocity_targets(NV_VEL_BS, tg)
+    with Handle(p, [st.pcount + 64], states=[st]) as h:
+        h.set_direct_split(split)
+        ud = h.calc_velocity_direct_at(0, tg)
+    assert rel_err(ud, uo).max() <= TOL
