@@ -251,6 +251,12 @@ int nv_set_walk_parts(nv_handle *h, int32_t parts);
  * bit for bit).  0 (the default) takes 64 when the direct-sum systems' slots give at least
  * two blocks of 64 per SM, else the largest split with about four blocks per SM. */
 int nv_set_direct_split(nv_handle *h, int32_t targets_per_block);
+/* How pclose (systems with tree_theta 0, src/line.f90:135-160) finds each point's nearest
+ * live non-neighbour: 0 (the default) from a cell list of the live points, rebuilt on every
+ * reconnection step, searching rings of cells around the point until no unsearched cell can
+ * hold a closer one; 1 by scanning every slot, as the reference does.  Both give the
+ * reference's closest and closestd bit for bit (ties to the lowest slot). */
+int nv_set_pclose_method(nv_handle *h, int32_t method);
 
 /* Turn per-step stage timing on (default) or off.  With timing on, nv_step waits for each
  * step and adds its device time per stage to nv_stage_times; off, steps are queued back to

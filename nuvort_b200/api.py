@@ -71,6 +71,7 @@ def lib():
     L.nv_set_root_band.argtypes = [vp, C.c_double]
     L.nv_set_walk_parts.argtypes = [vp, C.c_int32]
     L.nv_set_direct_split.argtypes = [vp, C.c_int32]
+    L.nv_set_pclose_method.argtypes = [vp, C.c_int32]
     L.nv_step_launches.argtypes = [vp, P(i32)]
     L.nv_measure_fp64_peak.argtypes = [i32, P(C.c_double)]
     L.nv_measure_fp32_peak.argtypes = [i32, P(C.c_double)]
@@ -244,6 +245,10 @@ class Handle:
         """Plain FP64 direct sum: 64 = one thread per target; 1, 2, 4, 8 = that many targets per
         block, terms computed by many threads and added in the reference order; 0 = automatic."""
         _check(lib().nv_set_direct_split(self.h, int(targets_per_block)))
+
+    def set_pclose_method(self, method: int):
+        """pclose of tree-less systems: 0 = cell list (default), 1 = scan every slot."""
+        _check(lib().nv_set_pclose_method(self.h, int(method)))
 
     def set_insert_iterations(self, n: int):
         """Fixed-point rounds of the parallel pinsert (0: the serial sweep every step)."""

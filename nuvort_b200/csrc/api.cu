@@ -852,6 +852,14 @@ int nv_set_direct_split(nv_handle *h, int32_t targets_per_block) {
   return NV_OK;
 }
 
+int nv_set_pclose_method(nv_handle *h, int32_t method) {
+  if (!h || (method != 0 && method != 1))
+    return set_error(NV_ERR_ARG, "nv_set_pclose_method: method must be 0 (cell list) or 1 (every slot)");
+  h->pclose_method = method;
+  h->graph_valid = false;  // the captured step holds the chosen kernels
+  return NV_OK;
+}
+
 int nv_set_insert_iterations(nv_handle *h, int32_t n) {
   if (!h || n < 0 || n > 64) return set_error(NV_ERR_ARG, "nv_set_insert_iterations: n must be 0..64");
   h->ins_iters = n;

@@ -63,6 +63,7 @@ struct nv_handle {
   int2 *d_work_lia = nullptr;
   int n_work_lia = 0;
   int direct_tb = 64;  // targets per block of the direct sum and of the FP64 tree walk (which assumes 64)
+  int pclose_method = 0;  // nv_set_pclose_method: 0 cell list, 1 every slot (brute force)
   int direct_split = 0;  // nv_set_direct_split: 0 automatic, 64 one thread per target, 1/2/4/8 split kernel
   int direct_g = 64;     // targets per block of the direct sum in use
   int2 *d_work_split = nullptr;  // (system, first slot) items of direct_g slots for the split kernel

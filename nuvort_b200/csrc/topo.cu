@@ -15,6 +15,10 @@
 //      parallel form for the common case (see below) and sweeps only when that cannot apply.
 // A slot that is neither marked nor touched has a test that is false in the serial sweep
 // too, so the events are the reference's, event for event and in the same order.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
 #include <cub/cub.cuh>
 
 #include "handle.cuh"
@@ -33,6 +37,23 @@ struct TopoBuffers {
   unsigned *l0 = nullptr, *l1 = nullptr;  // sweep bitmaps
   void *cub_tmp = nullptr;
   size_t cub_bytes = 0;
+  // cell list of the closest-point search of the systems without a tree (pclose)
+  struct CellGrid *grid = nullptr;  // per system; nc = 0 for tree systems
+  long long n_cells = 0;            // cells of all systems
+  int *cell_of = nullptr;           // per slot: its cell, -1 if not listed
+  int *cell_cnt = nullptr;          // per cell: members (counted, then used as a fill cursor)
+  int *cell_start = nullptr;        // per cell: first entry in cell_items (exclusive sum, n_cells + 1)
+  int *cell_items = nullptr;        // slots grouped by cell
+  bool any_cells = false;
+};
+
+// A system's cell grid over its box [-L/2, L/2)^3 (points outside are clamped to the edge
+// cells): nc[a] cells of width L[a]/nc[a] >= wmin along axis a, cells numbered from base.
+struct CellGrid {
+  double inv_w[3], half[3];
+  double wmin;
+  int nc[3];
+  long long base;
 };
 
 namespace {
@@ -196,8 +217,110 @@ __device__ void norm_tanf(const State &S, int g, double t[3]) {  // general.f90:
   for (int c = 0; c < 3; ++c) t[c] = e_div(t[c], len);
 }
 
+// ---- pclose on a cell list -------------------------------------------------------------------
+// The reference's pclose (line.f90:135-160) is the exact nearest live non-neighbour by the
+// non-periodic distance, the first j in ascending order among equal distances (strict <), and
+// it leaves closest alone when no j comes below 100.  The cell list finds the same point: the
+// target searches rings of cells around its own (Chebyshev ring r), keeps the minimum of
+// (distance, slot) -- the lowest slot among equal distances, whatever the visiting order -- and
+// stops once that distance is below r * wmin: every point outside rings 0..r lies in a cell at
+// least r+1 cells away along some axis, so at least r whole cell widths away.  (A point within
+// rounding of a cell face may be filed one cell off; the stop test keeps a relative margin of
+// 1e-10, far above that rounding.)
+__device__ __forceinline__ int cell_coord(const CellGrid &G, int a, double x) {
+  const double f = (x + G.half[a]) * G.inv_w[a];
+  int c = f < 0. ? 0 : (int)f;
+  return c >= G.nc[a] ? G.nc[a] - 1 : c;
+}
+
+__global__ void k_cell_count(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn,
+                             const int *__restrict__ sys_of, const CellGrid *__restrict__ grid,
+                             const double *__restrict__ X, const int *__restrict__ nxt, int *__restrict__ cell_of,
+                             int *__restrict__ cnt, long long T, const unsigned *err) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= T) return;
+  int c = -1;
+  const int s = sys_of[g];
+  const SysConst &sc = scs[s];
+  const CellGrid &G = grid[s];
+  const int k = (int)(g - sc.base);
+  if (!*err && G.nc[0] > 0 && recon_step(sc, dyn[s]) && k >= 1 && k <= dyn[s].pcount && nxt[g] != 0) {
+    double x[3];
+    load3(X, T, (int)g, x);
+    c = (int)(G.base + ((long long)cell_coord(G, 2, x[2]) * G.nc[1] + cell_coord(G, 1, x[1])) * G.nc[0] +
+              cell_coord(G, 0, x[0]));
+    atomicAdd(&cnt[c], 1);
+  }
+  cell_of[g] = c;
+}
+
+// Files each listed slot into its cell (the order inside a cell does not matter: the search
+// takes the minimum of (distance, slot)).
+__global__ void k_cell_fill(const int *__restrict__ cell_of, const int *__restrict__ start, int *__restrict__ cnt,
+                            int *__restrict__ items, long long T) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= T) return;
+  const int c = cell_of[g];
+  if (c < 0) return;
+  items[start[c] + atomicSub(&cnt[c], 1) - 1] = (int)g;
+}
+
+__global__ void k_pclose_cells(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn,
+                               const int *__restrict__ sys_of, const CellGrid *__restrict__ grid,
+                               const double *__restrict__ X, const int *__restrict__ nxt, const int *__restrict__ prv,
+                               const int *__restrict__ cell_of, const int *__restrict__ start,
+                               const int *__restrict__ items, int *__restrict__ cl, double *__restrict__ CD,
+                               long long T) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= T || cell_of[g] < 0) return;  // listed: live slot of a cell-list system on a recon step
+  const int s = sys_of[g];
+  const CellGrid &G = grid[s];
+  const int ni = nxt[g], pi = prv[g];
+  double xi[3];
+  load3(X, T, (int)g, xi);
+  const int cx = cell_coord(G, 0, xi[0]), cy = cell_coord(G, 1, xi[1]), cz = cell_coord(G, 2, xi[2]);
+  const int rmax = max(max(G.nc[0], G.nc[1]), G.nc[2]) - 1;
+  bool found = false;
+  double best = 100.;
+  int bj = cl[g];
+  for (int r = 0; r <= rmax; ++r) {
+    for (int dz = -r; dz <= r; ++dz) {
+      const int z = cz + dz;
+      if (z < 0 || z >= G.nc[2]) continue;
+      for (int dy = -r; dy <= r; ++dy) {
+        const int y = cy + dy;
+        if (y < 0 || y >= G.nc[1]) continue;
+        const bool shell = dz == -r || dz == r || dy == -r || dy == r;
+        for (int dx = -r; dx <= r; dx += (shell || r == 0) ? 1 : 2 * r) {  // interior rows: the two end cells
+          const int x = cx + dx;
+          if (x < 0 || x >= G.nc[0]) continue;
+          const long long c = G.base + ((long long)z * G.nc[1] + y) * G.nc[0] + x;
+          for (int e = start[c]; e < start[c + 1]; ++e) {
+            const int j = items[e];
+            if (j == g || j == ni || j == pi) continue;
+            double xj[3];
+            load3(X, T, j, xj);
+            const double d2 =
+                e_add(e_add(e_sq(e_sub(xi[0], xj[0])), e_sq(e_sub(xi[1], xj[1]))), e_sq(e_sub(xi[2], xj[2])));
+            const double dist = e_sqrt(d2);
+            if (found ? (dist < best || (dist == best && j < bj)) : dist < best) {
+              best = dist;
+              bj = j;
+              found = true;
+            }
+          }
+        }
+      }
+    }
+    if (found && best < (double)r * G.wmin * (1. - 1e-10)) break;
+  }
+  cl[g] = bj;
+  CD[g] = best;
+}
+
 // pclose (line.f90:135-160): exact nearest non-neighbour, non-periodic distance, strict <
-// so ties keep the lowest j.  One thread per target slot.
+// so ties keep the lowest j.  One thread per target slot, every slot scanned: kept as the
+// method to compare the cell list with (nv_set_pclose_method).
 __global__ void k_pclose_brute(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn,
                                const int *__restrict__ sys_of, const double *__restrict__ X,
                                const int *__restrict__ nxt, const int *__restrict__ prv, int *__restrict__ cl,
@@ -1615,7 +1738,40 @@ void topo_alloc(nv_handle *h) {
   cudaMalloc(&tb->pos_h, n * sizeof(int));
   cudaMalloc(&tb->l0, (n / 32 + 2) * sizeof(unsigned));
   cudaMalloc(&tb->l1, (n / 1024 + 2) * sizeof(unsigned));
-  cub::DeviceScan::ExclusiveSum(nullptr, tb->cub_bytes, tb->flag_a, tb->pos_a, (int)n);
+  // cell grids of the systems without a tree: about two slots per cell at full capacity,
+  // cells at least as wide as delta/2 and at most 256 per axis
+  std::vector<CellGrid> grids(h->nsys);
+  long long cells = 0;
+  for (int s = 0; s < h->nsys; ++s) {
+    CellGrid &G = grids[s];
+    std::memset(&G, 0, sizeof G);
+    const SysConst &sc = h->sc[s];
+    if (sc.use_tree) continue;
+    const double vol = sc.box[0] * sc.box[1] * sc.box[2];
+    const double w = std::max(std::cbrt(vol * 2.0 / std::max(h->cap[s], 1)), 0.5 * sc.delta);
+    G.wmin = 1e300;
+    for (int a = 0; a < 3; ++a) {
+      G.nc[a] = (int)std::min(256.0, std::max(1.0, std::floor(sc.box[a] / w)));
+      G.inv_w[a] = G.nc[a] / sc.box[a];
+      G.half[a] = sc.box[a] / 2;
+      G.wmin = std::min(G.wmin, sc.box[a] / G.nc[a]);
+    }
+    G.base = cells;
+    cells += (long long)G.nc[0] * G.nc[1] * G.nc[2];
+  }
+  tb->n_cells = cells;
+  tb->any_cells = cells > 0 && cells < (1LL << 30);
+  size_t scan_n = n;
+  if (tb->any_cells) {
+    cudaMalloc(&tb->grid, h->nsys * sizeof(CellGrid));
+    cudaMemcpy(tb->grid, grids.data(), h->nsys * sizeof(CellGrid), cudaMemcpyHostToDevice);
+    cudaMalloc(&tb->cell_of, n * sizeof(int));
+    cudaMalloc(&tb->cell_cnt, (cells + 1) * sizeof(int));
+    cudaMalloc(&tb->cell_start, (cells + 1) * sizeof(int));
+    cudaMalloc(&tb->cell_items, n * sizeof(int));
+    scan_n = std::max(scan_n, (size_t)cells + 1);
+  }
+  cub::DeviceScan::ExclusiveSum(nullptr, tb->cub_bytes, tb->flag_a, tb->pos_a, (int)scan_n);
   cudaMalloc(&tb->cub_tmp, std::max<size_t>(tb->cub_bytes, 16));
   h->topo = tb;
 }
@@ -1629,6 +1785,8 @@ void topo_free(nv_handle *h) {
   cudaFree(tb->dec); cudaFree(tb->newslot); cudaFree(tb->xnew);
   cudaFree(tb->unew); cudaFree(tb->segnx); cudaFree(tb->fh[0]); cudaFree(tb->fh[1]); cudaFree(tb->pos_h);
   cudaFree(tb->l0); cudaFree(tb->l1);
+  cudaFree(tb->grid); cudaFree(tb->cell_of); cudaFree(tb->cell_cnt); cudaFree(tb->cell_start);
+  cudaFree(tb->cell_items);
   cudaFree(tb->cub_tmp);
   delete tb;
   h->topo = nullptr;
@@ -1696,9 +1854,23 @@ void launch_pinsert(nv_handle *h) {
 void launch_pclose(nv_handle *h, bool only_brute) {
   bool any_brute = false, any_tree = false;
   for (auto &s : h->sc) (s.use_tree ? any_tree : any_brute) = true;
-  if (any_brute)
+  TopoBuffers *tb = h->topo;
+  if (any_brute && (h->pclose_method == 1 || !tb->any_cells)) {
     k_pclose_brute<<<grid_for(h->T, 128), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->nxt, h->prv,
                                                                h->closest, h->closestd, h->T, h->d_err);
+  } else if (any_brute) {
+    const long long T = h->T;
+    cudaMemsetAsync(tb->cell_cnt, 0, (tb->n_cells + 1) * sizeof(int), h->stream);
+    k_cell_count<<<grid_for(T, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, tb->grid, h->x, h->nxt,
+                                                        tb->cell_of, tb->cell_cnt, T, h->d_err);
+    size_t bytes = tb->cub_bytes;
+    cub::DeviceScan::ExclusiveSum(tb->cub_tmp, bytes, tb->cell_cnt, tb->cell_start, (int)(tb->n_cells + 1),
+                                  h->stream);
+    k_cell_fill<<<grid_for(T, TB), TB, 0, h->stream>>>(tb->cell_of, tb->cell_start, tb->cell_cnt, tb->cell_items, T);
+    k_pclose_cells<<<grid_for(T, 128), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, tb->grid, h->x, h->nxt,
+                                                            h->prv, tb->cell_of, tb->cell_start, tb->cell_items,
+                                                            h->closest, h->closestd, T);
+  }
   if (any_tree && !only_brute) launch_closest_tree(h);
 }
 

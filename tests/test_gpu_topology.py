@@ -207,3 +207,85 @@ def test_pinsert_interleaved_free_slots_second_order(iters):
     assert ea == eb
     _assert_same(a, b)
     assert ca.insert_count == cb.insert_count and ca.pcount == cb.pcount
+
+
+def _pclose_both(p, st, itime=1):
+    """closest/closestd after the pclose stage: cell list, every-slot scan, oracle."""
+    from nuvort_b200.api import Handle
+    out = []
+    for method in (0, 1):
+        with Handle(p, [st.pcount + 64], states=[st]) as h:
+            h.set_pclose_method(method)
+            h.set_clock(0, 0.0, itime)
+            h.stage("pclose")
+            out.append(h.download())
+    o = Oracle(p, st, t=0.0, itime=itime)
+    o.stage("pclose")
+    out.append(o.download())
+    return out
+
+
+def _assert_same_closest(states):
+    a, b, c = states
+    for name in ("closest", "closestd"):
+        assert np.array_equal(getattr(a, name), getattr(c, name)), name
+        assert np.array_equal(getattr(b, name), getattr(c, name)), name
+
+
+def test_pclose_cell_list_32k_bs():
+    # a 32,768-point direct-sum tangle: the cell list, the every-slot scan and the oracle
+    # give the same nearest non-neighbour and distance for every point
+    st = tangle(1, 0.001, n_points=32768)
+    st.closest = np.arange(1, st.pcount + 1, dtype=np.int32)[::-1].copy()  # stale values must be replaced
+    st.closestd = np.zeros(st.pcount)
+    p = config0_params(delta=0.001, dt=5e-6)
+    _assert_same_closest(_pclose_both(p, st))
+
+
+def test_pclose_cell_list_ties_outside_points_and_no_candidate():
+    # squares of 8 points on a 2^-9 cm lattice: many exactly equal distances, so the lowest
+    # slot must win; some squares lie partly outside the box (clamped to the edge cells); a
+    # small triangle sits far from everything else (a long ring search)
+    h9 = 2.0 ** -9
+    rng = np.random.default_rng(5)
+    xs, nx, pv = [], [], []
+    base = 0
+    for q in range(60):
+        c = rng.integers(-27, 27, 3) * h9
+        if q % 10 == 0:
+            c[q % 3] = 0.05 + 2 * h9  # beyond the upper face
+        ring = [(-1, -1), (0, -1), (1, -1), (1, 0), (1, 1), (0, 1), (-1, 1), (-1, 0)]
+        ax = q % 3
+        for (u, v) in ring:
+            pt = c.copy()
+            pt[(ax + 1) % 3] += u * h9
+            pt[(ax + 2) % 3] += v * h9
+            xs.append(pt)
+        n = len(ring)
+        nx += [base + (k + 1) % n + 1 for k in range(n)]
+        pv += [base + (k - 1) % n + 1 for k in range(n)]
+        base += n
+    far = np.array([[0.04, 0.04, 0.04], [0.04 + h9, 0.04, 0.04], [0.04, 0.04 + h9, 0.04]])
+    xs += list(far)
+    nx += [base + 2, base + 3, base + 1]
+    pv += [base + 3, base + 1, base + 2]
+    x = np.ascontiguousarray(np.array(xs))
+    N = len(x)
+    st = State(x=x, infront=np.array(nx, np.int32), behind=np.array(pv, np.int32),
+               closest=np.full(N, 7, np.int32), closestd=np.zeros(N))
+    p = config0_params(delta=0.002)
+    res = _pclose_both(p, st)
+    _assert_same_closest(res)
+    c = res[2]
+    assert np.any(c.closestd[:-3] == h9)  # ties exist
+    assert np.all(c.closestd < 100)  # the triangle's points find the nearest square point
+
+
+def test_pclose_no_candidate_keeps_closest():
+    # one 3-point loop alone: every other slot is itself or a neighbour
+    x = np.array([[0.0, 0.0, 0.0], [0.001, 0.0, 0.0], [0.0, 0.001, 0.0]])
+    st = State(x=x, infront=np.array([2, 3, 1], np.int32), behind=np.array([3, 1, 2], np.int32),
+               closest=np.array([3, 1, 2], np.int32), closestd=np.zeros(3))
+    a, b, c = _pclose_both(config0_params(), st)
+    _assert_same_closest((a, b, c))
+    assert np.all(c.closestd == 100.0) and np.array_equal(c.closest, [3, 1, 2])
