@@ -220,11 +220,14 @@ int nv_stage_times(nv_handle *h, double *ms, int32_t n);
  * pairs of the direct sum) are evaluated in FP64; the rest in FP32, except interactions that
  * are ill-conditioned in FP32 (checked per interaction), which also run in FP64.  Default 2. */
 int nv_set_near_factor(nv_handle *h, double factor);
-/* Mixed precision: a far term runs in FP64 instead of FP32 when FP32 would cancel digits:
- * |r||e| + r.e < angle |r||e|, |r x circ|^2 < line |circ|^2 min(|r|^2,|e|^2) or
- * |e|^2 < end max(|r|^2,|circ|^2) (r, e: target to the segment's ends).  Defaults 0.1,
- * 1e-3, 1e-2 (mixed vs FP64 velocity within 1e-7 RMS on the benchmark tangles); smaller
- * values trade accuracy for speed.  angle must be at least 1e-3. */
+/* Mixed precision: a far term runs in FP64 instead of FP32 when FP32 would lose digits:
+ * |r||e| + r.e < angle |r||e| (the segment subtends nearly 180 degrees at the target),
+ * |r x circ|^2 < line |circ|^2 min(|r|^2,|e|^2) (the target near the segment's line) or
+ * |e|^2 < end max(|r|^2,|circ|^2) (near its far end), r, e: target to the segment's ends.
+ * Defaults 0.1, 1e-3, 1e-2 (mixed vs FP64 velocity within 1e-7 RMS on the benchmark
+ * tangles); smaller values trade accuracy for speed (angle 0 turns that guard off).  line
+ * must be at least 1e-9: it also keeps the FP32 term away from its singularity (a target on
+ * the segment). */
 int nv_set_fp32_guards(nv_handle *h, double angle, double line, double end);
 /* pinsert places the insertions of new points that the sweep reaches again by a fixed-point
  * iteration (default 6 rounds); a system that has not converged runs the serial sweep.

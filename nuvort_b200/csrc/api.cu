@@ -812,9 +812,9 @@ int nv_set_near_factor(nv_handle *h, double factor) {
 }
 
 int nv_set_fp32_guards(nv_handle *h, double angle, double line, double end) {
-  if (!h || !(angle >= 1e-3 && angle <= 2) || !(line >= 0 && line <= 1) || !(end >= 0 && end <= 1))
-    return set_error(NV_ERR_ARG, "nv_set_fp32_guards: angle in [1e-3,2] (it also keeps the FP32 "
-                                 "term away from its singularity), line and end in [0,1]");
+  if (!h || !(angle >= 0 && angle <= 2) || !(line >= 1e-9 && line <= 1) || !(end >= 0 && end <= 1))
+    return set_error(NV_ERR_ARG, "nv_set_fp32_guards: angle in [0,2], line in [1e-9,1] (it also keeps the "
+                                 "FP32 term away from its singularity, a target on the segment), end in [0,1]");
   h->guards.angle = (float)angle;
   h->guards.line = (float)line;
   h->guards.end = (float)end;

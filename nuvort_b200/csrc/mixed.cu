@@ -61,10 +61,10 @@ __global__ void __launch_bounds__(kTB) k_direct_mixed(const SysConst *__restrict
     th[c] = (float)t;
     tl[c] = (float)(t - (double)th[c]);
   }
-  const float gq = (float)(sc.quant_circ / (4.0 * NV_PI));
+  const double gq64 = sc.quant_circ / (4.0 * NV_PI);
+  const float gq = (float)gq64;
   const double nr = near_factor * sc.delta;
   const float near2 = (float)(nr * nr);
-  const double qc = sc.quant_circ, two_pi = sc.two_pi;
 
   const int nt = (pc + TJ - 1) / TJ;
   auto issue = [&](int t) {
@@ -116,8 +116,11 @@ __global__ void __launch_bounds__(kTB) k_direct_mixed(const SysConst *__restrict
             const float re = fmaf(rx, ex, fmaf(ry, ey, rz * ez));
             const float r1 = a * rsqrtf(a), r2 = ee * rsqrtf(ee);
             const float pp = r1 * r2;
-            if (!(pp + re < gd.angle * pp || cr2 < gd.line * D.w * fminf(a, ee) || ee < gd.end * fmaxf(a, D.w))) {
-              const float f = __fdividef(gq * (r1 + r2), pp * (pp + re));  // MUFU reciprocal
+            if (!(cr2 < gd.line * D.w * fminf(a, ee) || ee < gd.end * fmaxf(a, D.w) || pp + re < gd.angle * pp)) {
+              // pp + r.e = |r x d|^2 / (pp - r.e) when r.e < 0: no cancellation either way
+              const bool obtuse = re < 0.f;
+              const float num = gq * (r1 + r2) * (obtuse ? pp - re : 1.f);
+              const float f = __fdividef(num, pp * (obtuse ? cr2 : pp + re));  // MUFU reciprocal
               ux = fmaf(f, crx, ux);
               uy = fmaf(f, cry, uy);
               uz = fmaf(f, crz, uz);
@@ -125,8 +128,9 @@ __global__ void __launch_bounds__(kTB) k_direct_mixed(const SysConst *__restrict
             }
           }
           {
-            // near field and ill-conditioned pairs: the reference expression in FP64
-            // (timestep.f90:162-170, 188-196) from the FP64 segment records
+            // near field and ill-conditioned pairs in FP64 from the FP64 segment records: the
+            // reference's skip decision (4ac - b^2 == 0, timestep.f90:166,192) in its own
+            // arithmetic, the value from the cancellation-free form
             const double4 A = seg64[2 * (long long)gj], B = seg64[2 * (long long)gj + 1];
             double r[3];
             if (m == 0) {
@@ -138,8 +142,10 @@ __global__ void __launch_bounds__(kTB) k_direct_mixed(const SysConst *__restrict
             }
             const double d[3] = {B.x, B.y, B.z};
             const double aa = e_add(e_add(e_sq(r[0]), e_sq(r[1])), e_sq(r[2]));
-            double tm[3];
-            if (bs_term_exact(r, d, aa, B.w, qc, two_pi, tm)) {
+            const double bb = e_mul(2.0, dot3(r, d));
+            if (e_sub(e_mul(e_mul(4.0, aa), B.w), e_mul(bb, bb)) != 0.0) {
+              double tm[3];
+              term64_stable(r, d, aa, gq64, tm);
               nx += tm[0];
               ny += tm[1];
               nz += tm[2];

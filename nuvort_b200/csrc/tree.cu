@@ -1268,7 +1268,8 @@ __global__ void __launch_bounds__(128, kSplit ? 8 : 9) k_tree_walk_mixed(const S
     pi_ = prv[g];
   }
   const float near2 = (float)(near_factor * sc.delta * near_factor * sc.delta);
-  const float gq = (float)(sc.quant_circ / (4.0 * NV_PI));
+  const double gq64 = sc.quant_circ / (4.0 * NV_PI);
+  const float gq = (float)gq64;
   const bool second = sc.tree_extra_correction && sc.tree_theta > 1.1547;
   float fx = 0, fy = 0, fz = 0;  // FP32 partial over at most kFlush far interactions
   // FP64: near field plus the flushed FP32 partials (touched only at a flush or an FP64 term)
@@ -1291,7 +1292,8 @@ __global__ void __launch_bounds__(128, kSplit ? 8 : 9) k_tree_walk_mixed(const S
     r[2] = e_sub(e_add(C.z, s2), xi[2]);
     return e_add(e_add(e_sq(r[0]), e_sq(r[1])), e_sq(r[2]));
   };
-  // FP64 evaluation of an accepted node (tree.f90:289-307)
+  // FP64 evaluation of an accepted node: the reference's singularity check and skip decision
+  // in its own arithmetic (tree.f90:289-303), the value from the cancellation-free form
   auto exact_term = [&](int cur) {
     double r[3];
     const double d2 = exact_r(cur, r);
@@ -1307,14 +1309,11 @@ __global__ void __launch_bounds__(128, kSplit ? 8 : 9) k_tree_walk_mixed(const S
     const double c = dot3(circ, circ);
     const double D = e_sub(e_mul(e_mul(4.0, a), c), e_mul(b, b));
     if (D < NV_EPS) return;
-    double cr[3];
-    cross3(r, circ, cr);
-    const double qc = sc.quant_circ;
-    const double den = e_mul(sc.two_pi, D);
-    const double fac = e_sub(e_div(e_add(e_mul(2.0, c), b), e_sqrt(e_add(e_add(a, b), c))), e_div(b, e_sqrt(a)));
-    nx += e_mul(e_div(e_mul(cr[0], qc), den), fac);
-    ny += e_mul(e_div(e_mul(cr[1], qc), den), fac);
-    nz += e_mul(e_div(e_mul(cr[2], qc), den), fac);
+    double tm[3];
+    term64_stable(r, circ, d2, gq64, tm);
+    nx += tm[0];
+    ny += tm[1];
+    nz += tm[2];
     ++evals;
     ++n64;
   };
@@ -1408,14 +1407,16 @@ __global__ void __launch_bounds__(128, kSplit ? 8 : 9) k_tree_walk_mixed(const S
             // ia = 1/|r|, ib = 1/|r + circ|; pp = |r||r + circ|
             const float ia = rsqrtf(d2), ib = rsqrtf(ee);
             const float pp = (d2 * ia) * (ee * ib);
-            const float den = pp + re;
-            if (den < gd.angle * pp || cr2 < Q.w * fminf(d2, ee) || ee < gd.end * fmaxf(d2, B.w)) {
-              // the segment subtends more than 120 degrees at the target, the target lies
-              // near its line or near its far end: FP32 would cancel digits there
+            if (cr2 < Q.w * fminf(d2, ee) || ee < gd.end * fmaxf(d2, B.w) || pp + re < gd.angle * pp) {
+              // the target lies near the segment's line or near its far end (or the optional
+              // angle guard): FP32 would cancel digits there
               exact_term(cur);
             } else {
-              // (|r| + |r+circ|) / (pp (pp + r.(r+circ))) = (ia + ib) / (pp + r.(r+circ))
-              const float f = __fdividef(gq * (ia + ib), den);  // MUFU reciprocal
+              // (|r| + |e|) / (pp (pp + r.e)) = (ia + ib) / (pp + r.e), e = r + circ, with
+              // pp + r.e = |r x circ|^2 / (pp - r.e) when r.e < 0 (no cancellation either way)
+              const bool obtuse = re < 0.f;
+              const float num = gq * (ia + ib) * (obtuse ? pp - re : 1.f);
+              const float f = __fdividef(num, obtuse ? cr2 : pp + re);  // MUFU reciprocal
               fx = fmaf(f, cx, fx);
               fy = fmaf(f, cy, fy);
               fz = fmaf(f, cz, fz);

@@ -134,3 +134,28 @@ def test_walk_parts_argument_checked():
         for bad in (-1, 3, 16):
             with pytest.raises(NuvortError):
                 h.set_walk_parts(bad)
+
+
+def test_fp64_stable_form_matches_reference_arithmetic():
+    # With a near radius beyond the box every pair of the mixed direct sum takes the FP64
+    # path: the reference's skip decision, the value from the cancellation-free form with
+    # reciprocals and reciprocal square roots by Newton's iteration.  Its error bound: a few
+    # FP64 roundings per term, so every point agrees with the plain path to 1e-13 relative.
+    from helpers import rel_err
+    from nuvort_b200.api import Handle
+    st = tangle(1, 0.001, n_points=2048)
+    up, _ = _vel(config1_params("BS", precision="fp64"), st)
+    with Handle(config1_params("BS", precision="mixed"), [st.pcount + 64], states=[st]) as h:
+        h.set_near_factor(1e9)
+        um = h.calc_velocity()
+    assert rel_err(um, up).max() <= 1e-13
+
+
+def test_fp32_guard_arguments():
+    from nuvort_b200.api import Handle, NuvortError
+    st = tangle(1, 0.001, n_points=1024)
+    with Handle(config1_params("Tree", precision="mixed"), [st.pcount + 64], states=[st]) as h:
+        h.set_fp32_guards(0.0, 1e-3, 1e-2)  # the angle guard may be off
+        for bad in ((-0.1, 1e-3, 1e-2), (0.1, 0.0, 1e-2), (0.1, 1e-3, 2.0)):
+            with pytest.raises(NuvortError):
+                h.set_fp32_guards(*bad)
