@@ -307,6 +307,82 @@ int nv_calc_velocity_bs_static(const nv_params *p, int32_t pcount, const double 
                                const int32_t *d_infront, const int32_t *d_behind, double t,
                                double *d_u3, void *stream);
 
+/* ---- diagnostics, snapshots and restart files (src/diagnostic.f90, src/output.f90) ----- */
+/* One row of data/ts.log (print_info, src/output.f90:20-44) and the values behind it.  The
+ * velocity and curvature figures come from the last nv_calculate_diagnostics, avg_sep and
+ * total_length from the last pinsert, the counters from the system's state. */
+typedef struct nv_ts_row {
+  int32_t itime;             /* step of the row (ts.log prints itime/shots)                    */
+  int32_t live;              /* count(f(:)%infront>0)                                          */
+  int32_t recon_count;
+  int32_t wall_recon_count;  /* always 0: no solid walls here                                  */
+  int32_t remove_count;
+  int32_t reserved;
+  int64_t tree_eval;         /* accepted tree interactions of the last velocity pass (the
+                                reference's counter is a default integer and wraps past 2^31) */
+  double t;
+  double delta;
+  double avg_sep;            /* pinsert's average separation (ts.log prints avg_sep/delta)      */
+  double total_length;       /* pinsert's summed segment length                                */
+  double maxu, maxdu;        /* velocity_info: max |u|, max |u1 - u2| over every slot            */
+  double mean_u_sup, mean_u_mf; /* velocity_info: sums of |u_sup|, |u_mf| over every slot / live */
+  double kappa_bar, kappa_min, kappa_max; /* curv_info (kappa_min: huge(0.) if no curvature > 0) */
+} nv_ts_row;
+
+/* calculate_diagnostics (src/diagnostic.f90:9-74) for every system: ghostp, then
+ * velocity_info, curv_info and stretching_rate as device reductions; the per-point curvature
+ * and stretching are kept for snapshots.  The reference calls it when mod(itime,shots)==0;
+ * the caller decides when.  Sums run in a fixed parallel order (within ~1e-13 relative of the
+ * reference's sequential sums); maxima and minima are exact. */
+int nv_calculate_diagnostics(nv_handle *h);
+/* The ts.log row of system sys (NV_ERR_STATE before the first nv_calculate_diagnostics). */
+int nv_ts_row_get(nv_handle *h, int32_t sys, nv_ts_row *row);
+/* The row as print_info writes it to data/ts.log, format
+ * (i6.4,f13.7,i10.1,i13.1,i13.1,f7.4,f13.6,f13.5,f13.5,f10.2,i13.1,i13.1) with itime/shots,
+ * t, live, recon_count, wall_recon_count, avg_sep/delta, total_length, maxu, maxdu,
+ * kappa_bar, remove_count, tree_eval; no newline.  cap: size of buf. */
+int nv_format_ts_row(const nv_ts_row *row, int32_t shots, char *buf, int32_t cap);
+
+/* Every field of type(qvort) (src/cdata.f90:19-31) that this library keeps, for file I/O:
+ * point-major 3-vectors as in nv_host_state.  The pinning fields (wpinned, pinnedi, pinnedb)
+ * are always zero and .false. here (no solid walls). */
+typedef struct nv_full_state {
+  int32_t pcount;
+  double *x, *u, *u1, *u2, *u_mf, *u_sup;  /* [3*pcount]                               */
+  double *curv, *stretch;                  /* [pcount]                                 */
+  double *ghosti, *ghostb;                 /* [3*pcount]                               */
+  int32_t *infront, *behind, *closest;     /* [pcount]                                 */
+  double *closestd;                        /* [pcount]                                 */
+} nv_full_state;
+
+/* Every field of system sys (u_sup and u_mf of its last velocity pass, curv and stretch of
+ * its last diagnostics); arrays of at least cap slots; st->pcount receives pcount. */
+int nv_download_full(nv_handle *h, int32_t sys, nv_full_state *st, int32_t cap);
+/* nv_upload plus u_sup, u_mf, curv and stretch (NULL: zero). */
+int nv_upload_full(nv_handle *h, int32_t sys, const nv_full_state *st);
+
+/* printf (src/output.f90:47-70): the stream file data/var%04d.log that the MATLAB tools read
+ * (bin/vortex/vortex_load.m): t, pcount, x(1..3), infront, u(1..3), u_mf(1..3), curv,
+ * stretch, each over all pcount slots, little-endian, no record markers. */
+int nv_write_snapshot(nv_handle *h, int32_t sys, const char *path);
+/* data_dump (src/output.f90:85-94): data/var.dat as gfortran's unformatted sequential write
+ * of pcount, recon_count, itime, t and f, each a record framed by 4-byte length markers; f
+ * holds pcount type(qvort) records of 248 bytes (reals 8, integers and logicals 4).  Files
+ * whose f record would exceed 2^31-1 bytes (8.6M points) are refused (NV_ERR_UNSUPPORTED). */
+int nv_write_dump(nv_handle *h, int32_t sys, const char *path);
+/* data_restore (src/initial.f90:151-166): reads a var.dat into system sys (state, t, itime,
+ * recon_count); the next step is itime+1.  NV_ERR_IO if the file cannot be read or is not such
+ * a file, NV_ERR_CAPACITY if its pcount exceeds the system's capacity, NV_ERR_UNSUPPORTED if
+ * it holds pinned points. */
+int nv_restore_dump(nv_handle *h, int32_t sys, const char *path);
+/* The same formats between host arrays and files, without a handle or a GPU. */
+int nv_snapshot_write_file(const nv_full_state *st, double t, const char *path);
+int nv_dump_write_file(const nv_full_state *st, int32_t recon_count, int32_t itime, double t, const char *path);
+/* Reads a var.dat: *pcount_out receives its pcount; the arrays of st (NULL to skip one) are
+ * filled when they hold at least cap >= pcount slots (else NV_ERR_ARG after setting the count). */
+int nv_dump_read_file(const char *path, nv_full_state *st, int32_t cap, int32_t *pcount_out, int32_t *recon_count,
+                      int32_t *itime, double *t);
+
 /* Diagnostic counters of system sys for the last step, for profiling the topology stages:
  * [0] pinsert candidates, [1] insertions, [2] steps that needed the serial pinsert sweep
  * (cumulative), [3] precon candidates, [4] premove candidates, [5] insertions made by new

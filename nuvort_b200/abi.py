@@ -86,6 +86,54 @@ class NvHostState(C.Structure):
     ]
 
 
+class NvFullState(C.Structure):
+    """nv_full_state: every kept field of type(qvort) (file I/O)."""
+    _fields_ = [
+        ("pcount", C.c_int32),
+        ("x", C.POINTER(C.c_double)),
+        ("u", C.POINTER(C.c_double)),
+        ("u1", C.POINTER(C.c_double)),
+        ("u2", C.POINTER(C.c_double)),
+        ("u_mf", C.POINTER(C.c_double)),
+        ("u_sup", C.POINTER(C.c_double)),
+        ("curv", C.POINTER(C.c_double)),
+        ("stretch", C.POINTER(C.c_double)),
+        ("ghosti", C.POINTER(C.c_double)),
+        ("ghostb", C.POINTER(C.c_double)),
+        ("infront", C.POINTER(C.c_int32)),
+        ("behind", C.POINTER(C.c_int32)),
+        ("closest", C.POINTER(C.c_int32)),
+        ("closestd", C.POINTER(C.c_double)),
+    ]
+
+
+class NvTsRow(C.Structure):
+    """nv_ts_row: one data/ts.log row (print_info) and the values behind it."""
+    _fields_ = [
+        ("itime", C.c_int32),
+        ("live", C.c_int32),
+        ("recon_count", C.c_int32),
+        ("wall_recon_count", C.c_int32),
+        ("remove_count", C.c_int32),
+        ("reserved", C.c_int32),
+        ("tree_eval", C.c_int64),
+        ("t", C.c_double),
+        ("delta", C.c_double),
+        ("avg_sep", C.c_double),
+        ("total_length", C.c_double),
+        ("maxu", C.c_double),
+        ("maxdu", C.c_double),
+        ("mean_u_sup", C.c_double),
+        ("mean_u_mf", C.c_double),
+        ("kappa_bar", C.c_double),
+        ("kappa_min", C.c_double),
+        ("kappa_max", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+
+
 class NvEvent(C.Structure):
     _fields_ = [("itime", C.c_int32), ("kind", C.c_int32), ("i", C.c_int32), ("j", C.c_int32)]
 
@@ -208,6 +256,11 @@ class State:
     ghostb: Optional[np.ndarray] = None
     closest: Optional[np.ndarray] = None
     closestd: Optional[np.ndarray] = None
+    # fields only the diagnostics and the files use: f(:)%u_mf, u_sup (n, 3), curv, stretch (n,)
+    u_mf: Optional[np.ndarray] = None
+    u_sup: Optional[np.ndarray] = None
+    curv: Optional[np.ndarray] = None
+    stretch: Optional[np.ndarray] = None
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -221,17 +274,37 @@ class State:
                      u=z3(), u1=z3(), u2=z3(), ghosti=z3(), ghostb=z3(),
                      closest=np.zeros(cap, np.int32), closestd=np.zeros(cap, np.float64))
 
+    @staticmethod
+    def empty_full(cap: int) -> "State":
+        st = State.empty(cap)
+        st.u_mf = np.zeros((cap, 3), np.float64)
+        st.u_sup = np.zeros((cap, 3), np.float64)
+        st.curv = np.zeros(cap, np.float64)
+        st.stretch = np.zeros(cap, np.float64)
+        return st
+
     def copy(self) -> "State":
         cp = lambda a: None if a is None else np.array(a, copy=True)
-        return State(x=cp(self.x), infront=cp(self.infront), behind=cp(self.behind), u=cp(self.u),
-                     u1=cp(self.u1), u2=cp(self.u2), ghosti=cp(self.ghosti), ghostb=cp(self.ghostb),
-                     closest=cp(self.closest), closestd=cp(self.closestd))
+        return State(**{f: cp(getattr(self, f)) for f in FIELDS})
 
     def trimmed(self, n: int) -> "State":
         cut = lambda a: None if a is None else np.ascontiguousarray(a[:n])
-        return State(x=cut(self.x), infront=cut(self.infront), behind=cut(self.behind), u=cut(self.u),
-                     u1=cut(self.u1), u2=cut(self.u2), ghosti=cut(self.ghosti), ghostb=cut(self.ghostb),
-                     closest=cut(self.closest), closestd=cut(self.closestd))
+        return State(**{f: cut(getattr(self, f)) for f in FIELDS})
+
+    def to_full_c(self) -> NvFullState:
+        """nv_full_state over this state's arrays (float64 / int32, made contiguous)."""
+        self.to_c()
+        for name in ("u_mf", "u_sup", "curv", "stretch"):
+            a = getattr(self, name)
+            if a is not None:
+                setattr(self, name, np.ascontiguousarray(a, dtype=np.float64))
+        s = NvFullState()
+        s.pcount = self.pcount
+        for name in ("x", "u", "u1", "u2", "u_mf", "u_sup", "curv", "stretch", "ghosti", "ghostb", "closestd"):
+            setattr(s, name, _dptr(getattr(self, name)))
+        for name in ("infront", "behind", "closest"):
+            setattr(s, name, _iptr(getattr(self, name)))
+        return s
 
     def to_c(self) -> NvHostState:
         for name in ("x", "u", "u1", "u2", "ghosti", "ghostb", "closestd"):
@@ -259,6 +332,10 @@ class State:
     @property
     def live(self) -> np.ndarray:
         return self.infront > 0
+
+
+FIELDS = ("x", "infront", "behind", "u", "u1", "u2", "ghosti", "ghostb", "closest", "closestd", "u_mf", "u_sup",
+          "curv", "stretch")
 
 
 TREE_NODE_DTYPE = np.dtype([("pos", "<f8", 3), ("width", "<f8"), ("cent", "<f8", 3), ("circ", "<f8", 3),

@@ -16,8 +16,8 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
-from .abi import (ERR_NAMES, NV_OK, NvCounters, NvEvent, NvHostState, NvParams, NvTreeNode, State,
-                  tree_nodes_to_numpy)
+from .abi import (ERR_NAMES, NV_OK, NvCounters, NvEvent, NvFullState, NvHostState, NvParams, NvTreeNode, NvTsRow,
+                  State, tree_nodes_to_numpy)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libnuvort_gpu.so")
@@ -77,6 +77,17 @@ def lib():
     L.nv_measure_fp32_peak.argtypes = [i32, P(C.c_double)]
     L.nv_diagnostics.argtypes = [vp, i32, P(C.c_int64), i32]
     L.nv_calc_velocity_direct_at.argtypes = [vp, i32, P(i32), i32, P(C.c_double)]
+    L.nv_calculate_diagnostics.argtypes = [vp]
+    L.nv_ts_row_get.argtypes = [vp, i32, P(NvTsRow)]
+    L.nv_format_ts_row.argtypes = [P(NvTsRow), i32, C.c_char_p, i32]
+    L.nv_download_full.argtypes = [vp, i32, P(NvFullState), i32]
+    L.nv_upload_full.argtypes = [vp, i32, P(NvFullState)]
+    L.nv_write_snapshot.argtypes = [vp, i32, C.c_char_p]
+    L.nv_write_dump.argtypes = [vp, i32, C.c_char_p]
+    L.nv_restore_dump.argtypes = [vp, i32, C.c_char_p]
+    L.nv_snapshot_write_file.argtypes = [P(NvFullState), C.c_double, C.c_char_p]
+    L.nv_dump_write_file.argtypes = [P(NvFullState), i32, i32, C.c_double, C.c_char_p]
+    L.nv_dump_read_file.argtypes = [C.c_char_p, P(NvFullState), i32, P(i32), P(i32), P(i32), P(C.c_double)]
     _lib = L
     return L
 
@@ -114,6 +125,36 @@ def measure_fp32_peak(device: int = 0) -> float:
 
 def check_params(p: NvParams):
     _check(lib().nv_check_params(C.byref(p)))
+
+
+def format_ts_row(row: NvTsRow, shots: int = 1) -> str:
+    """The data/ts.log line print_info writes for this row (src/output.f90:38-40)."""
+    buf = C.create_string_buffer(256)
+    _check(lib().nv_format_ts_row(C.byref(row), int(shots), buf, 256))
+    return buf.value.decode()
+
+
+def snapshot_write_file(st: State, t: float, path: str):
+    """printf's data/var%04d.log stream file (src/output.f90:47-70) from host arrays."""
+    c = st.to_full_c()
+    _check(lib().nv_snapshot_write_file(C.byref(c), float(t), path.encode()))
+
+
+def dump_write_file(st: State, recon_count: int, itime: int, t: float, path: str):
+    """data_dump's data/var.dat (src/output.f90:85-94) from host arrays."""
+    c = st.to_full_c()
+    _check(lib().nv_dump_write_file(C.byref(c), int(recon_count), int(itime), float(t), path.encode()))
+
+
+def dump_read_file(path: str):
+    """(State with every kept field, recon_count, itime, t) of a var.dat (src/initial.f90:151-166)."""
+    n, rc_, it, t = C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
+    _check(lib().nv_dump_read_file(path.encode(), None, 0, C.byref(n), C.byref(rc_), C.byref(it), C.byref(t)))
+    st = State.empty_full(max(n.value, 1))
+    c = st.to_full_c()
+    _check(lib().nv_dump_read_file(path.encode(), C.byref(c), max(n.value, 1), C.byref(n), C.byref(rc_),
+                                   C.byref(it), C.byref(t)))
+    return st.trimmed(n.value), rc_.value, it.value, t.value
 
 
 class Handle:
@@ -214,6 +255,37 @@ class Handle:
         _check(lib().nv_calc_velocity_direct_at(self.h, int(sys), tg.ctypes.data_as(C.POINTER(C.c_int32)),
                                                 tg.shape[0], u.ctypes.data_as(C.POINTER(C.c_double))))
         return u
+
+    def upload_full(self, sys: int, st: State):
+        """upload plus u_sup, u_mf, curv and stretch."""
+        c = st.to_full_c()
+        _check(lib().nv_upload_full(self.h, int(sys), C.byref(c)))
+
+    def download_full(self, sys: int = 0) -> State:
+        """Every kept field of f(:), u_sup/u_mf/curv/stretch included."""
+        cap = self.capacity[sys]
+        st = State.empty_full(cap)
+        c = st.to_full_c()
+        _check(lib().nv_download_full(self.h, int(sys), C.byref(c), cap))
+        return st.trimmed(c.pcount)
+
+    def calculate_diagnostics(self):
+        """calculate_diagnostics (src/diagnostic.f90:9-74) for every system, on the device."""
+        _check(lib().nv_calculate_diagnostics(self.h))
+
+    def ts_row(self, sys: int = 0) -> NvTsRow:
+        row = NvTsRow()
+        _check(lib().nv_ts_row_get(self.h, int(sys), C.byref(row)))
+        return row
+
+    def write_snapshot(self, sys: int, path: str):
+        _check(lib().nv_write_snapshot(self.h, int(sys), path.encode()))
+
+    def write_dump(self, sys: int, path: str):
+        _check(lib().nv_write_dump(self.h, int(sys), path.encode()))
+
+    def restore_dump(self, sys: int, path: str):
+        _check(lib().nv_restore_dump(self.h, int(sys), path.encode()))
 
     def diagnostics(self, sys: int = 0) -> list:
         out = (C.c_int64 * 12)()

@@ -394,6 +394,20 @@ void accumulate_stage_times(nv_handle *h) {
 
 }  // namespace
 
+// Restart bookkeeping for data_restore (io.cpp): the clock and recon_count of a dump.
+int set_restart_counters(nv_handle *h, int sys, double t, int itime, int recon_count) {
+  if (!h || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "bad system");
+  int rc = set_device(h);
+  if (rc || (rc = pull_dyn_one(h, sys))) return rc;
+  h->h_dyn[sys].t = t;
+  h->h_dyn[sys].itime = itime;
+  h->h_dyn[sys].recon_count = recon_count;
+  NV_CUDA(cudaMemcpy(h->d_dyn + sys, &h->h_dyn[sys], sizeof(SysDyn), cudaMemcpyHostToDevice));
+  return NV_OK;
+}
+
+int sys_capacity(nv_handle *h, int sys) { return (h && sys >= 0 && sys < h->nsys) ? h->cap[sys] : -1; }
+
 // Per-system constants for callers outside this file (the static-scratch entry point).
 SysConst sysconst_for(const nv_params &p, int base, int cap) { return make_sysconst(p, base, cap); }
 
@@ -508,8 +522,13 @@ int nv_create(const nv_params *params, int32_t nsys, const int32_t *capacity, in
       (rc = dalloc(&h->gi, 3 * T)) || (rc = dalloc(&h->gb, 3 * T)) || (rc = dalloc(&h->closestd, T)) ||
       (rc = dalloc(&h->nxt, T)) || (rc = dalloc(&h->prv, T)) || (rc = dalloc(&h->closest, T)) ||
       (rc = dalloc(&h->sys_of, T)) || (rc = dalloc(&h->seg, 2 * T)) || (rc = dalloc(&h->d_err, 1)) ||
-      (rc = dalloc(&h->d_event_count, 1)) || (rc = dalloc(&h->d_upck, 2)))
+      (rc = dalloc(&h->d_event_count, 1)) || (rc = dalloc(&h->d_upck, 2)) || (rc = dalloc(&h->usm, 6 * T)) ||
+      (rc = dalloc(&h->cs, 2 * T)) || (rc = dalloc(&h->d_drec, nsys)))
     return bail(rc);
+  for (auto &c : h->sc) {  // the velocity passes keep u_sup and u_mf there
+    c.usm = h->usm;
+    c.usm_T = T;
+  }
   {
     int maxcap = 0;
     for (int s = 0; s < nsys; ++s) maxcap = std::max(maxcap, h->cap[s]);
@@ -550,7 +569,7 @@ int nv_destroy(nv_handle *h) {
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   tree_free(h);
   topo_free(h);
-  void *ptrs[] = {h->partial, h->stage, h->d_upck, h->d_sc, h->d_dyn, h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv,
+  void *ptrs[] = {h->usm, h->cs, h->d_drec, h->partial, h->stage, h->d_upck, h->d_sc, h->d_dyn, h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv,
                   h->closest, h->sys_of, h->seg, h->seg32, h->d_err, h->d_events, h->d_event_count,
                   h->d_work_direct, h->d_work_tree, h->d_work_lia, h->d_work_img, h->d_work_timg, h->d_work_split};
   for (void *p : ptrs)
@@ -613,6 +632,9 @@ int nv_upload(nv_handle *h, int32_t sys, const nv_host_state *st) {
       (rc = put(h->u2, st->u2, 3)) || (rc = put(h->gi, st->ghosti, 3)) || (rc = put(h->gb, st->ghostb, 3)) ||
       (rc = put(h->closestd, st->closestd, 1)))
     return rc;
+  // the new f(:) carries no u_sup, u_mf, curv or stretch yet (nv_upload_full sets them)
+  k_put_rows<<<grid_for(rows, 256), 256, 0, sm>>>(h->usm, T, base, rows, n, 6, nullptr);
+  k_put_rows<<<grid_for(rows, 256), 256, 0, sm>>>(h->cs, T, base, rows, n, 2, nullptr);
   SysDyn &d = h->h_dyn[sys];
   // keep the clock and counters; replace the slot count (pull_dyn_one waits for the copies)
   rc = pull_dyn_one(h, sys);
@@ -656,6 +678,108 @@ int nv_download(nv_handle *h, int32_t sys, nv_host_state *st, int32_t cap) {
       (rc = get_link(h->closest, st->closest)) || (rc = get(h->closestd, st->closestd, 1)))
     return rc;
   NV_CUDA(cudaStreamSynchronize(sm));
+  return NV_OK;
+}
+
+int nv_upload_full(nv_handle *h, int32_t sys, const nv_full_state *st) {
+  if (!h || !st || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_upload_full: bad arguments");
+  nv_host_state hs;
+  std::memset(&hs, 0, sizeof hs);
+  hs.pcount = st->pcount;
+  hs.x = st->x;
+  hs.u = st->u;
+  hs.u1 = st->u1;
+  hs.u2 = st->u2;
+  hs.ghosti = st->ghosti;
+  hs.ghostb = st->ghostb;
+  hs.infront = st->infront;
+  hs.behind = st->behind;
+  hs.closest = st->closest;
+  hs.closestd = st->closestd;
+  int rc = nv_upload(h, sys, &hs);  // checks the links before writing anything
+  if (rc) return rc;
+  const int n = st->pcount, base = h->base[sys], rows = h->cap[sys] + 1;
+  const long long T = h->T;
+  cudaStream_t sm = h->stream;
+  auto put = [&](double *dev, const double *src, int comps) -> int {
+    if (src && n > 0)
+      NV_CUDA(cudaMemcpyAsync(h->stage, src, (size_t)comps * n * sizeof(double), cudaMemcpyHostToDevice, sm));
+    k_put_rows<<<grid_for(rows, 256), 256, 0, sm>>>(dev, T, base, rows, n, comps, src ? h->stage : nullptr);
+    return NV_OK;
+  };
+  if ((rc = put(h->usm, st->u_sup, 3)) || (rc = put(h->usm + 3 * T, st->u_mf, 3)) || (rc = put(h->cs, st->curv, 1)) ||
+      (rc = put(h->cs + T, st->stretch, 1)))
+    return rc;
+  NV_CUDA(cudaStreamSynchronize(sm));
+  return NV_OK;
+}
+
+int nv_download_full(nv_handle *h, int32_t sys, nv_full_state *st, int32_t cap) {
+  if (!h || !st || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_download_full: bad arguments");
+  nv_host_state hs;
+  std::memset(&hs, 0, sizeof hs);
+  hs.x = st->x;
+  hs.u = st->u;
+  hs.u1 = st->u1;
+  hs.u2 = st->u2;
+  hs.ghosti = st->ghosti;
+  hs.ghostb = st->ghostb;
+  hs.infront = st->infront;
+  hs.behind = st->behind;
+  hs.closest = st->closest;
+  hs.closestd = st->closestd;
+  int rc = nv_download(h, sys, &hs, cap);
+  st->pcount = hs.pcount;
+  if (rc) return rc;
+  const int n = hs.pcount, base = h->base[sys];
+  const long long T = h->T;
+  cudaStream_t sm = h->stream;
+  auto get = [&](const double *dev, double *dst, int comps) -> int {
+    if (!dst || n == 0) return NV_OK;
+    k_get_rows<<<grid_for(n, 256), 256, 0, sm>>>(dev, T, base, n, comps, h->stage);
+    NV_CUDA(cudaMemcpyAsync(dst, h->stage, (size_t)comps * n * sizeof(double), cudaMemcpyDeviceToHost, sm));
+    return NV_OK;
+  };
+  if ((rc = get(h->usm, st->u_sup, 3)) || (rc = get(h->usm + 3 * T, st->u_mf, 3)) || (rc = get(h->cs, st->curv, 1)) ||
+      (rc = get(h->cs + T, st->stretch, 1)))
+    return rc;
+  NV_CUDA(cudaStreamSynchronize(sm));
+  return NV_OK;
+}
+
+int nv_calculate_diagnostics(nv_handle *h) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  int rc = set_device(h);
+  if (rc || (rc = diag_launch(h))) return rc;
+  return finish(h);
+}
+
+int nv_ts_row_get(nv_handle *h, int32_t sys, nv_ts_row *row) {
+  if (!h || !row || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_ts_row_get: bad arguments");
+  int rc = set_device(h);
+  if (rc || (rc = pull_dyn_one(h, sys))) return rc;
+  DiagRec r;
+  NV_CUDA(cudaMemcpy(&r, h->d_drec + sys, sizeof r, cudaMemcpyDeviceToHost));
+  if (!r.valid) return set_error(NV_ERR_STATE, "nv_ts_row_get: no diagnostics yet (call nv_calculate_diagnostics)");
+  const SysDyn &d = h->h_dyn[sys];
+  std::memset(row, 0, sizeof *row);
+  row->itime = d.itime;
+  row->live = r.live;
+  row->recon_count = d.recon_count;
+  row->wall_recon_count = 0;
+  row->remove_count = d.remove_count;
+  row->tree_eval = (int64_t)d.tree_eval;
+  row->t = d.t;
+  row->delta = h->params[sys].delta;
+  row->avg_sep = d.avg_sep;
+  row->total_length = d.total_length;
+  row->maxu = r.maxu;
+  row->maxdu = r.maxdu;
+  row->mean_u_sup = r.sum_usup / r.live;  // velocity_info: sum over f(:) / count(infront>0)
+  row->mean_u_mf = r.sum_umf / r.live;
+  row->kappa_bar = r.sum_curv / r.live;   // curv_info
+  row->kappa_min = r.kappa_min;
+  row->kappa_max = r.kappa_max;
   return NV_OK;
 }
 

@@ -83,7 +83,7 @@ __global__ void k_velocity_lia(const SysConst *__restrict__ scs, const SysDyn *_
   load3(GI, T, g, gi);
   load3(GB, T, g, gb);
   local_velocity(sc, x, gi, gb, u, fdot);
-  mf_epilogue(sc, dyn[w.x].t, fdot, u);
+  mf_epilogue(sc, dyn[w.x].t, fdot, u, g);
   store3(U, T, g, u);
 }
 

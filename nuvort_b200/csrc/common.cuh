@@ -54,6 +54,10 @@ struct SysConst {
   int use_tree;       // tree_theta>0 (run.f90:29,37)
   int base, cap;
   int sched_tree;     // non-local sum by the tree walk (velocity==Tree)
+  // f(:)%u_sup and f(:)%u_mf (timestep.f90:123,137) of the handle's slots: [6][usm_T],
+  // components 0-2 u_sup, 3-5 u_mf; null where they are not kept
+  double *usm;
+  long long usm_T;
 };
 
 struct SysDyn {
@@ -72,6 +76,17 @@ struct SysDyn {
   int ins_conv;      // pinsert's fixed-point iteration has converged
   int ins_mismatch;  // positions where the iteration's H and H' differ
   long long diag[12];  // see nv_diagnostics
+  double total_length;  // pinsert: sum of the segment lengths it measured (line.f90:39)
+  double avg_sep;       // pinsert: total_length / (old_pcount - empty slots) (line.f90:95)
+};
+
+// Reductions of calculate_diagnostics (diagnostic.f90:9-74) per system.
+struct DiagRec {
+  double maxu, maxdu;         // velocity_info
+  double sum_usup, sum_umf;   // sums of |u_sup|, |u_mf| over every slot
+  double sum_curv, kappa_max, kappa_min;  // curv_info (kappa_min over curvatures > 0; 0 if none)
+  int live;                   // count(f(:)%infront>0)
+  int valid;                  // set by a diagnostics pass
 };
 
 // Order-sensitive digest of one event (system-local slots; a loop kill's j is its count):
@@ -183,11 +198,17 @@ __device__ __forceinline__ void local_velocity(const SysConst &sc, const double 
   for (int c = 0; c < 3; ++c) u[c] = e_mul(beta, cr[c]);
 }
 
-// Mutual friction and imposed flow (timestep.f90:126-140); u holds u_sup on entry.
+// Mutual friction and imposed flow (timestep.f90:123-140); u holds u_sup on entry.  For the
+// velocity pass of a step (slot g >= 0) u_sup and u_mf are kept as the reference stores them
+// in f(g) (u_mf only when it is computed); g < 0 keeps nothing.
 __device__ __forceinline__ void mf_epilogue(const SysConst &sc, double t, const double fdot[3],
-                                            double u[3]) {
+                                            double u[3], long long g = -1) {
+  const bool keep = sc.usm && g >= 0;
+  if (keep)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) sc.usm[c * sc.usm_T + g] = u[c];
   if (sc.mf_on && t < sc.normal_fluid_cutoff) {
-    double un[3], w[3], c1[3], c2[3];
+    double un[3], w[3], c1[3], c2[3], umf[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) un[c] = (t < sc.t_zero_normal_fluid) ? sc.vn[c] : 0.0;
 #pragma unroll
@@ -195,7 +216,12 @@ __device__ __forceinline__ void mf_epilogue(const SysConst &sc, double t, const 
     cross3(fdot, w, c1);
     cross3(fdot, c1, c2);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], e_sub(e_mul(sc.alpha[0], c1[c]), e_mul(sc.alpha[1], c2[c])));
+    for (int c = 0; c < 3; ++c) umf[c] = e_sub(e_mul(sc.alpha[0], c1[c]), e_mul(sc.alpha[1], c2[c]));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], umf[c]);
+    if (keep)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) sc.usm[(3 + c) * sc.usm_T + g] = umf[c];
   }
 #pragma unroll
   for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], sc.super_velocity[c]);

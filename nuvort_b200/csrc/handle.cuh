@@ -36,6 +36,9 @@ struct nv_handle {
   double4 *seg = nullptr;   // FP64 segment records, 2 per slot
   float4 *seg32 = nullptr;  // FP32 segment records, 3 per slot (mixed precision)
   double *partial = nullptr; // per-image partial sums [image][component][slot] (mixed precision)
+  double *usm = nullptr;     // f(:)%u_sup, f(:)%u_mf of the last velocity pass [6][T]
+  double *cs = nullptr;      // f(:)%curv, f(:)%stretch of the last diagnostics [2][T]
+  struct DiagRec *d_drec = nullptr;  // per system: the last diagnostics' reductions
   double *stage = nullptr;   // nv_upload / nv_download staging: host arrays as they are, 3 x (largest capacity + 1) doubles
   int *d_upck = nullptr;     // nv_upload checks: [0] link errors (1 out of range, 2 empty-slot mismatch), [1] live slots
   int4 *d_work_img = nullptr;  // (system, image, first slot) items of the mixed direct sum
@@ -115,6 +118,8 @@ void launch_closest_tree(nv_handle *h);
 void join_root_sums(nv_handle *h);     // the main stream waits for the roots' exact sums
 void launch_walk_fixup(nv_handle *h);  // deferred root tests of the last tree walk
 int tree_dump(nv_handle *h, int sys, void *buf, int cap, int *n);
+// diagnostics (diag.cu): ghosts, per-point curvature and stretching, per-system reductions
+int diag_launch(nv_handle *h);
 // topology (topo.cu)
 void topo_alloc(nv_handle *h);
 void topo_free(nv_handle *h);

@@ -35,6 +35,10 @@ struct TopoBuffers {
   int *fh[2] = {nullptr, nullptr};  // higher-order insertion positions, H and H'
   int *pos_h = nullptr;     // exclusive prefix sum of H
   unsigned *l0 = nullptr, *l1 = nullptr;  // sweep bitmaps
+  // pinsert's measured segment lengths (total_length, line.f90:39): per slot the stale and
+  // the fresh distance, the one the sweep used, and per inserting slot the distance its new
+  // point measured when the sweep reached it (-1: not reached)
+  double *len_st = nullptr, *len_fr = nullptr, *seglen = nullptr, *dn_new = nullptr;
   void *cub_tmp = nullptr;
   size_t cub_bytes = 0;
   // cell list of the closest-point search of the systems without a tree (pclose)
@@ -132,6 +136,7 @@ struct State {
   double *X, *U, *U1, *U2, *GI, *GB, *CD;
   int *nxt, *prv, *cl;
   long long T;
+  double *seglen;  // pinsert: the length each visited slot measured
 };
 
 __device__ void clear_particle(const State &S, int g) {  // general.f90:10-20
@@ -393,10 +398,12 @@ __device__ __forceinline__ void ghost_of(const SysConst &sc, const double x[3], 
 // bit0 stale test, bit1 fresh test (ghost of the current infront position); list = either.
 __global__ void k_ins_mark(const SysConst *__restrict__ scs, SysDyn *__restrict__ dyn, const int *__restrict__ sys_of,
                            const double *__restrict__ X, const double *__restrict__ GI, const int *__restrict__ nxt,
-                           int *fa, int *fb, int *dec, long long T, const unsigned *err) {
+                           int *fa, int *fb, int *dec, double *len_st, double *len_fr, long long T,
+                           const unsigned *err) {
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (g > T) return;
   int a = 0, b = 0, dv = 0;
+  double lst = 0., lfr = 0.;
   if (g < T && !*err) {
     const int s = sys_of[g];
     const SysConst &sc = scs[s];
@@ -410,7 +417,9 @@ __global__ void k_ins_mark(const SysConst *__restrict__ scs, SysDyn *__restrict_
         load3(GI, T, (int)g, gi);
         load3(X, T, nxt[g], gf);
         ghost_adjust(sc, x, gf);
-        const int st = dist_gen(x, gi) > sc.delta, fr = dist_gen(x, gf) > sc.delta;
+        lst = dist_gen(x, gi);
+        lfr = dist_gen(x, gf);
+        const int st = lst > sc.delta, fr = lfr > sc.delta;
         dv = st | (fr << 1);
         a = st | fr;
         dyn[s].live = 1;
@@ -419,7 +428,58 @@ __global__ void k_ins_mark(const SysConst *__restrict__ scs, SysDyn *__restrict_
   }
   fa[g] = a;
   fb[g] = b;
-  if (g < T) dec[g] = dv;
+  if (g < T) {
+    dec[g] = dv;
+    len_st[g] = lst;
+    len_fr[g] = lfr;
+  }
+}
+
+// The length each live slot's test measured (line.f90:38-39): with the ghosts its
+// predecessor's insertion refreshed when that predecessor lies below it and inserts (the
+// same rule as its decision), else with the step-start ghosts; 0 for empty slots.  New points
+// the sweep reaches are written when the insertions are applied.
+__global__ void k_ins_len(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn,
+                          const int *__restrict__ sys_of, const int *__restrict__ nxt, const int *__restrict__ prv,
+                          const int *__restrict__ dec, const double *__restrict__ len_st,
+                          const double *__restrict__ len_fr, double *__restrict__ seglen, long long T) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= T) return;
+  double v = 0.;
+  const int s = sys_of[g];
+  const int k = (int)(g - scs[s].base);
+  if (k >= 1 && k <= dyn[s].pcount && nxt[g] != 0) {
+    const int p = prv[g];
+    v = (p < g && (dec[p] & 4)) ? len_fr[g] : len_st[g];
+  }
+  seglen[g] = v;
+}
+
+// total_length and avg_sep of the pinsert just made (line.f90:39,95), one block per system:
+// the measured lengths summed in a fixed order (per thread by stride, then a tree over the
+// block; the reference adds them one after another, which agrees to ~1e-13 relative) and
+// divided by old_pcount minus the empty slots left among the pcount slots.
+__global__ void __launch_bounds__(256) k_ins_total(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys,
+                                                   const double *__restrict__ seglen, const unsigned *err) {
+  __shared__ double part[256];
+  const int s = blockIdx.x;
+  if (s >= nsys || *err) return;
+  const SysConst &sc = scs[s];
+  const int pc = dyn[s].pcount;
+  double acc = 0.;
+  for (int k = 1 + threadIdx.x; k <= pc; k += 256) acc += seglen[sc.base + k];
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    SysDyn &d = dyn[s];
+    d.total_length = part[0];
+    const int empty = d.pcount - d.nlive;
+    d.avg_sep = part[0] / (double)(d.old_pcount - empty);
+  }
 }
 
 // Outcomes: known where the two tests agree (decided here, in parallel); where they differ
@@ -466,6 +526,7 @@ __global__ void k_ins_begin(SysDyn *dyn, int nsys) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys) return;
   dyn[s].live = 0;
+  dyn[s].old_pcount = dyn[s].pcount;
   dyn[s].ins_fallback = 0;
   dyn[s].ins_conv = 0;
   dyn[s].ins_mismatch = 0;
@@ -510,7 +571,7 @@ __global__ void k_ins_chain(const SysConst *__restrict__ scs, SysDyn *dyn, const
                             const int *__restrict__ pos_c, const int *__restrict__ list_c,
                             const int *__restrict__ pos_b, const int *__restrict__ list_b, const int *__restrict__ dec,
                             const int *__restrict__ pos_h, int *fout, int *newslot, int *segnx, double *xnew,
-                            double *unew, const int *__restrict__ nev_total, unsigned *err) {
+                            double *unew, double *dn_new, const int *__restrict__ nev_total, unsigned *err) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= *nev_total || *err) return;
   int k = list_c[t];
@@ -572,10 +633,15 @@ __global__ void k_ins_chain(const SysConst *__restrict__ scs, SysDyn *dyn, const
       xprev[c] = x[c];
     }
     int at = k, e = slot;
-    while (e > at && e <= old_last) {
+    for (;;) {
+      if (!(e > at && e <= old_last)) {  // the sweep never reaches at's new point
+        dn_new[at] = -1.0;
+        break;
+      }
       double gie[3], gbe[3], xq[3], uq[3];
       ghost_of(sc, xe, xnx, gie);
       const double dn = dist_gen(xe, gie);
+      dn_new[at] = dn;  // the length the new point e measures when the sweep reaches it
       if (!(dn > sc.delta)) break;
       fout[e] = 1;
       const int q = slot_of(e);
@@ -650,8 +716,8 @@ __global__ void k_ins_apply(const SysConst *__restrict__ scs, SysDyn *dyn, const
                             const int *__restrict__ pos_h, const int *__restrict__ fh,
                             const int *__restrict__ newslot, const int *__restrict__ segnx,
                             const double *__restrict__ xnew, const double *__restrict__ unew,
-                            const int *__restrict__ nev_total, DevEvent *ev, int *ev_count, int ev_cap,
-                            unsigned *err) {
+                            const double *__restrict__ dn_new, const int *__restrict__ nev_total, DevEvent *ev,
+                            int *ev_count, int ev_cap, unsigned *err) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= *nev_total || *err) return;
   const int k = list_c[t];
@@ -683,6 +749,7 @@ __global__ void k_ins_apply(const SysConst *__restrict__ scs, SysDyn *dyn, const
     S.CD[q] = 0;
     S.prv[q] = g;
     S.nxt[g] = q;
+    if (dn_new[g] >= 0.) S.seglen[q] = dn_new[g];
     const int seq = seq0 + (pos_c[g] - ev0) + (pos_h[g] - h0);
     const int a = atomicAdd(ev_count, 1);
     if (a < ev_cap) ev[a] = DevEvent{s, seq, itime, NV_EV_INSERT, g, q};
@@ -1530,6 +1597,7 @@ __global__ void __launch_bounds__(32) k_insert_sweep(const SysConst *__restrict_
     load3(S.GI, T, i, gi);
     load3(S.GB, T, i, gb);
     const double disti = dist_gen(x, gi);
+    S.seglen[i] = disti;
     if (!(disti > sc.delta)) return true;
     int p;
     if (!take_slot(p)) return false;
@@ -1693,7 +1761,8 @@ __global__ void __launch_bounds__(32) k_insert_sweep(const SysConst *__restrict_
 }
 
 State make_state(nv_handle *h) {
-  return State{h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv, h->closest, h->T};
+  return State{h->x,  h->u,       h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv, h->closest, h->T,
+               h->topo->seglen};
 }
 
 void compact(nv_handle *h, int *flag, int *pos, int *list) {
@@ -1738,6 +1807,11 @@ void topo_alloc(nv_handle *h) {
   cudaMalloc(&tb->pos_h, n * sizeof(int));
   cudaMalloc(&tb->l0, (n / 32 + 2) * sizeof(unsigned));
   cudaMalloc(&tb->l1, (n / 1024 + 2) * sizeof(unsigned));
+  cudaMalloc(&tb->len_st, n * sizeof(double));
+  cudaMalloc(&tb->len_fr, n * sizeof(double));
+  cudaMalloc(&tb->seglen, n * sizeof(double));
+  cudaMalloc(&tb->dn_new, n * sizeof(double));
+  cudaMemset(tb->seglen, 0, n * sizeof(double));
   // cell grids of the systems without a tree: about two slots per cell at full capacity,
   // cells at least as wide as delta/2 and at most 256 per axis
   std::vector<CellGrid> grids(h->nsys);
@@ -1785,6 +1859,7 @@ void topo_free(nv_handle *h) {
   cudaFree(tb->dec); cudaFree(tb->newslot); cudaFree(tb->xnew);
   cudaFree(tb->unew); cudaFree(tb->segnx); cudaFree(tb->fh[0]); cudaFree(tb->fh[1]); cudaFree(tb->pos_h);
   cudaFree(tb->l0); cudaFree(tb->l1);
+  cudaFree(tb->len_st); cudaFree(tb->len_fr); cudaFree(tb->seglen); cudaFree(tb->dn_new);
   cudaFree(tb->grid); cudaFree(tb->cell_of); cudaFree(tb->cell_cnt); cudaFree(tb->cell_start);
   cudaFree(tb->cell_items);
   cudaFree(tb->cub_tmp);
@@ -1798,7 +1873,8 @@ void launch_pinsert(nv_handle *h) {
   const long long T = h->T;
   k_ins_begin<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_dyn, h->nsys);
   k_ins_mark<<<grid_for(T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->x, h->gi, h->nxt,
-                                                         tb->flag_a, tb->flag_b, tb->dec, T, h->d_err);
+                                                         tb->flag_a, tb->flag_b, tb->dec, tb->len_st, tb->len_fr, T,
+                                                         h->d_err);
   compact(h, tb->flag_a, tb->pos_a, tb->list_a);  // candidates (either test passes)
   compact(h, tb->flag_b, tb->pos_b, tb->list_b);  // free slots
   k_zero_flags<<<grid_for(T + 1, TB), TB, 0, h->stream>>>(tb->flag_c, T);
@@ -1811,6 +1887,8 @@ void launch_pinsert(nv_handle *h) {
   k_ins_decide_case<<<grid_for(T, 128), 128, 0, h->stream>>>(tb->list_a, ncand, h->prv, tb->dec, tb->flag_c,
                                                              h->d_err);
   compact(h, tb->flag_c, tb->pos_c, tb->list_c);  // insertions, in sweep order
+  k_ins_len<<<grid_for(T, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->nxt, h->prv, tb->dec, tb->len_st,
+                                                   tb->len_fr, tb->seglen, T);
   const State S = make_state(h);
   // the number of insertions (pos_c[T]) is known only on the device: launch over every
   // slot, threads beyond the count return at once
@@ -1830,13 +1908,13 @@ void launch_pinsert(nv_handle *h) {
     cub::DeviceScan::ExclusiveSum(tb->cub_tmp, bytes, fin, tb->pos_h, (int)(T + 1), h->stream);
     k_ins_chain<<<grid, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, S, tb->pos_c, tb->list_c, tb->pos_b,
                                              tb->list_b, tb->dec, tb->pos_h, fout, tb->newslot, tb->segnx, tb->xnew,
-                                             tb->unew, nev, h->d_err);
+                                             tb->unew, tb->dn_new, nev, h->d_err);
     k_ins_compare<<<grid_for(T, TB), TB, 0, h->stream>>>(h->d_dyn, h->sys_of, fin, fout, T);
     k_ins_converge<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_dyn, h->nsys, it + 1, it + 1 == iters);
   }
   const int *fh = tb->fh[iters > 0 ? (iters - 1) & 1 : 0];  // pos_h is its prefix sum
   k_ins_apply<<<grid, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, S, tb->pos_c, tb->list_c, tb->pos_h, fh,
-                                           tb->newslot, tb->segnx, tb->xnew, tb->unew, nev, h->d_events,
+                                           tb->newslot, tb->segnx, tb->xnew, tb->unew, tb->dn_new, nev, h->d_events,
                                            h->d_event_count, h->event_cap, h->d_err);
   k_ins_ghosts<<<grid, 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, S, tb->list_c, fh, tb->newslot, nev,
                                             h->d_err);
@@ -1849,6 +1927,7 @@ void launch_pinsert(nv_handle *h) {
   k_insert_sweep<<<h->nsys, 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, S, tb->pos_a, tb->list_a, tb->pos_b,
                                                 tb->list_b, sw, h->d_err, h->d_events, h->d_event_count,
                                                 h->event_cap);
+  k_ins_total<<<h->nsys, 256, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, tb->seglen, h->d_err);
 }
 
 void launch_pclose(nv_handle *h, bool only_brute) {

@@ -16,7 +16,7 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
-from nuvort_b200.abi import (NvCounters, NvEvent, NvParams, NvTreeNode, State, NV_OK,
+from nuvort_b200.abi import (NvCounters, NvEvent, NvFullState, NvParams, NvTreeNode, NvTsRow, State, NV_OK,
                              ERR_NAMES, tree_nodes_to_numpy)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -60,6 +60,12 @@ def lib():
         L.or_calc_velocity.argtypes = [vp, P(C.c_double)]
         L.or_calc_velocity_targets.argtypes = [vp, C.c_int32, P(C.c_int32), C.c_int32, P(C.c_double)]
         L.or_tree_dump.argtypes = [vp, P(NvTreeNode), C.c_int32, P(C.c_int32)]
+        L.or_calculate_diagnostics.argtypes = [vp]
+        L.or_ts_row_get.argtypes = [vp, P(NvTsRow)]
+        L.or_download_full.argtypes = [vp, P(NvFullState), C.c_int32]
+        L.or_upload_full.argtypes = [vp, P(NvFullState)]
+        L.or_write_snapshot.argtypes = [vp, C.c_char_p]
+        L.or_write_dump.argtypes = [vp, C.c_char_p]
         L.or_set_threads.argtypes = [C.c_int32]
         L.or_get_threads.restype = C.c_int32
         L.or_last_error.restype = C.c_char_p
@@ -154,6 +160,31 @@ class Oracle:
         _check(lib().or_calc_velocity_targets(self.h, int(velocity), tg.ctypes.data_as(C.POINTER(C.c_int32)),
                                               tg.shape[0], u.ctypes.data_as(C.POINTER(C.c_double))))
         return u
+
+    def calculate_diagnostics(self):
+        _check(lib().or_calculate_diagnostics(self.h))
+
+    def ts_row(self) -> NvTsRow:
+        row = NvTsRow()
+        _check(lib().or_ts_row_get(self.h, C.byref(row)))
+        return row
+
+    def download_full(self) -> State:
+        n = self.counters().pcount
+        st = State.empty_full(max(n, 1))
+        c = st.to_full_c()
+        _check(lib().or_download_full(self.h, C.byref(c), max(n, 1)))
+        return st.trimmed(c.pcount)
+
+    def upload_full(self, st: State):
+        c = st.to_full_c()
+        _check(lib().or_upload_full(self.h, C.byref(c)))
+
+    def write_snapshot(self, path: str):
+        _check(lib().or_write_snapshot(self.h, path.encode()))
+
+    def write_dump(self, path: str):
+        _check(lib().or_write_dump(self.h, path.encode()))
 
     def tree_dump(self) -> np.ndarray:
         n = C.c_int32()

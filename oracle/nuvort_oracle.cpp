@@ -35,6 +35,7 @@ thread_local long long tests_tls = 0;  // opening tests of the calling thread
 
 struct Pt {  // type(qvort), src/cdata.f90:19-29 (pinning fields omitted: periodic/open only)
   double x[3], u[3], u1[3], u2[3], u_mf[3], u_sup[3];
+  double curv, stretch;
   double ghosti[3], ghostb[3];
   int infront, behind, closest;
   double closestd;
@@ -78,6 +79,11 @@ struct Sys {
   long long tree_eval = 0;
   long long tree_tests = 0;
   double total_length = 0.0, avg_sep = 0.0;
+  // calculate_diagnostics (diagnostic.f90:9-74)
+  double maxu = 0.0, maxdu = 0.0, mean_u_sup = 0.0, mean_u_mf = 0.0;
+  double kappa_bar = 0.0, kappa_min = 0.0, kappa_max = 0.0;
+  int diag_live = 0;
+  bool diag_valid = false;
   std::vector<std::array<double, 3>> shifts;  // periodic_loop_array
   Node *vtree = nullptr;
   std::vector<std::unique_ptr<Node>> pool;
@@ -545,6 +551,63 @@ struct Sys {
     }
   }
 
+  // ---- diagnostic.f90:9-74 calculate_diagnostics ------------------------------------------
+  void calculate_diagnostics() {
+    ghostp();
+    // velocity_info (:22-34): maxval/sum over every slot of f(:), divided by the live count
+    int live = 0;
+    for (int i = 1; i <= pcount; ++i) live += f[i].infront > 0;
+    double mu = -1.7976931348623157e308, mdu = -1.7976931348623157e308, ssup = 0.0, smf = 0.0;
+    for (int i = 1; i <= pcount; ++i) {
+      const Pt &q = f[i];
+      const double a = std::sqrt(q.u[0] * q.u[0] + q.u[1] * q.u[1] + q.u[2] * q.u[2]);
+      if (a > mu) mu = a;
+      const double b = std::sqrt((q.u1[0] - q.u2[0]) * (q.u1[0] - q.u2[0]) + (q.u1[1] - q.u2[1]) * (q.u1[1] - q.u2[1]) +
+                                 (q.u1[2] - q.u2[2]) * (q.u1[2] - q.u2[2]));
+      if (b > mdu) mdu = b;
+    }
+    for (int i = 1; i <= pcount; ++i)
+      ssup = ssup + std::sqrt(f[i].u_sup[0] * f[i].u_sup[0] + f[i].u_sup[1] * f[i].u_sup[1] +
+                              f[i].u_sup[2] * f[i].u_sup[2]);
+    for (int i = 1; i <= pcount; ++i)
+      smf = smf + std::sqrt(f[i].u_mf[0] * f[i].u_mf[0] + f[i].u_mf[1] * f[i].u_mf[1] + f[i].u_mf[2] * f[i].u_mf[2]);
+    maxu = mu;
+    maxdu = mdu;
+    mean_u_sup = ssup / live;
+    mean_u_mf = smf / live;
+    // curv_info (:37-57): curvature (general.f90:53-61) per point, 0 for empty slots
+    double sum = 0.0, kmax = -1.7976931348623157e308, kmin = 1.7976931348623157e308;
+    for (int i = 1; i <= pcount; ++i) {
+      double curvi = 0.0;
+      if (f[i].infront != 0) {
+        double fddot[3];
+        get_deriv_2(i, fddot);
+        curvi = std::sqrt(dot3(fddot, fddot));
+      }
+      f[i].curv = curvi;
+    }
+    for (int i = 1; i <= pcount; ++i) sum = sum + f[i].curv;
+    for (int i = 1; i <= pcount; ++i) {
+      if (f[i].curv > kmax) kmax = f[i].curv;
+      if (f[i].curv > 0.0 && f[i].curv < kmin) kmin = f[i].curv;
+    }
+    kappa_bar = sum / live;
+    kappa_max = kmax;
+    kappa_min = kmin;
+    // stretching_rate (:60-74): u . s''
+    for (int i = 1; i <= pcount; ++i) {
+      if (f[i].infront == 0) {
+        f[i].stretch = 0.0;
+      } else {
+        double s_ddot[3];
+        get_deriv_2(i, s_ddot);
+        f[i].stretch = dot3(f[i].u, s_ddot);
+      }
+    }
+    diag_live = live;
+    diag_valid = true;
+  }
+
   // ---- line.f90:18-96 pinsert -----------------------------------------------------------------
   int pinsert() {
     int live = 0;
@@ -788,6 +851,137 @@ int or_counters_get(or_handle *h, nv_counters *c) {
   c->itime = s.itime;
   c->n_events = (int32_t)s.events.size();
   c->t = s.t;
+  return NV_OK;
+}
+
+int or_calculate_diagnostics(or_handle *h) {
+  h->s.calculate_diagnostics();
+  return NV_OK;
+}
+
+int or_ts_row_get(or_handle *h, nv_ts_row *row) {  // the values print_info writes (output.f90:20-44)
+  const Sys &s = h->s;
+  if (!s.diag_valid) return fail(NV_ERR_STATE, "no diagnostics yet");
+  std::memset(row, 0, sizeof *row);
+  row->itime = s.itime;
+  row->live = s.diag_live;
+  row->recon_count = s.recon_count;
+  row->wall_recon_count = 0;
+  row->remove_count = s.remove_count;
+  row->tree_eval = s.tree_eval;
+  row->t = s.t;
+  row->delta = s.p.delta;
+  row->avg_sep = s.avg_sep;
+  row->total_length = s.total_length;
+  row->maxu = s.maxu;
+  row->maxdu = s.maxdu;
+  row->mean_u_sup = s.mean_u_sup;
+  row->mean_u_mf = s.mean_u_mf;
+  row->kappa_bar = s.kappa_bar;
+  row->kappa_min = s.kappa_min;
+  row->kappa_max = s.kappa_max;
+  return NV_OK;
+}
+
+int or_download_full(or_handle *h, nv_full_state *st, int32_t cap) {
+  if (!h || !st) return fail(NV_ERR_ARG, "null argument");
+  const Sys &s = h->s;
+  if (s.pcount > cap) return fail(NV_ERR_ARG, "download: capacity too small");
+  st->pcount = s.pcount;
+  for (int k = 1; k <= s.pcount; ++k) {
+    const Pt &q = s.f[k];
+    for (int c = 0; c < 3; ++c) {
+      const int o = 3 * (k - 1) + c;
+      if (st->x) st->x[o] = q.x[c];
+      if (st->u) st->u[o] = q.u[c];
+      if (st->u1) st->u1[o] = q.u1[c];
+      if (st->u2) st->u2[o] = q.u2[c];
+      if (st->u_mf) st->u_mf[o] = q.u_mf[c];
+      if (st->u_sup) st->u_sup[o] = q.u_sup[c];
+      if (st->ghosti) st->ghosti[o] = q.ghosti[c];
+      if (st->ghostb) st->ghostb[o] = q.ghostb[c];
+    }
+    if (st->curv) st->curv[k - 1] = q.curv;
+    if (st->stretch) st->stretch[k - 1] = q.stretch;
+    if (st->infront) st->infront[k - 1] = q.infront;
+    if (st->behind) st->behind[k - 1] = q.behind;
+    if (st->closest) st->closest[k - 1] = q.closest;
+    if (st->closestd) st->closestd[k - 1] = q.closestd;
+  }
+  return NV_OK;
+}
+
+int or_upload_full(or_handle *h, const nv_full_state *st) {
+  nv_host_state hs{st->pcount, st->x, st->u, st->u1, st->u2, st->ghosti, st->ghostb,
+                   st->infront, st->behind, st->closest, st->closestd};
+  int rc = or_upload(h, &hs);
+  if (rc) return rc;
+  for (int k = 1; k <= st->pcount; ++k) {
+    Pt &q = h->s.f[k];
+    for (int c = 0; c < 3; ++c) {
+      q.u_mf[c] = st->u_mf ? st->u_mf[3 * (k - 1) + c] : 0.0;
+      q.u_sup[c] = st->u_sup ? st->u_sup[3 * (k - 1) + c] : 0.0;
+    }
+    q.curv = st->curv ? st->curv[k - 1] : 0.0;
+    q.stretch = st->stretch ? st->stretch[k - 1] : 0.0;
+  }
+  return NV_OK;
+}
+
+// printf (output.f90:47-70): the unformatted stream file, one write per statement.
+int or_write_snapshot(or_handle *h, const char *path) {
+  const Sys &s = h->s;
+  FILE *fp = std::fopen(path, "wb");
+  if (!fp) return fail(NV_ERR_IO, "cannot open file");
+  const int32_t pc = s.pcount;
+  std::fwrite(&s.t, sizeof(double), 1, fp);                                        // write(98) t
+  std::fwrite(&pc, sizeof(int32_t), 1, fp);                                        // write(98) pcount
+  for (int c = 0; c < 3; ++c)                                                      // f(:)%x(1..3)
+    for (int i = 1; i <= pc; ++i) std::fwrite(&s.f[i].x[c], sizeof(double), 1, fp);
+  for (int i = 1; i <= pc; ++i) std::fwrite(&s.f[i].infront, sizeof(int32_t), 1, fp);  // f(:)%infront
+  for (int c = 0; c < 3; ++c)                                                      // f(:)%u(1..3)
+    for (int i = 1; i <= pc; ++i) std::fwrite(&s.f[i].u[c], sizeof(double), 1, fp);
+  for (int c = 0; c < 3; ++c)                                                      // f(:)%u_mf(1..3)
+    for (int i = 1; i <= pc; ++i) std::fwrite(&s.f[i].u_mf[c], sizeof(double), 1, fp);
+  for (int i = 1; i <= pc; ++i) std::fwrite(&s.f[i].curv, sizeof(double), 1, fp);     // f(:)%curv
+  for (int i = 1; i <= pc; ++i) std::fwrite(&s.f[i].stretch, sizeof(double), 1, fp);  // f(:)%stretch
+  std::fclose(fp);
+  return NV_OK;
+}
+
+// data_dump (output.f90:85-94) as gfortran writes it: each write statement one sequential
+// record, a 4-byte byte count before and after; f element after element, component after
+// component (type qvort, cdata.f90:19-29; real(8), integer(4), logical(4)).
+int or_write_dump(or_handle *h, const char *path) {
+  const Sys &s = h->s;
+  FILE *fp = std::fopen(path, "wb");
+  if (!fp) return fail(NV_ERR_IO, "cannot open file");
+  auto rec_int = [&](int32_t v) {
+    const int32_t m = 4;
+    std::fwrite(&m, 4, 1, fp); std::fwrite(&v, 4, 1, fp); std::fwrite(&m, 4, 1, fp);
+  };
+  rec_int(s.pcount);       // write(53) pcount
+  rec_int(s.recon_count);  // write(53) recon_count
+  rec_int(s.itime);        // write(53) itime
+  {
+    const int32_t m = 8;  // write(53) t
+    std::fwrite(&m, 4, 1, fp); std::fwrite(&s.t, 8, 1, fp); std::fwrite(&m, 4, 1, fp);
+  }
+  const int32_t m = 248 * s.pcount;  // write(53) f
+  std::fwrite(&m, 4, 1, fp);
+  const int32_t zero = 0;
+  for (int i = 1; i <= s.pcount; ++i) {
+    const Pt &q = s.f[i];
+    std::fwrite(q.x, 8, 3, fp); std::fwrite(q.u, 8, 3, fp); std::fwrite(q.u1, 8, 3, fp);
+    std::fwrite(q.u2, 8, 3, fp); std::fwrite(q.u_mf, 8, 3, fp); std::fwrite(q.u_sup, 8, 3, fp);
+    std::fwrite(&q.curv, 8, 1, fp); std::fwrite(&q.stretch, 8, 1, fp);
+    std::fwrite(q.ghosti, 8, 3, fp); std::fwrite(q.ghostb, 8, 3, fp);
+    std::fwrite(&q.infront, 4, 1, fp); std::fwrite(&q.behind, 4, 1, fp); std::fwrite(&q.closest, 4, 1, fp);
+    std::fwrite(&q.closestd, 8, 1, fp);
+    for (int c = 0; c < 5; ++c) std::fwrite(&zero, 4, 1, fp);  // wpinned(3), pinnedi, pinnedb: .false.
+  }
+  std::fwrite(&m, 4, 1, fp);
+  std::fclose(fp);
   return NV_OK;
 }
 

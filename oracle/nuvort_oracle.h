@@ -67,6 +67,16 @@ int or_calc_velocity(or_handle *h, double *u3);
  * Used as the FP64 direct-sum error oracle on subsamples and for the CPU baseline. */
 int or_calc_velocity_targets(or_handle *h, int32_t velocity, const int32_t *targets,
                              int32_t n, double *u3);
+/* calculate_diagnostics (src/diagnostic.f90:9-74) and the values print_info writes
+ * (src/output.f90:20-44), with sequential sums as the reference's sum intrinsic makes them. */
+int or_calculate_diagnostics(or_handle *h);
+int or_ts_row_get(or_handle *h, nv_ts_row *row);
+/* Every kept field of f(:), and the upload of one (u_sup, u_mf, curv, stretch included). */
+int or_download_full(or_handle *h, nv_full_state *st, int32_t cap);
+int or_upload_full(or_handle *h, const nv_full_state *st);
+/* printf (src/output.f90:47-70) and data_dump (src/output.f90:85-94) files. */
+int or_write_snapshot(or_handle *h, const char *path);
+int or_write_dump(or_handle *h, const char *path);
 /* Dump the current tree (built by or_construct_tree) in preorder. */
 int or_tree_dump(or_handle *h, or_tree_node *buf, int32_t cap, int32_t *n);
 
