@@ -13,6 +13,8 @@ module nuvort_gpu
   integer(c_int32_t), parameter :: NV_VEL_LIA = 0, NV_VEL_BS = 1, NV_VEL_TREE = 2
   integer(c_int32_t), parameter :: NV_BC_PERIODIC = 0, NV_BC_OPEN = 1, NV_BC_SOLID = 2
   integer(c_int32_t), parameter :: NV_NF_ZERO = 0, NV_NF_XFLOW = 1, NV_NF_UNIFORM = 2
+  integer(c_int32_t), parameter :: NV_NF_SHEAR_XFLOW = 3, NV_NF_CHANNEL = 4, NV_NF_YCHANNEL = 5
+  integer(c_int32_t), parameter :: NV_NF_NOISEY_XFLOW = 6, NV_NF_LAIZET_DNS = 7, NV_NF_TURB_DNS = 8
   integer(c_int32_t), parameter :: NV_PREC_FP64 = 0, NV_PREC_MIXED = 1
 
   type, bind(c) :: nv_params
@@ -25,6 +27,7 @@ module nuvort_gpu
     real(c_double) :: tree_theta, norm_vel_xflow
     real(c_double) :: norm_vel_vec(3), alpha(2), super_velocity(3)
     real(c_double) :: normal_fluid_cutoff, t_zero_normal_fluid
+    real(c_double) :: norm_shear_omega
   end type
 
   type, bind(c) :: nv_host_state
@@ -163,8 +166,16 @@ contains
     if (boundary_x == 'solid') p%boundary(1) = NV_BC_SOLID
     if (boundary_y == 'solid') p%boundary(2) = NV_BC_SOLID
     if (boundary_z == 'solid') p%boundary(3) = NV_BC_SOLID
-    p%normal_velocity = NV_NF_ZERO
-    if (normal_velocity == 'xflow') p%normal_velocity = NV_NF_XFLOW
+    select case (trim(normal_velocity))
+      case ('xflow') ; p%normal_velocity = NV_NF_XFLOW
+      case ('shear_xflow') ; p%normal_velocity = NV_NF_SHEAR_XFLOW
+      case ('channel') ; p%normal_velocity = NV_NF_CHANNEL
+      case ('ychannel') ; p%normal_velocity = NV_NF_YCHANNEL
+      case ('noisey_xflow') ; p%normal_velocity = NV_NF_NOISEY_XFLOW
+      case ('laizetDNS') ; p%normal_velocity = NV_NF_LAIZET_DNS
+      case ('turbDNS') ; p%normal_velocity = NV_NF_TURB_DNS
+      case default ; p%normal_velocity = NV_NF_ZERO
+    end select
     p%tree_extra_correction = merge(1, 0, tree_extra_correction)
     p%nan_test = merge(1, 0, NAN_test)
     p%overide_timestep_check = merge(1, 0, overide_timestep_check)
@@ -172,6 +183,7 @@ contains
     p%box_size = box_size ; p%tree_theta = tree_theta ; p%norm_vel_xflow = norm_vel_xflow
     p%alpha = alpha ; p%super_velocity = super_velocity
     p%normal_fluid_cutoff = normal_fluid_cutoff ; p%t_zero_normal_fluid = t_zero_normal_fluid
+    p%norm_shear_omega = norm_shear_omega
   end subroutine
 
   subroutine nv_check(rc, where)

@@ -52,9 +52,16 @@ enum {
 /* ---- option values (the run.in strings of src/cdata.f90:131-241) -------------------- */
 enum { NV_VEL_LIA = 0, NV_VEL_BS = 1, NV_VEL_TREE = 2 };               /* velocity */
 enum { NV_BC_PERIODIC = 0, NV_BC_OPEN = 1, NV_BC_SOLID = 2 };          /* boundary_x/y/z */
-/* normal_velocity: 'zero' and 'xflow' as in src/normal_fluid.f90:94-97; 'uniform' is an
- * extension (a constant vector norm_vel_vec) that the reference lacks. */
-enum { NV_NF_ZERO = 0, NV_NF_XFLOW = 1, NV_NF_UNIFORM = 2 };
+/* normal_velocity, the fields of get_normal_velocity (src/normal_fluid.f90:83-118): 'zero',
+ * 'xflow', 'shear_xflow' (A sin(2 pi z/L_z + omega t) along x), 'ychannel' (A (1-(2y/L_y)^2)
+ * along x), 'channel' (the 10-term duct series), 'noisey_xflow' (A times a noise sample that
+ * advances once per pmotion; samples from nv_set_normal_fluid_noise), 'laizetDNS' and
+ * 'turbDNS' (trilinear interpolation on a stored grid, nv_set_normal_fluid_grid).  'uniform'
+ * is an extension (a constant vector norm_vel_vec) that the reference lacks. */
+enum {
+  NV_NF_ZERO = 0, NV_NF_XFLOW = 1, NV_NF_UNIFORM = 2, NV_NF_SHEAR_XFLOW = 3, NV_NF_CHANNEL = 4,
+  NV_NF_YCHANNEL = 5, NV_NF_NOISEY_XFLOW = 6, NV_NF_LAIZET_DNS = 7, NV_NF_TURB_DNS = 8
+};
 /* precision of the non-local sum: FP64 reproduces the reference's arithmetic; MIXED runs the
  * far field in FP32 with compensated accumulation and keeps the near field in FP64. */
 enum { NV_PREC_FP64 = 0, NV_PREC_MIXED = 1 };
@@ -88,6 +95,7 @@ typedef struct nv_params {
   double super_velocity[3];       /* imposed superflow                       cdata.f90:206 */
   double normal_fluid_cutoff;     /* default 1e8                             cdata.f90:198 */
   double t_zero_normal_fluid;     /* default 1e8                             cdata.f90:200 */
+  double norm_shear_omega;        /* shear_xflow frequency, default 0        cdata.f90:232 */
 } nv_params;
 
 /* Host view of one system's filament state (the fields of type(qvort), cdata.f90:19-29,
@@ -247,6 +255,18 @@ int nv_set_root_band(nv_handle *h, double scale);
  * is the same bit for bit); 1 keeps one thread per target.  0 (the default) picks the split
  * from the number of work items and the SM count. */
 int nv_set_walk_parts(nv_handle *h, int32_t parts);
+/* Data of the normal-fluid fields that the reference reads from files.  noisey_xflow: the n
+ * multipliers of noise_file (src/normal_fluid.f90:156-162; the reference reads 100000), used
+ * one per step from the first, wrapping after the last (randomise_normal_fluid, :340-348).
+ * laizetDNS / turbDNS: the velocity grid as the reference reads it (setup_laizet :164-190,
+ * setup_turbDNS :192-216): u holds the three components one after another, each nx*ny*nz
+ * values in Fortran order (x fastest); laizetDNS needs nx,ny,nz = 128,129,84 and the 129
+ * values of yp.dat (its u is halved as setup_laizet does), turbDNS 256,256,256 (yp NULL).
+ * Point positions below the first grid node, which the reference reads out of its array,
+ * wrap on the periodic axes and clamp on laizet's y axis. */
+int nv_set_normal_fluid_noise(nv_handle *h, int32_t sys, const double *noise, int32_t n);
+int nv_set_normal_fluid_grid(nv_handle *h, int32_t sys, const double *u, int32_t nx, int32_t ny, int32_t nz,
+                             const double *yp);
 /* Split of the plain FP64 direct sum's work.  64: one thread per target, each summing its
  * terms as it computes them.  1, 2, 4 or 8: a block of 128 threads per that many targets;
  * three warps compute the terms tile by tile and one lane per (target, component) adds them

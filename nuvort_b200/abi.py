@@ -34,13 +34,17 @@ ERR_NAMES = {v: k for k, v in globals().items() if k.startswith("NV_ERR_") or k 
 NV_VEL_LIA, NV_VEL_BS, NV_VEL_TREE = 0, 1, 2
 NV_BC_PERIODIC, NV_BC_OPEN, NV_BC_SOLID = 0, 1, 2
 NV_NF_ZERO, NV_NF_XFLOW, NV_NF_UNIFORM = 0, 1, 2
+NV_NF_SHEAR_XFLOW, NV_NF_CHANNEL, NV_NF_YCHANNEL, NV_NF_NOISEY_XFLOW = 3, 4, 5, 6
+NV_NF_LAIZET_DNS, NV_NF_TURB_DNS = 7, 8
 NV_PREC_FP64, NV_PREC_MIXED = 0, 1
 NV_EV_INSERT, NV_EV_RECON, NV_EV_REMOVE, NV_EV_LOOPKILL = 1, 2, 3, 4
 NV_TREE_MAX_DEPTH = 42
 
 VELOCITY = {"LIA": NV_VEL_LIA, "BS": NV_VEL_BS, "Tree": NV_VEL_TREE}
 BOUNDARY = {"periodic": NV_BC_PERIODIC, "open": NV_BC_OPEN, "solid": NV_BC_SOLID}
-NORMAL = {"zero": NV_NF_ZERO, "xflow": NV_NF_XFLOW, "uniform": NV_NF_UNIFORM}
+NORMAL = {"zero": NV_NF_ZERO, "xflow": NV_NF_XFLOW, "uniform": NV_NF_UNIFORM, "shear_xflow": NV_NF_SHEAR_XFLOW,
+          "channel": NV_NF_CHANNEL, "ychannel": NV_NF_YCHANNEL, "noisey_xflow": NV_NF_NOISEY_XFLOW,
+          "laizetDNS": NV_NF_LAIZET_DNS, "turbDNS": NV_NF_TURB_DNS}
 
 
 class NvParams(C.Structure):
@@ -67,6 +71,7 @@ class NvParams(C.Structure):
         ("super_velocity", C.c_double * 3),
         ("normal_fluid_cutoff", C.c_double),
         ("t_zero_normal_fluid", C.c_double),
+        ("norm_shear_omega", C.c_double),
     ]
 
 
@@ -191,6 +196,7 @@ def default_params() -> NvParams:
     p.norm_vel_xflow = 0.5
     p.normal_fluid_cutoff = 1e8
     p.t_zero_normal_fluid = 1e8
+    p.norm_shear_omega = 0.0
     return p
 
 

@@ -77,6 +77,8 @@ def lib():
     L.nv_measure_fp32_peak.argtypes = [i32, P(C.c_double)]
     L.nv_diagnostics.argtypes = [vp, i32, P(C.c_int64), i32]
     L.nv_calc_velocity_direct_at.argtypes = [vp, i32, P(i32), i32, P(C.c_double)]
+    L.nv_set_normal_fluid_noise.argtypes = [vp, i32, P(C.c_double), i32]
+    L.nv_set_normal_fluid_grid.argtypes = [vp, i32, P(C.c_double), i32, i32, i32, P(C.c_double)]
     L.nv_calculate_diagnostics.argtypes = [vp]
     L.nv_ts_row_get.argtypes = [vp, i32, P(NvTsRow)]
     L.nv_format_ts_row.argtypes = [P(NvTsRow), i32, C.c_char_p, i32]
@@ -268,6 +270,19 @@ class Handle:
         c = st.to_full_c()
         _check(lib().nv_download_full(self.h, int(sys), C.byref(c), cap))
         return st.trimmed(c.pcount)
+
+    def set_normal_fluid_noise(self, sys: int, noise):
+        """noisey_xflow samples (one per step, wrapping)."""
+        a = np.ascontiguousarray(np.asarray(noise, dtype=np.float64))
+        _check(lib().nv_set_normal_fluid_noise(self.h, int(sys), a.ctypes.data_as(C.POINTER(C.c_double)), a.size))
+
+    def set_normal_fluid_grid(self, sys: int, u, yp=None):
+        """laizetDNS / turbDNS grid: u of shape (3, nz, ny, nx) (the file's order), yp for laizetDNS."""
+        a = np.ascontiguousarray(np.asarray(u, dtype=np.float64))
+        _, nz, ny, nx = a.shape
+        y = None if yp is None else np.ascontiguousarray(np.asarray(yp, dtype=np.float64))
+        _check(lib().nv_set_normal_fluid_grid(self.h, int(sys), a.ctypes.data_as(C.POINTER(C.c_double)), nx, ny, nz,
+                                              None if y is None else y.ctypes.data_as(C.POINTER(C.c_double))))
 
     def calculate_diagnostics(self):
         """calculate_diagnostics (src/diagnostic.f90:9-74) for every system, on the device."""

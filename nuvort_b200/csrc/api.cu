@@ -117,6 +117,20 @@ int set_device(nv_handle *h) {
   return NV_OK;
 }
 
+// A normal fluid that needs data the caller has not given (nv_set_normal_fluid_*).
+int nf_missing(const nv_handle *h) {
+  for (int s = 0; s < h->nsys; ++s) {
+    const SysConst &c = h->sc[s];
+    if (!c.mf_on) continue;
+    if (c.nf_kind == NV_NF_NOISEY_XFLOW && !c.nf_noise)
+      return set_error(NV_ERR_STATE, "noisey_xflow needs its noise samples (nv_set_normal_fluid_noise)");
+    if ((c.nf_kind == NV_NF_LAIZET_DNS || c.nf_kind == NV_NF_TURB_DNS) && !c.nf_grid)
+      return set_error(NV_ERR_STATE, "laizetDNS/turbDNS need their grid (nv_set_normal_fluid_grid)");
+  }
+  return NV_OK;
+}
+
+
 SysConst make_sysconst(const nv_params &p, int base, int cap) {
   SysConst s;
   std::memset(&s, 0, sizeof s);
@@ -140,6 +154,9 @@ SysConst make_sysconst(const nv_params &p, int base, int cap) {
   for (int c = 0; c < 3; ++c) s.super_velocity[c] = p.super_velocity[c];
   s.normal_fluid_cutoff = p.normal_fluid_cutoff;
   s.t_zero_normal_fluid = p.t_zero_normal_fluid;
+  s.nf_kind = p.normal_velocity;
+  s.nf_a = p.norm_vel_xflow;
+  s.nf_omega = p.norm_shear_omega;
   s.bsize = std::max(p.box_size[0], std::max(p.box_size[1], p.box_size[2]));
   // create_periodic_loop_array (boundary.f90:143-175): i,j,k in -1..1, k fastest.
   int n = 0;
@@ -434,6 +451,7 @@ int nv_params_default(nv_params *p) {
   p->norm_vel_xflow = 0.5;
   p->normal_fluid_cutoff = 1E8;
   p->t_zero_normal_fluid = 1E8;
+  p->norm_shear_omega = 0.;
   return NV_OK;
 }
 
@@ -451,8 +469,8 @@ int nv_check_params(const nv_params *p) {
   }
   if (p->velocity != NV_VEL_LIA && p->velocity != NV_VEL_BS && p->velocity != NV_VEL_TREE)
     return set_error(NV_ERR_ARG, "correct value for \"velocity\" in run.in has not been set");
-  if (p->normal_velocity != NV_NF_ZERO && p->normal_velocity != NV_NF_XFLOW && p->normal_velocity != NV_NF_UNIFORM)
-    return set_error(NV_ERR_UNSUPPORTED, "only zero, xflow and uniform normal fluid fields are supported");
+  if (p->normal_velocity < NV_NF_ZERO || p->normal_velocity > NV_NF_TURB_DNS)
+    return set_error(NV_ERR_ARG, "correct parameter for normal_veloctity not set");
   if (p->tree_theta > 0)
     for (int c = 0; c < 3; ++c)
       if (p->boundary[c] == NV_BC_OPEN)
@@ -549,7 +567,10 @@ int nv_create(const nv_params *params, int32_t nsys, const int32_t *capacity, in
   if (cudaMemcpy(h->sys_of, sys_of.data(), T * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
     return bail(set_error(NV_ERR_CUDA, "upload of slot map failed"));
   h->h_dyn.assign(nsys, SysDyn{});
-  for (auto &d : h->h_dyn) std::memset(&d, 0, sizeof d);
+  for (auto &d : h->h_dyn) {
+    std::memset(&d, 0, sizeof d);
+    d.noise_counter = 1;
+  }
   if (cudaMemcpy(h->d_dyn, h->h_dyn.data(), nsys * sizeof(SysDyn), cudaMemcpyHostToDevice) != cudaSuccess)
     return bail(set_error(NV_ERR_CUDA, "upload of system state failed"));
   if ((rc = rebuild_worklists(h))) return bail(rc);
@@ -569,6 +590,7 @@ int nv_destroy(nv_handle *h) {
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   tree_free(h);
   topo_free(h);
+  for (void *p : h->nf_buffers) cudaFree(p);
   void *ptrs[] = {h->usm, h->cs, h->d_drec, h->partial, h->stage, h->d_upck, h->d_sc, h->d_dyn, h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv,
                   h->closest, h->sys_of, h->seg, h->seg32, h->d_err, h->d_events, h->d_event_count,
                   h->d_work_direct, h->d_work_tree, h->d_work_lia, h->d_work_img, h->d_work_timg, h->d_work_split};
@@ -860,6 +882,7 @@ int nv_construct_tree(nv_handle *h) {
 }
 int nv_pmotion(nv_handle *h) {
   if (!h) return set_error(NV_ERR_ARG, "null handle");
+  if (nf_missing(h)) return NV_ERR_STATE;
   int rc = set_device(h);
   if (rc) return rc;
   launch_velocity(h);
@@ -916,6 +939,7 @@ int nv_end_step(nv_handle *h) {
 
 int nv_step(nv_handle *h, int32_t nsteps) {
   if (!h || nsteps < 0) return set_error(NV_ERR_ARG, "nv_step: bad arguments");
+  if (nf_missing(h)) return NV_ERR_STATE;
   int rc = set_device(h);
   if (rc || (rc = capture_step(h))) return rc;
   for (int k = 0; k < nsteps; ++k) {
@@ -984,6 +1008,73 @@ int nv_set_pclose_method(nv_handle *h, int32_t method) {
   return NV_OK;
 }
 
+// Normal-fluid data: copy to the device, point the system's constants at it.
+namespace {
+int nf_upload(nv_handle *h, const double *src, size_t n, const double **dst) {
+  void *p = nullptr;
+  NV_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(double)));
+  h->nf_buffers.push_back(p);
+  NV_CUDA(cudaMemcpy(p, src, n * sizeof(double), cudaMemcpyHostToDevice));
+  *dst = static_cast<const double *>(p);
+  return NV_OK;
+}
+int sc_refresh(nv_handle *h, int sys) {
+  NV_CUDA(cudaMemcpy(h->d_sc + sys, &h->sc[sys], sizeof(SysConst), cudaMemcpyHostToDevice));
+  h->graph_valid = false;
+  return NV_OK;
+}
+}  // namespace
+
+int nv_set_normal_fluid_noise(nv_handle *h, int32_t sys, const double *noise, int32_t n) {
+  if (!h || sys < 0 || sys >= h->nsys || !noise || n < 1)
+    return set_error(NV_ERR_ARG, "nv_set_normal_fluid_noise: bad arguments");
+  int rc = set_device(h);
+  if (rc || (rc = nf_upload(h, noise, (size_t)n, &h->sc[sys].nf_noise))) return rc;
+  h->sc[sys].nf_noise_n = n;
+  return sc_refresh(h, sys);
+}
+
+int nv_set_normal_fluid_grid(nv_handle *h, int32_t sys, const double *u, int32_t nx, int32_t ny, int32_t nz,
+                             const double *yp) {
+  if (!h || sys < 0 || sys >= h->nsys || !u) return set_error(NV_ERR_ARG, "nv_set_normal_fluid_grid: bad arguments");
+  SysConst &sc = h->sc[sys];
+  const bool laizet = sc.nf_kind == NV_NF_LAIZET_DNS;
+  if (!laizet && sc.nf_kind != NV_NF_TURB_DNS)
+    return set_error(NV_ERR_STATE, "nv_set_normal_fluid_grid: the system's normal_velocity is not laizetDNS or turbDNS");
+  if (laizet ? (nx != 128 || ny != 129 || nz != 84 || !yp) : (nx != 256 || ny != 256 || nz != 256))
+    return set_error(NV_ERR_ARG, "nv_set_normal_fluid_grid: laizetDNS takes 128x129x84 and yp, turbDNS 256^3");
+  int rc = set_device(h);
+  if (rc) return rc;
+  const size_t nn = (size_t)nx * ny * nz;
+  std::vector<double> g(u, u + 3 * nn);
+  if (laizet)
+    for (auto &v : g) v = v / 2.;  // laizet_u=laizet_u/2. (normal_fluid.f90:178)
+  std::vector<double> ax[3];
+  const double pi = NV_PI;
+  ax[0].resize(nx);
+  ax[1].resize(ny);
+  ax[2].resize(nz);
+  if (laizet) {  // setup_laizet (normal_fluid.f90:183-189)
+    for (int i = 1; i <= nx; ++i) ax[0][i - 1] = (i - 1) * (1. / 128) * 4 * pi - 2 * pi;
+    for (int j = 0; j < ny; ++j) ax[1][j] = yp[j];
+    for (int i = 1; i <= nz; ++i) ax[2][i - 1] = (i - 1) * (1. / 84) * 4 * pi / 3 - 4 * pi / 6;
+    sc.nf_step[0] = (1. / 128) * 4 * pi;
+    sc.nf_step[1] = 0.;
+    sc.nf_step[2] = (1. / 84) * 4 * pi / 3;
+  } else {  // setup_turbDNS (normal_fluid.f90:203-214)
+    for (int a = 0; a < 3; ++a) {
+      for (int i = 1; i <= 256; ++i) ax[a][i - 1] = (i - 1) * (1. / 256) * sc.box[a] - sc.box[a] / 2.;
+      sc.nf_step[a] = (1. / 256) * sc.box[a];
+    }
+  }
+  if ((rc = nf_upload(h, g.data(), g.size(), &sc.nf_grid))) return rc;
+  for (int a = 0; a < 3; ++a) {
+    if ((rc = nf_upload(h, ax[a].data(), ax[a].size(), &sc.nf_axis[a]))) return rc;
+    sc.nf_n[a] = (int)ax[a].size();
+  }
+  return sc_refresh(h, sys);
+}
+
 int nv_set_insert_iterations(nv_handle *h, int32_t n) {
   if (!h || n < 0 || n > 64) return set_error(NV_ERR_ARG, "nv_set_insert_iterations: n must be 0..64");
   h->ins_iters = n;
@@ -1007,6 +1098,7 @@ int nv_step_launches(nv_handle *h, int32_t *n) {
 
 int nv_calc_velocity(nv_handle *h, int32_t sys, double *u3) {
   if (!h || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_calc_velocity: bad arguments");
+  if (nf_missing(h)) return NV_ERR_STATE;
   int rc = set_device(h);
   if (rc) return rc;
   time_begin(h, ST_GHOST);

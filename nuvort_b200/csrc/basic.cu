@@ -83,7 +83,7 @@ __global__ void k_velocity_lia(const SysConst *__restrict__ scs, const SysDyn *_
   load3(GI, T, g, gi);
   load3(GB, T, g, gb);
   local_velocity(sc, x, gi, gb, u, fdot);
-  mf_epilogue(sc, dyn[w.x].t, fdot, u, g);
+  mf_epilogue(sc, dyn[w.x], x, fdot, u, g);
   store3(U, T, g, u);
 }
 
@@ -148,6 +148,16 @@ __global__ void k_wrap(const SysConst *__restrict__ scs, const SysDyn *__restric
   if ((mode & 2) && sc.nan_test && (isnan(x[0]) || isnan(x[1]) || isnan(x[2]))) set_err(err, DERR_NAN);
 }
 
+// randomise_normal_fluid (normal_fluid.f90:340-348), at the end of pmotion: the next noise
+// sample, wrapping after the last.
+__global__ void k_nf_advance(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, const unsigned *err) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys || *err || scs[s].nf_kind != NV_NF_NOISEY_XFLOW) return;
+  int c = dyn[s].noise_counter + 1;
+  if (c > scs[s].nf_noise_n) c = 1;
+  dyn[s].noise_counter = c;
+}
+
 __global__ void k_end_step(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, const unsigned *err) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys || *err) return;
@@ -193,6 +203,9 @@ void launch_velocity(nv_handle *h) {
 void launch_ab3(nv_handle *h) {
   k_ab3<<<grid_for(h->T, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->nxt, h->x, h->u, h->u1,
                                                    h->u2, h->T, h->d_err);
+  bool noise = false;
+  for (auto &s : h->sc) noise |= s.nf_kind == NV_NF_NOISEY_XFLOW;
+  if (noise) k_nf_advance<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, h->d_err);
 }
 
 // mode bit 1: periodic wrap; bit 2: NaN check.

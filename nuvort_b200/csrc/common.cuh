@@ -58,6 +58,16 @@ struct SysConst {
   // components 0-2 u_sup, 3-5 u_mf; null where they are not kept
   double *usm;
   long long usm_T;
+  // position-dependent normal fluid (normal_fluid.f90:83-118); vn above serves zero / xflow /
+  // uniform
+  int nf_kind;                 // NV_NF_*
+  double nf_a, nf_omega;       // norm_vel_xflow, norm_shear_omega
+  const double *nf_noise;      // noisey_xflow samples
+  int nf_noise_n;
+  const double *nf_grid;       // laizetDNS / turbDNS: u [3][nz][ny][nx]
+  const double *nf_axis[3];    // xp, yp, zp
+  int nf_n[3];
+  double nf_step[3];           // grid spacing of the interpolation weights (y of laizet: 0, from yp)
 };
 
 struct SysDyn {
@@ -75,6 +85,7 @@ struct SysDyn {
   int ins_fallback;  // pinsert needs the serial sweep this step
   int ins_conv;      // pinsert's fixed-point iteration has converged
   int ins_mismatch;  // positions where the iteration's H and H' differ
+  int noise_counter; // noisey_xflow: 1-based sample in use (xflow_noise_counter)
   long long diag[12];  // see nv_diagnostics
   double total_length;  // pinsert: sum of the segment lengths it measured (line.f90:39)
   double avg_sep;       // pinsert: total_length / (old_pcount - empty slots) (line.f90:95)
@@ -198,19 +209,123 @@ __device__ __forceinline__ void local_velocity(const SysConst &sc, const double 
   for (int c = 0; c < 3; ++c) u[c] = e_mul(beta, cr[c]);
 }
 
-// Mutual friction and imposed flow (timestep.f90:123-140); u holds u_sup on entry.  For the
-// velocity pass of a step (slot g >= 0) u_sup and u_mf are kept as the reference stores them
-// in f(g) (u_mf only when it is computed); g < 0 keeps nothing.
-__device__ __forceinline__ void mf_epilogue(const SysConst &sc, double t, const double fdot[3],
-                                            double u[3], long long g = -1) {
+// Grid node of a coordinate for the DNS interpolation (laizet_interp / turbDNS_interp,
+// normal_fluid.f90:225-338): n = minloc(|x - axis|) (the first on a tie); if x lies above it
+// the pair is (n, n+1), else (n-1, n); n+1 past the last node wraps to the first on a
+// periodic axis.  Positions below the first node (the reference then reads index 0, outside
+// its array) wrap to the last node on a periodic axis, clamp on a closed one.
+__device__ __forceinline__ void grid_pair(const double *__restrict__ ax, int n, double x, bool periodic, int &lo,
+                                          int &hi) {
+  int best = 0;
+  double bd = fabs(x - ax[0]);
+  for (int i = 1; i < n; ++i) {
+    const double d = fabs(x - ax[i]);
+    if (d < bd) {
+      bd = d;
+      best = i;
+    }
+  }
+  if (x > ax[best]) {
+    lo = best;
+    hi = best + 1;
+  } else {
+    lo = best - 1;
+    hi = best;
+  }
+  if (lo < 0) lo = periodic ? n - 1 : 0;
+  if (hi >= n) hi = periodic ? 0 : n - 1;
+}
+
+// get_normal_velocity (normal_fluid.f90:83-118) at x and time t, +super_velocity; un must be
+// the field the caller uses when t < t_zero_normal_fluid.
+__device__ __forceinline__ void normal_velocity(const SysConst &sc, int noise_counter, const double x[3], double t,
+                                                double un[3]) {
+  switch (sc.nf_kind) {
+    case NV_NF_SHEAR_XFLOW:  // :98-99
+      un[0] = e_mul(sc.nf_a, sin(e_add(e_div(e_mul(2 * NV_PI, x[2]), sc.box[2]), e_mul(t, sc.nf_omega))));
+      un[1] = un[2] = 0.0;
+      break;
+    case NV_NF_YCHANNEL: {  // :100-101
+      const double q = e_div(e_mul(2.0, x[1]), sc.box[1]);
+      un[0] = e_mul(sc.nf_a, e_sub(1.0, e_mul(q, q)));
+      un[1] = un[2] = 0.0;
+      break;
+    }
+    case NV_NF_CHANNEL: {  // :102-108
+      double cossum = 0.0;
+      for (int ii = 1; ii <= 10; ++ii) {
+        const double ak = e_mul((double)(2 * ii - 1), e_div(NV_PI, 2.0));
+        const double sgn = (ii & 1) ? -1.0 : 1.0;  // (-1)**ii
+        const double ak3 = e_mul(e_mul(ak, ak), ak);
+        const double ch = cosh(e_div(e_mul(e_mul(ak, 2.0), x[1]), sc.box[1]));
+        const double co = cos(e_div(e_mul(e_mul(ak, 2.0), x[2]), sc.box[2]));
+        cossum = e_add(cossum, e_div(e_mul(e_mul(4.0, e_div(sgn, ak3)), e_mul(ch, co)), cosh(ak)));
+      }
+      const double q = e_div(e_mul(2.0, x[2]), sc.box[2]);
+      un[0] = e_mul(e_mul(sc.nf_a, e_add(e_sub(1.0, e_mul(q, q)), cossum)), 1.2);
+      un[1] = un[2] = 0.0;
+      break;
+    }
+    case NV_NF_NOISEY_XFLOW:  // :96-97 with the sample of this step (no samples: no flow)
+      un[0] = sc.nf_noise ? e_mul(sc.nf_noise[noise_counter - 1], sc.nf_a) : 0.0;
+      un[1] = un[2] = 0.0;
+      break;
+    case NV_NF_LAIZET_DNS:
+    case NV_NF_TURB_DNS: {  // :225-338 trilinear interpolation (no grid: no flow)
+      if (!sc.nf_grid) {
+        un[0] = un[1] = un[2] = 0.0;
+        break;
+      }
+      const bool turb = sc.nf_kind == NV_NF_TURB_DNS;
+      int lo[3], hi[3];
+      for (int a = 0; a < 3; ++a) grid_pair(sc.nf_axis[a], sc.nf_n[a], x[a], turb || a != 1, lo[a], hi[a]);
+      const double xd = e_div(e_sub(x[0], sc.nf_axis[0][lo[0]]), sc.nf_step[0]);
+      const double yd = turb ? e_div(e_sub(x[1], sc.nf_axis[1][lo[1]]), sc.nf_step[1])
+                             : e_div(e_sub(x[1], sc.nf_axis[1][lo[1]]), e_sub(sc.nf_axis[1][hi[1]], sc.nf_axis[1][lo[1]]));
+      const double zd = e_div(e_sub(x[2], sc.nf_axis[2][lo[2]]), sc.nf_step[2]);
+      const long long nx = sc.nf_n[0], nxy = (long long)sc.nf_n[0] * sc.nf_n[1], nn = nxy * sc.nf_n[2];
+      auto at = [&](int i, int j, int k, int c) { return sc.nf_grid[c * nn + k * nxy + j * nx + i]; };
+      for (int c = 0; c < 3; ++c) {
+        const double c00 = e_add(e_mul(at(lo[0], lo[1], lo[2], c), e_sub(1.0, xd)), e_mul(at(hi[0], lo[1], lo[2], c), xd));
+        const double c10 = e_add(e_mul(at(lo[0], hi[1], lo[2], c), e_sub(1.0, xd)), e_mul(at(hi[0], hi[1], lo[2], c), xd));
+        const double c01 = e_add(e_mul(at(lo[0], lo[1], hi[2], c), e_sub(1.0, xd)), e_mul(at(hi[0], lo[1], hi[2], c), xd));
+        const double c11 = e_add(e_mul(at(lo[0], hi[1], hi[2], c), e_sub(1.0, xd)), e_mul(at(hi[0], hi[1], hi[2], c), xd));
+        const double c0 = e_add(e_mul(c00, e_sub(1.0, yd)), e_mul(c10, yd));
+        const double c1 = e_add(e_mul(c01, e_sub(1.0, yd)), e_mul(c11, yd));
+        un[c] = e_add(e_mul(c0, e_sub(1.0, zd)), e_mul(c1, zd));
+      }
+      break;
+    }
+    default:  // zero, xflow, uniform: a constant field
+      for (int c = 0; c < 3; ++c) un[c] = e_sub(sc.vn[c], sc.super_velocity[c]);
+  }
+  for (int c = 0; c < 3; ++c) un[c] = e_add(un[c], sc.super_velocity[c]);  // :117
+}
+
+// Mutual friction and imposed flow (timestep.f90:123-140); u holds u_sup on entry, x is the
+// point's position (the normal fluid's argument).  For the velocity pass of a step (slot
+// g >= 0) u_sup and u_mf are kept as the reference stores them in f(g) (u_mf only when it is
+// computed); g < 0 keeps nothing.
+__device__ __forceinline__ void mf_epilogue(const SysConst &sc, const SysDyn &dy, const double x[3],
+                                            const double fdot[3], double u[3], long long g = -1) {
+  const double t = dy.t;
   const bool keep = sc.usm && g >= 0;
   if (keep)
 #pragma unroll
     for (int c = 0; c < 3; ++c) sc.usm[c * sc.usm_T + g] = u[c];
   if (sc.mf_on && t < sc.normal_fluid_cutoff) {
     double un[3], w[3], c1[3], c2[3], umf[3];
+    if (t < sc.t_zero_normal_fluid) {
+      if (sc.nf_kind <= NV_NF_UNIFORM) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) un[c] = (t < sc.t_zero_normal_fluid) ? sc.vn[c] : 0.0;
+        for (int c = 0; c < 3; ++c) un[c] = sc.vn[c];
+      } else {
+        normal_velocity(sc, dy.noise_counter, x, t, un);
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) un[c] = 0.0;
+    }
 #pragma unroll
     for (int c = 0; c < 3; ++c) w[c] = e_sub(un[c], u[c]);
     cross3(fdot, w, c1);

@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(64) k_direct_fp64(
   for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], ub0[c]);
 #pragma unroll
   for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], ubs[c]);
-  mf_epilogue(sc, dyn[w.x].t, fdot, u, targets ? -1 : g);
+  mf_epilogue(sc, dyn[w.x], xi, fdot, u, targets ? -1 : g);
   if (targets) {
     const int idx = w.y + tid;
     for (int c = 0; c < 3; ++c) Uout[3 * (long long)idx + c] = u[c];
@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(128) k_direct_fp64_split(
   for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], s_sum[tid][c][0]);
 #pragma unroll
   for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], s_sum[tid][c][1]);
-  mf_epilogue(sc, dyn[w.x].t, fdot, u, targets ? -1 : g);
+  mf_epilogue(sc, dyn[w.x], xi, fdot, u, targets ? -1 : g);
   if (targets) {
     const int idx = w.y + tid;
     for (int c = 0; c < 3; ++c) Uout[3 * (long long)idx + c] = u[c];

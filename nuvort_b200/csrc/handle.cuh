@@ -36,6 +36,7 @@ struct nv_handle {
   double4 *seg = nullptr;   // FP64 segment records, 2 per slot
   float4 *seg32 = nullptr;  // FP32 segment records, 3 per slot (mixed precision)
   double *partial = nullptr; // per-image partial sums [image][component][slot] (mixed precision)
+  std::vector<void *> nf_buffers;  // normal-fluid noise and grid data (nv_set_normal_fluid_*)
   double *usm = nullptr;     // f(:)%u_sup, f(:)%u_mf of the last velocity pass [6][T]
   double *cs = nullptr;      // f(:)%curv, f(:)%stretch of the last diagnostics [2][T]
   struct DiagRec *d_drec = nullptr;  // per system: the last diagnostics' reductions

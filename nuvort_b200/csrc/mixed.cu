@@ -197,7 +197,7 @@ __global__ void k_mixed_combine(const SysConst *__restrict__ scs, const SysDyn *
   for (int m = 1; m <= sc.n_shift; ++m)
     for (int c = 0; c < 3; ++c) bs[c] += partial[((long long)m * 3 + c) * T + g];
   for (int c = 0; c < 3; ++c) u[c] = e_add(e_add(u[c], b0[c]), bs[c]);
-  mf_epilogue(sc, dyn[w.x].t, fdot, u, g);
+  mf_epilogue(sc, dyn[w.x], xi, fdot, u, g);
   store3(U, T, g, u);
 }
 

@@ -164,10 +164,20 @@ extern "C" int nv_read_run_file(const char *path, nv_params *p) {
     else if (label == "tree_extra_correction") ok = read_logical(&p->tree_extra_correction);
     else if (label == "normal_velocity") {
       ok = read_string(sv);
-      if (ok) p->normal_velocity = sv == "zero" ? NV_NF_ZERO : sv == "xflow" ? NV_NF_XFLOW : sv == "uniform" ? NV_NF_UNIFORM : 100;
+      if (ok)
+        p->normal_velocity = sv == "zero" ? NV_NF_ZERO : sv == "xflow" ? NV_NF_XFLOW : sv == "uniform" ? NV_NF_UNIFORM
+                           : sv == "shear_xflow"  ? NV_NF_SHEAR_XFLOW
+                           : sv == "channel"      ? NV_NF_CHANNEL
+                           : sv == "ychannel"     ? NV_NF_YCHANNEL
+                           : sv == "noisey_xflow" ? NV_NF_NOISEY_XFLOW
+                           : sv == "laizetDNS"    ? NV_NF_LAIZET_DNS
+                           : sv == "turbDNS"      ? NV_NF_TURB_DNS
+                                                  : 100;
     } else if (label == "normal_fluid_cutoff") ok = read_reals(&p->normal_fluid_cutoff, 1);
     else if (label == "t_zero_normal_fluid") ok = read_reals(&p->t_zero_normal_fluid, 1);
     else if (label == "norm_vel_xflow") ok = read_reals(&p->norm_vel_xflow, 1);
+    else if (label == "norm_shear_omega") ok = read_reals(&p->norm_shear_omega, 1);
+    else if (label == "noise_file") ok = read_string(sv);  // the caller loads it: nv_set_normal_fluid_noise
     else if (label == "alpha") ok = read_reals(p->alpha, 2);
     else if (label == "super_velocity") ok = read_reals(p->super_velocity, 3);
     else if (label == "initf") ok = read_string(sv);

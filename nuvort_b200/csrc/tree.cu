@@ -936,7 +936,7 @@ __device__ void fp64_epilogue(const SysConst &sc, const SysDyn &dy, int g, const
   for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], ub0[c]);
 #pragma unroll
   for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], ubs[c]);
-  mf_epilogue(sc, dy.t, fdot, u, g);
+  mf_epilogue(sc, dy, xi, fdot, u, g);
   store3(U, T, g, u);
 }
 

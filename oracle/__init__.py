@@ -60,6 +60,8 @@ def lib():
         L.or_calc_velocity.argtypes = [vp, P(C.c_double)]
         L.or_calc_velocity_targets.argtypes = [vp, C.c_int32, P(C.c_int32), C.c_int32, P(C.c_double)]
         L.or_tree_dump.argtypes = [vp, P(NvTreeNode), C.c_int32, P(C.c_int32)]
+        L.or_set_normal_fluid_noise.argtypes = [vp, P(C.c_double), C.c_int32]
+        L.or_set_normal_fluid_grid.argtypes = [vp, P(C.c_double), C.c_int32, C.c_int32, C.c_int32, P(C.c_double)]
         L.or_calculate_diagnostics.argtypes = [vp]
         L.or_ts_row_get.argtypes = [vp, P(NvTsRow)]
         L.or_download_full.argtypes = [vp, P(NvFullState), C.c_int32]
@@ -160,6 +162,17 @@ class Oracle:
         _check(lib().or_calc_velocity_targets(self.h, int(velocity), tg.ctypes.data_as(C.POINTER(C.c_int32)),
                                               tg.shape[0], u.ctypes.data_as(C.POINTER(C.c_double))))
         return u
+
+    def set_normal_fluid_noise(self, noise):
+        a = np.ascontiguousarray(np.asarray(noise, dtype=np.float64))
+        _check(lib().or_set_normal_fluid_noise(self.h, a.ctypes.data_as(C.POINTER(C.c_double)), a.size))
+
+    def set_normal_fluid_grid(self, u, yp=None):
+        a = np.ascontiguousarray(np.asarray(u, dtype=np.float64))
+        _, nz, ny, nx = a.shape
+        y = None if yp is None else np.ascontiguousarray(np.asarray(yp, dtype=np.float64))
+        _check(lib().or_set_normal_fluid_grid(self.h, a.ctypes.data_as(C.POINTER(C.c_double)), nx, ny, nz,
+                                              None if y is None else y.ctypes.data_as(C.POINTER(C.c_double))))
 
     def calculate_diagnostics(self):
         _check(lib().or_calculate_diagnostics(self.h))

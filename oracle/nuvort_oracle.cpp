@@ -283,16 +283,103 @@ struct Sys {
     }
   }
 
-  // ---- normal_fluid.f90:83-118 get_normal_velocity (zero / xflow / uniform) ---------------
+  // ---- normal_fluid.f90:83-118 get_normal_velocity -------------------------------------
+  // noisey_xflow samples (load_noise :156-162) and the counter randomise_normal_fluid advances
+  std::vector<double> xflow_noise;
+  int xflow_noise_counter = 1;
+  // laizetDNS / turbDNS grid (setup_laizet :164-190, setup_turbDNS :192-216), Fortran order
+  std::vector<double> laizet_u, xp, yp, zp;
+  int gn[3] = {0, 0, 0};
+
+  double grid_u(int i, int j, int k, int c) const {  // laizet_u(i,j,k,c), 1-based
+    return laizet_u[(size_t)(i - 1) + (size_t)gn[0] * ((j - 1) + (size_t)gn[1] * ((k - 1) + (size_t)gn[2] * (c - 1)))];
+  }
+  // nearest node by minloc(abs(x-axis)) (first on a tie), then the bracketing pair; the index
+  // the reference would take below the first node (0, outside its array) wraps on a periodic
+  // axis and clamps on a closed one, as the library does
+  static void pair_of(const std::vector<double> &ax, double x, bool periodic, int &n, int &nn) {
+    const int m = (int)ax.size();
+    n = 1;
+    for (int i = 2; i <= m; ++i)
+      if (std::fabs(x - ax[i - 1]) < std::fabs(x - ax[n - 1])) n = i;
+    if (x > ax[n - 1]) {
+      nn = n + 1;
+    } else {
+      n = n - 1;
+      nn = n + 1;
+    }
+    if (n < 1) n = periodic ? m : 1;
+    if (nn > m) nn = periodic ? 1 : m;
+  }
+  void dns_interp(const double *x, double *u, bool turb) const {  // :225-338
+    int nx, nnx, ny, nny, nz, nnz;
+    pair_of(xp, x[0], true, nx, nnx);
+    pair_of(yp, x[1], turb, ny, nny);
+    pair_of(zp, x[2], true, nz, nnz);
+    double xd, yd, zd;
+    if (turb) {
+      xd = (x[0] - xp[nx - 1]) / ((1. / 256) * p.box_size[0]);
+      yd = (x[1] - yp[ny - 1]) / ((1. / 256) * p.box_size[1]);
+      zd = (x[2] - zp[nz - 1]) / ((1. / 256) * p.box_size[2]);
+    } else {
+      xd = (x[0] - xp[nx - 1]) / ((1. / 128) * 4 * pi);
+      yd = (x[1] - yp[ny - 1]) / (yp[nny - 1] - yp[ny - 1]);
+      zd = (x[2] - zp[nz - 1]) / ((1. / 84) * 4 * pi / 3);
+    }
+    for (int c = 1; c <= 3; ++c) {
+      const double c00 = grid_u(nx, ny, nz, c) * (1 - xd) + grid_u(nnx, ny, nz, c) * xd;
+      const double c10 = grid_u(nx, nny, nz, c) * (1 - xd) + grid_u(nnx, nny, nz, c) * xd;
+      const double c01 = grid_u(nx, ny, nnz, c) * (1 - xd) + grid_u(nnx, ny, nnz, c) * xd;
+      const double c11 = grid_u(nx, nny, nnz, c) * (1 - xd) + grid_u(nnx, nny, nnz, c) * xd;
+      const double c0 = c00 * (1 - yd) + c10 * yd;
+      const double c1 = c01 * (1 - yd) + c11 * yd;
+      u[c - 1] = c0 * (1 - zd) + c1 * zd;
+    }
+  }
   void get_normal_velocity(const double *x, double *u) const {
-    (void)x;
     u[0] = u[1] = u[2] = 0.0;
-    if (p.normal_velocity == NV_NF_XFLOW) {
-      u[0] = p.norm_vel_xflow;
-    } else if (p.normal_velocity == NV_NF_UNIFORM) {
-      u[0] = p.norm_vel_vec[0]; u[1] = p.norm_vel_vec[1]; u[2] = p.norm_vel_vec[2];
+    switch (p.normal_velocity) {
+      case NV_NF_XFLOW:
+        u[0] = p.norm_vel_xflow;
+        break;
+      case NV_NF_UNIFORM:  // the library's extension
+        u[0] = p.norm_vel_vec[0]; u[1] = p.norm_vel_vec[1]; u[2] = p.norm_vel_vec[2];
+        break;
+      case NV_NF_NOISEY_XFLOW:
+        u[0] = xflow_noise.empty() ? 0.0 : xflow_noise[xflow_noise_counter - 1] * p.norm_vel_xflow;
+        break;
+      case NV_NF_SHEAR_XFLOW:
+        u[0] = p.norm_vel_xflow * std::sin(2 * pi * x[2] / p.box_size[2] + t * p.norm_shear_omega);
+        break;
+      case NV_NF_YCHANNEL:
+        u[0] = p.norm_vel_xflow * (1. - sq(2. * x[1] / p.box_size[1]));
+        break;
+      case NV_NF_CHANNEL: {
+        double cossum = 0.0;
+        for (int ii = 1; ii <= 10; ++ii) {
+          const double ak = (2 * ii - 1) * (pi / 2);
+          const double m1 = (ii % 2) ? -1.0 : 1.0;  // (-1)**ii
+          cossum = cossum + 4 * (m1 / (ak * ak * ak)) *
+                                (std::cosh(ak * 2 * x[1] / p.box_size[1]) * std::cos(ak * 2 * x[2] / p.box_size[2])) /
+                                std::cosh(ak);
+        }
+        u[0] = p.norm_vel_xflow * (1. - sq(2 * x[2] / p.box_size[2]) + cossum) * 1.2;
+        break;
+      }
+      case NV_NF_LAIZET_DNS:
+      case NV_NF_TURB_DNS:
+        if (!laizet_u.empty()) dns_interp(x, u, p.normal_velocity == NV_NF_TURB_DNS);
+        break;
+      default:
+        break;
     }
     for (int c = 0; c < 3; ++c) u[c] = u[c] + p.super_velocity[c];
+  }
+  void randomise_normal_fluid() {  // :340-348
+    if (p.normal_velocity == NV_NF_NOISEY_XFLOW && !xflow_noise.empty()) {
+      xflow_noise_counter = xflow_noise_counter + 1;
+      if (xflow_noise_counter > (int)xflow_noise.size()) xflow_noise_counter = 1;
+    }
   }
 
   // ---- timestep.f90:49-141 calc_velocity --------------------------------------------------
@@ -384,6 +471,7 @@ struct Sys {
       }
       for (int c = 0; c < 3; ++c) { q.u2[c] = q.u1[c]; q.u1[c] = q.u[c]; }
     }
+    randomise_normal_fluid();  // timestep.f90:44
     return NV_OK;
   }
 
@@ -851,6 +939,34 @@ int or_counters_get(or_handle *h, nv_counters *c) {
   c->itime = s.itime;
   c->n_events = (int32_t)s.events.size();
   c->t = s.t;
+  return NV_OK;
+}
+
+int or_set_normal_fluid_noise(or_handle *h, const double *noise, int32_t n) {
+  if (!h || !noise || n < 1) return fail(NV_ERR_ARG, "bad noise");
+  h->s.xflow_noise.assign(noise, noise + n);
+  h->s.xflow_noise_counter = 1;
+  return NV_OK;
+}
+
+int or_set_normal_fluid_grid(or_handle *h, const double *u, int32_t nx, int32_t ny, int32_t nz, const double *yp) {
+  Sys &s = h->s;
+  const bool laizet = s.p.normal_velocity == NV_NF_LAIZET_DNS;
+  const size_t nn = (size_t)nx * ny * nz;
+  s.laizet_u.assign(u, u + 3 * nn);
+  if (laizet)
+    for (auto &v : s.laizet_u) v = v / 2.;  // setup_laizet: laizet_u=laizet_u/2.
+  s.gn[0] = nx; s.gn[1] = ny; s.gn[2] = nz;
+  s.xp.resize(nx); s.yp.resize(ny); s.zp.resize(nz);
+  if (laizet) {
+    for (int i = 1; i <= nx; ++i) s.xp[i - 1] = (i - 1) * (1. / 128) * 4 * pi - 2 * pi;
+    for (int j = 0; j < ny; ++j) s.yp[j] = yp[j];
+    for (int i = 1; i <= nz; ++i) s.zp[i - 1] = (i - 1) * (1. / 84) * 4 * pi / 3 - 4 * pi / 6;
+  } else {
+    for (int i = 1; i <= nx; ++i) s.xp[i - 1] = (i - 1) * (1. / 256) * s.p.box_size[0] - s.p.box_size[0] / 2.;
+    for (int i = 1; i <= ny; ++i) s.yp[i - 1] = (i - 1) * (1. / 256) * s.p.box_size[1] - s.p.box_size[1] / 2.;
+    for (int i = 1; i <= nz; ++i) s.zp[i - 1] = (i - 1) * (1. / 256) * s.p.box_size[2] - s.p.box_size[2] / 2.;
+  }
   return NV_OK;
 }
 

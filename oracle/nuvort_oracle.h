@@ -67,6 +67,9 @@ int or_calc_velocity(or_handle *h, double *u3);
  * Used as the FP64 direct-sum error oracle on subsamples and for the CPU baseline. */
 int or_calc_velocity_targets(or_handle *h, int32_t velocity, const int32_t *targets,
                              int32_t n, double *u3);
+/* Data of the file-based normal fluids, as nv_set_normal_fluid_noise / _grid take it. */
+int or_set_normal_fluid_noise(or_handle *h, const double *noise, int32_t n);
+int or_set_normal_fluid_grid(or_handle *h, const double *u, int32_t nx, int32_t ny, int32_t nz, const double *yp);
 /* calculate_diagnostics (src/diagnostic.f90:9-74) and the values print_info writes
  * (src/output.f90:20-44), with sequential sums as the reference's sum intrinsic makes them. */
 int or_calculate_diagnostics(or_handle *h);

@@ -95,3 +95,15 @@ def test_run_in_uniform_extension(tmp_path):
     f.write_text("normal_velocity uniform\nnorm_vel_vec 0 0 0.5\n")
     p = api.read_run_file(str(f))
     assert p.normal_velocity == NV_NF_UNIFORM and list(p.norm_vel_vec) == [0.0, 0.0, 0.5]
+
+
+def test_run_in_normal_fluid_fields(tmp_path):
+    from nuvort_b200.abi import NV_NF_SHEAR_XFLOW, NV_NF_TURB_DNS
+    from nuvort_b200.api import read_run_file
+    f = tmp_path / "run.in"
+    f.write_text("normal_velocity shear_xflow\nnorm_shear_omega 3.5\nnoise_file noise/wn_snr_25.log\n"
+                 "norm_vel_xflow 0.25\n")
+    p = read_run_file(str(f))
+    assert p.normal_velocity == NV_NF_SHEAR_XFLOW and p.norm_shear_omega == 3.5 and p.norm_vel_xflow == 0.25
+    f.write_text("normal_velocity turbDNS\n")
+    assert read_run_file(str(f)).normal_velocity == NV_NF_TURB_DNS
