@@ -57,3 +57,45 @@ def test_shard_balances_quadratic_work():
     # greedy longest-first: no rank exceeds the largest system or 4/3 of the mean load
     assert max(loads) <= max(max(c ** 2 for c in counts), 4 / 3 * sum(loads) / 3)
     assert shard_systems(counts, 1, 0) == list(range(6))
+
+
+def _bench_worker(rank, world, port, q):
+    import datetime
+    import sys
+
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    params, states, cfg = bench.workload("ensemble512", rank, crossover=3000, world=world)
+    mine = sorted((st.pcount, round(p.alpha[0], 12)) for p, st in zip(params, states))
+    _, (pts,) = reduce_max_sum(dist, "cpu", [0.0], [float(sum(st.pcount for st in states))])
+    q.put((rank, mine, pts, cfg["points"]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_bench_ensemble_split_over_two_gloo_ranks():
+    # bench.py --gpus 2 splits ONE ensemble: the two ranks' systems reassemble it exactly
+    # (no system twice, none lost) and the summed points are the whole ensemble's
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    params, states, cfg = bench.workload("ensemble512", 0, crossover=3000, world=1)
+    whole = sorted((st.pcount, round(p.alpha[0], 12)) for p, st in zip(params, states))
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_bench_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=300) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (_, m0, pts0, tot0), (_, m1, pts1, tot1) = res
+    assert len(m0) > 0 and len(m1) > 0
+    assert sorted(m0 + m1) == whole
+    assert pts0 == pts1 == float(sum(st.pcount for st in states)) == tot0 == tot1 == cfg["points"]
