@@ -44,6 +44,14 @@ module nuvort_gpu
     integer(c_int64_t) :: event_hash  ! unsigned on the C side; compare bit patterns only
   end type
 
+  !> one data/ts.log row (print_info) and the values behind it
+  type, bind(c) :: nv_ts_row
+    integer(c_int32_t) :: itime, live, recon_count, wall_recon_count, remove_count, reserved
+    integer(c_int64_t) :: tree_eval
+    real(c_double) :: t, delta, avg_sep, total_length, maxu, maxdu, mean_u_sup, mean_u_mf
+    real(c_double) :: kappa_bar, kappa_min, kappa_max
+  end type
+
   interface
     integer(c_int) function nv_params_default(p) bind(c, name='nv_params_default')
       import :: c_int, nv_params
@@ -134,6 +142,53 @@ module nuvort_gpu
     integer(c_int) function nv_end_step(h) bind(c, name='nv_end_step')
       import :: c_int, c_ptr
       type(c_ptr), value :: h
+    end function
+    integer(c_int) function nv_calculate_diagnostics(h) bind(c, name='nv_calculate_diagnostics')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function nv_ts_row_get(h, sys, row) bind(c, name='nv_ts_row_get')
+      import :: c_int, c_int32_t, c_ptr, nv_ts_row
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: sys
+      type(nv_ts_row), intent(out) :: row
+    end function
+    integer(c_int) function nv_format_ts_row(row, shots, buf, cap) bind(c, name='nv_format_ts_row')
+      import :: c_int, c_int32_t, c_char, nv_ts_row
+      type(nv_ts_row), intent(in) :: row
+      integer(c_int32_t), value :: shots, cap
+      character(kind=c_char), dimension(*), intent(out) :: buf
+    end function
+    integer(c_int) function nv_write_snapshot(h, sys, path) bind(c, name='nv_write_snapshot')
+      import :: c_int, c_int32_t, c_ptr, c_char
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: sys
+      character(kind=c_char), dimension(*), intent(in) :: path
+    end function
+    integer(c_int) function nv_write_dump(h, sys, path) bind(c, name='nv_write_dump')
+      import :: c_int, c_int32_t, c_ptr, c_char
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: sys
+      character(kind=c_char), dimension(*), intent(in) :: path
+    end function
+    integer(c_int) function nv_restore_dump(h, sys, path) bind(c, name='nv_restore_dump')
+      import :: c_int, c_int32_t, c_ptr, c_char
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: sys
+      character(kind=c_char), dimension(*), intent(in) :: path
+    end function
+    integer(c_int) function nv_set_normal_fluid_noise(h, sys, noise, n) bind(c, name='nv_set_normal_fluid_noise')
+      import :: c_int, c_int32_t, c_ptr, c_double
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: sys, n
+      real(c_double), dimension(*), intent(in) :: noise
+    end function
+    integer(c_int) function nv_set_normal_fluid_grid(h, sys, u, nx, ny, nz, yp) &
+        bind(c, name='nv_set_normal_fluid_grid')
+      import :: c_int, c_int32_t, c_ptr, c_double
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: sys, nx, ny, nz
+      real(c_double), dimension(*), intent(in) :: u, yp
     end function
     type(c_ptr) function nv_last_error() bind(c, name='nv_last_error')
       import :: c_ptr
