@@ -110,16 +110,28 @@ typedef struct nv_host_state {
   int32_t *behind;    /* [pcount] (required)                                     */
   int32_t *closest;   /* [pcount] reconnection candidate (optional)              */
   double *closestd;   /* [pcount] its distance (optional)                        */
+  /* solid walls (optional; NULL: no pinned points): a point pinned in front (pinnedi, its
+   * infront is itself: the segment ends in the wall) or behind (pinnedb), and the wall it is
+   * pinned to, wpinned(1:3) in -1, 0, +1 (src/cdata.f90:27-28) */
+  int32_t *wpinned;   /* [3*pcount]                                              */
+  int32_t *pinnedi;   /* [pcount] logical 0/1                                    */
+  int32_t *pinnedb;   /* [pcount] logical 0/1                                    */
 } nv_host_state;
 
 /* Topology events, logged in the order the reference's serial sweeps make them. */
-enum { NV_EV_INSERT = 1, NV_EV_RECON = 2, NV_EV_REMOVE = 3, NV_EV_LOOPKILL = 4 };
+enum { NV_EV_INSERT = 1, NV_EV_RECON = 2, NV_EV_REMOVE = 3, NV_EV_LOOPKILL = 4, NV_EV_WALL = 5,
+       NV_EV_CLEAR = 6 };
 typedef struct nv_event {
   int32_t itime; /* step number (the reference's itime)                                  */
   int32_t kind;  /* NV_EV_*                                                              */
-  int32_t i;     /* INSERT: point i; RECON: point i; REMOVE: point i; LOOPKILL: start p   */
+  int32_t i;     /* INSERT: point i; RECON: point i; REMOVE: point i; LOOPKILL: start p;
+                    WALL: the point wall_recon cleared (src/reconnection.f90:66-150);
+                    CLEAR: point i pinned behind, cleared with the point in front of it
+                    when that one is pinned in front (line.f90:125-127,
+                    reconnection.f90:71-75)                                             */
   int32_t j;     /* INSERT: new slot; RECON: partner j; REMOVE: removed slot;
-                    LOOPKILL: points cleared                                            */
+                    LOOPKILL: points cleared; WALL: points cleared (1-3); CLEAR: points
+                    cleared (2, or 1 for a point pinned at both ends)                   */
 } nv_event;
 
 typedef struct nv_counters {
@@ -138,6 +150,8 @@ typedef struct nv_counters {
                             for two runs exactly when their event sequences agree
                             (up to 64-bit collisions), whether or not the log kept
                             them all                                            */
+  int32_t wall_recon_count; /* wall_recon cuts so far (wall_recon_count)         */
+  int32_t reserved;
 } nv_counters;
 
 /* One octree node (type node, src/tree.f90:20-32) as dumped in preorder by nv_tree_dump:
@@ -195,6 +209,7 @@ int nv_pinsert(nv_handle *h);           /* pinsert           src/line.f90:18-96 
 int nv_pclose(nv_handle *h);            /* pclose_tree (tree_theta>0, src/tree.f90:190-244)
                                            or pclose (src/line.f90:135-160)             */
 int nv_precon(nv_handle *h);            /* precon            src/reconnection.f90:11-61  */
+int nv_wall_recon(nv_handle *h);        /* wall_recon        src/reconnection.f90:66-150 */
 int nv_premove(nv_handle *h);           /* premove           src/line.f90:102-130        */
 int nv_enforce_boundary(nv_handle *h);  /* enforce_boundary  src/boundary.f90:91-138     */
 int nv_empty_tree(nv_handle *h);        /* empty_tree        src/tree.f90:160-186        */
@@ -363,9 +378,8 @@ int nv_ts_row_get(nv_handle *h, int32_t sys, nv_ts_row *row);
  * kappa_bar, remove_count, tree_eval; no newline.  cap: size of buf. */
 int nv_format_ts_row(const nv_ts_row *row, int32_t shots, char *buf, int32_t cap);
 
-/* Every field of type(qvort) (src/cdata.f90:19-31) that this library keeps, for file I/O:
- * point-major 3-vectors as in nv_host_state.  The pinning fields (wpinned, pinnedi, pinnedb)
- * are always zero and .false. here (no solid walls). */
+/* Every field of type(qvort) (src/cdata.f90:19-31), for file I/O: point-major 3-vectors as
+ * in nv_host_state. */
 typedef struct nv_full_state {
   int32_t pcount;
   double *x, *u, *u1, *u2, *u_mf, *u_sup;  /* [3*pcount]                               */
@@ -373,6 +387,8 @@ typedef struct nv_full_state {
   double *ghosti, *ghostb;                 /* [3*pcount]                               */
   int32_t *infront, *behind, *closest;     /* [pcount]                                 */
   double *closestd;                        /* [pcount]                                 */
+  int32_t *wpinned;                        /* [3*pcount] (NULL: zero)                  */
+  int32_t *pinnedi, *pinnedb;              /* [pcount] logical 0/1 (NULL: .false.)     */
 } nv_full_state;
 
 /* Every field of system sys (u_sup and u_mf of its last velocity pass, curv and stretch of
@@ -392,8 +408,8 @@ int nv_write_snapshot(nv_handle *h, int32_t sys, const char *path);
 int nv_write_dump(nv_handle *h, int32_t sys, const char *path);
 /* data_restore (src/initial.f90:151-166): reads a var.dat into system sys (state, t, itime,
  * recon_count); the next step is itime+1.  NV_ERR_IO if the file cannot be read or is not such
- * a file, NV_ERR_CAPACITY if its pcount exceeds the system's capacity, NV_ERR_UNSUPPORTED if
- * it holds pinned points. */
+ * a file, NV_ERR_CAPACITY if its pcount exceeds the system's capacity, NV_ERR_ARG if it holds
+ * pinned points and the system has no solid wall. */
 int nv_restore_dump(nv_handle *h, int32_t sys, const char *path);
 /* The same formats between host arrays and files, without a handle or a GPU. */
 int nv_snapshot_write_file(const nv_full_state *st, double t, const char *path);

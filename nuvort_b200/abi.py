@@ -37,7 +37,9 @@ NV_NF_ZERO, NV_NF_XFLOW, NV_NF_UNIFORM = 0, 1, 2
 NV_NF_SHEAR_XFLOW, NV_NF_CHANNEL, NV_NF_YCHANNEL, NV_NF_NOISEY_XFLOW = 3, 4, 5, 6
 NV_NF_LAIZET_DNS, NV_NF_TURB_DNS = 7, 8
 NV_PREC_FP64, NV_PREC_MIXED = 0, 1
-NV_EV_INSERT, NV_EV_RECON, NV_EV_REMOVE, NV_EV_LOOPKILL = 1, 2, 3, 4
+NV_EV_INSERT, NV_EV_RECON, NV_EV_REMOVE, NV_EV_LOOPKILL, NV_EV_WALL, NV_EV_CLEAR = 1, 2, 3, 4, 5, 6
+# events whose j is a count of points, not a slot
+EV_COUNT_KINDS = (NV_EV_LOOPKILL, NV_EV_WALL, NV_EV_CLEAR)
 NV_TREE_MAX_DEPTH = 42
 
 VELOCITY = {"LIA": NV_VEL_LIA, "BS": NV_VEL_BS, "Tree": NV_VEL_TREE}
@@ -88,6 +90,9 @@ class NvHostState(C.Structure):
         ("behind", C.POINTER(C.c_int32)),
         ("closest", C.POINTER(C.c_int32)),
         ("closestd", C.POINTER(C.c_double)),
+        ("wpinned", C.POINTER(C.c_int32)),
+        ("pinnedi", C.POINTER(C.c_int32)),
+        ("pinnedb", C.POINTER(C.c_int32)),
     ]
 
 
@@ -109,6 +114,9 @@ class NvFullState(C.Structure):
         ("behind", C.POINTER(C.c_int32)),
         ("closest", C.POINTER(C.c_int32)),
         ("closestd", C.POINTER(C.c_double)),
+        ("wpinned", C.POINTER(C.c_int32)),
+        ("pinnedi", C.POINTER(C.c_int32)),
+        ("pinnedb", C.POINTER(C.c_int32)),
     ]
 
 
@@ -157,6 +165,8 @@ class NvCounters(C.Structure):
         ("n_events", C.c_int32),
         ("t", C.c_double),
         ("event_hash", C.c_uint64),
+        ("wall_recon_count", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -250,7 +260,9 @@ class State:
     """Host copy of one system's filament state: 1-based slots stored at rows 0..pcount-1.
 
     ``x``, ``u``, ``u1``, ``u2``, ``ghosti``, ``ghostb`` are (n, 3) float64; ``infront``,
-    ``behind``, ``closest`` are int32 (0 = empty / none); ``closestd`` float64.
+    ``behind``, ``closest`` are int32 (0 = empty / none); ``closestd`` float64.  Solid walls:
+    ``wpinned`` (n, 3) int32 in -1/0/1, ``pinnedi``, ``pinnedb`` (n,) int32 0/1 (None: no
+    pinned points).
     """
     x: np.ndarray
     infront: np.ndarray
@@ -267,6 +279,9 @@ class State:
     u_sup: Optional[np.ndarray] = None
     curv: Optional[np.ndarray] = None
     stretch: Optional[np.ndarray] = None
+    wpinned: Optional[np.ndarray] = None
+    pinnedi: Optional[np.ndarray] = None
+    pinnedb: Optional[np.ndarray] = None
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -278,7 +293,9 @@ class State:
         z3 = lambda: np.zeros((cap, 3), np.float64)
         return State(x=z3(), infront=np.zeros(cap, np.int32), behind=np.zeros(cap, np.int32),
                      u=z3(), u1=z3(), u2=z3(), ghosti=z3(), ghostb=z3(),
-                     closest=np.zeros(cap, np.int32), closestd=np.zeros(cap, np.float64))
+                     closest=np.zeros(cap, np.int32), closestd=np.zeros(cap, np.float64),
+                     wpinned=np.zeros((cap, 3), np.int32), pinnedi=np.zeros(cap, np.int32),
+                     pinnedb=np.zeros(cap, np.int32))
 
     @staticmethod
     def empty_full(cap: int) -> "State":
@@ -308,7 +325,7 @@ class State:
         s.pcount = self.pcount
         for name in ("x", "u", "u1", "u2", "u_mf", "u_sup", "curv", "stretch", "ghosti", "ghostb", "closestd"):
             setattr(s, name, _dptr(getattr(self, name)))
-        for name in ("infront", "behind", "closest"):
+        for name in ("infront", "behind", "closest", "wpinned", "pinnedi", "pinnedb"):
             setattr(s, name, _iptr(getattr(self, name)))
         return s
 
@@ -317,7 +334,7 @@ class State:
             a = getattr(self, name)
             if a is not None:
                 setattr(self, name, np.ascontiguousarray(a, dtype=np.float64))
-        for name in ("infront", "behind", "closest"):
+        for name in ("infront", "behind", "closest", "wpinned", "pinnedi", "pinnedb"):
             a = getattr(self, name)
             if a is not None:
                 setattr(self, name, np.ascontiguousarray(a, dtype=np.int32))
@@ -333,6 +350,9 @@ class State:
         s.behind = _iptr(self.behind)
         s.closest = _iptr(self.closest)
         s.closestd = _dptr(self.closestd)
+        s.wpinned = _iptr(self.wpinned)
+        s.pinnedi = _iptr(self.pinnedi)
+        s.pinnedb = _iptr(self.pinnedb)
         return s
 
     @property
@@ -341,7 +361,7 @@ class State:
 
 
 FIELDS = ("x", "infront", "behind", "u", "u1", "u2", "ghosti", "ghostb", "closest", "closestd", "u_mf", "u_sup",
-          "curv", "stretch")
+          "curv", "stretch", "wpinned", "pinnedi", "pinnedb")
 
 
 TREE_NODE_DTYPE = np.dtype([("pos", "<f8", 3), ("width", "<f8"), ("cent", "<f8", 3), ("circ", "<f8", 3),

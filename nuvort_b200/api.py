@@ -24,9 +24,10 @@ LIB_PATH = os.path.join(HERE, "lib", "libnuvort_gpu.so")
 
 _lib = None
 
-STAGES = ("ghostp", "construct_tree", "pmotion", "pinsert", "pclose", "precon", "premove",
+STAGES = ("ghostp", "construct_tree", "pmotion", "pinsert", "pclose", "precon", "wall_recon", "premove",
           "enforce_boundary", "empty_tree", "end_step")
-STATE_FIELDS = ("x", "infront", "behind", "u", "u1", "u2", "ghosti", "ghostb", "closest", "closestd")
+STATE_FIELDS = ("x", "infront", "behind", "u", "u1", "u2", "ghosti", "ghostb", "closest", "closestd", "wpinned",
+                "pinnedi", "pinnedb")
 STAGE_TIMES = ("ghost", "tree", "velocity", "ab3", "topology", "step", "insert", "close", "recon", "remove")
 
 

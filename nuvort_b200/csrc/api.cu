@@ -65,6 +65,33 @@ __global__ void k_upload_check(const int *__restrict__ inf, const int *__restric
   if ((threadIdx.x & 31) == 0 && bl) atomicAdd(&check[1], __popc(bl));
 }
 
+// Pinned records from the staged host arrays (wpinned [3n], pinnedi [n], pinnedb [n]; null:
+// not pinned) into the system's slots, empty beyond n.
+__global__ void k_put_pin(int *__restrict__ pin, int base, int rows, int n, const int *__restrict__ wp,
+                          const int *__restrict__ pi, const int *__restrict__ pb) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= rows) return;
+  int v = 0;
+  if (k >= 1 && k <= n) {
+    int w[3] = {0, 0, 0};
+    if (wp)
+      for (int c = 0; c < 3; ++c) w[c] = wp[3 * (k - 1) + c];
+    v = pin_encode(pi && pi[k - 1], pb && pb[k - 1], w);
+  }
+  pin[base + k] = v;
+}
+
+__global__ void k_get_pin(const int *__restrict__ pin, int base, int n, int *__restrict__ wp, int *__restrict__ pi,
+                          int *__restrict__ pb) {
+  const int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > n) return;
+  const int v = pin ? pin[base + k] : 0;
+  if (wp)
+    for (int c = 0; c < 3; ++c) wp[3 * (k - 1) + c] = pin_w(v, c);
+  if (pi) pi[k - 1] = pin_i(v);
+  if (pb) pb[k - 1] = pin_b(v);
+}
+
 __global__ void k_get_rows(const double *__restrict__ dev, long long T, int base, int n, int comps,
                            double *__restrict__ host) {
   const int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -177,6 +204,22 @@ SysConst make_sysconst(const nv_params &p, int base, int cap) {
         ++n;
       }
   s.n_shift = n;
+  // create_mirror_loop_array (boundary.f90:180-212): the reflections -1..1 on the solid axes,
+  // k fastest, without (0,0,0)
+  int nm = 0;
+  for (int i = -1; i <= 1; ++i)
+    for (int j = -1; j <= 1; ++j)
+      for (int k = -1; k <= 1; ++k) {
+        const int r[3] = {i, j, k};
+        bool ok = true;
+        for (int c = 0; c < 3; ++c)
+          if (p.boundary[c] != NV_BC_SOLID && r[c] != 0) ok = false;
+        if (!ok || (i == 0 && j == 0 && k == 0)) continue;
+        for (int c = 0; c < 3; ++c) s.mirror[nm][c] = r[c];
+        ++nm;
+      }
+  s.n_mirror = nm;
+  for (int c = 0; c < 3; ++c) s.solid[c] = p.boundary[c] == NV_BC_SOLID;
   s.velocity = p.velocity;
   for (int c = 0; c < 3; ++c) s.periodic[c] = p.boundary[c] == NV_BC_PERIODIC;
   s.tree_extra_correction = p.tree_extra_correction != 0;
@@ -351,6 +394,7 @@ void enqueue_step(nv_handle *h) {
   time_end(h, ST_CLOSE);
   time_begin(h, ST_RECON);
   launch_precon(h);
+  launch_wall_recon(h);  // systems with solid walls; the others have no pinned points
   time_end(h, ST_RECON);
   time_begin(h, ST_REMOVE);
   launch_premove(h);
@@ -462,10 +506,10 @@ int nv_check_params(const nv_params *p) {
   if (!(std::min(p->box_size[0], std::min(p->box_size[1], p->box_size[2])) > 0.))
     return set_error(NV_ERR_ARG, "box size is less than or equal zero");
   for (int c = 0; c < 3; ++c) {
-    if (p->boundary[c] == NV_BC_SOLID)
-      return set_error(NV_ERR_UNSUPPORTED, "solid boundaries (mirror images, pinning) are not supported");
-    if (p->boundary[c] != NV_BC_PERIODIC && p->boundary[c] != NV_BC_OPEN)
+    if (p->boundary[c] != NV_BC_PERIODIC && p->boundary[c] != NV_BC_OPEN && p->boundary[c] != NV_BC_SOLID)
       return set_error(NV_ERR_ARG, "incorrect boundary parameter");
+    if (p->boundary[c] == NV_BC_SOLID && p->precision == NV_PREC_MIXED)
+      return set_error(NV_ERR_UNSUPPORTED, "solid boundaries run in the plain FP64 precision only");
   }
   if (p->velocity != NV_VEL_LIA && p->velocity != NV_VEL_BS && p->velocity != NV_VEL_TREE)
     return set_error(NV_ERR_ARG, "correct value for \"velocity\" in run.in has not been set");
@@ -546,6 +590,16 @@ int nv_create(const nv_params *params, int32_t nsys, const int32_t *capacity, in
   for (auto &c : h->sc) {  // the velocity passes keep u_sup and u_mf there
     c.usm = h->usm;
     c.usm_T = T;
+    h->any_solid |= c.solid[0] || c.solid[1] || c.solid[2];
+  }
+  if (h->any_solid) {  // pinned records and the tree's mirror sums of the solid-wall systems
+    if ((rc = dalloc(&h->pin, T)) || (rc = dalloc(&h->umir, 3 * T))) return bail(rc);
+    for (auto &c : h->sc)
+      if (c.solid[0] || c.solid[1] || c.solid[2]) {
+        c.pin = h->pin;
+        c.umir = h->umir;
+        h->any_mirror |= c.sched_tree && c.n_mirror > 0;
+      }
   }
   {
     int maxcap = 0;
@@ -591,7 +645,7 @@ int nv_destroy(nv_handle *h) {
   tree_free(h);
   topo_free(h);
   for (void *p : h->nf_buffers) cudaFree(p);
-  void *ptrs[] = {h->usm, h->cs, h->d_drec, h->partial, h->stage, h->d_upck, h->d_sc, h->d_dyn, h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv,
+  void *ptrs[] = {h->pin, h->umir, h->usm, h->cs, h->d_drec, h->partial, h->stage, h->d_upck, h->d_sc, h->d_dyn, h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv,
                   h->closest, h->sys_of, h->seg, h->seg32, h->d_err, h->d_events, h->d_event_count,
                   h->d_work_direct, h->d_work_tree, h->d_work_lia, h->d_work_img, h->d_work_timg, h->d_work_split};
   for (void *p : ptrs)
@@ -615,6 +669,11 @@ int nv_upload(nv_handle *h, int32_t sys, const nv_host_state *st) {
   if (!st->x || !st->infront || !st->behind) return set_error(NV_ERR_ARG, "nv_upload: x, infront, behind are required");
   const int n = st->pcount, cap = h->cap[sys], base = h->base[sys];
   if (n < 0 || n > cap) return set_error(NV_ERR_ARG, "nv_upload: pcount exceeds the system's capacity");
+  const SysConst &scs = h->sc[sys];
+  if (!(scs.solid[0] || scs.solid[1] || scs.solid[2]))
+    for (int k = 0; k < n; ++k)
+      if ((st->pinnedi && st->pinnedi[k]) || (st->pinnedb && st->pinnedb[k]))
+        return set_error(NV_ERR_ARG, "nv_upload: pinned points need a solid boundary (system left unchanged)");
   int rc = set_device(h);
   if (rc) return rc;
   const long long T = h->T;
@@ -657,6 +716,22 @@ int nv_upload(nv_handle *h, int32_t sys, const nv_host_state *st) {
   // the new f(:) carries no u_sup, u_mf, curv or stretch yet (nv_upload_full sets them)
   k_put_rows<<<grid_for(rows, 256), 256, 0, sm>>>(h->usm, T, base, rows, n, 6, nullptr);
   k_put_rows<<<grid_for(rows, 256), 256, 0, sm>>>(h->cs, T, base, rows, n, 2, nullptr);
+  if (h->pin) {  // pinned records (the staging buffer holds 5n ints)
+    const int *wp = nullptr, *pi = nullptr, *pb = nullptr;
+    if (n > 0 && st->wpinned) {
+      NV_CUDA(cudaMemcpyAsync(stage_i, st->wpinned, 3 * (size_t)n * sizeof(int), cudaMemcpyHostToDevice, sm));
+      wp = stage_i;
+    }
+    if (n > 0 && st->pinnedi) {
+      NV_CUDA(cudaMemcpyAsync(stage_i + 3 * (size_t)n, st->pinnedi, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, sm));
+      pi = stage_i + 3 * (size_t)n;
+    }
+    if (n > 0 && st->pinnedb) {
+      NV_CUDA(cudaMemcpyAsync(stage_i + 4 * (size_t)n, st->pinnedb, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, sm));
+      pb = stage_i + 4 * (size_t)n;
+    }
+    k_put_pin<<<grid_for(rows, 256), 256, 0, sm>>>(h->pin, base, rows, n, wp, pi, pb);
+  }
   SysDyn &d = h->h_dyn[sys];
   // keep the clock and counters; replace the slot count (pull_dyn_one waits for the copies)
   rc = pull_dyn_one(h, sys);
@@ -699,6 +774,16 @@ int nv_download(nv_handle *h, int32_t sys, nv_host_state *st, int32_t cap) {
       (rc = get_link(h->nxt, st->infront)) || (rc = get_link(h->prv, st->behind)) ||
       (rc = get_link(h->closest, st->closest)) || (rc = get(h->closestd, st->closestd, 1)))
     return rc;
+  if (n > 0 && (st->wpinned || st->pinnedi || st->pinnedb)) {  // pinned records, one int array at a time
+    int *out[3] = {st->wpinned, st->pinnedi, st->pinnedb};
+    const int per[3] = {3, 1, 1};
+    for (int q = 0; q < 3; ++q) {
+      if (!out[q]) continue;
+      k_get_pin<<<grid_for(n, 256), 256, 0, sm>>>(h->pin, base, n, q == 0 ? stage_i : nullptr, q == 1 ? stage_i : nullptr,
+                                                 q == 2 ? stage_i : nullptr);
+      NV_CUDA(cudaMemcpyAsync(out[q], stage_i, (size_t)per[q] * n * sizeof(int), cudaMemcpyDeviceToHost, sm));
+    }
+  }
   NV_CUDA(cudaStreamSynchronize(sm));
   return NV_OK;
 }
@@ -718,6 +803,9 @@ int nv_upload_full(nv_handle *h, int32_t sys, const nv_full_state *st) {
   hs.behind = st->behind;
   hs.closest = st->closest;
   hs.closestd = st->closestd;
+  hs.wpinned = st->wpinned;
+  hs.pinnedi = st->pinnedi;
+  hs.pinnedb = st->pinnedb;
   int rc = nv_upload(h, sys, &hs);  // checks the links before writing anything
   if (rc) return rc;
   const int n = st->pcount, base = h->base[sys], rows = h->cap[sys] + 1;
@@ -750,6 +838,9 @@ int nv_download_full(nv_handle *h, int32_t sys, nv_full_state *st, int32_t cap) 
   hs.behind = st->behind;
   hs.closest = st->closest;
   hs.closestd = st->closestd;
+  hs.wpinned = st->wpinned;
+  hs.pinnedi = st->pinnedi;
+  hs.pinnedb = st->pinnedb;
   int rc = nv_download(h, sys, &hs, cap);
   st->pcount = hs.pcount;
   if (rc) return rc;
@@ -788,7 +879,7 @@ int nv_ts_row_get(nv_handle *h, int32_t sys, nv_ts_row *row) {
   row->itime = d.itime;
   row->live = r.live;
   row->recon_count = d.recon_count;
-  row->wall_recon_count = 0;
+  row->wall_recon_count = d.wall_recon_count;
   row->remove_count = d.remove_count;
   row->tree_eval = (int64_t)d.tree_eval;
   row->t = d.t;
@@ -832,6 +923,8 @@ int nv_counters_get(nv_handle *h, int32_t sys, nv_counters *c) {
   c->n_events = d.event_seq;
   c->t = d.t;
   c->event_hash = d.ev_hash;
+  c->wall_recon_count = d.wall_recon_count;
+  c->reserved = 0;
   return NV_OK;
 }
 
@@ -856,7 +949,8 @@ int nv_events_get(nv_handle *h, int32_t sys, nv_event *buf, int32_t cap, int32_t
       buf[m].itime = e.itime;
       buf[m].kind = e.kind;
       buf[m].i = e.i ? e.i - base : 0;
-      buf[m].j = (e.kind == NV_EV_LOOPKILL) ? e.j : (e.j ? e.j - base : 0);
+      const bool count = e.kind == NV_EV_LOOPKILL || e.kind == NV_EV_WALL || e.kind == NV_EV_CLEAR;
+      buf[m].j = count ? e.j : (e.j ? e.j - base : 0);
     }
     ++m;
   }
@@ -908,6 +1002,13 @@ int nv_precon(nv_handle *h) {
   int rc = set_device(h);
   if (rc) return rc;
   launch_precon(h);
+  return finish(h);
+}
+int nv_wall_recon(nv_handle *h) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  int rc = set_device(h);
+  if (rc) return rc;
+  launch_wall_recon(h);
   return finish(h);
 }
 int nv_premove(nv_handle *h) {

@@ -46,17 +46,18 @@ __global__ void k_ghost(const SysConst *__restrict__ scs, const SysDyn *__restri
   }
   const SysConst &sc = scs[s];
   const int b = prv[g];
-  double x[3], gi[3], gb[3];
+  const int pin = sc.pin ? sc.pin[g] : 0;
+  double x[3], xi[3], xb[3], gi[3], gb[3];
   load3(X, T, (int)g, x);
-  load3(X, T, n, gi);
-  load3(X, T, b, gb);
-  ghost_adjust(sc, x, gi);
-  ghost_adjust(sc, x, gb);
+  load3(X, T, n, xi);
+  load3(X, T, b, xb);
+  ghosts_of(sc, pin, x, xi, xb, gi, gb);
   store3(GI, T, (int)g, gi);
   store3(GB, T, (int)g, gb);
   double d[3] = {e_sub(gi[0], x[0]), e_sub(gi[1], x[1]), e_sub(gi[2], x[2])};
   const double c = e_add(e_add(e_sq(d[0]), e_sq(d[1])), e_sq(d[2]));
-  seg[2 * g] = make_double4(x[0], x[1], x[2], 1.0);
+  // a segment pinned in front goes into the wall: no Biot-Savart source (timestep.f90:161,187)
+  seg[2 * g] = make_double4(x[0], x[1], x[2], pin_i(pin) ? 0.0 : 1.0);
   seg[2 * g + 1] = make_double4(d[0], d[1], d[2], c);
   if (seg32) {  // FP32 record: position split hi + lo (x = hi + lo to ~1e-16), segment vector
     const float h0 = (float)x[0], h1 = (float)x[1], h2 = (float)x[2];
@@ -142,6 +143,17 @@ __global__ void k_wrap(const SysConst *__restrict__ scs, const SysDyn *__restric
       const double L = sc.box[c];
       if (x[c] > (L / 2.0)) { x[c] = e_sub(x[c], L); moved = true; }
       else if (x[c] < (-L / 2.0)) { x[c] = e_add(x[c], L); moved = true; }
+    }
+    // a pinned point is set back on its wall (boundary.f90:123-136): the axis of the first
+    // largest |wpinned| component, at +-0.499999999 of the box
+    const int pin = sc.pin ? sc.pin[g] : 0;
+    if (pin_i(pin) || pin_b(pin)) {
+      int pc = 0;
+      for (int c = 1; c < 3; ++c)
+        if (abs(pin_w(pin, c)) > abs(pin_w(pin, pc))) pc = c;
+      const int w = pin_w(pin, pc);
+      if (w > 0) { x[pc] = e_mul(0.499999999, sc.box[pc]); moved = true; }
+      else if (w < 0) { x[pc] = e_mul(-0.499999999, sc.box[pc]); moved = true; }
     }
     if (moved) store3(X, T, (int)g, x);
   }

@@ -68,7 +68,29 @@ struct SysConst {
   const double *nf_axis[3];    // xp, yp, zp
   int nf_n[3];
   double nf_step[3];           // grid spacing of the interpolation weights (y of laizet: 0, from yp)
+  // solid walls (boundary.f90:26-42,180-212; timestep.f90:201-234): pinned flags per slot
+  // (global index; see pin_*), the mirror images' reflections in create_mirror_loop_array
+  // order, the tree's mirror sums per slot; all null / 0 for a system without solid walls
+  const int *pin;
+  double *umir;
+  int n_mirror;
+  int mirror[26][3];
+  int solid[3];
 };
+
+// Pinned-point record of a slot: bit 0 pinnedi, bit 1 pinnedb, bits 2-7 wpinned(1..3), two
+// bits each (0, +1, or 3 for -1).  0 for every point away from a solid wall.
+__host__ __device__ __forceinline__ bool pin_i(int p) { return p & 1; }
+__host__ __device__ __forceinline__ bool pin_b(int p) { return p & 2; }
+__host__ __device__ __forceinline__ int pin_w(int p, int c) {
+  const int v = (p >> (2 + 2 * c)) & 3;
+  return v == 3 ? -1 : v;
+}
+__host__ __device__ __forceinline__ int pin_encode(int pinnedi, int pinnedb, const int w[3]) {
+  int p = (pinnedi ? 1 : 0) | (pinnedb ? 2 : 0);
+  for (int c = 0; c < 3; ++c) p |= ((w[c] < 0 ? 3 : w[c] > 0 ? 1 : 0) << (2 + 2 * c));
+  return p;
+}
 
 struct SysDyn {
   int pcount;
@@ -86,6 +108,7 @@ struct SysDyn {
   int ins_conv;      // pinsert's fixed-point iteration has converged
   int ins_mismatch;  // positions where the iteration's H and H' differ
   int noise_counter; // noisey_xflow: 1-based sample in use (xflow_noise_counter)
+  int wall_recon_count;  // wall_recon cuts (reconnection.f90:91)
   long long diag[12];  // see nv_diagnostics
   double total_length;  // pinsert: sum of the segment lengths it measured (line.f90:39)
   double avg_sep;       // pinsert: total_length / (old_pcount - empty slots) (line.f90:95)
@@ -128,6 +151,12 @@ __device__ __forceinline__ double e_div(double a, double b) { return __ddiv_rn(a
 __device__ __forceinline__ double e_sqrt(double a) { return __dsqrt_rn(a); }
 __device__ __forceinline__ double e_sq(double a) { return __dmul_rn(a, a); }
 
+// p + 2|r| (r L/2 - p): the cartesian reflection of one coordinate in the wall r (-1, 0, +1)
+// of an axis of length L, in the reference's order (timestep.f90:221-222, boundary.f90:35)
+__device__ __forceinline__ double reflect1(double p, int r, double L) {
+  return e_add(p, e_mul((double)(2 * (r < 0 ? -r : r)), e_sub(e_mul(e_mul(0.5, (double)r), L), p)));
+}
+
 // dist_gen (derivatives.f90:40-47)
 __device__ __forceinline__ double dist_gen(const double a[3], const double b[3]) {
   return e_sqrt(e_add(e_add(e_sq(e_sub(a[0], b[0])), e_sq(e_sub(a[1], b[1]))), e_sq(e_sub(a[2], b[2]))));
@@ -166,6 +195,28 @@ __device__ __forceinline__ void ghost_adjust(const SysConst &sc, const double x[
   }
 }
 
+// get_ghost_p (boundary.f90:26-84) from the neighbours' positions xi = x(infront), xb =
+// x(behind): a point pinned in front (pinnedi, the segment into the wall) takes its behind
+// point and that point's reflection in its wall as the point in front; pinned behind, the
+// mirror image; both then unwrapped across the periodic faces.
+__device__ __forceinline__ void ghosts_of(const SysConst &sc, int pin, const double x[3], const double xi[3],
+                                          const double xb[3], double gi[3], double gb[3]) {
+  for (int c = 0; c < 3; ++c) {
+    if (pin_i(pin)) {
+      gb[c] = xb[c];
+      gi[c] = reflect1(xb[c], pin_w(pin, c), sc.box[c]);
+    } else if (pin_b(pin)) {
+      gi[c] = xi[c];
+      gb[c] = reflect1(xi[c], pin_w(pin, c), sc.box[c]);
+    } else {
+      gi[c] = xi[c];
+      gb[c] = xb[c];
+    }
+  }
+  ghost_adjust(sc, x, gi);
+  ghost_adjust(sc, x, gb);
+}
+
 // get_deriv_1 / get_deriv_2 (derivatives.f90:11-36)
 __device__ __forceinline__ void deriv1(const double x[3], const double gi[3], const double gb[3],
                                        double s[3]) {
@@ -186,6 +237,31 @@ __device__ __forceinline__ void deriv2(const double x[3], const double gi[3], co
 #pragma unroll
   for (int c = 0; c < 3; ++c)
     s[c] = e_mul(2.0, e_add(e_sub(e_div(gi[c], d1), e_div(x[c], d2)), e_div(gb[c], d3)));
+}
+
+// new point of an insertion (line.f90:62-79)
+__device__ __forceinline__ void new_point(const double x[3], const double gi[3], const double gb[3], double disti,
+                                          double xn[3]) {
+  double fdd[3];
+  deriv2(x, gi, gb, fdd);
+  double curv = e_sqrt(dot3(fdd, fdd));
+  const double mid[3] = {e_mul(0.5, e_add(x[0], gi[0])), e_mul(0.5, e_add(x[1], gi[1])), e_mul(0.5, e_add(x[2], gi[2]))};
+  for (int c = 0; c < 3; ++c) xn[c] = mid[c];
+  if (curv > 1E-5) {
+    curv = e_div(1.0, curv);
+    const double disc = e_sub(e_mul(curv, curv), e_mul(0.25, e_mul(disti, disti)));
+    if (disc > 0.) {
+      const double sfac = e_mul(e_sub(e_sqrt(disc), curv), curv);
+      for (int c = 0; c < 3; ++c) xn[c] = e_add(mid[c], e_mul(sfac, fdd[c]));
+    }
+  }
+}
+
+// A system with solid walls carries pinned records; its topology stages run as the exact
+// serial sweeps of solid.cu and the parallel ones skip it.
+__device__ __forceinline__ bool walled(const SysConst &sc) { return sc.pin != nullptr; }
+__device__ __forceinline__ bool pinned_at(const SysConst &sc, int g) {
+  return sc.pin && (sc.pin[g] & 3);
 }
 
 // Local part of calc_velocity (timestep.f90:60-80,102-105): u = beta s' x s''.
@@ -360,3 +436,36 @@ __device__ __forceinline__ bool bs_term_exact(const double r[3], const double d[
 }
 
 __device__ __forceinline__ void set_err(unsigned *err, unsigned bit) { atomicOr(err, bit); }
+
+// biot_savart_mirror's test (timestep.f90:214-217) of whether target g skips its own image
+// in mirror m: the sum of wpinned(g) - reflect is zero and the sum of wpinned(g) is below 2
+// (component sums, as the reference writes them).
+__device__ __forceinline__ bool mirror_skips_own(const SysConst &sc, int pin_g, int m) {
+  int d = 0, w = 0;
+  for (int c = 0; c < 3; ++c) {
+    d += pin_w(pin_g, c) - sc.mirror[m][c];
+    w += pin_w(pin_g, c);
+  }
+  return d == 0 && w < 2;
+}
+
+// One term of biot_savart_mirror (timestep.f90:201-234): segment j (x_j to ghosti_j) reflected
+// in mirror m, its orientation reversed (from the reflected ghost to the reflected point), at
+// target g (position xi, pinned record pin_g, behind pi); false when the reference skips it.
+__device__ __forceinline__ bool mirror_term(const SysConst &sc, int m, const double *__restrict__ X,
+                                            const double *__restrict__ GI, const int *__restrict__ nxt, long long T,
+                                            int j, int g, int pi, int pin_g, bool skip_own, const double xi[3],
+                                            double out[3]) {
+  if (nxt[j] == 0 || pin_i(sc.pin[j])) return false;
+  if (skip_own && ((pin_b(pin_g) && j == g) || (pin_i(pin_g) && j == pi))) return false;
+  double sgi[3], s[3];
+  for (int c = 0; c < 3; ++c) {
+    sgi[c] = reflect1(X[c * T + j], sc.mirror[m][c], sc.box[c]);
+    s[c] = reflect1(GI[c * T + j], sc.mirror[m][c], sc.box[c]);
+  }
+  const double a = e_add(e_add(e_sq(e_sub(xi[0], s[0])), e_sq(e_sub(xi[1], s[1]))), e_sq(e_sub(xi[2], s[2])));
+  const double r[3] = {e_sub(s[0], xi[0]), e_sub(s[1], xi[1]), e_sub(s[2], xi[2])};
+  const double d[3] = {e_sub(sgi[0], s[0]), e_sub(sgi[1], s[1]), e_sub(sgi[2], s[2])};
+  const double c = e_add(e_add(e_sq(e_sub(s[0], sgi[0])), e_sq(e_sub(s[1], sgi[1]))), e_sq(e_sub(s[2], sgi[2])));
+  return bs_term_exact(r, d, a, c, sc.quant_circ, sc.two_pi, out);
+}

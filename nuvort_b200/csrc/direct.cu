@@ -143,6 +143,20 @@ __global__ void __launch_bounds__(64) k_direct_fp64(
     for (int q = consumed; q < issued; ++q) mbar_wait(&bar[q & 1], (unsigned)((q >> 1) & 1));
   if (!active) return;
 
+  // solid walls: the mirror images, in mirror order, each over j ascending (timestep.f90:94-98)
+  double um[3] = {0, 0, 0};
+  if (sc.n_mirror) {
+    const int pin_g = sc.pin[g];
+    for (int m = 0; m < sc.n_mirror; ++m) {
+      const bool own = mirror_skips_own(sc, pin_g, m);
+      for (int j = base + 1; j <= base + pc; ++j) {
+        double tm[3];
+        if (mirror_term(sc, m, X, GI, nxt, T, j, g, pi, pin_g, own, xi, tm))
+          for (int c = 0; c < 3; ++c) um[c] = e_add(um[c], tm[c]);
+      }
+    }
+  }
+
   double gi[3], gb[3], u[3], fdot[3];
   load3(GI, T, g, gi);
   load3(GB, T, g, gb);
@@ -151,6 +165,9 @@ __global__ void __launch_bounds__(64) k_direct_fp64(
   for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], ub0[c]);
 #pragma unroll
   for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], ubs[c]);
+  if (sc.n_mirror)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], um[c]);
   mf_epilogue(sc, dyn[w.x], xi, fdot, u, targets ? -1 : g);
   if (targets) {
     const int idx = w.y + tid;
@@ -181,8 +198,8 @@ __global__ void __launch_bounds__(128) k_direct_fp64_split(
   constexpr int LD = TJ + 1;           // padded row: the adding lanes read different banks
   __shared__ double s_terms[2][3 * G][LD];
   __shared__ double s_x[G][3];
-  __shared__ double s_sum[G][3][2];
-  __shared__ int s_g[G], s_p[G], s_act[G];
+  __shared__ double s_sum[G][3][3];
+  __shared__ int s_g[G], s_p[G], s_act[G], s_pin[G];
   __shared__ int s_abort;
 
   const int2 w = work[blockIdx.x];
@@ -206,6 +223,7 @@ __global__ void __launch_bounds__(128) k_direct_fp64_split(
     s_g[tid] = g;
     s_act[tid] = act;
     s_p[tid] = act ? prv[g] : -1;
+    s_pin[tid] = act && sc.pin ? sc.pin[g] : 0;
     double xi[3] = {0, 0, 0};
     if (act) load3(X, T, g, xi);
     for (int c = 0; c < 3; ++c) s_x[tid][c] = xi[c];
@@ -214,9 +232,9 @@ __global__ void __launch_bounds__(128) k_direct_fp64_split(
   if (s_abort) return;
 
   const int nt = (pc + TJ - 1) / TJ;
-  const int Q = (1 + sc.n_shift) * nt;
+  const int Q = (1 + sc.n_shift + sc.n_mirror) * nt;  // unshifted, shifted, then mirror images
   const double qc = sc.quant_circ, two_pi = sc.two_pi;
-  double acc0 = 0.0, accs = 0.0;  // adding lanes: unshifted and shifted sums of one component
+  double acc0 = 0.0, accs = 0.0, accm = 0.0;  // adding lanes: unshifted, shifted, mirror sums
   for (int q = 0; q <= Q; ++q) {
     if (tid >= 32) {
       if (q < Q) {  // terms of step q
@@ -236,7 +254,12 @@ __global__ void __launch_bounds__(128) k_direct_fp64_split(
           if (jj >= n) continue;
           const int gj = base + 1 + t * TJ + jj;
           double tm[3] = {0.0, 0.0, 0.0};
-          if (s_act[tq] && gj != s_p[tq] && (m > 0 || gj != s_g[tq])) {
+          if (m > sc.n_shift) {  // mirror image m - 1 - n_shift
+            const int mm = m - 1 - sc.n_shift;
+            if (!s_act[tq] || !mirror_term(sc, mm, X, GI, nxt, T, gj, s_g[tq], s_p[tq], s_pin[tq],
+                                           mirror_skips_own(sc, s_pin[tq], mm), s_x[tq], tm))
+              tm[0] = tm[1] = tm[2] = 0.0;
+          } else if (s_act[tq] && gj != s_p[tq] && (m > 0 || gj != s_g[tq])) {
             const double4 A = seg[2 * (long long)gj], B = seg[2 * (long long)gj + 1];
             if (A.w != 0.0) {
               double rr[3];
@@ -263,17 +286,19 @@ __global__ void __launch_bounds__(128) k_direct_fp64_split(
       const int m = (q - 1) / nt, t = (q - 1) % nt;
       const int n = min(TJ, pc - t * TJ);
       const double *row = s_terms[(q - 1) & 1][tid];
-      double acc = m == 0 ? acc0 : accs;
+      double acc = m == 0 ? acc0 : m <= sc.n_shift ? accs : accm;
 #pragma unroll 8
       for (int jj = 0; jj < n; ++jj) acc = e_add(acc, row[jj]);
       if (m == 0) acc0 = acc;
-      else accs = acc;
+      else if (m <= sc.n_shift) accs = acc;
+      else accm = acc;
     }
     __syncthreads();
   }
   if (tid < 3 * G) {
     s_sum[tid / 3][tid % 3][0] = acc0;
     s_sum[tid / 3][tid % 3][1] = accs;
+    s_sum[tid / 3][tid % 3][2] = accm;
   }
   __syncthreads();
   if (tid >= G || !s_act[tid]) return;
@@ -287,6 +312,9 @@ __global__ void __launch_bounds__(128) k_direct_fp64_split(
   for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], s_sum[tid][c][0]);
 #pragma unroll
   for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], s_sum[tid][c][1]);
+  if (sc.n_mirror)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], s_sum[tid][c][2]);
   mf_epilogue(sc, dyn[w.x], xi, fdot, u, targets ? -1 : g);
   if (targets) {
     const int idx = w.y + tid;

@@ -38,6 +38,9 @@ struct nv_handle {
   double *partial = nullptr; // per-image partial sums [image][component][slot] (mixed precision)
   std::vector<void *> nf_buffers;  // normal-fluid noise and grid data (nv_set_normal_fluid_*)
   double *usm = nullptr;     // f(:)%u_sup, f(:)%u_mf of the last velocity pass [6][T]
+  int *pin = nullptr;        // solid walls: pinned record per slot [T] (pin_* in common.cuh)
+  double *umir = nullptr;    // solid walls: the tree's mirror sums per slot [3][T]
+  bool any_solid = false, any_mirror = false;  // a system with solid walls (with tree walks)
   double *cs = nullptr;      // f(:)%curv, f(:)%stretch of the last diagnostics [2][T]
   struct DiagRec *d_drec = nullptr;  // per system: the last diagnostics' reductions
   double *stage = nullptr;   // nv_upload / nv_download staging: host arrays as they are, 3 x (largest capacity + 1) doubles
@@ -128,6 +131,11 @@ void launch_pinsert(nv_handle *h);
 void launch_pclose(nv_handle *h, bool only_brute);
 void launch_precon(nv_handle *h);
 void launch_premove(nv_handle *h);
+// solid walls (solid.cu): the serial topology stages of the systems with solid walls
+void launch_solid_pinsert(nv_handle *h);
+void launch_solid_precon(nv_handle *h);
+void launch_wall_recon(nv_handle *h);
+void launch_solid_premove(nv_handle *h);
 
 int set_error(int code, const std::string &msg);
 // status code and message for a non-zero device error word (DERR_* bits)

@@ -157,9 +157,9 @@ int nv_dump_write_file(const nv_full_state *st, int32_t recon_count, int32_t iti
     put(b, (int32_t)ival(st->behind, k));
     put(b, (int32_t)ival(st->closest, k));
     put(b, val(st->closestd, k));
-    for (int c = 0; c < 3; ++c) put(b, (int32_t)0);  // wpinned
-    put(b, (int32_t)0);                              // pinnedi = .false.
-    put(b, (int32_t)0);                              // pinnedb = .false.
+    for (int c = 0; c < 3; ++c) put(b, (int32_t)(st->wpinned ? st->wpinned[3 * k + c] : 0));
+    put(b, (int32_t)ival(st->pinnedi, k));  // logical: .true. is 1, .false. 0
+    put(b, (int32_t)ival(st->pinnedb, k));
   }
   ok = ok && write_record(f.f, b);
   if (!ok) return set_error(NV_ERR_IO, std::string("short write: ") + path);
@@ -210,9 +210,10 @@ int nv_dump_read_file(const char *path, nv_full_state *st, int32_t cap, int32_t 
     q += 12;
     if (st->closestd) st->closestd[k] = get<double>(q);
     q += 8;
-    for (int c = 0; c < 5; ++c)  // wpinned(3), pinnedi, pinnedb
-      if (get<int32_t>(q + 4 * c) != 0)
-        return set_error(NV_ERR_UNSUPPORTED, "nv_dump_read_file: pinned points (solid walls) are not supported");
+    for (int c = 0; c < 3; ++c)
+      if (st->wpinned) st->wpinned[3 * k + c] = get<int32_t>(q + 4 * c);
+    if (st->pinnedi) st->pinnedi[k] = get<int32_t>(q + 12) != 0;
+    if (st->pinnedb) st->pinnedb[k] = get<int32_t>(q + 16) != 0;
   }
   return NV_OK;
 }
@@ -224,15 +225,16 @@ namespace {
 // Host arrays for one system's full state.
 struct FullArrays {
   std::vector<double> x, u, u1, u2, umf, usup, curv, stretch, gi, gb, cd;
-  std::vector<int32_t> inf, beh, cl;
+  std::vector<int32_t> inf, beh, cl, wp, pi, pb;
   nv_full_state st;
   explicit FullArrays(int cap) {
     const size_t n3 = 3 * (size_t)cap, n = (size_t)cap;
     x.resize(n3); u.resize(n3); u1.resize(n3); u2.resize(n3); umf.resize(n3); usup.resize(n3);
     gi.resize(n3); gb.resize(n3); curv.resize(n); stretch.resize(n); cd.resize(n);
-    inf.resize(n); beh.resize(n); cl.resize(n);
-    st = nv_full_state{0, x.data(), u.data(), u1.data(), u2.data(), umf.data(), usup.data(), curv.data(),
-                       stretch.data(), gi.data(), gb.data(), inf.data(), beh.data(), cl.data(), cd.data()};
+    inf.resize(n); beh.resize(n); cl.resize(n); wp.resize(n3); pi.resize(n); pb.resize(n);
+    st = nv_full_state{0,          x.data(),  u.data(),  u1.data(), u2.data(),  umf.data(), usup.data(), curv.data(),
+                       stretch.data(), gi.data(), gb.data(), inf.data(), beh.data(), cl.data(),  cd.data(),
+                       wp.data(),  pi.data(), pb.data()};
   }
 };
 

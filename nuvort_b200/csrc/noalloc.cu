@@ -141,6 +141,9 @@ extern "C" int nv_calc_velocity_bs_static(const nv_params *p, int32_t pcount, co
     return set_error(NV_ERR_ARG, "nv_calc_velocity_bs_static: only velocity BS (the direct sum) is provided");
   int rc = nv_check_params(p);
   if (rc != NV_OK) return rc;
+  for (int c = 0; c < 3; ++c)
+    if (p->boundary[c] == NV_BC_SOLID)
+      return set_error(NV_ERR_UNSUPPORTED, "nv_calc_velocity_bs_static: solid boundaries need pinned records");
   unsigned char *base = nullptr;
   if ((rc = scratch_base(&base)) != NV_OK) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);

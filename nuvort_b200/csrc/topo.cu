@@ -177,7 +177,7 @@ __global__ void k_mark_recon(const SysConst *__restrict__ scs, const SysDyn *__r
     const int s = sys_of[g];
     const SysConst &sc = scs[s];
     const int k = (int)(g - sc.base);
-    if (k >= 1 && k <= dyn[s].pcount && recon_step(sc, dyn[s]) && nxt[g] != 0) {
+    if (k >= 1 && k <= dyn[s].pcount && recon_step(sc, dyn[s]) && nxt[g] != 0 && !walled(sc)) {
       const double cd = CD[g];
       a = (cd < sc.delta / 2.) && (cd > NV_EPS);
     }
@@ -196,7 +196,7 @@ __global__ void k_mark_remove(const SysConst *__restrict__ scs, const SysDyn *__
     const int s = sys_of[g];
     const SysConst &sc = scs[s];
     const int k = (int)(g - sc.base);
-    if (k >= 1 && k <= dyn[s].pcount && recon_step(sc, dyn[s]) && nxt[g] != 0) {
+    if (k >= 1 && k <= dyn[s].pcount && recon_step(sc, dyn[s]) && nxt[g] != 0 && !walled(sc)) {
       double x[3], y[3];
       load3(X, T, (int)g, x);
       load3(X, T, nxt[nxt[g]], y);
@@ -249,7 +249,10 @@ __global__ void k_cell_count(const SysConst *__restrict__ scs, const SysDyn *__r
   const SysConst &sc = scs[s];
   const CellGrid &G = grid[s];
   const int k = (int)(g - sc.base);
-  if (!*err && G.nc[0] > 0 && recon_step(sc, dyn[s]) && k >= 1 && k <= dyn[s].pcount && nxt[g] != 0) {
+  if (!*err && G.nc[0] > 0 && recon_step(sc, dyn[s]) && k >= 1 && k <= dyn[s].pcount && nxt[g] != 0 &&
+      pinned_at(sc, (int)g)) {
+    c = -2;  // a pinned point: neither a target nor a candidate (line.f90:142-149)
+  } else if (!*err && G.nc[0] > 0 && recon_step(sc, dyn[s]) && k >= 1 && k <= dyn[s].pcount && nxt[g] != 0) {
     double x[3];
     load3(X, T, (int)g, x);
     c = (int)(G.base + ((long long)cell_coord(G, 2, x[2]) * G.nc[1] + cell_coord(G, 1, x[1])) * G.nc[0] +
@@ -277,7 +280,9 @@ __global__ void k_pclose_cells(const SysConst *__restrict__ scs, const SysDyn *_
                                const int *__restrict__ items, int *__restrict__ cl, double *__restrict__ CD,
                                long long T) {
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= T || cell_of[g] < 0) return;  // listed: live slot of a cell-list system on a recon step
+  if (g >= T) return;
+  if (cell_of[g] == -2) CD[g] = 100.;  // pinned: closestd=100 and no search
+  if (cell_of[g] < 0) return;  // listed: live unpinned slot of a cell-list system on a recon step
   const int s = sys_of[g];
   const CellGrid &G = grid[s];
   const int ni = nxt[g], pi = prv[g];
@@ -338,6 +343,10 @@ __global__ void k_pclose_brute(const SysConst *__restrict__ scs, const SysDyn *_
   const int pc = dyn[s].pcount;
   const int k = (int)(g - sc.base);
   if (k < 1 || k > pc || nxt[g] == 0) return;
+  if (pinned_at(sc, (int)g)) {  // pinned points are not tested (line.f90:142-144)
+    CD[g] = 100.;
+    return;
+  }
   const int ni = nxt[g], pi = prv[g];
   double xi[3];
   load3(X, T, (int)g, xi);
@@ -345,7 +354,7 @@ __global__ void k_pclose_brute(const SysConst *__restrict__ scs, const SysDyn *_
   double best2 = 1e300;
   int bj = cl[g];
   for (int j = sc.base + 1; j <= sc.base + pc; ++j) {
-    if (nxt[j] == 0 || j == g || j == ni || j == pi) continue;
+    if (nxt[j] == 0 || j == g || j == ni || j == pi || pinned_at(sc, j)) continue;
     double xj[3];
     load3(X, T, j, xj);
     const double d2 = e_add(e_add(e_sq(e_sub(xi[0], xj[0])), e_sq(e_sub(xi[1], xj[1]))), e_sq(e_sub(xi[2], xj[2])));
@@ -361,23 +370,6 @@ __global__ void k_pclose_brute(const SysConst *__restrict__ scs, const SysDyn *_
   CD[g] = best;
 }
 
-
-// new point of an insertion (line.f90:62-79)
-__device__ void new_point(const double x[3], const double gi[3], const double gb[3], double disti, double xn[3]) {
-  double fdd[3];
-  deriv2(x, gi, gb, fdd);
-  double curv = e_sqrt(dot3(fdd, fdd));
-  const double mid[3] = {e_mul(0.5, e_add(x[0], gi[0])), e_mul(0.5, e_add(x[1], gi[1])), e_mul(0.5, e_add(x[2], gi[2]))};
-  for (int c = 0; c < 3; ++c) xn[c] = mid[c];
-  if (curv > 1E-5) {
-    curv = e_div(1.0, curv);
-    const double disc = e_sub(e_mul(curv, curv), e_mul(0.25, e_mul(disti, disti)));
-    if (disc > 0.) {
-      const double sfac = e_mul(e_sub(e_sqrt(disc), curv), curv);
-      for (int c = 0; c < 3; ++c) xn[c] = e_add(mid[c], e_mul(sfac, fdd[c]));
-    }
-  }
-}
 
 // g as seen from x: the nearest periodic image (get_ghost_p's adjustment)
 __device__ __forceinline__ void ghost_of(const SysConst &sc, const double x[3], const double g[3], double out[3]) {
@@ -408,7 +400,7 @@ __global__ void k_ins_mark(const SysConst *__restrict__ scs, SysDyn *__restrict_
     const int s = sys_of[g];
     const SysConst &sc = scs[s];
     const int k = (int)(g - sc.base);
-    if (k >= 1 && k <= dyn[s].pcount) {
+    if (k >= 1 && k <= dyn[s].pcount && !walled(sc)) {
       if (nxt[g] == 0) {
         b = 1;
       } else {
@@ -465,6 +457,7 @@ __global__ void __launch_bounds__(256) k_ins_total(const SysConst *__restrict__ 
   const int s = blockIdx.x;
   if (s >= nsys || *err) return;
   const SysConst &sc = scs[s];
+  if (walled(sc)) return;  // the serial sweep of solid.cu sums its own lengths
   const int pc = dyn[s].pcount;
   double acc = 0.;
   for (int k = 1 + threadIdx.x; k <= pc; k += 256) acc += seglen[sc.base + k];
@@ -797,6 +790,7 @@ __global__ void k_ins_finish(const SysConst *__restrict__ scs, SysDyn *dyn, int 
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nsys || *err) return;
   const SysConst &sc = scs[s];
+  if (walled(sc)) return;
   SysDyn &d = dyn[s];
   if (d.live == 0) {
     atomicOr(err, DERR_EMPTY);
@@ -1124,7 +1118,7 @@ __global__ void __launch_bounds__(kRound) k_recon_sweep(const SysConst *__restri
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   if (s >= nsys || *err) return;
   const SysConst &sc = scs[s];
-  if (!recon_step(sc, dyn[s])) return;
+  if (!recon_step(sc, dyn[s]) || walled(sc)) return;
   const int base = sc.base;
   for (int q = tid; q < RoundTouched::kCap; q += kRound) tkeys[q] = 0;
   for (int q = tid; q < kMapCap; q += kRound) mkey[q] = 0;
@@ -1264,7 +1258,7 @@ __global__ void __launch_bounds__(kRound) k_remove_sweep(const SysConst *__restr
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   if (s >= nsys || *err) return;
   const SysConst &sc = scs[s];
-  if (!recon_step(sc, dyn[s])) return;
+  if (!recon_step(sc, dyn[s]) || walled(sc)) return;
   const int base = sc.base;
   for (int q = tid; q < RoundTouched::kCap; q += kRound) tkeys[q] = 0;
   for (int q = tid; q < kMapCap; q += kRound) mkey[q] = 0;
@@ -1538,8 +1532,8 @@ __global__ void __launch_bounds__(32) k_insert_sweep(const SysConst *__restrict_
   const int s = blockIdx.x;
   const int lane = threadIdx.x;
   if (s >= nsys || *err) return;
-  if (!dyn[s].ins_fallback) return;
   const SysConst &sc = scs[s];
+  if (!dyn[s].ins_fallback || walled(sc)) return;
   const int base = sc.base;
   for (int q = lane; q < Set::kCap; q += 32) tkeys[q] = 0;
   Set tc{tkeys, 0, 0, base};
@@ -1928,6 +1922,7 @@ void launch_pinsert(nv_handle *h) {
                                                 tb->list_b, sw, h->d_err, h->d_events, h->d_event_count,
                                                 h->event_cap);
   k_ins_total<<<h->nsys, 256, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, tb->seglen, h->d_err);
+  launch_solid_pinsert(h);
 }
 
 void launch_pclose(nv_handle *h, bool only_brute) {
@@ -1961,6 +1956,7 @@ void launch_precon(nv_handle *h) {
   compact(h, tb->flag_a, tb->pos_a, tb->list_a);
   k_recon_sweep<<<h->nsys, kRound, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a, tb->list_a,
                                                h->d_err, h->d_events, h->d_event_count, h->event_cap);
+  launch_solid_precon(h);
 }
 
 void launch_premove(nv_handle *h) {
@@ -1975,4 +1971,5 @@ void launch_premove(nv_handle *h) {
   k_remove_sweep<<<h->nsys, kRound, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a, tb->list_a,
                                                 tb->flag_a, sw, h->d_err, h->d_events, h->d_event_count,
                                                 h->event_cap);
+  launch_solid_premove(h);
 }

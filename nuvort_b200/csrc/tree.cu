@@ -292,7 +292,8 @@ __device__ void make_children(TreeBuffers &tb, int p, const int cnt[8], int *id0
 // no child), which lists each child's members in slot order, as the warp and block splits
 // do node by node.
 __global__ void k_root_digits(const double *__restrict__ X, long long T, TreeBuffers tb,
-                              const int *__restrict__ sys_of, const int *__restrict__ pos) {
+                              const int *__restrict__ sys_of, const int *__restrict__ pos,
+                              const SysConst *__restrict__ scs) {
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= T) return;
   const int n_live = pos[T];
@@ -304,7 +305,9 @@ __global__ void k_root_digits(const double *__restrict__ X, long long T, TreeBuf
   const int g = tb.members[q];
   const int s = sys_of[g];
   int d = 8;
-  if (tb.nI[s].x >= 2) {
+  // a point pinned in front (its segment goes into the wall) counts in the root's centre but
+  // belongs to no child (new_tree, tree.f90:128)
+  if (tb.nI[s].x >= 2 && !(scs[s].pin && pin_i(scs[s].pin[g]))) {
     double x[3];
     load_x(X, T, g, x);
     d = octant(x, tb.nP[s], tb.nA[s].w / 2.0);
@@ -936,8 +939,96 @@ __device__ void fp64_epilogue(const SysConst &sc, const SysDyn &dy, int g, const
   for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], ub0[c]);
 #pragma unroll
   for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], ubs[c]);
+  if (sc.n_mirror)  // the mirrored trees' sum, walked before (k_tree_walk_mirror)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) u[c] = e_add(u[c], sc.umir[c * T + g]);
   mf_epilogue(sc, dy, xi, fdot, u, g);
   store3(U, T, g, u);
+}
+
+// tree_walk_mirror (tree.f90:321-392) for every mirror of target g, in mirror order, into
+// acc: each node's centre and centre + circulation reflected in the wall; theta = width/dist
+// (the reference computes the corrected angle and then overwrites it with this one); a leaf
+// whose segment goes into the wall, and the target's own image as biot_savart_mirror skips
+// it, add nothing; the accept test includes the root (its circulation is zero, so an accepted
+// root adds nothing either).
+__device__ void walk_mirror(const TreeBuffers &tb, int root, const SysConst &sc, const double xi[3], int g, int pi_,
+                            int pin_g, const int *__restrict__ prv, double acc[3], unsigned long long &evals,
+                            unsigned long long &tests, bool &singular) {
+  const double qc = sc.quant_circ, two_pi = sc.two_pi, theta0 = sc.tree_theta;
+  for (int m = 0; m < sc.n_mirror; ++m) {
+    const bool own = mirror_skips_own(sc, pin_g, m);
+    int node = root;
+    while (node != kEnd) {
+      const double4 A = ldg4(&tb.nA[node]);
+      const int4 I = __ldg(&tb.nI[node]);
+      if (I.x == 0) {
+        node = I.z;
+        continue;
+      }
+      ++tests;
+      const double4 B = ldg4(&tb.nB[node]);
+      const double cent[3] = {A.x, A.y, A.z}, circ[3] = {B.x, B.y, B.z};
+      double s[3], sgi[3];
+      for (int c = 0; c < 3; ++c) {
+        s[c] = reflect1(e_add(cent[c], circ[c]), sc.mirror[m][c], sc.box[c]);
+        sgi[c] = reflect1(cent[c], sc.mirror[m][c], sc.box[c]);
+      }
+      const double dist = e_sqrt(e_add(e_add(e_sq(e_sub(xi[0], s[0])), e_sq(e_sub(xi[1], s[1]))), e_sq(e_sub(xi[2], s[2]))));
+      const double theta = e_div(A.w, dist);
+      if (I.x == 1 || theta < theta0) {
+        node = (node == root) ? kEnd : I.z;
+        if (I.x == 1) {
+          const int j = __ldg(prv + I.w);
+          if (pin_i(sc.pin[j])) continue;
+          if (own && ((pin_b(pin_g) && g == j) || (pin_i(pin_g) && j == pi_))) continue;
+          if (dist < NV_EPS) {
+            singular = true;
+            continue;
+          }
+        }
+        const double vect[3] = {e_sub(s[0], xi[0]), e_sub(s[1], xi[1]), e_sub(s[2], xi[2])};
+        const double dv[3] = {e_sub(sgi[0], s[0]), e_sub(sgi[1], s[1]), e_sub(sgi[2], s[2])};
+        const double a = e_mul(dist, dist);
+        const double b = e_mul(2.0, dot3(vect, dv));
+        const double c = e_add(e_add(e_sq(e_sub(s[0], sgi[0])), e_sq(e_sub(s[1], sgi[1]))), e_sq(e_sub(s[2], sgi[2])));
+        const double D = e_sub(e_mul(e_mul(4.0, a), c), e_mul(b, b));
+        if (D < NV_EPS) continue;
+        double cr[3];
+        cross3(vect, dv, cr);
+        const double den = e_mul(two_pi, D);
+        const double fac = e_sub(e_div(e_add(e_mul(2.0, c), b), e_sqrt(e_add(e_add(a, b), c))), e_div(b, e_sqrt(a)));
+#pragma unroll
+        for (int k = 0; k < 3; ++k) acc[k] = e_add(acc[k], e_mul(e_div(e_mul(cr[k], qc), den), fac));
+        ++evals;
+      } else {
+        node = I.y != kEnd ? I.y : (node == root ? kEnd : I.z);
+      }
+    }
+  }
+}
+
+// The mirror sums of every live target of the tree systems with solid walls (one thread
+// each), written to umir for the FP64 walk's epilogue.  Runs after the roots' exact centres.
+__global__ void k_tree_walk_mirror(const SysConst *__restrict__ scs, SysDyn *dyn, const int2 *__restrict__ work,
+                                   const double *__restrict__ X, const int *__restrict__ nxt,
+                                   const int *__restrict__ prv, long long T, TreeBuffers tb, unsigned *err) {
+  const int2 w = work[blockIdx.x];
+  const SysConst &sc = scs[w.x];
+  if (!sc.n_mirror) return;
+  const int g = w.y + threadIdx.x;
+  const int k = g - sc.base;
+  unsigned long long evals = 0, tests = 0;
+  bool singular = false;
+  if (!*err && k >= 1 && k <= dyn[w.x].pcount && k <= sc.cap && nxt[g] != 0) {
+    double xi[3], acc[3] = {0, 0, 0};
+    load3(X, T, g, xi);
+    walk_mirror(tb, w.x, sc, xi, g, prv[g], sc.pin[g], prv, acc, evals, tests, singular);
+    for (int c = 0; c < 3; ++c) sc.umir[c * T + g] = acc[c];
+  }
+  if (singular) atomicOr(err, DERR_SINGULAR);
+  if (evals) atomicAdd(&dyn[w.x].tree_eval, evals);
+  if (tests) atomicAdd(&dyn[w.x].tree_tests, tests);
 }
 
 // The tree sums of target g (timestep.f90:49-141 with tree_walk): over the unshifted image
@@ -1092,6 +1183,10 @@ __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *_
     CD[g] = cd;
     return;
   }
+  if (pinned_at(sc, (int)g)) {  // pinned points are not tested (tree.f90:198-199)
+    CD[g] = cd;
+    return;
+  }
   const int pi_ = prv[g];
   int best = cl[g];
   double xi[3];
@@ -1141,7 +1236,7 @@ __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *_
           const int j = prv[I.w];
           if (I.x > 1) {
             best = 0;
-          } else if (j != (int)g && ni != j && pi_ != j) {
+          } else if (j != (int)g && ni != j && pi_ != j && !pinned_at(sc, j)) {  // pinned j: nothing
             best = j;
             cd = e_sqrt(d2);
             cd2 = cd * cd;
@@ -1614,7 +1709,7 @@ void launch_tree_build(nv_handle *h) {
   k_root_sums<<<h->nsys, kSumThreads, kSumSmem, h->side>>>(h->x, T, *tb, h->nsys, h->nxt, h->d_err);
   cudaEventRecord(h->join_ev, h->side);
   const int sms = n_sms();
-  k_root_digits<<<grid_for(T, TB), TB, 0, h->stream>>>(h->x, T, *tb, h->sys_of, tb->pos);
+  k_root_digits<<<grid_for(T, TB), TB, 0, h->stream>>>(h->x, T, *tb, h->sys_of, tb->pos, h->d_sc);
   {
     size_t sb = tb->rsort_bytes;
     cub::DeviceRadixSort::SortPairs(tb->rsort_tmp, sb, tb->rkey[0], tb->rkey[1], tb->rval[0], tb->rval[1], (int)T, 0,
@@ -1664,6 +1759,11 @@ void launch_walk_fixup(nv_handle *h) {
 void launch_tree_walk(nv_handle *h) {
   TreeBuffers *tb = h->tree;
   if (!tb || h->n_work_tree == 0) return;
+  if (h->any_mirror) {  // solid walls: the mirrored trees first, on the roots' exact centres
+    join_root_sums(h);
+    k_tree_walk_mirror<<<h->n_work_tree, 64, 0, h->stream>>>(h->d_sc, h->d_dyn, h->d_work_tree, h->x, h->nxt, h->prv,
+                                                             h->T, *tb, h->d_err);
+  }
   cudaMemsetAsync(tb->defer_n, 0, sizeof(int), h->stream);
   // two threads per target while the one-thread blocks would fill the GPU less than ~4
   // times (automatic), or as nv_set_walk_parts asks

@@ -118,3 +118,79 @@ def ensemble(seed: int, n_systems: int, nmin: int, nmax: int, delta: float,
     counts = np.maximum(np.round(counts).astype(int), 64)
     sub = rng.integers(0, 2**31 - 1, size=n_systems)
     return [random_rings(int(s), delta, box, n_points=int(n)) for s, n in zip(sub, counts)]
+
+
+def _pinned_state(x: np.ndarray, infront: np.ndarray, behind: np.ndarray, wpinned: np.ndarray,
+                  pinnedi: np.ndarray, pinnedb: np.ndarray) -> State:
+    n = x.shape[0]
+    z = lambda: np.zeros((n, 3), np.float64)
+    return State(x=np.ascontiguousarray(x), infront=infront.astype(np.int32), behind=behind.astype(np.int32),
+                 u=z(), u1=z(), u2=z(), ghosti=z(), ghostb=z(), closest=np.zeros(n, np.int32),
+                 closestd=np.zeros(n, np.float64), wpinned=wpinned.astype(np.int32),
+                 pinnedi=pinnedi.astype(np.int32), pinnedb=pinnedb.astype(np.int32))
+
+
+def half_loop(n: int, delta: float, box: Sequence[float] = (0.1, 0.1, 0.1), axis: int = 0) -> State:
+    """A half ring of n points standing on the solid wall at +L/2 of ``axis`` (0: x, the
+    setup_half_loop of src/initial_cond.f90:41-75; 2: z, setup_half_loopz :79-113): radius
+    0.75 n delta / pi, its first point pinned behind and its last pinned in front, both to
+    that wall.  Only x (in the x-y plane) and z (in the z-y plane) are set up there."""
+    if axis not in (0, 2):
+        raise ValueError("half loops stand on the x or z wall")
+    R = (0.75 * n * delta) / math.pi
+    k = np.arange(n)
+    s = np.sin(math.pi * k / (n - 1))
+    c = np.cos(math.pi * k / (n - 1))
+    x = np.zeros((n, 3), np.float64)
+    x[:, axis] = 0.5 * box[axis] - R * s
+    x[:, 1] = R * c
+    infront = np.minimum(k + 2, n)  # 1-based: the last point is its own infront
+    behind = np.maximum(k, 1)       # the first point is its own behind
+    w = np.zeros((n, 3), np.int32)
+    w[0, axis] = w[-1, axis] = 1
+    pi_ = np.zeros(n, np.int32)
+    pb_ = np.zeros(n, np.int32)
+    pi_[-1] = 1
+    pb_[0] = 1
+    return _pinned_state(x, infront, behind, w, pi_, pb_)
+
+
+def lattice(line_count: int, delta: float, box: Sequence[float] = (0.1, 0.1, 0.1),
+            lattice_ratio: float = 0.5) -> State:
+    """Straight lines from the +z wall to the -z wall on a triangular (hexagonal-number)
+    lattice, as setup_lattice (src/initial_cond.f90:252-318) draws them:
+    3 line_count (line_count - 1) + 1 lines of nint(L_z / (0.75 delta)) points each; a line's
+    first point sits on the +z wall pinned behind (wpinned 0,0,1), its last on the -z wall
+    pinned in front (wpinned 0,0,-1)."""
+    nl = 3 * line_count * (line_count - 1) + 1
+    per = int(math.floor(box[2] / (0.75 * delta) + 0.5))  # nint
+    r = [0.0]
+    th = [0.0]
+    for i in range(2, line_count + 1):
+        for j in range(1, (i - 1) * 6 + 1):
+            t = 2.0 * math.pi * (j - 1) / ((i - 1) * 6)
+            th.append(t)
+            r.append(0.5 * lattice_ratio * min(box[0], box[1]) * ((i - 1) / (line_count - 1)) *
+                     math.cos(math.pi / 6) / math.cos(math.fmod(t, 2 * math.pi / 6) - math.pi / 6))
+    n = nl * per
+    x = np.zeros((n, 3), np.float64)
+    infront = np.zeros(n, np.int64)
+    behind = np.zeros(n, np.int64)
+    w = np.zeros((n, 3), np.int32)
+    pi_ = np.zeros(n, np.int32)
+    pb_ = np.zeros(n, np.int32)
+    j = np.arange(per)
+    for i in range(nl):
+        rows = i * per + j  # 0-based rows; slot = row + 1
+        x[rows, 0] = r[i] * math.cos(th[i])
+        x[rows, 1] = r[i] * math.sin(th[i])
+        x[rows, 2] = box[2] / 2.0 - box[2] * j / (per - 1)
+        infront[rows] = rows + 2
+        behind[rows] = rows
+        infront[rows[-1]] = rows[-1] + 1
+        behind[rows[0]] = rows[0] + 1
+        pb_[rows[0]] = 1
+        w[rows[0], 2] = 1
+        pi_[rows[-1]] = 1
+        w[rows[-1], 2] = -1
+    return _pinned_state(x, infront, behind, w, pi_, pb_)

@@ -48,7 +48,8 @@ def lib():
         vp = C.c_void_p
         L.or_create.argtypes = [P(NvParams), P(vp)]
         for name in ("or_destroy", "or_ghostp", "or_construct_tree", "or_pmotion", "or_pinsert",
-                     "or_pclose", "or_precon", "or_premove", "or_enforce_boundary", "or_empty_tree",
+                     "or_pclose", "or_precon", "or_wall_recon", "or_premove", "or_enforce_boundary",
+                     "or_empty_tree",
                      "or_end_step"):
             getattr(L, name).argtypes = [vp]
         L.or_upload.argtypes = [vp, vp]

@@ -33,12 +33,14 @@ const double eps = 2.220446049250313e-16;  // epsilon(0.) for real(8)
 thread_local std::string g_err;
 thread_local long long tests_tls = 0;  // opening tests of the calling thread
 
-struct Pt {  // type(qvort), src/cdata.f90:19-29 (pinning fields omitted: periodic/open only)
+struct Pt {  // type(qvort), src/cdata.f90:19-29
   double x[3], u[3], u1[3], u2[3], u_mf[3], u_sup[3];
   double curv, stretch;
   double ghosti[3], ghostb[3];
   int infront, behind, closest;
   double closestd;
+  int wpinned[3];          // the wall a pinned point sits on (-1, 0 or 1 per axis)
+  bool pinnedi, pinnedb;   // the segment in front / behind goes into that wall
 };
 
 struct Node {  // type node, src/tree.f90:20-32
@@ -46,6 +48,7 @@ struct Node {  // type node, src/tree.f90:20-32
   int pcount;
   Node *child[8];  // fbl, fbr, ftl, ftr, bbl, bbr, btl, btr
   double centx, centy, centz;
+  double vec_cent[3];  // (centx, centy, centz), set with them
   double circ[3];
   int first;       // slot of parray(1)
   int first_next;  // parray(1)%infront at construction
@@ -85,6 +88,8 @@ struct Sys {
   int diag_live = 0;
   bool diag_valid = false;
   std::vector<std::array<double, 3>> shifts;  // periodic_loop_array
+  std::vector<std::array<int, 3>> mirrors;    // mirror_loop_array
+  int wall_recon_count = 0;
   Node *vtree = nullptr;
   std::vector<std::unique_ptr<Node>> pool;
   std::vector<nv_event> events;
@@ -109,6 +114,29 @@ struct Sys {
         }
   }
 
+  // ---- boundary.f90:180-212 create_mirror_loop_array --------------------------------------
+  void make_mirrors() {
+    mirrors.clear();
+    for (int i = -1; i <= 1; ++i)
+      for (int j = -1; j <= 1; ++j)
+        for (int k = -1; k <= 1; ++k) {
+          int ii, jj, kk;
+          if (p.boundary[0] == NV_BC_SOLID) ii = i;
+          else { if (i != 0) continue; ii = 0; }
+          if (p.boundary[1] == NV_BC_SOLID) jj = j;
+          else { if (j != 0) continue; jj = 0; }
+          if (p.boundary[2] == NV_BC_SOLID) kk = k;
+          else { if (k != 0) continue; kk = 0; }
+          if (ii == 0 && jj == 0 && kk == 0) continue;
+          mirrors.push_back({ii, jj, kk});
+        }
+  }
+  // v + 2|r|(0.5 r L - v) per component: the reflection of v in the walls r names
+  void reflect(const double *v, const int *r, double *out) const {
+    for (int c = 0; c < 3; ++c)
+      out[c] = v[c] + 2 * std::abs(r[c]) * (0.5 * r[c] * p.box_size[c] - v[c]);
+  }
+
   void ensure_size(int n) {
     if ((int)f.size() < n + 1) {
       Pt z;
@@ -123,13 +151,23 @@ struct Sys {
       q.x[c] = 0; q.u[c] = 0; q.u1[c] = 0; q.u2[c] = 0; q.ghosti[c] = 0; q.ghostb[c] = 0;
     }
     q.infront = 0; q.behind = 0; q.closest = 0; q.closestd = 0;
+    q.pinnedi = false; q.pinnedb = false;
+    q.wpinned[0] = q.wpinned[1] = q.wpinned[2] = 0;
   }
 
-  // ---- boundary.f90:26-84 get_ghost_p (non-pinned branch) ------------------------------
+  // ---- boundary.f90:26-84 get_ghost_p ------------------------------------------------------
   void get_ghost_p(int i, double *gi, double *gb) {
-    for (int c = 0; c < 3; ++c) {
-      gi[c] = f[f[i].infront].x[c];
-      gb[c] = f[f[i].behind].x[c];
+    if (f[i].pinnedi) {
+      for (int c = 0; c < 3; ++c) gb[c] = f[f[i].behind].x[c];
+      reflect(f[f[i].behind].x, f[i].wpinned, gi);
+    } else if (f[i].pinnedb) {
+      for (int c = 0; c < 3; ++c) gi[c] = f[f[i].infront].x[c];
+      reflect(f[f[i].infront].x, f[i].wpinned, gb);
+    } else {
+      for (int c = 0; c < 3; ++c) {
+        gi[c] = f[f[i].infront].x[c];
+        gb[c] = f[f[i].behind].x[c];
+      }
     }
     for (int c = 0; c < 3; ++c) {
       if (p.boundary[c] != NV_BC_PERIODIC) continue;
@@ -149,7 +187,7 @@ struct Sys {
     }
   }
 
-  void enforce_boundary() {  // boundary.f90:91-138 (periodic part)
+  void enforce_boundary() {  // boundary.f90:91-138
 #pragma omp parallel for schedule(static)
     for (int i = 1; i <= pcount; ++i) {
       if (f[i].infront == 0) continue;
@@ -158,6 +196,13 @@ struct Sys {
         const double L = p.box_size[c];
         if (f[i].x[c] > (L / 2.0)) f[i].x[c] = f[i].x[c] - L;
         else if (f[i].x[c] < (-L / 2.0)) f[i].x[c] = f[i].x[c] + L;
+      }
+      if (f[i].pinnedi || f[i].pinnedb) {  // back onto the wall: maxloc(abs(wpinned)), first on ties
+        int pc = 0;
+        for (int c = 1; c < 3; ++c)
+          if (std::abs(f[i].wpinned[c]) > std::abs(f[i].wpinned[pc])) pc = c;
+        if (f[i].wpinned[pc] > 0) f[i].x[pc] = 0.499999999 * p.box_size[pc];
+        else if (f[i].wpinned[pc] < 0) f[i].x[pc] = -0.499999999 * p.box_size[pc];
       }
     }
   }
@@ -190,6 +235,7 @@ struct Sys {
     for (int j = 1; j <= pcount; ++j) {
       const Pt &qj = f[j];
       if (qj.infront == 0 || i == j || qi.behind == j) continue;
+      if (qj.pinnedi) continue;  // the segment into the wall
       double r[3], d[3];
       for (int c = 0; c < 3; ++c) { r[c] = qj.x[c] - qi.x[c]; d[c] = qj.ghosti[c] - qj.x[c]; }
       double a_bs = dist_gen_sq(qj.x, qi.x);
@@ -213,6 +259,7 @@ struct Sys {
     for (int j = 1; j <= pcount; ++j) {
       const Pt &qj = f[j];
       if (qj.infront == 0 || qi.behind == j) continue;
+      if (qj.pinnedi) continue;
       double xs[3], r[3], d[3];
       for (int c = 0; c < 3; ++c) {
         xs[c] = qj.x[c] + shift[c];
@@ -232,6 +279,85 @@ struct Sys {
         ub[c] = ub[c] * fac;
         u[c] = u[c] + ub[c];
       }
+    }
+  }
+
+  // the own-image skip of the mirror sums (timestep.f90:215-218, tree.f90:365-368)
+  bool own_image_skipped(int i, int j, const int *reflect) const {
+    const Pt &qi = f[i];
+    const int d = (qi.wpinned[0] - reflect[0]) + (qi.wpinned[1] - reflect[1]) + (qi.wpinned[2] - reflect[2]);
+    if (d == 0 && (qi.wpinned[0] + qi.wpinned[1] + qi.wpinned[2]) < 2) {
+      if (qi.pinnedb && i == j) return true;
+      if (qi.pinnedi && j == qi.behind) return true;
+    }
+    return false;
+  }
+  // ---- timestep.f90:201-234 biot_savart_mirror ----------------------------------------------
+  void biot_savart_mirror(int i, double *u, const int *reflect_) const {
+    const Pt &qi = f[i];
+    for (int j = 1; j <= pcount; ++j) {
+      const Pt &qj = f[j];
+      if (qj.infront == 0 || qj.pinnedi) continue;
+      if (own_image_skipped(i, j, reflect_)) continue;
+      double s_gi_img[3], s_img[3], r[3], d[3];
+      reflect(qj.x, reflect_, s_gi_img);
+      reflect(qj.ghosti, reflect_, s_img);
+      for (int c = 0; c < 3; ++c) { r[c] = s_img[c] - qi.x[c]; d[c] = s_gi_img[c] - s_img[c]; }
+      double a_bs = dist_gen_sq(qi.x, s_img);
+      double b_bs = 2.0 * dot3(r, d);
+      double c_bs = dist_gen_sq(s_img, s_gi_img);
+      if (4 * a_bs * c_bs - b_bs * b_bs == 0) continue;
+      double ub[3];
+      cross_product(r, d, ub);
+      const double den = (2 * pi) * (4 * a_bs * c_bs - b_bs * b_bs);
+      const double fac = (2 * c_bs + b_bs) / std::sqrt(a_bs + b_bs + c_bs) - (b_bs / std::sqrt(a_bs));
+      for (int c = 0; c < 3; ++c) {
+        ub[c] = ub[c] * p.quant_circ / den;
+        ub[c] = ub[c] * fac;
+        u[c] = u[c] + ub[c];
+      }
+    }
+  }
+
+  // ---- tree.f90:321-396 tree_walk_mirror -----------------------------------------------------
+  // theta is width/dist whatever tree_extra_correction says: the reference computes the
+  // corrected value and then overwrites it (tree.f90:354).
+  void tree_walk_mirror(int i, const Node *n, const int *reflect_, double *u, long long &evals,
+                        int &singular) const {
+    if (n->pcount == 0) return;
+    ++tests_tls;
+    const Pt &qi = f[i];
+    double s_img[3], s_gi_img[3], sc_[3];
+    for (int c = 0; c < 3; ++c) sc_[c] = n->vec_cent[c] + n->circ[c];
+    reflect(n->vec_cent, reflect_, s_gi_img);
+    reflect(sc_, reflect_, s_img);
+    const double dist = dist_gen(qi.x, s_img);
+    const double theta = n->width / dist;
+    if (n->pcount == 1 || theta < p.tree_theta) {
+      if (n->pcount == 1) {
+        const int j = f[n->first_next].behind;
+        if (f[j].pinnedi) return;
+        if (own_image_skipped(i, j, reflect_)) return;
+        if (dist < eps) { singular = 1; return; }
+      }
+      double r[3], d[3];
+      for (int c = 0; c < 3; ++c) { r[c] = s_img[c] - qi.x[c]; d[c] = s_gi_img[c] - s_img[c]; }
+      double a_bs = dist * dist;
+      double b_bs = 2.0 * dot3(r, d);
+      double c_bs = dist_gen_sq(s_img, s_gi_img);
+      if (4 * a_bs * c_bs - b_bs * b_bs < eps) return;
+      double ub[3];
+      cross_product(r, d, ub);
+      const double den = (2 * pi) * (4 * a_bs * c_bs - b_bs * b_bs);
+      const double fac = (2 * c_bs + b_bs) / std::sqrt(a_bs + b_bs + c_bs) - (b_bs / std::sqrt(a_bs));
+      for (int c = 0; c < 3; ++c) {
+        ub[c] = ub[c] * p.quant_circ / den;
+        ub[c] = ub[c] * fac;
+        u[c] = u[c] + ub[c];
+      }
+      ++evals;
+    } else {
+      for (int k = 0; k < 8; ++k) tree_walk_mirror(i, n->child[k], reflect_, u, evals, singular);
     }
   }
 
@@ -407,6 +533,9 @@ struct Sys {
         u_bs[0] = u_bs[1] = u_bs[2] = 0.0;
         for (const auto &s : shifts) biot_savart_shift(i, u_bs, s.data());
         for (int c = 0; c < 3; ++c) u[c] = u[c] + u_bs[c];
+        double u_mir[3] = {0.0, 0.0, 0.0};
+        for (const auto &m : mirrors) biot_savart_mirror(i, u_mir, m.data());
+        for (int c = 0; c < 3; ++c) u[c] = u[c] + u_mir[c];
       } else {
         const double zero[3] = {0.0, 0.0, 0.0};
         tree_walk(i, vtree, zero, u_bs, evals, singular);
@@ -414,6 +543,9 @@ struct Sys {
         u_bs[0] = u_bs[1] = u_bs[2] = 0.0;
         for (const auto &s : shifts) tree_walk(i, vtree, s.data(), u_bs, evals, singular);
         for (int c = 0; c < 3; ++c) u[c] = u[c] + u_bs[c];
+        double u_mir[3] = {0.0, 0.0, 0.0};
+        for (const auto &m : mirrors) tree_walk_mirror(i, vtree, m.data(), u_mir, evals, singular);
+        for (int c = 0; c < 3; ++c) u[c] = u[c] + u_mir[c];
       }
     }
     for (int c = 0; c < 3; ++c) qi.u_sup[c] = u[c];
@@ -494,6 +626,7 @@ struct Sys {
     for (int k : parray) {
       const Pt &q = f[k];
       if (q.infront == 0) continue;
+      if (q.pinnedi) continue;  // the segment into the wall is not part of the tree
       if ((q.x[0] >= posx) && (q.x[0] < (posx + width)) && (q.x[1] >= posy) &&
           (q.x[1] < (posy + width)) && (q.x[2] >= posz) && (q.x[2] < (posz + width))) {
         counter = counter + 1;
@@ -511,6 +644,7 @@ struct Sys {
       n->centy = n->centy / counter;
       n->centz = n->centz / counter;
     }
+    n->vec_cent[0] = n->centx; n->vec_cent[1] = n->centy; n->vec_cent[2] = n->centz;
     n->pcount = counter;
     if (counter > 0) { n->first = mine[0]; n->first_next = f[mine[0]].infront; }
     build_tree(n, mine);
@@ -546,6 +680,7 @@ struct Sys {
       if (f[i].infront > 0) { sx = sx + f[i].x[0]; sy = sy + f[i].x[1]; sz = sz + f[i].x[2]; ++cnt; }
     }
     r->centx = sx / cnt; r->centy = sy / cnt; r->centz = sz / cnt;
+    r->vec_cent[0] = r->centx; r->vec_cent[1] = r->centy; r->vec_cent[2] = r->centz;
     r->circ[0] = r->circ[1] = r->circ[2] = 0.0;
     r->first = 1;
     r->first_next = pcount >= 1 ? f[1].infront : 0;
@@ -585,8 +720,12 @@ struct Sys {
         if (n->pcount > 1) {
           f[i].closest = 0;
         } else if ((i != j) && (f[i].infront != j) && (f[i].behind != j)) {
-          f[i].closest = j;
-          f[i].closestd = dist;
+          if (f[j].pinnedi || f[j].pinnedb) {
+            // pinned: nothing
+          } else {
+            f[i].closest = j;
+            f[i].closestd = dist;
+          }
         }
       }
     } else {
@@ -598,6 +737,7 @@ struct Sys {
     for (int i = 1; i <= pcount; ++i) {
       f[i].closestd = 100.0;
       if (f[i].infront == 0) continue;
+      if (f[i].pinnedi || f[i].pinnedb) continue;
       closest_tree(i, vtree);
     }
   }
@@ -607,9 +747,10 @@ struct Sys {
     for (int i = 1; i <= pcount; ++i) {
       if (f[i].infront == 0) continue;
       f[i].closestd = 100.0;
+      if (f[i].pinnedi || f[i].pinnedb) continue;
       for (int j = 1; j <= pcount; ++j) {
         if (f[j].infront == 0) continue;
-        if ((i != j) && (f[i].infront != j) && (f[i].behind != j)) {
+        if ((i != j) && (f[i].infront != j) && (f[i].behind != j) && !f[j].pinnedi && !f[j].pinnedb) {
           const double dist = dist_gen(f[i].x, f[j].x);
           if (dist < f[i].closestd) { f[i].closest = j; f[i].closestd = dist; }
         }
@@ -622,6 +763,7 @@ struct Sys {
     int counter = 1;
     int next = particle;
     for (int i = 1; i <= pcount; ++i) {
+      if (f[next].pinnedi || f[next].pinnedb) return;
       next = f[next].infront;
       if (next == particle) break;
       counter = counter + 1;
@@ -705,6 +847,7 @@ struct Sys {
     total_length = 0.0;
     for (int i = 1; i <= old_pcount; ++i) {
       if (f[i].infront == 0) continue;
+      if (f[i].pinnedi) continue;
       const double disti = dist_gen(f[i].x, f[i].ghosti);
       total_length = total_length + disti;
       if (disti > p.delta) {
@@ -734,6 +877,8 @@ struct Sys {
         }
         for (int c = 0; c < 3; ++c) qn.u[c] = 0.5 * (f[i].u[c] + f[f[i].infront].u[c]);
         for (int c = 0; c < 3; ++c) { qn.u1[c] = 0.0; qn.u2[c] = 0.0; }
+        qn.pinnedi = false; qn.pinnedb = false;
+        qn.wpinned[0] = qn.wpinned[1] = qn.wpinned[2] = 0;
         qn.behind = i;
         qn.infront = f[i].infront;
         get_ghost_p(par_new, qn.ghosti, qn.ghostb);
@@ -756,7 +901,9 @@ struct Sys {
   void premove() {
     for (int i = 1; i <= pcount; ++i) {
       if (f[i].infront == 0) continue;
+      if (f[i].pinnedi) continue;
       const int infront = f[i].infront;
+      if (f[infront].pinnedi) continue;
       const double distii = dist_gen(f[i].x, f[f[infront].infront].x);
       if (distii < .99 * p.delta) {
         const int tinfront = f[f[i].infront].infront;
@@ -766,6 +913,45 @@ struct Sys {
         events.push_back(nv_event{itime, NV_EV_REMOVE, i, infront});
         loop_killer(i);
         remove_count = remove_count + 1;
+      }
+      clear_wall_pair(i);
+    }
+  }
+  // two wall points next to each other cleared together (line.f90:125-127,
+  // reconnection.f90:71-75); logged as one event with the number of points cleared
+  bool clear_wall_pair(int i) {
+    if (!f[i].pinnedb) return false;  // (a cleared i is not pinned: f(0) is never read)
+    const int nx = f[i].infront;
+    if (!f[nx].pinnedi) return false;
+    events.push_back(nv_event{itime, NV_EV_CLEAR, i, nx == i ? 1 : 2});
+    clear_particle(nx);
+    clear_particle(i);
+    return true;
+  }
+
+  // ---- reconnection.f90:66-150 wall_recon ------------------------------------------------------
+  void wall_recon() {
+    for (int i = 1; i <= pcount; ++i) {
+      if (f[i].infront == 0) continue;
+      clear_wall_pair(i);
+      if (f[i].pinnedi || f[i].pinnedb) continue;
+      for (int a = 0; a < 3; ++a) {  // the x, y and z blocks in turn
+        if (p.boundary[a] != NV_BC_SOLID) continue;
+        int side = 0;
+        if (f[i].x[a] > 0.5 * (p.box_size[a] - p.delta)) side = 1;
+        else if (f[i].x[a] < -0.5 * (p.box_size[a] - p.delta)) side = -1;
+        if (side == 0) continue;
+        const int pari = f[i].infront, parb = f[i].behind;
+        f[pari].pinnedb = true; f[pari].behind = pari;
+        for (int c = 0; c < 3; ++c) f[pari].wpinned[c] = c == a ? side : 0;
+        f[parb].pinnedi = true; f[parb].infront = parb;
+        for (int c = 0; c < 3; ++c) f[parb].wpinned[c] = c == a ? side : 0;
+        clear_particle(i);
+        int cleared = 1;
+        if (f[pari].pinnedi && f[pari].pinnedb) { clear_particle(pari); ++cleared; }
+        if (f[parb].pinnedi && f[parb].pinnedb) { clear_particle(parb); ++cleared; }
+        events.push_back(nv_event{itime, NV_EV_WALL, i, cleared});
+        wall_recon_count = wall_recon_count + 1;
       }
     }
   }
@@ -827,6 +1013,7 @@ struct Sys {
       if (p.tree_theta > 0) pclose_tree();
       else pclose();
       precon();
+      wall_recon();
       premove();
     }
     enforce_boundary();
@@ -852,11 +1039,10 @@ extern "C" {
 
 int or_create(const nv_params *p, or_handle **out) {
   if (!p || !out) return fail(NV_ERR_ARG, "null argument");
-  for (int c = 0; c < 3; ++c)
-    if (p->boundary[c] == NV_BC_SOLID) return fail(NV_ERR_UNSUPPORTED, "solid boundaries are not supported");
   auto *h = new or_handle();
   h->s.p = *p;
   h->s.make_shifts();
+  h->s.make_mirrors();
   h->s.ensure_size(0);
   *out = h;
   return NV_OK;
@@ -889,6 +1075,9 @@ int or_upload(or_handle *h, const nv_host_state *st) {
     q.behind = st->behind[k - 1];
     q.closest = st->closest ? st->closest[k - 1] : 0;
     q.closestd = st->closestd ? st->closestd[k - 1] : 0.0;
+    for (int c = 0; c < 3; ++c) q.wpinned[c] = st->wpinned ? st->wpinned[3 * (k - 1) + c] : 0;
+    q.pinnedi = st->pinnedi && st->pinnedi[k - 1];
+    q.pinnedb = st->pinnedb && st->pinnedb[k - 1];
   }
   s.events.clear();
   return NV_OK;
@@ -914,6 +1103,10 @@ int or_download(or_handle *h, nv_host_state *st, int32_t cap) {
     if (st->behind) st->behind[k - 1] = q.behind;
     if (st->closest) st->closest[k - 1] = q.closest;
     if (st->closestd) st->closestd[k - 1] = q.closestd;
+    for (int c = 0; c < 3; ++c)
+      if (st->wpinned) st->wpinned[3 * (k - 1) + c] = q.wpinned[c];
+    if (st->pinnedi) st->pinnedi[k - 1] = q.pinnedi;
+    if (st->pinnedb) st->pinnedb[k - 1] = q.pinnedb;
   }
   return NV_OK;
 }
@@ -934,6 +1127,7 @@ int or_counters_get(or_handle *h, nv_counters *c) {
   c->remove_count = s.remove_count;
   c->insert_count = s.insert_count;
   c->loop_kills = s.loop_kills;
+  c->wall_recon_count = s.wall_recon_count;
   c->tree_eval = s.tree_eval;
   c->tree_tests = s.tree_tests;
   c->itime = s.itime;
@@ -982,7 +1176,7 @@ int or_ts_row_get(or_handle *h, nv_ts_row *row) {  // the values print_info writ
   row->itime = s.itime;
   row->live = s.diag_live;
   row->recon_count = s.recon_count;
-  row->wall_recon_count = 0;
+  row->wall_recon_count = s.wall_recon_count;
   row->remove_count = s.remove_count;
   row->tree_eval = s.tree_eval;
   row->t = s.t;
@@ -1023,13 +1217,17 @@ int or_download_full(or_handle *h, nv_full_state *st, int32_t cap) {
     if (st->behind) st->behind[k - 1] = q.behind;
     if (st->closest) st->closest[k - 1] = q.closest;
     if (st->closestd) st->closestd[k - 1] = q.closestd;
+    for (int c = 0; c < 3; ++c)
+      if (st->wpinned) st->wpinned[3 * (k - 1) + c] = q.wpinned[c];
+    if (st->pinnedi) st->pinnedi[k - 1] = q.pinnedi;
+    if (st->pinnedb) st->pinnedb[k - 1] = q.pinnedb;
   }
   return NV_OK;
 }
 
 int or_upload_full(or_handle *h, const nv_full_state *st) {
   nv_host_state hs{st->pcount, st->x, st->u, st->u1, st->u2, st->ghosti, st->ghostb,
-                   st->infront, st->behind, st->closest, st->closestd};
+                   st->infront, st->behind, st->closest, st->closestd, st->wpinned, st->pinnedi, st->pinnedb};
   int rc = or_upload(h, &hs);
   if (rc) return rc;
   for (int k = 1; k <= st->pcount; ++k) {
@@ -1085,7 +1283,6 @@ int or_write_dump(or_handle *h, const char *path) {
   }
   const int32_t m = 248 * s.pcount;  // write(53) f
   std::fwrite(&m, 4, 1, fp);
-  const int32_t zero = 0;
   for (int i = 1; i <= s.pcount; ++i) {
     const Pt &q = s.f[i];
     std::fwrite(q.x, 8, 3, fp); std::fwrite(q.u, 8, 3, fp); std::fwrite(q.u1, 8, 3, fp);
@@ -1094,7 +1291,8 @@ int or_write_dump(or_handle *h, const char *path) {
     std::fwrite(q.ghosti, 8, 3, fp); std::fwrite(q.ghostb, 8, 3, fp);
     std::fwrite(&q.infront, 4, 1, fp); std::fwrite(&q.behind, 4, 1, fp); std::fwrite(&q.closest, 4, 1, fp);
     std::fwrite(&q.closestd, 8, 1, fp);
-    for (int c = 0; c < 5; ++c) std::fwrite(&zero, 4, 1, fp);  // wpinned(3), pinnedi, pinnedb: .false.
+    const int32_t pin[5] = {q.wpinned[0], q.wpinned[1], q.wpinned[2], q.pinnedi ? 1 : 0, q.pinnedb ? 1 : 0};
+    std::fwrite(pin, 4, 5, fp);  // wpinned(3), pinnedi, pinnedb (gfortran .true. is 1)
   }
   std::fwrite(&m, 4, 1, fp);
   std::fclose(fp);
@@ -1135,6 +1333,7 @@ int or_pclose(or_handle *h) {
   return NV_OK;
 }
 int or_precon(or_handle *h) { h->s.precon(); return NV_OK; }
+int or_wall_recon(or_handle *h) { h->s.wall_recon(); return NV_OK; }
 int or_premove(or_handle *h) { h->s.premove(); return NV_OK; }
 int or_enforce_boundary(or_handle *h) { h->s.enforce_boundary(); return NV_OK; }
 int or_empty_tree(or_handle *h) { h->s.empty_tree(); return NV_OK; }

@@ -54,6 +54,7 @@ int or_pmotion(or_handle *h);
 int or_pinsert(or_handle *h);
 int or_pclose(or_handle *h);
 int or_precon(or_handle *h);
+int or_wall_recon(or_handle *h);
 int or_premove(or_handle *h);
 int or_enforce_boundary(or_handle *h);
 int or_empty_tree(or_handle *h);

@@ -56,6 +56,8 @@ def test_timestep_check():
 
 def test_unsupported_options_are_refused():
     p = make_params(dt=2e-5, delta=0.002, box_size=0.1, boundary_x="solid")
+    api.check_params(p)  # solid walls run in FP64
+    p = make_params(dt=2e-5, delta=0.002, box_size=0.1, boundary_x="solid", precision="mixed")
     with pytest.raises(api.NuvortError) as e:
         api.check_params(p)
     assert e.value.code == NV_ERR_UNSUPPORTED

@@ -92,7 +92,7 @@ def test_snapshot_layout_matches_matlab_reader(stepped, tmp_path):
 
 def test_dump_reader_refusals(stepped, tmp_path):
     from nuvort_b200 import api
-    from nuvort_b200.abi import NV_ERR_IO, NV_ERR_UNSUPPORTED
+    from nuvort_b200.abi import NV_ERR_IO
     path = tmp_path / "var.dat"
     stepped.write_dump(str(path))
     raw = path.read_bytes()
@@ -102,11 +102,12 @@ def test_dump_reader_refusals(stepped, tmp_path):
     assert e.value.code == NV_ERR_IO
     pinned = bytearray(raw)
     first = 3 * 12 + 16 + 4  # start of f's first element
+    pinned[first + 228:first + 232] = struct.pack("<i", -1)  # wpinned(1) = -1
     pinned[first + 240:first + 244] = struct.pack("<i", 1)  # pinnedi = .true.
     (tmp_path / "pinned.dat").write_bytes(bytes(pinned))
-    with pytest.raises(api.NuvortError) as e:
-        api.dump_read_file(str(tmp_path / "pinned.dat"))
-    assert e.value.code == NV_ERR_UNSUPPORTED
+    st, _, _, _ = api.dump_read_file(str(tmp_path / "pinned.dat"))  # the reader keeps the pinned fields
+    assert st.pinnedi[0] == 1 and st.pinnedb[0] == 0 and list(st.wpinned[0]) == [-1, 0, 0]
+    assert not st.pinnedi[1:].any() and not st.wpinned[1:].any()
     with pytest.raises(api.NuvortError) as e:
         api.dump_read_file(str(tmp_path / "missing.dat"))
     assert e.value.code == NV_ERR_IO

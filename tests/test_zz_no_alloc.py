@@ -129,3 +129,13 @@ def test_static_entry_refuses_oversized_systems():
     rc = f(C.byref(p), 32769, 1, 1, 1, 0.0, 1, None)  # refused before any pointer is used
     assert rc == NV_ERR_CAPACITY
     assert b"32768" in L.nv_last_error()
+
+
+def test_static_entry_refuses_solid_walls():
+    # pinned records are not among its arguments: a system with a solid wall is refused
+    # before any pointer is used, and the output stays unwritten
+    from nuvort_b200.abi import NV_ERR_UNSUPPORTED
+    st = tangle(0, 0.002, n_rings=4)
+    rc, u, msg = _static_call(config0_params(boundary_y="solid"), st, fill=-7.0)
+    assert rc == NV_ERR_UNSUPPORTED and "solid" in msg
+    assert np.all(u == -7.0)
