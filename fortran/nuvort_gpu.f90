@@ -30,10 +30,14 @@ module nuvort_gpu
     real(c_double) :: norm_shear_omega
   end type
 
+  integer(c_int32_t), parameter :: NV_EV_INSERT = 1, NV_EV_RECON = 2, NV_EV_REMOVE = 3
+  integer(c_int32_t), parameter :: NV_EV_LOOPKILL = 4, NV_EV_WALL = 5, NV_EV_CLEAR = 6
+
   type, bind(c) :: nv_host_state
     integer(c_int32_t) :: pcount
     type(c_ptr) :: x, u, u1, u2, ghosti, ghostb
     type(c_ptr) :: infront, behind, closest, closestd
+    type(c_ptr) :: wpinned, pinnedi, pinnedb  ! solid walls: wpinned(3,pcount), logicals as 0/1
   end type
 
   type, bind(c) :: nv_counters
@@ -42,6 +46,7 @@ module nuvort_gpu
     integer(c_int32_t) :: itime, n_events
     real(c_double) :: t
     integer(c_int64_t) :: event_hash  ! unsigned on the C side; compare bit patterns only
+    integer(c_int32_t) :: wall_recon_count, reserved
   end type
 
   !> one data/ts.log row (print_info) and the values behind it
@@ -124,6 +129,10 @@ module nuvort_gpu
       type(c_ptr), value :: h
     end function
     integer(c_int) function nv_precon(h) bind(c, name='nv_precon')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function nv_wall_recon(h) bind(c, name='nv_wall_recon')
       import :: c_int, c_ptr
       type(c_ptr), value :: h
     end function
@@ -265,7 +274,7 @@ contains
     type(nv_params) :: p(1)
     integer(c_int32_t) :: caps(1)
     real(c_double), allocatable, target :: x(:,:), u(:,:), u1(:,:), u2(:,:)
-    integer(c_int32_t), allocatable, target :: inf(:), beh(:)
+    integer(c_int32_t), allocatable, target :: inf(:), beh(:), wp(:,:), pi(:), pb(:)
     type(nv_host_state) :: st
     integer :: i
     if (.not. c_associated(nv_h)) then
@@ -274,15 +283,23 @@ contains
       call nv_check(nv_create(p, 1_c_int32_t, caps, 0_c_int32_t, nv_h), 'nuvort_gpu:nv_create')
     end if
     allocate(x(3,pcount), u(3,pcount), u1(3,pcount), u2(3,pcount), inf(pcount), beh(pcount))
+    allocate(wp(3,pcount), pi(pcount), pb(pcount))
     do i = 1, pcount
       x(:,i) = f(i)%x ; u(:,i) = f(i)%u ; u1(:,i) = f(i)%u1 ; u2(:,i) = f(i)%u2
       inf(i) = f(i)%infront ; beh(i) = f(i)%behind
+      wp(:,i) = f(i)%wpinned
+      pi(i) = merge(1, 0, f(i)%pinnedi) ; pb(i) = merge(1, 0, f(i)%pinnedb)
     end do
     st%pcount = pcount
     st%x = c_loc(x) ; st%u = c_loc(u) ; st%u1 = c_loc(u1) ; st%u2 = c_loc(u2)
     st%ghosti = c_null_ptr ; st%ghostb = c_null_ptr
     st%infront = c_loc(inf) ; st%behind = c_loc(beh)
     st%closest = c_null_ptr ; st%closestd = c_null_ptr
+    if (n_mirror > 0) then
+      st%wpinned = c_loc(wp) ; st%pinnedi = c_loc(pi) ; st%pinnedb = c_loc(pb)
+    else
+      st%wpinned = c_null_ptr ; st%pinnedi = c_null_ptr ; st%pinnedb = c_null_ptr
+    end if
     call nv_check(nv_upload(nv_h, 0_c_int32_t, st), 'nuvort_gpu:nv_upload')
     call nv_check(nv_set_clock(nv_h, 0_c_int32_t, t, int(itime, c_int32_t)), 'nuvort_gpu:nv_set_clock')
   end subroutine
@@ -292,16 +309,18 @@ contains
     use cdata
     integer, intent(in) :: cap
     real(c_double), allocatable, target :: x(:,:), u(:,:), u1(:,:), u2(:,:)
-    integer(c_int32_t), allocatable, target :: inf(:), beh(:)
+    integer(c_int32_t), allocatable, target :: inf(:), beh(:), wp(:,:), pi(:), pb(:)
     type(qvort), allocatable :: tmp(:)
     type(nv_host_state) :: st
     type(nv_counters) :: c
     integer :: i
     allocate(x(3,cap), u(3,cap), u1(3,cap), u2(3,cap), inf(cap), beh(cap))
+    allocate(wp(3,cap), pi(cap), pb(cap))
     st%x = c_loc(x) ; st%u = c_loc(u) ; st%u1 = c_loc(u1) ; st%u2 = c_loc(u2)
     st%ghosti = c_null_ptr ; st%ghostb = c_null_ptr
     st%infront = c_loc(inf) ; st%behind = c_loc(beh)
     st%closest = c_null_ptr ; st%closestd = c_null_ptr
+    st%wpinned = c_loc(wp) ; st%pinnedi = c_loc(pi) ; st%pinnedb = c_loc(pb)
     call nv_check(nv_download(nv_h, 0_c_int32_t, st, int(cap, c_int32_t)), 'nuvort_gpu:nv_download')
     if (st%pcount > size(f)) then
       allocate(tmp(st%pcount)) ; tmp(:)%infront = 0
@@ -312,9 +331,11 @@ contains
     do i = 1, pcount
       f(i)%x = x(:,i) ; f(i)%u = u(:,i) ; f(i)%u1 = u1(:,i) ; f(i)%u2 = u2(:,i)
       f(i)%infront = inf(i) ; f(i)%behind = beh(i)
+      f(i)%wpinned = wp(:,i) ; f(i)%pinnedi = pi(i) /= 0 ; f(i)%pinnedb = pb(i) /= 0
     end do
     call nv_check(nv_counters_get(nv_h, 0_c_int32_t, c), 'nuvort_gpu:nv_counters_get')
     recon_count = c%recon_count ; remove_count = c%remove_count ; t = c%t
+    wall_recon_count = c%wall_recon_count
   end subroutine
 
 end module
