@@ -339,6 +339,7 @@ def compare_arms(params, states, args, local, flush, torch, dist, steps, warmup,
         for h in (hm, hp):  # fresh state for the timed run
             for s, st in enumerate(states):
                 h.upload(s, st, t=0.0, itime=0)
+        hm.set_event_margins(True)  # how close the compared events came to flipping
     for _ in range(warmup):
         hm.step(1)
         if hp is not None:
@@ -366,7 +367,31 @@ def compare_arms(params, states, args, local, flush, torch, dist, steps, warmup,
         err["events_compared"] = int(sum(c.n_events for c in cp))
         err["steps_compared"] = warmup + steps
         err["events_compared_by"] = "per-system event count and order-sensitive 64-bit digest"
+        err.update(margin_report(hm, hp, params, len(states)))
     return out, hm, hp, caps
+
+
+def margin_report(hm, hp, params, nsys):
+    """The mixed arm's event margins (smallest relative distance of any topology test from
+    its threshold, over every step run) against the largest position difference between the
+    two arms at the end: a distance test moves by at most 2 dev / threshold and the tangent
+    dot by about 4 dev / delta, so margins far above 4 dev / delta leave the events safe."""
+    keys = ("insert", "remove", "recon_distance", "recon_dot")
+    mins = {k: 1e300 for k in keys}
+    dev, need = 0.0, 0.0
+    for s in range(nsys):
+        mg = hm.event_margins(s)
+        for k in keys:
+            mins[k] = min(mins[k], mg[k])
+        a, b = hm.download(s), hp.download(s)
+        if a.pcount == b.pcount and np.array_equal(a.infront, b.infront):
+            d = float(np.max(np.abs(a.x - b.x))) if a.pcount else 0.0
+            dev = max(dev, d)
+            need = max(need, 4.0 * d / params[s].delta)
+    worst = min(mins.values())
+    return {"event_margins_min": {k: (v if v < 1e300 else None) for k, v in mins.items()},
+            "position_dev_max_cm": dev,
+            "margin_over_need": (worst / need) if need > 0 else None}
 
 
 def roofline_of(params, states, m, steps, precision, local):

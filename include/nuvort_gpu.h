@@ -42,7 +42,8 @@ enum {
   NV_ERR_NAN = -6,         /* NaN position (NAN_finder, src/general.f90:172-190) */
   NV_ERR_EMPTY = -7,       /* no live points left (src/line.f90:25-27) */
   NV_ERR_TIMESTEP = -8,    /* dt fails timestep_check (src/initial.f90:169-180) */
-  NV_ERR_UNSUPPORTED = -9, /* option outside this library (solid walls, grid normal fluid) */
+  NV_ERR_UNSUPPORTED = -9, /* option combination outside this library (e.g. solid walls in
+                              mixed precision) */
   NV_ERR_STATE = -10,      /* call out of order (e.g. tree search with no tree built) */
   NV_ERR_QUEUE = -11,      /* serial topology resolver overflowed its work queue */
   NV_ERR_IO = -12,         /* run.in (or a snapshot/restart file) could not be opened or read */
@@ -270,6 +271,17 @@ int nv_set_root_band(nv_handle *h, double scale);
  * is the same bit for bit); 1 keeps one thread per target.  0 (the default) picks the split
  * from the number of work items and the SM count. */
 int nv_set_walk_parts(nv_handle *h, int32_t parts);
+/* Event margins: how close the topology tests came to deciding the other way.  While on,
+ * each system keeps the smallest |value - threshold| / threshold of pinsert's segment length
+ * against delta (line.f90:41), premove's distance against .99 delta (line.f90:115), precon's
+ * closestd against delta/2 (reconnection.f90:24) and precon's tangent dot product against 0.9
+ * (reconnection.f90:34).  The pinsert margin covers exactly the lengths the reference
+ * measures; the others cover every value the device evaluates, which includes every value
+ * the reference evaluates, so they are never above the reference's.  nv_set_event_margins
+ * switches them on (1) or off (0) and resets them; out[4] of nv_event_margins_get receives
+ * them, 1e300 where no test ran. */
+int nv_set_event_margins(nv_handle *h, int32_t on);
+int nv_event_margins_get(nv_handle *h, int32_t sys, double *out);
 /* Data of the normal-fluid fields that the reference reads from files.  noisey_xflow: the n
  * multipliers of noise_file (src/normal_fluid.f90:156-162; the reference reads 100000), used
  * one per step from the first, wrapping after the last (randomise_normal_fluid, :340-348).
@@ -350,7 +362,7 @@ typedef struct nv_ts_row {
   int32_t itime;             /* step of the row (ts.log prints itime/shots)                    */
   int32_t live;              /* count(f(:)%infront>0)                                          */
   int32_t recon_count;
-  int32_t wall_recon_count;  /* always 0: no solid walls here                                  */
+  int32_t wall_recon_count;  /* wall_recon cuts so far (wall_recon_count)                      */
   int32_t remove_count;
   int32_t reserved;
   int64_t tree_eval;         /* accepted tree interactions of the last velocity pass (the

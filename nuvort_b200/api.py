@@ -71,6 +71,8 @@ def lib():
     L.nv_set_fp32_guards.argtypes = [vp, C.c_double, C.c_double, C.c_double]
     L.nv_set_root_band.argtypes = [vp, C.c_double]
     L.nv_set_walk_parts.argtypes = [vp, C.c_int32]
+    L.nv_set_event_margins.argtypes = [vp, C.c_int32]
+    L.nv_event_margins_get.argtypes = [vp, i32, P(C.c_double)]
     L.nv_set_direct_split.argtypes = [vp, C.c_int32]
     L.nv_set_pclose_method.argtypes = [vp, C.c_int32]
     L.nv_step_launches.argtypes = [vp, P(i32)]
@@ -328,6 +330,16 @@ class Handle:
         """Split of the tree walks' work (mixed: central image over groups of root children;
         FP64: unshifted / shifted images on two threads per target); 0: automatic."""
         _check(lib().nv_set_walk_parts(self.h, int(parts)))
+
+    def set_event_margins(self, on: bool = True):
+        """Switch the event-margin record on (and reset it) or off."""
+        _check(lib().nv_set_event_margins(self.h, int(bool(on))))
+
+    def event_margins(self, sys: int = 0) -> dict:
+        """Smallest relative margins of the topology tests since set_event_margins(True)."""
+        out = (C.c_double * 4)()
+        _check(lib().nv_event_margins_get(self.h, int(sys), out))
+        return dict(zip(("insert", "remove", "recon_distance", "recon_dot"), list(out)))
 
     def set_direct_split(self, targets_per_block: int):
         """Plain FP64 direct sum: 64 = one thread per target; 1, 2, 4, 8 = that many targets per

@@ -1089,6 +1089,28 @@ int nv_set_walk_parts(nv_handle *h, int32_t parts) {
   return NV_OK;
 }
 
+int nv_set_event_margins(nv_handle *h, int32_t on) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  int rc = set_device(h);
+  if (rc) return rc;
+  for (int s = 0; s < h->nsys; ++s) {
+    if ((rc = pull_dyn_one(h, s))) return rc;
+    SysDyn &d = h->h_dyn[s];
+    d.margin_on = on ? 1 : 0;
+    for (double &v : d.margin) v = 1e300;
+    NV_CUDA(cudaMemcpy(h->d_dyn + s, &d, sizeof(SysDyn), cudaMemcpyHostToDevice));
+  }
+  return NV_OK;
+}
+
+int nv_event_margins_get(nv_handle *h, int32_t sys, double *out) {
+  if (!h || !out || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_event_margins_get: bad arguments");
+  int rc = set_device(h);
+  if (rc || (rc = pull_dyn_one(h, sys))) return rc;
+  for (int k = 0; k < 4; ++k) out[k] = h->h_dyn[sys].margin[k];
+  return NV_OK;
+}
+
 int nv_set_direct_split(nv_handle *h, int32_t targets_per_block) {
   const int g = targets_per_block;
   if (!h || !(g == 0 || g == 1 || g == 2 || g == 4 || g == 8 || g == 64))

@@ -112,7 +112,23 @@ struct SysDyn {
   long long diag[12];  // see nv_diagnostics
   double total_length;  // pinsert: sum of the segment lengths it measured (line.f90:39)
   double avg_sep;       // pinsert: total_length / (old_pcount - empty slots) (line.f90:95)
+  // Event margins while margin_on: the smallest |value - threshold| / threshold of the
+  // topology tests since they were switched on -- [0] pinsert's length > delta, [1] premove's
+  // distance < .99 delta, [2] precon's closestd < delta/2, [3] precon's tangent dot > 0.9.
+  int margin_on;
+  double margin[4];
 };
+
+// Lowers margin[k] of d to |value - thr| / thr while the margins are on (the IEEE order of
+// non-negative doubles is that of their bit patterns; most values lose to the plain read).
+__device__ __forceinline__ void margin_note_abs(SysDyn &d, int k, double absdiff, double thr) {
+  const double v = absdiff / thr;
+  if (v < *(volatile double *)&d.margin[k])
+    atomicMin((unsigned long long *)&d.margin[k], (unsigned long long)__double_as_longlong(v));
+}
+__device__ __forceinline__ void margin_note(SysDyn &d, int k, double value, double thr) {
+  if (d.margin_on) margin_note_abs(d, k, fabs(value - thr), thr);
+}
 
 // Reductions of calculate_diagnostics (diagnostic.f90:9-74) per system.
 struct DiagRec {

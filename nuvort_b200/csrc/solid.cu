@@ -109,6 +109,7 @@ __global__ void k_solid_pinsert(const SysConst *__restrict__ scs, SysDyn *dyn, i
     load3(S.GB, T, g, gb);
     const double disti = dist_gen(x, gi);
     total_length = e_add(total_length, disti);
+    margin_note(d, 0, disti, sc.delta);
     if (!(disti > sc.delta)) continue;
     // the first empty slot (minloc(f(:)%infront)), else the array grows by one
     while (free_at <= d.pcount && S.nxt[base + free_at] != 0) ++free_at;
@@ -182,6 +183,7 @@ __global__ void k_solid_precon(const SysConst *__restrict__ scs, SysDyn *dyn, in
     if (S.nxt[g] == 0) continue;
     const int pari = S.nxt[g], parb = S.prv[g];
     const double cd = S.CD[g];
+    if (cd > NV_EPS) margin_note(d, 2, cd, sc.delta / 2.);
     if (!((cd < sc.delta / 2.) && (cd > NV_EPS))) continue;
     const int j = S.cl[g];
     if (j == pari || j == parb || j == 0) continue;
@@ -199,6 +201,7 @@ __global__ void k_solid_precon(const SysConst *__restrict__ scs, SysDyn *dyn, in
       for (int c = 0; c < 3; ++c) t[c] = e_div(t[c], len);
     }
     const double dot_val = dot3(t1, t2);
+    margin_note(d, 3, dot_val, 0.9);
     if (dot_val > 0.9) continue;
     double xi[3], gii[3], gbi[3], xj[3], gij[3], gbj[3], xpi[3], xpj[3];
     load3(S.X, T, g, xi);
@@ -296,7 +299,9 @@ __global__ void k_solid_premove(const SysConst *__restrict__ scs, SysDyn *dyn, i
     double xi[3], xt[3];
     load3(S.X, T, g, xi);
     load3(S.X, T, tinfront, xt);
-    if (dist_gen(xi, xt) < thr) {
+    const double dii = dist_gen(xi, xt);
+    margin_note(d, 1, dii, thr);
+    if (dii < thr) {
       S.prv[tinfront] = g;
       S.nxt[g] = tinfront;
       clear_slot(S, infront);

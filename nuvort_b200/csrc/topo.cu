@@ -167,7 +167,7 @@ __device__ __forceinline__ void refresh_ghosts(const SysConst &sc, const State &
 
 // ---- pass 1 kernels: marks ----------------------------------------------------------------
 // precon marks: live slot with delta/2 > closestd > epsilon(1.) (reconnection.f90:185).
-__global__ void k_mark_recon(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn, const int *__restrict__ sys_of,
+__global__ void k_mark_recon(const SysConst *__restrict__ scs, SysDyn *dyn, const int *__restrict__ sys_of,
                              const double *__restrict__ CD, const int *__restrict__ nxt, int *fa, long long T,
                              const unsigned *err) {
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -180,13 +180,14 @@ __global__ void k_mark_recon(const SysConst *__restrict__ scs, const SysDyn *__r
     if (k >= 1 && k <= dyn[s].pcount && recon_step(sc, dyn[s]) && nxt[g] != 0 && !walled(sc)) {
       const double cd = CD[g];
       a = (cd < sc.delta / 2.) && (cd > NV_EPS);
+      if (cd > NV_EPS) margin_note(dyn[s], 2, cd, sc.delta / 2.);
     }
   }
   fa[g] = a;
 }
 
 // premove marks: live slot with |x_i - x_{i+2}| < .99 delta (line.f90:113-115).
-__global__ void k_mark_remove(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn, const int *__restrict__ sys_of,
+__global__ void k_mark_remove(const SysConst *__restrict__ scs, SysDyn *dyn, const int *__restrict__ sys_of,
                               const double *__restrict__ X, const int *__restrict__ nxt, int *fa, long long T,
                               const unsigned *err) {
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -200,7 +201,9 @@ __global__ void k_mark_remove(const SysConst *__restrict__ scs, const SysDyn *__
       double x[3], y[3];
       load3(X, T, (int)g, x);
       load3(X, T, nxt[nxt[g]], y);
-      a = dist_gen(x, y) < e_mul(.99, sc.delta);
+      const double dii = dist_gen(x, y);
+      a = dii < e_mul(.99, sc.delta);
+      margin_note(dyn[s], 1, dii, e_mul(.99, sc.delta));
     }
   }
   fa[g] = a;
@@ -459,8 +462,13 @@ __global__ void __launch_bounds__(256) k_ins_total(const SysConst *__restrict__ 
   const SysConst &sc = scs[s];
   if (walled(sc)) return;  // the serial sweep of solid.cu sums its own lengths
   const int pc = dyn[s].pcount;
-  double acc = 0.;
-  for (int k = 1 + threadIdx.x; k <= pc; k += 256) acc += seglen[sc.base + k];
+  const bool margins = dyn[s].margin_on;
+  double acc = 0., near = 1e300;  // near: the smallest |length - delta| (event margins)
+  for (int k = 1 + threadIdx.x; k <= pc; k += 256) {
+    const double l = seglen[sc.base + k];
+    acc += l;
+    if (margins && l > 0.) near = fmin(near, fabs(l - sc.delta));  // the lengths the tests measured
+  }
   part[threadIdx.x] = acc;
   __syncthreads();
   for (int w = 128; w > 0; w >>= 1) {
@@ -472,6 +480,16 @@ __global__ void __launch_bounds__(256) k_ins_total(const SysConst *__restrict__ 
     d.total_length = part[0];
     const int empty = d.pcount - d.nlive;
     d.avg_sep = part[0] / (double)(d.old_pcount - empty);
+  }
+  if (margins) {
+    __syncthreads();
+    part[threadIdx.x] = near;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+      if (threadIdx.x < w) part[threadIdx.x] = fmin(part[threadIdx.x], part[threadIdx.x + w]);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0 && part[0] < 1e300) margin_note_abs(dyn[s], 0, part[0], sc.delta);
   }
 }
 
@@ -1135,6 +1153,7 @@ __global__ void __launch_bounds__(kRound) k_recon_sweep(const SysConst *__restri
     if (tid < n) {
       const int i = list_a[c0 + tid];
       const ReconIn in = recon_decide(S, i, half_delta, S.cl[i]);
+      if (in.yes >= 0) margin_note(dyn[s], 3, in.dot_val, 0.9);
       r.i = i;
       r.yes = in.yes;
       r.pari = in.pari;
@@ -1173,6 +1192,7 @@ __global__ void __launch_bounds__(kRound) k_recon_sweep(const SysConst *__restri
             yes = -1;
           } else {
             const ReconIn q = recon_decide(S, i, half_delta, S.cl[i]);
+            if (q.yes >= 0) margin_note(dyn[s], 3, q.dot_val, 0.9);
             yes = q.yes;
             pari = q.pari;
             parjb = q.parjb;
@@ -1337,7 +1357,9 @@ __global__ void __launch_bounds__(kRound) k_remove_sweep(const SysConst *__restr
     double xi[3], xt[3];
     load3(S.X, T, i, xi);
     load3(S.X, T, tinfront, xt);
-    if (!(dist_gen(xi, xt) < thr)) return;
+    const double dii = dist_gen(xi, xt);
+    margin_note(dyn[s], 1, dii, thr);
+    if (!(dii < thr)) return;
     S.prv[tinfront] = i;
     S.nxt[i] = tinfront;
     tc.add(i, 1u);
@@ -1391,7 +1413,9 @@ __global__ void __launch_bounds__(kRound) k_remove_sweep(const SysConst *__restr
         double xi[3], xt[3];
         load3(S.X, T, r.i, xi);
         load3(S.X, T, r.tinf, xt);
-        r.yes = dist_gen(xi, xt) < thr;
+        const double dii = dist_gen(xi, xt);
+        margin_note(dyn[s], 1, dii, thr);
+        r.yes = dii < thr;
         if (r.yes) {
           r.pv = S.prv[r.i];
           r.c1 = S.nxt[r.tinf];

@@ -1161,9 +1161,77 @@ __device__ __forceinline__ double cube_dist2(const double x[3], const double4 P,
   return d2;
 }
 
+// An upper bound on the distance the closest-point walk settles on: the distance of a leaf
+// that walk accepts and counts, or 100.  A node whose cell holds the target is opened by the
+// walk (its centroid lies in the same cell, so width/dist >= 1/sqrt(3) > .5), so every child
+// of such a node is reached; a child that is a single point is accepted, and below such a
+// child the walk's own opening test decides what is reached.  Any accepted leaf's distance,
+// formed as the walk forms it, is at least the walk's final closestd.  The search follows
+// the cells that hold the target down from the root, takes the nearest counted leaf child on
+// the way, and then walks, with the reference's opening test, the subtree of the deepest
+// node on that path that holds at least kBoundNode points (a few dozen visits): warps whose
+// targets all get a bound near their final closestd prune the rest of their walks alike.
+constexpr int kBoundNode = 16;
+
+__device__ double closest_bound(const TreeBuffers &tb, const SysConst &sc, int root, const double xi[3], int g,
+                                int ni, int pi_, const int *__restrict__ prv) {
+  double best = 100.;
+  auto counted = [&](int j) { return j != g && j != ni && j != pi_ && !pinned_at(sc, j); };
+  auto dist_to = [&](const double4 &A) {
+    return e_sqrt(e_add(e_add(e_sq(e_sub(xi[0], A.x)), e_sq(e_sub(xi[1], A.y))), e_sq(e_sub(xi[2], A.z))));
+  };
+  {  // the root's cell must hold the target too (it always does between enforce_boundary calls)
+    const double4 P = ldg4(&tb.nP[root]);
+    const double w = tb.nA[root].w;
+    if (!(xi[0] >= P.x && xi[0] < P.x + w && xi[1] >= P.y && xi[1] < P.y + w && xi[2] >= P.z && xi[2] < P.z + w))
+      return best;
+  }
+  int node = root, deep = root;
+  for (int depth = 0; depth <= kMaxLevels && node != kEnd; ++depth) {
+    const int4 I = __ldg(&tb.nI[node]);
+    if (I.x <= 1 || I.y == kEnd) break;
+    if (I.x >= kBoundNode) deep = node;
+    const int stop = I.z;  // the node after the last child's subtree
+    int next = kEnd;
+    for (int c = I.y; c != kEnd && c != stop;) {
+      const int4 Ic = __ldg(&tb.nI[c]);
+      if (Ic.x == 1) {
+        if (counted(__ldg(prv + Ic.w))) best = fmin(best, dist_to(ldg4(&tb.nA[c])));
+      } else if (Ic.x > 1 && next == kEnd) {
+        const double4 P = ldg4(&tb.nP[c]);
+        const double w = tb.nA[c].w;
+        if (xi[0] >= P.x && xi[0] < P.x + w && xi[1] >= P.y && xi[1] < P.y + w && xi[2] >= P.z && xi[2] < P.z + w)
+          next = c;
+      }
+      c = Ic.z;
+    }
+    node = next;
+  }
+  // the walk below `deep` (opened: it holds the target), with the reference's opening test
+  const int4 Id = __ldg(&tb.nI[deep]);
+  if (Id.x <= 1) return best;
+  for (int n = Id.y; n != kEnd && n != Id.z;) {
+    const int4 I = __ldg(&tb.nI[n]);
+    if (I.x == 0) {
+      n = I.z;
+      continue;
+    }
+    const double4 A = ldg4(&tb.nA[n]);
+    const double dist = dist_to(A);
+    if (I.x == 1 || e_div(A.w, dist) < .5) {
+      if (I.x == 1 && counted(__ldg(prv + I.w))) best = fmin(best, dist);
+      n = I.z;
+    } else {
+      n = I.y != kEnd ? I.y : I.z;
+    }
+  }
+  return best;
+}
+
 // pclose_tree + closest_tree (tree.f90:190-244): theta = width/dist < .5, no shift, no
 // correction; the candidate is prv(first member's infront at build time) with the links of
-// now (after pinsert).
+// now (after pinsert).  Subtrees whose cells lie farther than min(cd, closest_bound) are
+// skipped: they hold no leaf or node that could still change closest or closestd.
 template <bool kPrefetch>
 __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn,
                                const int *__restrict__ sys_of, const double *__restrict__ X,
@@ -1200,6 +1268,7 @@ __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *_
   // slack of the subtree skip below: covers the rounding of the centroids (sums of up to
   // 2^24 positions) and of the distances
   const double margin = 1e-8 * sc.bsize;
+  const double bound = closest_bound(tb, sc, s, xi, (int)g, ni, pi_, prv);
   int node = s;
   double4 A = ldg4(&tb.nA[node]);
   int4 I = __ldg(&tb.nI[node]);
@@ -1243,7 +1312,8 @@ __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *_
           }
         }
       } else if (ny != kEnd &&
-                 !(node != s && cube_dist2(xi, ldg4(&tb.nP[node]), A.w) > (cd + margin) * (cd + margin))) {
+                 !(node != s && cube_dist2(xi, ldg4(&tb.nP[node]), A.w) >
+                               (fmin(cd, bound) + margin) * (fmin(cd, bound) + margin))) {
         down = true;
       }
       // (an opened node whose cell lies farther than cd: every member of this node lies in
@@ -1366,7 +1436,10 @@ __global__ void __launch_bounds__(128, kSplit ? 8 : 9) k_tree_walk_mixed(const S
   const double gq64 = sc.quant_circ / (4.0 * NV_PI);
   const float gq = (float)gq64;
   const bool second = sc.tree_extra_correction && sc.tree_theta > 1.1547;
-  float fx = 0, fy = 0, fz = 0;  // FP32 partial over at most kFlush far interactions
+  // FP32 partial over at most kFlush far interactions: a lane adds at most one term per
+  // node visit and the warp promotes every lane's partial to FP64 after kFlush visits
+  float fx = 0, fy = 0, fz = 0;
+  int since_flush = 0;  // warp-uniform
   // FP64: near field plus the flushed FP32 partials (touched only at a flush or an FP64 term)
   __shared__ double s_acc[kSplit ? 1 : 3][128];
   double r_acc0 = 0., r_acc1 = 0., r_acc2 = 0.;
@@ -1515,12 +1588,7 @@ __global__ void __launch_bounds__(128, kSplit ? 8 : 9) k_tree_walk_mixed(const S
               fx = fmaf(f, cx, fx);
               fy = fmaf(f, cy, fy);
               fz = fmaf(f, cz, fz);
-              if ((++evals & (kFlush - 1)) == 0) {  // at most kFlush FP32 terms per partial
-                nx += (double)fx;
-                ny += (double)fy;
-                nz += (double)fz;
-                fx = fy = fz = 0.f;
-              }
+              ++evals;
             }
           }
         }
@@ -1556,6 +1624,13 @@ __global__ void __launch_bounds__(128, kSplit ? 8 : 9) k_tree_walk_mixed(const S
       --top;
     } else {
       more = false;
+    }
+    if (++since_flush == kFlush) {  // at most kFlush FP32 terms per partial
+      nx += (double)fx;
+      ny += (double)fy;
+      nz += (double)fz;
+      fx = fy = fz = 0.f;
+      since_flush = 0;
     }
   }
   if (singular) atomicOr(err, DERR_SINGULAR);

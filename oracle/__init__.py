@@ -69,6 +69,8 @@ def lib():
         L.or_upload_full.argtypes = [vp, P(NvFullState)]
         L.or_write_snapshot.argtypes = [vp, C.c_char_p]
         L.or_write_dump.argtypes = [vp, C.c_char_p]
+        L.or_set_event_margins.argtypes = [vp, C.c_int32]
+        L.or_event_margins_get.argtypes = [vp, P(C.c_double)]
         L.or_set_threads.argtypes = [C.c_int32]
         L.or_get_threads.restype = C.c_int32
         L.or_last_error.restype = C.c_char_p
@@ -199,6 +201,14 @@ class Oracle:
 
     def write_dump(self, path: str):
         _check(lib().or_write_dump(self.h, path.encode()))
+
+    def set_event_margins(self, on: bool = True):
+        _check(lib().or_set_event_margins(self.h, int(bool(on))))
+
+    def event_margins(self) -> dict:
+        out = (C.c_double * 4)()
+        _check(lib().or_event_margins_get(self.h, out))
+        return dict(zip(("insert", "remove", "recon_distance", "recon_dot"), list(out)))
 
     def tree_dump(self) -> np.ndarray:
         n = C.c_int32()

@@ -90,6 +90,16 @@ struct Sys {
   std::vector<std::array<double, 3>> shifts;  // periodic_loop_array
   std::vector<std::array<int, 3>> mirrors;    // mirror_loop_array
   int wall_recon_count = 0;
+  // event margins (the library's nv_event_margins_get): smallest |value - thr| / thr of
+  // pinsert's length, premove's distance, precon's closestd and tangent dot, over the values
+  // the routines below evaluate
+  bool margin_on = false;
+  double margin[4] = {1e300, 1e300, 1e300, 1e300};
+  void note(int k, double value, double thr) {
+    if (!margin_on) return;
+    const double v = std::fabs(value - thr) / thr;
+    if (v < margin[k]) margin[k] = v;
+  }
   Node *vtree = nullptr;
   std::vector<std::unique_ptr<Node>> pool;
   std::vector<nv_event> events;
@@ -850,6 +860,7 @@ struct Sys {
       if (f[i].pinnedi) continue;
       const double disti = dist_gen(f[i].x, f[i].ghosti);
       total_length = total_length + disti;
+      note(0, disti, p.delta);
       if (disti > p.delta) {
         int par_new = 0;
         for (int k = 1; k <= pcount; ++k) if (f[k].infront == 0) { par_new = k; break; }
@@ -905,6 +916,7 @@ struct Sys {
       const int infront = f[i].infront;
       if (f[infront].pinnedi) continue;
       const double distii = dist_gen(f[i].x, f[f[infront].infront].x);
+      note(1, distii, .99 * p.delta);
       if (distii < .99 * p.delta) {
         const int tinfront = f[f[i].infront].infront;
         f[tinfront].behind = i;
@@ -961,6 +973,7 @@ struct Sys {
     for (int i = 1; i <= pcount; ++i) {
       if (f[i].infront == 0) continue;
       const int pari = f[i].infront, parb = f[i].behind;
+      if (f[i].closestd > eps) note(2, f[i].closestd, p.delta / 2.0);
       if ((f[i].closestd < p.delta / 2.0) && (f[i].closestd > eps)) {
         const int j = f[i].closest;
         if (j == pari) continue;
@@ -972,6 +985,7 @@ struct Sys {
         norm_tanf(i, t1);
         norm_tanf(j, t2);
         const double dot_val = dot3(t1, t2);
+        note(3, dot_val, 0.9);
         if (dot_val > 0.9) {
           // parallel: no reconnection
         } else {
@@ -1334,6 +1348,15 @@ int or_pclose(or_handle *h) {
 }
 int or_precon(or_handle *h) { h->s.precon(); return NV_OK; }
 int or_wall_recon(or_handle *h) { h->s.wall_recon(); return NV_OK; }
+int or_set_event_margins(or_handle *h, int32_t on) {
+  h->s.margin_on = on != 0;
+  for (double &v : h->s.margin) v = 1e300;
+  return NV_OK;
+}
+int or_event_margins_get(or_handle *h, double *out) {
+  for (int k = 0; k < 4; ++k) out[k] = h->s.margin[k];
+  return NV_OK;
+}
 int or_premove(or_handle *h) { h->s.premove(); return NV_OK; }
 int or_enforce_boundary(or_handle *h) { h->s.enforce_boundary(); return NV_OK; }
 int or_empty_tree(or_handle *h) { h->s.empty_tree(); return NV_OK; }

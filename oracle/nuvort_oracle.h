@@ -55,6 +55,9 @@ int or_pinsert(or_handle *h);
 int or_pclose(or_handle *h);
 int or_precon(or_handle *h);
 int or_wall_recon(or_handle *h);
+/* Event margins, as nv_set_event_margins / nv_event_margins_get define them. */
+int or_set_event_margins(or_handle *h, int32_t on);
+int or_event_margins_get(or_handle *h, double *out);
 int or_premove(or_handle *h);
 int or_enforce_boundary(or_handle *h);
 int or_empty_tree(or_handle *h);
