@@ -39,6 +39,8 @@ struct TopoBuffers {
   // the fresh distance, the one the sweep used, and per inserting slot the distance its new
   // point measured when the sweep reached it (-1: not reached)
   double *len_st = nullptr, *len_fr = nullptr, *seglen = nullptr, *dn_new = nullptr;
+  int total_parts = 1;                          // blocks per system summing the lengths
+  double *psum = nullptr, *pnear = nullptr;     // per (system, part): their sum and nearest to delta
   void *cub_tmp = nullptr;
   size_t cub_bytes = 0;
   // cell list of the closest-point search of the systems without a tree (pclose)
@@ -450,47 +452,64 @@ __global__ void k_ins_len(const SysConst *__restrict__ scs, const SysDyn *__rest
   seglen[g] = v;
 }
 
-// total_length and avg_sep of the pinsert just made (line.f90:39,95), one block per system:
-// the measured lengths summed in a fixed order (per thread by stride, then a tree over the
-// block; the reference adds them one after another, which agrees to ~1e-13 relative) and
-// divided by old_pcount minus the empty slots left among the pcount slots.
-__global__ void __launch_bounds__(256) k_ins_total(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys,
-                                                   const double *__restrict__ seglen, const unsigned *err) {
-  __shared__ double part[256];
-  const int s = blockIdx.x;
+// total_length and avg_sep of the pinsert just made (line.f90:39,95): the measured lengths
+// summed in a fixed order -- block (s, p) sums part p of system s's slots (per thread by
+// stride, then a tree over the block), and k_ins_total adds the parts in order (the reference
+// adds them one after another, which agrees to ~1e-13 relative) -- divided by old_pcount minus
+// the empty slots left among the pcount slots.  Many blocks per large system: one block
+// summing a million lengths takes milliseconds.
+constexpr int kTotalThreads = 256;
+__global__ void __launch_bounds__(kTotalThreads) k_ins_part(const SysConst *__restrict__ scs, const SysDyn *dyn,
+                                                            int nsys, int parts, const double *__restrict__ seglen,
+                                                            double *__restrict__ psum, double *__restrict__ pnear,
+                                                            const unsigned *err) {
+  __shared__ double sum_[kTotalThreads], near_[kTotalThreads];
+  const int s = blockIdx.x / parts, p = blockIdx.x % parts;
   if (s >= nsys || *err) return;
   const SysConst &sc = scs[s];
   if (walled(sc)) return;  // the serial sweep of solid.cu sums its own lengths
   const int pc = dyn[s].pcount;
   const bool margins = dyn[s].margin_on;
+  const int per = (pc + parts - 1) / parts;
+  const int k0 = 1 + p * per, k1 = min(pc, k0 + per - 1);
   double acc = 0., near = 1e300;  // near: the smallest |length - delta| (event margins)
-  for (int k = 1 + threadIdx.x; k <= pc; k += 256) {
+  for (int k = k0 + threadIdx.x; k <= k1; k += kTotalThreads) {
     const double l = seglen[sc.base + k];
     acc += l;
     if (margins && l > 0.) near = fmin(near, fabs(l - sc.delta));  // the lengths the tests measured
   }
-  part[threadIdx.x] = acc;
+  sum_[threadIdx.x] = acc;
+  near_[threadIdx.x] = near;
   __syncthreads();
-  for (int w = 128; w > 0; w >>= 1) {
-    if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+  for (int w = kTotalThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      sum_[threadIdx.x] += sum_[threadIdx.x + w];
+      near_[threadIdx.x] = fmin(near_[threadIdx.x], near_[threadIdx.x + w]);
+    }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    SysDyn &d = dyn[s];
-    d.total_length = part[0];
-    const int empty = d.pcount - d.nlive;
-    d.avg_sep = part[0] / (double)(d.old_pcount - empty);
+    psum[blockIdx.x] = sum_[0];
+    pnear[blockIdx.x] = near_[0];
   }
-  if (margins) {
-    __syncthreads();
-    part[threadIdx.x] = near;
-    __syncthreads();
-    for (int w = 128; w > 0; w >>= 1) {
-      if (threadIdx.x < w) part[threadIdx.x] = fmin(part[threadIdx.x], part[threadIdx.x + w]);
-      __syncthreads();
-    }
-    if (threadIdx.x == 0 && part[0] < 1e300) margin_note_abs(dyn[s], 0, part[0], sc.delta);
+}
+
+__global__ void k_ins_total(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys, int parts,
+                            const double *__restrict__ psum, const double *__restrict__ pnear, const unsigned *err) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys || *err) return;
+  const SysConst &sc = scs[s];
+  if (walled(sc)) return;
+  SysDyn &d = dyn[s];
+  double tot = 0., near = 1e300;
+  for (int p = 0; p < parts; ++p) {
+    tot += psum[s * parts + p];
+    near = fmin(near, pnear[s * parts + p]);
   }
+  d.total_length = tot;
+  const int empty = d.pcount - d.nlive;
+  d.avg_sep = tot / (double)(d.old_pcount - empty);
+  if (d.margin_on && near < 1e300) margin_note_abs(d, 0, near, sc.delta);
 }
 
 // Outcomes: known where the two tests agree (decided here, in parallel); where they differ
@@ -1830,6 +1849,13 @@ void topo_alloc(nv_handle *h) {
   cudaMalloc(&tb->seglen, n * sizeof(double));
   cudaMalloc(&tb->dn_new, n * sizeof(double));
   cudaMemset(tb->seglen, 0, n * sizeof(double));
+  {
+    int maxcap = 1;
+    for (int s = 0; s < h->nsys; ++s) maxcap = std::max(maxcap, h->cap[s]);
+    tb->total_parts = std::min(64, (maxcap + 16383) / 16384);
+    cudaMalloc(&tb->psum, (size_t)h->nsys * tb->total_parts * sizeof(double));
+    cudaMalloc(&tb->pnear, (size_t)h->nsys * tb->total_parts * sizeof(double));
+  }
   // cell grids of the systems without a tree: about two slots per cell at full capacity,
   // cells at least as wide as delta/2 and at most 256 per axis
   std::vector<CellGrid> grids(h->nsys);
@@ -1878,6 +1904,7 @@ void topo_free(nv_handle *h) {
   cudaFree(tb->unew); cudaFree(tb->segnx); cudaFree(tb->fh[0]); cudaFree(tb->fh[1]); cudaFree(tb->pos_h);
   cudaFree(tb->l0); cudaFree(tb->l1);
   cudaFree(tb->len_st); cudaFree(tb->len_fr); cudaFree(tb->seglen); cudaFree(tb->dn_new);
+  cudaFree(tb->psum); cudaFree(tb->pnear);
   cudaFree(tb->grid); cudaFree(tb->cell_of); cudaFree(tb->cell_cnt); cudaFree(tb->cell_start);
   cudaFree(tb->cell_items);
   cudaFree(tb->cub_tmp);
@@ -1945,7 +1972,10 @@ void launch_pinsert(nv_handle *h) {
   k_insert_sweep<<<h->nsys, 32, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, S, tb->pos_a, tb->list_a, tb->pos_b,
                                                 tb->list_b, sw, h->d_err, h->d_events, h->d_event_count,
                                                 h->event_cap);
-  k_ins_total<<<h->nsys, 256, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, tb->seglen, h->d_err);
+  k_ins_part<<<h->nsys * tb->total_parts, kTotalThreads, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, tb->total_parts,
+                                                                         tb->seglen, tb->psum, tb->pnear, h->d_err);
+  k_ins_total<<<grid_for(h->nsys, 128), 128, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, tb->total_parts, tb->psum,
+                                                             tb->pnear, h->d_err);
   launch_solid_pinsert(h);
 }
 
