@@ -483,27 +483,28 @@ def run_ours(args):
     if not args.no_e2e:
         # the caller's persistent host arrays f(:) (x, u, u1, u2, infront, behind), as the
         # reference keeps them between steps
+        # (page-locked, one array per field with every system's rows; all systems in one call
+        # each way)
         fields = ("x", "u", "u1", "u2", "infront", "behind")
-        bufs = [api.State.empty(c) for c in caps]
-        hosts = [hm.download(s, out=bufs[s], fields=fields) for s in range(len(states))]
-        nb = lambda s: sum(a.nbytes for a in (s.x, s.u, s.u1, s.u2, s.infront, s.behind) if a is not None)
+        hb = api.BatchBuffers(hm, fields)
+        hb.download()
         h2d = d2h = e_pts = 0
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            for s, host in enumerate(hosts):
-                hs = api.State(x=host.x, infront=host.infront, behind=host.behind, u=host.u, u1=host.u1, u2=host.u2)
-                hm.upload(s, hs)
-                h2d += nb(hs)
-                e_pts += int(np.count_nonzero(host.infront))
+            hb.upload()
+            h2d += hb.bytes_of(fields)
+            e_pts += hb.live_points()
             hm.step(1)
-            hosts = [hm.download(s, out=bufs[s], fields=fields) for s in range(len(states))]
-            d2h += sum(nb(x) for x in hosts)
+            hb.download()
+            d2h += hb.bytes_of(fields)
         e2e_s = time.perf_counter() - t0
+        hb.close()
         (e2e_s,), (e_pts,) = reduce_max_sum(dist, "cuda", [e2e_s], [float(e_pts)])
         e2e = {"value": e_pts / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
-               "path": "nv_upload (host f(:) -> device) + nv_step(1) + nv_download (device -> host) per step"}
+               "path": "nv_upload_many (page-locked host f(:) of every system -> device) + nv_step(1) + "
+                       "nv_download_many (device -> host) per step"}
     hm.close()
     if hp is not None:
         hp.close()

@@ -25,6 +25,7 @@
 #ifndef NUVORT_GPU_H
 #define NUVORT_GPU_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -430,6 +431,18 @@ int nv_dump_write_file(const nv_full_state *st, int32_t recon_count, int32_t iti
  * filled when they hold at least cap >= pcount slots (else NV_ERR_ARG after setting the count). */
 int nv_dump_read_file(const char *path, nv_full_state *st, int32_t cap, int32_t *pcount_out, int32_t *recon_count,
                       int32_t *itime, double *t);
+
+/* nv_upload / nv_download for `count` distinct systems sys[i] with states st[i] (nv_download_many:
+ * arrays of cap[i] slots): the same results as count single calls, with every system's
+ * copies and kernels in flight together and one wait.  Each optional array is given for every
+ * listed system or for none.  A rejected link check changes no system.  Systems with solid
+ * walls, or pinned arrays, go through the single calls one by one.  With page-locked host
+ * arrays (nv_host_register) the copies run asynchronously at full bandwidth. */
+int nv_upload_many(nv_handle *h, int32_t count, const int32_t *sys, const nv_host_state *st);
+int nv_download_many(nv_handle *h, int32_t count, const int32_t *sys, nv_host_state *st, const int32_t *cap);
+/* Page-locks (cudaHostRegister) or releases a host range, e.g. the caller's f(:) arrays. */
+int nv_host_register(void *p, size_t bytes);
+int nv_host_unregister(void *p);
 
 /* Diagnostic counters of system sys for the last step, for profiling the topology stages:
  * [0] pinsert candidates, [1] insertions, [2] steps that needed the serial pinsert sweep

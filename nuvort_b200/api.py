@@ -72,6 +72,10 @@ def lib():
     L.nv_set_root_band.argtypes = [vp, C.c_double]
     L.nv_set_walk_parts.argtypes = [vp, C.c_int32]
     L.nv_set_event_margins.argtypes = [vp, C.c_int32]
+    L.nv_upload_many.argtypes = [vp, i32, P(i32), P(NvHostState)]
+    L.nv_download_many.argtypes = [vp, i32, P(i32), P(NvHostState), P(i32)]
+    L.nv_host_register.argtypes = [vp, C.c_size_t]
+    L.nv_host_unregister.argtypes = [vp]
     L.nv_event_margins_get.argtypes = [vp, i32, P(C.c_double)]
     L.nv_set_direct_split.argtypes = [vp, C.c_int32]
     L.nv_set_pclose_method.argtypes = [vp, C.c_int32]
@@ -100,6 +104,75 @@ def lib():
 def _check(rc: int):
     if rc != NV_OK:
         raise NuvortError(rc, lib().nv_last_error().decode())
+
+
+def host_register(a: np.ndarray):
+    """Page-lock a C-contiguous host array (cudaHostRegister) for asynchronous full-speed copies."""
+    _check(lib().nv_host_register(C.c_void_p(a.ctypes.data), C.c_size_t(a.nbytes)))
+
+
+def host_unregister(a: np.ndarray):
+    _check(lib().nv_host_unregister(C.c_void_p(a.ctypes.data)))
+
+
+class BatchBuffers:
+    """Host arrays of every system of a handle, as a host keeping f(:) per system would: one
+    page-locked array per field with each system's rows at a fixed offset, and the C state
+    records built once, so that a transfer of all systems is one nv_upload_many or
+    nv_download_many call."""
+
+    FIELDS3 = ("x", "u", "u1", "u2", "ghosti", "ghostb")
+    FIELDS1 = ("infront", "behind", "closest", "closestd")
+
+    def __init__(self, handle: "Handle", fields: Sequence[str] = ("x", "u", "u1", "u2", "infront", "behind")):
+        self.handle = handle
+        caps = list(handle.capacity)
+        self.n = len(caps)
+        self.offsets = np.concatenate([[0], np.cumsum(caps)[:-1]]).astype(np.int64)
+        tot = int(sum(caps))
+        self.arrays = {}
+        for f in fields:
+            if f in self.FIELDS3:
+                self.arrays[f] = np.zeros((tot, 3), np.float64)
+            elif f == "closestd":
+                self.arrays[f] = np.zeros(tot, np.float64)
+            else:
+                self.arrays[f] = np.zeros(tot, np.int32)
+        for a in self.arrays.values():
+            host_register(a)
+        self.cs = (NvHostState * self.n)()
+        for s in range(self.n):
+            rec = self.cs[s]
+            rec.pcount = 0
+            o = int(self.offsets[s])
+            for f, a in self.arrays.items():
+                ptr = a[o:].ctypes.data
+                setattr(rec, f, C.cast(ptr, C.POINTER(C.c_double if a.dtype == np.float64 else C.c_int32)))
+        self.sys = (C.c_int32 * self.n)(*range(self.n))
+        self.caps = (C.c_int32 * self.n)(*caps)
+
+    def download(self):
+        _check(lib().nv_download_many(self.handle.h, self.n, self.sys, self.cs, self.caps))
+
+    def upload(self):
+        _check(lib().nv_upload_many(self.handle.h, self.n, self.sys, self.cs))
+
+    def pcounts(self) -> List[int]:
+        return [self.cs[s].pcount for s in range(self.n)]
+
+    def live_points(self) -> int:
+        """Live slots of all systems (rows past a system's pcount are never written: zero)."""
+        return int(np.count_nonzero(self.arrays["infront"]))
+
+    def bytes_of(self, fields: Sequence[str]) -> int:
+        """Bytes that one transfer of the given fields moves (at the current pcounts)."""
+        n = sum(self.pcounts())
+        return int(sum(n * self.arrays[f].itemsize * (3 if f in self.FIELDS3 else 1) for f in fields))
+
+    def close(self):
+        for a in self.arrays.values():
+            host_unregister(a)
+        self.arrays = {}
 
 
 def version() -> str:
@@ -223,6 +296,34 @@ class Handle:
         cst = st.to_c()
         _check(lib().nv_download(self.h, int(sys), C.byref(cst), cap))
         return st.trimmed(cst.pcount)
+
+    def upload_many(self, states: Sequence[State], systems: Optional[Sequence[int]] = None):
+        """nv_upload of every (system, state) pair at once (default systems 0..len-1)."""
+        systems = list(range(len(states))) if systems is None else list(systems)
+        cs = (NvHostState * max(len(states), 1))(*[st.to_c() for st in states])
+        sy = (C.c_int32 * max(len(systems), 1))(*systems)
+        _check(lib().nv_upload_many(self.h, len(states), sy, cs))
+
+    def download_many(self, outs: Optional[Sequence[State]] = None, fields: Optional[Sequence[str]] = None,
+                      systems: Optional[Sequence[int]] = None) -> List[State]:
+        """nv_download of several systems at once; outs as in download (one State per system)."""
+        systems = list(range(self.nsys)) if systems is None else list(systems)
+        caps = [self.capacity[s] for s in systems]
+        sts = []
+        for i, s in enumerate(systems):
+            st = outs[i] if outs is not None else State.empty(caps[i])
+            if fields is not None:
+                st = State(**{f: (getattr(st, f) if f in fields else None) for f in STATE_FIELDS})
+            for f in STATE_FIELDS:
+                a = getattr(st, f)
+                if a is not None and (a.shape[0] < caps[i] or not a.flags.c_contiguous):
+                    raise ValueError(f"download_many: {f} must be C-contiguous with {caps[i]} rows")
+            sts.append(st)
+        cs = (NvHostState * max(len(sts), 1))(*[st.to_c() for st in sts])
+        sy = (C.c_int32 * max(len(systems), 1))(*systems)
+        cp = (C.c_int32 * max(len(caps), 1))(*caps)
+        _check(lib().nv_download_many(self.h, len(sts), sy, cs, cp))
+        return [st.trimmed(cs[i].pcount) for i, st in enumerate(sts)]
 
     def set_clock(self, sys: int, t: float, itime: int):
         _check(lib().nv_set_clock(self.h, int(sys), float(t), int(itime)))

@@ -106,6 +106,54 @@ __global__ void k_get_links(const int *__restrict__ dev, int base, int n, int *_
   host[k - 1] = v ? v - base : 0;
 }
 
+// ---- batched transfers: one launch per array over every listed system ---------------------
+// tab[i] = (base, rows = cap + 1, n, offset of the system's rows in the staging buffer);
+// blockIdx.y is the system, blockIdx.x covers its rows.
+__global__ void k_upload_check_many(const int4 *__restrict__ tab, const int *__restrict__ inf,
+                                    const int *__restrict__ beh, const int *__restrict__ clo,
+                                    int *__restrict__ check) {
+  const int4 t = tab[blockIdx.y];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  bool live = false;
+  if (k < t.z) {
+    const int a = inf[t.w + k], b = beh[t.w + k], c = clo ? clo[t.w + k] : 0;
+    if (a < 0 || a > t.z || b < 0 || b > t.z || c < 0 || c > t.z) atomicOr(&check[2 * blockIdx.y], 1);
+    if ((a == 0) != (b == 0)) atomicOr(&check[2 * blockIdx.y], 2);
+    live = a > 0;
+  }
+  const unsigned bl = __ballot_sync(0xffffffffu, live);
+  if ((threadIdx.x & 31) == 0 && bl) atomicAdd(&check[2 * blockIdx.y + 1], __popc(bl));
+}
+__global__ void k_put_links_many(int *__restrict__ dev, const int4 *__restrict__ tab, const int *__restrict__ host) {
+  const int4 t = tab[blockIdx.y];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= t.y) return;
+  const int v = host && k >= 1 && k <= t.z ? host[t.w + k - 1] : 0;
+  dev[t.x + k] = v ? t.x + v : 0;
+}
+__global__ void k_put_rows_many(double *__restrict__ dev, long long T, const int4 *__restrict__ tab, int comps,
+                                const double *__restrict__ host) {
+  const int4 t = tab[blockIdx.y];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= t.y) return;
+  for (int c = 0; c < comps; ++c)
+    dev[c * T + t.x + k] = host && k >= 1 && k <= t.z ? host[(long long)comps * (t.w + k - 1) + c] : 0.0;
+}
+__global__ void k_get_rows_many(const double *__restrict__ dev, long long T, const int4 *__restrict__ tab, int comps,
+                                double *__restrict__ host) {
+  const int4 t = tab[blockIdx.y];
+  const int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > t.z) return;
+  for (int c = 0; c < comps; ++c) host[(long long)comps * (t.w + k - 1) + c] = dev[c * T + t.x + k];
+}
+__global__ void k_get_links_many(const int *__restrict__ dev, const int4 *__restrict__ tab, int *__restrict__ host) {
+  const int4 t = tab[blockIdx.y];
+  const int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > t.z) return;
+  const int v = dev[t.x + k];
+  host[t.w + k - 1] = v ? v - t.x : 0;
+}
+
 int err_code_from_bits(unsigned bits, std::string &msg) {
   if (bits & DERR_SINGULAR) { msg = "tree_walk: singularity in BS (tree) velocity field (dist<epsilon)"; return NV_ERR_SINGULAR; }
   if (bits & DERR_TREE_DEPTH) { msg = "octree deeper than NV_TREE_MAX_DEPTH levels (coincident points?)"; return NV_ERR_TREE_DEPTH; }
@@ -472,6 +520,44 @@ int sys_capacity(nv_handle *h, int sys) { return (h && sys >= 0 && sys < h->nsys
 // Per-system constants for callers outside this file (the static-scratch entry point).
 SysConst sysconst_for(const nv_params &p, int base, int cap) { return make_sysconst(p, base, cap); }
 
+// ---- batched transfers ------------------------------------------------------------------
+namespace {
+int ensure_batch(nv_handle *h) {
+  if (h->bstage) return NV_OK;
+  int rc;
+  if ((rc = dalloc(&h->bstage, 3 * (size_t)h->T)) || (rc = dalloc(&h->d_btab, (size_t)h->nsys)) ||
+      (rc = dalloc(&h->d_bcheck, 2 * (size_t)h->nsys)))
+    return rc;
+  return NV_OK;
+}
+// every listed state gives the optional array or none does
+template <class F>
+bool all_or_none(int count, const nv_host_state *st, F field) {
+  int given = 0;
+  for (int i = 0; i < count; ++i) given += field(st[i]) != nullptr;
+  return given == 0 || given == count;
+}
+bool fields_consistent(int count, const nv_host_state *st) {
+  return all_or_none(count, st, [](const nv_host_state &s) { return (const void *)s.u; }) &&
+         all_or_none(count, st, [](const nv_host_state &s) { return (const void *)s.u1; }) &&
+         all_or_none(count, st, [](const nv_host_state &s) { return (const void *)s.u2; }) &&
+         all_or_none(count, st, [](const nv_host_state &s) { return (const void *)s.ghosti; }) &&
+         all_or_none(count, st, [](const nv_host_state &s) { return (const void *)s.ghostb; }) &&
+         all_or_none(count, st, [](const nv_host_state &s) { return (const void *)s.closest; }) &&
+         all_or_none(count, st, [](const nv_host_state &s) { return (const void *)s.closestd; });
+}
+int batch_args(nv_handle *h, int count, const int32_t *sys, const void *st, const char *who) {
+  if (!h || count < 0 || (count > 0 && (!sys || !st))) return set_error(NV_ERR_ARG, std::string(who) + ": bad arguments");
+  std::vector<char> seen(h->nsys, 0);
+  for (int i = 0; i < count; ++i) {
+    if (sys[i] < 0 || sys[i] >= h->nsys || seen[sys[i]])
+      return set_error(NV_ERR_ARG, std::string(who) + ": systems must be distinct and in range");
+    seen[sys[i]] = 1;
+  }
+  return NV_OK;
+}
+}  // namespace
+
 extern "C" {
 
 const char *nv_last_error(void) { return g_err.c_str(); }
@@ -645,7 +731,7 @@ int nv_destroy(nv_handle *h) {
   tree_free(h);
   topo_free(h);
   for (void *p : h->nf_buffers) cudaFree(p);
-  void *ptrs[] = {h->pin, h->umir, h->usm, h->cs, h->d_drec, h->partial, h->stage, h->d_upck, h->d_sc, h->d_dyn, h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv,
+  void *ptrs[] = {h->bstage, h->d_btab, h->d_bcheck, h->pin, h->umir, h->usm, h->cs, h->d_drec, h->partial, h->stage, h->d_upck, h->d_sc, h->d_dyn, h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd, h->nxt, h->prv,
                   h->closest, h->sys_of, h->seg, h->seg32, h->d_err, h->d_events, h->d_event_count,
                   h->d_work_direct, h->d_work_tree, h->d_work_lia, h->d_work_img, h->d_work_timg, h->d_work_split};
   for (void *p : ptrs)
@@ -785,6 +871,179 @@ int nv_download(nv_handle *h, int32_t sys, nv_host_state *st, int32_t cap) {
     }
   }
   NV_CUDA(cudaStreamSynchronize(sm));
+  return NV_OK;
+}
+
+
+int nv_upload_many(nv_handle *h, int32_t count, const int32_t *sys, const nv_host_state *st) {
+  int rc = batch_args(h, count, sys, st, "nv_upload_many");
+  if (rc) return rc;
+  bool one_by_one = false;  // systems with solid walls go through nv_upload one at a time
+  for (int i = 0; i < count; ++i) {
+    const nv_host_state &s = st[i];
+    if (!s.x || !s.infront || !s.behind) return set_error(NV_ERR_ARG, "nv_upload_many: x, infront, behind are required");
+    if (s.pcount < 0 || s.pcount > h->cap[sys[i]])
+      return set_error(NV_ERR_ARG, "nv_upload_many: pcount exceeds a system's capacity");
+    if (h->sc[sys[i]].pin || s.wpinned || s.pinnedi || s.pinnedb) one_by_one = true;
+  }
+  if (one_by_one) {
+    for (int i = 0; i < count; ++i)
+      if ((rc = nv_upload(h, sys[i], &st[i]))) return rc;
+    return NV_OK;
+  }
+  if (!fields_consistent(count, st))
+    return set_error(NV_ERR_ARG, "nv_upload_many: each optional array must be given for every listed system or none");
+  if (count == 0) return NV_OK;
+  if ((rc = set_device(h)) || (rc = ensure_batch(h))) return rc;
+  cudaStream_t sm = h->stream;
+  const long long T = h->T;
+  std::vector<int4> tab(count);
+  long long N = 0;
+  int maxrows = 1;
+  for (int i = 0; i < count; ++i) {
+    const int s = sys[i];
+    tab[i] = make_int4(h->base[s], h->cap[s] + 1, st[i].pcount, (int)N);
+    N += st[i].pcount;
+    maxrows = std::max(maxrows, h->cap[s] + 1);
+  }
+  NV_CUDA(cudaMemcpyAsync(h->d_btab, tab.data(), count * sizeof(int4), cudaMemcpyHostToDevice, sm));
+  const dim3 grid(grid_for(maxrows, 256), count);
+  // links: staged and checked for every system before any system changes
+  int *si = reinterpret_cast<int *>(h->bstage);
+  int *s_inf = si, *s_beh = si + N, *s_clo = si + 2 * N;
+  const bool clo = st[0].closest != nullptr;
+  for (int i = 0; i < count; ++i) {
+    const size_t n = st[i].pcount, o = tab[i].w;
+    if (!n) continue;
+    NV_CUDA(cudaMemcpyAsync(s_inf + o, st[i].infront, n * sizeof(int), cudaMemcpyHostToDevice, sm));
+    NV_CUDA(cudaMemcpyAsync(s_beh + o, st[i].behind, n * sizeof(int), cudaMemcpyHostToDevice, sm));
+    if (clo) NV_CUDA(cudaMemcpyAsync(s_clo + o, st[i].closest, n * sizeof(int), cudaMemcpyHostToDevice, sm));
+  }
+  NV_CUDA(cudaMemsetAsync(h->d_bcheck, 0, 2 * count * sizeof(int), sm));
+  k_upload_check_many<<<grid, 256, 0, sm>>>(h->d_btab, s_inf, s_beh, clo ? s_clo : nullptr, h->d_bcheck);
+  std::vector<int> check(2 * count);
+  NV_CUDA(cudaMemcpyAsync(check.data(), h->d_bcheck, 2 * count * sizeof(int), cudaMemcpyDeviceToHost, sm));
+  NV_CUDA(cudaStreamSynchronize(sm));
+  for (int i = 0; i < count; ++i) {
+    if (check[2 * i] & 1)
+      return set_error(NV_ERR_ARG, "nv_upload_many: link out of range in system " + std::to_string(sys[i]) +
+                                       " (no system changed)");
+    if (check[2 * i] & 2)
+      return set_error(NV_ERR_ARG, "nv_upload_many: infront/behind disagree on an empty slot in system " +
+                                       std::to_string(sys[i]) + " (no system changed)");
+  }
+  ++h->links_epoch;
+  k_put_links_many<<<grid, 256, 0, sm>>>(h->nxt, h->d_btab, s_inf);
+  k_put_links_many<<<grid, 256, 0, sm>>>(h->prv, h->d_btab, s_beh);
+  k_put_links_many<<<grid, 256, 0, sm>>>(h->closest, h->d_btab, clo ? s_clo : nullptr);
+  // each double array of every system into the staging buffer, then one launch to the slots
+  // (in stream order, so the buffer is reused array after array)
+  auto put = [&](double *dev, double *const nv_host_state::*field, int comps) -> int {
+    const bool given = st[0].*field != nullptr;
+    if (given)
+      for (int i = 0; i < count; ++i)
+        if (st[i].pcount)
+          NV_CUDA(cudaMemcpyAsync(h->bstage + (size_t)comps * tab[i].w, st[i].*field,
+                                  (size_t)comps * st[i].pcount * sizeof(double), cudaMemcpyHostToDevice, sm));
+    k_put_rows_many<<<grid, 256, 0, sm>>>(dev, T, h->d_btab, comps, given ? h->bstage : nullptr);
+    return NV_OK;
+  };
+  if ((rc = put(h->x, &nv_host_state::x, 3)) || (rc = put(h->u, &nv_host_state::u, 3)) ||
+      (rc = put(h->u1, &nv_host_state::u1, 3)) || (rc = put(h->u2, &nv_host_state::u2, 3)) ||
+      (rc = put(h->gi, &nv_host_state::ghosti, 3)) || (rc = put(h->gb, &nv_host_state::ghostb, 3)) ||
+      (rc = put(h->closestd, &nv_host_state::closestd, 1)))
+    return rc;
+  k_put_rows_many<<<grid, 256, 0, sm>>>(h->usm, T, h->d_btab, 6, nullptr);
+  k_put_rows_many<<<grid, 256, 0, sm>>>(h->cs, T, h->d_btab, 2, nullptr);
+  // the clocks and counters stay; the slot counts are replaced
+  NV_CUDA(cudaMemcpyAsync(h->h_dyn.data(), h->d_dyn, h->nsys * sizeof(SysDyn), cudaMemcpyDeviceToHost, sm));
+  NV_CUDA(cudaStreamSynchronize(sm));
+  for (int i = 0; i < count; ++i) {
+    SysDyn &d = h->h_dyn[sys[i]];
+    d.pcount = st[i].pcount;
+    d.nlive = check[2 * i + 1];
+  }
+  NV_CUDA(cudaMemcpyAsync(h->d_dyn, h->h_dyn.data(), h->nsys * sizeof(SysDyn), cudaMemcpyHostToDevice, sm));
+  NV_CUDA(cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), sm));
+  NV_CUDA(cudaStreamSynchronize(sm));
+  return NV_OK;
+}
+
+int nv_download_many(nv_handle *h, int32_t count, const int32_t *sys, nv_host_state *st, const int32_t *cap) {
+  int rc = batch_args(h, count, sys, st, "nv_download_many");
+  if (rc) return rc;
+  if (count > 0 && !cap) return set_error(NV_ERR_ARG, "nv_download_many: bad arguments");
+  bool one_by_one = false;  // pinned records go through nv_download one system at a time
+  for (int i = 0; i < count; ++i)
+    if (st[i].wpinned || st[i].pinnedi || st[i].pinnedb) one_by_one = true;
+  if (one_by_one) {
+    for (int i = 0; i < count; ++i)
+      if ((rc = nv_download(h, sys[i], &st[i], cap[i]))) return rc;
+    return NV_OK;
+  }
+  if (!fields_consistent(count, st) ||
+      !all_or_none(count, st, [](const nv_host_state &s) { return (const void *)s.x; }) ||
+      !all_or_none(count, st, [](const nv_host_state &s) { return (const void *)s.infront; }) ||
+      !all_or_none(count, st, [](const nv_host_state &s) { return (const void *)s.behind; }))
+    return set_error(NV_ERR_ARG, "nv_download_many: each array must be asked for every listed system or none");
+  if (count == 0) return NV_OK;
+  if ((rc = set_device(h)) || (rc = ensure_batch(h))) return rc;
+  cudaStream_t sm = h->stream;
+  const long long T = h->T;
+  NV_CUDA(cudaMemcpyAsync(h->h_dyn.data(), h->d_dyn, h->nsys * sizeof(SysDyn), cudaMemcpyDeviceToHost, sm));
+  NV_CUDA(cudaStreamSynchronize(sm));
+  std::vector<int4> tab(count);
+  long long N = 0;
+  int maxn = 1;
+  for (int i = 0; i < count; ++i) {
+    const int s = sys[i], n = h->h_dyn[s].pcount;
+    st[i].pcount = n;
+    if (n > cap[i]) return set_error(NV_ERR_ARG, "nv_download_many: arrays hold fewer slots than pcount");
+    tab[i] = make_int4(h->base[s], h->cap[s] + 1, n, (int)N);
+    N += n;
+    maxn = std::max(maxn, n);
+  }
+  NV_CUDA(cudaMemcpyAsync(h->d_btab, tab.data(), count * sizeof(int4), cudaMemcpyHostToDevice, sm));
+  const dim3 grid(grid_for(maxn, 256), count);
+  // one launch per array over every system into the staging buffer, then a copy per system
+  // (stream order keeps the buffer from being overwritten before its copies are done)
+  auto get = [&](const double *dev, double *nv_host_state::*field, int comps) -> int {
+    if (!(st[0].*field)) return NV_OK;
+    k_get_rows_many<<<grid, 256, 0, sm>>>(dev, T, h->d_btab, comps, h->bstage);
+    for (int i = 0; i < count; ++i)
+      if (st[i].pcount)
+        NV_CUDA(cudaMemcpyAsync(st[i].*field, h->bstage + (size_t)comps * tab[i].w,
+                                (size_t)comps * st[i].pcount * sizeof(double), cudaMemcpyDeviceToHost, sm));
+    return NV_OK;
+  };
+  int *si = reinterpret_cast<int *>(h->bstage);
+  auto get_link = [&](const int *dev, int32_t *nv_host_state::*field) -> int {
+    if (!(st[0].*field)) return NV_OK;
+    k_get_links_many<<<grid, 256, 0, sm>>>(dev, h->d_btab, si);
+    for (int i = 0; i < count; ++i)
+      if (st[i].pcount)
+        NV_CUDA(cudaMemcpyAsync(st[i].*field, si + tab[i].w, (size_t)st[i].pcount * sizeof(int),
+                                cudaMemcpyDeviceToHost, sm));
+    return NV_OK;
+  };
+  if ((rc = get(h->x, &nv_host_state::x, 3)) || (rc = get(h->u, &nv_host_state::u, 3)) ||
+      (rc = get(h->u1, &nv_host_state::u1, 3)) || (rc = get(h->u2, &nv_host_state::u2, 3)) ||
+      (rc = get(h->gi, &nv_host_state::ghosti, 3)) || (rc = get(h->gb, &nv_host_state::ghostb, 3)) ||
+      (rc = get_link(h->nxt, &nv_host_state::infront)) || (rc = get_link(h->prv, &nv_host_state::behind)) ||
+      (rc = get_link(h->closest, &nv_host_state::closest)) || (rc = get(h->closestd, &nv_host_state::closestd, 1)))
+    return rc;
+  NV_CUDA(cudaStreamSynchronize(sm));
+  return NV_OK;
+}
+
+int nv_host_register(void *p, size_t bytes) {
+  if (!p || bytes == 0) return set_error(NV_ERR_ARG, "nv_host_register: bad arguments");
+  NV_CUDA(cudaHostRegister(p, bytes, cudaHostRegisterDefault));
+  return NV_OK;
+}
+int nv_host_unregister(void *p) {
+  if (!p) return set_error(NV_ERR_ARG, "nv_host_unregister: bad arguments");
+  NV_CUDA(cudaHostUnregister(p));
   return NV_OK;
 }
 

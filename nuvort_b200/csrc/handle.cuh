@@ -44,6 +44,9 @@ struct nv_handle {
   double *cs = nullptr;      // f(:)%curv, f(:)%stretch of the last diagnostics [2][T]
   struct DiagRec *d_drec = nullptr;  // per system: the last diagnostics' reductions
   double *stage = nullptr;   // nv_upload / nv_download staging: host arrays as they are, 3 x (largest capacity + 1) doubles
+  double *bstage = nullptr;  // nv_upload_many / nv_download_many staging: every listed system's array at once, 3T doubles
+  int4 *d_btab = nullptr;    // their per-system table (base, rows, n, offset), nsys entries
+  int *d_bcheck = nullptr;   // their link checks, two ints per system
   int *d_upck = nullptr;     // nv_upload checks: [0] link errors (1 out of range, 2 empty-slot mismatch), [1] live slots
   int4 *d_work_img = nullptr;  // (system, image, first slot) items of the mixed direct sum
   int n_work_img = 0;
