@@ -199,6 +199,43 @@ module nuvort_gpu
       integer(c_int32_t), value :: sys, nx, ny, nz
       real(c_double), dimension(*), intent(in) :: u, yp
     end function
+    !> event margins of the topology tests (smallest relative distance from each threshold)
+    integer(c_int) function nv_set_event_margins(h, on) bind(c, name='nv_set_event_margins')
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: on
+    end function
+    integer(c_int) function nv_event_margins_get(h, sys, out) bind(c, name='nv_event_margins_get')
+      import :: c_int, c_int32_t, c_ptr, c_double
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: sys
+      real(c_double), intent(out) :: out(4)
+    end function
+    !> every listed system at once (st(i) describes system sys(i), 0-based)
+    integer(c_int) function nv_upload_many(h, count, sys, st) bind(c, name='nv_upload_many')
+      import :: c_int, c_int32_t, c_ptr, nv_host_state
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: count
+      integer(c_int32_t), intent(in) :: sys(*)
+      type(nv_host_state), intent(in) :: st(*)
+    end function
+    integer(c_int) function nv_download_many(h, count, sys, st, cap) bind(c, name='nv_download_many')
+      import :: c_int, c_int32_t, c_ptr, nv_host_state
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: count
+      integer(c_int32_t), intent(in) :: sys(*), cap(*)
+      type(nv_host_state), intent(inout) :: st(*)
+    end function
+    !> page-lock (cudaHostRegister) a host range, e.g. f(:)'s packed arrays
+    integer(c_int) function nv_host_register(p, bytes) bind(c, name='nv_host_register')
+      import :: c_int, c_ptr, c_size_t
+      type(c_ptr), value :: p
+      integer(c_size_t), value :: bytes
+    end function
+    integer(c_int) function nv_host_unregister(p) bind(c, name='nv_host_unregister')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: p
+    end function
     type(c_ptr) function nv_last_error() bind(c, name='nv_last_error')
       import :: c_ptr
     end function
