@@ -218,6 +218,67 @@ __device__ __forceinline__ void load_x(const double *__restrict__ X, long long T
 
 // Create the non-empty children of node p (counts cnt[0..7]); returns first child id via
 // *id0 and member base via *mb0 (or -1 on overflow).  Called by one thread.
+// What a node's split reserves: child ids, member slots, entries of the next level's block
+// and warp split lists, entries of the block-summed node list.
+struct SplitNeeds {
+  int nchild, kept, nblk, nwrp, nbig;
+};
+__device__ SplitNeeds split_needs(const int cnt[8]) {
+  SplitNeeds n{0, 0, 0, 0, 0};
+#pragma unroll
+  for (int d = 0; d < 8; ++d) {
+    n.nchild += cnt[d] != 0;
+    n.kept += cnt[d];
+    if (cnt[d] >= 2) {
+      if (cnt[d] > kBigNode) ++n.nblk;
+      else ++n.nwrp;
+    }
+    if (cnt[d] > kBlockSumNode) ++n.nbig;
+  }
+  return n;
+}
+
+// The children of node p at reserved offsets (id0, mb0, qb, qw, qg); false when they do not
+// fit the buffers (error set).
+__device__ bool write_children(TreeBuffers &tb, int p, const int cnt[8], const SplitNeeds &n, int id0, int mb0,
+                               int qb, int qw, int qg, unsigned *err) {
+  if (id0 + n.nchild > tb.max_nodes || (long long)mb0 + n.kept > tb.max_members || qb + n.nblk > tb.max_blk ||
+      qw + n.nwrp > tb.max_wrp || qg + n.nbig > tb.max_big) {
+    atomicOr(err, DERR_TREE_NODES);
+    return false;
+  }
+  const int4 Ip = tb.nI[p];
+  const int depth = tb.nDepth[p] + 1;
+  const int lb = depth % 3;
+  const double4 P = tb.nP[p];
+  const double h = tb.nA[p].w / 2.0;
+  int off = 0, k = 0, kb = 0, kw = 0, kg = 0;
+#pragma unroll
+  for (int d = 0; d < 8; ++d) {
+    if (!cnt[d]) continue;
+    const int id = id0 + k;
+    const bool last = (k == n.nchild - 1);
+    const double cx = (d & 1) ? e_add(P.x, h) : P.x;
+    const double cz = (d & 2) ? e_add(P.z, h) : P.z;
+    const double cy = (d & 4) ? e_add(P.y, h) : P.y;
+    tb.nP[id] = make_double4(cx, cy, cz, 0);
+    tb.nA[id] = make_double4(0, 0, 0, h);
+    tb.nI[id] = make_int4(cnt[d], kEnd, last ? Ip.z : id + 1, 0);
+    tb.nR[id] = make_int2(mb0 + off, cnt[d]);
+    tb.nDepth[id] = depth;
+    tb.nSib[id] = last ? kEnd : id + 1;
+    if (cnt[d] >= 2) {  // the child's level list of nodes still to split
+      if (cnt[d] > kBigNode) tb.split_blk[lb][qb + kb++] = id;
+      else tb.split_wrp[lb][qw + kw++] = id;
+    }
+    if (cnt[d] > kBlockSumNode) tb.bigl[qg + kg++] = id;
+    off += cnt[d];
+    ++k;
+  }
+  tb.nI[p].y = id0;
+  return true;
+}
+
 __device__ void make_children(TreeBuffers &tb, int p, const int cnt[8], int *id0_out, int *mb0_out, unsigned *err) {
   int mask = 0, kept = 0;
 #pragma unroll
@@ -344,13 +405,12 @@ __global__ void k_root_scatter(TreeBuffers tb, const int *__restrict__ pos, long
 
 // Split node p (at most kBigNode members) with one warp: count the members per octant, make
 // the children, then write each member to its child's list in member order (stable).
-__device__ void split_node_warp(const double *__restrict__ X, long long T, TreeBuffers &tb, int p, int lane,
-                                unsigned *err) {
-  const unsigned lt = (1u << lane) - 1u;
+// Node p's member count per octant (the warp's lanes over its member list).
+__device__ void warp_count(const double *__restrict__ X, long long T, const TreeBuffers &tb, int p, int lane,
+                           int cnt[8]) {
   const int2 R = tb.nR[p];
   const double4 P = tb.nP[p];
   const double h = tb.nA[p].w / 2.0;
-  int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (int k0 = 0; k0 < R.y; k0 += 32) {
     const int k = k0 + lane;
     int d = 8;
@@ -362,11 +422,15 @@ __device__ void split_node_warp(const double *__restrict__ X, long long T, TreeB
 #pragma unroll
     for (int dd = 0; dd < 8; ++dd) cnt[dd] += __popc(__ballot_sync(0xffffffffu, d == dd));
   }
-  int id0 = -1, mb0 = -1;
-  if (lane == 0) make_children(tb, p, cnt, &id0, &mb0, err);
-  id0 = __shfl_sync(0xffffffffu, id0, 0);
-  mb0 = __shfl_sync(0xffffffffu, mb0, 0);
-  if (id0 < 0) return;
+}
+
+// Node p's members into its children's lists (stable: slot order kept), from member slot mb0.
+__device__ void warp_scatter(const double *__restrict__ X, long long T, TreeBuffers &tb, int p, int lane,
+                             const int cnt[8], int mb0) {
+  const unsigned lt = (1u << lane) - 1u;
+  const int2 R = tb.nR[p];
+  const double4 P = tb.nP[p];
+  const double h = tb.nA[p].w / 2.0;
   int base_off[8], run[8];
   {
     int off = 0;
@@ -497,17 +561,69 @@ __global__ void __launch_bounds__(1024) k_split_level(const double *__restrict__
     split_node_block(X, T, tb, p, err);
     __syncthreads();
   }
-  const int lane = threadIdx.x & 31;
+  // Nodes split by a warp, kWarpNodes consecutive ones at a time: the warp counts each
+  // node's children, lane 0 reserves the ids, member slots and list entries of all of them
+  // with one atomic per counter (one per node contended on the few counters at the levels
+  // with most nodes), then the warp writes each node's children and scatters its members.
+  constexpr int kWarpNodes = 4;
+  __shared__ int s_cnt[32][kWarpNodes][8];  // per warp of the block: counts per octant
+  __shared__ int s_mb[32][kWarpNodes];      // and the member slot of each node's children (-1: none)
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const int nwl = min(tb.ctr[kCtrSplit + 3 + b], tb.max_wrp);
-  for (int wq = warp; wq < nwl; wq += nwarps) {
-    const int p = tb.split_wrp[b][wq];
-    if (tb.nDepth[p] >= kMaxLevels) {
-      if (lane == 0) atomicOr(err, DERR_TREE_DEPTH);
-      continue;
+  const int lb = (level + 1) % 3;  // the children's level lists
+  // several nodes per warp only where nodes far outnumber warps (the small, numerous nodes of
+  // the deep levels); elsewhere one node per warp keeps every warp busy
+  const int kn = nwl >= 8 * nwarps ? kWarpNodes : 1;
+  for (int wq0 = warp * kn; wq0 < nwl; wq0 += nwarps * kn) {
+    int pj[kWarpNodes];
+#pragma unroll
+    for (int j = 0; j < kWarpNodes; ++j) {
+      pj[j] = j < kn && wq0 + j < nwl ? tb.split_wrp[b][wq0 + j] : -1;
+      if (pj[j] >= 0 && tb.nDepth[pj[j]] >= kMaxLevels) {
+        if (lane == 0) atomicOr(err, DERR_TREE_DEPTH);
+        pj[j] = -1;
+      }
     }
-    split_node_warp(X, T, tb, p, lane, err);
+    for (int j = 0; j < kn; ++j) {
+      int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (pj[j] >= 0) warp_count(X, T, tb, pj[j], lane, cnt);
+      if (lane < 8) s_cnt[wib][j][lane] = cnt[lane];
+    }
+    __syncwarp();
+    int off[kWarpNodes][5];
+    if (lane == 0) {
+      int tot[5] = {0, 0, 0, 0, 0};
+      for (int j = 0; j < kn; ++j) {
+        const SplitNeeds nd = split_needs(s_cnt[wib][j]);
+        const int v[5] = {nd.nchild, nd.kept, nd.nblk, nd.nwrp, nd.nbig};
+        for (int c = 0; c < 5; ++c) {
+          off[j][c] = tot[c];
+          tot[c] += v[c];
+        }
+      }
+      int *ctrs[5] = {&tb.ctr[0], &tb.ctr[1], &tb.ctr[kCtrSplit + lb], &tb.ctr[kCtrSplit + 3 + lb], &tb.ctr[kCtrBig]};
+      int base[5];
+      for (int c = 0; c < 5; ++c) base[c] = tot[c] ? atomicAdd(ctrs[c], tot[c]) : 0;
+      for (int j = 0; j < kn; ++j) {
+        int ok = 0;
+        const SplitNeeds nd = split_needs(s_cnt[wib][j]);
+        if (pj[j] >= 0 && nd.nchild > 0)
+          ok = write_children(tb, pj[j], s_cnt[wib][j], nd, base[0] + off[j][0], base[1] + off[j][1],
+                              base[2] + off[j][2], base[3] + off[j][3], base[4] + off[j][4], err);
+        s_mb[wib][j] = ok ? base[1] + off[j][1] : -1;
+      }
+    }
+    __syncwarp();
+    for (int j = 0; j < kn; ++j) {
+      const int mb0 = s_mb[wib][j];
+      if (pj[j] < 0 || mb0 < 0) continue;
+      int cnt[8];
+      for (int d = 0; d < 8; ++d) cnt[d] = s_cnt[wib][j][d];
+      warp_scatter(X, T, tb, pj[j], lane, cnt, mb0);
+    }
+    __syncwarp();
   }
 }
 
