@@ -483,8 +483,8 @@ def run_ours(args):
     if not args.no_e2e:
         # the caller's persistent host arrays f(:) (x, u, u1, u2, infront, behind), as the
         # reference keeps them between steps
-        # (page-locked, one array per field with every system's rows; all systems in one call
-        # each way)
+        # (page-locked, one array per field with every system's rows packed one after another;
+        # all systems in one call and one copy per array each way)
         fields = ("x", "u", "u1", "u2", "infront", "behind")
         hb = api.BatchBuffers(hm, fields)
         hb.download()
@@ -503,8 +503,8 @@ def run_ours(args):
         (e2e_s,), (e_pts,) = reduce_max_sum(dist, "cuda", [e2e_s], [float(e_pts)])
         e2e = {"value": e_pts / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
-               "path": "nv_upload_many (page-locked host f(:) of every system -> device) + nv_step(1) + "
-                       "nv_download_many (device -> host) per step"}
+               "path": "nv_upload_packed (page-locked host f(:) of every system -> device) + nv_step(1) + "
+                       "nv_download_packed (device -> host) per step"}
     hm.close()
     if hp is not None:
         hp.close()

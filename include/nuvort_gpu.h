@@ -440,6 +440,13 @@ int nv_dump_read_file(const char *path, nv_full_state *st, int32_t cap, int32_t 
  * arrays (nv_host_register) the copies run asynchronously at full bandwidth. */
 int nv_upload_many(nv_handle *h, int32_t count, const int32_t *sys, const nv_host_state *st);
 int nv_download_many(nv_handle *h, int32_t count, const int32_t *sys, nv_host_state *st, const int32_t *cap);
+/* Every system of the handle at once with the host arrays packed: system s's rows follow
+ * system s-1's, from row pcounts[0] + ... + pcounts[s-1] (links system-local, 1-based, as in
+ * nv_upload); all->pcount is the total.  One copy per array each way.  nv_download_packed
+ * fills pcounts[nsys] and all->pcount (arrays of cap_rows rows).  Systems with solid walls
+ * and pinned arrays are refused (NV_ERR_UNSUPPORTED): use the per-system calls. */
+int nv_upload_packed(nv_handle *h, const nv_host_state *all, const int32_t *pcounts);
+int nv_download_packed(nv_handle *h, nv_host_state *all, int64_t cap_rows, int32_t *pcounts);
 /* Page-locks (cudaHostRegister) or releases a host range, e.g. the caller's f(:) arrays. */
 int nv_host_register(void *p, size_t bytes);
 int nv_host_unregister(void *p);

@@ -74,6 +74,8 @@ def lib():
     L.nv_set_event_margins.argtypes = [vp, C.c_int32]
     L.nv_upload_many.argtypes = [vp, i32, P(i32), P(NvHostState)]
     L.nv_download_many.argtypes = [vp, i32, P(i32), P(NvHostState), P(i32)]
+    L.nv_upload_packed.argtypes = [vp, P(NvHostState), P(i32)]
+    L.nv_download_packed.argtypes = [vp, P(NvHostState), C.c_int64, P(i32)]
     L.nv_host_register.argtypes = [vp, C.c_size_t]
     L.nv_host_unregister.argtypes = [vp]
     L.nv_event_margins_get.argtypes = [vp, i32, P(C.c_double)]
@@ -116,57 +118,52 @@ def host_unregister(a: np.ndarray):
 
 
 class BatchBuffers:
-    """Host arrays of every system of a handle, as a host keeping f(:) per system would: one
-    page-locked array per field with each system's rows at a fixed offset, and the C state
-    records built once, so that a transfer of all systems is one nv_upload_many or
-    nv_download_many call."""
+    """Host arrays of every system of a handle, packed as nv_upload_packed / nv_download_packed
+    take them (system s's rows follow system s-1's), page-locked, with the C state record
+    built once: a transfer of all systems is one call and one copy per array."""
 
     FIELDS3 = ("x", "u", "u1", "u2", "ghosti", "ghostb")
-    FIELDS1 = ("infront", "behind", "closest", "closestd")
 
     def __init__(self, handle: "Handle", fields: Sequence[str] = ("x", "u", "u1", "u2", "infront", "behind")):
         self.handle = handle
-        caps = list(handle.capacity)
-        self.n = len(caps)
-        self.offsets = np.concatenate([[0], np.cumsum(caps)[:-1]]).astype(np.int64)
-        tot = int(sum(caps))
+        self.n = handle.nsys
+        self.cap_rows = int(sum(handle.capacity))
         self.arrays = {}
         for f in fields:
             if f in self.FIELDS3:
-                self.arrays[f] = np.zeros((tot, 3), np.float64)
+                self.arrays[f] = np.zeros((self.cap_rows, 3), np.float64)
             elif f == "closestd":
-                self.arrays[f] = np.zeros(tot, np.float64)
+                self.arrays[f] = np.zeros(self.cap_rows, np.float64)
             else:
-                self.arrays[f] = np.zeros(tot, np.int32)
+                self.arrays[f] = np.zeros(self.cap_rows, np.int32)
         for a in self.arrays.values():
             host_register(a)
-        self.cs = (NvHostState * self.n)()
-        for s in range(self.n):
-            rec = self.cs[s]
-            rec.pcount = 0
-            o = int(self.offsets[s])
-            for f, a in self.arrays.items():
-                ptr = a[o:].ctypes.data
-                setattr(rec, f, C.cast(ptr, C.POINTER(C.c_double if a.dtype == np.float64 else C.c_int32)))
-        self.sys = (C.c_int32 * self.n)(*range(self.n))
-        self.caps = (C.c_int32 * self.n)(*caps)
+        self.rec = NvHostState()
+        self.rec.pcount = 0
+        for f, a in self.arrays.items():
+            setattr(self.rec, f, C.cast(a.ctypes.data, C.POINTER(C.c_double if a.dtype == np.float64 else C.c_int32)))
+        self.pc = (C.c_int32 * self.n)()
 
     def download(self):
-        _check(lib().nv_download_many(self.handle.h, self.n, self.sys, self.cs, self.caps))
+        _check(lib().nv_download_packed(self.handle.h, C.byref(self.rec), self.cap_rows, self.pc))
 
     def upload(self):
-        _check(lib().nv_upload_many(self.handle.h, self.n, self.sys, self.cs))
+        _check(lib().nv_upload_packed(self.handle.h, C.byref(self.rec), self.pc))
 
     def pcounts(self) -> List[int]:
-        return [self.cs[s].pcount for s in range(self.n)]
+        return list(self.pc)
+
+    def rows(self, sys: int, field: str) -> np.ndarray:
+        """System sys's rows of a field (a view)."""
+        o = int(sum(self.pc[:sys]))
+        return self.arrays[field][o:o + self.pc[sys]]
 
     def live_points(self) -> int:
-        """Live slots of all systems (rows past a system's pcount are never written: zero)."""
-        return int(np.count_nonzero(self.arrays["infront"]))
+        return int(np.count_nonzero(self.arrays["infront"][:self.rec.pcount]))
 
     def bytes_of(self, fields: Sequence[str]) -> int:
-        """Bytes that one transfer of the given fields moves (at the current pcounts)."""
-        n = sum(self.pcounts())
+        """Bytes that one transfer of the given fields moves."""
+        n = self.rec.pcount
         return int(sum(n * self.arrays[f].itemsize * (3 if f in self.FIELDS3 else 1) for f in fields))
 
     def close(self):

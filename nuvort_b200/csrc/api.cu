@@ -875,6 +875,135 @@ int nv_download(nv_handle *h, int32_t sys, nv_host_state *st, int32_t cap) {
 }
 
 
+}  // extern "C"
+
+// The batched transfers of count systems sys[i] (n[i] points each), whatever the host layout:
+// `stage(kind, dst)` copies host array `kind` of every listed system into the staging buffer
+// at the packed offsets (system i's rows from row off[i] = n[0] + ... + n[i-1]); kinds 0-2 are
+// infront, behind, closest, 3-9 x, u, u1, u2, ghosti, ghostb, closestd.
+namespace {
+enum { kInf, kBeh, kClo, kX, kU, kU1, kU2, kGi, kGb, kCd, kKinds };
+const int kComps[kKinds] = {1, 1, 1, 3, 3, 3, 3, 3, 3, 1};
+
+template <class Stage>
+int upload_batch(nv_handle *h, int count, const int32_t *sys, const int *n, const bool given[kKinds], Stage stage,
+                 const char *who) {
+  int rc;
+  if ((rc = set_device(h)) || (rc = ensure_batch(h))) return rc;
+  cudaStream_t sm = h->stream;
+  const long long T = h->T;
+  std::vector<int4> tab(count);
+  long long N = 0;
+  int maxrows = 1;
+  for (int i = 0; i < count; ++i) {
+    tab[i] = make_int4(h->base[sys[i]], h->cap[sys[i]] + 1, n[i], (int)N);
+    N += n[i];
+    maxrows = std::max(maxrows, h->cap[sys[i]] + 1);
+  }
+  NV_CUDA(cudaMemcpyAsync(h->d_btab, tab.data(), count * sizeof(int4), cudaMemcpyHostToDevice, sm));
+  const dim3 grid(grid_for(maxrows, 256), count);
+  // links: staged and checked for every system before any system changes
+  int *si = reinterpret_cast<int *>(h->bstage);
+  int *s_inf = si, *s_beh = si + N, *s_clo = si + 2 * N;
+  if ((rc = stage(kInf, s_inf)) || (rc = stage(kBeh, s_beh)) || (given[kClo] && (rc = stage(kClo, s_clo)))) return rc;
+  NV_CUDA(cudaMemsetAsync(h->d_bcheck, 0, 2 * count * sizeof(int), sm));
+  k_upload_check_many<<<grid, 256, 0, sm>>>(h->d_btab, s_inf, s_beh, given[kClo] ? s_clo : nullptr, h->d_bcheck);
+  std::vector<int> check(2 * count);
+  NV_CUDA(cudaMemcpyAsync(check.data(), h->d_bcheck, 2 * count * sizeof(int), cudaMemcpyDeviceToHost, sm));
+  NV_CUDA(cudaStreamSynchronize(sm));
+  for (int i = 0; i < count; ++i) {
+    if (check[2 * i] & 1)
+      return set_error(NV_ERR_ARG, std::string(who) + ": link out of range in system " + std::to_string(sys[i]) +
+                                       " (no system changed)");
+    if (check[2 * i] & 2)
+      return set_error(NV_ERR_ARG, std::string(who) + ": infront/behind disagree on an empty slot in system " +
+                                       std::to_string(sys[i]) + " (no system changed)");
+  }
+  ++h->links_epoch;
+  k_put_links_many<<<grid, 256, 0, sm>>>(h->nxt, h->d_btab, s_inf);
+  k_put_links_many<<<grid, 256, 0, sm>>>(h->prv, h->d_btab, s_beh);
+  k_put_links_many<<<grid, 256, 0, sm>>>(h->closest, h->d_btab, given[kClo] ? s_clo : nullptr);
+  // each double array of every system into the staging buffer, then one launch to the slots
+  // (in stream order, so the buffer is reused array after array)
+  double *dev[kKinds] = {nullptr, nullptr, nullptr, h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd};
+  for (int kind = kX; kind < kKinds; ++kind) {
+    if (given[kind] && (rc = stage(kind, h->bstage))) return rc;
+    k_put_rows_many<<<grid, 256, 0, sm>>>(dev[kind], T, h->d_btab, kComps[kind], given[kind] ? h->bstage : nullptr);
+  }
+  k_put_rows_many<<<grid, 256, 0, sm>>>(h->usm, T, h->d_btab, 6, nullptr);
+  k_put_rows_many<<<grid, 256, 0, sm>>>(h->cs, T, h->d_btab, 2, nullptr);
+  // the clocks and counters stay; the slot counts are replaced
+  NV_CUDA(cudaMemcpyAsync(h->h_dyn.data(), h->d_dyn, h->nsys * sizeof(SysDyn), cudaMemcpyDeviceToHost, sm));
+  NV_CUDA(cudaStreamSynchronize(sm));
+  for (int i = 0; i < count; ++i) {
+    SysDyn &d = h->h_dyn[sys[i]];
+    d.pcount = n[i];
+    d.nlive = check[2 * i + 1];
+  }
+  NV_CUDA(cudaMemcpyAsync(h->d_dyn, h->h_dyn.data(), h->nsys * sizeof(SysDyn), cudaMemcpyHostToDevice, sm));
+  NV_CUDA(cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), sm));
+  NV_CUDA(cudaStreamSynchronize(sm));
+  return NV_OK;
+}
+
+// `fetch(kind, src, tab)` copies array `kind` of every listed system from the staging buffer
+// (packed offsets tab[i].w) to the host.  n_out[i] receives each system's pcount first;
+// `fits(i, n)` refuses a system whose arrays are too small.
+template <class Fits, class Fetch>
+int download_batch(nv_handle *h, int count, const int32_t *sys, const bool want[kKinds], int *n_out, Fits fits,
+                   Fetch fetch) {
+  int rc;
+  if ((rc = set_device(h)) || (rc = ensure_batch(h))) return rc;
+  cudaStream_t sm = h->stream;
+  const long long T = h->T;
+  NV_CUDA(cudaMemcpyAsync(h->h_dyn.data(), h->d_dyn, h->nsys * sizeof(SysDyn), cudaMemcpyDeviceToHost, sm));
+  NV_CUDA(cudaStreamSynchronize(sm));
+  std::vector<int4> tab(count);
+  long long N = 0;
+  int maxn = 1;
+  for (int i = 0; i < count; ++i) {
+    const int s = sys[i], n = h->h_dyn[s].pcount;
+    n_out[i] = n;
+    if ((rc = fits(i, n))) return rc;
+    tab[i] = make_int4(h->base[s], h->cap[s] + 1, n, (int)N);
+    N += n;
+    maxn = std::max(maxn, n);
+  }
+  NV_CUDA(cudaMemcpyAsync(h->d_btab, tab.data(), count * sizeof(int4), cudaMemcpyHostToDevice, sm));
+  const dim3 grid(grid_for(maxn, 256), count);
+  // one launch per array over every system into the staging buffer, then the copies out
+  // (stream order keeps the buffer from being overwritten before its copies are done)
+  const double *dev[kKinds] = {nullptr, nullptr, nullptr, h->x, h->u, h->u1, h->u2, h->gi, h->gb, h->closestd};
+  const int *devl[3] = {h->nxt, h->prv, h->closest};
+  for (int kind = 0; kind < kKinds; ++kind) {
+    if (!want[kind]) continue;
+    if (kind <= kClo) k_get_links_many<<<grid, 256, 0, sm>>>(devl[kind], h->d_btab, reinterpret_cast<int *>(h->bstage));
+    else k_get_rows_many<<<grid, 256, 0, sm>>>(dev[kind], T, h->d_btab, kComps[kind], h->bstage);
+    if ((rc = fetch(kind, tab))) return rc;
+  }
+  NV_CUDA(cudaStreamSynchronize(sm));
+  return NV_OK;
+}
+
+void *field_of(const nv_host_state &s, int kind) {
+  switch (kind) {
+    case kInf: return s.infront;
+    case kBeh: return s.behind;
+    case kClo: return s.closest;
+    case kX: return s.x;
+    case kU: return s.u;
+    case kU1: return s.u1;
+    case kU2: return s.u2;
+    case kGi: return s.ghosti;
+    case kGb: return s.ghostb;
+    default: return s.closestd;
+  }
+}
+size_t elem_bytes(int kind) { return kind <= kClo ? sizeof(int) : sizeof(double); }
+}  // namespace
+
+extern "C" {
+
 int nv_upload_many(nv_handle *h, int32_t count, const int32_t *sys, const nv_host_state *st) {
   int rc = batch_args(h, count, sys, st, "nv_upload_many");
   if (rc) return rc;
@@ -894,79 +1023,25 @@ int nv_upload_many(nv_handle *h, int32_t count, const int32_t *sys, const nv_hos
   if (!fields_consistent(count, st))
     return set_error(NV_ERR_ARG, "nv_upload_many: each optional array must be given for every listed system or none");
   if (count == 0) return NV_OK;
-  if ((rc = set_device(h)) || (rc = ensure_batch(h))) return rc;
+  std::vector<int> n(count), off(count);
+  for (int i = 0, o = 0; i < count; ++i) {
+    n[i] = st[i].pcount;
+    off[i] = o;
+    o += n[i];
+  }
+  bool given[kKinds];
+  for (int kind = 0; kind < kKinds; ++kind) given[kind] = field_of(st[0], kind) != nullptr;
   cudaStream_t sm = h->stream;
-  const long long T = h->T;
-  std::vector<int4> tab(count);
-  long long N = 0;
-  int maxrows = 1;
-  for (int i = 0; i < count; ++i) {
-    const int s = sys[i];
-    tab[i] = make_int4(h->base[s], h->cap[s] + 1, st[i].pcount, (int)N);
-    N += st[i].pcount;
-    maxrows = std::max(maxrows, h->cap[s] + 1);
-  }
-  NV_CUDA(cudaMemcpyAsync(h->d_btab, tab.data(), count * sizeof(int4), cudaMemcpyHostToDevice, sm));
-  const dim3 grid(grid_for(maxrows, 256), count);
-  // links: staged and checked for every system before any system changes
-  int *si = reinterpret_cast<int *>(h->bstage);
-  int *s_inf = si, *s_beh = si + N, *s_clo = si + 2 * N;
-  const bool clo = st[0].closest != nullptr;
-  for (int i = 0; i < count; ++i) {
-    const size_t n = st[i].pcount, o = tab[i].w;
-    if (!n) continue;
-    NV_CUDA(cudaMemcpyAsync(s_inf + o, st[i].infront, n * sizeof(int), cudaMemcpyHostToDevice, sm));
-    NV_CUDA(cudaMemcpyAsync(s_beh + o, st[i].behind, n * sizeof(int), cudaMemcpyHostToDevice, sm));
-    if (clo) NV_CUDA(cudaMemcpyAsync(s_clo + o, st[i].closest, n * sizeof(int), cudaMemcpyHostToDevice, sm));
-  }
-  NV_CUDA(cudaMemsetAsync(h->d_bcheck, 0, 2 * count * sizeof(int), sm));
-  k_upload_check_many<<<grid, 256, 0, sm>>>(h->d_btab, s_inf, s_beh, clo ? s_clo : nullptr, h->d_bcheck);
-  std::vector<int> check(2 * count);
-  NV_CUDA(cudaMemcpyAsync(check.data(), h->d_bcheck, 2 * count * sizeof(int), cudaMemcpyDeviceToHost, sm));
-  NV_CUDA(cudaStreamSynchronize(sm));
-  for (int i = 0; i < count; ++i) {
-    if (check[2 * i] & 1)
-      return set_error(NV_ERR_ARG, "nv_upload_many: link out of range in system " + std::to_string(sys[i]) +
-                                       " (no system changed)");
-    if (check[2 * i] & 2)
-      return set_error(NV_ERR_ARG, "nv_upload_many: infront/behind disagree on an empty slot in system " +
-                                       std::to_string(sys[i]) + " (no system changed)");
-  }
-  ++h->links_epoch;
-  k_put_links_many<<<grid, 256, 0, sm>>>(h->nxt, h->d_btab, s_inf);
-  k_put_links_many<<<grid, 256, 0, sm>>>(h->prv, h->d_btab, s_beh);
-  k_put_links_many<<<grid, 256, 0, sm>>>(h->closest, h->d_btab, clo ? s_clo : nullptr);
-  // each double array of every system into the staging buffer, then one launch to the slots
-  // (in stream order, so the buffer is reused array after array)
-  auto put = [&](double *dev, double *const nv_host_state::*field, int comps) -> int {
-    const bool given = st[0].*field != nullptr;
-    if (given)
-      for (int i = 0; i < count; ++i)
-        if (st[i].pcount)
-          NV_CUDA(cudaMemcpyAsync(h->bstage + (size_t)comps * tab[i].w, st[i].*field,
-                                  (size_t)comps * st[i].pcount * sizeof(double), cudaMemcpyHostToDevice, sm));
-    k_put_rows_many<<<grid, 256, 0, sm>>>(dev, T, h->d_btab, comps, given ? h->bstage : nullptr);
+  auto stage = [&](int kind, void *dst) -> int {
+    const int c = kComps[kind];
+    const size_t e = elem_bytes(kind);
+    for (int i = 0; i < count; ++i)
+      if (n[i])
+        NV_CUDA(cudaMemcpyAsync(static_cast<char *>(dst) + (size_t)c * off[i] * e, field_of(st[i], kind),
+                                (size_t)c * n[i] * e, cudaMemcpyHostToDevice, sm));
     return NV_OK;
   };
-  if ((rc = put(h->x, &nv_host_state::x, 3)) || (rc = put(h->u, &nv_host_state::u, 3)) ||
-      (rc = put(h->u1, &nv_host_state::u1, 3)) || (rc = put(h->u2, &nv_host_state::u2, 3)) ||
-      (rc = put(h->gi, &nv_host_state::ghosti, 3)) || (rc = put(h->gb, &nv_host_state::ghostb, 3)) ||
-      (rc = put(h->closestd, &nv_host_state::closestd, 1)))
-    return rc;
-  k_put_rows_many<<<grid, 256, 0, sm>>>(h->usm, T, h->d_btab, 6, nullptr);
-  k_put_rows_many<<<grid, 256, 0, sm>>>(h->cs, T, h->d_btab, 2, nullptr);
-  // the clocks and counters stay; the slot counts are replaced
-  NV_CUDA(cudaMemcpyAsync(h->h_dyn.data(), h->d_dyn, h->nsys * sizeof(SysDyn), cudaMemcpyDeviceToHost, sm));
-  NV_CUDA(cudaStreamSynchronize(sm));
-  for (int i = 0; i < count; ++i) {
-    SysDyn &d = h->h_dyn[sys[i]];
-    d.pcount = st[i].pcount;
-    d.nlive = check[2 * i + 1];
-  }
-  NV_CUDA(cudaMemcpyAsync(h->d_dyn, h->h_dyn.data(), h->nsys * sizeof(SysDyn), cudaMemcpyHostToDevice, sm));
-  NV_CUDA(cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), sm));
-  NV_CUDA(cudaStreamSynchronize(sm));
-  return NV_OK;
+  return upload_batch(h, count, sys, n.data(), given, stage, "nv_upload_many");
 }
 
 int nv_download_many(nv_handle *h, int32_t count, const int32_t *sys, nv_host_state *st, const int32_t *cap) {
@@ -987,53 +1062,73 @@ int nv_download_many(nv_handle *h, int32_t count, const int32_t *sys, nv_host_st
       !all_or_none(count, st, [](const nv_host_state &s) { return (const void *)s.behind; }))
     return set_error(NV_ERR_ARG, "nv_download_many: each array must be asked for every listed system or none");
   if (count == 0) return NV_OK;
-  if ((rc = set_device(h)) || (rc = ensure_batch(h))) return rc;
+  bool want[kKinds];
+  for (int kind = 0; kind < kKinds; ++kind) want[kind] = field_of(st[0], kind) != nullptr;
+  std::vector<int> n(count);
   cudaStream_t sm = h->stream;
-  const long long T = h->T;
-  NV_CUDA(cudaMemcpyAsync(h->h_dyn.data(), h->d_dyn, h->nsys * sizeof(SysDyn), cudaMemcpyDeviceToHost, sm));
-  NV_CUDA(cudaStreamSynchronize(sm));
-  std::vector<int4> tab(count);
-  long long N = 0;
-  int maxn = 1;
-  for (int i = 0; i < count; ++i) {
-    const int s = sys[i], n = h->h_dyn[s].pcount;
-    st[i].pcount = n;
-    if (n > cap[i]) return set_error(NV_ERR_ARG, "nv_download_many: arrays hold fewer slots than pcount");
-    tab[i] = make_int4(h->base[s], h->cap[s] + 1, n, (int)N);
-    N += n;
-    maxn = std::max(maxn, n);
+  auto fits = [&](int i, int pc) -> int {
+    st[i].pcount = pc;
+    return pc > cap[i] ? set_error(NV_ERR_ARG, "nv_download_many: arrays hold fewer slots than pcount") : NV_OK;
+  };
+  auto fetch = [&](int kind, const std::vector<int4> &tab) -> int {
+    const int c = kComps[kind];
+    const size_t e = elem_bytes(kind);
+    for (int i = 0; i < count; ++i)
+      if (tab[i].z)
+        NV_CUDA(cudaMemcpyAsync(field_of(st[i], kind), reinterpret_cast<char *>(h->bstage) + (size_t)c * tab[i].w * e,
+                                (size_t)c * tab[i].z * e, cudaMemcpyDeviceToHost, sm));
+    return NV_OK;
+  };
+  return download_batch(h, count, sys, want, n.data(), fits, fetch);
+}
+
+int nv_upload_packed(nv_handle *h, const nv_host_state *all, const int32_t *pcounts) {
+  if (!h || !all || !pcounts) return set_error(NV_ERR_ARG, "nv_upload_packed: bad arguments");
+  if (!all->x || !all->infront || !all->behind) return set_error(NV_ERR_ARG, "nv_upload_packed: x, infront, behind are required");
+  if (all->wpinned || all->pinnedi || all->pinnedb) return set_error(NV_ERR_UNSUPPORTED, "nv_upload_packed: no pinned records (use nv_upload)");
+  long long tot = 0;
+  std::vector<int32_t> sys(h->nsys);
+  std::vector<int> n(h->nsys);
+  for (int s = 0; s < h->nsys; ++s) {
+    if (h->sc[s].pin) return set_error(NV_ERR_UNSUPPORTED, "nv_upload_packed: a system has solid walls (use nv_upload)");
+    if (pcounts[s] < 0 || pcounts[s] > h->cap[s]) return set_error(NV_ERR_ARG, "nv_upload_packed: pcount exceeds a system's capacity");
+    sys[s] = s;
+    n[s] = pcounts[s];
+    tot += pcounts[s];
   }
-  NV_CUDA(cudaMemcpyAsync(h->d_btab, tab.data(), count * sizeof(int4), cudaMemcpyHostToDevice, sm));
-  const dim3 grid(grid_for(maxn, 256), count);
-  // one launch per array over every system into the staging buffer, then a copy per system
-  // (stream order keeps the buffer from being overwritten before its copies are done)
-  auto get = [&](const double *dev, double *nv_host_state::*field, int comps) -> int {
-    if (!(st[0].*field)) return NV_OK;
-    k_get_rows_many<<<grid, 256, 0, sm>>>(dev, T, h->d_btab, comps, h->bstage);
-    for (int i = 0; i < count; ++i)
-      if (st[i].pcount)
-        NV_CUDA(cudaMemcpyAsync(st[i].*field, h->bstage + (size_t)comps * tab[i].w,
-                                (size_t)comps * st[i].pcount * sizeof(double), cudaMemcpyDeviceToHost, sm));
+  if (tot != all->pcount) return set_error(NV_ERR_ARG, "nv_upload_packed: all->pcount must be the sum of pcounts");
+  bool given[kKinds];
+  for (int kind = 0; kind < kKinds; ++kind) given[kind] = field_of(*all, kind) != nullptr;
+  cudaStream_t sm = h->stream;
+  auto stage = [&](int kind, void *dst) -> int {  // the packed host array is the staging layout
+    if (tot) NV_CUDA(cudaMemcpyAsync(dst, field_of(*all, kind), (size_t)kComps[kind] * tot * elem_bytes(kind),
+                                     cudaMemcpyHostToDevice, sm));
     return NV_OK;
   };
-  int *si = reinterpret_cast<int *>(h->bstage);
-  auto get_link = [&](const int *dev, int32_t *nv_host_state::*field) -> int {
-    if (!(st[0].*field)) return NV_OK;
-    k_get_links_many<<<grid, 256, 0, sm>>>(dev, h->d_btab, si);
-    for (int i = 0; i < count; ++i)
-      if (st[i].pcount)
-        NV_CUDA(cudaMemcpyAsync(st[i].*field, si + tab[i].w, (size_t)st[i].pcount * sizeof(int),
-                                cudaMemcpyDeviceToHost, sm));
+  return upload_batch(h, h->nsys, sys.data(), n.data(), given, stage, "nv_upload_packed");
+}
+
+int nv_download_packed(nv_handle *h, nv_host_state *all, int64_t cap_rows, int32_t *pcounts) {
+  if (!h || !all || !pcounts) return set_error(NV_ERR_ARG, "nv_download_packed: bad arguments");
+  if (all->wpinned || all->pinnedi || all->pinnedb) return set_error(NV_ERR_UNSUPPORTED, "nv_download_packed: no pinned records (use nv_download)");
+  std::vector<int32_t> sys(h->nsys);
+  for (int s = 0; s < h->nsys; ++s) sys[s] = s;
+  bool want[kKinds];
+  for (int kind = 0; kind < kKinds; ++kind) want[kind] = field_of(*all, kind) != nullptr;
+  long long tot = 0;
+  auto fits = [&](int i, int pc) -> int {
+    tot += pc;
+    return tot > cap_rows ? set_error(NV_ERR_ARG, "nv_download_packed: arrays hold fewer rows than the systems' points") : NV_OK;
+  };
+  cudaStream_t sm = h->stream;
+  auto fetch = [&](int kind, const std::vector<int4> &) -> int {
+    if (tot) NV_CUDA(cudaMemcpyAsync(field_of(*all, kind), h->bstage, (size_t)kComps[kind] * tot * elem_bytes(kind),
+                                     cudaMemcpyDeviceToHost, sm));
     return NV_OK;
   };
-  if ((rc = get(h->x, &nv_host_state::x, 3)) || (rc = get(h->u, &nv_host_state::u, 3)) ||
-      (rc = get(h->u1, &nv_host_state::u1, 3)) || (rc = get(h->u2, &nv_host_state::u2, 3)) ||
-      (rc = get(h->gi, &nv_host_state::ghosti, 3)) || (rc = get(h->gb, &nv_host_state::ghostb, 3)) ||
-      (rc = get_link(h->nxt, &nv_host_state::infront)) || (rc = get_link(h->prv, &nv_host_state::behind)) ||
-      (rc = get_link(h->closest, &nv_host_state::closest)) || (rc = get(h->closestd, &nv_host_state::closestd, 1)))
-    return rc;
-  NV_CUDA(cudaStreamSynchronize(sm));
-  return NV_OK;
+  int rc = download_batch(h, h->nsys, sys.data(), want, pcounts, fits, fetch);
+  if (rc == NV_OK) all->pcount = (int32_t)tot;
+  return rc;
 }
 
 int nv_host_register(void *p, size_t bytes) {

@@ -108,15 +108,20 @@ def test_batch_buffers_round_trip():
             assert hb.pcounts() == [s.pcount for s in sts]
             assert hb.live_points() == sum(int(np.count_nonzero(s.infront)) for s in sts)
             for s, st in enumerate(sts):
-                o = int(hb.offsets[s])
-                assert np.array_equal(hb.arrays["x"][o:o + st.pcount], st.x)
+                assert np.array_equal(hb.rows(s, "x"), st.x)
             h.step(2)
             hb.download()
             ref = h.download_many()
             hb.upload()  # the same state back: nothing changes
             for s, r in enumerate(ref):
-                o = int(hb.offsets[s])
-                assert np.array_equal(hb.arrays["infront"][o:o + r.pcount], r.infront)
+                assert np.array_equal(hb.rows(s, "infront"), r.infront)
                 assert np.array_equal(h.download(s).x, r.x)
+            # a packed upload with a bad link in one system changes nothing
+            from nuvort_b200.api import NuvortError
+            hb.rows(3, "infront")[7] = hb.pcounts()[3] + 5
+            with pytest.raises(NuvortError):
+                hb.upload()
+            for s, r in enumerate(ref):
+                assert np.array_equal(h.download(s).infront, r.infront)
         finally:
             hb.close()
