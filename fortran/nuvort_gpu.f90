@@ -226,6 +226,20 @@ module nuvort_gpu
       integer(c_int32_t), intent(in) :: sys(*), cap(*)
       type(nv_host_state), intent(inout) :: st(*)
     end function
+    !> every system at once, host arrays packed system after system (pcounts(nsys))
+    integer(c_int) function nv_upload_packed(h, all, pcounts) bind(c, name='nv_upload_packed')
+      import :: c_int, c_int32_t, c_ptr, nv_host_state
+      type(c_ptr), value :: h
+      type(nv_host_state), intent(in) :: all
+      integer(c_int32_t), intent(in) :: pcounts(*)
+    end function
+    integer(c_int) function nv_download_packed(h, all, cap_rows, pcounts) bind(c, name='nv_download_packed')
+      import :: c_int, c_int32_t, c_int64_t, c_ptr, nv_host_state
+      type(c_ptr), value :: h
+      type(nv_host_state), intent(inout) :: all
+      integer(c_int64_t), value :: cap_rows
+      integer(c_int32_t), intent(out) :: pcounts(*)
+    end function
     !> page-lock (cudaHostRegister) a host range, e.g. f(:)'s packed arrays
     integer(c_int) function nv_host_register(p, bytes) bind(c, name='nv_host_register')
       import :: c_int, c_ptr, c_size_t
