@@ -283,6 +283,24 @@ int nv_set_walk_parts(nv_handle *h, int32_t parts);
  * them, 1e300 where no test ran. */
 int nv_set_event_margins(nv_handle *h, int32_t on);
 int nv_event_margins_get(nv_handle *h, int32_t sys, double *out);
+/* One tangle over several GPUs (one process and handle per GPU, each holding the whole
+ * state): nv_step_velocity runs a step up to and including the velocity pass,
+ * nv_step_finish the rest (AB3 update, topology, wrap, clock), the two together exactly
+ * nv_step(1).  With nv_set_walk_range a tree-walk system's velocity pass computes only the
+ * targets at walk positions lo <= q < hi (the walk order: the live points in Morton order at
+ * positions 1 .. live, then the empty slots).  The ends fall on warp boundaries: lo - 1 a
+ * multiple of 32, and hi - 1 one too or hi = cap + 1 (the mixed walk's 32 targets of a warp
+ * share their FP32 partial sums' flush points, which a warp cut in two would change); other
+ * ends are refused with NV_ERR_ARG.  nv_velocity_pack copies the velocities of
+ * positions lo .. lo+count-1 into a device buffer [count][3] and nv_velocity_unpack writes
+ * them back, so that ranks split the positions, exchange their parts between the two halves
+ * (an all-gather), and every rank continues with the full velocity field: the same step,
+ * bit for bit, as one GPU's.  Default range: all positions. */
+int nv_set_walk_range(nv_handle *h, int32_t sys, int32_t lo, int32_t hi);
+int nv_velocity_pack(nv_handle *h, int32_t sys, int32_t lo, int32_t count, double *d_buf);
+int nv_velocity_unpack(nv_handle *h, int32_t sys, int32_t lo, int32_t count, const double *d_buf);
+int nv_step_velocity(nv_handle *h);
+int nv_step_finish(nv_handle *h);
 /* Data of the normal-fluid fields that the reference reads from files.  noisey_xflow: the n
  * multipliers of noise_file (src/normal_fluid.f90:156-162; the reference reads 100000), used
  * one per step from the first, wrapping after the last (randomise_normal_fluid, :340-348).

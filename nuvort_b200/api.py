@@ -75,6 +75,11 @@ def lib():
     L.nv_upload_many.argtypes = [vp, i32, P(i32), P(NvHostState)]
     L.nv_download_many.argtypes = [vp, i32, P(i32), P(NvHostState), P(i32)]
     L.nv_upload_packed.argtypes = [vp, P(NvHostState), P(i32)]
+    L.nv_set_walk_range.argtypes = [vp, i32, i32, i32]
+    L.nv_velocity_pack.argtypes = [vp, i32, i32, i32, vp]
+    L.nv_velocity_unpack.argtypes = [vp, i32, i32, i32, vp]
+    L.nv_step_velocity.argtypes = [vp]
+    L.nv_step_finish.argtypes = [vp]
     L.nv_download_packed.argtypes = [vp, P(NvHostState), C.c_int64, P(i32)]
     L.nv_host_register.argtypes = [vp, C.c_size_t]
     L.nv_host_unregister.argtypes = [vp]
@@ -428,6 +433,27 @@ class Handle:
         """Split of the tree walks' work (mixed: central image over groups of root children;
         FP64: unshifted / shifted images on two threads per target); 0: automatic."""
         _check(lib().nv_set_walk_parts(self.h, int(parts)))
+
+    def set_walk_range(self, sys: int, lo: int, hi: int):
+        """Tree walks compute only walk positions lo <= q < hi of system sys (one tangle split
+        over GPUs); (1, capacity + 1) restores all."""
+        _check(lib().nv_set_walk_range(self.h, int(sys), int(lo), int(hi)))
+
+    def velocity_pack(self, sys: int, lo: int, count: int, dev_ptr: int):
+        """Velocities of walk positions lo .. lo+count-1 into a device buffer [count][3] (a
+        CUDA pointer, e.g. a torch tensor's data_ptr())."""
+        _check(lib().nv_velocity_pack(self.h, int(sys), int(lo), int(count), C.c_void_p(int(dev_ptr))))
+
+    def velocity_unpack(self, sys: int, lo: int, count: int, dev_ptr: int):
+        _check(lib().nv_velocity_unpack(self.h, int(sys), int(lo), int(count), C.c_void_p(int(dev_ptr))))
+
+    def step_velocity(self):
+        """The first half of a step: up to and including the velocity pass."""
+        _check(lib().nv_step_velocity(self.h))
+
+    def step_finish(self):
+        """The second half: AB3 update, topology, wrap, clock."""
+        _check(lib().nv_step_finish(self.h))
 
     def set_event_margins(self, on: bool = True):
         """Switch the event-margin record on (and reset it) or off."""

@@ -154,10 +154,27 @@ __global__ void k_get_links_many(const int *__restrict__ dev, const int4 *__rest
   host[t.w + k - 1] = v ? v - t.x : 0;
 }
 
+// velocities of walk positions [lo, hi) of system s to / from a packed buffer [count][3]
+__global__ void k_vel_pack(const double *__restrict__ U, long long T, const int *__restrict__ perm, int base, int lo,
+                           int count, double *__restrict__ buf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int g = perm[base + lo + i];
+  for (int c = 0; c < 3; ++c) buf[3 * (long long)i + c] = U[c * T + g];
+}
+__global__ void k_vel_unpack(double *__restrict__ U, long long T, const int *__restrict__ perm, int base, int lo,
+                             int count, const double *__restrict__ buf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int g = perm[base + lo + i];
+  for (int c = 0; c < 3; ++c) U[c * T + g] = buf[3 * (long long)i + c];
+}
+
 int err_code_from_bits(unsigned bits, std::string &msg) {
   if (bits & DERR_SINGULAR) { msg = "tree_walk: singularity in BS (tree) velocity field (dist<epsilon)"; return NV_ERR_SINGULAR; }
   if (bits & DERR_TREE_DEPTH) { msg = "octree deeper than NV_TREE_MAX_DEPTH levels (coincident points?)"; return NV_ERR_TREE_DEPTH; }
   if (bits & DERR_TREE_NODES) { msg = "octree node buffer exhausted"; return NV_ERR_TREE_DEPTH; }
+  if (bits & DERR_WALK) { msg = "tree walk visited more nodes than the octree holds (a malformed tree)"; return NV_ERR_TREE_DEPTH; }
   if (bits & DERR_NAN) { msg = "there is a NAN in the (filament) f%x array"; return NV_ERR_NAN; }
   if (bits & DERR_EMPTY) { msg = "pinsert: vortex line length is 0, run over"; return NV_ERR_EMPTY; }
   if (bits & DERR_CAPACITY) { msg = "pinsert: system capacity exhausted"; return NV_ERR_CAPACITY; }
@@ -278,6 +295,8 @@ SysConst make_sysconst(const nv_params &p, int base, int cap) {
   s.sched_tree = p.velocity == NV_VEL_TREE;
   s.base = base;
   s.cap = cap;
+  s.walk_lo = 1;
+  s.walk_hi = cap + 1;
   return s;
 }
 
@@ -1430,6 +1449,71 @@ int nv_set_root_band(nv_handle *h, double scale) {
   h->root_band_scale = scale;
   h->graph_valid = false;  // a launch argument of the captured step
   return NV_OK;
+}
+
+int nv_set_walk_range(nv_handle *h, int32_t sys, int32_t lo, int32_t hi) {
+  if (!h || sys < 0 || sys >= h->nsys) return set_error(NV_ERR_ARG, "nv_set_walk_range: bad arguments");
+  SysConst &c = h->sc[sys];
+  if (!c.sched_tree || c.velocity == NV_VEL_LIA || c.pin)
+    return set_error(NV_ERR_UNSUPPORTED, "nv_set_walk_range: tree-walk systems without solid walls only");
+  if (lo < 1 || hi < lo || hi > c.cap + 1) return set_error(NV_ERR_ARG, "nv_set_walk_range: need 1 <= lo <= hi <= cap + 1");
+  if ((lo - 1) % 32 != 0 || ((hi - 1) % 32 != 0 && hi != c.cap + 1))
+    return set_error(NV_ERR_ARG, "nv_set_walk_range: lo - 1 and hi - 1 must be multiples of 32 (or hi = cap + 1)");
+  int rc = set_device(h);
+  if (rc) return rc;
+  c.walk_lo = lo;
+  c.walk_hi = hi;
+  NV_CUDA(cudaMemcpy(h->d_sc + sys, &c, sizeof(SysConst), cudaMemcpyHostToDevice));
+  return NV_OK;
+}
+
+int nv_velocity_pack(nv_handle *h, int32_t sys, int32_t lo, int32_t count, double *d_buf) {
+  if (!h || sys < 0 || sys >= h->nsys || lo < 1 || count < 0 || lo + count > h->cap[sys] + 1 || (count && !d_buf))
+    return set_error(NV_ERR_ARG, "nv_velocity_pack: bad arguments");
+  const int *perm = tree_perm(h);
+  if (!perm) return set_error(NV_ERR_STATE, "nv_velocity_pack: no walk order (no tree built)");
+  int rc = set_device(h);
+  if (rc) return rc;
+  if (count) k_vel_pack<<<grid_for(count, 256), 256, 0, h->stream>>>(h->u, h->T, perm, h->base[sys], lo, count, d_buf);
+  return finish(h);
+}
+
+int nv_velocity_unpack(nv_handle *h, int32_t sys, int32_t lo, int32_t count, const double *d_buf) {
+  if (!h || sys < 0 || sys >= h->nsys || lo < 1 || count < 0 || lo + count > h->cap[sys] + 1 || (count && !d_buf))
+    return set_error(NV_ERR_ARG, "nv_velocity_unpack: bad arguments");
+  const int *perm = tree_perm(h);
+  if (!perm) return set_error(NV_ERR_STATE, "nv_velocity_unpack: no walk order (no tree built)");
+  int rc = set_device(h);
+  if (rc) return rc;
+  if (count) k_vel_unpack<<<grid_for(count, 256), 256, 0, h->stream>>>(h->u, h->T, perm, h->base[sys], lo, count, d_buf);
+  return finish(h);
+}
+
+int nv_step_velocity(nv_handle *h) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  if (nf_missing(h)) return NV_ERR_STATE;
+  int rc = set_device(h);
+  if (rc) return rc;
+  launch_begin_step(h);
+  launch_ghost(h);
+  if (any_use_tree(h) || h->any_tree) launch_tree_build(h);
+  launch_velocity(h);
+  return finish(h);
+}
+
+int nv_step_finish(nv_handle *h) {
+  if (!h) return set_error(NV_ERR_ARG, "null handle");
+  int rc = set_device(h);
+  if (rc) return rc;
+  launch_ab3(h);
+  launch_pinsert(h);
+  launch_pclose(h, false);
+  launch_precon(h);
+  launch_wall_recon(h);
+  launch_premove(h);
+  launch_wrap(h, 3);
+  launch_end_step(h);
+  return finish(h);
 }
 
 int nv_set_walk_parts(nv_handle *h, int32_t parts) {

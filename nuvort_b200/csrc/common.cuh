@@ -29,6 +29,7 @@ enum : unsigned {
   DERR_QUEUE = 1u << 5,
   DERR_TIMEOUT = 1u << 6,
   DERR_TREE_NODES = 1u << 7,
+  DERR_WALK = 1u << 8,  // a tree walk visited more nodes than the tree holds
 };
 
 struct SysConst {
@@ -76,6 +77,10 @@ struct SysConst {
   int n_mirror;
   int mirror[26][3];
   int solid[3];
+  // the tree walks compute targets at walk positions walk_lo <= q < walk_hi only (the walk
+  // order: the system's dummy slot, its live points in Morton order, its empty slots); all
+  // by default, a range when one tangle's velocity is split over several GPUs
+  int walk_lo, walk_hi;
 };
 
 // Pinned-point record of a slot: bit 0 pinnedi, bit 1 pinnedb, bits 2-7 wpinned(1..3), two

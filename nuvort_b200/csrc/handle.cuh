@@ -114,6 +114,8 @@ void launch_direct_targets(nv_handle *h, int sys, const int *d_targets, int n, d
 void launch_direct_mixed(nv_handle *h);
 void launch_mixed_combine(nv_handle *h, int which);
 void launch_tree_walk_mixed(nv_handle *h);
+const int *tree_iperm(nv_handle *h);  // slot -> walk position of the last tree build (or null)
+const int *tree_perm(nv_handle *h);   // walk position (global: base + q) -> slot
 // tree (tree.cu)
 constexpr int kMaxWalkParts = 8;  // the central image's walk splits over at most the root's 8 children
 int n_sms_host();                  // SMs of the current device

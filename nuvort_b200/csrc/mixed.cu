@@ -178,13 +178,18 @@ __global__ void k_mixed_combine(const SysConst *__restrict__ scs, const SysDyn *
                                 const int2 *__restrict__ work, const double *__restrict__ X,
                                 const double *__restrict__ GI, const double *__restrict__ GB,
                                 const int *__restrict__ nxt, const double *__restrict__ partial,
-                                double *__restrict__ U, long long T, int extra, const unsigned *err) {
+                                double *__restrict__ U, long long T, int extra, const int *__restrict__ iperm,
+                                const unsigned *err) {
   if (*err) return;
   const int2 w = work[blockIdx.x];
   const SysConst &sc = scs[w.x];
   const int g = w.y + threadIdx.x;
   const int k = g - sc.base;
   if (k > dyn[w.x].pcount || k > sc.cap || nxt[g] == 0) return;
+  if (iperm && (sc.walk_lo > 1 || sc.walk_hi <= sc.cap)) {  // a walk range: its targets only
+    const int q = iperm[g] - sc.base;
+    if (q < sc.walk_lo || q >= sc.walk_hi) return;
+  }
   double xi[3], gi[3], gb[3], u[3], fdot[3];
   load3(X, T, g, xi);
   load3(GI, T, g, gi);
@@ -218,7 +223,8 @@ void launch_mixed_combine(nv_handle *h, int which) {
   if (n == 0) return;
   const int extra = which == 2 ? h->walk_parts_used - 1 : 0;
   k_mixed_combine<<<n, h->direct_tb, 0, h->stream>>>(h->d_sc, h->d_dyn, wl, h->x, h->gi, h->gb, h->nxt, h->partial,
-                                                     h->u, h->T, extra, h->d_err);
+                                                     h->u, h->T, extra, which == 2 ? tree_iperm(h) : nullptr,
+                                                     h->d_err);
 }
 
 int mixed_tiles_per_block() { return kTB; }

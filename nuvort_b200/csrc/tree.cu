@@ -79,6 +79,7 @@ struct TreeBuffers {
   unsigned long long *okey[2] = {nullptr, nullptr};
   int *oval[2] = {nullptr, nullptr};
   int *perm = nullptr;  // = oval[1]: position base+q of system s -> slot
+  int *iperm = nullptr; // slot -> its position in the walk order (inverse of perm)
   void *sort_tmp = nullptr;
   size_t sort_bytes = 0;
   int key_bits = 0;
@@ -178,6 +179,11 @@ __global__ void k_order_keys(const SysConst *__restrict__ scs, const SysDyn *__r
   }
   key[g] = ((unsigned long long)s << 34) | inner;
   val[g] = (int)g;
+}
+
+__global__ void k_inv_perm(const int *__restrict__ perm, int *__restrict__ iperm, long long T) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < T) iperm[perm[i]] = (int)i;
 }
 
 __global__ void k_iota(int *v, long long n) {
@@ -989,11 +995,16 @@ __device__ __forceinline__ void defer_push(const TreeBuffers &tb, int g, int m, 
 __device__ __forceinline__ void walk_fp64(const TreeBuffers &tb, int start, const SysConst &sc, const double xi[3],
                                           int gi_, int pi_, const int *__restrict__ prv, const double s[3], bool unshifted,
                                           double acc[3], unsigned long long &evals, unsigned long long &tests,
-                                          bool &singular) {
+                                          bool &singular, bool &overrun) {
   const double qc = sc.quant_circ, two_pi = sc.two_pi, theta0 = sc.tree_theta;
   const bool corr = sc.tree_extra_correction;
   int node = start;
+  int left = tb.ctr[0];  // a walk of a well-formed tree visits each node at most once
   while (node != kEnd) {
+    if (--left < 0) {
+      overrun = true;
+      break;
+    }
     const double4 A = ldg4(&tb.nA[node]);
     const int4 I = __ldg(&tb.nI[node]);
     if (I.x == 0) {
@@ -1070,12 +1081,17 @@ __device__ void fp64_epilogue(const SysConst &sc, const SysDyn &dy, int g, const
 // root adds nothing either).
 __device__ void walk_mirror(const TreeBuffers &tb, int root, const SysConst &sc, const double xi[3], int g, int pi_,
                             int pin_g, const int *__restrict__ prv, double acc[3], unsigned long long &evals,
-                            unsigned long long &tests, bool &singular) {
+                            unsigned long long &tests, bool &singular, bool &overrun) {
   const double qc = sc.quant_circ, two_pi = sc.two_pi, theta0 = sc.tree_theta;
   for (int m = 0; m < sc.n_mirror; ++m) {
     const bool own = mirror_skips_own(sc, pin_g, m);
     int node = root;
+    int left = tb.ctr[0];
     while (node != kEnd) {
+      if (--left < 0) {
+        overrun = true;
+        break;
+      }
       const double4 A = ldg4(&tb.nA[node]);
       const int4 I = __ldg(&tb.nI[node]);
       if (I.x == 0) {
@@ -1135,14 +1151,15 @@ __global__ void k_tree_walk_mirror(const SysConst *__restrict__ scs, SysDyn *dyn
   const int g = w.y + threadIdx.x;
   const int k = g - sc.base;
   unsigned long long evals = 0, tests = 0;
-  bool singular = false;
+  bool singular = false, overrun = false;
   if (!*err && k >= 1 && k <= dyn[w.x].pcount && k <= sc.cap && nxt[g] != 0) {
     double xi[3], acc[3] = {0, 0, 0};
     load3(X, T, g, xi);
-    walk_mirror(tb, w.x, sc, xi, g, prv[g], sc.pin[g], prv, acc, evals, tests, singular);
+    walk_mirror(tb, w.x, sc, xi, g, prv[g], sc.pin[g], prv, acc, evals, tests, singular, overrun);
     for (int c = 0; c < 3; ++c) sc.umir[c * T + g] = acc[c];
   }
   if (singular) atomicOr(err, DERR_SINGULAR);
+  if (overrun) atomicOr(err, DERR_WALK);
   if (evals) atomicAdd(&dyn[w.x].tree_eval, evals);
   if (tests) atomicAdd(&dyn[w.x].tree_tests, tests);
 }
@@ -1178,14 +1195,15 @@ __device__ bool fp64_target(const SysConst &sc, const SysDyn &dy, int sys, int g
   }
   if (part != 2) tests += t0;  // the root tests are counted once
   const int pi_ = prv[g];
-  bool singular = false;
+  bool singular = false, overrun = false;
 #pragma unroll
   for (int c = 0; c < 3; ++c) ub0[c] = ubs[c] = 0.;
-  if (part != 2) walk_fp64(tb, start[0], sc, xi, g, pi_, prv, zero, true, ub0, evals, tests, singular);
+  if (part != 2) walk_fp64(tb, start[0], sc, xi, g, pi_, prv, zero, true, ub0, evals, tests, singular, overrun);
   if (part != 1)
     for (int m = 0; m < sc.n_shift; ++m)
-      walk_fp64(tb, start[m + 1], sc, xi, g, pi_, prv, sc.shift[m], false, ubs, evals, tests, singular);
+      walk_fp64(tb, start[m + 1], sc, xi, g, pi_, prv, sc.shift[m], false, ubs, evals, tests, singular, overrun);
   if (singular) atomicOr(err, DERR_SINGULAR);
+  if (overrun) atomicOr(err, DERR_WALK);
   if (part == 0) fp64_epilogue(sc, dy, g, X, GI, GB, U, T, ub0, ubs);
   return true;
 }
@@ -1211,7 +1229,7 @@ __global__ void __launch_bounds__(128) k_tree_walk_fp64(const SysConst *__restri
   unsigned long long evals = 0, tests = 0;
   double ub0[3] = {0, 0, 0}, ubs[3] = {0, 0, 0};
   bool done = false;
-  if (!*err && k >= 1 && k <= dyn[w.x].pcount && nxt[g] != 0)
+  if (!*err && k >= 1 && k <= dyn[w.x].pcount && nxt[g] != 0 && q >= sc.walk_lo && q < sc.walk_hi)
     done = fp64_target(sc, dyn[w.x], w.x, g, X, GI, GB, prv, U, T, tb, true, part, ub0, ubs, evals, tests, err);
   if (part == 1)
     for (int c = 0; c < 3; ++c) s_ub0[c][t] = ub0[c];
@@ -1250,10 +1268,11 @@ __global__ void k_walk_fixup(const SysConst *__restrict__ scs, SysDyn *dyn, cons
       double xi[3], acc[3] = {0, 0, 0};
       const double zero[3] = {0, 0, 0};
       load3(X, T, g, xi);
-      bool singular = false;
+      bool singular = false, overrun = false;
       walk_fp64(tb, s, sc, xi, g, prv[g], prv, m == 0 ? zero : sc.shift[m - 1], m == 0, acc, evals, tests,
-                singular);
+                singular, overrun);
       if (singular) atomicOr(err, DERR_SINGULAR);
+      if (overrun) atomicOr(err, DERR_WALK);
       const long long o = (long long)m * 3 * T + g;
       partial[o] = acc[0];
       partial[o + T] = acc[1];
@@ -1326,7 +1345,8 @@ __device__ double closest_bound(const TreeBuffers &tb, const SysConst &sc, int r
   // the walk below `deep` (opened: it holds the target), with the reference's opening test
   const int4 Id = __ldg(&tb.nI[deep]);
   if (Id.x <= 1) return best;
-  for (int n = Id.y; n != kEnd && n != Id.z;) {
+  int left = tb.ctr[0];  // (a malformed tree only loosens the bound; the main walk reports it)
+  for (int n = Id.y; n != kEnd && n != Id.z && --left >= 0;) {
     const int4 I = __ldg(&tb.nI[n]);
     if (I.x == 0) {
       n = I.z;
@@ -1352,7 +1372,7 @@ template <bool kPrefetch>
 __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *__restrict__ dyn,
                                const int *__restrict__ sys_of, const double *__restrict__ X,
                                const int *__restrict__ nxt, const int *__restrict__ prv, int *__restrict__ cl,
-                               double *__restrict__ CD, long long T, TreeBuffers tb, const unsigned *err) {
+                               double *__restrict__ CD, long long T, TreeBuffers tb, unsigned *err) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= T || *err) return;
   const long long g = tb.perm[t];  // the walk order: neighbouring threads, neighbouring targets
@@ -1388,7 +1408,12 @@ __global__ void k_closest_tree(const SysConst *__restrict__ scs, const SysDyn *_
   int node = s;
   double4 A = ldg4(&tb.nA[node]);
   int4 I = __ldg(&tb.nI[node]);
+  int left = tb.ctr[0];  // a walk of a well-formed tree visits each node at most once
   for (;;) {
+    if (--left < 0) {
+      atomicOr(err, DERR_WALK);
+      break;
+    }
     // kPrefetch (few targets, latency-bound): the records of both possible successors (next
     // in preorder past the subtree, first child) are requested before this node is decided,
     // so their loads overlap the test; with a full GPU the extra loads cost more than that
@@ -1533,7 +1558,10 @@ __global__ void __launch_bounds__(128, kSplit ? 8 : 9) k_tree_walk_mixed(const S
   const int g = q >= 1 && q <= sc.cap ? tb.perm[sc.base + q] : sc.base;
   const int k = g - sc.base;
   unsigned evals = 0, tests = 0, n64 = 0, nband = 0;
-  const bool valid = !*err && k >= 1 && k <= dyn[w.x].pcount && nxt[g] != 0;
+  // A walk range's ends fall on warp boundaries (nv_set_walk_range): a warp walks all its
+  // targets or none, and the warp's visits (the union of its lanes' walks), which set where
+  // the FP32 partials are flushed, are the same as without a range.
+  const bool valid = !*err && k >= 1 && k <= dyn[w.x].pcount && nxt[g] != 0 && q >= sc.walk_lo && q < sc.walk_hi;
   const unsigned live = __ballot_sync(0xffffffffu, valid);
   float xh[3] = {0, 0, 0}, xl[3] = {0, 0, 0};  // target - shift, FP32 high and low parts
   int pi_ = 0;
@@ -1636,7 +1664,12 @@ __global__ void __launch_bounds__(128, kSplit ? 8 : 9) k_tree_walk_mixed(const S
   int cur = start;
   unsigned mask = open0;
   bool more = open0 && start != kEnd;
+  int left = tb.ctr[0];  // the warp visits each node of a well-formed tree at most once
   while (more) {
+    if (--left < 0) {
+      if (lane == 0) atomicOr(err, DERR_WALK);
+      break;
+    }
     const WalkNode *wn = tb.mx.W + cur;
     // the whole 64-byte record at once: one load latency per node instead of a chain
     const int4 D = __ldg(&wn->d);
@@ -1785,6 +1818,8 @@ int n_sms() {
 }  // namespace
 
 int n_sms_host() { return n_sms(); }
+const int *tree_iperm(nv_handle *h) { return h->tree ? h->tree->iperm : nullptr; }
+const int *tree_perm(nv_handle *h) { return h->tree ? h->tree->perm : nullptr; }
 
 void tree_alloc(nv_handle *h) {
   bool need = false;
@@ -1850,6 +1885,7 @@ void tree_alloc(nv_handle *h) {
     cudaMalloc(&tb->oval[b], (size_t)T * sizeof(int));
   }
   tb->perm = tb->oval[1];
+  cudaMalloc(&tb->iperm, (size_t)T * sizeof(int));
   k_iota<<<grid_for(T, TB), TB, 0, h->stream>>>(tb->perm, T);  // a permutation before the first build
   int sb = 1;
   while ((1LL << sb) < h->nsys) ++sb;
@@ -1866,7 +1902,7 @@ void tree_free(nv_handle *h) {
   void *ptrs[] = {tb->nA, tb->nB, tb->nP, tb->nI, tb->nR, tb->nDepth, tb->nLeaf, tb->nSib, tb->members, tb->bigl, tb->root_apx, tb->root_part, tb->defer, tb->defer_n,
                   tb->rkey[0], tb->rkey[1], tb->rval[0], tb->rval[1], tb->root_cnt, tb->root_mb, tb->rsort_tmp, tb->ctr,
                   tb->flag, tb->pos, tb->cub_tmp, tb->mx.C, tb->mx.W, tb->mx.G, tb->okey[0], tb->okey[1],
-                  tb->oval[0], tb->oval[1], tb->sort_tmp, tb->split_blk[0], tb->split_blk[1],
+                  tb->oval[0], tb->oval[1], tb->iperm, tb->sort_tmp, tb->split_blk[0], tb->split_blk[1],
                   tb->split_blk[2], tb->split_wrp[0], tb->split_wrp[1], tb->split_wrp[2]};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1896,6 +1932,7 @@ void launch_tree_build(nv_handle *h) {
     cub::DeviceRadixSort::SortPairs(tb->sort_tmp, sb, tb->okey[0], tb->okey[1], tb->oval[0], tb->oval[1], (int)T, 0,
                                     tb->key_bits, h->side);
   }
+  k_inv_perm<<<grid_for(T, TB), TB, 0, h->side>>>(tb->perm, tb->iperm, T);
   cudaEventRecord(h->sort_ev, h->side);
   k_root_sums<<<h->nsys, kSumThreads, kSumSmem, h->side>>>(h->x, T, *tb, h->nsys, h->nxt, h->d_err);
   cudaEventRecord(h->join_ev, h->side);

@@ -1,7 +1,13 @@
-"""Multi-GPU helpers: independent systems shard across ranks with no data-path collective.
+"""Multi-GPU helpers.  One process per GPU (torchrun).
 
-One process per GPU (torchrun).  The only collectives are for measurement and bookkeeping:
-a barrier around timed regions and the reductions of per-rank timings (max) and work (sum).
+* Independent systems shard across ranks (`shard_systems`) with no data-path collective;
+  the only collectives are a barrier around timed regions and the reductions of per-rank
+  timings (max) and work (sum).
+* One tangle splits its velocity pass over the ranks (`TangleSplit`): every rank keeps the
+  whole state and builds the same tree; each computes the targets of its range of the walk
+  order, the ranges' velocities are all-gathered, and every rank finishes the step (AB3
+  update and topology) on the full field, so that all ranks hold the one-GPU state, bit for
+  bit, after every step.
 """
 from __future__ import annotations
 
@@ -30,3 +36,66 @@ def reduce_max_sum(dist, device, maxes: Sequence[float], sums: Sequence[float]):
         dist.all_reduce(mx, op=dist.ReduceOp.MAX)
         dist.all_reduce(sm, op=dist.ReduceOp.SUM)
     return [float(v) for v in mx], [float(v) for v in sm]
+
+
+WARP = 32  # walk positions per warp of the tree walks
+
+
+def split_ranges(live: int, world: int) -> List[tuple]:
+    """Walk-position ranges [lo, hi) of the ranks: positions 1 .. live (the live points in the
+    walk order) in near-equal contiguous parts of whole warps (every end but live + 1 at
+    1 + a multiple of 32), so that no warp of the mixed walk is cut in two."""
+    warps = -(-live // WARP)
+    out = []
+    for r in range(world):
+        lo = min(1 + (r * warps) // world * WARP, live + 1)
+        hi = min(1 + ((r + 1) * warps) // world * WARP, live + 1)
+        out.append((lo, hi))
+    return out
+
+
+def walk_range(lo: int, hi: int, cap: int) -> tuple:
+    """The nv_set_walk_range arguments for positions [lo, hi) of split_ranges: an end at
+    live + 1 off a warp boundary becomes cap + 1 (the positions past live hold no target),
+    and an empty range (1, 1)."""
+    if hi <= lo:
+        return 1, 1
+    return lo, hi if (hi - 1) % WARP == 0 else cap + 1
+
+
+class TangleSplit:
+    """A step of one tangle (system `sys` of `handle`) with its velocity pass split over the
+    ranks of `dist` (torch.distributed, initialised; NCCL with CUDA tensors or gloo with CPU
+    ones).  `device` is where the exchange buffers live ("cuda" for the library's own
+    velocities, which nv_velocity_pack/unpack read and write in device memory)."""
+
+    def __init__(self, handle, sys: int, dist, device: str = "cuda"):
+        self.h = handle
+        self.sys = sys
+        self.dist = dist
+        self.rank = dist.get_rank()
+        self.world = dist.get_world_size()
+        self.device = device
+
+    def step(self):
+        import torch
+        live = int(self.h.counters(self.sys).live)  # the same on every rank
+        ranges = split_ranges(live, self.world)
+        lo, hi = ranges[self.rank]
+        self.h.set_walk_range(self.sys, *walk_range(lo, hi, self.h.capacity[self.sys]))
+        self.h.step_velocity()
+        width = max(b - a for a, b in ranges)
+        # uninitialised: the rows past hi - lo are sent but never read, and no fill kernel on
+        # torch's stream races the library's pack on its own stream
+        mine = torch.empty((max(width, 1), 3), dtype=torch.float64, device=self.device)
+        self.h.velocity_pack(self.sys, lo, hi - lo, mine.data_ptr())
+        parts = [torch.empty_like(mine) for _ in range(self.world)]
+        if self.device != "cpu":
+            torch.cuda.synchronize()
+        self.dist.all_gather(parts, mine)
+        if self.device != "cpu":
+            torch.cuda.synchronize()
+        for r, (a, b) in enumerate(ranges):
+            if r != self.rank and b > a:
+                self.h.velocity_unpack(self.sys, a, b - a, parts[r].data_ptr())
+        self.h.step_finish()
