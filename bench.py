@@ -28,7 +28,10 @@ on a seeded subsample of points, and whether their topology event logs agree.
 Multi-GPU (torchrun, one rank per GPU): an ensemble's systems are split across the ranks by
 a greedy balance of sum N^2 (nuvort_b200.dist.shard_systems), the same ensemble whatever the
 rank count (strong scaling, no collective on the data path); a single-tangle workload runs one
-replica per rank (seed + rank, weak scaling).
+replica per rank (seed + rank, weak scaling), or, with --split-tangle, one tangle over all the
+ranks: each computes the velocities of its range of the walk order, the ranges are
+all-gathered (NCCL) and every rank finishes the step on the full field (strong scaling; the
+line checks that the ranks agree and that rank 0's state equals an unsplit run's).
 
 --impl reference times the CPU oracle -- the line-by-line C++ restatement of the reference
 Fortran (the Fortran itself cannot be built here: no Fortran compiler) -- on all host
@@ -548,6 +551,93 @@ def run_ours(args):
     return 0
 
 
+def run_split_tangle(args):
+    """One tangle on every rank, its velocity pass split over the ranks (TangleSplit: walk
+    ranges of whole warps, an all-gather of the velocities, every rank finishing the step on
+    the full field).  Strong scaling: the job advances one tangle whatever N.  Each timed
+    step is bracketed by events on torch's stream with the device idle on both sides (the
+    library's calls return with their stream drained), so a step's time covers the ranks'
+    launches, the exchange and the host calls between them; max over ranks.  At the end the
+    ranks' states are compared (a digest of every rank's positions and links), and rank 0
+    runs the same steps unsplit (nv_step) and compares bit for bit."""
+    import datetime
+    import hashlib
+
+    import torch
+    import torch.distributed as dist
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180), device_id=dev)
+    else:  # a one-rank group: the same code path, the exchange a copy
+        import socket
+        with socket.socket() as s:
+            s.bind(("127.0.0.1", 0))
+            port = s.getsockname()[1]
+        dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                                timeout=datetime.timedelta(seconds=180), device_id=dev)
+    from nuvort_b200 import api
+    from nuvort_b200.dist import TangleSplit, reduce_max_sum
+    params, states, cfg = workload(args.workload, 0)  # the same tangle (seed) on every rank
+    caps = [int(s.pcount * 1.6) + 256 for s in states]
+    hp = with_precision(params, args.precision)
+    h = api.Handle(hp, caps, device=local, states=states)
+    ts = TangleSplit(h, 0, dist, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        ts.step()
+    dist.barrier()
+    torch.cuda.synchronize()
+    per_step, pts = [], 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            pts += int(h.counters(0).live)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ts.step()
+            torch.cuda.synchronize()
+            e1.record()
+            e1.synchronize()
+            per_step.append(e0.elapsed_time(e1))
+    dist.barrier()
+    st = h.download(0)
+    dig = hashlib.sha256(st.x.tobytes() + st.infront.tobytes() + st.behind.tobytes()).digest()
+    d = torch.tensor(list(dig[:8]), dtype=torch.float64, device="cuda")
+    (step_ms,), _ = reduce_max_sum(dist, "cuda", [sum(per_step)], [float(pts)])
+    dmax, dsum = reduce_max_sum(dist, "cuda", list(d.tolist()), list(d.tolist()))
+    identical = all(abs(a * world - b) < 0.5 for a, b in zip(dmax, dsum))  # every rank's digest equal
+    launches = h.step_launches() + 1 + (world - 1)  # the step's kernels, the pack, the unpacks
+    h.close()
+    out = None
+    if rank == 0:
+        ref = api.Handle(hp, caps, device=local, states=states)
+        ref.step(args.warmup + args.steps)
+        sr = ref.download(0)
+        ref.close()
+        one_gpu = bool(np.array_equal(sr.x, st.x) and np.array_equal(sr.infront, st.infront)
+                       and np.array_equal(sr.behind, st.behind))
+        out = {"metric": METRIC, "value": pts / (step_ms * 1e-3), "unit": UNIT, "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms / args.steps,
+               "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+               "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+               "config": dict(cfg, workload=cfg["workload"].replace("seed 3+rank", "seed 3").replace(
+                   "seed 1+rank", "seed 1"), precision=args.precision,
+                   split=(f"one tangle on {world} rank(s): walk ranges of whole warps, all-gather of the "
+                          "velocities, every rank finishing the step"),
+                   l2="256 MiB buffer written between timed steps"),
+               "impl": "ours", "clocks": clk.summary(), "gpu_launches": launches * args.steps,
+               "ranks_identical": identical, "matches_one_gpu": one_gpu,
+               "per_step_ms": [round(x, 4) for x in per_step]}
+    dist.barrier()
+    dist.destroy_process_group()
+    if out:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -567,10 +657,17 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--split-tangle", action="store_true",
+                    help="tangle workloads: one tangle over all ranks, its velocity pass split by walk ranges "
+                         "(default: one replica per rank)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.split_tangle:
+        if args.workload not in ("tangle32k", "tangle1m"):
+            ap.error("--split-tangle takes a tangle workload (tangle32k, tangle1m)")
+        return run_split_tangle(args)
     return run_ours(args)
 
 
