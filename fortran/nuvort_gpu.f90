@@ -250,6 +250,31 @@ module nuvort_gpu
       import :: c_int, c_ptr
       type(c_ptr), value :: p
     end function
+    !> one tangle over several GPUs: the step's two halves, the walk range of this rank and the
+    !> exchange of velocities by walk position (device buffers, e.g. for an MPI/NCCL all-gather)
+    integer(c_int) function nv_step_velocity(h) bind(c, name='nv_step_velocity')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function nv_step_finish(h) bind(c, name='nv_step_finish')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function nv_set_walk_range(h, sys, lo, hi) bind(c, name='nv_set_walk_range')
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: sys, lo, hi
+    end function
+    integer(c_int) function nv_velocity_pack(h, sys, lo, count, d_buf) bind(c, name='nv_velocity_pack')
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: h, d_buf
+      integer(c_int32_t), value :: sys, lo, count
+    end function
+    integer(c_int) function nv_velocity_unpack(h, sys, lo, count, d_buf) bind(c, name='nv_velocity_unpack')
+      import :: c_int, c_int32_t, c_ptr
+      type(c_ptr), value :: h, d_buf
+      integer(c_int32_t), value :: sys, lo, count
+    end function
     type(c_ptr) function nv_last_error() bind(c, name='nv_last_error')
       import :: c_ptr
     end function
