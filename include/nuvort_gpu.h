@@ -360,10 +360,10 @@ int nv_measure_fp32_peak(int32_t device, double *tflops);
  *   t        simulation time (mutual friction cut-offs)
  *   d_u3     device [3*pcount] output velocities (0 for empty slots)
  *   stream   a cudaStream_t (NULL = the default stream); the call waits for it to finish
- * The first call on a device (and the first after a device reset, which creates a new
- * context) looks up the array's device address with cudaGetSymbolAddress; make that first
- * call before any stream capture begins.  Each call waits for `stream` to finish its work and
- * then reads the device error word back to the host before it returns.  A call that fails
+ * Each call looks up the array's device address in the current context (so a device reset
+ * between calls is safe), waits for `stream` to finish its work and then reads the device
+ * error word back to the host before it returns; none of that is allowed while a stream is
+ * being captured, so no call may be made during a stream capture.  A call that fails
  * (NV_ERR_ARG for links outside 0..pcount or infront/behind disagreeing on an empty slot,
  * NV_ERR_TIMEOUT for a device wait that gave up) leaves d_u3 unwritten.  Every call uses the
  * same array and leaves its contents behind; calls whose work overlaps on the GPU (two host
