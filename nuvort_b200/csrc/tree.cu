@@ -29,7 +29,7 @@ constexpr int kBigNode = 2048;  // nodes with more members are split by a whole 
 constexpr int kBlockSumNode = 8192;  // nodes with more members are summed by a whole block
 constexpr int kCtrBig = kMaxLevels + 6;  // ctr[kCtrBig]: entries of the block-summed node list
 constexpr int kCtrBigSnap = kMaxLevels + 7;  // entries listed when the early block sums start
-constexpr int kSnapLevel = 4;  // after this level's split the early block sums start
+constexpr int kSnapLevel = 1;  // the early block sums: the big nodes of depth 1, listed by the root's split
 // ctr[kCtrSplit + b]: entries of the level lists of nodes to split, by level % 3 = b:
 // [+0..+2] nodes above kBigNode members (split by a block), [+3..+5] the others with >= 2
 constexpr int kCtrSplit = kMaxLevels + 8;
@@ -410,30 +410,65 @@ __global__ void k_root_scatter(TreeBuffers tb, const int *__restrict__ pos, long
 }
 
 // Split node p (at most kBigNode members) with one warp: count the members per octant, make
-// the children, then write each member to its child's list in member order (stable).
+// the children, then write each member to its child's list in member order (stable).  Each
+// lane takes kUnroll members per pass (k0 + 32 u + lane), their loads in flight together.
+constexpr int kUnroll = 4;
+constexpr int kSplitThreads = 512;
+
+// Octants (8: outside every child, or past `end`) and slots of members k0 + 32 u + lane of
+// the list mem[0 .. end).
+__device__ __forceinline__ void octants_of(const double *__restrict__ X, long long T, const int *mem, int k0, int end,
+                                           int lane, const double4 &P, double h, int d[kUnroll], int slot[kUnroll]) {
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u) {
+    const int k = k0 + 32 * u + lane;
+    slot[u] = k < end ? mem[k] : -1;
+  }
+  double x[kUnroll][3];
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u)
+    if (slot[u] >= 0) load_x(X, T, slot[u], x[u]);
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u) d[u] = slot[u] >= 0 ? octant(x[u], P, h) : 8;
+}
+
+// Members k0 .. of a pass ranked in member order: the stable position of each in its child's
+// list (base_off + run + the lanes before it with the same octant), -1 for none.
+__device__ __forceinline__ void rank_and_write(TreeBuffers &tb, int mb0, const int base_off[8], int run[8],
+                                               const int d[kUnroll], const int slot[kUnroll], int lane) {
+  const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u) {
+    int mypos = -1;
+#pragma unroll
+    for (int dd = 0; dd < 8; ++dd) {
+      const unsigned b = __ballot_sync(0xffffffffu, d[u] == dd);
+      if (d[u] == dd) mypos = mb0 + base_off[dd] + run[dd] + __popc(b & lt);
+      run[dd] += __popc(b);
+    }
+    if (mypos >= 0) tb.members[mypos] = slot[u];
+  }
+}
+
 // Node p's member count per octant (the warp's lanes over its member list).
 __device__ void warp_count(const double *__restrict__ X, long long T, const TreeBuffers &tb, int p, int lane,
                            int cnt[8]) {
   const int2 R = tb.nR[p];
   const double4 P = tb.nP[p];
   const double h = tb.nA[p].w / 2.0;
-  for (int k0 = 0; k0 < R.y; k0 += 32) {
-    const int k = k0 + lane;
-    int d = 8;
-    if (k < R.y) {
-      double x[3];
-      load_x(X, T, tb.members[R.x + k], x);
-      d = octant(x, P, h);
-    }
+  for (int k0 = 0; k0 < R.y; k0 += 32 * kUnroll) {
+    int d[kUnroll], slot[kUnroll];
+    octants_of(X, T, tb.members + R.x, k0, R.y, lane, P, h, d, slot);
 #pragma unroll
-    for (int dd = 0; dd < 8; ++dd) cnt[dd] += __popc(__ballot_sync(0xffffffffu, d == dd));
+    for (int u = 0; u < kUnroll; ++u)
+#pragma unroll
+      for (int dd = 0; dd < 8; ++dd) cnt[dd] += __popc(__ballot_sync(0xffffffffu, d[u] == dd));
   }
 }
 
 // Node p's members into its children's lists (stable: slot order kept), from member slot mb0.
 __device__ void warp_scatter(const double *__restrict__ X, long long T, TreeBuffers &tb, int p, int lane,
                              const int cnt[8], int mb0) {
-  const unsigned lt = (1u << lane) - 1u;
   const int2 R = tb.nR[p];
   const double4 P = tb.nP[p];
   const double h = tb.nA[p].w / 2.0;
@@ -447,23 +482,100 @@ __device__ void warp_scatter(const double *__restrict__ X, long long T, TreeBuff
       run[dd] = 0;
     }
   }
-  for (int k0 = 0; k0 < R.y; k0 += 32) {
-    const int k = k0 + lane;
-    int d = 8, slot = 0;
-    if (k < R.y) {
-      double x[3];
-      slot = tb.members[R.x + k];
-      load_x(X, T, slot, x);
-      d = octant(x, P, h);
-    }
-    int mypos = -1;
+  for (int k0 = 0; k0 < R.y; k0 += 32 * kUnroll) {
+    int d[kUnroll], slot[kUnroll];
+    octants_of(X, T, tb.members + R.x, k0, R.y, lane, P, h, d, slot);
+    rank_and_write(tb, mb0, base_off, run, d, slot, lane);
+  }
+}
+
+// The counters a split reserves from, for children at list level lb.
+__device__ __forceinline__ int *split_ctr(TreeBuffers &tb, int c, int lb) {
+  return c == 0 ? &tb.ctr[0]
+       : c == 1 ? &tb.ctr[1]
+       : c == 2 ? &tb.ctr[kCtrSplit + lb]
+       : c == 3 ? &tb.ctr[kCtrSplit + 3 + lb]
+                : &tb.ctr[kCtrBig];
+}
+
+// Node p split by the whole warp: count, lane 0 reserves and writes the children, scatter.
+__device__ void warp_split_one(const double *__restrict__ X, long long T, TreeBuffers &tb, int p, int lane, int lb,
+                               unsigned *err) {
+  int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  warp_count(X, T, tb, p, lane, cnt);
+  const SplitNeeds nd = split_needs(cnt);
+  int mb0 = -1;
+  if (lane == 0 && nd.nchild > 0) {
+    const int v[5] = {nd.nchild, nd.kept, nd.nblk, nd.nwrp, nd.nbig};
+    int base[5];
 #pragma unroll
-    for (int dd = 0; dd < 8; ++dd) {
-      const unsigned b = __ballot_sync(0xffffffffu, d == dd);
-      if (d == dd) mypos = mb0 + base_off[dd] + run[dd] + __popc(b & lt);
-      run[dd] += __popc(b);
+    for (int c = 0; c < 5; ++c) base[c] = v[c] ? atomicAdd(split_ctr(tb, c, lb), v[c]) : 0;
+    if (write_children(tb, p, cnt, nd, base[0], base[1], base[2], base[3], base[4], err)) mb0 = base[1];
+  }
+  mb0 = __shfl_sync(0xffffffffu, mb0, 0);
+  if (mb0 >= 0) warp_scatter(X, T, tb, p, lane, cnt, mb0);
+}
+
+// Nodes with at most kLaneNode members, when a level lists many (the deep levels), are split
+// by one lane each: the lane counts its node's members per octant (digits kept, 4 bits a
+// member), the warp makes one reservation per counter for its lanes' nodes, and each lane
+// writes its children and scatters its members in member order.
+constexpr int kLaneNode = 16;
+
+__device__ void lane_split(const double *__restrict__ X, long long T, TreeBuffers &tb, int p, int2 R, int lane,
+                           int lb, unsigned *err) {
+  const bool mine = p >= 0;
+  int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long digs = 0;
+  if (mine) {
+    const double4 P = tb.nP[p];
+    const double h = tb.nA[p].w / 2.0;
+    unsigned long long cp = 0;  // eight counts of 5 bits
+    for (int k = 0; k < R.y; ++k) {
+      double x[3];
+      load_x(X, T, tb.members[R.x + k], x);
+      const int d = octant(x, P, h);
+      digs |= (unsigned long long)d << (4 * k);
+      if (d < 8) cp += 1ull << (5 * d);
     }
-    if (mypos >= 0) tb.members[mypos] = slot;
+#pragma unroll
+    for (int dd = 0; dd < 8; ++dd) cnt[dd] = (int)((cp >> (5 * dd)) & 31u);
+  }
+  const SplitNeeds nd = mine ? split_needs(cnt) : SplitNeeds{0, 0, 0, 0, 0};
+  const int v[5] = {nd.nchild, nd.kept, nd.nblk, nd.nwrp, nd.nbig};
+  int off[5], base[5];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) {  // exclusive prefix over the lanes, the total in lane 31
+    int x = v[c];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    off[c] = x - v[c];
+    base[c] = 0;
+    if (lane == 31 && x) base[c] = atomicAdd(split_ctr(tb, c, lb), x);
+    base[c] = __shfl_sync(0xffffffffu, base[c], 31);
+  }
+  if (!mine || nd.nchild == 0) return;
+  const int mb0 = base[1] + off[1];
+  if (!write_children(tb, p, cnt, nd, base[0] + off[0], mb0, base[2] + off[2], base[3] + off[3], base[4] + off[4],
+                      err))
+    return;
+  unsigned long long op = 0, run = 0;  // children's list offsets and fill, 5 bits each
+  int o = 0;
+#pragma unroll
+  for (int dd = 0; dd < 8; ++dd) {
+    op |= (unsigned long long)o << (5 * dd);
+    o += cnt[dd];
+  }
+  for (int k = 0; k < R.y; ++k) {
+    const int d = (int)((digs >> (4 * k)) & 15u);
+    if (d < 8) {
+      const int at = (int)(((op >> (5 * d)) & 31u) + ((run >> (5 * d)) & 31u));
+      run += 1ull << (5 * d);
+      tb.members[mb0 + at] = tb.members[R.x + k];
+    }
   }
 }
 
@@ -475,23 +587,19 @@ __device__ void split_node_block(const double *__restrict__ X, long long T, Tree
   __shared__ int wcnt[32][8];
   __shared__ int s_id0, s_mb0, s_cnt[8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const unsigned lt = (1u << lane) - 1u;
   const int2 R = tb.nR[p];
   const double4 P = tb.nP[p];
   const double h = tb.nA[p].w / 2.0;
   const int per = (R.y + nw - 1) / nw;
   const int s0 = w * per, s1 = min(R.y, s0 + per);
   int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  for (int k0 = s0; k0 < s1; k0 += 32) {
-    const int k = k0 + lane;
-    int d = 8;
-    if (k < s1) {
-      double x[3];
-      load_x(X, T, tb.members[R.x + k], x);
-      d = octant(x, P, h);
-    }
+  for (int k0 = s0; k0 < s1; k0 += 32 * kUnroll) {
+    int d[kUnroll], slot[kUnroll];
+    octants_of(X, T, tb.members + R.x, k0, s1, lane, P, h, d, slot);
 #pragma unroll
-    for (int dd = 0; dd < 8; ++dd) cnt[dd] += __popc(__ballot_sync(0xffffffffu, d == dd));
+    for (int u = 0; u < kUnroll; ++u)
+#pragma unroll
+      for (int dd = 0; dd < 8; ++dd) cnt[dd] += __popc(__ballot_sync(0xffffffffu, d[u] == dd));
   }
   if (lane == 0)
 #pragma unroll
@@ -526,31 +634,19 @@ __device__ void split_node_block(const double *__restrict__ X, long long T, Tree
       off += s_cnt[dd];
       run[dd] = 0;
     }
-    for (int k0 = s0; k0 < s1; k0 += 32) {
-      const int k = k0 + lane;
-      int d = 8, slot = 0;
-      if (k < s1) {
-        double x[3];
-        slot = tb.members[R.x + k];
-        load_x(X, T, slot, x);
-        d = octant(x, P, h);
-      }
-      int mypos = -1;
-#pragma unroll
-      for (int dd = 0; dd < 8; ++dd) {
-        const unsigned b = __ballot_sync(0xffffffffu, d == dd);
-        if (d == dd) mypos = mb0 + base_off[dd] + run[dd] + __popc(b & lt);
-        run[dd] += __popc(b);
-      }
-      if (mypos >= 0) tb.members[mypos] = slot;
+    for (int k0 = s0; k0 < s1; k0 += 32 * kUnroll) {
+      int d[kUnroll], slot[kUnroll];
+      octants_of(X, T, tb.members + R.x, k0, s1, lane, P, h, d, slot);
+      rank_and_write(tb, mb0, base_off, run, d, slot, lane);
     }
   }
 }
 
 // One level of the build: the listed big nodes by blocks, then the other listed nodes by
-// warps.  The children's lists (level + 1) fill as nodes split; the list of level + 2 is
+// warps.  One block of kSplitThreads per SM, with registers for the loads of several
+// members (or nodes) per lane in flight at once.  The children's lists (level + 1) fill as nodes split; the list of level + 2 is
 // idle during this level (read at level - 1, filled at level + 1) and is emptied here.
-__global__ void __launch_bounds__(1024) k_split_level(const double *__restrict__ X, long long T, TreeBuffers tb,
+__global__ void __launch_bounds__(kSplitThreads, 1) k_split_level(const double *__restrict__ X, long long T, TreeBuffers tb,
                                                       int level, unsigned *err) {
   const int b = level % 3, b2 = (level + 2) % 3;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -567,69 +663,40 @@ __global__ void __launch_bounds__(1024) k_split_level(const double *__restrict__
     split_node_block(X, T, tb, p, err);
     __syncthreads();
   }
-  // Nodes split by a warp, kWarpNodes consecutive ones at a time: the warp counts each
-  // node's children, lane 0 reserves the ids, member slots and list entries of all of them
-  // with one atomic per counter (one per node contended on the few counters at the levels
-  // with most nodes), then the warp writes each node's children and scatters its members.
-  constexpr int kWarpNodes = 4;
-  __shared__ int s_cnt[32][kWarpNodes][8];  // per warp of the block: counts per octant
-  __shared__ int s_mb[32][kWarpNodes];      // and the member slot of each node's children (-1: none)
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  // The other listed nodes by warps.  Where they outnumber the warps twice over (the small,
+  // numerous nodes of the deep levels) a warp takes an equal share of them, up to 32: each
+  // lane splits its own when it has at most kLaneNode members, and the warp the larger ones
+  // one at a time; elsewhere a warp splits one node at a time.
+  const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const int nwl = min(tb.ctr[kCtrSplit + 3 + b], tb.max_wrp);
   const int lb = (level + 1) % 3;  // the children's level lists
-  // several nodes per warp only where nodes far outnumber warps (the small, numerous nodes of
-  // the deep levels); elsewhere one node per warp keeps every warp busy
-  const int kn = nwl >= 8 * nwarps ? kWarpNodes : 1;
-  for (int wq0 = warp * kn; wq0 < nwl; wq0 += nwarps * kn) {
-    int pj[kWarpNodes];
-#pragma unroll
-    for (int j = 0; j < kWarpNodes; ++j) {
-      pj[j] = j < kn && wq0 + j < nwl ? tb.split_wrp[b][wq0 + j] : -1;
-      if (pj[j] >= 0 && tb.nDepth[pj[j]] >= kMaxLevels) {
+  if (nwl >= 2 * nwarps) {
+    const int per = min(32, (nwl + nwarps - 1) / nwarps);  // nodes per warp: every warp busy
+    for (int wq0 = warp * per; wq0 < nwl; wq0 += nwarps * per) {
+      int p = lane < per && wq0 + lane < nwl ? tb.split_wrp[b][wq0 + lane] : -1;
+      if (p >= 0 && tb.nDepth[p] >= kMaxLevels) {
+        atomicOr(err, DERR_TREE_DEPTH);
+        p = -1;
+      }
+      const int2 R = p >= 0 ? tb.nR[p] : make_int2(0, 0);
+      const bool small = p >= 0 && R.y <= kLaneNode;
+      lane_split(X, T, tb, small ? p : -1, R, lane, lb, err);
+      for (unsigned big = __ballot_sync(0xffffffffu, p >= 0 && !small); big; big &= big - 1) {
+        const int pp = __shfl_sync(0xffffffffu, p, __ffs(big) - 1);
+        warp_split_one(X, T, tb, pp, lane, lb, err);
+      }
+    }
+  } else {
+    for (int wq = warp; wq < nwl; wq += nwarps) {
+      const int p = tb.split_wrp[b][wq];
+      if (tb.nDepth[p] >= kMaxLevels) {
         if (lane == 0) atomicOr(err, DERR_TREE_DEPTH);
-        pj[j] = -1;
+        continue;
       }
+      warp_split_one(X, T, tb, p, lane, lb, err);
     }
-    for (int j = 0; j < kn; ++j) {
-      int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      if (pj[j] >= 0) warp_count(X, T, tb, pj[j], lane, cnt);
-      if (lane < 8) s_cnt[wib][j][lane] = cnt[lane];
-    }
-    __syncwarp();
-    int off[kWarpNodes][5];
-    if (lane == 0) {
-      int tot[5] = {0, 0, 0, 0, 0};
-      for (int j = 0; j < kn; ++j) {
-        const SplitNeeds nd = split_needs(s_cnt[wib][j]);
-        const int v[5] = {nd.nchild, nd.kept, nd.nblk, nd.nwrp, nd.nbig};
-        for (int c = 0; c < 5; ++c) {
-          off[j][c] = tot[c];
-          tot[c] += v[c];
-        }
-      }
-      int *ctrs[5] = {&tb.ctr[0], &tb.ctr[1], &tb.ctr[kCtrSplit + lb], &tb.ctr[kCtrSplit + 3 + lb], &tb.ctr[kCtrBig]};
-      int base[5];
-      for (int c = 0; c < 5; ++c) base[c] = tot[c] ? atomicAdd(ctrs[c], tot[c]) : 0;
-      for (int j = 0; j < kn; ++j) {
-        int ok = 0;
-        const SplitNeeds nd = split_needs(s_cnt[wib][j]);
-        if (pj[j] >= 0 && nd.nchild > 0)
-          ok = write_children(tb, pj[j], s_cnt[wib][j], nd, base[0] + off[j][0], base[1] + off[j][1],
-                              base[2] + off[j][2], base[3] + off[j][3], base[4] + off[j][4], err);
-        s_mb[wib][j] = ok ? base[1] + off[j][1] : -1;
-      }
-    }
-    __syncwarp();
-    for (int j = 0; j < kn; ++j) {
-      const int mb0 = s_mb[wib][j];
-      if (pj[j] < 0 || mb0 < 0) continue;
-      int cnt[8];
-      for (int d = 0; d < 8; ++d) cnt[d] = s_cnt[wib][j][d];
-      warp_scatter(X, T, tb, pj[j], lane, cnt, mb0);
-    }
-    __syncwarp();
   }
 }
 
@@ -653,7 +720,12 @@ __device__ __forceinline__ void finish_node(TreeBuffers &tb, int id, bool root, 
   const double hw = w / 2.;
   const double geo = e_sqrt(e_add(e_add(e_sq(e_sub(cx, e_add(P.x, hw))), e_sq(e_sub(cy, e_add(P.y, hw)))),
                                    e_sq(e_sub(cz, e_add(P.z, hw)))));
-  tb.nA[id] = make_double4(cx, cy, cz, w);
+  // the centre only: the width (nA.w) is not written, since the split of this node may be
+  // reading it at the same time (the depth-1 nodes are summed beside the level-1 split)
+  double *a = reinterpret_cast<double *>(&tb.nA[id]);
+  a[0] = cx;
+  a[1] = cy;
+  a[2] = cz;
   tb.nB[id] = make_double4(qx, qy, qz, geo);
   if (!root) {
     const int first = R.y > 0 ? tb.members[R.x] : 0;
@@ -865,9 +937,9 @@ __global__ void __launch_bounds__(kSumThreads) k_node_sums_block(const double *_
                                                                   const double *__restrict__ GI,
                                                                   const int *__restrict__ nxt, long long T,
                                                                   TreeBuffers tb, int part, unsigned *err) {
-  // part 0: the nodes listed by the snapshot (split by then, so their member lists are
-  // final), summed beside the deeper levels' splits; part 1: the ones listed after it
-  // (only nodes at depth <= kSnapLevel: already split, so nothing else writes them)
+  // part 0: the big depth-1 nodes, listed by the roots' split (their member lists final),
+  // summed beside the level splits (which read their width and write their first child,
+  // fields the sums leave alone); part 1, after the levels: every other big node
   extern __shared__ double sm_dyn[];
   const int snap = tb.ctr[kCtrBigSnap];
   const int nbig = part == 0 ? snap : min(tb.ctr[kCtrBig], tb.max_big);
@@ -1945,16 +2017,15 @@ void launch_tree_build(nv_handle *h) {
   }
   k_root_children<<<grid_for(h->nsys, 64), 64, 0, h->stream>>>(*tb, h->nsys, h->d_err);
   k_root_scatter<<<grid_for(T, TB), TB, 0, h->stream>>>(*tb, tb->pos, T);
-  for (int L = 1; L < kMaxLevels; ++L) {
-    k_split_level<<<sms, 1024, 0, h->stream>>>(h->x, T, *tb, L, h->d_err);
-    if (L == kSnapLevel) {  // the large shallow nodes' sums overlap the deeper splits
-      k_big_snapshot<<<1, 32, 0, h->stream>>>(*tb);
-      cudaEventRecord(h->fork2_ev, h->stream);
-      cudaStreamWaitEvent(h->side2, h->fork2_ev, 0);
-      k_node_sums_block<<<sms, kSumThreads, kSumSmem, h->side2>>>(h->x, h->gi, h->nxt, T, *tb, 0, h->d_err);
-      cudaEventRecord(h->join2_ev, h->side2);
-    }
-  }
+  // the big depth-1 nodes' sums (the longest sequential chains after the roots') start as soon
+  // as the roots' split has listed them and written their member lists, beside the levels
+  k_big_snapshot<<<1, 32, 0, h->stream>>>(*tb);
+  cudaEventRecord(h->fork2_ev, h->stream);
+  cudaStreamWaitEvent(h->side2, h->fork2_ev, 0);
+  k_node_sums_block<<<sms, kSumThreads, kSumSmem, h->side2>>>(h->x, h->gi, h->nxt, T, *tb, 0, h->d_err);
+  cudaEventRecord(h->join2_ev, h->side2);
+  for (int L = 1; L < kMaxLevels; ++L)
+    k_split_level<<<sms, kSplitThreads, 0, h->stream>>>(h->x, T, *tb, L, h->d_err);
   k_node_sums_block<<<sms, kSumThreads, kSumSmem, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, 1, h->d_err);
   k_node_sums_big<<<sms * 8, 128, 0, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->nsys, h->d_err);
   k_node_sums_small<<<sms * 8, 128, 0, h->stream>>>(h->x, h->gi, h->nxt, T, *tb, h->nsys, h->d_err);
