@@ -801,28 +801,30 @@ __device__ __forceinline__ void warp_node_sums(const double *__restrict__ X, con
     __syncwarp();
     if (k0 + 32 < count) gather(k0 + 32);
     const int cnt = min(32, count - k0);
-    if (cnt == 32) {
-      if (lane < 3) {
-        double r[32];
-#pragma unroll
-        for (int l = 0; l < 32; ++l) r[l] = buf[lane][l];
-#pragma unroll
-        for (int l = 0; l < 32; ++l) acc = e_add(acc, r[l]);
-      } else if (lane < 6 && circ) {
+    // centre lanes 0-2: acc + x; circulation lanes 3-5: (acc + gi) - x.  With circulations
+    // the centre lanes subtract +0 (which returns its operand, -0 included), so that the six
+    // chains run as one instruction stream instead of two divergent ones in turn
+    const int ncomp = circ ? 6 : 3;
+    const bool sub = lane >= 3;
+    const double *a = buf[lane < 6 ? lane : 0], *bq = buf[sub && lane < 6 ? lane - 3 : 0];
+    if (lane < ncomp) {
+      if (!circ) {
+        for (int l = 0; l < cnt; ++l) acc = e_add(acc, a[l]);
+      } else if (cnt == 32) {
         double r[32], q[32];
 #pragma unroll
         for (int l = 0; l < 32; ++l) {
-          r[l] = buf[lane][l];
-          q[l] = buf[lane - 3][l];
+          r[l] = a[l];
+          const double x = bq[l];
+          q[l] = sub ? x : 0.0;
         }
 #pragma unroll
         for (int l = 0; l < 32; ++l) acc = e_sub(e_add(acc, r[l]), q[l]);
-      }
-    } else {
-      if (lane < 3) {
-        for (int l = 0; l < cnt; ++l) acc = e_add(acc, buf[lane][l]);
-      } else if (lane < 6 && circ) {
-        for (int l = 0; l < cnt; ++l) acc = e_sub(e_add(acc, buf[lane][l]), buf[lane - 3][l]);
+      } else {
+        for (int l = 0; l < cnt; ++l) {
+          const double x = bq[l];
+          acc = e_sub(e_add(acc, a[l]), sub ? x : 0.0);
+        }
       }
     }
   }
@@ -903,28 +905,40 @@ __device__ void block_node_sums(const double *__restrict__ X, const double *__re
       cp_async_wait_depth();     // tile t + 1 has landed
     } else if (lane < ncomp) {
       const double *slot = sm + (size_t)(t % kSumDepth) * 6 * kSumRow;
+      // as in warp_node_sums: with circulations the centre lanes subtract +0, one stream
+      const bool sub = lane >= 3;
       const double *a = slot + lane * kSumRow;
-      const double *b = slot + (lane >= 3 ? lane - 3 : lane) * kSumRow;
+      const double *b = slot + (sub ? lane - 3 : 0) * kSumRow;
       const int cnt = min(kSumTile, count - t * kSumTile);
-      if (cnt == kSumTile) {
+      if (!circ) {
+        if (cnt == kSumTile) {
+          for (int e0 = 0; e0 < kSumTile; e0 += 32) {
+            double r[32];
+#pragma unroll
+            for (int l = 0; l < 32; ++l) r[l] = a[e0 + l];
+#pragma unroll
+            for (int l = 0; l < 32; ++l) acc = e_add(acc, r[l]);
+          }
+        } else {
+          for (int l = 0; l < cnt; ++l) acc = e_add(acc, a[l]);
+        }
+      } else if (cnt == kSumTile) {
         for (int e0 = 0; e0 < kSumTile; e0 += 32) {
           double r[32], q[32];
 #pragma unroll
-          for (int l = 0; l < 32; ++l) r[l] = a[e0 + l];
-          if (lane < 3) {
-#pragma unroll
-            for (int l = 0; l < 32; ++l) acc = e_add(acc, r[l]);
-          } else {
-#pragma unroll
-            for (int l = 0; l < 32; ++l) q[l] = b[e0 + l];
-#pragma unroll
-            for (int l = 0; l < 32; ++l) acc = e_sub(e_add(acc, r[l]), q[l]);
+          for (int l = 0; l < 32; ++l) {
+            r[l] = a[e0 + l];
+            const double x = b[e0 + l];
+            q[l] = sub ? x : 0.0;
           }
+#pragma unroll
+          for (int l = 0; l < 32; ++l) acc = e_sub(e_add(acc, r[l]), q[l]);
         }
-      } else if (lane < 3) {
-        for (int l = 0; l < cnt; ++l) acc = e_add(acc, a[l]);
       } else {
-        for (int l = 0; l < cnt; ++l) acc = e_sub(e_add(acc, a[l]), b[l]);
+        for (int l = 0; l < cnt; ++l) {
+          const double x = b[l];
+          acc = e_sub(e_add(acc, a[l]), sub ? x : 0.0);
+        }
       }
     }
     __syncthreads();
