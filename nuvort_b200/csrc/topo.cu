@@ -1087,6 +1087,10 @@ __device__ int loop_count(const State &S, int particle, int pcount, const int (&
 // the shared-memory touched set after every event, for the candidates the sweep has not
 // reached yet); every other candidate's test fails in the serial sweep too.
 constexpr int kRound = 256;
+// precon's rounds are larger: its candidates are many (every close pair), its events few, and
+// a round's fixed cost (the prefetch's chain of dependent loads) is paid once per round
+constexpr int kReconRound = 512;
+constexpr int kReconWords = kReconRound / 32;
 constexpr int kExtraHeap = 1024;  // pending extra slots of the premove sweep held in shared memory
 constexpr int kRoundWords = kRound / 32;
 using RoundTouched = SlotSet<11, 1024>;
@@ -1141,15 +1145,15 @@ struct ReconRec {
   int i, yes, pari, j, parjb, nj, a1, a2, a3, b2;
 };
 
-__global__ void __launch_bounds__(kRound) k_recon_sweep(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys,
+__global__ void __launch_bounds__(kReconRound) k_recon_sweep(const SysConst *__restrict__ scs, SysDyn *dyn, int nsys,
                                                         State S, const int *__restrict__ pos_a,
                                                         const int *__restrict__ list_a, unsigned *err, DevEvent *ev,
                                                         int *ev_count, int ev_cap) {
   __shared__ int tkeys[RoundTouched::kCap];
   __shared__ int mkey[kMapCap], midx[kMapCap];
   __shared__ DevEvent ebuf[kEventStage];
-  __shared__ ReconRec rec[kRound];
-  __shared__ unsigned ymask[kRoundWords], nmask[kRoundWords];
+  __shared__ ReconRec rec[kReconRound];
+  __shared__ unsigned ymask[kReconWords], nmask[kReconWords];
   __shared__ int s_used;
   const int s = blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -1157,8 +1161,8 @@ __global__ void __launch_bounds__(kRound) k_recon_sweep(const SysConst *__restri
   const SysConst &sc = scs[s];
   if (!recon_step(sc, dyn[s]) || walled(sc)) return;
   const int base = sc.base;
-  for (int q = tid; q < RoundTouched::kCap; q += kRound) tkeys[q] = 0;
-  for (int q = tid; q < kMapCap; q += kRound) mkey[q] = 0;
+  for (int q = tid; q < RoundTouched::kCap; q += kReconRound) tkeys[q] = 0;
+  for (int q = tid; q < kMapCap; q += kReconRound) mkey[q] = 0;
   RoundTouched tc{tkeys, 0, 0, base};
   const CandMap map{mkey, midx};
   EventStage es{ebuf, 0, ev, ev_count, ev_cap};
@@ -1166,8 +1170,8 @@ __global__ void __launch_bounds__(kRound) k_recon_sweep(const SysConst *__restri
   Tally d = Tally::of(dyn[s], base);  // thread 0 applies the events
   const double half_delta = sc.delta / 2.;
   __syncthreads();
-  for (int c0 = li; c0 < le; c0 += kRound) {
-    const int n = min(kRound, le - c0);
+  for (int c0 = li; c0 < le; c0 += kReconRound) {
+    const int n = min(kReconRound, le - c0);
     ReconRec r{0, -1, 0, 0, 0, 0, 0, 0, 0, 0};
     if (tid < n) {
       const int i = list_a[c0 + tid];
@@ -1258,8 +1262,8 @@ __global__ void __launch_bounds__(kRound) k_recon_sweep(const SysConst *__restri
     }
     __syncthreads();
     if (s_used)
-      for (int q = tid; q < RoundTouched::kCap; q += kRound) tkeys[q] = 0;
-    for (int q = tid; q < kMapCap; q += kRound) mkey[q] = 0;
+      for (int q = tid; q < RoundTouched::kCap; q += kReconRound) tkeys[q] = 0;
+    for (int q = tid; q < kMapCap; q += kReconRound) mkey[q] = 0;
     __syncthreads();
   }
   if (tid == 0) {
@@ -2008,7 +2012,7 @@ void launch_precon(nv_handle *h) {
   k_mark_recon<<<grid_for(h->T + 1, TB), TB, 0, h->stream>>>(h->d_sc, h->d_dyn, h->sys_of, h->closestd, h->nxt,
                                                               tb->flag_a, h->T, h->d_err);
   compact(h, tb->flag_a, tb->pos_a, tb->list_a);
-  k_recon_sweep<<<h->nsys, kRound, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a, tb->list_a,
+  k_recon_sweep<<<h->nsys, kReconRound, 0, h->stream>>>(h->d_sc, h->d_dyn, h->nsys, make_state(h), tb->pos_a, tb->list_a,
                                                h->d_err, h->d_events, h->d_event_count, h->event_cap);
   launch_solid_precon(h);
 }
