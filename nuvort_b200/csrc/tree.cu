@@ -839,15 +839,22 @@ __global__ void __launch_bounds__(128) k_node_sums_big(const double *__restrict_
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   const int n = tb.ctr[0];
-  for (int id = nsys + warp; id < n; id += nwarps) {
-    const int2 R = tb.nR[id];
-    if (R.y <= kSmallNode || R.y > kBlockSumNode) continue;
-    double acc;
-    warp_node_sums(X, GI, T, tb.members + R.x, R.y, true, sm[wl], lane, acc);
-    const double cx = __shfl_sync(0xffffffffu, acc, 0), cy = __shfl_sync(0xffffffffu, acc, 1),
-                 cz = __shfl_sync(0xffffffffu, acc, 2), qx = __shfl_sync(0xffffffffu, acc, 3),
-                 qy = __shfl_sync(0xffffffffu, acc, 4), qz = __shfl_sync(0xffffffffu, acc, 5);
-    if (lane == 0) finish_node(tb, id, false, cx, cy, cz, qx, qy, qz, nxt, err);
+  // The warp's nodes are ids nsys + warp + j nwarps (consecutive ids, often one level's
+  // nodes of similar size, go to different warps); their records are read 32 at a time and
+  // the ones in this kernel's size range summed in turn.
+  for (long long j0 = 0; nsys + warp + j0 * nwarps < n; j0 += 32) {
+    const long long idl = nsys + warp + (j0 + lane) * nwarps;
+    const int2 Rl = idl < n ? tb.nR[idl] : make_int2(0, 0);
+    for (unsigned m = __ballot_sync(0xffffffffu, Rl.y > kSmallNode && Rl.y <= kBlockSumNode); m; m &= m - 1) {
+      const int l = __ffs(m) - 1;
+      const int2 R = make_int2(__shfl_sync(0xffffffffu, Rl.x, l), __shfl_sync(0xffffffffu, Rl.y, l));
+      double acc;
+      warp_node_sums(X, GI, T, tb.members + R.x, R.y, true, sm[wl], lane, acc);
+      const double cx = __shfl_sync(0xffffffffu, acc, 0), cy = __shfl_sync(0xffffffffu, acc, 1),
+                   cz = __shfl_sync(0xffffffffu, acc, 2), qx = __shfl_sync(0xffffffffu, acc, 3),
+                   qy = __shfl_sync(0xffffffffu, acc, 4), qz = __shfl_sync(0xffffffffu, acc, 5);
+      if (lane == 0) finish_node(tb, (int)(nsys + warp + (j0 + l) * nwarps), false, cx, cy, cz, qx, qy, qz, nxt, err);
+    }
   }
 }
 
