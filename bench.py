@@ -325,6 +325,11 @@ def compare_arms(params, states, args, local, flush, torch, dist, steps, warmup,
     caps = [int(s.pcount * 1.6) + 256 for s in states]
     hm = api.Handle(with_precision(params, args.precision), caps, device=local, states=states)
     hp = api.Handle(with_precision(params, "fp64"), caps, device=local, states=states) if args.compare else None
+    # block shapes of each arm's velocity pass, measured on these systems (velocity passes only)
+    from nuvort_b200.autotune import tune_launch_shapes
+    shapes = {"product": tune_launch_shapes(hm)}
+    if hp is not None:
+        shapes["plain_fp64"] = tune_launch_shapes(hp)
     err = {}
     if hp is not None:
         um = [hm.calc_velocity(s) for s in range(len(states))]
@@ -358,7 +363,7 @@ def compare_arms(params, states, args, local, flush, torch, dist, steps, warmup,
     if dist:
         dist.barrier()
     out = {"pts": pts, "per_step": per_step, "vel_ms": vel_ms, "evals": evals, "tests": tests, "stages": stages,
-           "launches": launches, "clocks": clk.summary(), "err": err, "plain": None}
+           "launches": launches, "clocks": clk.summary(), "err": err, "plain": None, "shapes": shapes}
     if hp is not None:
         ppts, pper, pvel, _, _ = timed_steps(hp, steps, flush, torch)
         # every event of every system, through the device digest (the event log may be full)
@@ -434,6 +439,7 @@ def tangle1m_summary(args, local, flush, torch):
            "value": m["pts"] / (step_ms * 1e-3), "ms_per_step": step_ms / steps,
            "velocity_stage": {"ms_per_step": m["vel_ms"] / steps, "point_evals_per_s": m["pts"] / (m["vel_ms"] * 1e-3)},
            "stage_ms_per_step": {k: round(v, 4) for k, v in m["stages"].items()},
+           "launch_shapes": m["shapes"],
            "roofline": roofline_of(params, states, m, steps, args.precision, local), "clocks": m["clocks"]}
     if m["plain"]:
         p = m["plain"]
@@ -526,6 +532,7 @@ def run_ours(args):
                                "stage alone is in velocity_stage",
                 "velocity_stage": {"ms_per_step": vel_ms / args.steps, "point_evals_per_s": all_pts / (vel_ms * 1e-3)},
                 "stage_ms_per_step": {k: round(v, 4) for k, v in m["stages"].items()},
+                "launch_shapes": m["shapes"],
                 "roofline": roofline_of(params, states, m, args.steps, args.precision, local),
                 "hbm_peak_gbs": peaks.get("hbm_gbs"), "clocks": m["clocks"],
                 "gpu_launches": m["launches"] * args.steps, "per_step_ms": [round(x, 4) for x in m["per_step"]]}

@@ -1,4 +1,5 @@
-"""Autotuner for the batched ensemble: the direct-sum / tree crossover, measured on the device.
+"""Autotuner: the direct-sum / tree crossover of the batched ensemble, and the block shapes of
+the velocity pass (tune_launch_shapes), measured on the device.
 
 A system of N points costs the direct sum 27 N^2 pair terms and the tree walk roughly
 27 N log N node visits plus a tree build, so below some N the direct sum is cheaper.  The
@@ -95,3 +96,51 @@ def tune_crossover(device: int = 0, precision: str = "mixed", delta: float = 0.0
     with open(_CACHE, "w") as f:
         json.dump(allc, f, indent=1)
     return dict(result, cached=False)
+
+
+def _velocity_ms(handle, repeats: int) -> float:
+    """Host-timed velocity pass of every system of `handle` (nv_calc_velocity, which waits for
+    its stream): the fastest of `repeats` after one warm-up."""
+    import time
+    handle.calc_velocity(0)
+    best = float("inf")
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        handle.calc_velocity(0)
+        best = min(best, (time.perf_counter() - t0) * 1e3)
+    return best
+
+
+def tune_launch_shapes(handle, repeats: int = 3) -> Dict:
+    """Block shapes of the velocity pass, measured on `handle`'s own systems, the fastest kept
+    (set on the handle):
+
+    * walk_parts (nv_set_walk_parts) for tree-walk systems: the mixed walk's central image over
+      1, 2, 4 or 8 groups of root children (more, shorter blocks for small systems); the
+      plain FP64 walk's unshifted and shifted images on one or two threads per target;
+    * direct split (nv_set_direct_split) for plain FP64 direct-sum systems: one thread per
+      target (64) or 8, 4, 2, 1 targets per block, each target's terms spread over the block.
+
+    The plain FP64 choices do not change a result (both walk splits and every direct split add
+    the same terms in the reference's order); the mixed walk's parts group its FP32 partial
+    sums differently (within the mixed tolerance).  Runs velocity passes only: the systems'
+    positions and links are unchanged (the next step recomputes the velocities)."""
+    from .abi import NV_PREC_MIXED, NV_VEL_BS, NV_VEL_TREE
+    mixed = any(p.precision == NV_PREC_MIXED for p in handle.params)
+    tree = any(p.velocity == NV_VEL_TREE for p in handle.params)
+    direct = not mixed and any(p.velocity == NV_VEL_BS for p in handle.params)
+    def trial(setter, candidates):
+        ms = {}
+        for c in candidates:
+            setter(c)
+            ms[c] = _velocity_ms(handle, repeats)
+        choice = min(ms, key=ms.get)
+        setter(choice)
+        return {"choice": choice, "ms": ms}
+
+    out: Dict = {}
+    if tree:
+        out["walk_parts"] = trial(handle.set_walk_parts, (1, 2, 4, 8) if mixed else (1, 2))
+    if direct:
+        out["direct_split"] = trial(handle.set_direct_split, (64, 8, 4, 2, 1))
+    return out

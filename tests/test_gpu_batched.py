@@ -66,3 +66,34 @@ def test_autotuned_crossover_is_measured():
     assert len(r["trials"]) == 2
     for t in r["trials"]:
         assert t["direct_ms_per_point"] > 0 and t["tree_ms_per_point"] > 0
+
+
+def _velocities(h, n):
+    return np.concatenate([h.calc_velocity(s) for s in range(n)])
+
+
+def test_launch_shapes_tuned_on_the_handle():
+    # the ensemble's direct-sum and tree systems: the tuner times each candidate shape, keeps
+    # the fastest, and the plain FP64 velocities are bit-identical under the chosen shapes;
+    # the mixed walk's parts regroup FP32 partial sums only (within 1e-7 relative RMS)
+    from nuvort_b200.api import Handle
+    from nuvort_b200.autotune import tune_launch_shapes
+    states, params = _ensemble()
+    caps = [s.pcount + 600 for s in states]
+    with Handle(params, caps, states=states) as h:
+        before = _velocities(h, len(states))
+        r = tune_launch_shapes(h, repeats=1)
+        assert r["walk_parts"]["choice"] in (1, 2) and set(r["walk_parts"]["ms"]) == {1, 2}
+        assert r["direct_split"]["choice"] in (64, 8, 4, 2, 1) and len(r["direct_split"]["ms"]) == 5
+        assert all(v > 0 for v in r["direct_split"]["ms"].values())
+        assert np.array_equal(_velocities(h, len(states)), before)
+    mixed = []
+    for p in params:
+        q = type(p).from_buffer_copy(p)
+        q.precision = 1
+        mixed.append(q)
+    with Handle(mixed, caps, states=states) as h:
+        before = _velocities(h, len(states))
+        r = tune_launch_shapes(h, repeats=1)
+        assert r["walk_parts"]["choice"] in (1, 2, 4, 8) and "direct_split" not in r
+        assert rms_rel(_velocities(h, len(states)), before) <= 1e-7
