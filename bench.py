@@ -213,11 +213,13 @@ def measured_peaks():
         return {}
 
 
-def profile_traffic(kernel: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/traffic.json)."""
+def profile_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch of `kernel` on `workload` from its committed ncu summary
+    (profiles/traffic.json), or None where no capture of that workload exists."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            return json.load(f).get(kernel)
+            entry = json.load(f).get(kernel, {}).get(workload)
+        return dict(entry, workload=workload) if entry else None
     except Exception:
         return None
 
@@ -402,7 +404,7 @@ def margin_report(hm, hp, params, nsys):
             "margin_over_need": (worst / need) if need > 0 else None}
 
 
-def roofline_of(params, states, m, steps, precision, local):
+def roofline_of(params, states, m, steps, precision, local, workload):
     from nuvort_b200 import api
     from nuvort_b200.abi import NV_VEL_BS
     mixed = precision == "mixed"
@@ -417,7 +419,7 @@ def roofline_of(params, states, m, steps, precision, local):
                   "direct_pair_images": pairs, "ms": m["vel_ms"] / steps}
     achieved = flops / (m["vel_ms"] / steps * 1e-3) / 1e12
     return {"bound": "fp32" if mixed else "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": achieved / peak if peak else None, "traffic": profile_traffic(kernel), "kernel": kernel,
+            "frac": achieved / peak if peak else None, "traffic": profile_traffic(kernel, workload), "kernel": kernel,
             "peak_source": ("FP32" if mixed else "FP64") + " FMA rate measured on this GPU by nv_measure_fp"
                            + ("32" if mixed else "64") + "_peak (MEASURED_PEAKS.json covers HBM and bf16 tensor "
                            "only); algorithmic flops = 43 per interaction or pair-image + 12 per opening test; "
@@ -440,7 +442,8 @@ def tangle1m_summary(args, local, flush, torch):
            "velocity_stage": {"ms_per_step": m["vel_ms"] / steps, "point_evals_per_s": m["pts"] / (m["vel_ms"] * 1e-3)},
            "stage_ms_per_step": {k: round(v, 4) for k, v in m["stages"].items()},
            "launch_shapes": m["shapes"],
-           "roofline": roofline_of(params, states, m, steps, args.precision, local), "clocks": m["clocks"]}
+           "roofline": roofline_of(params, states, m, steps, args.precision, local, "tangle1m"),
+           "clocks": m["clocks"]}
     if m["plain"]:
         p = m["plain"]
         out["plain_fp64"] = {"value": p["pts"] / (p["step_ms"] * 1e-3), "ms_per_step": p["step_ms"] / steps,
@@ -533,7 +536,7 @@ def run_ours(args):
                 "velocity_stage": {"ms_per_step": vel_ms / args.steps, "point_evals_per_s": all_pts / (vel_ms * 1e-3)},
                 "stage_ms_per_step": {k: round(v, 4) for k, v in m["stages"].items()},
                 "launch_shapes": m["shapes"],
-                "roofline": roofline_of(params, states, m, args.steps, args.precision, local),
+                "roofline": roofline_of(params, states, m, args.steps, args.precision, local, args.workload),
                 "hbm_peak_gbs": peaks.get("hbm_gbs"), "clocks": m["clocks"],
                 "gpu_launches": m["launches"] * args.steps, "per_step_ms": [round(x, 4) for x in m["per_step"]]}
         if plain:
