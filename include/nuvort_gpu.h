@@ -39,7 +39,8 @@ enum {
   NV_ERR_CUDA = -2,        /* CUDA runtime failure */
   NV_ERR_CAPACITY = -3,    /* pinsert needed a slot beyond the system's capacity */
   NV_ERR_SINGULAR = -4,    /* tree walk met dist<epsilon (src/tree.f90:289-295) */
-  NV_ERR_TREE_DEPTH = -5,  /* octree deeper than NV_TREE_MAX_DEPTH levels */
+  NV_ERR_TREE_DEPTH = -5,  /* octree deeper than NV_TREE_MAX_DEPTH levels, its node buffer
+                              exhausted, or a walk longer than the tree (a malformed tree) */
   NV_ERR_NAN = -6,         /* NaN position (NAN_finder, src/general.f90:172-190) */
   NV_ERR_EMPTY = -7,       /* no live points left (src/line.f90:25-27) */
   NV_ERR_TIMESTEP = -8,    /* dt fails timestep_check (src/initial.f90:169-180) */
