@@ -80,6 +80,13 @@ class TangleSplit:
     def step(self):
         import torch
         live = int(self.h.counters(self.sys).live)  # the same on every rank
+        # every rank checks that: ranks that disagreed would size the all-gather differently
+        # and wait on one another instead of failing
+        agree = torch.tensor([live, -live], dtype=torch.int64, device=self.device)
+        self.dist.all_reduce(agree, op=self.dist.ReduceOp.MAX)
+        if int(agree[0]) != -int(agree[1]):
+            raise RuntimeError(f"TangleSplit: the ranks' live counts differ (from {-int(agree[1])} to "
+                               f"{int(agree[0])}); their states have diverged")
         ranges = split_ranges(live, self.world)
         lo, hi = ranges[self.rank]
         self.h.set_walk_range(self.sys, *walk_range(lo, hi, self.h.capacity[self.sys]))

@@ -170,6 +170,38 @@ def _split_worker(rank, world, port, q):
     dist.destroy_process_group()
 
 
+def _diverged_worker(rank, world, port, q):
+    import datetime
+
+    import torch.distributed as dist
+    from nuvort_b200.dist import TangleSplit
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    h = _FakeTangle(1001 + rank, seed=5)  # the ranks' tangles differ: a diverged state
+    try:
+        TangleSplit(h, 0, dist, device="cpu").step()
+        q.put((rank, "stepped"))
+    except RuntimeError as e:
+        q.put((rank, "refused" if "live counts differ" in str(e) else str(e)))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_tangle_split_refuses_diverged_ranks():
+    # ranks whose live counts differ stop with an error on every rank, before the exchange
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_diverged_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = dict(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+    assert out == {0: "refused", 1: "refused"}
+
+
 def test_tangle_split_over_two_gloo_ranks():
     # each rank computes half of the walk order; after the exchange both hold the full field
     from nuvort_b200.dist import split_ranges
